@@ -1,0 +1,116 @@
+"""ctypes binding of libbsproj.so (the C ABI declared in include/bsproj.h).
+
+The product path has no CPU fallback: if the library is missing or no CUDA
+device is present, every call raises.  Argument conversion accepts torch
+tensors and any object exposing ``__cuda_array_interface__`` (the reference
+passes Warp arrays that way, python/boilingsim/fluid.py:649-652).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libbsproj.so")
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_L = ctypes.c_int64
+_F = ctypes.c_float
+
+# name -> (restype, argtypes); mirrors include/bsproj.h
+SIGNATURES = {
+    # reference-compatible launchers
+    "jacobi_pressure_launch": (_I, [_P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I, _I]),
+    "pressure_solve_launch": (_I, [_P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I, _I, _I]),
+    "laplacian_spmv_launch": (_I, [_P, _P, _P, _I, _I, _I, _I, _I]),
+    "diag_inverse_apply_launch": (_I, [_P, _P, _P, _I, _I, _I, _I, _I]),
+    "dot_launch": (_I, [_P, _P, _I, _P, _P]),
+    "axpy_device_launch": (_I, [_P, _P, _P, _I, _I]),
+    "scaled_axpy_launch": (_I, [_P, _P, _P, _P, _I]),
+    "divide_scalars_launch": (_I, [_P, _P, _P]),
+    "compute_b_launch": (_I, [_P, _P, _P, _I, _I, _I, _F, _I]),
+    "zero_buffer_launch": (_I, [_P, _I]),
+    "scale_inplace_launch": (_I, [_P, _I, _F]),
+    "pressure_solve_pcg_launch": (_I, [_P, _P, _P, _I, _I, _I, _F, _F, _F, _I, _I, _F, _I]
+                                  + [_P] * 13 + [ctypes.POINTER(ctypes.c_int)]),
+    # B200-native
+    "bsp_version": (ctypes.c_char_p, []),
+    "bsp_error_string": (ctypes.c_char_p, [_I]),
+    "bsp_mask_from_mat": (_I, [_P, _P, _I, _I, _I, _I, _I, _P]),
+    "bsp_jacobi_sweep": (_I, [_P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _P]),
+    "bsp_jacobi_solve": (_I, [_P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I, _I, _P]),
+    "bsp_divergence": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _P, _P]),
+    "bsp_subtract_gradient": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _P]),
+    "bsp_enforce_no_slip": (_I, [_P, _P, _P, _P, _I, _I, _I, _P]),
+    "bsp_projection_jacobi": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I, _I,
+                                   _P, _P]),
+    "bsp_spmv": (_I, [_P, _P, _P, _I, _I, _I, _P]),
+    "bsp_selftest_div6": (_I, [_P, _P]),
+}
+
+_lib = None
+
+
+class BspError(RuntimeError):
+    """A non-zero status from the native library (cudaError_t or BSP_ERR_*)."""
+
+    def __init__(self, fn: str, code: int, msg: str):
+        super().__init__(f"{fn} failed with status {code}: {msg}")
+        self.code = code
+
+
+def lib() -> ctypes.CDLL:
+    """Load libbsproj.so once; raise loudly if it is absent (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python boiling-sim_b200/build.py` "
+                "(there is no CPU fallback for the projection path)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(fn: str, code: int) -> None:
+    if code != 0:
+        msg = lib().bsp_error_string(int(code)).decode()
+        raise BspError(fn, int(code), msg)
+
+
+def call(fn: str, *args) -> int:
+    """Call ``fn`` and raise BspError on a non-zero status."""
+    code = getattr(lib(), fn)(*args)
+    if fn not in ("bsp_version", "bsp_error_string"):
+        check(fn, code)
+    return code
+
+
+def ptr(x) -> int:
+    """Device address of a torch tensor / CUDA-array-interface object / int."""
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    if hasattr(x, "data_ptr"):
+        return int(x.data_ptr())
+    cai = getattr(x, "__cuda_array_interface__", None)
+    if cai is not None:
+        return int(cai["data"][0])
+    raise TypeError(f"cannot take a device pointer of {type(x)!r}")
+
+
+def stream_handle(stream=None) -> int:
+    """cudaStream_t of ``stream`` or of torch's current stream."""
+    import torch
+
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)

@@ -1,0 +1,205 @@
+"""Pressure projection on the MAC grid -- host-side mirror of the reference API.
+
+Drop-in for ``python/boilingsim/fluid.py`` (the projection part): the same
+function names, arguments and results, backed by the sm_100a kernels of
+libbsproj.so instead of Warp.  Fields are torch CUDA tensors (or any object
+with ``__cuda_array_interface__`` of the right dtype and layout):
+
+* ``Grid``:  p (nx,ny,nz) f32, mat (nx,ny,nz) int32, ux (nx+1,ny,nz),
+  uy (nx,ny+1,nz), uz (nx,ny,nz+1) f32 -- ``geometry.py:253-314``;
+* ``FluidWorkspace``: div_u, p_tmp (nx,ny,nz) f32 -- ``fluid.py:500-528``.
+
+Solver selection follows ``_select_pressure_solver`` (``fluid.py:585-609``):
+``BOILINGSIM_PRESSURE_SOLVER`` = ``jacobi`` (default; fixed
+``pressure_max_iter`` sweeps), ``cg-rust`` (Jacobi-preconditioned CG to
+``pressure_tol``), ``b200-jacobi`` (the uint8-mask sweep path), and
+``BOILINGSIM_USE_RUST_PRESSURE=1`` selects the fused fixed-count Jacobi
+launcher.  Every back-end runs on the GPU; there is no CPU path.
+"""
+from __future__ import annotations
+
+import os
+from dataclasses import dataclass, field
+
+import torch
+
+from . import _lib
+from ._lib import call, ptr, stream_handle
+
+MAT_FLUID, MAT_POT_WALL, MAT_AIR, MAT_CARROT = 0, 1, 2, 3
+
+
+@dataclass
+class SolverConfig:
+    """The projection knobs of ``config.py:161-182``."""
+
+    pressure_tol: float = 1e-5
+    pressure_max_iter: int = 200
+
+
+@dataclass
+class ScenarioConfig:
+    """The part of ``ScenarioConfig`` (``config.py:808``) the projection reads."""
+
+    solver: SolverConfig = field(default_factory=SolverConfig)
+
+
+@dataclass
+class Grid:
+    nx: int
+    ny: int
+    nz: int
+    dx: float
+    p: torch.Tensor
+    mat: torch.Tensor
+    ux: torch.Tensor
+    uy: torch.Tensor
+    uz: torch.Tensor
+    mask: torch.Tensor | None = None  # uint8 cell classes, derived once from mat
+
+    @property
+    def shape(self):
+        return (self.nx, self.ny, self.nz)
+
+    @classmethod
+    def from_numpy(cls, mat, ux, uy, uz, dx, device="cuda:0"):
+        nx, ny, nz = mat.shape
+        t = lambda a, dt: torch.as_tensor(a, dtype=dt).contiguous().to(device)  # noqa: E731
+        return cls(nx, ny, nz, float(dx), torch.zeros((nx, ny, nz), dtype=torch.float32,
+                                                      device=device),
+                   t(mat, torch.int32), t(ux, torch.float32), t(uy, torch.float32),
+                   t(uz, torch.float32))
+
+
+@dataclass
+class FluidWorkspace:
+    div_u: torch.Tensor
+    p_tmp: torch.Tensor
+    max_div: torch.Tensor  # (1,) device float: max|div| of the last projection
+
+
+def allocate_fluid_workspace(grid: Grid, device: str = "cuda:0") -> FluidWorkspace:
+    shp = grid.shape
+    return FluidWorkspace(torch.zeros(shp, dtype=torch.float32, device=device),
+                          torch.zeros(shp, dtype=torch.float32, device=device),
+                          torch.zeros(1, dtype=torch.float32, device=device))
+
+
+def cell_mask(mat: torch.Tensor, mat_fluid: int = MAT_FLUID, mat_air: int = MAT_AIR,
+              stream=None) -> torch.Tensor:
+    """uint8 cell mask of an int32 material grid: class (0 fluid, 1 air,
+    2 solid) in bits 0-1, number of solid face neighbours in bits 2-4."""
+    if mat.dtype != torch.int32 or not mat.is_contiguous():
+        raise TypeError("mat must be a contiguous int32 CUDA tensor")
+    out = torch.empty(mat.shape, dtype=torch.uint8, device=mat.device)
+    nx, ny, nz = mat.shape
+    call("bsp_mask_from_mat", ptr(out), ptr(mat), nx, ny, nz, mat_fluid, mat_air,
+         stream_handle(stream))
+    return out
+
+
+def grid_mask(grid: Grid) -> torch.Tensor:
+    if grid.mask is None:
+        grid.mask = cell_mask(grid.mat)
+    return grid.mask
+
+
+def _select_pressure_solver() -> str:
+    """``fluid.py:585-609`` with the B200 back-ends added."""
+    use_rust_jacobi = os.environ.get("BOILINGSIM_USE_RUST_PRESSURE") == "1"
+    solver = os.environ.get("BOILINGSIM_PRESSURE_SOLVER", "jacobi").lower()
+    valid = ("jacobi", "cg-rust", "b200-jacobi")
+    if solver not in valid:
+        raise ValueError(f"BOILINGSIM_PRESSURE_SOLVER={solver!r} is not recognised; "
+                         f"valid values are {', '.join(repr(v) for v in valid)}.")
+    if use_rust_jacobi and solver == "cg-rust":
+        raise ValueError("BOILINGSIM_USE_RUST_PRESSURE=1 and BOILINGSIM_PRESSURE_SOLVER=cg-rust "
+                         "are mutually exclusive -- they route through different code paths.")
+    if solver == "cg-rust":
+        return "cg-rust"
+    if use_rust_jacobi:
+        return "rust-jacobi"
+    return solver
+
+
+# ---------------------------------------------------------------------------
+# kernel-level calls (Warp kernel signatures of fluid.py, launched on torch's
+# current stream)
+# ---------------------------------------------------------------------------
+
+def compute_divergence(div_u, ux, uy, uz, mask, dx, max_abs_div=None, stream=None):
+    nx, ny, nz = div_u.shape
+    call("bsp_divergence", ptr(div_u), ptr(ux), ptr(uy), ptr(uz), ptr(mask), nx, ny, nz,
+         float(dx), ptr(max_abs_div), stream_handle(stream))
+
+
+def jacobi_pressure_step(p_new, p_old, div_u, mat, dx, dt, rho, mat_fluid=MAT_FLUID,
+                         mat_air=MAT_AIR, stream=None):
+    """One sweep.  ``mat`` may be the int32 material grid (reference layout) or
+    the uint8 class mask."""
+    nx, ny, nz = p_new.shape
+    if mat.dtype == torch.uint8:
+        call("bsp_jacobi_sweep", ptr(p_new), ptr(p_old), ptr(div_u), ptr(mat), nx, ny, nz,
+             float(dx), float(dt), float(rho), stream_handle(stream))
+    else:
+        # reference launcher: legacy default stream, as jacobi_pressure.cu:203
+        call("jacobi_pressure_launch", ptr(p_new), ptr(p_old), ptr(div_u), ptr(mat), nx, ny,
+             nz, float(dx), float(dt), float(rho), mat_fluid, mat_air)
+
+
+def subtract_pressure_gradient(ux, uy, uz, p, mask, dx, dt, rho, stream=None):
+    nx, ny, nz = p.shape
+    call("bsp_subtract_gradient", ptr(ux), ptr(uy), ptr(uz), ptr(p), ptr(mask), nx, ny, nz,
+         float(dx), float(dt), float(rho), stream_handle(stream))
+
+
+def enforce_no_slip(grid: Grid, device: str = "cuda:0", stream=None) -> None:
+    """``fluid.py:154-165``."""
+    call("bsp_enforce_no_slip", ptr(grid.ux), ptr(grid.uy), ptr(grid.uz), ptr(grid_mask(grid)),
+         grid.nx, grid.ny, grid.nz, stream_handle(stream))
+
+
+# ---------------------------------------------------------------------------
+# the projection (fluid.py:612-734)
+# ---------------------------------------------------------------------------
+
+def pressure_projection(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, dt: float,
+                        rho: float, device: str = "cuda:0") -> float:
+    """Enforce incompressibility: solve the pressure Poisson problem, correct u.
+
+    Returns max |div u| after the correction (a diagnostic), as the reference.
+    The reference reads the whole divergence field back to the host for this
+    (fluid.py:733-734); here it is reduced on the device and 4 bytes are read.
+    """
+    nx, ny, nz = grid.shape
+    dx = float(grid.dx)
+    mask = grid_mask(grid)
+    s = stream_handle()
+    solver = _select_pressure_solver()
+    n_iter = int(cfg.solver.pressure_max_iter)
+    if solver in ("jacobi", "b200-jacobi"):
+        call("bsp_projection_jacobi", ptr(grid.p), ptr(ws.p_tmp), ptr(ws.div_u), ptr(grid.ux),
+             ptr(grid.uy), ptr(grid.uz), ptr(mask), nx, ny, nz, dx, float(dt), float(rho),
+             n_iter, 0, ptr(ws.max_div), s)
+    else:
+        grid.p.zero_()
+        ws.p_tmp.zero_()
+        compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, mask, dx)
+        # the reference launchers run on the legacy default stream
+        torch.cuda.current_stream().synchronize()
+        if solver == "rust-jacobi":
+            call("pressure_solve_launch", ptr(grid.p), ptr(ws.p_tmp), ptr(ws.div_u),
+                 ptr(grid.mat), nx, ny, nz, dx, float(dt), float(rho), n_iter, MAT_FLUID,
+                 MAT_AIR)
+        else:
+            from .sim_core import pcg_workspace, SimCore
+            w = pcg_workspace(grid.shape, grid.p.device)
+            SimCore(0).pressure_solve_pcg(
+                ptr(grid.p), ptr(ws.div_u), ptr(grid.mat), nx, ny, nz, dx, float(dt),
+                float(rho), float(cfg.solver.pressure_tol), n_iter, *[ptr(w[k]) for k in (
+                    "b", "r", "z", "p_search", "Ap", "dot_ws", "alpha", "beta", "rzold",
+                    "rznew", "bsq", "rsq", "pAp")], MAT_FLUID, MAT_AIR)
+        torch.cuda.synchronize()
+        subtract_pressure_gradient(grid.ux, grid.uy, grid.uz, grid.p, mask, dx, dt, rho)
+        compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, mask, dx, ws.max_div)
+    return float(ws.max_div.item())

@@ -1,0 +1,79 @@
+// bsp_common.cuh -- shared device helpers for the B200 pressure-projection library.
+//
+// Grid layout (identical to the reference, crates/cuda-kernels/src/jacobi_pressure.cu:16-18):
+// cell (i, j, k) of an (nx, ny, nz) field lives at (i*ny + j)*nz + k, k fastest.
+// MAC faces: ux (nx+1, ny, nz), uy (nx, ny+1, nz), uz (nx, ny, nz+1).
+//
+// Cell classes.  The reference passes an int32 material id per cell plus the
+// two ids it treats specially (mat_fluid, mat_air); every other id is a solid
+// (python/boilingsim/fluid.py:222-240).  The product path stores one byte per
+// cell instead: BSP_FLUID / BSP_AIR / BSP_SOLID.  Cells outside the grid are
+// air (jacobi_pressure.cu:121-124).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "../../include/bsproj.h"
+
+#define BSP_FLUID 0
+#define BSP_AIR 1
+#define BSP_SOLID 2
+
+namespace bsp {
+
+__device__ __forceinline__ int64_t idx3(int i, int j, int k, int ny, int nz) {
+  return ((int64_t)i * ny + j) * nz + k;
+}
+
+// uint8 mask byte: bits 0-1 cell class, bits 2-4 number of solid face
+// neighbours (the Jacobi preconditioner's 6 - n_solid, diag_inverse_apply.cu:62-78).
+__device__ __forceinline__ uint32_t mcls(uint32_t mbyte) { return mbyte & 3u; }
+__device__ __forceinline__ uint32_t mnsolid(uint32_t mbyte) { return (mbyte >> 2) & 7u; }
+
+__device__ __forceinline__ uint32_t classify(int m, int mat_fluid, int mat_air) {
+  return m == mat_fluid ? BSP_FLUID : (m == mat_air ? BSP_AIR : BSP_SOLID);
+}
+
+// Neighbour value under the mixed boundary rule: fluid -> its pressure,
+// air (free surface) -> 0 (Dirichlet), solid -> p_self (Neumann ghost).
+__device__ __forceinline__ float nbr(uint32_t cls, float p_n, float p_self) {
+  return cls == BSP_FLUID ? p_n : (cls == BSP_AIR ? 0.0f : p_self);
+}
+
+// Correctly rounded x / 6 in three instructions.  Method: the
+// Markstein-style correction for a divisor known in advance (Brisebarre,
+// Muller, Raina, "Accelerating correctly rounded floating-point division when
+// the divisor is known in advance", IEEE Trans. Computers 53(8), 2004):
+// q0 = RN(x z) with z = RN(1/6), r = x - 6 q0 (exact by fma), q = RN(q0 + r z).
+// Verified bit-identical to IEEE x / 6 for every one of the 2^32 float
+// inputs once results below 8 * FLT_MIN, signed zero, inf and NaN take the
+// IEEE division (the exhaustive check is bsp_selftest_div6 and the CPU test).
+__device__ __forceinline__ float div6(float x) {
+  const float z = 0.16666667163372039795f;  // RN(1/6)
+  const float ax = fabsf(x);
+  if (!(ax >= 0x1p-120f && ax <= 3.40282347e38f)) return __fdiv_rn(x, 6.0f);
+  const float q0 = __fmul_rn(x, z);
+  const float r = __fmaf_rn(-q0, 6.0f, x);
+  return __fmaf_rn(r, z, q0);
+}
+
+// One Jacobi update of a fluid cell with the reference's exact operation
+// order (fluid.py:273-276): s = l + r + d + u + b + f left to right,
+// rhs = rho*dx*dx*div/dt, p = (s - rhs)/6.  rdd = (rho*dx)*dx.
+__device__ __forceinline__ float jacobi_update(float l, float r, float d, float u, float b,
+                                               float f, float div, float rdd, float dt) {
+  float s = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(l, r), d), u), b), f);
+  float rhs = __fdiv_rn(__fmul_rn(rdd, div), dt);
+  return div6(__fsub_rn(s, rhs));
+}
+
+// A p for a fluid cell, laplacian_spmv.cu:140: 6 p_self - s, contracted to one
+// fma as the reference's default nvcc build does.
+__device__ __forceinline__ float spmv_update(float l, float r, float d, float u, float b,
+                                             float f, float ps) {
+  float s = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(l, r), d), u), b), f);
+  return __fmaf_rn(6.0f, ps, -s);
+}
+
+__device__ __forceinline__ uint32_t byte_of(uint32_t w, int q) { return (w >> (8 * q)) & 0xffu; }
+
+}  // namespace bsp

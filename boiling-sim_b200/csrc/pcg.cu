@@ -1,0 +1,287 @@
+// pcg.cu -- Jacobi-preconditioned conjugate gradient as ONE persistent kernel.
+//
+// Algorithm: crates/cuda-kernels/src/pressure_solve_pcg.cu:89-243 --
+//   b = -(rho dx^2/dt) div on fluid cells; p = 0; r = b; z = D^-1 r; ps = z;
+//   loop: Ap = A ps; alpha = rz/pAp; p += alpha ps; r -= alpha Ap;
+//         [it >= 8, it % 5 == 0: stop if r.r < tol^2 b.b]
+//         z = D^-1 r; beta = rz_new/rz; ps = z + beta ps.
+// with A = 6I - S (laplacian_spmv.cu:62-143) and D = 6 - n_solid
+// (diag_inverse_apply.cu:44-89).
+//
+// B200 design: the reference issues ~10 launches and a blocking device->host
+// copy per check; here one cooperative launch runs the whole loop.  Each
+// iteration is two grid-wide phases separated by bounded grid barriers:
+//   A: ps = z + beta ps_prev is formed on the fly (centre and neighbours), the
+//      stencil A ps is applied and stored with ps; partial ps.Ap.
+//   B: p, r, z updated elementwise; partial r.z and r.r.
+// All inner products are FP64 with a fixed reduction order (deterministic for a
+// given grid size).  Vector arithmetic stays FP32 with the reference's
+// expressions (y = fma(a, x, y)).
+// Work unit: one (i, j) row of nz cells per warp, lanes striding over k.
+#include "grid_sync.cuh"
+
+namespace bsp {
+
+int num_sms();
+
+constexpr int PCG_THREADS = 512;
+
+template <class MaskT>
+struct PcgArgs {
+  float *p;
+  const float *div;
+  const MaskT *mask;
+  float *r, *z, *ps0, *ps1, *Ap;
+  double *partials;  // 3 * stride doubles
+  GridCtl *ctl;
+  float *outs[7];  // optional device floats: alpha beta rzold rznew bsq rsq pAp
+  int nx, ny, nz, mf, ma, max_iter, stride;
+  float scale;   // -(rho dx dx)/dt as float
+  double tol2;   // tol^2
+};
+
+__device__ __forceinline__ uint32_t pcg_cls(const uint8_t *m, int64_t c, int, int) {
+  return mcls(__ldg(m + c));
+}
+__device__ __forceinline__ uint32_t pcg_cls(const int32_t *m, int64_t c, int mf, int ma) {
+  return classify(__ldg(m + c), mf, ma);
+}
+__device__ __forceinline__ int pcg_nsolid(const uint8_t *m, int64_t c, int, int, int, int, int,
+                                          int, int, int) {
+  return (int)mnsolid(__ldg(m + c));
+}
+__device__ __forceinline__ int pcg_nsolid(const int32_t *m, int64_t c, int i, int j, int k,
+                                          int nx, int ny, int nz, int mf, int ma) {
+  const int64_t plane = (int64_t)ny * nz;
+  int ns = 0;
+#define SOL(cond, off) ns += ((cond) && classify(__ldg(m + c + (off)), mf, ma) == BSP_SOLID) ? 1 : 0
+  SOL(i > 0, -plane);
+  SOL(i + 1 < nx, plane);
+  SOL(j > 0, -(int64_t)nz);
+  SOL(j + 1 < ny, (int64_t)nz);
+  SOL(k > 0, -1);
+  SOL(k + 1 < nz, 1);
+#undef SOL
+  return ns;
+}
+
+__device__ __forceinline__ float dinv_apply(float r, int ns) {
+  const float d = 6.0f - (float)ns;
+  return d <= 0.0f ? r : __fdiv_rn(r, d);
+}
+
+template <class MaskT>
+__global__ void __launch_bounds__(PCG_THREADS) pcg_persistent_kernel(PcgArgs<MaskT> a) {
+  __shared__ double sh[32 * 3];
+  const int lane = threadIdx.x & 31;
+  const int gw = blockIdx.x * (PCG_THREADS / 32) + (threadIdx.x >> 5);
+  const int tw = gridDim.x * (PCG_THREADS / 32);
+  const int nx = a.nx, ny = a.ny, nz = a.nz, mf = a.mf, ma = a.ma;
+  const int64_t rows = (int64_t)nx * ny;
+  const int64_t plane = (int64_t)ny * nz;
+
+  // ---- init: b, r = b, z = D^-1 r, p = 0; partial b.b and r.z ------------------
+  {
+    double v[2] = {0.0, 0.0};
+    for (int64_t u = gw; u < rows; u += tw) {
+      const int i = (int)(u / ny), j = (int)(u - (int64_t)(u / ny) * ny);
+      const int64_t base = u * nz;
+      for (int k = lane; k < nz; k += 32) {
+        const int64_t c = base + k;
+        float b = 0.0f, z = 0.0f;
+        if (pcg_cls(a.mask, c, mf, ma) == BSP_FLUID) {
+          b = __fmul_rn(a.scale, __ldg(a.div + c));
+          z = dinv_apply(b, pcg_nsolid(a.mask, c, i, j, k, nx, ny, nz, mf, ma));
+        }
+        a.r[c] = b;
+        a.z[c] = z;
+        a.p[c] = 0.0f;
+        v[0] += (double)b * (double)b;
+        v[1] += (double)b * (double)z;
+      }
+    }
+    block_partials<2>(v, a.partials, a.stride, sh);
+  }
+  if (!grid_barrier(a.ctl)) return;
+  double tot[3];
+  {
+    double t2[2];
+    grid_totals<2>(a.partials, a.stride, t2, sh);
+    tot[0] = t2[0];
+    tot[1] = t2[1];
+  }
+  const double bsq = tot[0];
+  double rz = tot[1];
+  double alpha = 0.0, beta = 0.0, rz_new = 0.0, rsq = bsq, pAp = 0.0;
+  int iters = 0;
+  int status = BSP_OK;
+  if (!(bsq == bsq) || bsq > 1.0e300) status = BSP_ERR_NONFINITE;
+  if (status == BSP_OK && bsq != 0.0) {
+    const double tol_sq_bsq = a.tol2 * bsq;
+    int it = 0;
+    for (it = 0; it < a.max_iter; ++it) {
+      float *cur = (it & 1) ? a.ps1 : a.ps0;
+      const float *prev = (it & 1) ? a.ps0 : a.ps1;
+      const float bf = (float)beta;
+      const bool first = (it == 0);
+      // ---- phase A: ps = z + beta ps_prev; Ap = A ps; partial ps.Ap -------------
+      {
+        double v[1] = {0.0};
+        for (int64_t u = gw; u < rows; u += tw) {
+          const int i = (int)(u / ny), j = (int)(u - (int64_t)(u / ny) * ny);
+          const int64_t base = u * nz;
+          for (int k = lane; k < nz; k += 32) {
+            const int64_t c = base + k;
+            if (pcg_cls(a.mask, c, mf, ma) != BSP_FLUID) {
+              cur[c] = 0.0f;
+              a.Ap[c] = 0.0f;
+              continue;
+            }
+            // z and ps are written inside this kernel: plain (coherent) loads,
+            // never the read-only __ldg path.
+#define PS(x) (first ? a.z[(x)] : __fmaf_rn(bf, prev[(x)], a.z[(x)]))
+            const float psc = PS(c);
+#define NB(cond, off)                                                         \
+  ((cond) ? ([&]() {                                                          \
+    const uint32_t cn = pcg_cls(a.mask, c + (off), mf, ma);                   \
+    return cn == BSP_FLUID ? PS(c + (off)) : (cn == BSP_AIR ? 0.0f : psc);    \
+  })()                                                                        \
+          : 0.0f)
+            const float l = NB(i > 0, -plane), rr = NB(i + 1 < nx, plane);
+            const float d = NB(j > 0, -(int64_t)nz), up = NB(j + 1 < ny, (int64_t)nz);
+            const float bk = NB(k > 0, -1), f = NB(k + 1 < nz, 1);
+#undef NB
+#undef PS
+            const float ap = spmv_update(l, rr, d, up, bk, f, psc);
+            cur[c] = psc;
+            a.Ap[c] = ap;
+            v[0] += (double)psc * (double)ap;
+          }
+        }
+        block_partials<1>(v, a.partials, a.stride, sh);
+      }
+      if (!grid_barrier(a.ctl)) return;
+      {
+        double t1[1];
+        grid_totals<1>(a.partials, a.stride, t1, sh);
+        pAp = t1[0];
+      }
+      alpha = (pAp == 0.0) ? 0.0 : rz / pAp;
+      const float af = (float)alpha;
+      // ---- phase B: p += alpha ps; r -= alpha Ap; z = D^-1 r; partial r.z, r.r --
+      {
+        double v[2] = {0.0, 0.0};
+        for (int64_t u = gw; u < rows; u += tw) {
+          const int i = (int)(u / ny), j = (int)(u - (int64_t)(u / ny) * ny);
+          const int64_t base = u * nz;
+          for (int k = lane; k < nz; k += 32) {
+            const int64_t c = base + k;
+            if (pcg_cls(a.mask, c, mf, ma) != BSP_FLUID) continue;
+            const float pc = __fmaf_rn(af, cur[c], a.p[c]);
+            const float rc = __fmaf_rn(-af, a.Ap[c], a.r[c]);
+            const float zc = dinv_apply(rc, pcg_nsolid(a.mask, c, i, j, k, nx, ny, nz, mf, ma));
+            a.p[c] = pc;
+            a.r[c] = rc;
+            a.z[c] = zc;
+            v[0] += (double)rc * (double)zc;
+            v[1] += (double)rc * (double)rc;
+          }
+        }
+        block_partials<2>(v, a.partials + a.stride, a.stride, sh);
+      }
+      if (!grid_barrier(a.ctl)) return;
+      {
+        double t2[2];
+        grid_totals<2>(a.partials + a.stride, a.stride, t2, sh);
+        rz_new = t2[0];
+        rsq = t2[1];
+      }
+      if (it >= 8 && (it % 5) == 0 && rsq < tol_sq_bsq) {
+        ++it;
+        break;
+      }
+      beta = (rz == 0.0) ? 0.0 : rz_new / rz;
+      rz = rz_new;
+    }
+    iters = it;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.ctl->iters = iters;
+    a.ctl->status = status;
+    const double vals[7] = {alpha, beta, rz, rz_new, bsq, rsq, pAp};
+#pragma unroll
+    for (int q = 0; q < 7; ++q)
+      if (a.outs[q]) *a.outs[q] = (float)vals[q];
+  }
+}
+
+template <class MaskT>
+static cudaError_t launch_pcg(PcgArgs<MaskT> &a, int max_blocks, cudaStream_t s) {
+  int occ = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &occ, pcg_persistent_kernel<MaskT>, PCG_THREADS, 0);
+  if (e != cudaSuccess) return e;
+  if (occ <= 0) return cudaErrorCooperativeLaunchTooLarge;
+  int nb = occ * num_sms();
+  if (nb > max_blocks) nb = max_blocks;
+  const int64_t rows = (int64_t)a.nx * a.ny;
+  const int64_t need = (rows + (PCG_THREADS / 32) - 1) / (PCG_THREADS / 32);
+  if (need < nb) nb = (int)(need > 0 ? need : 1);
+  a.stride = nb;
+  void *args[] = {&a};
+  return cudaLaunchCooperativeKernel((const void *)pcg_persistent_kernel<MaskT>, dim3(nb),
+                                     dim3(PCG_THREADS), args, 0, s);
+}
+
+// dot_workspace layout (>= 4096 bytes): [0,64) GridCtl, [64, 64 + 8*3*nb) partials
+constexpr int COMPAT_MAX_BLOCKS = (4096 - 64) / 24;
+
+}  // namespace bsp
+
+using namespace bsp;
+
+extern "C" cudaError_t pressure_solve_pcg_launch(
+    float *p_out, const float *div_u, const int *mat, int nx, int ny, int nz, float dx, float dt,
+    float rho, int mat_fluid, int mat_air, float pressure_tol, int max_iter, float *ws_b,
+    float *ws_r, float *ws_z, float *ws_p_search, float *ws_Ap, float *dot_workspace,
+    float *dev_alpha, float *dev_beta, float *dev_rzold, float *dev_rznew, float *dev_bsq,
+    float *dev_rsq, float *dev_pAp, int *iter_count_host) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) {
+    if (iter_count_host) *iter_count_host = 0;
+    return cudaSuccess;
+  }
+  if (((uintptr_t)dot_workspace & 7u) != 0) return cudaErrorInvalidValue;
+  GridCtl *ctl = reinterpret_cast<GridCtl *>(dot_workspace);
+  cudaError_t e = cudaMemsetAsync(ctl, 0, sizeof(GridCtl), 0);
+  if (e != cudaSuccess) return e;
+  PcgArgs<int32_t> a{};
+  a.p = p_out;
+  a.div = div_u;
+  a.mask = mat;
+  a.r = ws_r;
+  a.z = ws_z;
+  a.ps0 = ws_p_search;
+  a.ps1 = ws_b;  // b is not needed after the first pass: it holds the second search buffer
+  a.Ap = ws_Ap;
+  a.partials = reinterpret_cast<double *>(reinterpret_cast<char *>(dot_workspace) + 64);
+  a.ctl = ctl;
+  float *dst[7] = {dev_alpha, dev_beta, dev_rzold, dev_rznew, dev_bsq, dev_rsq, dev_pAp};
+  for (int q = 0; q < 7; ++q) a.outs[q] = dst[q];
+  a.nx = nx;
+  a.ny = ny;
+  a.nz = nz;
+  a.mf = mat_fluid;
+  a.ma = mat_air;
+  a.max_iter = max_iter < 0 ? 0 : max_iter;
+  a.scale = -rho * dx * dx / dt;  // pressure_solve_pcg.cu:137 evaluation order
+  a.tol2 = (double)pressure_tol * (double)pressure_tol;
+  e = launch_pcg<int32_t>(a, COMPAT_MAX_BLOCKS, 0);
+  if (e != cudaSuccess) return e;
+  GridCtl h{};
+  e = cudaMemcpy(&h, ctl, sizeof(GridCtl), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return e;
+  if (h.err != 0) return (cudaError_t)h.err;
+  if (h.status != 0) return (cudaError_t)h.status;
+  if (iter_count_host) *iter_count_host = h.iters;
+  return cudaGetLastError();
+}

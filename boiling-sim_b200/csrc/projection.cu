@@ -1,0 +1,206 @@
+// projection.cu -- divergence, gradient subtract, no-slip and the Jacobi projection.
+//
+// Reference semantics:
+//   compute_divergence                 python/boilingsim/fluid.py:201-218
+//   subtract_pressure_gradient_{x,y,z} python/boilingsim/fluid.py:279-330
+//   enforce_no_slip_{ux,uy,uz}         python/boilingsim/fluid.py:111-165
+//   pressure_projection (sequence)     python/boilingsim/fluid.py:612-734
+//
+// The reference ends every projection with a full-field device->host copy of
+// the diagnostic divergence to take max|div| on the host (fluid.py:733-734);
+// here the diagnostic kernel reduces max|div| on the device and only 4 bytes
+// are left for the caller to read.
+#include "bsp_common.cuh"
+
+namespace bsp {
+
+int num_sms();
+template <int OP, class MaskT>
+cudaError_t launch_stencil(float *out, const float *p, const float *div, const MaskT *mask,
+                           int nx, int ny, int nz, float dx, float dt, float rho, int mf,
+                           int ma, cudaStream_t s);
+int jacobi_solve_impl(float *p, float *p_tmp, const float *div_u, const uint8_t *mask, int nx,
+                      int ny, int nz, float dx, float dt, float rho, int n_iter, int tblock,
+                      cudaStream_t stream);
+
+// Block = (128 k, 2 j); grid = (k tiles, j tiles, i).  One cell per thread.
+__global__ void __launch_bounds__(256) divergence_kernel(
+    float *__restrict__ div, const float *__restrict__ ux, const float *__restrict__ uy,
+    const float *__restrict__ uz, const uint8_t *__restrict__ mask, int nx, int ny, int nz,
+    float dx, unsigned int *__restrict__ max_bits) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  float a = 0.0f;
+  if (k < nz && j < ny) {
+    const int64_t c = idx3(i, j, k, ny, nz);
+    float v = 0.0f;
+    if (mcls(__ldg(mask + c)) == BSP_FLUID) {
+      const float u1 = __ldg(ux + ((int64_t)(i + 1) * ny + j) * nz + k);
+      const float u0 = __ldg(ux + ((int64_t)i * ny + j) * nz + k);
+      const float v1 = __ldg(uy + ((int64_t)i * (ny + 1) + j + 1) * nz + k);
+      const float v0 = __ldg(uy + ((int64_t)i * (ny + 1) + j) * nz + k);
+      const float w1 = __ldg(uz + ((int64_t)i * ny + j) * (nz + 1) + k + 1);
+      const float w0 = __ldg(uz + ((int64_t)i * ny + j) * (nz + 1) + k);
+      const float dudx = __fdiv_rn(__fsub_rn(u1, u0), dx);
+      const float dvdy = __fdiv_rn(__fsub_rn(v1, v0), dx);
+      const float dwdz = __fdiv_rn(__fsub_rn(w1, w0), dx);
+      v = __fadd_rn(__fadd_rn(dudx, dvdy), dwdz);
+    }
+    div[c] = v;
+    a = fabsf(v);
+  }
+  if (max_bits) {
+    // |div| >= 0, so its bit pattern orders like the value.
+    unsigned int bits = __float_as_uint(a);
+    for (int o = 16; o > 0; o >>= 1) bits = max(bits, __shfl_xor_sync(0xffffffffu, bits, o));
+    __shared__ unsigned int wmax[8];
+    const int t = threadIdx.y * blockDim.x + threadIdx.x;
+    if ((t & 31) == 0) wmax[t >> 5] = bits;
+    __syncthreads();
+    if (t == 0) {
+      unsigned int m = 0;
+      for (int w = 0; w < (int)(blockDim.x * blockDim.y) / 32; ++w) m = max(m, wmax[w]);
+      atomicMax(max_bits, m);
+    }
+  }
+}
+
+// One thread per cell c = (i, j, k): updates the x-face (i, j, k) if i >= 1,
+// the y-face if j >= 1 and the z-face if k >= 1, each only when both cells
+// adjacent to the face are fluid.  u -= ((dt/rho) * dp) / dx.
+__global__ void __launch_bounds__(256) gradient_kernel(
+    float *__restrict__ ux, float *__restrict__ uy, float *__restrict__ uz,
+    const float *__restrict__ p, const uint8_t *__restrict__ mask, int nx, int ny, int nz,
+    float dx, float dtr) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k >= nz || j >= ny) return;
+  const int64_t c = idx3(i, j, k, ny, nz);
+  if (mcls(__ldg(mask + c)) != BSP_FLUID) return;
+  const float pc = __ldg(p + c);
+  const int64_t plane = (int64_t)ny * nz;
+  if (i >= 1 && mcls(__ldg(mask + c - plane)) == BSP_FLUID) {
+    float *f = ux + ((int64_t)i * ny + j) * nz + k;
+    *f = __fsub_rn(*f, __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, __ldg(p + c - plane))), dx));
+  }
+  if (j >= 1 && mcls(__ldg(mask + c - nz)) == BSP_FLUID) {
+    float *f = uy + ((int64_t)i * (ny + 1) + j) * nz + k;
+    *f = __fsub_rn(*f, __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, __ldg(p + c - nz))), dx));
+  }
+  if (k >= 1 && mcls(__ldg(mask + c - 1)) == BSP_FLUID) {
+    float *f = uz + ((int64_t)i * ny + j) * (nz + 1) + k;
+    *f = __fsub_rn(*f, __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pc, __ldg(p + c - 1))), dx));
+  }
+}
+
+// One thread per lattice point (i, j, k) in [0,nx] x [0,ny] x [0,nz]; each point
+// owns the x-, y- and z-face with its index where that face exists.
+__global__ void __launch_bounds__(256) no_slip_kernel(float *__restrict__ ux,
+                                                      float *__restrict__ uy,
+                                                      float *__restrict__ uz,
+                                                      const uint8_t *__restrict__ mask, int nx,
+                                                      int ny, int nz) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k > nz || j > ny) return;
+  auto fluid = [&](int a, int b, int c) {
+    return mcls(__ldg(mask + idx3(a, b, c, ny, nz))) == BSP_FLUID;
+  };
+  if (j < ny && k < nz) {
+    if (i == 0 || i == nx || !fluid(i - 1, j, k) || !fluid(i, j, k))
+      ux[((int64_t)i * ny + j) * nz + k] = 0.0f;
+  }
+  if (i < nx && k < nz) {
+    if (j == 0 || j == ny || !fluid(i, j - 1, k) || !fluid(i, j, k))
+      uy[((int64_t)i * (ny + 1) + j) * nz + k] = 0.0f;
+  }
+  if (i < nx && j < ny) {
+    if (k == 0 || k == nz || !fluid(i, j, k - 1) || !fluid(i, j, k))
+      uz[((int64_t)i * ny + j) * (nz + 1) + k] = 0.0f;
+  }
+}
+
+cudaError_t divergence_impl(float *div, const float *ux, const float *uy, const float *uz,
+                            const uint8_t *mask, int nx, int ny, int nz, float dx,
+                            float *max_abs_div, cudaStream_t s) {
+  if (max_abs_div) {
+    cudaError_t e = cudaMemsetAsync(max_abs_div, 0, sizeof(float), s);
+    if (e != cudaSuccess) return e;
+  }
+  dim3 block(128, 2);
+  dim3 grid((nz + 127) / 128, (ny + 1) / 2, nx);
+  divergence_kernel<<<grid, block, 0, s>>>(div, ux, uy, uz, mask, nx, ny, nz, dx,
+                                           reinterpret_cast<unsigned int *>(max_abs_div));
+  return cudaGetLastError();
+}
+
+cudaError_t gradient_impl(float *ux, float *uy, float *uz, const float *p, const uint8_t *mask,
+                          int nx, int ny, int nz, float dx, float dt, float rho, cudaStream_t s) {
+  const float dtr = dt / rho;
+  dim3 block(128, 2);
+  dim3 grid((nz + 127) / 128, (ny + 1) / 2, nx);
+  gradient_kernel<<<grid, block, 0, s>>>(ux, uy, uz, p, mask, nx, ny, nz, dx, dtr);
+  return cudaGetLastError();
+}
+
+static inline bool dims_ok(int nx, int ny, int nz) {
+  return nx > 0 && ny > 0 && nz > 0 && nx < 65535 && (int64_t)nx * ny * nz <= ((int64_t)1 << 40);
+}
+
+}  // namespace bsp
+
+using namespace bsp;
+
+extern "C" int bsp_divergence(float *div_u, const float *ux, const float *uy, const float *uz,
+                              const uint8_t *mask, int nx, int ny, int nz, float dx,
+                              float *max_abs_div, cudaStream_t stream) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_OK;
+  if (!div_u || !ux || !uy || !uz || !mask) return BSP_ERR_NULL;
+  if (!dims_ok(nx, ny, nz)) return BSP_ERR_SHAPE;
+  return (int)divergence_impl(div_u, ux, uy, uz, mask, nx, ny, nz, dx, max_abs_div, stream);
+}
+
+extern "C" int bsp_subtract_gradient(float *ux, float *uy, float *uz, const float *p,
+                                     const uint8_t *mask, int nx, int ny, int nz, float dx,
+                                     float dt, float rho, cudaStream_t stream) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_OK;
+  if (!ux || !uy || !uz || !p || !mask) return BSP_ERR_NULL;
+  if (!dims_ok(nx, ny, nz)) return BSP_ERR_SHAPE;
+  return (int)gradient_impl(ux, uy, uz, p, mask, nx, ny, nz, dx, dt, rho, stream);
+}
+
+extern "C" int bsp_enforce_no_slip(float *ux, float *uy, float *uz, const uint8_t *mask, int nx,
+                                   int ny, int nz, cudaStream_t stream) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_OK;
+  if (!ux || !uy || !uz || !mask) return BSP_ERR_NULL;
+  if (!dims_ok(nx + 1, ny, nz)) return BSP_ERR_SHAPE;
+  dim3 block(128, 2);
+  dim3 grid((nz + 1 + 127) / 128, (ny + 2) / 2, nx + 1);
+  no_slip_kernel<<<grid, block, 0, stream>>>(ux, uy, uz, mask, nx, ny, nz);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int bsp_projection_jacobi(float *p, float *p_tmp, float *div_u, float *ux, float *uy,
+                                     float *uz, const uint8_t *mask, int nx, int ny, int nz,
+                                     float dx, float dt, float rho, int n_iter, int tblock,
+                                     float *max_div_dev, cudaStream_t stream) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_OK;
+  if (!p || !p_tmp || !div_u || !ux || !uy || !uz || !mask) return BSP_ERR_NULL;
+  if (!dims_ok(nx, ny, nz)) return BSP_ERR_SHAPE;
+  if (p == p_tmp) return BSP_ERR_ALIAS;
+  const size_t bytes = sizeof(float) * (size_t)nx * ny * nz;
+  cudaError_t e = cudaMemsetAsync(p, 0, bytes, stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(p_tmp, 0, bytes, stream);
+  if (e != cudaSuccess) return (int)e;
+  e = divergence_impl(div_u, ux, uy, uz, mask, nx, ny, nz, dx, nullptr, stream);
+  if (e != cudaSuccess) return (int)e;
+  int st = jacobi_solve_impl(p, p_tmp, div_u, mask, nx, ny, nz, dx, dt, rho, n_iter, tblock,
+                             stream);
+  if (st != BSP_OK) return st;
+  e = gradient_impl(ux, uy, uz, p, mask, nx, ny, nz, dx, dt, rho, stream);
+  if (e != cudaSuccess) return (int)e;
+  return (int)divergence_impl(div_u, ux, uy, uz, mask, nx, ny, nz, dx, max_div_dev, stream);
+}
