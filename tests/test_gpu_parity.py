@@ -187,7 +187,8 @@ def test_divergence_gradient_no_slip_bit_exact(cuda):
     want = O.divergence(ux, uy, uz, mat, 0.003)
     assert np.array_equal(bits(host(div)), bits(want))
     assert float(host(mx)[0]) == float(np.abs(want).max())
-    call("bsp_subtract_gradient", *[ptr(u) for u in U], ptr(dev(p)), ptr(m), nx, ny, nz, 0.003,
+    p_d = dev(p)  # keep device buffers referenced while the kernel may run
+    call("bsp_subtract_gradient", *[ptr(u) for u in U], ptr(p_d), ptr(m), nx, ny, nz, 0.003,
          0.01, 997.0, 0)
     wg = O.subtract_gradient(ux, uy, uz, p, mat, 0.003, 0.01, 997.0)
     for got, w in zip(U, wg):
@@ -227,7 +228,8 @@ def test_dot_fp64_deterministic(cuda):
     y = rng.standard_normal(n).astype(np.float32)
     ws = torch.zeros(1024, device="cuda")
     res = torch.zeros(1, device="cuda")
-    call("dot_launch", ptr(dev(x)), ptr(dev(y)), n, ptr(ws), ptr(res))
+    xd, yd = dev(x), dev(y)
+    call("dot_launch", ptr(xd), ptr(yd), n, ptr(ws), ptr(res))
     want = float(np.dot(x.astype(np.float64), y.astype(np.float64)))
     assert abs(float(host(res)[0]) - want) <= 1e-6 * abs(want) + 1e-3
 
@@ -245,7 +247,8 @@ def _run_pcg(mat, div, dx, dt, rho, tol, max_iter):
     p = z(nx, ny, nz)
     ws = [z(nx, ny, nz) for _ in range(5)] + [z(1024)] + [z(1) for _ in range(7)]
     it = ctypes.c_int(-1)
-    call("pressure_solve_pcg_launch", ptr(p), ptr(dev(div)), ptr(dev(mat, torch.int32)), nx, ny,
+    div_d, mat_d = dev(div), dev(mat, torch.int32)
+    call("pressure_solve_pcg_launch", ptr(p), ptr(div_d), ptr(mat_d), nx, ny,
          nz, dx, dt, rho, 0, 2, tol, max_iter, *[ptr(w) for w in ws], ctypes.byref(it))
     return host(p), it.value, float(host(ws[10])[0])
 
