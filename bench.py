@@ -1,0 +1,360 @@
+"""Benchmark: pressure projections per second to FP64 relative residual 1e-6 on
+the 384x384x256 pot (dx = 0.5 mm).
+
+One step = one full projection of the reference's pressure_projection
+(python/boilingsim/fluid.py:612-734) with the to-tolerance solver: restore
+the pre-projection velocities, divergence, solve A p = b to
+||b - A p||_2 <= 1e-6 ||b||_2 (FP64 residual of the FP64 iterate), gradient
+subtract, diagnostic max|div| on the device.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--storage fp32|fp16|bf16]
+
+N > 1 runs N independent replicas (one per GPU, launched by torchrun); the
+path does not shard, so there is no collective on the data path.  Prints one
+JSON line on rank 0.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "boiling-sim_b200"))
+
+METRIC = "projections/s to rel-residual 1e-6 at 384²×256: learned+mixed vs plain FP32"
+DX, DT, RHO, TOL, SEED = 0.0005, 0.01, 997.0, 1e-6, 7
+WORKLOAD = ("pot 384x384x256 dx=0.5mm (R_in 168, wall 12, water line 213, carrot r36 L180), "
+            "velocities N(0,0.05) box-smoothed 3x + plume 0.1 m/s seed 7, full projection to "
+            "FP64 rel-residual 1e-6")
+# Iterations the reference's Jacobi-preconditioned CG needs to meet its own
+# stopping rule (recursive ||r|| < 1e-6 ||b||, checked every 5 iterations from
+# iteration 8) on this workload; measured with this library's reference-
+# compatible pressure_solve_pcg_launch (same algorithm) when a GPU is present.
+REF_PCG_ITERS_FALLBACK = 1281
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _workload():
+    from boilingsim_b200 import scenes as S
+
+    mat = S.pot_mat(S.POT_384)
+    ux, uy, uz = S.velocity_field(mat, seed=SEED)
+    return mat, ux, uy, uz
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index: int):
+        self.path = f"/tmp/bsp_clocks_{os.getpid()}.csv"
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        load = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": float(np.median(load)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference(mat, ux, uy, uz, ref_iters):
+    """The reference's projection algorithm (divergence, Jacobi-PCG to its own
+    stopping rule, gradient subtract, diagnostic divergence) restated in C
+    (oracle/, OpenMP on all host threads), timed on a bounded sample: the
+    divergence/gradient passes once and PCG iterations 2 -> 12 on the full
+    workload; projections/s = 1 / (t_div + ref_iters * t_iter + t_grad + t_div)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    t0 = time.perf_counter()
+    div = O.divergence(ux, uy, uz, mat, DX)
+    t_div = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.pcg(div, mat, DX, DT, RHO, 1e-30, 2)
+    t2 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.pcg(div, mat, DX, DT, RHO, 1e-30, 12)
+    t12 = time.perf_counter() - t0
+    t_iter = max(t12 - t2, 1e-9) / 10.0
+    p = np.zeros(mat.shape, np.float32)
+    t0 = time.perf_counter()
+    O.subtract_gradient(ux, uy, uz, p, mat, DX, DT, RHO)
+    t_grad = time.perf_counter() - t0
+    t_proj = 2 * t_div + ref_iters * t_iter + t_grad
+    return {"value": 1.0 / t_proj, "unit": "projections/s", "cores": threads, "kind": "port",
+            "sample": (f"full 384x384x256 workload: divergence and gradient once, PCG iterations "
+                       f"2->12 timed ({t_iter*1e3:.1f} ms/iteration); projection = "
+                       f"{ref_iters} PCG iterations (the reference's stopping rule at tol 1e-6)"),
+            "s_per_projection": t_proj}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-iters", type=int, default=0,
+                    help="reference PCG iteration count to use instead of measuring it")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        mat, ux, uy, uz = _workload()
+        base = cpu_reference(mat, ux, uy, uz, REF_PCG_ITERS_FALLBACK)
+        line = {"metric": METRIC, "value": base["value"], "unit": "projections/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1e3 * base["s_per_projection"], "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "impl": "reference",
+                "config": {"workload": WORKLOAD, "method": "Jacobi-preconditioned CG (reference "
+                           "pressure_solve_pcg algorithm), CPU C restatement"},
+                "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": base["value"], "unit": "projections/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from boilingsim_b200 import _lib
+    from boilingsim_b200 import fluid as F
+    from boilingsim_b200.solver import TolSolver
+
+    dev = torch.device("cuda", local)
+    mat, ux, uy, uz = _workload()
+    nx, ny, nz = mat.shape
+    n = mat.size
+    mat_t = torch.as_tensor(mat).to(dev)
+    mask = F.cell_mask(mat_t)
+    u0 = [torch.as_tensor(a).to(dev) for a in (ux, uy, uz)]
+    u = [a.clone() for a in u0]
+    p = torch.zeros(mat.shape, dtype=torch.float32, device=dev)
+    div = torch.zeros_like(p)
+    max_div = torch.zeros(1, dtype=torch.float32, device=dev)
+    solver = TolSolver(mask, args.storage, device=dev)
+    stream = torch.cuda.current_stream()
+    last = {}
+
+    def step():
+        for a, b in zip(u, u0):
+            a.copy_(b, non_blocking=True)
+        F.compute_divergence(div, *u, mask, DX)
+        res = solver.solve(div, DX, DT, RHO, tol=TOL, p=p)
+        F.subtract_pressure_gradient(*u, p, mask, DX, DT, RHO)
+        F.compute_divergence(div, *u, mask, DX, max_div)
+        last["res"] = res
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = Clocks(local)
+    _lib.call("bsp_profile_enable", 1)
+    _lib.lib().bsp_profile_read(None, None, 0)  # clear
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    _lib.call("bsp_profile_enable", 0)
+    import ctypes
+
+    ncls = 10
+    prof_ms = (ctypes.c_double * ncls)()
+    prof_n = (ctypes.c_longlong * ncls)()
+    _lib.lib().bsp_profile_read(prof_ms, prof_n, ncls)
+    clk = clocks.stop()
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    res = last["res"]
+    inner = res.inner_iterations
+
+    # ---- roofline of the dominant kernel class -------------------------------------
+    ts = 2 if args.storage != "fp32" else 4
+    # algorithmic bytes per fine cell per launch, by class
+    per_cell = {0: 13.0, 1: ts + 1 + ts / 8, 2: ts + 1 + ts / 8 + ts, 3: 3 * ts + 1 + 2 * ts,
+                4: 4 + ts + ts + ts + 1 + 4 + ts, 5: 8 + 4 + 1 + (ts + 4) / 2, 6: 8 + 4 + 8}
+    names = {0: "jacobi_sweep", 1: "mg_restrict_fine", 2: "mg_prolong_smooth_fine",
+             3: "cg_direction_Ap", 4: "cg_update", 5: "residual_fp64", 6: "x_update_fp64",
+             7: "mg_coarse_levels", 8: "control_and_setup", 9: "divergence_gradient"}
+    dom = max((c for c in per_cell if prof_n[c] > 0), key=lambda c: prof_ms[c])
+    avg_ms = prof_ms[dom] / prof_n[dom]
+    bytes_launch = per_cell[dom] * n
+    peak, peak_kind = _peaks()
+    achieved = bytes_launch / (avg_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": names[dom], "achieved": round(achieved, 1),
+                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": None, "peak_source": peak_kind,
+                "algorithmic_bytes_per_launch": bytes_launch,
+                "avg_launch_ms": round(avg_ms, 5),
+                "share_of_step": round(prof_ms[dom] / (ms * args.steps), 3)}
+    kernel_ms = {names[c]: round(prof_ms[c] / args.steps, 4) for c in range(ncls) if prof_n[c]}
+    launches = int(sum(prof_n))  # every kernel launch of the timed steps is instrumented
+
+    # ---- plain FP32 Jacobi sweep (the stencil's own roofline) -----------------------
+    rhs = torch.empty_like(p)
+    q = torch.empty_like(p)
+    _lib.call("bsp_profile_enable", 1)
+    _lib.lib().bsp_profile_read(None, None, 0)
+    _lib.call("bsp_jacobi_solve", _lib.ptr(p), _lib.ptr(q), _lib.ptr(div), _lib.ptr(rhs),
+              _lib.ptr(mask), nx, ny, nz, DX, DT, RHO, 200, 0, _lib.stream_handle())
+    torch.cuda.synchronize()
+    _lib.call("bsp_profile_enable", 0)
+    _lib.lib().bsp_profile_read(prof_ms, prof_n, ncls)
+    sweep_ms = prof_ms[0] / max(1, prof_n[0])
+    sweep = {"ms": round(sweep_ms, 5), "GB/s": round(13.0 * n / (sweep_ms * 1e-3) / 1e9, 1),
+             "frac": round(13.0 * n / (sweep_ms * 1e-3) / 1e9 / peak, 4)}
+
+    # ---- end to end through the public API with host buffers --------------------------
+    host_u = [torch.as_tensor(a).pin_memory() for a in (ux, uy, uz)]
+    host_out = [torch.empty(a.shape, dtype=torch.float32).pin_memory() for a in (ux, uy, uz)]
+    host_p = torch.empty(mat.shape, dtype=torch.float32).pin_memory()
+    grid = F.Grid(nx, ny, nz, DX, p, mat_t, *u, mask=mask)
+    ws = F.FluidWorkspace(div, q, max_div)
+    cfg = F.ScenarioConfig(F.SolverConfig(pressure_tol=TOL))
+    os.environ["BOILINGSIM_PRESSURE_SOLVER"] = {"fp32": "b200-mg", "fp16": "b200-mixed",
+                                                "bf16": "b200-bf16"}[args.storage]
+    F._TOL_SOLVERS.clear()
+    F._TOL_SOLVERS[(id(grid), grid.shape, args.storage)] = solver
+
+    def e2e_step():
+        for d, h in zip(u, host_u):
+            d.copy_(h, non_blocking=True)
+        md = F.pressure_projection(grid, ws, cfg, DT, RHO)
+        host_p.copy_(p, non_blocking=True)
+        for h, d in zip(host_out, u):
+            h.copy_(d, non_blocking=True)
+        torch.cuda.synchronize()
+        return md
+
+    e2e_step()
+    e2e_steps = max(2, min(args.steps, 5))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    h2d = sum(a.numel() * 4 for a in host_u)
+    d2h = sum(a.numel() * 4 for a in host_out) + host_p.numel() * 4 + 4
+
+    # ---- reference-algorithm iteration count (Jacobi-PCG, its own stopping rule) ------
+    ref_iters = args.ref_iters or REF_PCG_ITERS_FALLBACK
+    if rank == 0 and not args.ref_iters:
+        try:
+            from boilingsim_b200.sim_core import SimCore, pcg_workspace
+
+            w = pcg_workspace(mat.shape, dev)
+            ref_iters = SimCore(local).pressure_solve_pcg(
+                _lib.ptr(p), _lib.ptr(div), _lib.ptr(mat_t), nx, ny, nz, DX, DT, RHO, 1e-6, 20000,
+                *[_lib.ptr(w[k]) for k in ("b", "r", "z", "p_search", "Ap", "dot_ws", "alpha",
+                                             "beta", "rzold", "rznew", "bsq", "rsq", "pAp")])
+        except Exception:
+            ref_iters = REF_PCG_ITERS_FALLBACK
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference(mat, ux, uy, uz, ref_iters)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+
+    if rank == 0:
+        value = world * 1e3 / ms
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "projections/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "storage": args.storage,
+                       "method": "FP64 iterative refinement + multigrid-preconditioned CG "
+                                 "(Jacobi smoothing), FP64 reductions",
+                       "inputs": "600 MB resident (> 126 MB L2); velocities restored each step",
+                       "parallelism": f"replicas x{world}"},
+            "solve": {"inner_iterations": inner, "outer_iterations": res.outer_iterations,
+                      "levels": res.levels, "rel_residual_fp64": res.rel_residual,
+                      "status": res.status},
+            "kernel_ms_per_step": kernel_ms,
+            "roofline": roofline,
+            "plain_fp32_jacobi_sweep": sweep,
+            "reference_pcg_iterations_to_tol": ref_iters,
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(1.0 / e2e_s, 3), "unit": "projections/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -39,7 +39,10 @@ SIGNATURES = {
     "bsp_error_string": (ctypes.c_char_p, [_I]),
     "bsp_mask_from_mat": (_I, [_P, _P, _I, _I, _I, _I, _I, _P]),
     "bsp_jacobi_sweep": (_I, [_P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _P]),
-    "bsp_jacobi_solve": (_I, [_P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I, _I, _P]),
+    "bsp_jacobi_solve": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I, _I, _P]),
+    "bsp_set_tuning": (_I, [_I, _I]),
+    "bsp_profile_enable": (_I, [_I]),
+    "bsp_profile_read": (_I, [_P, _P, _I]),
     "bsp_divergence": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _P, _P]),
     "bsp_subtract_gradient": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _P]),
     "bsp_enforce_no_slip": (_I, [_P, _P, _P, _P, _I, _I, _I, _P]),
@@ -47,7 +50,28 @@ SIGNATURES = {
                                    _P, _P]),
     "bsp_spmv": (_I, [_P, _P, _P, _I, _I, _I, _P]),
     "bsp_selftest_div6": (_I, [_P, _P]),
+    "bsp_solve_params_default": (None, [_P]),
+    "bsp_solver_workspace_bytes": (ctypes.c_size_t, [_I, _I, _I, _I]),
+    "bsp_solve_tol": (_I, [_P, _P, _P, _I, _I, _I, _F, _F, _F, _P, _P, ctypes.c_size_t, _P, _P,
+                           _P]),
 }
+
+
+class BspSolveParams(ctypes.Structure):
+    """include/bsproj.h: BspSolveParams."""
+
+    _fields_ = [("tol", ctypes.c_double), ("inner_tol", ctypes.c_double),
+                ("max_outer", ctypes.c_int), ("max_inner", ctypes.c_int),
+                ("storage", ctypes.c_int), ("warm_start", ctypes.c_int),
+                ("check_every", ctypes.c_int)]
+
+
+class BspSolveInfo(ctypes.Structure):
+    """include/bsproj.h: BspSolveInfo."""
+
+    _fields_ = [("outer_iterations", ctypes.c_int), ("inner_iterations", ctypes.c_int),
+                ("levels", ctypes.c_int), ("pad", ctypes.c_int),
+                ("rel_residual", ctypes.c_double)]
 
 _lib = None
 

@@ -87,8 +87,8 @@ def allocate_fluid_workspace(grid: Grid, device: str = "cuda:0") -> FluidWorkspa
 
 def cell_mask(mat: torch.Tensor, mat_fluid: int = MAT_FLUID, mat_air: int = MAT_AIR,
               stream=None) -> torch.Tensor:
-    """uint8 cell mask of an int32 material grid: class (0 fluid, 1 air,
-    2 solid) in bits 0-1, number of solid face neighbours in bits 2-4."""
+    """uint8 cell mask of an int32 material grid: bit 7 fluid, bit 6 solid
+    (air: neither), bits 0-2 the number of solid face neighbours."""
     if mat.dtype != torch.int32 or not mat.is_contiguous():
         raise TypeError("mat must be a contiguous int32 CUDA tensor")
     out = torch.empty(mat.shape, dtype=torch.uint8, device=mat.device)
@@ -104,11 +104,25 @@ def grid_mask(grid: Grid) -> torch.Tensor:
     return grid.mask
 
 
+_TOL_SOLVERS: dict = {}
+
+
+def _tol_solver(grid: Grid, storage: str):
+    """Per (grid, storage) cached solver: the workspace is allocated once."""
+    from .solver import TolSolver
+
+    key = (id(grid), grid.shape, storage)
+    if key not in _TOL_SOLVERS:
+        _TOL_SOLVERS.clear()
+        _TOL_SOLVERS[key] = TolSolver(grid_mask(grid), storage)
+    return _TOL_SOLVERS[key]
+
+
 def _select_pressure_solver() -> str:
     """``fluid.py:585-609`` with the B200 back-ends added."""
     use_rust_jacobi = os.environ.get("BOILINGSIM_USE_RUST_PRESSURE") == "1"
     solver = os.environ.get("BOILINGSIM_PRESSURE_SOLVER", "jacobi").lower()
-    valid = ("jacobi", "cg-rust", "b200-jacobi")
+    valid = ("jacobi", "cg-rust", "b200-jacobi", "b200-mg", "b200-mixed", "b200-bf16")
     if solver not in valid:
         raise ValueError(f"BOILINGSIM_PRESSURE_SOLVER={solver!r} is not recognised; "
                          f"valid values are {', '.join(repr(v) for v in valid)}.")
@@ -181,6 +195,16 @@ def pressure_projection(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, dt:
         call("bsp_projection_jacobi", ptr(grid.p), ptr(ws.p_tmp), ptr(ws.div_u), ptr(grid.ux),
              ptr(grid.uy), ptr(grid.uz), ptr(mask), nx, ny, nz, dx, float(dt), float(rho),
              n_iter, 0, ptr(ws.max_div), s)
+    elif solver.startswith("b200-"):
+        # to-tolerance back-ends: multigrid-preconditioned CG inside FP64
+        # refinement, stopping at ||b - A p|| <= pressure_tol ||b|| (FP64)
+        storage = {"b200-mg": "fp32", "b200-mixed": "fp16", "b200-bf16": "bf16"}[solver]
+        tol_solver = _tol_solver(grid, storage)
+        compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, mask, dx)
+        tol_solver.solve(ws.div_u, dx, dt, rho, tol=float(cfg.solver.pressure_tol), p=grid.p,
+                         raise_on_fail=False)
+        subtract_pressure_gradient(grid.ux, grid.uy, grid.uz, grid.p, mask, dx, dt, rho)
+        compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, mask, dx, ws.max_div)
     else:
         grid.p.zero_()
         ws.p_tmp.zero_()

@@ -1,0 +1,96 @@
+"""To-tolerance pressure solve (host side of ``bsp_solve_tol``).
+
+Solves the reference's projection system A p = b (pressure_solve_pcg.cu:129-139)
+to a relative FP64 residual ``tol`` with FP64 iterative refinement around a
+multigrid-preconditioned CG whose inner vectors are stored in FP32, FP16 or
+BF16.  The workspace is allocated once per (shape, storage) by the caller-side
+cache below and passed to the library, which itself never allocates.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib
+from ._lib import BspSolveInfo, BspSolveParams, call, ptr, stream_handle
+
+STORAGE = {"fp32": 0, "fp16": 1, "bf16": 2}
+
+
+@dataclass
+class SolveResult:
+    p: torch.Tensor            # float32 pressure (0 on non-fluid cells)
+    p64_dev: torch.Tensor      # FP64 iterate on the device
+    status: int
+    outer_iterations: int
+    inner_iterations: int
+    levels: int
+    rel_residual: float        # the device's FP64 relative residual
+
+    @property
+    def iterations(self) -> int:
+        return self.inner_iterations
+
+    @property
+    def p64(self) -> np.ndarray:
+        return self.p64_dev.cpu().numpy()
+
+
+class TolSolver:
+    """Reusable solver for one grid shape: owns the workspace and the mask."""
+
+    def __init__(self, mask: torch.Tensor, storage: str = "fp32", device="cuda:0"):
+        if mask.dtype != torch.uint8 or not mask.is_cuda:
+            raise TypeError("mask must be the uint8 cell mask on the GPU")
+        self.mask = mask.contiguous()
+        self.shape = tuple(mask.shape)
+        self.storage = STORAGE[storage]
+        nx, ny, nz = self.shape
+        nbytes = int(_lib.lib().bsp_solver_workspace_bytes(nx, ny, nz, self.storage))
+        # 256-byte alignment: torch's caching allocator hands out 512-byte aligned blocks
+        self.ws = torch.empty(nbytes, dtype=torch.uint8, device=mask.device)
+        self.x64 = torch.empty(self.shape, dtype=torch.float64, device=mask.device)
+        self.params = BspSolveParams()
+        _lib.lib().bsp_solve_params_default(ctypes.byref(self.params))
+        self.params.storage = self.storage
+
+    def solve(self, div: torch.Tensor, dx: float, dt: float, rho: float, tol: float = 1e-6,
+              p: torch.Tensor | None = None, warm_start: bool = False, inner_tol: float | None = None,
+              max_outer: int | None = None, max_inner: int | None = None,
+              check_every: int | None = None, stream=None, raise_on_fail: bool = True) -> SolveResult:
+        nx, ny, nz = self.shape
+        if p is None:
+            p = torch.zeros(self.shape, dtype=torch.float32, device=self.mask.device)
+        prm = BspSolveParams.from_buffer_copy(self.params)
+        prm.tol = float(tol)
+        prm.warm_start = 1 if warm_start else 0
+        if inner_tol is not None:
+            prm.inner_tol = float(inner_tol)
+        if max_outer is not None:
+            prm.max_outer = int(max_outer)
+        if max_inner is not None:
+            prm.max_inner = int(max_inner)
+        if check_every is not None:
+            prm.check_every = int(check_every)
+        info = BspSolveInfo()
+        code = _lib.lib().bsp_solve_tol(ptr(p), ptr(div), ptr(self.mask), nx, ny, nz, float(dx),
+                                         float(dt), float(rho), ctypes.byref(prm), ptr(self.ws),
+                                         self.ws.numel(), ptr(self.x64), ctypes.byref(info),
+                                         stream_handle(stream))
+        if code not in (0, 10005) or (raise_on_fail and code != 0):
+            _lib.check("bsp_solve_tol", code)
+        return SolveResult(p, self.x64, code, info.outer_iterations, info.inner_iterations,
+                           info.levels, info.rel_residual)
+
+
+def solve_tolerance(div, mat, dx, dt, rho, tol=1e-6, storage="fp32", **kw) -> SolveResult:
+    """Convenience wrapper on numpy inputs (int32 material ids, float32 div)."""
+    from .fluid import cell_mask
+
+    mat_t = torch.as_tensor(np.ascontiguousarray(mat, np.int32)).cuda()
+    div_t = torch.as_tensor(np.ascontiguousarray(div, np.float32)).cuda()
+    solver = TolSolver(cell_mask(mat_t), storage)
+    return solver.solve(div_t, dx, dt, rho, tol=tol, **kw)

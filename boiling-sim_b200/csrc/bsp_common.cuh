@@ -24,10 +24,20 @@ __device__ __forceinline__ int64_t idx3(int i, int j, int k, int ny, int nz) {
   return ((int64_t)i * ny + j) * nz + k;
 }
 
-// uint8 mask byte: bits 0-1 cell class, bits 2-4 number of solid face
+// uint8 mask byte: bit 7 = fluid, bit 6 = solid (air = neither, so a zero byte
+// is air, like a cell outside the grid), bits 0-2 = number of solid face
 // neighbours (the Jacobi preconditioner's 6 - n_solid, diag_inverse_apply.cu:62-78).
-__device__ __forceinline__ uint32_t mcls(uint32_t mbyte) { return mbyte & 3u; }
-__device__ __forceinline__ uint32_t mnsolid(uint32_t mbyte) { return (mbyte >> 2) & 7u; }
+// Bit 7 and bit 6 let a warp turn four packed mask bytes into all-ones /
+// all-zero select words with one prmt (sign replication) each.
+#define BSP_MFLUID 0x80u
+#define BSP_MSOLID 0x40u
+__device__ __forceinline__ uint32_t mcls(uint32_t mbyte) {
+  return (mbyte & BSP_MFLUID) ? BSP_FLUID : ((mbyte & BSP_MSOLID) ? BSP_SOLID : BSP_AIR);
+}
+__device__ __forceinline__ uint32_t mnsolid(uint32_t mbyte) { return mbyte & 7u; }
+__device__ __forceinline__ uint32_t enc_cls(uint32_t cls) {
+  return cls == BSP_FLUID ? BSP_MFLUID : (cls == BSP_SOLID ? BSP_MSOLID : 0u);
+}
 
 __device__ __forceinline__ uint32_t classify(int m, int mat_fluid, int mat_air) {
   return m == mat_fluid ? BSP_FLUID : (m == mat_air ? BSP_AIR : BSP_SOLID);
@@ -49,11 +59,33 @@ __device__ __forceinline__ float nbr(uint32_t cls, float p_n, float p_self) {
 // IEEE division (the exhaustive check is bsp_selftest_div6 and the CPU test).
 __device__ __forceinline__ float div6(float x) {
   const float z = 0.16666667163372039795f;  // RN(1/6)
-  const float ax = fabsf(x);
-  if (!(ax >= 0x1p-120f && ax <= 3.40282347e38f)) return __fdiv_rn(x, 6.0f);
   const float q0 = __fmul_rn(x, z);
   const float r = __fmaf_rn(-q0, 6.0f, x);
-  return __fmaf_rn(r, z, q0);
+  const float q = __fmaf_rn(r, z, q0);
+  const float ax = fabsf(x);
+  if (ax >= 0x1p-120f && ax <= 3.40282347e38f) return q;
+  return ax == 0.0f ? x : __fdiv_rn(x, 6.0f);  // +-0 / 6 = +-0; tiny, inf, NaN: IEEE
+}
+
+// Branch-free neighbour select on bit patterns: for the mask byte q of word
+// mw (bit 7 fluid, bit 6 solid) return p_n if fluid, p_self if solid, +0 if air.
+// sw is mw << 1 (solid bit moved to bit 7).
+// prmt.b32 in its default mode: a selector nibble with bit 3 set replicates the
+// sign bit of the selected byte over the output byte (__byte_perm ignores
+// that bit, so the instruction is issued directly).
+__device__ __forceinline__ uint32_t sign_bytes(uint32_t w, uint32_t sel) {
+  uint32_t d;
+  asm("prmt.b32 %0, %1, 0, %2;" : "=r"(d) : "r"(w), "r"(sel));
+  return d;
+}
+__device__ __forceinline__ float sel_nbr(uint32_t mw, uint32_t sw, int q, float pn, float ps) {
+  const uint32_t sel = (uint32_t)(8 | q) * 0x1111u;  // replicate the sign bit of byte q
+  const uint32_t fm = sign_bytes(mw, sel);
+  const uint32_t sm = sign_bytes(sw, sel);
+  return __uint_as_float((__float_as_uint(pn) & fm) | (__float_as_uint(ps) & sm));
+}
+__device__ __forceinline__ uint32_t fluid_word(uint32_t mw, int q) {
+  return sign_bytes(mw, (uint32_t)(8 | q) * 0x1111u);
 }
 
 // One Jacobi update of a fluid cell with the reference's exact operation

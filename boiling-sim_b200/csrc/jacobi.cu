@@ -1,6 +1,13 @@
 // jacobi.cu -- fixed-count Jacobi solve (crates/cuda-kernels/src/jacobi_pressure.cu:228-270
 // on the uint8 class mask): n_iter ping-pong sweeps p -> p_tmp -> p ..., result in p.
+//
+// When the caller provides an rhs buffer (or the projection, which owns div_u
+// for the duration of the solve), rho dx^2 div / dt is evaluated once per cell
+// and every sweep reads it: the same float each sweep of the reference
+// computes, so the result is bit-identical and the per-cell IEEE division
+// leaves the sweep loop.
 #include "bsp_common.cuh"
+#include "profile.cuh"
 
 namespace bsp {
 
@@ -8,21 +15,32 @@ template <int OP, class MaskT>
 cudaError_t launch_stencil(float *out, const float *p, const float *div, const MaskT *mask,
                            int nx, int ny, int nz, float dx, float dt, float rho, int mf,
                            int ma, cudaStream_t s);
+cudaError_t launch_rhs(float *rhs, const float *div, const uint8_t *mask, int64_t n, float dx,
+                       float dt, float rho, cudaStream_t s);
 
-int jacobi_solve_impl(float *p, float *p_tmp, const float *div_u, const uint8_t *mask, int nx,
-                      int ny, int nz, float dx, float dt, float rho, int n_iter, int tblock,
-                      cudaStream_t stream) {
+int jacobi_solve_impl(float *p, float *p_tmp, const float *div_u, float *rhs_ws,
+                      const uint8_t *mask, int nx, int ny, int nz, float dx, float dt, float rho,
+                      int n_iter, int tblock, cudaStream_t stream) {
   (void)tblock;
   if (n_iter <= 0) return BSP_OK;
+  const int64_t n = (int64_t)nx * ny * nz;
+  if (rhs_ws) {
+    cudaError_t e = launch_rhs(rhs_ws, div_u, mask, n, dx, dt, rho, stream);
+    if (e != cudaSuccess) return (int)e;
+  }
   for (int it = 0; it < n_iter; ++it) {
     float *dst = (it & 1) == 0 ? p_tmp : p;
     const float *src = (it & 1) == 0 ? p : p_tmp;
-    cudaError_t e = launch_stencil<0, uint8_t>(dst, src, div_u, mask, nx, ny, nz, dx, dt, rho,
-                                               BSP_FLUID, BSP_AIR, stream);
+    ProfScope ps(PROF_SWEEP, stream);
+    cudaError_t e =
+        rhs_ws ? launch_stencil<2, uint8_t>(dst, src, rhs_ws, mask, nx, ny, nz, dx, dt, rho,
+                                            BSP_FLUID, BSP_AIR, stream)
+               : launch_stencil<0, uint8_t>(dst, src, div_u, mask, nx, ny, nz, dx, dt, rho,
+                                            BSP_FLUID, BSP_AIR, stream);
     if (e != cudaSuccess) return (int)e;
   }
   if (n_iter & 1) {
-    cudaError_t e = cudaMemcpyAsync(p, p_tmp, sizeof(float) * (size_t)nx * ny * nz,
+    cudaError_t e = cudaMemcpyAsync(p, p_tmp, sizeof(float) * (size_t)n,
                                     cudaMemcpyDeviceToDevice, stream);
     if (e != cudaSuccess) return (int)e;
   }
@@ -31,12 +49,12 @@ int jacobi_solve_impl(float *p, float *p_tmp, const float *div_u, const uint8_t 
 
 }  // namespace bsp
 
-extern "C" int bsp_jacobi_solve(float *p, float *p_tmp, const float *div_u,
+extern "C" int bsp_jacobi_solve(float *p, float *p_tmp, const float *div_u, float *rhs_ws,
                                 const uint8_t *mask, int nx, int ny, int nz, float dx, float dt,
                                 float rho, int n_iter, int tblock, cudaStream_t stream) {
   if (nx <= 0 || ny <= 0 || nz <= 0 || n_iter <= 0) return BSP_OK;
   if (!p || !p_tmp || !div_u || !mask) return BSP_ERR_NULL;
-  if (p == p_tmp) return BSP_ERR_ALIAS;
-  return bsp::jacobi_solve_impl(p, p_tmp, div_u, mask, nx, ny, nz, dx, dt, rho, n_iter, tblock,
-                                stream);
+  if (p == p_tmp || rhs_ws == p || rhs_ws == p_tmp) return BSP_ERR_ALIAS;
+  return bsp::jacobi_solve_impl(p, p_tmp, div_u, rhs_ws, mask, nx, ny, nz, dx, dt, rho, n_iter,
+                                tblock, stream);
 }

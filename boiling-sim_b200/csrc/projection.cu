@@ -11,6 +11,7 @@
 // here the diagnostic kernel reduces max|div| on the device and only 4 bytes
 // are left for the caller to read.
 #include "bsp_common.cuh"
+#include "profile.cuh"
 
 namespace bsp {
 
@@ -19,9 +20,9 @@ template <int OP, class MaskT>
 cudaError_t launch_stencil(float *out, const float *p, const float *div, const MaskT *mask,
                            int nx, int ny, int nz, float dx, float dt, float rho, int mf,
                            int ma, cudaStream_t s);
-int jacobi_solve_impl(float *p, float *p_tmp, const float *div_u, const uint8_t *mask, int nx,
-                      int ny, int nz, float dx, float dt, float rho, int n_iter, int tblock,
-                      cudaStream_t stream);
+int jacobi_solve_impl(float *p, float *p_tmp, const float *div_u, float *rhs_ws,
+                      const uint8_t *mask, int nx, int ny, int nz, float dx, float dt, float rho,
+                      int n_iter, int tblock, cudaStream_t stream);
 
 // Block = (128 k, 2 j); grid = (k tiles, j tiles, i).  One cell per thread.
 __global__ void __launch_bounds__(256) divergence_kernel(
@@ -132,6 +133,7 @@ cudaError_t divergence_impl(float *div, const float *ux, const float *uy, const 
   }
   dim3 block(128, 2);
   dim3 grid((nz + 127) / 128, (ny + 1) / 2, nx);
+  ProfScope ps(PROF_PROJ, s);
   divergence_kernel<<<grid, block, 0, s>>>(div, ux, uy, uz, mask, nx, ny, nz, dx,
                                            reinterpret_cast<unsigned int *>(max_abs_div));
   return cudaGetLastError();
@@ -142,6 +144,7 @@ cudaError_t gradient_impl(float *ux, float *uy, float *uz, const float *p, const
   const float dtr = dt / rho;
   dim3 block(128, 2);
   dim3 grid((nz + 127) / 128, (ny + 1) / 2, nx);
+  ProfScope ps(PROF_PROJ, s);
   gradient_kernel<<<grid, block, 0, s>>>(ux, uy, uz, p, mask, nx, ny, nz, dx, dtr);
   return cudaGetLastError();
 }
@@ -179,6 +182,7 @@ extern "C" int bsp_enforce_no_slip(float *ux, float *uy, float *uz, const uint8_
   if (!dims_ok(nx + 1, ny, nz)) return BSP_ERR_SHAPE;
   dim3 block(128, 2);
   dim3 grid((nz + 1 + 127) / 128, (ny + 2) / 2, nx + 1);
+  ProfScope ps(PROF_PROJ, stream);
   no_slip_kernel<<<grid, block, 0, stream>>>(ux, uy, uz, mask, nx, ny, nz);
   return (int)cudaGetLastError();
 }
@@ -197,8 +201,10 @@ extern "C" int bsp_projection_jacobi(float *p, float *p_tmp, float *div_u, float
   if (e != cudaSuccess) return (int)e;
   e = divergence_impl(div_u, ux, uy, uz, mask, nx, ny, nz, dx, nullptr, stream);
   if (e != cudaSuccess) return (int)e;
-  int st = jacobi_solve_impl(p, p_tmp, div_u, mask, nx, ny, nz, dx, dt, rho, n_iter, tblock,
-                             stream);
+  // div_u belongs to the projection until the diagnostic divergence below
+  // overwrites it, so it holds rho dx^2 div / dt (in place) during the sweeps.
+  int st = jacobi_solve_impl(p, p_tmp, div_u, div_u, mask, nx, ny, nz, dx, dt, rho, n_iter,
+                             tblock, stream);
   if (st != BSP_OK) return st;
   e = gradient_impl(ux, uy, uz, p, mask, nx, ny, nz, dx, dt, rho, stream);
   if (e != cudaSuccess) return (int)e;

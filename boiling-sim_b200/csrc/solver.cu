@@ -1,0 +1,916 @@
+// solver.cu -- to-tolerance pressure solve: FP64 iterative refinement around a
+// multigrid-preconditioned conjugate gradient with reduced-precision storage.
+//
+// The linear system is the reference's (pressure_solve_pcg.cu:129-139,
+// laplacian_spmv.cu:62-143):  A p = b,  (A p)_c = 6 p_c - sum g(n),
+// g = p_n (fluid) | 0 (air, Dirichlet) | p_c (solid, Neumann),
+// b_c = -rho dx^2 div_c / dt, on fluid cells.  Stopping rule
+// ||b - A p||_2 <= tol ||b||_2 (python/boilingsim/config.py:166-176), with the
+// residual evaluated in FP64 from an FP64 iterate.
+//
+// Structure (all on the device; the host only reads a done flag between
+// chunks of iterations):
+//   outer (FP64):  r = b - A x;  stop if ||r|| <= tol ||b||;
+//                  rhat = s r (stored as T);  solve A e ~= rhat;  x += e / s
+//   inner (FP32 arithmetic, T storage): CG preconditioned by one V-cycle,
+//                  stopped when ||r_inner|| <= eta ||rhat|| or after max_inner.
+//   V-cycle (Jacobi smoothing, weight OMEGA, one pre and one post sweep):
+//     down l -> l+1: e_l = OMEGA D^-1 r_l (from zero, not stored);
+//                    r_{l+1}[C] = 1/2 sum_{fluid children c} (r_l - A_l e_l)[c]
+//     coarsest:      COARSE_SWEEPS Jacobi sweeps from zero in one CTA
+//     up l+1 -> l:   e^ = OMEGA D^-1 r_l + e_{l+1}[parent];
+//                    e_l = e^ + OMEGA D^-1 (r_l - A_l e^)
+//   Coarse cells: AIR if any child is air adjacent to fluid, else FLUID if any
+//   child is fluid, else SOLID (air away from fluid is treated as solid so
+//   thin pot walls never turn into free surfaces at coarse levels).
+// All inner products are FP64 with a fixed reduction order.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "bsp_common.cuh"
+#include "profile.cuh"
+#include "solver.cuh"
+
+namespace bsp {
+
+int num_sms();
+
+constexpr float OMEGA = 6.0f / 7.0f;
+constexpr int COARSE_SWEEPS = 64;
+constexpr int RED_THREADS = 256;
+
+// ---- storage conversions --------------------------------------------------------
+__device__ __forceinline__ float ld(const float *p, int64_t c) { return p[c]; }
+__device__ __forceinline__ float ld(const __half *p, int64_t c) { return __half2float(p[c]); }
+__device__ __forceinline__ float ld(const __nv_bfloat16 *p, int64_t c) {
+  return __bfloat162float(p[c]);
+}
+__device__ __forceinline__ void stv(float *p, int64_t c, float v) { p[c] = v; }
+__device__ __forceinline__ void stv(__half *p, int64_t c, float v) { p[c] = __float2half_rn(v); }
+__device__ __forceinline__ void stv(__nv_bfloat16 *p, int64_t c, float v) {
+  p[c] = __float2bfloat16_rn(v);
+}
+
+// value as it reads back after a store through T
+__device__ __forceinline__ float rnd(float v, const float *) { return v; }
+__device__ __forceinline__ float rnd(float v, const __half *) {
+  return __half2float(__float2half_rn(v));
+}
+__device__ __forceinline__ float rnd(float v, const __nv_bfloat16 *) {
+  return __bfloat162float(__float2bfloat16_rn(v));
+}
+
+__device__ __forceinline__ uint32_t mk(const uint8_t *m, int64_t c) { return __ldg(m + c); }
+
+// Row-unit iteration: one warp per (i, j) row, lanes striding over k.
+struct RowIter {
+  int64_t u, rows, step;
+  __device__ RowIter(int nx, int ny)
+      : u((int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)),
+        rows((int64_t)nx * ny),
+        step((int64_t)gridDim.x * (blockDim.x >> 5)) {}
+};
+
+// ---- deterministic block partials ------------------------------------------------
+template <int K>
+__device__ __forceinline__ void store_partials(double (&v)[K], double *partials) {
+  __shared__ double sh[K][32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < K; ++q)
+    for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+  if (lane == 0)
+#pragma unroll
+    for (int q = 0; q < K; ++q) sh[q][warp] = v[q];
+  __syncthreads();
+  if (threadIdx.x < K) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += sh[threadIdx.x][w];
+    partials[threadIdx.x * PARTIAL_STRIDE + blockIdx.x] = s;
+  }
+}
+
+template <int K>
+__device__ __forceinline__ void store_partials_max(double (&v)[K], double m, double *partials) {
+  // slot K holds a max instead of a sum
+  __shared__ double shm[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if (lane == 0) shm[warp] = m;
+  store_partials<K>(v, partials);
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s = fmax(s, shm[w]);
+    partials[K * PARTIAL_STRIDE + blockIdx.x] = s;
+  }
+}
+
+// Sum of slot q over nblocks partials, fixed order; valid in thread 0 of a
+// RED_THREADS-thread block.
+__device__ double reduce_slot(const double *partials, int q, int nblocks, bool is_max) {
+  __shared__ double sh[RED_THREADS];
+  double s = 0.0;
+  for (int b = threadIdx.x; b < nblocks; b += RED_THREADS) {
+    const double v = partials[q * PARTIAL_STRIDE + b];
+    s = is_max ? fmax(s, v) : s + v;
+  }
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int w = RED_THREADS / 2; w > 0; w >>= 1) {
+    if (threadIdx.x < w) sh[threadIdx.x] = is_max ? fmax(sh[threadIdx.x], sh[threadIdx.x + w])
+                                                  : sh[threadIdx.x] + sh[threadIdx.x + w];
+    __syncthreads();
+  }
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+// ---- level setup ------------------------------------------------------------------
+// Effective class: fluid, air adjacent to fluid (Dirichlet), otherwise solid.
+__global__ void eff_class_kernel(uint8_t *__restrict__ out, const uint8_t *__restrict__ cls_in,
+                                 int nx, int ny, int nz) {
+  RowIter it(nx, ny);
+  const int lane = threadIdx.x & 31;
+  const int64_t plane = (int64_t)ny * nz;
+  for (; it.u < it.rows; it.u += it.step) {
+    const int i = (int)(it.u / ny), j = (int)(it.u % ny);
+    for (int k = lane; k < nz; k += 32) {
+      const int64_t c = it.u * nz + k;
+      uint32_t cl = mcls(cls_in[c]);
+      if (cl == BSP_AIR) {
+        bool adj = false;
+#define FL(cond, off) adj |= (cond) && mcls(cls_in[c + (off)]) == BSP_FLUID
+        FL(i > 0, -plane);
+        FL(i + 1 < nx, plane);
+        FL(j > 0, -(int64_t)nz);
+        FL(j + 1 < ny, (int64_t)nz);
+        FL(k > 0, -1);
+        FL(k + 1 < nz, 1);
+#undef FL
+        if (!adj) cl = BSP_SOLID;
+      }
+      out[c] = (uint8_t)enc_cls(cl);
+    }
+  }
+}
+
+// Coarse class from 2x2x2 children of effective classes.
+__global__ void coarsen_kernel(uint8_t *__restrict__ coarse, const uint8_t *__restrict__ fine,
+                               int fx, int fy, int fz, int cx, int cy, int cz) {
+  RowIter it(cx, cy);
+  const int lane = threadIdx.x & 31;
+  for (; it.u < it.rows; it.u += it.step) {
+    const int I = (int)(it.u / cy), J = (int)(it.u % cy);
+    for (int K = lane; K < cz; K += 32) {
+      bool air = false, fl = false;
+      for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+          for (int d = 0; d < 2; ++d) {
+            const int i = 2 * I + a, j = 2 * J + b, k = 2 * K + d;
+            if (i < fx && j < fy && k < fz) {
+              const uint32_t cl = mcls(fine[((int64_t)i * fy + j) * fz + k]);
+              air |= cl == BSP_AIR;
+              fl |= cl == BSP_FLUID;
+            }
+          }
+      coarse[it.u * cz + K] = (uint8_t)enc_cls(air ? BSP_AIR : (fl ? BSP_FLUID : BSP_SOLID));
+    }
+  }
+}
+
+// Add the solid-neighbour count (bits 2-4); out-of-range neighbours are air.
+__global__ void nsolid_kernel(uint8_t *__restrict__ m, int nx, int ny, int nz) {
+  RowIter it(nx, ny);
+  const int lane = threadIdx.x & 31;
+  const int64_t plane = (int64_t)ny * nz;
+  for (; it.u < it.rows; it.u += it.step) {
+    const int i = (int)(it.u / ny), j = (int)(it.u % ny);
+    for (int k = lane; k < nz; k += 32) {
+      const int64_t c = it.u * nz + k;
+      uint32_t ns = 0;
+#define SO(cond, off) ns += ((cond) && mcls(m[c + (off)]) == BSP_SOLID) ? 1u : 0u
+      SO(i > 0, -plane);
+      SO(i + 1 < nx, plane);
+      SO(j > 0, -(int64_t)nz);
+      SO(j + 1 < ny, (int64_t)nz);
+      SO(k > 0, -1);
+      SO(k + 1 < nz, 1);
+#undef SO
+      m[c] = (uint8_t)((m[c] & (BSP_MFLUID | BSP_MSOLID)) | ns);
+    }
+  }
+}
+
+// ---- stencil helpers ----------------------------------------------------------------
+__device__ __forceinline__ float dg(uint32_t mb) { return 6.0f - (float)mnsolid(mb); }
+
+// e = OMEGA r / D on a fluid cell.
+template <class T>
+__device__ __forceinline__ float pre_e(const T *r, int64_t c, uint32_t mb) {
+  return OMEGA * ld(r, c) / dg(mb);
+}
+
+// ---- V-cycle kernels ----------------------------------------------------------------
+template <class T>
+__global__ void __launch_bounds__(256) mg_down_kernel(Level<T> f, Level<T> co,
+                                                      const SolverState *st) {
+  if (st->inner_done) return;
+  RowIter it(co.nx, co.ny);
+  const int lane = threadIdx.x & 31;
+  const int64_t plane = (int64_t)f.ny * f.nz;
+  for (; it.u < it.rows; it.u += it.step) {
+    const int I = (int)(it.u / co.ny), J = (int)(it.u % co.ny);
+    for (int K = lane; K < co.nz; K += 32) {
+      const int64_t C = it.u * co.nz + K;
+      float acc = 0.0f;
+      if (mcls(mk(co.mask, C)) == BSP_FLUID) {
+        for (int a = 0; a < 2; ++a)
+          for (int b = 0; b < 2; ++b)
+            for (int d = 0; d < 2; ++d) {
+              const int i = 2 * I + a, j = 2 * J + b, k = 2 * K + d;
+              if (i >= f.nx || j >= f.ny || k >= f.nz) continue;
+              const int64_t c = ((int64_t)i * f.ny + j) * f.nz + k;
+              const uint32_t mc = mk(f.mask, c);
+              if (mcls(mc) != BSP_FLUID) continue;
+              const float ec = pre_e(f.r, c, mc);
+#define NB(cond, off)                                                          \
+  ((cond) ? ([&]() {                                                           \
+    const uint32_t mn = mk(f.mask, c + (off));                                 \
+    const uint32_t cn = mcls(mn);                                              \
+    return cn == BSP_FLUID ? pre_e(f.r, c + (off), mn) : (cn == BSP_AIR ? 0.0f : ec); \
+  })()                                                                         \
+          : 0.0f)
+              const float s = NB(i > 0, -plane) + NB(i + 1 < f.nx, plane) +
+                              NB(j > 0, -(int64_t)f.nz) + NB(j + 1 < f.ny, (int64_t)f.nz) +
+                              NB(k > 0, -1) + NB(k + 1 < f.nz, 1);
+#undef NB
+              acc += ld(f.r, c) - (6.0f * ec - s);
+            }
+        acc *= 0.5f;
+      }
+      stv(co.r, C, acc);
+    }
+  }
+}
+
+// Coarsest level: one CTA, whole level in shared memory, Jacobi from zero.
+template <class T>
+__global__ void __launch_bounds__(512) mg_coarse_kernel(Level<T> L, const SolverState *stt) {
+  if (stt->inner_done) return;
+  extern __shared__ float sm[];
+  const int n = L.nx * L.ny * L.nz;
+  float *e0 = sm, *e1 = sm + n, *rr = sm + 2 * n;
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    e0[c] = 0.0f;
+    rr[c] = ld(L.r, c);
+  }
+  __syncthreads();
+  const int plane = L.ny * L.nz;
+  for (int s = 0; s < COARSE_SWEEPS; ++s) {
+    for (int c = threadIdx.x; c < n; c += blockDim.x) {
+      const uint32_t mc = mk(L.mask, c);
+      if (mcls(mc) != BSP_FLUID) {
+        e1[c] = 0.0f;
+        continue;
+      }
+      const int k = c % L.nz, j = (c / L.nz) % L.ny, i = c / plane;
+      const float ec = e0[c];
+#define NB(cond, off)                                                                    \
+  ((cond) ? (mcls(mk(L.mask, c + (off))) == BSP_FLUID                                    \
+                 ? e0[c + (off)]                                                         \
+                 : (mcls(mk(L.mask, c + (off))) == BSP_AIR ? 0.0f : ec))                 \
+          : 0.0f)
+      const float sum = NB(i > 0, -plane) + NB(i + 1 < L.nx, plane) + NB(j > 0, -L.nz) +
+                        NB(j + 1 < L.ny, L.nz) + NB(k > 0, -1) + NB(k + 1 < L.nz, 1);
+#undef NB
+      e1[c] = ec + (rr[c] - (6.0f * ec - sum)) / dg(mc);
+    }
+    __syncthreads();
+    float *t = e0;
+    e0 = e1;
+    e1 = t;
+  }
+  for (int c = threadIdx.x; c < n; c += blockDim.x) stv(L.e, c, e0[c]);
+}
+
+// Up: e^ = OMEGA D^-1 r + e_coarse[parent]; e = e^ + OMEGA D^-1 (r - A e^).
+// Writes e to `out` (the level's e, or z at level 0) and, at level 0, the
+// partial r.z.
+template <class T, bool FINE>
+__global__ void __launch_bounds__(256) mg_up_kernel(Level<T> f, Level<T> co, T *out,
+                                                    double *partials, const SolverState *st) {
+  if (st->inner_done) return;
+  RowIter it(f.nx, f.ny);
+  const int lane = threadIdx.x & 31;
+  const int64_t plane = (int64_t)f.ny * f.nz;
+  double rz = 0.0;
+  for (; it.u < it.rows; it.u += it.step) {
+    const int i = (int)(it.u / f.ny), j = (int)(it.u % f.ny);
+    for (int k = lane; k < f.nz; k += 32) {
+      const int64_t c = it.u * f.nz + k;
+      const uint32_t mc = mk(f.mask, c);
+      if (mcls(mc) != BSP_FLUID) {
+        stv(out, c, 0.0f);
+        continue;
+      }
+      auto ehat = [&](int ii, int jj, int kk, int64_t cc, uint32_t mb) {
+        const int64_t P = ((int64_t)(ii >> 1) * co.ny + (jj >> 1)) * co.nz + (kk >> 1);
+        return pre_e(f.r, cc, mb) + ld(co.e, P);
+      };
+      const float ec = ehat(i, j, k, c, mc);
+#define NB(cond, di, dj, dk, off)                                                     \
+  ((cond) ? ([&]() {                                                                  \
+    const uint32_t mn = mk(f.mask, c + (off));                                        \
+    const uint32_t cn = mcls(mn);                                                     \
+    return cn == BSP_FLUID ? ehat(i + di, j + dj, k + dk, c + (off), mn)              \
+                           : (cn == BSP_AIR ? 0.0f : ec);                             \
+  })()                                                                                \
+          : 0.0f)
+      const float s = NB(i > 0, -1, 0, 0, -plane) + NB(i + 1 < f.nx, 1, 0, 0, plane) +
+                      NB(j > 0, 0, -1, 0, -(int64_t)f.nz) +
+                      NB(j + 1 < f.ny, 0, 1, 0, (int64_t)f.nz) + NB(k > 0, 0, 0, -1, -1) +
+                      NB(k + 1 < f.nz, 0, 0, 1, 1);
+#undef NB
+      const float rc = ld(f.r, c);
+      const float e = ec + OMEGA * (rc - (6.0f * ec - s)) / dg(mc);
+      stv(out, c, e);
+      if (FINE) rz += (double)rc * (double)ld(out, c);
+    }
+  }
+  if (FINE) {
+    double v[1] = {rz};
+    store_partials<1>(v, partials);
+  }
+}
+
+// ---- CG kernels ---------------------------------------------------------------------
+// ps = z + beta ps_prev (first iteration: ps = z), formed at the centre and the
+// neighbours; Ap = A ps; partial ps.Ap.
+template <class T>
+__global__ void __launch_bounds__(256) cg_ps_ap_kernel(int nx, int ny, int nz,
+                                                       const uint8_t *mask, const T *z,
+                                                       const T *prev, T *cur, T *Ap,
+                                                       double *partials, const SolverState *st) {
+  if (st->inner_done) return;
+  const bool first = st->inner_it == 0;
+  const float beta = (float)st->beta;
+  RowIter it(nx, ny);
+  const int lane = threadIdx.x & 31;
+  const int64_t plane = (int64_t)ny * nz;
+  double pap = 0.0;
+  for (; it.u < it.rows; it.u += it.step) {
+    const int i = (int)(it.u / ny), j = (int)(it.u % ny);
+    for (int k = lane; k < nz; k += 32) {
+      const int64_t c = it.u * nz + k;
+      if (mcls(mk(mask, c)) != BSP_FLUID) {
+        stv(cur, c, 0.0f);
+        stv(Ap, c, 0.0f);
+        continue;
+      }
+#define PS(x) (first ? ld(z, (x)) : rnd(fmaf(beta, ld(prev, (x)), ld(z, (x))), cur))
+      const float psc = PS(c);
+#define NB(cond, off)                                                        \
+  ((cond) ? ([&]() {                                                         \
+    const uint32_t cn = mcls(mk(mask, c + (off)));                           \
+    return cn == BSP_FLUID ? PS(c + (off)) : (cn == BSP_AIR ? 0.0f : psc);   \
+  })()                                                                       \
+          : 0.0f)
+      const float s = NB(i > 0, -plane) + NB(i + 1 < nx, plane) + NB(j > 0, -(int64_t)nz) +
+                      NB(j + 1 < ny, (int64_t)nz) + NB(k > 0, -1) + NB(k + 1 < nz, 1);
+#undef NB
+#undef PS
+      stv(cur, c, psc);
+      const float psq = ld(cur, c);  // the stored (possibly rounded) direction
+      const float ap = 6.0f * psq - s;
+      stv(Ap, c, ap);
+      pap += (double)psq * (double)ld(Ap, c);
+    }
+  }
+  double v[1] = {pap};
+  store_partials<1>(v, partials);
+}
+
+// e += alpha ps; r -= alpha Ap; partial r.r
+template <class T>
+__global__ void __launch_bounds__(256) cg_update_kernel(int64_t n, const uint8_t *mask,
+                                                        float *e, T *r, const T *ps,
+                                                        const T *Ap, double *partials,
+                                                        const SolverState *st) {
+  if (st->inner_done) return;
+  const float alpha = (float)st->alpha;
+  double rr = 0.0;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    if (mcls(mk(mask, c)) != BSP_FLUID) continue;
+    e[c] = fmaf(alpha, ld(ps, c), e[c]);
+    stv(r, c, fmaf(-alpha, ld(Ap, c), ld(r, c)));
+    const float rv = ld(r, c);
+    rr += (double)rv * (double)rv;
+  }
+  double v[1] = {rr};
+  store_partials<1>(v, partials);
+}
+
+// ---- outer (FP64) kernels --------------------------------------------------------------
+// r = b - A x in FP64 on fluid cells; partial ||r||^2 and max|r|; if WRITE,
+// rhat = scale r (stored as T), inner r = rhat, e = 0.
+template <class T, bool WRITE>
+__global__ void __launch_bounds__(256) residual64_kernel(int nx, int ny, int nz,
+                                                         const uint8_t *mask, const float *div,
+                                                         const double *x, double bscale,
+                                                         T *rhat, float *e, double *partials,
+                                                         const SolverState *st) {
+  if (st->done) return;
+  const double scale = st->scale;
+  RowIter it(nx, ny);
+  const int lane = threadIdx.x & 31;
+  const int64_t plane = (int64_t)ny * nz;
+  double rr = 0.0, rmax = 0.0;
+  for (; it.u < it.rows; it.u += it.step) {
+    const int i = (int)(it.u / ny), j = (int)(it.u % ny);
+    for (int k = lane; k < nz; k += 32) {
+      const int64_t c = it.u * nz + k;
+      const uint32_t mc = mk(mask, c);
+      double r = 0.0;
+      if (mcls(mc) == BSP_FLUID) {
+        const double xc = x[c];
+#define NB(cond, off)                                                        \
+  ((cond) ? ([&]() {                                                         \
+    const uint32_t cn = mcls(mk(mask, c + (off)));                           \
+    return cn == BSP_FLUID ? x[c + (off)] : (cn == BSP_AIR ? 0.0 : xc);      \
+  })()                                                                       \
+          : 0.0)
+        const double s = NB(i > 0, -plane) + NB(i + 1 < nx, plane) + NB(j > 0, -(int64_t)nz) +
+                         NB(j + 1 < ny, (int64_t)nz) + NB(k > 0, -1) + NB(k + 1 < nz, 1);
+#undef NB
+        r = bscale * (double)__ldg(div + c) - (6.0 * xc - s);
+      }
+      rr += r * r;
+      rmax = fmax(rmax, fabs(r));
+      if (WRITE) {
+        stv(rhat, c, (float)(r * scale));
+        e[c] = 0.0f;
+      }
+    }
+  }
+  double v[1] = {rr};
+  store_partials_max<1>(v, rmax, partials);
+}
+
+// x += e / scale (FP64); at the end the float output is refreshed too.
+__global__ void xupdate_kernel(int64_t n, double *x, const float *e, float *p_out,
+                               const SolverState *st) {
+  if (st->done && !st->finalize) return;
+  const double inv = 1.0 / st->scale;
+  const bool add = !st->done;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    double v = x[c];
+    if (add) {
+      v += (double)e[c] * inv;
+      x[c] = v;
+    }
+    if (p_out) p_out[c] = (float)v;
+  }
+}
+
+// ---- scalar (control) kernels, one block --------------------------------------------
+// Outer check after a residual pass.  Sets done / status, scale for rhat.
+__global__ void __launch_bounds__(RED_THREADS) outer_check_kernel(SolverState *st,
+                                                                  const double *partials,
+                                                                  int nblocks, int fp32_store) {
+  if (st->done) return;
+  const double rr = reduce_slot(partials, 0, nblocks, false);
+  const double rmax = reduce_slot(partials, 1, nblocks, true);
+  if (threadIdx.x != 0) return;
+  st->r64_norm2 = rr;
+  st->rel = st->b_norm2 > 0.0 ? sqrt(rr / st->b_norm2) : 0.0;
+  if (!(rr == rr) || rr > 1e300) {
+    st->status = BSP_ERR_NONFINITE;
+    st->done = 1;
+    return;
+  }
+  if (st->b_norm2 == 0.0 || st->rel <= st->tol) {
+    st->done = 1;
+    st->status = BSP_OK;
+    return;
+  }
+  if (st->outer_it >= st->max_outer) {
+    st->done = 1;
+    st->status = BSP_NOT_CONVERGED;
+    return;
+  }
+  // FP32 storage: scale 1/||r||_inf keeps rhat O(1); half precision: the same
+  // keeps |rhat| <= 1 so FP16 never overflows on the right-hand side.
+  st->scale = rmax > 0.0 ? 1.0 / rmax : 1.0;
+  (void)fp32_store;
+  st->inner_it = 0;
+  st->inner_done = 0;
+  st->rhat_norm2 = rr * st->scale * st->scale;
+  st->outer_it += 1;
+}
+
+__global__ void __launch_bounds__(RED_THREADS) beta_kernel(SolverState *st,
+                                                           const double *partials, int nblocks) {
+  if (st->inner_done) return;
+  const double rz = reduce_slot(partials, 0, nblocks, false);
+  if (threadIdx.x != 0) return;
+  st->beta = (st->inner_it == 0 || st->rz == 0.0) ? 0.0 : rz / st->rz;
+  st->rz = rz;
+}
+
+__global__ void __launch_bounds__(RED_THREADS) alpha_kernel(SolverState *st,
+                                                            const double *partials, int nblocks) {
+  if (st->inner_done) return;
+  const double pap = reduce_slot(partials, 0, nblocks, false);
+  if (threadIdx.x != 0) return;
+  st->alpha = pap > 0.0 ? st->rz / pap : 0.0;
+}
+
+__global__ void __launch_bounds__(RED_THREADS) inner_check_kernel(SolverState *st,
+                                                                  const double *partials,
+                                                                  int nblocks) {
+  if (st->inner_done) return;
+  const double rr = reduce_slot(partials, 0, nblocks, false);
+  if (threadIdx.x != 0) return;
+  st->inner_it += 1;
+  st->total_inner += 1;
+  st->rr_inner = rr;
+  if (!(rr == rr) || rr <= st->eta * st->eta * st->rhat_norm2 ||
+      st->inner_it >= st->max_inner || st->alpha == 0.0)
+    st->inner_done = 1;
+}
+
+// ---- host side ----------------------------------------------------------------------
+static inline int row_blocks(int64_t rows) {
+  int64_t b = (rows + 7) / 8;
+  int64_t cap = (int64_t)num_sms() * 8;
+  if (cap > PARTIAL_STRIDE) cap = PARTIAL_STRIDE;
+  return (int)(b < cap ? (b > 0 ? b : 1) : cap);
+}
+static inline int flat_blocks(int64_t n) {
+  int64_t b = (n + 255) / 256;
+  int64_t cap = (int64_t)num_sms() * 8;
+  if (cap > PARTIAL_STRIDE) cap = PARTIAL_STRIDE;
+  return (int)(b < cap ? (b > 0 ? b : 1) : cap);
+}
+
+static inline size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+int build_hierarchy(int nx, int ny, int nz, int *dims /* 3*MAX_LEVELS */) {
+  int L = 0;
+  int x = nx, y = ny, z = nz;
+  for (;;) {
+    dims[3 * L] = x;
+    dims[3 * L + 1] = y;
+    dims[3 * L + 2] = z;
+    ++L;
+    if (L == MAX_LEVELS) break;
+    // at least two levels: the level-0 up-pass produces z and its r.z partial
+    if (L >= 2 && (int64_t)x * y * z <= COARSEST_CELLS) break;
+    if (L >= 2 && (x <= 2 || y <= 2 || z <= 2)) break;
+    x = (x + 1) / 2;
+    y = (y + 1) / 2;
+    z = (z + 1) / 2;
+  }
+  return L;
+}
+
+size_t storage_bytes(int storage) { return storage == BSP_STORE_FP32 ? 4 : 2; }
+
+// Workspace layout (all 256-byte aligned):
+//   SolverState | partials (3 * PARTIAL_STRIDE doubles) | x (n doubles) | e (n floats)
+//   | z, ps0, ps1, Ap, r (n T each) | per level l >= 1: mask, r, e (T)
+//   | per level l >= 1 ... ; level-0 effective-class scratch reuses the level-1 slot order.
+struct Layout {
+  size_t state, partials, x, e, z, ps0, ps1, Ap, r, lvl_mask[MAX_LEVELS], lvl_r[MAX_LEVELS],
+      lvl_e[MAX_LEVELS], eff0, total;
+  int L, dims[3 * MAX_LEVELS];
+};
+
+Layout make_layout(int nx, int ny, int nz, int storage) {
+  Layout lo{};
+  const size_t n = (size_t)nx * ny * nz, ts = storage_bytes(storage);
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    size_t o = off;
+    off += al256(b);
+    return o;
+  };
+  lo.state = take(sizeof(SolverState));
+  lo.partials = take(sizeof(double) * 3 * PARTIAL_STRIDE);
+  lo.x = take(8 * n);
+  lo.e = take(4 * n);
+  lo.z = take(ts * n);
+  lo.ps0 = take(ts * n);
+  lo.ps1 = take(ts * n);
+  lo.Ap = take(ts * n);
+  lo.r = take(ts * n);
+  lo.eff0 = take(n);
+  lo.L = build_hierarchy(nx, ny, nz, lo.dims);
+  for (int l = 1; l < lo.L; ++l) {
+    const size_t nl = (size_t)lo.dims[3 * l] * lo.dims[3 * l + 1] * lo.dims[3 * l + 2];
+    lo.lvl_mask[l] = take(nl);
+    lo.lvl_r[l] = take(ts * nl);
+    lo.lvl_e[l] = take(ts * nl);
+  }
+  lo.total = off;
+  return lo;
+}
+
+template <class T>
+struct Ctx {
+  Layout lo;
+  char *base;
+  SolverState *st;
+  double *partials;
+  Level<T> lv[MAX_LEVELS];
+  int nx, ny, nz;
+  int64_t n;
+  const uint8_t *mask0;
+};
+
+template <class T>
+Ctx<T> make_ctx(void *ws, const uint8_t *mask, int nx, int ny, int nz, int storage) {
+  Ctx<T> cx{};
+  cx.lo = make_layout(nx, ny, nz, storage);
+  cx.base = (char *)ws;
+  cx.st = (SolverState *)(cx.base + cx.lo.state);
+  cx.partials = (double *)(cx.base + cx.lo.partials);
+  cx.nx = nx;
+  cx.ny = ny;
+  cx.nz = nz;
+  cx.n = (int64_t)nx * ny * nz;
+  cx.mask0 = mask;
+  for (int l = 0; l < cx.lo.L; ++l) {
+    Level<T> &L = cx.lv[l];
+    L.nx = cx.lo.dims[3 * l];
+    L.ny = cx.lo.dims[3 * l + 1];
+    L.nz = cx.lo.dims[3 * l + 2];
+    if (l == 0) {
+      L.mask = mask;
+      L.r = (T *)(cx.base + cx.lo.r);
+      L.e = (T *)(cx.base + cx.lo.z);
+    } else {
+      L.mask = (uint8_t *)(cx.base + cx.lo.lvl_mask[l]);
+      L.r = (T *)(cx.base + cx.lo.lvl_r[l]);
+      L.e = (T *)(cx.base + cx.lo.lvl_e[l]);
+    }
+  }
+  return cx;
+}
+
+template <class T>
+cudaError_t setup_levels(Ctx<T> &cx, cudaStream_t s) {
+  // effective classes of level 0 (scratch), then coarsen level by level
+  uint8_t *eff0 = (uint8_t *)(cx.base + cx.lo.eff0);
+  {
+    ProfScope ps(PROF_CONTROL, s);
+    eff_class_kernel<<<row_blocks((int64_t)cx.nx * cx.ny), 256, 0, s>>>(eff0, cx.mask0, cx.nx,
+                                                                         cx.ny, cx.nz);
+  }
+  const uint8_t *prev = eff0;
+  for (int l = 1; l < cx.lo.L; ++l) {
+    Level<T> &f = cx.lv[l - 1], &c = cx.lv[l];
+    {
+      ProfScope ps(PROF_CONTROL, s);
+      coarsen_kernel<<<row_blocks((int64_t)c.nx * c.ny), 256, 0, s>>>(
+          (uint8_t *)c.mask, prev, f.nx, f.ny, f.nz, c.nx, c.ny, c.nz);
+    }
+    // effective reclassification in place is unsafe (neighbour reads): use the
+    // e-slot of this level as scratch for the raw coarse classes
+    uint8_t *tmp = (uint8_t *)c.e;
+    cudaMemcpyAsync(tmp, c.mask, (size_t)c.nx * c.ny * c.nz, cudaMemcpyDeviceToDevice, s);
+    {
+      ProfScope ps(PROF_CONTROL, s);
+      eff_class_kernel<<<row_blocks((int64_t)c.nx * c.ny), 256, 0, s>>>((uint8_t *)c.mask, tmp,
+                                                                         c.nx, c.ny, c.nz);
+    }
+    {
+      ProfScope ps(PROF_CONTROL, s);
+      nsolid_kernel<<<row_blocks((int64_t)c.nx * c.ny), 256, 0, s>>>((uint8_t *)c.mask, c.nx,
+                                                                      c.ny, c.nz);
+    }
+    prev = c.mask;
+  }
+  return cudaGetLastError();
+}
+
+template <class T>
+cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
+  const int L = cx.lo.L;
+  SolverState *st = cx.st;
+  // V-cycle on r -> z
+  for (int l = 0; l + 1 < L; ++l) {
+    Level<T> &f = cx.lv[l], &c = cx.lv[l + 1];
+    ProfScope ps(l == 0 ? PROF_MG_DOWN0 : PROF_MG_COARSE, s);
+    mg_down_kernel<T><<<row_blocks((int64_t)c.nx * c.ny), 256, 0, s>>>(f, c, st);
+  }
+  {
+    Level<T> &c = cx.lv[L - 1];
+    const int n = c.nx * c.ny * c.nz;
+    ProfScope ps(PROF_MG_COARSE, s);
+    mg_coarse_kernel<T><<<1, 512, 3 * n * sizeof(float), s>>>(c, st);
+  }
+  for (int l = L - 2; l >= 1; --l) {
+    Level<T> &f = cx.lv[l], &c = cx.lv[l + 1];
+    ProfScope ps(PROF_MG_COARSE, s);
+    mg_up_kernel<T, false><<<row_blocks((int64_t)f.nx * f.ny), 256, 0, s>>>(f, c, f.e,
+                                                                            cx.partials, st);
+  }
+  T *z = (T *)(cx.base + cx.lo.z);
+  const int nb0 = row_blocks((int64_t)cx.nx * cx.ny);
+  {
+    ProfScope ps(PROF_MG_UP0, s);
+    mg_up_kernel<T, true><<<nb0, 256, 0, s>>>(cx.lv[0], cx.lv[1], z, cx.partials, st);
+  }
+  {
+    ProfScope ps(PROF_CONTROL, s);
+    beta_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials, nb0);
+  }
+  T *cur = (T *)(cx.base + (it_parity ? cx.lo.ps1 : cx.lo.ps0));
+  T *prev = (T *)(cx.base + (it_parity ? cx.lo.ps0 : cx.lo.ps1));
+  T *Ap = (T *)(cx.base + cx.lo.Ap);
+  {
+    ProfScope ps(PROF_CG_PSAP, s);
+    cg_ps_ap_kernel<T><<<nb0, 256, 0, s>>>(cx.nx, cx.ny, cx.nz, cx.mask0, z, prev, cur, Ap,
+                                           cx.partials, st);
+  }
+  {
+    ProfScope ps(PROF_CONTROL, s);
+    alpha_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials, nb0);
+  }
+  const int nbf = flat_blocks(cx.n);
+  {
+    ProfScope ps(PROF_CG_UPDATE, s);
+    cg_update_kernel<T><<<nbf, 256, 0, s>>>(cx.n, cx.mask0, (float *)(cx.base + cx.lo.e),
+                                            cx.lv[0].r, cur, Ap, cx.partials, st);
+  }
+  {
+    ProfScope ps(PROF_CONTROL, s);
+    inner_check_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials, nbf);
+  }
+  return cudaGetLastError();
+}
+
+__global__ void f32_to_f64_kernel(int64_t n, const float *a, double *b, const uint8_t *mask) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x)
+    b[c] = mcls(mask[c]) == BSP_FLUID ? (double)a[c] : 0.0;
+}
+__global__ void f64_to_f32_kernel(int64_t n, const double *a, float *b, const uint8_t *mask) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x)
+    b[c] = mcls(mask[c]) == BSP_FLUID ? (float)a[c] : 0.0f;
+}
+__global__ void __launch_bounds__(RED_THREADS) bnorm_kernel(SolverState *st,
+                                                            const double *partials, int nblocks) {
+  const double bb = reduce_slot(partials, 0, nblocks, false);
+  if (threadIdx.x == 0) st->b_norm2 = bb;
+}
+
+template <class T>
+int solve_impl(void *ws, const uint8_t *mask, const float *div, float *p_out, int nx, int ny,
+               int nz, float dx, float dt, float rho, const BspSolveParams *prm,
+               BspSolveInfo *info, cudaStream_t s) {
+  Ctx<T> cx = make_ctx<T>(ws, mask, nx, ny, nz, prm->storage);
+  {
+    const Level<T> &c = cx.lv[cx.lo.L - 1];
+    if ((int64_t)c.nx * c.ny * c.nz > COARSEST_MAX) return BSP_ERR_SHAPE;
+  }
+  SolverState h{};
+  h.tol = prm->tol;
+  h.eta = prm->inner_tol;
+  h.max_outer = prm->max_outer;
+  h.max_inner = prm->max_inner;
+  h.scale = 1.0;
+  cudaError_t e = cudaMemcpyAsync(cx.st, &h, sizeof(h), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return (int)e;
+  e = setup_levels<T>(cx, s);
+  if (e != cudaSuccess) return (int)e;
+  double *x = (double *)(cx.base + cx.lo.x);
+  float *eb = (float *)(cx.base + cx.lo.e);
+  const int nbr = row_blocks((int64_t)nx * ny);
+  const int nbf = flat_blocks(cx.n);
+  const double bscale = -((double)rho * (double)dx * (double)dx) / (double)dt;
+  // ||b||^2: a residual pass with x = 0
+  e = cudaMemsetAsync(x, 0, sizeof(double) * cx.n, s);
+  if (e != cudaSuccess) return (int)e;
+  {
+    ProfScope ps(PROF_RESID64, s);
+    residual64_kernel<T, false><<<nbr, 256, 0, s>>>(nx, ny, nz, mask, div, x, bscale, nullptr,
+                                                   nullptr, cx.partials, cx.st);
+  }
+  {
+    ProfScope ps(PROF_CONTROL, s);
+    bnorm_kernel<<<1, RED_THREADS, 0, s>>>(cx.st, cx.partials, nbr);
+  }
+  if (prm->warm_start && p_out) {
+    ProfScope ps(PROF_CONTROL, s);
+    f32_to_f64_kernel<<<nbf, 256, 0, s>>>(cx.n, p_out, x, mask);
+  }
+  int flag = 0;
+  for (int outer = 0; outer <= prm->max_outer; ++outer) {
+    {
+      ProfScope ps(PROF_RESID64, s);
+      residual64_kernel<T, false><<<nbr, 256, 0, s>>>(nx, ny, nz, mask, div, x, bscale,
+                                                     nullptr, nullptr, cx.partials, cx.st);
+    }
+    {
+      ProfScope ps(PROF_CONTROL, s);
+      outer_check_kernel<<<1, RED_THREADS, 0, s>>>(cx.st, cx.partials, nbr,
+                                                   prm->storage == BSP_STORE_FP32);
+    }
+    {
+      ProfScope ps(PROF_RESID64, s);
+      residual64_kernel<T, true><<<nbr, 256, 0, s>>>(nx, ny, nz, mask, div, x, bscale,
+                                                    cx.lv[0].r, eb, cx.partials, cx.st);
+    }
+    // 4-byte flag read (pageable: the copy completes before the sync returns)
+    e = cudaMemcpyAsync(&flag, &cx.st->done, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess || flag) break;
+    for (int chunk = 0;; ++chunk) {
+      for (int q = 0; q < prm->check_every; ++q)
+        launch_inner_iteration<T>(cx, (chunk * prm->check_every + q) & 1, s);
+      e = cudaMemcpyAsync(&flag, &cx.st->inner_done, sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess || flag) break;
+    }
+    if (e != cudaSuccess) break;
+    ProfScope ps(PROF_XUPDATE, s);
+    xupdate_kernel<<<nbf, 256, 0, s>>>(cx.n, x, eb, nullptr, cx.st);
+  }
+  if (e != cudaSuccess) return (int)e;
+  SolverState fin{};
+  if (p_out) {
+    ProfScope ps(PROF_CONTROL, s);
+    f64_to_f32_kernel<<<nbf, 256, 0, s>>>(cx.n, x, p_out, mask);
+  }
+  e = cudaMemcpyAsync(&fin, cx.st, sizeof(SolverState), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return (int)e;
+  if (info) {
+    info->outer_iterations = fin.outer_it;
+    info->inner_iterations = fin.total_inner;
+    info->rel_residual = fin.rel;
+    info->levels = cx.lo.L;
+  }
+  return fin.status;
+}
+
+}  // namespace bsp
+
+using namespace bsp;
+
+extern "C" size_t bsp_solver_workspace_bytes(int nx, int ny, int nz, int storage) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return 0;
+  return make_layout(nx, ny, nz, storage).total;
+}
+
+extern "C" void bsp_solve_params_default(BspSolveParams *p) {
+  if (!p) return;
+  p->tol = 1e-6;
+  p->inner_tol = 1e-3;
+  p->max_outer = 8;
+  p->max_inner = 200;
+  p->storage = BSP_STORE_FP32;
+  p->warm_start = 0;
+  p->check_every = 8;
+}
+
+extern "C" int bsp_solve_tol(float *p, const float *div_u, const uint8_t *mask, int nx, int ny,
+                             int nz, float dx, float dt, float rho, const BspSolveParams *params,
+                             void *workspace, size_t workspace_bytes, double *x64_out,
+                             BspSolveInfo *info, cudaStream_t stream) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_OK;
+  if (!div_u || !mask || !params || !workspace) return BSP_ERR_NULL;
+  if (((uintptr_t)workspace & 255u) != 0) return BSP_ERR_ALIGN;
+  if (workspace_bytes < bsp_solver_workspace_bytes(nx, ny, nz, params->storage))
+    return BSP_ERR_WORKSPACE;
+  if (params->storage < 0 || params->storage > 2 || params->check_every <= 0 ||
+      params->max_inner <= 0 || params->max_outer < 0 || !(params->tol >= 0.0))
+    return BSP_ERR_ARG;
+  int st;
+  switch (params->storage) {
+    case BSP_STORE_FP16:
+      st = solve_impl<__half>(workspace, mask, div_u, p, nx, ny, nz, dx, dt, rho, params, info,
+                              stream);
+      break;
+    case BSP_STORE_BF16:
+      st = solve_impl<__nv_bfloat16>(workspace, mask, div_u, p, nx, ny, nz, dx, dt, rho, params,
+                                     info, stream);
+      break;
+    default:
+      st = solve_impl<float>(workspace, mask, div_u, p, nx, ny, nz, dx, dt, rho, params, info,
+                             stream);
+  }
+  if (x64_out && (st == BSP_OK || st == BSP_NOT_CONVERGED)) {
+    const Layout lo = make_layout(nx, ny, nz, params->storage);
+    cudaMemcpyAsync(x64_out, (char *)workspace + lo.x, sizeof(double) * (size_t)nx * ny * nz,
+                    cudaMemcpyDeviceToDevice, stream);
+  }
+  return st;
+}

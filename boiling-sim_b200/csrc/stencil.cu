@@ -17,6 +17,7 @@
 //   * generic kernel: one thread per cell, any shape or alignment.
 // Both produce bit-identical results (same per-cell operation order).
 #include "bsp_common.cuh"
+#include "profile.cuh"
 
 namespace bsp {
 
@@ -27,118 +28,134 @@ __device__ __forceinline__ uint32_t cls1(const uint8_t *m, int64_t c, int, int) 
 __device__ __forceinline__ uint32_t cls1(const int32_t *m, int64_t c, int mf, int ma) {
   return classify(__ldg(m + c), mf, ma);
 }
-__device__ __forceinline__ uint32_t cls4(const uint8_t *m, int64_t c, int, int) {
-  return __ldg(reinterpret_cast<const uint32_t *>(m + c)) & 0x03030303u;
+// Four packed mask bytes (bit 7 fluid, bit 6 solid) of cells c..c+3.
+__device__ __forceinline__ uint32_t mw4(const uint8_t *m, int64_t c, int, int) {
+  return __ldg(reinterpret_cast<const uint32_t *>(m + c));
 }
-__device__ __forceinline__ uint32_t cls4(const int32_t *m, int64_t c, int mf, int ma) {
+__device__ __forceinline__ uint32_t mw4(const int32_t *m, int64_t c, int mf, int ma) {
   int4 v = __ldg(reinterpret_cast<const int4 *>(m + c));
-  return classify(v.x, mf, ma) | (classify(v.y, mf, ma) << 8) |
-         (classify(v.z, mf, ma) << 16) | (classify(v.w, mf, ma) << 24);
+  return enc_cls(classify(v.x, mf, ma)) | (enc_cls(classify(v.y, mf, ma)) << 8) |
+         (enc_cls(classify(v.z, mf, ma)) << 16) | (enc_cls(classify(v.w, mf, ma)) << 24);
+}
+__device__ __forceinline__ uint32_t mw1(const uint8_t *m, int64_t c, int, int) {
+  return __ldg(m + c);
+}
+__device__ __forceinline__ uint32_t mw1(const int32_t *m, int64_t c, int mf, int ma) {
+  return enc_cls(classify(__ldg(m + c), mf, ma));
 }
 
-constexpr uint32_t AIR4 = 0x01010101u;
-
-enum Op { OP_JACOBI = 0, OP_SPMV = 1 };
+// Stencil flavours of the column kernel.
+enum Op {
+  OP_JACOBI = 0,      // p_new = (s - rho dx^2 div / dt) / 6, division per cell
+  OP_SPMV = 1,        // A p = 6 p - s
+  OP_JACOBI_RHS = 2,  // p_new = (s - rhs) / 6 with rhs = rho dx^2 div / dt precomputed
+};
 
 __device__ __forceinline__ float f4(const float4 &v, int q) {
   return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
 }
+__device__ __forceinline__ float4 ld4(const float *p) {
+  return __ldg(reinterpret_cast<const float4 *>(p));
+}
 
 // ---- column kernel ----------------------------------------------------------
-template <int OP, class MaskT>
+// CTA = 8 warps; warp w owns row j = blockIdx.y*8 + w and the 128 cells
+// k = blockIdx.x*128 + 4*lane .. +3, and marches i over [blockIdx.z*bi, +bi).
+// The i-1 / i / i+1 planes of p and of the mask stay in registers; j +- 1 come
+// from L1 (neighbouring warps' rows); k +- 1 from warp shuffles.  Neighbour
+// values are chosen with sel_nbr (two prmt + one lop3, no branches); the sum
+// order is the reference's l, r, d, u, b, f.
+template <int OP, class MaskT, bool FULL>
 __global__ void __launch_bounds__(256) stencil_col_kernel(
-    float *__restrict__ out, const float *__restrict__ p, const float *__restrict__ div,
+    float *__restrict__ out, const float *__restrict__ p, const float *__restrict__ src,
     const MaskT *__restrict__ mask, int nx, int ny, int nz, int bi, float rdd, float dt,
     int mf, int ma) {
   const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nz4 = nz >> 2;
-  const int k4 = blockIdx.x * 32 + lane;
-  const int j = blockIdx.y * 8 + warp;
+  const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
   if (j >= ny) return;  // warp-uniform
+  const int k = (blockIdx.x * 32 + lane) * 4;
+  const bool act = FULL || k < nz;
   const int i0 = blockIdx.z * bi;
   const int i1 = min(i0 + bi, nx);
-  const bool act = k4 < nz4;
-  const int k = k4 * 4;
   const int64_t plane = (int64_t)ny * nz;
-  const int64_t col = (int64_t)j * nz + k;
-  const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  const bool has_jm = j > 0, has_jp = j + 1 < ny;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  int64_t o = (int64_t)i0 * plane + (int64_t)j * nz + k;
 
-  float4 pm = zero4, pc = zero4;
-  uint32_t cmm = AIR4, cmc = AIR4;
-  if (act && i0 - 1 >= 0) {
-    pm = __ldg(reinterpret_cast<const float4 *>(p + (i0 - 1) * plane + col));
-    cmm = cls4(mask, (i0 - 1) * plane + col, mf, ma);
+  float4 pm = z4, pc = z4;
+  uint32_t mm = 0u, mc = 0u;  // 0 = air
+  if (act && i0 > 0) {
+    pm = ld4(p + o - plane);
+    mm = mw4(mask, o - plane, mf, ma);
   }
   if (act) {
-    pc = __ldg(reinterpret_cast<const float4 *>(p + i0 * plane + col));
-    cmc = cls4(mask, i0 * plane + col, mf, ma);
+    pc = ld4(p + o);
+    mc = mw4(mask, o, mf, ma);
   }
-  for (int i = i0; i < i1; ++i) {
-    const int64_t base = i * plane + col;
-    float4 pn = zero4, pjm = zero4, pjp = zero4, dv = zero4;
-    uint32_t cmn = AIR4, cjm = AIR4, cjp = AIR4;
+  for (int i = i0; i < i1; ++i, o += plane) {
+    float4 pn = z4, pjm = z4, pjp = z4, sv = z4;
+    uint32_t mn = 0u, mjm = 0u, mjp = 0u;
     if (act) {
       if (i + 1 < nx) {
-        pn = __ldg(reinterpret_cast<const float4 *>(p + base + plane));
-        cmn = cls4(mask, base + plane, mf, ma);
+        pn = ld4(p + o + plane);
+        mn = mw4(mask, o + plane, mf, ma);
       }
-      if (j > 0) {
-        pjm = __ldg(reinterpret_cast<const float4 *>(p + base - nz));
-        cjm = cls4(mask, base - nz, mf, ma);
+      if (has_jm) {
+        pjm = ld4(p + o - nz);
+        mjm = mw4(mask, o - nz, mf, ma);
       }
-      if (j + 1 < ny) {
-        pjp = __ldg(reinterpret_cast<const float4 *>(p + base + nz));
-        cjp = cls4(mask, base + nz, mf, ma);
+      if (has_jp) {
+        pjp = ld4(p + o + nz);
+        mjp = mw4(mask, o + nz, mf, ma);
       }
-      if (OP == OP_JACOBI) dv = __ldg(reinterpret_cast<const float4 *>(div + base));
+      if (OP != OP_SPMV) sv = ld4(src + o);
     }
-    // k neighbours across lanes
     float pkm = __shfl_up_sync(0xffffffffu, pc.w, 1);
-    uint32_t ckm = __shfl_up_sync(0xffffffffu, cmc, 1) >> 24;
+    uint32_t mkm = __shfl_up_sync(0xffffffffu, mc, 1);
     float pkp = __shfl_down_sync(0xffffffffu, pc.x, 1);
-    uint32_t ckp = __shfl_down_sync(0xffffffffu, cmc, 1) & 0xffu;
+    uint32_t mkp = __shfl_down_sync(0xffffffffu, mc, 1);
     if (lane == 0) {
-      pkm = 0.f;
-      ckm = BSP_AIR;
-      if (act && k > 0) {
-        pkm = __ldg(p + base - 1);
-        ckm = cls1(mask, base - 1, mf, ma);
-      }
+      const bool in = act && k > 0;
+      pkm = in ? __ldg(p + o - 1) : 0.0f;
+      mkm = in ? mw1(mask, o - 1, mf, ma) << 24 : 0u;
     }
     if (lane == 31) {
-      pkp = 0.f;
-      ckp = BSP_AIR;
-      if (act && k + 4 < nz) {
-        pkp = __ldg(p + base + 4);
-        ckp = cls1(mask, base + 4, mf, ma);
-      }
+      const bool in = act && k + 4 < nz;
+      pkp = in ? __ldg(p + o + 4) : 0.0f;
+      mkp = in ? mw1(mask, o + 4, mf, ma) : 0u;
     }
+    // mask words of the back (k-1) and front (k+1) neighbours of the 4 cells
+    const uint32_t mb = (mc << 8) | (mkm >> 24);
+    const uint32_t mfw = (mc >> 8) | (mkp << 24);
+    const float4 pb = make_float4(pkm, pc.x, pc.y, pc.z);
+    const float4 pf = make_float4(pc.y, pc.z, pc.w, pkp);
     if (act) {
-      float o[4];
+      float o4[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const uint32_t cs = byte_of(cmc, q);
         const float ps = f4(pc, q);
-        const float l = nbr(byte_of(cmm, q), f4(pm, q), ps);
-        const float r = nbr(byte_of(cmn, q), f4(pn, q), ps);
-        const float d = nbr(byte_of(cjm, q), f4(pjm, q), ps);
-        const float u = nbr(byte_of(cjp, q), f4(pjp, q), ps);
-        const float b = q == 0 ? nbr(ckm, pkm, ps) : nbr(byte_of(cmc, q - 1), f4(pc, q - 1), ps);
-        const float f = q == 3 ? nbr(ckp, pkp, ps) : nbr(byte_of(cmc, q + 1), f4(pc, q + 1), ps);
+        const float l = sel_nbr(mm, mm << 1, q, f4(pm, q), ps);
+        const float r = sel_nbr(mn, mn << 1, q, f4(pn, q), ps);
+        const float d = sel_nbr(mjm, mjm << 1, q, f4(pjm, q), ps);
+        const float u = sel_nbr(mjp, mjp << 1, q, f4(pjp, q), ps);
+        const float b = sel_nbr(mb, mb << 1, q, f4(pb, q), ps);
+        const float f = sel_nbr(mfw, mfw << 1, q, f4(pf, q), ps);
         float v;
-        if (OP == OP_JACOBI)
-          v = jacobi_update(l, r, d, u, b, f, f4(dv, q), rdd, dt);
-        else
+        if (OP == OP_SPMV) {
           v = spmv_update(l, r, d, u, b, f, ps);
-        o[q] = cs == BSP_FLUID ? v : 0.0f;
+        } else {
+          const float s = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(l, r), d), u), b), f);
+          const float rhs = OP == OP_JACOBI ? __fdiv_rn(__fmul_rn(rdd, f4(sv, q)), dt) : f4(sv, q);
+          v = div6(__fsub_rn(s, rhs));
+        }
+        o4[q] = __uint_as_float(__float_as_uint(v) & fluid_word(mc, q));
       }
-      *reinterpret_cast<float4 *>(out + base) = make_float4(o[0], o[1], o[2], o[3]);
+      *reinterpret_cast<float4 *>(out + o) = make_float4(o4[0], o4[1], o4[2], o4[3]);
     }
     pm = pc;
-    cmm = cmc;
+    mm = mc;
     pc = pn;
-    cmc = cmn;
+    mc = mn;
   }
 }
 
@@ -167,8 +184,14 @@ __global__ void __launch_bounds__(256) stencil_generic_kernel(
     const float d = NBR(j > 0, -(int64_t)nz), u = NBR(j + 1 < ny, (int64_t)nz);
     const float b = NBR(k > 0, -1), f = NBR(k + 1 < nz, 1);
 #undef NBR
-    out[c] = OP == OP_JACOBI ? jacobi_update(l, r, d, u, b, f, __ldg(div + c), rdd, dt)
-                             : spmv_update(l, r, d, u, b, f, ps);
+    if (OP == OP_SPMV) {
+      out[c] = spmv_update(l, r, d, u, b, f, ps);
+    } else {
+      const float s = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(l, r), d), u), b), f);
+      const float rhs =
+          OP == OP_JACOBI ? __fdiv_rn(__fmul_rn(rdd, __ldg(div + c)), dt) : __ldg(div + c);
+      out[c] = div6(__fsub_rn(s, rhs));
+    }
   }
 }
 
@@ -227,7 +250,7 @@ __global__ void mask_from_mat_kernel(uint8_t *__restrict__ mask, const int32_t *
     SOL(k > 0, -1);
     SOL(k + 1 < nz, 1);
 #undef SOL
-    mask[c] = (uint8_t)(cls | (ns << 2));
+    mask[c] = (uint8_t)(enc_cls(cls) | ns);
   }
 }
 
@@ -265,6 +288,9 @@ static inline int generic_blocks(int64_t n) {
 
 // i-extent per CTA of the column kernel: enough CTAs for ~8 waves of 148 SMs
 // while keeping the i-halo re-read (2/bi) small.
+// Autotuner override of the column kernel's i-extent (0 = heuristic below).
+int g_sweep_bi = 0;
+
 static inline int pick_bi(int nx, int ny, int nz) {
   const int64_t cols = (int64_t)((nz / 4 + 31) / 32) * ((ny + 7) / 8);
   const int64_t target = (int64_t)num_sms() * 8;
@@ -279,13 +305,17 @@ cudaError_t launch_stencil(float *out, const float *p, const float *div, const M
                            int ma, cudaStream_t s) {
   const float rdd = rho * dx * dx;  // (rho*dx)*dx in float, as the reference evaluates it
   const bool col_ok = (nz % 4 == 0) && aligned16(out) && aligned16(p) &&
-                      (OP != OP_JACOBI || aligned16(div)) &&
+                      (OP == OP_SPMV || aligned16(div)) &&
                       (sizeof(MaskT) == 4 ? aligned16(mask) : (((uintptr_t)mask & 3u) == 0));
   if (col_ok) {
-    const int bi = pick_bi(nx, ny, nz);
+    const int bi = g_sweep_bi > 0 ? g_sweep_bi : pick_bi(nx, ny, nz);
     dim3 grid((nz / 4 + 31) / 32, (ny + 7) / 8, (nx + bi - 1) / bi);
-    stencil_col_kernel<OP, MaskT><<<grid, 256, 0, s>>>(out, p, div, mask, nx, ny, nz, bi, rdd,
-                                                       dt, mf, ma);
+    if (nz % 128 == 0)
+      stencil_col_kernel<OP, MaskT, true><<<grid, 256, 0, s>>>(out, p, div, mask, nx, ny, nz,
+                                                               bi, rdd, dt, mf, ma);
+    else
+      stencil_col_kernel<OP, MaskT, false><<<grid, 256, 0, s>>>(out, p, div, mask, nx, ny, nz,
+                                                                bi, rdd, dt, mf, ma);
   } else {
     const int64_t n = (int64_t)nx * ny * nz;
     stencil_generic_kernel<OP, MaskT><<<generic_blocks(n), 256, 0, s>>>(out, p, div, mask, nx,
@@ -300,6 +330,29 @@ template cudaError_t launch_stencil<OP_JACOBI, uint8_t>(float *, const float *, 
 template cudaError_t launch_stencil<OP_SPMV, uint8_t>(float *, const float *, const float *,
                                                       const uint8_t *, int, int, int, float,
                                                       float, float, int, int, cudaStream_t);
+template cudaError_t launch_stencil<OP_JACOBI_RHS, uint8_t>(float *, const float *,
+                                                            const float *, const uint8_t *, int,
+                                                            int, int, float, float, float, int,
+                                                            int, cudaStream_t);
+
+// rhs[c] = (rho dx dx) div[c] / dt on fluid cells (0 elsewhere): the per-cell
+// constant of the Jacobi update, bit-identical to the value each sweep of the
+// reference computes (fluid.py:275).
+// rhs may alias div (in-place conversion): no __restrict__ on those two.
+__global__ void rhs_kernel(float *rhs, const float *div, const uint8_t *__restrict__ mask,
+                           int64_t n, float rdd, float dt) {
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x)
+    rhs[c] = (__ldg(mask + c) & BSP_MFLUID) ? __fdiv_rn(__fmul_rn(rdd, div[c]), dt) : 0.0f;
+}
+
+cudaError_t launch_rhs(float *rhs, const float *div, const uint8_t *mask, int64_t n, float dx,
+                       float dt, float rho, cudaStream_t s) {
+  const float rdd = rho * dx * dx;
+  ProfScope ps(PROF_PROJ, s);
+  rhs_kernel<<<generic_blocks(n), 256, 0, s>>>(rhs, div, mask, n, rdd, dt);
+  return cudaGetLastError();
+}
 
 static inline bool shape_ok(int nx, int ny, int nz) {
   return (int64_t)nx * ny * nz <= (int64_t)1 << 40;
@@ -400,4 +453,15 @@ extern "C" int bsp_selftest_div6(unsigned long long *mismatches_dev, cudaStream_
   if (e != cudaSuccess) return (int)e;
   selftest_div6_kernel<<<num_sms() * 8, 256, 0, stream>>>(mismatches_dev);
   return (int)cudaGetLastError();
+}
+
+extern "C" int bsp_set_tuning(int key, int value) {
+  switch (key) {
+    case BSP_TUNE_SWEEP_BI:
+      if (value < 0 || value > 4096) return BSP_ERR_ARG;
+      bsp::g_sweep_bi = value;
+      return BSP_OK;
+    default:
+      return BSP_ERR_ARG;
+  }
 }

@@ -43,10 +43,15 @@ extern "C" {
 #define BSP_ERR_ALIGN 10008        /* pointer alignment unusable */
 #define BSP_ERR_ARG 10009          /* other invalid argument */
 
-/* cell classes of the uint8 mask */
-#define BSP_CLASS_FLUID 0
-#define BSP_CLASS_AIR 1
-#define BSP_CLASS_SOLID 2
+/* uint8 cell mask: bit 7 fluid, bit 6 solid (air: neither -- a zero byte is
+ * air, like a cell outside the grid), bits 0-2 number of solid face neighbours */
+#define BSP_CLASS_FLUID 0x80
+#define BSP_CLASS_SOLID 0x40
+#define BSP_CLASS_AIR 0x00
+#define BSP_MASK_NSOLID 0x07
+
+/* autotuner keys of bsp_set_tuning */
+#define BSP_TUNE_SWEEP_BI 1 /* i-planes per CTA of the sweep kernels (0 = heuristic) */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */
@@ -129,7 +134,7 @@ const char *bsp_version(void);
 /* Message for a status code returned by any entry point (static storage). */
 const char *bsp_error_string(int code);
 
-/* mask[c] = class of mat[c] (BSP_CLASS_*, bits 0-1) | n_solid << 2, where
+/* mask[c] = class of mat[c] (BSP_CLASS_*) | n_solid, where
  * n_solid counts the face neighbours that are neither fluid nor air (the
  * Jacobi preconditioner diagonal is 6 - n_solid, diag_inverse_apply.cu:62-78).
  * Derived once per geometry: the reference's mat is static after
@@ -144,11 +149,31 @@ int bsp_jacobi_sweep(float *p_new, const float *p_old, const float *div_u,
                      float rho, cudaStream_t stream);
 
 /* n_iter sweeps, ping-pong p <-> p_tmp, result in p (jacobi_pressure.cu:228-270
- * on the uint8 mask).  tblock = sweeps fused per HBM pass (0 = autotuned,
- * 1 = one sweep per launch); results are bit-identical for every tblock. */
-int bsp_jacobi_solve(float *p, float *p_tmp, const float *div_u, const uint8_t *mask,
-                     int nx, int ny, int nz, float dx, float dt, float rho, int n_iter,
-                     int tblock, cudaStream_t stream);
+ * on the uint8 mask).  If rhs_ws (n floats, 16-byte aligned) is given, the
+ * per-cell constant rho dx^2 div / dt is evaluated into it once and the
+ * sweeps read it (bit-identical results, no division per sweep); rhs_ws may
+ * equal div_u, which then holds that constant afterwards.  tblock is
+ * reserved (sweeps fused per HBM pass; 0 or 1 today). */
+int bsp_jacobi_solve(float *p, float *p_tmp, const float *div_u, float *rhs_ws,
+                     const uint8_t *mask, int nx, int ny, int nz, float dx, float dt, float rho,
+                     int n_iter, int tblock, cudaStream_t stream);
+
+/* Set an autotuner parameter (BSP_TUNE_*) for subsequent launches in this
+ * process.  Not thread-safe against concurrent launches. */
+int bsp_set_tuning(int key, int value);
+
+/* Per-kernel-class event timing (tracing).  While enabled, every launch of an
+ * instrumented kernel is bracketed by CUDA events on its stream.  Classes:
+ * 0 sweep, 1 restriction from the fine level, 2 prolongation onto the fine
+ * level, 3 search direction + A ps, 4 CG vector update, 5 FP64 residual,
+ * 6 FP64 iterate update, 7 coarse multigrid levels, 8 control / setup
+ * kernels, 9 divergence / gradient / no-slip / rhs.
+ * bsp_profile_read waits for the recorded launches, writes the summed
+ * milliseconds and launch counts of classes 0..nclass-1 and clears the
+ * record. */
+#define BSP_PROF_NCLASS 10
+int bsp_profile_enable(int on);
+int bsp_profile_read(double *ms, long long *launches, int nclass);
 
 /* div = divergence of the MAC velocity on fluid cells, 0 elsewhere
  * (fluid.py:201-218).  If max_abs_div is non-NULL it receives max|div| as a
@@ -179,6 +204,51 @@ int bsp_projection_jacobi(float *p, float *p_tmp, float *div_u, float *ux, float
 /* Ap = (6I - S) p on the uint8 mask (laplacian_spmv.cu:62-143). */
 int bsp_spmv(float *Ap, const float *p, const uint8_t *mask, int nx, int ny, int nz,
              cudaStream_t stream);
+
+/* ---- to-tolerance solve ------------------------------------------------
+ * Solves A p = b (the system of pressure_solve_pcg.cu:129-139) to
+ * ||b - A p||_2 <= tol ||b||_2 with the residual evaluated in FP64 from an
+ * FP64 iterate: FP64 iterative refinement around a conjugate gradient
+ * preconditioned by a geometric multigrid V-cycle (Jacobi smoothing), inner
+ * vectors stored in FP32, FP16 or BF16, inner products in FP64.  Replaces the
+ * to-tolerance role of pressure_solve_pcg_launch (pressure_solve_pcg.cu:89-243,
+ * tolerance semantics python/boilingsim/config.py:166-176). */
+#define BSP_STORE_FP32 0
+#define BSP_STORE_FP16 1
+#define BSP_STORE_BF16 2
+
+typedef struct BspSolveParams {
+  double tol;       /* relative residual target (FP64 residual) */
+  double inner_tol; /* inner CG stops at ||r_inner|| <= inner_tol ||rhat|| */
+  int max_outer;    /* refinement passes */
+  int max_inner;    /* CG iterations per pass */
+  int storage;      /* BSP_STORE_* for the inner vectors and multigrid levels */
+  int warm_start;   /* 1: p holds the initial guess on entry; 0: cold start */
+  int check_every;  /* inner iterations enqueued between host reads of the done flag */
+} BspSolveParams;
+
+typedef struct BspSolveInfo {
+  int outer_iterations;
+  int inner_iterations;
+  int levels;
+  int pad;
+  double rel_residual; /* FP64 ||b - A x|| / ||b|| of the FP64 iterate */
+} BspSolveInfo;
+
+void bsp_solve_params_default(BspSolveParams *params);
+
+/* Bytes of caller-owned workspace the solve needs (256-byte aligned). */
+size_t bsp_solver_workspace_bytes(int nx, int ny, int nz, int storage);
+
+/* p (float, out; in when warm_start) receives the FP64 iterate rounded to
+ * float (0 on non-fluid cells); x64_out (optional, device doubles) receives
+ * the FP64 iterate itself.  Returns BSP_OK, BSP_NOT_CONVERGED, or an error.
+ * Synchronises the stream once per refinement pass and once per
+ * check_every inner iterations (4-byte flag reads). */
+int bsp_solve_tol(float *p, const float *div_u, const uint8_t *mask, int nx, int ny, int nz,
+                  float dx, float dt, float rho, const BspSolveParams *params, void *workspace,
+                  size_t workspace_bytes, double *x64_out, BspSolveInfo *info,
+                  cudaStream_t stream);
 
 /* Exhaustive self-check of the device division-by-6 against IEEE division
  * over all 2^32 float bit patterns; the mismatch count is written to the

@@ -249,6 +249,16 @@ def rel_residual(p, div, mat, dx, dt, rho, mat_fluid=MAT_FLUID, mat_air=MAT_AIR)
                                            mat_fluid, mat_air))
 
 
+def rel_residual64(p64, div, mat, dx, dt, rho, mat_fluid=MAT_FLUID, mat_air=MAT_AIR):
+    """||b - A p||_2 / ||b||_2 in FP64 for an FP64 pressure (non-fluid ignored)."""
+    mat = _c(mat, np.int32)
+    p = np.where(mat == mat_fluid, np.asarray(p64, np.float64), 0.0)
+    b = rhs_f64(div, mat, dx, dt, rho, mat_fluid)
+    r = b - apply_A_f64(p, mat, mat_fluid, mat_air)
+    bn = float(np.sqrt((b * b).sum()))
+    return float(np.sqrt((r * r).sum())) / bn if bn > 0 else 0.0
+
+
 def rel_error(p, p_star, mat, mat_fluid=MAT_FLUID):
     """||p - p*||_2 / ||p*||_2 over fluid cells."""
     f = np.asarray(mat) == mat_fluid

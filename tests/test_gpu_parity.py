@@ -100,11 +100,13 @@ def test_fixed_count_solve_single_carrot(cuda, n_iter):
     call("pressure_solve_launch", ptr(p), ptr(tmp), ptr(d), ptr(m), nx, ny, nz, 0.004, 0.01,
          997.0, n_iter, 0, 2)
     assert np.array_equal(bits(host(p)), bits(want))
-    p2 = torch.zeros_like(p)
-    tmp2 = torch.zeros_like(p)
-    call("bsp_jacobi_solve", ptr(p2), ptr(tmp2), ptr(d), ptr(mask_of(m)), nx, ny, nz, 0.004, 0.01,
-         997.0, n_iter, 0, 0)
-    assert np.array_equal(bits(host(p2)), bits(want))
+    m8 = mask_of(m)
+    for rhs_ws in (None, torch.zeros_like(p)):
+        p2 = torch.zeros_like(p)
+        tmp2 = torch.zeros_like(p)
+        call("bsp_jacobi_solve", ptr(p2), ptr(tmp2), ptr(d), ptr(rhs_ws), ptr(m8), nx, ny, nz,
+             0.004, 0.01, 997.0, n_iter, 0, 0)
+        assert np.array_equal(bits(host(p2)), bits(want))
 
 
 @pytest.mark.parametrize("spec", [S.POT_64, S.PotSpec(40, 36, 30, 14, 2, 24, 4, 12)],

@@ -1,0 +1,80 @@
+"""GPU tests of the to-tolerance solver (bsp_solve_tol) against the FP64 CPU
+oracle: the FP64 residual of the returned iterate, the error against the FP64
+oracle solve p*, storage variants, warm start, degenerate inputs."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from boilingsim_b200 import scenes as S
+from boilingsim_b200.fluid import cell_mask
+from boilingsim_b200.solver import TolSolver, solve_tolerance
+
+pytestmark = pytest.mark.gpu
+
+DX, DT, RHO = 0.002, 0.01, 997.0
+
+
+@pytest.fixture(scope="module")
+def pot64():
+    mat = S.pot_mat(S.POT_64)
+    ux, uy, uz = S.velocity_field(mat, seed=7)
+    div = O.divergence(ux, uy, uz, mat, DX)
+    p_star, _, rel = O.solve_f64(div, mat, DX, DT, RHO, tol=1e-13)
+    assert rel < 1e-12
+    return mat, div, p_star
+
+
+@pytest.mark.parametrize("storage,tol", [("fp32", 1e-6), ("fp32", 1e-9), ("fp16", 1e-6),
+                                         ("bf16", 1e-6)])
+def test_solve_reaches_fp64_residual(cuda, pot64, storage, tol):
+    mat, div, p_star = pot64
+    res = solve_tolerance(div, mat, DX, DT, RHO, tol=tol, storage=storage)
+    assert res.status == 0
+    rel = O.rel_residual64(res.p64, div, mat, DX, DT, RHO)
+    # the device's FP64 residual agrees with the oracle's evaluation
+    assert rel <= tol * 1.0001 and abs(rel - res.rel_residual) <= 1e-3 * rel + 1e-15
+    err = O.rel_error(res.p64, p_star, mat)
+    assert err < 50 * tol
+    # the float output is the FP64 iterate rounded
+    p32 = res.p.cpu().numpy()
+    assert np.array_equal(p32, np.where(mat == 0, res.p64, 0.0).astype(np.float32))
+    assert res.levels >= 3
+    assert res.inner_iterations < 120
+
+
+def test_warm_start_from_solution_needs_no_inner_work(cuda, pot64):
+    mat, div, p_star = pot64
+    mat_t = torch.as_tensor(mat).cuda()
+    solver = TolSolver(cell_mask(mat_t))
+    div_t = torch.as_tensor(div).cuda()
+    p0 = torch.as_tensor(p_star.astype(np.float32)).cuda()
+    res = solver.solve(div_t, DX, DT, RHO, tol=1e-5, p=p0, warm_start=True)
+    assert res.status == 0 and res.inner_iterations == 0
+
+
+def test_zero_rhs_gives_zero_pressure(cuda, pot64):
+    mat, div, _ = pot64
+    res = solve_tolerance(np.zeros_like(div), mat, DX, DT, RHO, tol=1e-6)
+    assert res.status == 0 and res.inner_iterations == 0
+    assert not res.p.cpu().numpy().any()
+
+
+def test_not_converged_is_reported(cuda, pot64):
+    mat, div, _ = pot64
+    res = solve_tolerance(div, mat, DX, DT, RHO, tol=1e-12, max_outer=1, max_inner=2,
+                          raise_on_fail=False)
+    assert res.status == 10005 and res.rel_residual > 1e-12
+
+
+@pytest.mark.parametrize("spec", [S.pot_192(2), S.PotSpec(70, 54, 37, 22, 3, 29, 5, 20)],
+                         ids=["pot192", "odd70x54x37"])
+def test_solve_other_shapes(cuda, spec):
+    mat = S.pot_mat(spec)
+    ux, uy, uz = S.velocity_field(mat, seed=11)
+    div = O.divergence(ux, uy, uz, mat, DX)
+    res = solve_tolerance(div, mat, DX, DT, RHO, tol=1e-6)
+    assert res.status == 0
+    assert O.rel_residual64(res.p64, div, mat, DX, DT, RHO) <= 1e-6
