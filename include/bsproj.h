@@ -250,6 +250,22 @@ int bsp_solve_tol(float *p, const float *div_u, const uint8_t *mask, int nx, int
                   size_t workspace_bytes, double *x64_out, BspSolveInfo *info,
                   cudaStream_t stream);
 
+/* *result_dev = x . y accumulated in FP64 (fixed reduction order), for
+ * callers that cannot allocate device memory.  No counterpart in the
+ * reference: it is dot_launch without the workspace argument, for hosts that
+ * reach this library through its C ABI holding only their own arrays, or
+ * that step under a device-memory budget fixed at start-up and may not call
+ * cudaMalloc.  Its partial sums live in a file-scope __device__ array of 1024
+ * doubles (8 KiB per GPU, kept until exit); n may be at most 67,108,864
+ * (1024 partials x 65,536 elements), larger n returns BSP_ERR_SHAPE.  All
+ * calls share that array: calls that overlap on the GPU race and must be
+ * serialised.  The first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) and should come before any stream capture.
+ * Allocates nothing; never calls cudaMalloc or cudaFree. */
+#define BSP_DOT_NOALLOC_MAX_N 67108864LL
+int bsp_dot_noalloc(const float *x, const float *y, int64_t n, double *result_dev,
+                    cudaStream_t stream);
+
 /* Exhaustive self-check of the device division-by-6 against IEEE division
  * over all 2^32 float bit patterns; the mismatch count is written to the
  * device counter *mismatches_dev (zeroed first). */
