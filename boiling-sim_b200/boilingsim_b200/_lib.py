@@ -64,7 +64,7 @@ class BspSolveParams(ctypes.Structure):
     _fields_ = [("tol", ctypes.c_double), ("inner_tol", ctypes.c_double),
                 ("max_outer", ctypes.c_int), ("max_inner", ctypes.c_int),
                 ("storage", ctypes.c_int), ("warm_start", ctypes.c_int),
-                ("check_every", ctypes.c_int)]
+                ("check_every", ctypes.c_int), ("reuse_setup", ctypes.c_int)]
 
 
 class BspSolveInfo(ctypes.Structure):

@@ -56,6 +56,11 @@ class TolSolver:
         self.params = BspSolveParams()
         _lib.lib().bsp_solve_params_default(ctypes.byref(self.params))
         self.params.storage = self.storage
+        # the mask is fixed for this solver's lifetime: build the multigrid
+        # levels on the first solve (never trust a record left by an earlier
+        # workspace at the same address), reuse them afterwards
+        self.params.reuse_setup = 0
+        self._setup_done = False
 
     def solve(self, div: torch.Tensor, dx: float, dt: float, rho: float, tol: float = 1e-6,
               p: torch.Tensor | None = None, warm_start: bool = False, inner_tol: float | None = None,
@@ -67,6 +72,7 @@ class TolSolver:
         prm = BspSolveParams.from_buffer_copy(self.params)
         prm.tol = float(tol)
         prm.warm_start = 1 if warm_start else 0
+        prm.reuse_setup = 1 if self._setup_done else 0
         if inner_tol is not None:
             prm.inner_tol = float(inner_tol)
         if max_outer is not None:
@@ -82,6 +88,7 @@ class TolSolver:
                                          stream_handle(stream))
         if code not in (0, 10005) or (raise_on_fail and code != 0):
             _lib.check("bsp_solve_tol", code)
+        self._setup_done = True
         return SolveResult(p, self.x64, code, info.outer_iterations, info.inner_iterations,
                            info.levels, info.rel_residual)
 

@@ -27,6 +27,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <mutex>
+
 #include "bsp_common.cuh"
 #include "profile.cuh"
 #include "solver.cuh"
@@ -36,6 +38,8 @@ namespace bsp {
 int num_sms();
 
 constexpr float OMEGA = 6.0f / 7.0f;
+// BSP_TUNE_FINE_COLUMN: level-0 kernels on the column layout (1) or per row (0)
+bool g_fine_col_enabled = true;
 constexpr int COARSE_SWEEPS = 64;
 constexpr int RED_THREADS = 256;
 
@@ -204,11 +208,17 @@ __global__ void nsolid_kernel(uint8_t *__restrict__ m, int nx, int ny, int nz) {
 
 // ---- stencil helpers ----------------------------------------------------------------
 __device__ __forceinline__ float dg(uint32_t mb) { return 6.0f - (float)mnsolid(mb); }
+// OMEGA / (6 - n_solid) by the approximate division (same as the level-0
+// column kernels); 0 where the diagonal vanishes.
+__device__ __forceinline__ float wdinv(uint32_t mb) {
+  const float d = dg(mb);
+  return d > 0.0f ? __fdividef(OMEGA, d) : 0.0f;
+}
 
 // e = OMEGA r / D on a fluid cell.
 template <class T>
 __device__ __forceinline__ float pre_e(const T *r, int64_t c, uint32_t mb) {
-  return OMEGA * ld(r, c) / dg(mb);
+  return ld(r, c) * wdinv(mb);
 }
 
 // ---- V-cycle kernels ----------------------------------------------------------------
@@ -254,9 +264,72 @@ __global__ void __launch_bounds__(256) mg_down_kernel(Level<T> f, Level<T> co,
   }
 }
 
-// Coarsest level: one CTA, whole level in shared memory, Jacobi from zero.
+// Dense inverse of the coarsest operator, once per geometry: A (FP64, n x n,
+// diagonal 6 - n_solid, -1 to fluid neighbours, identity rows on non-fluid
+// cells) is inverted in place by Gauss-Jordan elimination without pivoting
+// (the fluid block is symmetric positive definite when every fluid component
+// touches a Dirichlet cell).  *flag = 1 on success; 0 if a pivot is not
+// positive (a closed Neumann island), and the coarse solve then falls back to
+// Jacobi sweeps.  One CTA; A lives in the workspace.
 template <class T>
-__global__ void __launch_bounds__(512) mg_coarse_kernel(Level<T> L, const SolverState *stt) {
+__global__ void __launch_bounds__(1024) coarse_invert_kernel(Level<T> L, double *A, float *minv,
+                                                             int *flag) {
+  const int n = L.nx * L.ny * L.nz;
+  const int plane = L.ny * L.nz;
+  __shared__ double fcol[COARSEST_CELLS];
+  for (int q = threadIdx.x; q < n * n; q += blockDim.x) A[q] = 0.0;
+  __syncthreads();
+  for (int c = threadIdx.x; c < n; c += blockDim.x) {
+    const uint32_t mc = mk(L.mask, c);
+    if (mcls(mc) != BSP_FLUID) {
+      A[(int64_t)c * n + c] = 1.0;
+      continue;
+    }
+    A[(int64_t)c * n + c] = 6.0 - (double)mnsolid(mc);
+    const int k = c % L.nz, j = (c / L.nz) % L.ny, i = c / plane;
+#define OFF(cond, off) \
+  if ((cond) && mcls(mk(L.mask, c + (off))) == BSP_FLUID) A[(int64_t)c * n + c + (off)] = -1.0
+    OFF(i > 0, -plane);
+    OFF(i + 1 < L.nx, plane);
+    OFF(j > 0, -L.nz);
+    OFF(j + 1 < L.ny, L.nz);
+    OFF(k > 0, -1);
+    OFF(k + 1 < L.nz, 1);
+#undef OFF
+  }
+  __syncthreads();
+  for (int kp = 0; kp < n; ++kp) {
+    const double piv = A[(int64_t)kp * n + kp];
+    if (!(piv > 1e-12)) {  // uniform: every thread read the same value
+      if (threadIdx.x == 0) *flag = 0;
+      return;
+    }
+    __syncthreads();
+    for (int jj = threadIdx.x; jj < n; jj += blockDim.x) {
+      const double v = jj == kp ? 1.0 : A[(int64_t)kp * n + jj];
+      A[(int64_t)kp * n + jj] = v / piv;
+    }
+    for (int ii = threadIdx.x; ii < n; ii += blockDim.x) fcol[ii] = A[(int64_t)ii * n + kp];
+    __syncthreads();
+    for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+      const int ii = q / n, jj = q - ii * n;
+      if (ii == kp) continue;
+      const double a = jj == kp ? 0.0 : A[q];
+      A[q] = a - fcol[ii] * A[(int64_t)kp * n + jj];
+    }
+    __syncthreads();
+  }
+  for (int q = threadIdx.x; q < n * n; q += blockDim.x) minv[q] = (float)A[q];
+  if (threadIdx.x == 0) *flag = 1;
+}
+
+// Coarsest level: one CTA.  With the dense inverse, e = M r (M symmetric, so
+// thread t reads column t with coalesced loads); otherwise COARSE_SWEEPS
+// Jacobi sweeps from zero with the level in shared memory.
+template <class T>
+__global__ void __launch_bounds__(512) mg_coarse_kernel(Level<T> L, const float *minv,
+                                                        const int *direct,
+                                                        const SolverState *stt) {
   if (stt->inner_done) return;
   extern __shared__ float sm[];
   const int n = L.nx * L.ny * L.nz;
@@ -266,6 +339,26 @@ __global__ void __launch_bounds__(512) mg_coarse_kernel(Level<T> L, const Solver
     rr[c] = ld(L.r, c);
   }
   __syncthreads();
+  if (*direct) {
+    // n <= COARSEST_CELLS <= blockDim: split the j sum of each output over
+    // blockDim / n threads, then combine in a fixed order
+    __shared__ float part[512];
+    const int parts = blockDim.x / n;
+    const int t = threadIdx.x % n, pi = threadIdx.x / n;
+    if (pi < parts) {
+      const int j0 = (n * pi) / parts, j1 = (n * (pi + 1)) / parts;
+      float acc = 0.0f;
+      for (int jj = j0; jj < j1; ++jj) acc = fmaf(minv[(int64_t)jj * n + t], rr[jj], acc);
+      part[pi * n + t] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x < n) {
+      float acc = 0.0f;
+      for (int q = 0; q < parts; ++q) acc += part[q * n + threadIdx.x];
+      stv(L.e, threadIdx.x, mcls(mk(L.mask, threadIdx.x)) == BSP_FLUID ? acc : 0.0f);
+    }
+    return;
+  }
   const int plane = L.ny * L.nz;
   for (int s = 0; s < COARSE_SWEEPS; ++s) {
     for (int c = threadIdx.x; c < n; c += blockDim.x) {
@@ -333,7 +426,7 @@ __global__ void __launch_bounds__(256) mg_up_kernel(Level<T> f, Level<T> co, T *
                       NB(k + 1 < f.nz, 0, 0, 1, 1);
 #undef NB
       const float rc = ld(f.r, c);
-      const float e = ec + OMEGA * (rc - (6.0f * ec - s)) / dg(mc);
+      const float e = fmaf(rc - (6.0f * ec - s), wdinv(mc), ec);
       stv(out, c, e);
       if (FINE) rz += (double)rc * (double)ld(out, c);
     }
@@ -508,6 +601,9 @@ __global__ void __launch_bounds__(RED_THREADS) outer_check_kernel(SolverState *s
   st->inner_it = 0;
   st->inner_done = 0;
   st->rhat_norm2 = rr * st->scale * st->scale;
+  // Do not over-solve the last pass: an inner reduction by
+  // 0.5 tol ||b|| / ||r|| already meets the outer target.
+  st->eta_eff = fmax(st->eta, 0.5 * st->tol * sqrt(st->b_norm2 / rr));
   st->outer_it += 1;
 }
 
@@ -537,7 +633,7 @@ __global__ void __launch_bounds__(RED_THREADS) inner_check_kernel(SolverState *s
   st->inner_it += 1;
   st->total_inner += 1;
   st->rr_inner = rr;
-  if (!(rr == rr) || rr <= st->eta * st->eta * st->rhat_norm2 ||
+  if (!(rr == rr) || rr <= st->eta_eff * st->eta_eff * st->rhat_norm2 ||
       st->inner_it >= st->max_inner || st->alpha == 0.0)
     st->inner_done = 1;
 }
@@ -569,7 +665,6 @@ int build_hierarchy(int nx, int ny, int nz, int *dims /* 3*MAX_LEVELS */) {
     if (L == MAX_LEVELS) break;
     // at least two levels: the level-0 up-pass produces z and its r.z partial
     if (L >= 2 && (int64_t)x * y * z <= COARSEST_CELLS) break;
-    if (L >= 2 && (x <= 2 || y <= 2 || z <= 2)) break;
     x = (x + 1) / 2;
     y = (y + 1) / 2;
     z = (z + 1) / 2;
@@ -583,9 +678,10 @@ size_t storage_bytes(int storage) { return storage == BSP_STORE_FP32 ? 4 : 2; }
 //   SolverState | partials (3 * PARTIAL_STRIDE doubles) | x (n doubles) | e (n floats)
 //   | z, ps0, ps1, Ap, r (n T each) | per level l >= 1: mask, r, e (T)
 //   | per level l >= 1 ... ; level-0 effective-class scratch reuses the level-1 slot order.
+//   | coarsest-level dense inverse (float), its FP64 build scratch, direct flag
 struct Layout {
   size_t state, partials, x, e, z, ps0, ps1, Ap, r, lvl_mask[MAX_LEVELS], lvl_r[MAX_LEVELS],
-      lvl_e[MAX_LEVELS], eff0, total;
+      lvl_e[MAX_LEVELS], eff0, cinv, cA, cflag, total;
   int L, dims[3 * MAX_LEVELS];
 };
 
@@ -615,6 +711,14 @@ Layout make_layout(int nx, int ny, int nz, int storage) {
     lo.lvl_r[l] = take(ts * nl);
     lo.lvl_e[l] = take(ts * nl);
   }
+  {
+    const int l = lo.L - 1;
+    size_t nc = (size_t)lo.dims[3 * l] * lo.dims[3 * l + 1] * lo.dims[3 * l + 2];
+    if (nc > (size_t)COARSEST_CELLS) nc = 0;  // no direct solve: Jacobi sweeps
+    lo.cinv = take(sizeof(float) * nc * nc + 4);
+    lo.cA = take(sizeof(double) * nc * nc + 8);
+    lo.cflag = take(sizeof(int));
+  }
   lo.total = off;
   return lo;
 }
@@ -629,6 +733,7 @@ struct Ctx {
   int nx, ny, nz;
   int64_t n;
   const uint8_t *mask0;
+  bool col;  // level-0 kernels on the column layout (nz % 4 == 0, aligned mask)
 };
 
 template <class T>
@@ -643,6 +748,8 @@ Ctx<T> make_ctx(void *ws, const uint8_t *mask, int nx, int ny, int nz, int stora
   cx.nz = nz;
   cx.n = (int64_t)nx * ny * nz;
   cx.mask0 = mask;
+  cx.col = (nz % 4 == 0) && (((uintptr_t)mask & 15u) == 0) && g_fine_col_enabled &&
+           fine_grid_blocks(nx, ny, nz) <= PARTIAL_STRIDE;
   for (int l = 0; l < cx.lo.L; ++l) {
     Level<T> &L = cx.lv[l];
     L.nx = cx.lo.dims[3 * l];
@@ -694,6 +801,17 @@ cudaError_t setup_levels(Ctx<T> &cx, cudaStream_t s) {
     }
     prev = c.mask;
   }
+  {
+    Level<T> &c = cx.lv[cx.lo.L - 1];
+    int *flag = (int *)(cx.base + cx.lo.cflag);
+    const int64_t nc = (int64_t)c.nx * c.ny * c.nz;
+    cudaMemsetAsync(flag, 0, sizeof(int), s);
+    if (nc <= COARSEST_CELLS) {
+      ProfScope ps(PROF_CONTROL, s);
+      coarse_invert_kernel<T><<<1, 1024, 0, s>>>(c, (double *)(cx.base + cx.lo.cA),
+                                                 (float *)(cx.base + cx.lo.cinv), flag);
+    }
+  }
   return cudaGetLastError();
 }
 
@@ -701,29 +819,49 @@ template <class T>
 cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
   const int L = cx.lo.L;
   SolverState *st = cx.st;
+  // levels on the column layout when their rows allow float4 access
+  const bool col = cx.col;
+  auto level_col = [&](int l) {
+    const Level<T> &v = cx.lv[l];
+    if (l == 0) return col;
+    // coarse levels: only while a row keeps at least 16 lanes busy
+    return g_fine_col_enabled && v.nz % 4 == 0 && v.nz >= 64 &&
+           (int64_t)v.nx * v.ny * v.nz >= 131072 &&
+           fine_grid_blocks(v.nx, v.ny, v.nz) <= PARTIAL_STRIDE;
+  };
   // V-cycle on r -> z
   for (int l = 0; l + 1 < L; ++l) {
     Level<T> &f = cx.lv[l], &c = cx.lv[l + 1];
     ProfScope ps(l == 0 ? PROF_MG_DOWN0 : PROF_MG_COARSE, s);
-    mg_down_kernel<T><<<row_blocks((int64_t)c.nx * c.ny), 256, 0, s>>>(f, c, st);
+    if (level_col(l))
+      launch_fine_down<T>(f, c, st, s);
+    else
+      mg_down_kernel<T><<<row_blocks((int64_t)c.nx * c.ny), 256, 0, s>>>(f, c, st);
   }
   {
     Level<T> &c = cx.lv[L - 1];
     const int n = c.nx * c.ny * c.nz;
     ProfScope ps(PROF_MG_COARSE, s);
-    mg_coarse_kernel<T><<<1, 512, 3 * n * sizeof(float), s>>>(c, st);
+    mg_coarse_kernel<T><<<1, 512, 3 * n * sizeof(float), s>>>(
+        c, (const float *)(cx.base + cx.lo.cinv), (const int *)(cx.base + cx.lo.cflag), st);
   }
   for (int l = L - 2; l >= 1; --l) {
     Level<T> &f = cx.lv[l], &c = cx.lv[l + 1];
     ProfScope ps(PROF_MG_COARSE, s);
-    mg_up_kernel<T, false><<<row_blocks((int64_t)f.nx * f.ny), 256, 0, s>>>(f, c, f.e,
-                                                                            cx.partials, st);
+    if (level_col(l))  // its r.e partial is written but unused
+      launch_fine_up<T>(f, c, f.e, cx.partials, st, s);
+    else
+      mg_up_kernel<T, false><<<row_blocks((int64_t)f.nx * f.ny), 256, 0, s>>>(f, c, f.e,
+                                                                              cx.partials, st);
   }
   T *z = (T *)(cx.base + cx.lo.z);
-  const int nb0 = row_blocks((int64_t)cx.nx * cx.ny);
+  const int nb0 = col ? fine_grid_blocks(cx.nx, cx.ny, cx.nz) : row_blocks((int64_t)cx.nx * cx.ny);
   {
     ProfScope ps(PROF_MG_UP0, s);
-    mg_up_kernel<T, true><<<nb0, 256, 0, s>>>(cx.lv[0], cx.lv[1], z, cx.partials, st);
+    if (col)
+      launch_fine_up<T>(cx.lv[0], cx.lv[1], z, cx.partials, st, s);
+    else
+      mg_up_kernel<T, true><<<nb0, 256, 0, s>>>(cx.lv[0], cx.lv[1], z, cx.partials, st);
   }
   {
     ProfScope ps(PROF_CONTROL, s);
@@ -734,8 +872,11 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
   T *Ap = (T *)(cx.base + cx.lo.Ap);
   {
     ProfScope ps(PROF_CG_PSAP, s);
-    cg_ps_ap_kernel<T><<<nb0, 256, 0, s>>>(cx.nx, cx.ny, cx.nz, cx.mask0, z, prev, cur, Ap,
-                                           cx.partials, st);
+    if (col)
+      launch_fine_psap<T>(cx.nx, cx.ny, cx.nz, cx.mask0, z, prev, cur, Ap, cx.partials, st, s);
+    else
+      cg_ps_ap_kernel<T><<<nb0, 256, 0, s>>>(cx.nx, cx.ny, cx.nz, cx.mask0, z, prev, cur, Ap,
+                                             cx.partials, st);
   }
   {
     ProfScope ps(PROF_CONTROL, s);
@@ -770,6 +911,34 @@ __global__ void __launch_bounds__(RED_THREADS) bnorm_kernel(SolverState *st,
   if (threadIdx.x == 0) st->b_norm2 = bb;
 }
 
+// Host-side record of workspaces whose multigrid setup (coarse masks, coarsest
+// inverse) is current, for callers that pass reuse_setup = 1 (their mask does
+// not change between solves).
+struct SetupKey {
+  const void *ws, *mask;
+  int nx, ny, nz, storage;
+};
+static std::mutex g_setup_mu;
+static SetupKey g_setups[16];
+static int g_setup_next = 0;
+
+static bool setup_cached(const void *ws, const void *mask, int nx, int ny, int nz, int storage) {
+  std::lock_guard<std::mutex> lk(g_setup_mu);
+  for (const SetupKey &k : g_setups)
+    if (k.ws == ws && k.mask == mask && k.nx == nx && k.ny == ny && k.nz == nz &&
+        k.storage == storage)
+      return true;
+  return false;
+}
+static void remember_setup(const void *ws, const void *mask, int nx, int ny, int nz,
+                           int storage) {
+  std::lock_guard<std::mutex> lk(g_setup_mu);
+  for (SetupKey &k : g_setups)
+    if (k.ws == ws) k.ws = nullptr;  // a workspace holds one setup
+  g_setups[g_setup_next] = SetupKey{ws, mask, nx, ny, nz, storage};
+  g_setup_next = (g_setup_next + 1) % 16;
+}
+
 template <class T>
 int solve_impl(void *ws, const uint8_t *mask, const float *div, float *p_out, int nx, int ny,
                int nz, float dx, float dt, float rho, const BspSolveParams *prm,
@@ -787,8 +956,11 @@ int solve_impl(void *ws, const uint8_t *mask, const float *div, float *p_out, in
   h.scale = 1.0;
   cudaError_t e = cudaMemcpyAsync(cx.st, &h, sizeof(h), cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return (int)e;
-  e = setup_levels<T>(cx, s);
-  if (e != cudaSuccess) return (int)e;
+  if (!(prm->reuse_setup && setup_cached(ws, mask, nx, ny, nz, prm->storage))) {
+    e = setup_levels<T>(cx, s);
+    if (e != cudaSuccess) return (int)e;
+    remember_setup(ws, mask, nx, ny, nz, prm->storage);
+  }
   double *x = (double *)(cx.base + cx.lo.x);
   float *eb = (float *)(cx.base + cx.lo.e);
   const int nbr = row_blocks((int64_t)nx * ny);
@@ -879,6 +1051,7 @@ extern "C" void bsp_solve_params_default(BspSolveParams *p) {
   p->storage = BSP_STORE_FP32;
   p->warm_start = 0;
   p->check_every = 8;
+  p->reuse_setup = 0;
 }
 
 extern "C" int bsp_solve_tol(float *p, const float *div_u, const uint8_t *mask, int nx, int ny,

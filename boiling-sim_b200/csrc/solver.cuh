@@ -5,9 +5,9 @@
 namespace bsp {
 
 constexpr int MAX_LEVELS = 12;
-constexpr int COARSEST_CELLS = 512;   // the hierarchy stops at or below this size
+constexpr int COARSEST_CELLS = 256;   // the hierarchy stops at or below this size
 constexpr int COARSEST_MAX = 4096;    // one CTA holds the coarsest level in shared memory
-constexpr int PARTIAL_STRIDE = 2048;  // max blocks of any reducing kernel
+constexpr int PARTIAL_STRIDE = 16384;  // max blocks of any reducing kernel
 
 template <class T>
 struct Level {
@@ -20,12 +20,24 @@ struct Level {
 // Device-resident control block of one solve.  Written only by the one-block
 // control kernels; read by every other kernel at entry.
 struct SolverState {
-  double tol, eta;
+  double tol, eta, eta_eff;
   double b_norm2, r64_norm2, rel, scale, rhat_norm2;
   double rz, beta, alpha, rr_inner;
   int max_outer, max_inner;
   int outer_it, inner_it, total_inner;
   int done, inner_done, status, finalize, pad;
 };
+
+// Level-0 kernels on the column layout (mgfine.cu); nz % 4 == 0 required.
+int fine_grid_blocks(int nx, int ny, int nz);
+template <class T>
+void launch_fine_psap(int nx, int ny, int nz, const uint8_t *mask, const T *z, const T *prev,
+                      T *cur, T *Ap, double *partials, const SolverState *st, cudaStream_t s);
+template <class T>
+void launch_fine_up(const Level<T> &f, const Level<T> &c, T *z, double *partials,
+                    const SolverState *st, cudaStream_t s);
+template <class T>
+void launch_fine_down(const Level<T> &f, const Level<T> &c, const SolverState *st,
+                      cudaStream_t s);
 
 }  // namespace bsp

@@ -455,11 +455,19 @@ extern "C" int bsp_selftest_div6(unsigned long long *mismatches_dev, cudaStream_
   return (int)cudaGetLastError();
 }
 
+namespace bsp {
+extern bool g_fine_col_enabled;
+}
+
 extern "C" int bsp_set_tuning(int key, int value) {
   switch (key) {
     case BSP_TUNE_SWEEP_BI:
       if (value < 0 || value > 4096) return BSP_ERR_ARG;
       bsp::g_sweep_bi = value;
+      return BSP_OK;
+    case BSP_TUNE_FINE_COLUMN:
+      if (value < 0 || value > 1) return BSP_ERR_ARG;
+      bsp::g_fine_col_enabled = value != 0;
       return BSP_OK;
     default:
       return BSP_ERR_ARG;

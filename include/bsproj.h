@@ -51,7 +51,8 @@ extern "C" {
 #define BSP_MASK_NSOLID 0x07
 
 /* autotuner keys of bsp_set_tuning */
-#define BSP_TUNE_SWEEP_BI 1 /* i-planes per CTA of the sweep kernels (0 = heuristic) */
+#define BSP_TUNE_SWEEP_BI 1     /* i-planes per CTA of the sweep kernels (0 = heuristic) */
+#define BSP_TUNE_FINE_COLUMN 2  /* solver level-0 kernels: 1 column layout, 0 row layout */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */
@@ -225,6 +226,8 @@ typedef struct BspSolveParams {
   int storage;      /* BSP_STORE_* for the inner vectors and multigrid levels */
   int warm_start;   /* 1: p holds the initial guess on entry; 0: cold start */
   int check_every;  /* inner iterations enqueued between host reads of the done flag */
+  int reuse_setup;  /* 1: the mask is unchanged since the last solve on this workspace,
+                       reuse its multigrid setup (coarse masks, coarsest inverse) */
 } BspSolveParams;
 
 typedef struct BspSolveInfo {
