@@ -134,6 +134,81 @@ def cpu_reference(mat, ux, uy, uz, ref_iters):
             "s_per_projection": t_proj}
 
 
+def run_batched(args, dev, rank, world, dist):
+    """64 pot instances of uneven sizes (seeded draw, 48^3 .. 128x128x96), each
+    with its own seeded velocity field, solved FP32-stored to FP64 rel-residual
+    1e-6 by one graph launch per batch; compared with 64 sequential host-driven
+    solves of the same instances.  value = instances/s of the batched launch."""
+    import torch
+
+    from boilingsim_b200 import fluid as F
+    from boilingsim_b200 import scenes as S
+    from boilingsim_b200.solver import BatchSolver, TolSolver
+
+    specs = S.random_batch_specs(64, seed=SEED)
+    masks, divs, ps = [], [], []
+    cells = 0
+    for spec, seed in specs:
+        mat = S.pot_mat(spec)
+        ux, uy, uz = S.velocity_field(mat, seed=seed)
+        m = F.cell_mask(torch.as_tensor(mat).to(dev))
+        d = torch.zeros(mat.shape, dtype=torch.float32, device=dev)
+        F.compute_divergence(d, *[torch.as_tensor(a).to(dev) for a in (ux, uy, uz)], m, 0.002)
+        masks.append(m)
+        divs.append(d)
+        ps.append(torch.zeros_like(d))
+        cells += mat.size
+    batch = BatchSolver(masks, args.storage)
+    infos = batch.solve(divs, ps, 0.002, DT, RHO, tol=TOL)  # builds the graph
+    for _ in range(max(0, args.warmup - 1)):
+        batch.solve(divs, ps, 0.002, DT, RHO, tol=TOL, wait=False)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        batch.solve(divs, ps, 0.002, DT, RHO, tol=TOL, wait=False)
+    ev1.record()
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    infos = batch.solve(divs, ps, 0.002, DT, RHO, tol=TOL)
+    worst = max(i.rel_residual for i in infos)
+    # sequential host-driven solves of the same 64 instances
+    singles = [TolSolver(m, args.storage) for m in masks]
+    for s_, d, p in zip(singles, divs, ps):
+        s_.solve(d, 0.002, DT, RHO, tol=TOL, p=p)
+    torch.cuda.synchronize()
+    ev0.record()
+    for _ in range(max(1, args.steps // 2)):
+        for s_, d, p in zip(singles, divs, ps):
+            s_.solve(d, 0.002, DT, RHO, tol=TOL, p=p)
+    ev1.record()
+    torch.cuda.synchronize()
+    seq_ms = ev0.elapsed_time(ev1) / max(1, args.steps // 2)
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    if rank == 0:
+        print(json.dumps({
+            "metric": "instances/s, 64 uneven pot scenes to FP64 rel-residual 1e-6",
+            "value": round(world * 64e3 / ms, 2), "unit": "instances/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"64 pot scenes, sizes 48^3..128x128x96 (seed {SEED}), "
+                                   f"{cells} cells in total, dx 2 mm", "storage": args.storage,
+                       "launch": "one CUDA graph per batch (conditional WHILE loops per "
+                                 "instance)"},
+            "sequential_host_driven": {"value": round(64e3 / seq_ms, 2), "unit": "instances/s",
+                                       "ms_per_64": round(seq_ms, 3)},
+            "worst_rel_residual_fp64": worst,
+            "inner_iterations": [i.inner_iterations for i in infos][:8],
+        }), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -144,6 +219,14 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-iters", type=int, default=0,
                     help="reference PCG iteration count to use instead of measuring it")
+    ap.add_argument("--skip-extras", action="store_true",
+                    help="timed projections only (no sweep, e2e, reference iterations or CPU "
+                         "baseline): the short form used under ncu")
+    ap.add_argument("--only-sweep", action="store_true",
+                    help="run only the plain FP32 Jacobi sweep measurement (for ncu)")
+    ap.add_argument("--config", default="projection", choices=["projection", "batched"],
+                    help="projection: the headline 384x384x256 projection; batched: 64 uneven "
+                         "pot scenes (48^3 .. 128x128x96) solved by one graph launch")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -183,6 +266,9 @@ def main():
     from boilingsim_b200.solver import TolSolver
 
     dev = torch.device("cuda", local)
+    if args.config == "batched":
+        run_batched(args, dev, rank, world, dist)
+        return
     mat, ux, uy, uz = _workload()
     nx, ny, nz = mat.shape
     n = mat.size
@@ -206,6 +292,37 @@ def main():
         F.compute_divergence(div, *u, mask, DX, max_div)
         last["res"] = res
 
+    import ctypes
+
+    ncls = 10
+    prof_ms = (ctypes.c_double * ncls)()
+    prof_n = (ctypes.c_longlong * ncls)()
+    peak, peak_kind = _peaks()
+
+    def plain_sweep():
+        """200 sweeps of the reference-contract FP32 Jacobi kernel, event-timed."""
+        rhs = torch.empty_like(p)
+        q = torch.empty_like(p)
+        F.compute_divergence(div, *u0, mask, DX)
+        _lib.call("bsp_profile_enable", 1)
+        _lib.lib().bsp_profile_read(None, None, 0)
+        _lib.call("bsp_jacobi_solve", _lib.ptr(p), _lib.ptr(q), _lib.ptr(div), _lib.ptr(rhs),
+                  _lib.ptr(mask), nx, ny, nz, DX, DT, RHO, 200, 0, _lib.stream_handle())
+        torch.cuda.synchronize()
+        _lib.call("bsp_profile_enable", 0)
+        _lib.lib().bsp_profile_read(prof_ms, prof_n, ncls)
+        sweep_ms = prof_ms[0] / max(1, prof_n[0])
+        gbs = 13.0 * n / (sweep_ms * 1e-3) / 1e9
+        return {"ms": round(sweep_ms, 5), "GB/s": round(gbs, 1), "frac": round(gbs / peak, 4),
+                "bytes_per_cell": 13}
+
+    if args.only_sweep:
+        if rank == 0:
+            print(json.dumps({"plain_fp32_jacobi_sweep": plain_sweep()}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
+
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -223,11 +340,6 @@ def main():
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / args.steps
     _lib.call("bsp_profile_enable", 0)
-    import ctypes
-
-    ncls = 10
-    prof_ms = (ctypes.c_double * ncls)()
-    prof_n = (ctypes.c_longlong * ncls)()
     _lib.lib().bsp_profile_read(prof_ms, prof_n, ncls)
     clk = clocks.stop()
     if dist:
@@ -236,94 +348,96 @@ def main():
         ms = float(t.item())
         dist.barrier()
     res = last["res"]
-    inner = res.inner_iterations
 
     # ---- roofline of the dominant kernel class -------------------------------------
+    # Algorithmic bytes per grid cell per launch.  Stencil kernels touch every
+    # cell; the CG update and the FP64 residual read their vectors on fluid
+    # cells only (fraction ff of the grid).
+    ff = float((mat == 0).mean())
     ts = 2 if args.storage != "fp32" else 4
-    # algorithmic bytes per fine cell per launch, by class
-    per_cell = {0: 13.0, 1: ts + 1 + ts / 8, 2: ts + 1 + ts / 8 + ts, 3: 3 * ts + 1 + 2 * ts,
-                4: 4 + ts + ts + ts + 1 + 4 + ts, 5: 8 + 4 + 1 + (ts + 4) / 2, 6: 8 + 4 + 8}
+    per_cell = {0: 13.0,
+                1: ts + 1 + ts / 8,                      # r, mask -> r_coarse
+                2: ts + 1 + ts / 8 + ts,                 # r, mask, e_coarse -> z
+                3: 2 * ts + 1 + 2 * ts,                  # z, ps_prev, mask -> ps, Ap
+                4: 1 + ff * (4 + 3 * ts + 4 + ts),       # mask; e, ps, Ap, r -> e, r
+                5: 1 + ff * 12 + (ts + 4) / 2,           # mask, x, div; rhat, e (write pass)
+                6: 20.0}                                 # x, e -> x
     names = {0: "jacobi_sweep", 1: "mg_restrict_fine", 2: "mg_prolong_smooth_fine",
              3: "cg_direction_Ap", 4: "cg_update", 5: "residual_fp64", 6: "x_update_fp64",
              7: "mg_coarse_levels", 8: "control_and_setup", 9: "divergence_gradient"}
     dom = max((c for c in per_cell if prof_n[c] > 0), key=lambda c: prof_ms[c])
     avg_ms = prof_ms[dom] / prof_n[dom]
     bytes_launch = per_cell[dom] * n
-    peak, peak_kind = _peaks()
     achieved = bytes_launch / (avg_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": names[dom], "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": None, "peak_source": peak_kind,
-                "algorithmic_bytes_per_launch": bytes_launch,
+                "algorithmic_bytes_per_launch": round(bytes_launch),
                 "avg_launch_ms": round(avg_ms, 5),
                 "share_of_step": round(prof_ms[dom] / (ms * args.steps), 3)}
     kernel_ms = {names[c]: round(prof_ms[c] / args.steps, 4) for c in range(ncls) if prof_n[c]}
+    kernel_gbs = {names[c]: round(per_cell[c] * n / (prof_ms[c] / prof_n[c] * 1e-3) / 1e9, 1)
+                  for c in per_cell if prof_n[c]}
     launches = int(sum(prof_n))  # every kernel launch of the timed steps is instrumented
 
-    # ---- plain FP32 Jacobi sweep (the stencil's own roofline) -----------------------
-    rhs = torch.empty_like(p)
-    q = torch.empty_like(p)
-    _lib.call("bsp_profile_enable", 1)
-    _lib.lib().bsp_profile_read(None, None, 0)
-    _lib.call("bsp_jacobi_solve", _lib.ptr(p), _lib.ptr(q), _lib.ptr(div), _lib.ptr(rhs),
-              _lib.ptr(mask), nx, ny, nz, DX, DT, RHO, 200, 0, _lib.stream_handle())
-    torch.cuda.synchronize()
-    _lib.call("bsp_profile_enable", 0)
-    _lib.lib().bsp_profile_read(prof_ms, prof_n, ncls)
-    sweep_ms = prof_ms[0] / max(1, prof_n[0])
-    sweep = {"ms": round(sweep_ms, 5), "GB/s": round(13.0 * n / (sweep_ms * 1e-3) / 1e9, 1),
-             "frac": round(13.0 * n / (sweep_ms * 1e-3) / 1e9 / peak, 4)}
-
-    # ---- end to end through the public API with host buffers --------------------------
-    host_u = [torch.as_tensor(a).pin_memory() for a in (ux, uy, uz)]
-    host_out = [torch.empty(a.shape, dtype=torch.float32).pin_memory() for a in (ux, uy, uz)]
-    host_p = torch.empty(mat.shape, dtype=torch.float32).pin_memory()
-    grid = F.Grid(nx, ny, nz, DX, p, mat_t, *u, mask=mask)
-    ws = F.FluidWorkspace(div, q, max_div)
-    cfg = F.ScenarioConfig(F.SolverConfig(pressure_tol=TOL))
-    os.environ["BOILINGSIM_PRESSURE_SOLVER"] = {"fp32": "b200-mg", "fp16": "b200-mixed",
-                                                "bf16": "b200-bf16"}[args.storage]
-    F._TOL_SOLVERS.clear()
-    F._TOL_SOLVERS[(id(grid), grid.shape, args.storage)] = solver
-
-    def e2e_step():
-        for d, h in zip(u, host_u):
-            d.copy_(h, non_blocking=True)
-        md = F.pressure_projection(grid, ws, cfg, DT, RHO)
-        host_p.copy_(p, non_blocking=True)
-        for h, d in zip(host_out, u):
-            h.copy_(d, non_blocking=True)
-        torch.cuda.synchronize()
-        return md
-
-    e2e_step()
-    e2e_steps = max(2, min(args.steps, 5))
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        e2e_step()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    h2d = sum(a.numel() * 4 for a in host_u)
-    d2h = sum(a.numel() * 4 for a in host_out) + host_p.numel() * 4 + 4
-
-    # ---- reference-algorithm iteration count (Jacobi-PCG, its own stopping rule) ------
+    sweep = e2e = None
     ref_iters = args.ref_iters or REF_PCG_ITERS_FALLBACK
-    if rank == 0 and not args.ref_iters:
-        try:
-            from boilingsim_b200.sim_core import SimCore, pcg_workspace
-
-            w = pcg_workspace(mat.shape, dev)
-            ref_iters = SimCore(local).pressure_solve_pcg(
-                _lib.ptr(p), _lib.ptr(div), _lib.ptr(mat_t), nx, ny, nz, DX, DT, RHO, 1e-6, 20000,
-                *[_lib.ptr(w[k]) for k in ("b", "r", "z", "p_search", "Ap", "dot_ws", "alpha",
-                                             "beta", "rzold", "rznew", "bsq", "rsq", "pAp")])
-        except Exception:
-            ref_iters = REF_PCG_ITERS_FALLBACK
-
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_reference(mat, ux, uy, uz, ref_iters)
-        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if not args.skip_extras:
+        sweep = plain_sweep()
+
+        # ---- end to end through the public API with host buffers ----------------------
+        host_u = [torch.as_tensor(a).pin_memory() for a in (ux, uy, uz)]
+        host_out = [torch.empty(a.shape, dtype=torch.float32).pin_memory() for a in (ux, uy, uz)]
+        host_p = torch.empty(mat.shape, dtype=torch.float32).pin_memory()
+        grid = F.Grid(nx, ny, nz, DX, p, mat_t, *u, mask=mask)
+        ws = F.FluidWorkspace(div, torch.empty_like(p), max_div)
+        cfg = F.ScenarioConfig(F.SolverConfig(pressure_tol=TOL))
+        os.environ["BOILINGSIM_PRESSURE_SOLVER"] = {"fp32": "b200-mg", "fp16": "b200-mixed",
+                                                    "bf16": "b200-bf16"}[args.storage]
+        F._TOL_SOLVERS.clear()
+        F._TOL_SOLVERS[(id(grid), grid.shape, args.storage)] = solver
+
+        def e2e_step():
+            for d, h in zip(u, host_u):
+                d.copy_(h, non_blocking=True)
+            md = F.pressure_projection(grid, ws, cfg, DT, RHO)
+            host_p.copy_(p, non_blocking=True)
+            for h, d in zip(host_out, u):
+                h.copy_(d, non_blocking=True)
+            torch.cuda.synchronize()
+            return md
+
+        e2e_step()
+        e2e_steps = max(2, min(args.steps, 5))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            e2e_step()
+        e2e_s = (time.perf_counter() - t0) / e2e_steps
+        h2d = sum(a.numel() * 4 for a in host_u)
+        d2h = sum(a.numel() * 4 for a in host_out) + host_p.numel() * 4 + 4
+        e2e = {"value": round(1.0 / e2e_s, 3), "unit": "projections/s",
+               "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h}
+
+        # ---- reference-algorithm iteration count (Jacobi-PCG, its stopping rule) --------
+        if rank == 0 and not args.ref_iters:
+            try:
+                from boilingsim_b200.sim_core import SimCore, pcg_workspace
+
+                F.compute_divergence(div, *u0, mask, DX)
+                w = pcg_workspace(mat.shape, dev)
+                ref_iters = SimCore(local).pressure_solve_pcg(
+                    _lib.ptr(p), _lib.ptr(div), _lib.ptr(mat_t), nx, ny, nz, DX, DT, RHO, 1e-6,
+                    20000, *[_lib.ptr(w[k]) for k in ("b", "r", "z", "p_search", "Ap", "dot_ws",
+                                                       "alpha", "beta", "rzold", "rznew", "bsq",
+                                                       "rsq", "pAp")])
+            except Exception:
+                ref_iters = REF_PCG_ITERS_FALLBACK
+
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_reference(mat, ux, uy, uz, ref_iters)
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
     if rank == 0:
         value = world * 1e3 / ms
@@ -337,16 +451,16 @@ def main():
                                  "(Jacobi smoothing), FP64 reductions",
                        "inputs": "600 MB resident (> 126 MB L2); velocities restored each step",
                        "parallelism": f"replicas x{world}"},
-            "solve": {"inner_iterations": inner, "outer_iterations": res.outer_iterations,
-                      "levels": res.levels, "rel_residual_fp64": res.rel_residual,
-                      "status": res.status},
+            "solve": {"inner_iterations": res.inner_iterations,
+                      "outer_iterations": res.outer_iterations, "levels": res.levels,
+                      "rel_residual_fp64": res.rel_residual, "status": res.status},
             "kernel_ms_per_step": kernel_ms,
+            "kernel_algorithmic_GBs": kernel_gbs,
             "roofline": roofline,
             "plain_fp32_jacobi_sweep": sweep,
             "reference_pcg_iterations_to_tol": ref_iters,
             "cpu_baseline": cpu,
-            "e2e": {"value": round(1.0 / e2e_s, 3), "unit": "projections/s",
-                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
         }

@@ -41,6 +41,7 @@ SIGNATURES = {
     "bsp_jacobi_sweep": (_I, [_P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _P]),
     "bsp_jacobi_solve": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I, _I, _P]),
     "bsp_set_tuning": (_I, [_I, _I]),
+    "bsp_solve_batch": (_I, [_I, _P, _P, _P, _P]),
     "bsp_dot_noalloc": (_I, [_P, _P, _L, _P, _P]),
     "bsp_profile_enable": (_I, [_I]),
     "bsp_profile_read": (_I, [_P, _P, _I]),
@@ -64,7 +65,17 @@ class BspSolveParams(ctypes.Structure):
     _fields_ = [("tol", ctypes.c_double), ("inner_tol", ctypes.c_double),
                 ("max_outer", ctypes.c_int), ("max_inner", ctypes.c_int),
                 ("storage", ctypes.c_int), ("warm_start", ctypes.c_int),
-                ("check_every", ctypes.c_int), ("reuse_setup", ctypes.c_int)]
+                ("check_every", ctypes.c_int), ("reuse_setup", ctypes.c_int),
+                ("use_graph", ctypes.c_int)]
+
+
+class BspBatchItem(ctypes.Structure):
+    """include/bsproj.h: BspBatchItem."""
+
+    _fields_ = [("p", ctypes.c_void_p), ("div", ctypes.c_void_p), ("mask", ctypes.c_void_p),
+                ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+                ("dx", ctypes.c_float), ("dt", ctypes.c_float), ("rho", ctypes.c_float),
+                ("workspace", ctypes.c_void_p), ("workspace_bytes", ctypes.c_size_t)]
 
 
 class BspSolveInfo(ctypes.Structure):

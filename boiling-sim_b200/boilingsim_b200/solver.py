@@ -65,7 +65,11 @@ class TolSolver:
     def solve(self, div: torch.Tensor, dx: float, dt: float, rho: float, tol: float = 1e-6,
               p: torch.Tensor | None = None, warm_start: bool = False, inner_tol: float | None = None,
               max_outer: int | None = None, max_inner: int | None = None,
-              check_every: int | None = None, stream=None, raise_on_fail: bool = True) -> SolveResult:
+              check_every: int | None = None, stream=None, raise_on_fail: bool = True,
+              graph: bool = False) -> SolveResult:
+        """Solve A p = b for the divergence ``div``.  ``graph=True`` runs the
+        whole solve as one device-driven CUDA graph (built on the first call
+        with this set of buffers, replayed afterwards)."""
         nx, ny, nz = self.shape
         if p is None:
             p = torch.zeros(self.shape, dtype=torch.float32, device=self.mask.device)
@@ -73,6 +77,7 @@ class TolSolver:
         prm.tol = float(tol)
         prm.warm_start = 1 if warm_start else 0
         prm.reuse_setup = 1 if self._setup_done else 0
+        prm.use_graph = 1 if graph else 0
         if inner_tol is not None:
             prm.inner_tol = float(inner_tol)
         if max_outer is not None:
@@ -91,6 +96,48 @@ class TolSolver:
         self._setup_done = True
         return SolveResult(p, self.x64, code, info.outer_iterations, info.inner_iterations,
                            info.levels, info.rel_residual)
+
+
+class BatchSolver:
+    """Many independent pot scenes (uneven sizes) solved by one graph launch
+    (``bsp_solve_batch``).  Each instance owns its workspace; the masks are
+    fixed for the solver's lifetime."""
+
+    def __init__(self, masks, storage: str = "fp32"):
+        self.masks = [m.contiguous() for m in masks]
+        self.storage = STORAGE[storage]
+        lib = _lib.lib()
+        self.ws = []
+        for m in self.masks:
+            nx, ny, nz = m.shape
+            nbytes = int(lib.bsp_solver_workspace_bytes(nx, ny, nz, self.storage))
+            self.ws.append(torch.empty(nbytes, dtype=torch.uint8, device=m.device))
+        self.params = BspSolveParams()
+        lib.bsp_solve_params_default(ctypes.byref(self.params))
+        self.params.storage = self.storage
+        self.params.use_graph = 1
+        self._setup_done = False
+
+    def solve(self, divs, ps, dx, dt, rho, tol: float = 1e-6, wait: bool = True, stream=None):
+        """Solve every instance; ``ps`` (float32 tensors) receive the pressures.
+        With ``wait`` the call returns one BspSolveInfo per instance."""
+        n = len(self.masks)
+        items = (_lib.BspBatchItem * n)()
+        for q, (m, d, p, w) in enumerate(zip(self.masks, divs, ps, self.ws)):
+            nx, ny, nz = m.shape
+            items[q] = _lib.BspBatchItem(ptr(p), ptr(d), ptr(m), nx, ny, nz, float(dx),
+                                         float(dt), float(rho), ptr(w), w.numel())
+        prm = BspSolveParams.from_buffer_copy(self.params)
+        prm.tol = float(tol)
+        prm.reuse_setup = 1 if self._setup_done else 0
+        infos = (BspSolveInfo * n)() if wait else None
+        code = _lib.lib().bsp_solve_batch(
+            n, ctypes.cast(items, ctypes.c_void_p), ctypes.byref(prm),
+            ctypes.cast(infos, ctypes.c_void_p) if wait else None, stream_handle(stream))
+        self._items = items  # keep the item array alive until the launch completes
+        _lib.check("bsp_solve_batch", code)
+        self._setup_done = True
+        return list(infos) if wait else None
 
 
 def solve_tolerance(div, mat, dx, dt, rho, tol=1e-6, storage="fp32", **kw) -> SolveResult:

@@ -185,12 +185,16 @@ struct UpOp {
     const float4 rr = ld4s(r, o);
     const int64_t P = ((int64_t)(i >> 1) * ny1 + (j >> 1)) * nz1 + (k >> 1);
     const float2 ec = ld2s(e1, P);
-    return make_float4(fmaf(rr.x, wdq(mw, 0), ec.x), fmaf(rr.y, wdq(mw, 1), ec.x),
-                       fmaf(rr.z, wdq(mw, 2), ec.y), fmaf(rr.w, wdq(mw, 3), ec.y));
+    // the coarse correction is not zero on non-fluid fine cells: mask it
+    auto fl = [&](float v, int q) {
+      return __uint_as_float(__float_as_uint(v) & fluid_word(mw, q));
+    };
+    return make_float4(fl(fmaf(rr.x, wdq(mw, 0), ec.x), 0), fl(fmaf(rr.y, wdq(mw, 1), ec.x), 1),
+                       fl(fmaf(rr.z, wdq(mw, 2), ec.y), 2), fl(fmaf(rr.w, wdq(mw, 3), ec.y), 3));
   }
   __device__ float val1(int i, int j, int k, int64_t o, uint32_t mb) const {
     const int64_t P = ((int64_t)(i >> 1) * ny1 + (j >> 1)) * nz1 + (k >> 1);
-    return fmaf(ld1s(r, o), wdinv_ns(mb & 7u), ld1s(e1, P));
+    return (mb & BSP_MFLUID) ? fmaf(ld1s(r, o), wdinv_ns(mb & 7u), ld1s(e1, P)) : 0.0f;
   }
   __device__ void emit(int, int, int, int64_t o, bool act, uint32_t mc, const float4 &v,
                        const float (&s)[4], float2 *) {
@@ -336,18 +340,19 @@ __global__ void __launch_bounds__(256) fine_col_kernel(Op op, int nx, int ny, in
         vkp = op.val1(i, j, k + 4, o + 4, mbyte);
       }
     }
-    const uint32_t mbw = (mc << 8) | (mkm >> 24);
-    const uint32_t mfw = (mc >> 8) | (mkp << 24);
+    // Every operand is exactly 0 on non-fluid cells and outside the grid, so the
+    // boundary rule (fluid -> operand, air -> 0, solid -> centre operand) is
+    // the plain sum of the six neighbours plus n_solid(centre) x centre.
+    (void)mkm;
+    (void)mkp;
     const float4 vb = make_float4(vkm, vc.x, vc.y, vc.z);
     const float4 vf = make_float4(vc.y, vc.z, vc.w, vkp);
     float s[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const float c = q4(vc, q);
-      s[q] = sel_nbr(mm, mm << 1, q, q4(vm, q), c) + sel_nbr(mn, mn << 1, q, q4(vn, q), c) +
-             sel_nbr(mjm, mjm << 1, q, q4(vjm, q), c) +
-             sel_nbr(mjp, mjp << 1, q, q4(vjp, q), c) + sel_nbr(mbw, mbw << 1, q, q4(vb, q), c) +
-             sel_nbr(mfw, mfw << 1, q, q4(vf, q), c);
+      const float ns = (float)((mc >> (8 * q)) & 7u);
+      s[q] = fmaf(ns, q4(vc, q),
+                  ((q4(vm, q) + q4(vn, q)) + (q4(vjm, q) + q4(vjp, q))) + (q4(vb, q) + q4(vf, q)));
     }
     op.emit(i, j, k, o, act, mc, vc, s, xch);
     vm = vc;

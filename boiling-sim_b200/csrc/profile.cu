@@ -18,7 +18,10 @@ std::vector<Rec> g_recs;
 std::vector<cudaEvent_t> g_pool;
 }  // namespace
 
-bool prof_enabled() { return g_on; }
+thread_local bool g_suspended = false;
+
+bool prof_enabled() { return g_on && !g_suspended; }
+void prof_suspend(bool on) { g_suspended = on; }
 
 cudaEvent_t prof_event() {
   std::lock_guard<std::mutex> lk(g_mu);

@@ -23,6 +23,9 @@ enum ProfClass {
 };
 
 bool prof_enabled();
+// While a graph is being captured, event timing is suspended (events recorded
+// into a graph would be re-recorded on every replay).
+void prof_suspend(bool on);
 void prof_record(int cls, cudaEvent_t a, cudaEvent_t b);
 cudaEvent_t prof_event();
 

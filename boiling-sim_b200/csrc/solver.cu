@@ -27,7 +27,9 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "bsp_common.cuh"
 #include "profile.cuh"
@@ -1033,6 +1035,263 @@ int solve_impl(void *ws, const uint8_t *mask, const float *div, float *p_out, in
   return fin.status;
 }
 
+// ======================================================================================
+// Device-driven solve: the whole refinement loop as one CUDA graph.
+//
+//   prologue: state init, ||b||, (warm start x = p)
+//   WHILE outer (default 1):  FP64 residual, outer check, residual -> rhat,
+//                             arm inner condition,
+//                             WHILE inner: two CG iterations, inner condition
+//                             x += e / scale, outer condition
+//   epilogue: p = (float) x
+//
+// The condition kernels count their own executions and clear the condition
+// after max_inner + 2 (inner) / max_outer + 2 (outer) bodies, so both loops end
+// whatever the rest of the state holds.  No host synchronisation inside.
+// ======================================================================================
+__global__ void init_state_kernel(SolverState *st, double tol, double eta, int max_outer,
+                                  int max_inner) {
+  SolverState s{};
+  s.tol = tol;
+  s.eta = eta;
+  s.eta_eff = eta;
+  s.max_outer = max_outer;
+  s.max_inner = max_inner;
+  s.scale = 1.0;
+  *st = s;
+}
+__global__ void arm_inner_kernel(cudaGraphConditionalHandle hi, SolverState *st) {
+  st->guard_inner = 0;
+  cudaGraphSetConditional(hi, st->done ? 0u : 1u);
+}
+__global__ void inner_cond_kernel(cudaGraphConditionalHandle hi, SolverState *st) {
+  const int g = ++st->guard_inner;
+  cudaGraphSetConditional(hi, (!st->inner_done && g <= st->max_inner + 2) ? 1u : 0u);
+}
+__global__ void outer_cond_kernel(cudaGraphConditionalHandle ho, SolverState *st) {
+  const int g = ++st->guard_outer;
+  cudaGraphSetConditional(ho, (!st->done && g <= st->max_outer + 2) ? 1u : 0u);
+}
+
+static cudaStream_t capture_stream() {
+  static std::mutex mu;
+  static cudaStream_t streams[64] = {nullptr};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 0 || dev >= 64) return nullptr;
+  if (!streams[dev]) cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
+  return streams[dev];
+}
+
+static cudaError_t seg_begin(cudaStream_t cs, cudaGraph_t g,
+                             const std::vector<cudaGraphNode_t> &deps) {
+  return cudaStreamBeginCaptureToGraph(cs, g, deps.empty() ? nullptr : deps.data(), nullptr,
+                                       deps.size(), cudaStreamCaptureModeThreadLocal);
+}
+static cudaError_t seg_end(cudaStream_t cs, std::vector<cudaGraphNode_t> &leaves) {
+  cudaStreamCaptureStatus stt;
+  const cudaGraphNode_t *d = nullptr;
+  size_t nd = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(cs, &stt, nullptr, nullptr, &d, &nd);
+  if (e == cudaSuccess) leaves.assign(d, d + nd);
+  cudaGraph_t out = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(cs, &out);
+  return e != cudaSuccess ? e : e2;
+}
+static cudaError_t add_while(cudaGraph_t g, const std::vector<cudaGraphNode_t> &deps,
+                             cudaGraphConditionalHandle h, cudaGraphNode_t *node,
+                             cudaGraph_t *body) {
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaError_t e = cudaGraphAddNode(node, g, deps.empty() ? nullptr : deps.data(), deps.size(), &cp);
+  if (e == cudaSuccess) *body = cp.conditional.phGraph_out[0];
+  return e;
+}
+
+// Appends one instance's solve to graph g after `deps`; `deps` returns its leaves.
+template <class T>
+cudaError_t append_solve(Ctx<T> &cx, const float *div, float *p_out, float dx, float dt, float rho,
+                         const BspSolveParams *prm, cudaGraph_t g,
+                         std::vector<cudaGraphNode_t> &deps) {
+  cudaStream_t cs = capture_stream();
+  if (!cs) return cudaErrorInvalidDevice;
+  const int nx = cx.nx, ny = cx.ny, nz = cx.nz;
+  const uint8_t *mask = cx.mask0;
+  SolverState *st = cx.st;
+  double *x = (double *)(cx.base + cx.lo.x);
+  float *eb = (float *)(cx.base + cx.lo.e);
+  const int nbr = row_blocks((int64_t)nx * ny);
+  const int nbf = flat_blocks(cx.n);
+  const double bscale = -((double)rho * (double)dx * (double)dx) / (double)dt;
+  cudaError_t e;
+  std::vector<cudaGraphNode_t> leaves;
+  // prologue
+  if ((e = seg_begin(cs, g, deps)) != cudaSuccess) return e;
+  init_state_kernel<<<1, 1, 0, cs>>>(st, prm->tol, prm->inner_tol, prm->max_outer,
+                                     prm->max_inner);
+  cudaMemsetAsync(x, 0, sizeof(double) * cx.n, cs);
+  residual64_kernel<T, false><<<nbr, 256, 0, cs>>>(nx, ny, nz, mask, div, x, bscale, nullptr,
+                                                  nullptr, cx.partials, st);
+  bnorm_kernel<<<1, RED_THREADS, 0, cs>>>(st, cx.partials, nbr);
+  if (prm->warm_start && p_out) f32_to_f64_kernel<<<nbf, 256, 0, cs>>>(cx.n, p_out, x, mask);
+  if ((e = seg_end(cs, leaves)) != cudaSuccess) return e;
+  cudaGraphConditionalHandle ho, hi;
+  if ((e = cudaGraphConditionalHandleCreate(&ho, g, 1, cudaGraphCondAssignDefault)) != cudaSuccess)
+    return e;
+  if ((e = cudaGraphConditionalHandleCreate(&hi, g, 0, 0)) != cudaSuccess) return e;
+  cudaGraphNode_t node_o, node_i;
+  cudaGraph_t body_o, body_i;
+  if ((e = add_while(g, leaves, ho, &node_o, &body_o)) != cudaSuccess) return e;
+  // outer body, part 1
+  if ((e = seg_begin(cs, body_o, {})) != cudaSuccess) return e;
+  residual64_kernel<T, false><<<nbr, 256, 0, cs>>>(nx, ny, nz, mask, div, x, bscale, nullptr,
+                                                  nullptr, cx.partials, st);
+  outer_check_kernel<<<1, RED_THREADS, 0, cs>>>(st, cx.partials, nbr,
+                                                prm->storage == BSP_STORE_FP32);
+  residual64_kernel<T, true><<<nbr, 256, 0, cs>>>(nx, ny, nz, mask, div, x, bscale, cx.lv[0].r,
+                                                 eb, cx.partials, st);
+  arm_inner_kernel<<<1, 1, 0, cs>>>(hi, st);
+  if ((e = seg_end(cs, leaves)) != cudaSuccess) return e;
+  if ((e = add_while(body_o, leaves, hi, &node_i, &body_i)) != cudaSuccess) return e;
+  // inner body: two iterations (the search-direction buffers alternate)
+  if ((e = seg_begin(cs, body_i, {})) != cudaSuccess) return e;
+  launch_inner_iteration<T>(cx, 0, cs);
+  launch_inner_iteration<T>(cx, 1, cs);
+  inner_cond_kernel<<<1, 1, 0, cs>>>(hi, st);
+  if ((e = seg_end(cs, leaves)) != cudaSuccess) return e;
+  // outer body, part 2
+  if ((e = seg_begin(cs, body_o, {node_i})) != cudaSuccess) return e;
+  xupdate_kernel<<<nbf, 256, 0, cs>>>(cx.n, x, eb, nullptr, st);
+  outer_cond_kernel<<<1, 1, 0, cs>>>(ho, st);
+  if ((e = seg_end(cs, leaves)) != cudaSuccess) return e;
+  // epilogue
+  if ((e = seg_begin(cs, g, {node_o})) != cudaSuccess) return e;
+  if (p_out) f64_to_f32_kernel<<<nbf, 256, 0, cs>>>(cx.n, x, p_out, mask);
+  return seg_end(cs, deps);  // without p_out the segment is empty: leaves = {node_o}
+}
+
+// Executable graphs of recent solves, keyed by everything baked into them.
+struct GraphKey {
+  std::vector<uintptr_t> v;
+  bool operator==(const GraphKey &o) const { return v == o.v; }
+};
+struct GraphEntry {
+  GraphKey key;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+static std::mutex g_graph_mu;
+static std::vector<GraphEntry> g_graphs;
+
+static cudaGraphExec_t graph_lookup(const GraphKey &k) {
+  for (auto &e : g_graphs)
+    if (e.key == k) return e.exec;
+  return nullptr;
+}
+static void graph_store(const GraphKey &k, cudaGraph_t g, cudaGraphExec_t x) {
+  if (g_graphs.size() >= 8) {
+    cudaGraphExecDestroy(g_graphs.front().exec);
+    cudaGraphDestroy(g_graphs.front().graph);
+    g_graphs.erase(g_graphs.begin());
+  }
+  g_graphs.push_back(GraphEntry{k, g, x});
+}
+
+static void key_floats(GraphKey &k, float a, float b, float c) {
+  uint32_t u[3];
+  memcpy(&u[0], &a, 4);
+  memcpy(&u[1], &b, 4);
+  memcpy(&u[2], &c, 4);
+  for (uint32_t x : u) k.v.push_back(x);
+}
+static void key_params(GraphKey &k, const BspSolveParams *p);
+
+template <class T>
+static int finish_info(const Ctx<T> &cx, BspSolveInfo *info, cudaStream_t s) {
+  SolverState fin{};
+  cudaError_t e = cudaMemcpyAsync(&fin, cx.st, sizeof(SolverState), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return (int)e;
+  if (info) {
+    info->outer_iterations = fin.outer_it;
+    info->inner_iterations = fin.total_inner;
+    info->rel_residual = fin.rel;
+    info->levels = cx.lo.L;
+  }
+  return fin.status;
+}
+
+// One batch of solves (count >= 1) as one graph launch: independent branches,
+// one per instance.  Level setup runs (or is reused) before the launch.
+template <class T>
+int solve_graph_batch(int count, const BspBatchItem *items, const BspSolveParams *prm,
+                      BspSolveInfo *infos, cudaStream_t s) {
+  std::vector<Ctx<T>> cxs;
+  GraphKey key;
+  key.v.push_back((uintptr_t)count);
+  key_params(key, prm);
+  for (int q = 0; q < count; ++q) {
+    const BspBatchItem &it = items[q];
+    Ctx<T> cx = make_ctx<T>(it.workspace, it.mask, it.nx, it.ny, it.nz, prm->storage);
+    const Level<T> &c = cx.lv[cx.lo.L - 1];
+    if ((int64_t)c.nx * c.ny * c.nz > COARSEST_MAX) return BSP_ERR_SHAPE;
+    if (!(prm->reuse_setup &&
+          setup_cached(it.workspace, it.mask, it.nx, it.ny, it.nz, prm->storage))) {
+      cudaError_t e = setup_levels<T>(cx, s);
+      if (e != cudaSuccess) return (int)e;
+      remember_setup(it.workspace, it.mask, it.nx, it.ny, it.nz, prm->storage);
+    }
+    for (uintptr_t x : {(uintptr_t)it.workspace, (uintptr_t)it.mask, (uintptr_t)it.div,
+                        (uintptr_t)it.p, (uintptr_t)it.nx, (uintptr_t)it.ny, (uintptr_t)it.nz})
+      key.v.push_back(x);
+    key_floats(key, it.dx, it.dt, it.rho);
+    cxs.push_back(cx);
+  }
+  std::lock_guard<std::mutex> lk(g_graph_mu);
+  cudaGraphExec_t exec = graph_lookup(key);
+  if (!exec) {
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaGraphCreate(&g, 0);
+    prof_suspend(true);
+    for (int q = 0; q < count && e == cudaSuccess; ++q) {
+      std::vector<cudaGraphNode_t> deps;
+      e = append_solve<T>(cxs[q], items[q].div, items[q].p, items[q].dx, items[q].dt,
+                          items[q].rho, prm, g, deps);
+    }
+    prof_suspend(false);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, g, 0);
+    if (e != cudaSuccess) {
+      if (g) cudaGraphDestroy(g);
+      return (int)e;
+    }
+    graph_store(key, g, exec);
+  }
+  cudaError_t e = cudaGraphLaunch(exec, s);
+  if (e != cudaSuccess) return (int)e;
+  if (!infos) return BSP_OK;  // asynchronous: results land in p when the stream reaches them
+  int status = BSP_OK;
+  for (int q = 0; q < count; ++q) {
+    const int st = finish_info<T>(cxs[q], &infos[q], s);
+    if (st != BSP_OK && status == BSP_OK) status = st;
+  }
+  return status;
+}
+
+static void key_params(GraphKey &k, const BspSolveParams *p) {
+  uint64_t t, it;
+  memcpy(&t, &p->tol, 8);
+  memcpy(&it, &p->inner_tol, 8);
+  for (uintptr_t x : {(uintptr_t)t, (uintptr_t)it, (uintptr_t)p->max_outer,
+                      (uintptr_t)p->max_inner, (uintptr_t)p->storage,
+                      (uintptr_t)p->warm_start})
+    k.v.push_back(x);
+}
+
 }  // namespace bsp
 
 using namespace bsp;
@@ -1052,6 +1311,7 @@ extern "C" void bsp_solve_params_default(BspSolveParams *p) {
   p->warm_start = 0;
   p->check_every = 8;
   p->reuse_setup = 0;
+  p->use_graph = 0;
 }
 
 extern "C" int bsp_solve_tol(float *p, const float *div_u, const uint8_t *mask, int nx, int ny,
@@ -1067,18 +1327,32 @@ extern "C" int bsp_solve_tol(float *p, const float *div_u, const uint8_t *mask, 
       params->max_inner <= 0 || params->max_outer < 0 || !(params->tol >= 0.0))
     return BSP_ERR_ARG;
   int st;
-  switch (params->storage) {
-    case BSP_STORE_FP16:
-      st = solve_impl<__half>(workspace, mask, div_u, p, nx, ny, nz, dx, dt, rho, params, info,
-                              stream);
-      break;
-    case BSP_STORE_BF16:
-      st = solve_impl<__nv_bfloat16>(workspace, mask, div_u, p, nx, ny, nz, dx, dt, rho, params,
-                                     info, stream);
-      break;
-    default:
-      st = solve_impl<float>(workspace, mask, div_u, p, nx, ny, nz, dx, dt, rho, params, info,
-                             stream);
+  if (params->use_graph) {
+    const BspBatchItem item{p, div_u, mask, nx, ny, nz, dx, dt, rho, workspace, workspace_bytes};
+    switch (params->storage) {
+      case BSP_STORE_FP16:
+        st = solve_graph_batch<__half>(1, &item, params, info, stream);
+        break;
+      case BSP_STORE_BF16:
+        st = solve_graph_batch<__nv_bfloat16>(1, &item, params, info, stream);
+        break;
+      default:
+        st = solve_graph_batch<float>(1, &item, params, info, stream);
+    }
+  } else {
+    switch (params->storage) {
+      case BSP_STORE_FP16:
+        st = solve_impl<__half>(workspace, mask, div_u, p, nx, ny, nz, dx, dt, rho, params,
+                                info, stream);
+        break;
+      case BSP_STORE_BF16:
+        st = solve_impl<__nv_bfloat16>(workspace, mask, div_u, p, nx, ny, nz, dx, dt, rho,
+                                       params, info, stream);
+        break;
+      default:
+        st = solve_impl<float>(workspace, mask, div_u, p, nx, ny, nz, dx, dt, rho, params, info,
+                               stream);
+    }
   }
   if (x64_out && (st == BSP_OK || st == BSP_NOT_CONVERGED)) {
     const Layout lo = make_layout(nx, ny, nz, params->storage);
@@ -1086,4 +1360,30 @@ extern "C" int bsp_solve_tol(float *p, const float *div_u, const uint8_t *mask, 
                     cudaMemcpyDeviceToDevice, stream);
   }
   return st;
+}
+
+extern "C" int bsp_solve_batch(int count, const BspBatchItem *items,
+                               const BspSolveParams *params, BspSolveInfo *infos,
+                               cudaStream_t stream) {
+  if (count <= 0) return BSP_OK;
+  if (!items || !params) return BSP_ERR_NULL;
+  if (params->storage < 0 || params->storage > 2 || params->max_inner <= 0 ||
+      params->max_outer < 0 || !(params->tol >= 0.0))
+    return BSP_ERR_ARG;
+  for (int q = 0; q < count; ++q) {
+    const BspBatchItem &it = items[q];
+    if (it.nx <= 0 || it.ny <= 0 || it.nz <= 0) return BSP_ERR_SHAPE;
+    if (!it.p || !it.div || !it.mask || !it.workspace) return BSP_ERR_NULL;
+    if (((uintptr_t)it.workspace & 255u) != 0) return BSP_ERR_ALIGN;
+    if (it.workspace_bytes < bsp_solver_workspace_bytes(it.nx, it.ny, it.nz, params->storage))
+      return BSP_ERR_WORKSPACE;
+  }
+  switch (params->storage) {
+    case BSP_STORE_FP16:
+      return solve_graph_batch<__half>(count, items, params, infos, stream);
+    case BSP_STORE_BF16:
+      return solve_graph_batch<__nv_bfloat16>(count, items, params, infos, stream);
+    default:
+      return solve_graph_batch<float>(count, items, params, infos, stream);
+  }
 }

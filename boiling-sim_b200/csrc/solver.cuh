@@ -26,6 +26,9 @@ struct SolverState {
   int max_outer, max_inner;
   int outer_it, inner_it, total_inner;
   int done, inner_done, status, finalize, pad;
+  // loop guards of the graph-driven solve: counted by the condition kernels
+  // themselves so every WHILE node ends even if other state went wrong
+  int guard_inner, guard_outer;
 };
 
 // Level-0 kernels on the column layout (mgfine.cu); nz % 4 == 0 required.

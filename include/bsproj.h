@@ -228,7 +228,20 @@ typedef struct BspSolveParams {
   int check_every;  /* inner iterations enqueued between host reads of the done flag */
   int reuse_setup;  /* 1: the mask is unchanged since the last solve on this workspace,
                        reuse its multigrid setup (coarse masks, coarsest inverse) */
+  int use_graph;    /* 1: run the whole solve as one CUDA graph (conditional WHILE
+                       nodes, no host synchronisation; built once per pointer set) */
 } BspSolveParams;
+
+/* One instance of a batched solve. */
+typedef struct BspBatchItem {
+  float *p;              /* out: pressure (in, when warm_start) */
+  const float *div;      /* divergence */
+  const uint8_t *mask;   /* uint8 cell mask of this instance */
+  int nx, ny, nz;
+  float dx, dt, rho;
+  void *workspace;       /* bsp_solver_workspace_bytes(nx, ny, nz, storage) bytes */
+  size_t workspace_bytes;
+} BspBatchItem;
 
 typedef struct BspSolveInfo {
   int outer_iterations;
@@ -268,6 +281,17 @@ int bsp_solve_tol(float *p, const float *div_u, const uint8_t *mask, int nx, int
 #define BSP_DOT_NOALLOC_MAX_N 67108864LL
 int bsp_dot_noalloc(const float *x, const float *y, int64_t n, double *result_dev,
                     cudaStream_t stream);
+
+/* Solves `count` independent systems (uneven sizes allowed, one workspace
+ * each) with one CUDA graph launch: every instance is an independent branch
+ * of the graph running its own refinement and CG loops as conditional WHILE
+ * nodes, so small instances overlap on the GPU.  The graph is built on the
+ * first call for a given item set and replayed afterwards.  If infos is
+ * non-NULL the call waits for the batch and fills one BspSolveInfo per item
+ * (returning the first non-OK status); otherwise it returns after the
+ * launch.  Batched pot scenes of the benchmark configuration (64 instances). */
+int bsp_solve_batch(int count, const BspBatchItem *items, const BspSolveParams *params,
+                    BspSolveInfo *infos, cudaStream_t stream);
 
 /* Exhaustive self-check of the device division-by-6 against IEEE division
  * over all 2^32 float bit patterns; the mismatch count is written to the
