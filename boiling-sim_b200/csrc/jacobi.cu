@@ -17,10 +17,15 @@ cudaError_t launch_stencil(float *out, const float *p, const float *div, const M
                            int ma, cudaStream_t s);
 cudaError_t launch_rhs(float *rhs, const float *div, const uint8_t *mask, int64_t n, float dx,
                        float dt, float rho, cudaStream_t s);
+cudaError_t launch_sweep_znf(float *out, const float *p, const float *rhs, const uint8_t *mask,
+                             int nx, int ny, int nz, cudaStream_t s);
 
+// p_zero_nonfluid: the caller guarantees p holds +0 on non-fluid cells (the
+// projection zeroes p); every later source was written by a sweep, which
+// writes +0 there, so from the second sweep on the ZNF kernel applies.
 int jacobi_solve_impl(float *p, float *p_tmp, const float *div_u, float *rhs_ws,
                       const uint8_t *mask, int nx, int ny, int nz, float dx, float dt, float rho,
-                      int n_iter, int tblock, cudaStream_t stream) {
+                      int n_iter, int tblock, cudaStream_t stream, bool p_zero_nonfluid) {
   (void)tblock;
   if (n_iter <= 0) return BSP_OK;
   const int64_t n = (int64_t)nx * ny * nz;
@@ -32,9 +37,11 @@ int jacobi_solve_impl(float *p, float *p_tmp, const float *div_u, float *rhs_ws,
     float *dst = (it & 1) == 0 ? p_tmp : p;
     const float *src = (it & 1) == 0 ? p : p_tmp;
     ProfScope ps(PROF_SWEEP, stream);
+    const bool znf = it > 0 || p_zero_nonfluid;
     cudaError_t e =
-        rhs_ws ? launch_stencil<2, uint8_t>(dst, src, rhs_ws, mask, nx, ny, nz, dx, dt, rho,
-                                            BSP_FLUID, BSP_AIR, stream)
+        rhs_ws ? (znf ? launch_sweep_znf(dst, src, rhs_ws, mask, nx, ny, nz, stream)
+                      : launch_stencil<2, uint8_t>(dst, src, rhs_ws, mask, nx, ny, nz, dx, dt,
+                                                   rho, BSP_FLUID, BSP_AIR, stream))
                : launch_stencil<0, uint8_t>(dst, src, div_u, mask, nx, ny, nz, dx, dt, rho,
                                             BSP_FLUID, BSP_AIR, stream);
     if (e != cudaSuccess) return (int)e;
@@ -56,5 +63,5 @@ extern "C" int bsp_jacobi_solve(float *p, float *p_tmp, const float *div_u, floa
   if (!p || !p_tmp || !div_u || !mask) return BSP_ERR_NULL;
   if (p == p_tmp || rhs_ws == p || rhs_ws == p_tmp) return BSP_ERR_ALIAS;
   return bsp::jacobi_solve_impl(p, p_tmp, div_u, rhs_ws, mask, nx, ny, nz, dx, dt, rho, n_iter,
-                                tblock, stream);
+                                tblock, stream, false);
 }

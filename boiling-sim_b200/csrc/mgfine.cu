@@ -364,6 +364,105 @@ __global__ void __launch_bounds__(256) fine_col_kernel(Op op, int nx, int ny, in
   op.finish(sh);
 }
 
+// ---- FP64 residual on the column layout --------------------------------------------------
+// r = bscale div - (6 x - s) on fluid cells (0 elsewhere) with the FP64 iterate
+// x, which is exactly 0 on non-fluid cells, so s = sum of the six neighbours +
+// n_solid x_centre.  Partials: ||r||^2 (slot 0) and max|r| (slot 1).  WRITE:
+// rhat = scale r (storage T) and e = 0 on every cell.
+struct D4 {
+  double a, b, c, d;
+};
+__device__ __forceinline__ D4 ld4d(const double *p, int64_t o) {
+  const double2 u = *reinterpret_cast<const double2 *>(p + o);
+  const double2 v = *reinterpret_cast<const double2 *>(p + o + 2);
+  return D4{u.x, u.y, v.x, v.y};
+}
+__device__ __forceinline__ double dq(const D4 &v, int q) {
+  return q == 0 ? v.a : (q == 1 ? v.b : (q == 2 ? v.c : v.d));
+}
+
+template <class T, bool WRITE>
+__global__ void __launch_bounds__(256) resid64_col_kernel(int nx, int ny, int nz, int bi,
+                                                          const uint8_t *mask, const float *div,
+                                                          const double *x, double bscale, T *rhat,
+                                                          float *e, double *partials,
+                                                          const SolverState *st) {
+  if (st->done) return;
+  const double scale = st->scale;
+  __shared__ double shs[8], shm[8];
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
+  const int k = (blockIdx.x * 32 + lane) * 4;
+  const bool act = j < ny && k < nz;
+  const int i0 = blockIdx.z * bi;
+  const int i1 = min(i0 + bi, nx);
+  const int64_t plane = (int64_t)ny * nz;
+  const D4 z4{0, 0, 0, 0};
+  int64_t o = act ? (int64_t)i0 * plane + (int64_t)j * nz + k : 0;
+  D4 xm = z4, xc = z4;
+  if (act && i0 > 0) xm = ld4d(x, o - plane);
+  if (act) xc = ld4d(x, o);
+  double rr = 0.0, rmax = 0.0;
+  for (int i = i0; i < i1; ++i) {
+    D4 xn = z4, xjm = z4, xjp = z4;
+    if (act) {
+      if (i + 1 < nx) xn = ld4d(x, o + plane);
+      if (j > 0) xjm = ld4d(x, o - nz);
+      if (j + 1 < ny) xjp = ld4d(x, o + nz);
+    }
+    double xkm = __shfl_up_sync(0xffffffffu, xc.d, 1);
+    double xkp = __shfl_down_sync(0xffffffffu, xc.a, 1);
+    if (lane == 0) xkm = (act && k > 0) ? x[o - 1] : 0.0;
+    if (lane == 31) xkp = (act && k + 4 < nz) ? x[o + 4] : 0.0;
+    if (act) {
+      const uint32_t mc = __ldg(reinterpret_cast<const uint32_t *>(mask + o));
+      const float4 dv = *reinterpret_cast<const float4 *>(div + o);
+      const D4 xb{xkm, xc.a, xc.b, xc.c}, xf{xc.b, xc.c, xc.d, xkp};
+      float rq[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t mb = (mc >> (8 * q)) & 0xffu;
+        double r = 0.0;
+        if (mb & BSP_MFLUID) {
+          const double c = dq(xc, q);
+          const double s = ((dq(xm, q) + dq(xn, q)) + (dq(xjm, q) + dq(xjp, q))) +
+                           (dq(xb, q) + dq(xf, q)) + (double)(mb & 7u) * c;
+          r = bscale * (double)q4(dv, q) - (6.0 * c - s);
+        }
+        rr += r * r;
+        rmax = fmax(rmax, fabs(r));
+        rq[q] = (float)(r * scale);
+      }
+      if (WRITE) {
+        st4s(rhat, o, make_float4(rq[0], rq[1], rq[2], rq[3]));
+        *reinterpret_cast<float4 *>(e + o) = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+    }
+    xm = xc;
+    xc = xn;
+    if (act) o += plane;
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    rr += __shfl_xor_sync(0xffffffffu, rr, off);
+    rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, off));
+  }
+  if (lane == 0) {
+    shs[threadIdx.x >> 5] = rr;
+    shm[threadIdx.x >> 5] = rmax;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0.0, m = 0.0;
+    for (int w = 0; w < 8; ++w) {
+      a += shs[w];
+      m = fmax(m, shm[w]);
+    }
+    const int b = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+    partials[b] = a;
+    partials[PARTIAL_STRIDE + b] = m;
+  }
+}
+
 // ---- launchers --------------------------------------------------------------------------
 int num_sms();
 
@@ -432,7 +531,25 @@ void launch_fine_down(const Level<T> &f, const Level<T> &c, const SolverState *s
       op, f.nx, f.ny, f.nz, fine_bi(f.nx, f.ny, f.nz), st);
 }
 
+template <class T>
+int launch_resid64_col(int nx, int ny, int nz, const uint8_t *mask, const float *div,
+                       const double *x, double bscale, T *rhat, float *e, double *partials,
+                       const SolverState *st, bool write, cudaStream_t s) {
+  const dim3 g = fine_grid(nx, ny, nz);
+  const int bi = fine_bi(nx, ny, nz);
+  if (write)
+    resid64_col_kernel<T, true><<<g, 256, 0, s>>>(nx, ny, nz, bi, mask, div, x, bscale, rhat, e,
+                                                  partials, st);
+  else
+    resid64_col_kernel<T, false><<<g, 256, 0, s>>>(nx, ny, nz, bi, mask, div, x, bscale, rhat,
+                                                   e, partials, st);
+  return (int)(g.x * g.y * g.z);
+}
+
 #define INST(T)                                                                              \
+  template int launch_resid64_col<T>(int, int, int, const uint8_t *, const float *,          \
+                                     const double *, double, T *, float *, double *,         \
+                                     const SolverState *, bool, cudaStream_t);               \
   template void launch_fine_psap<T>(int, int, int, const uint8_t *, const T *, const T *, T *, \
                                     T *, double *, const SolverState *, cudaStream_t);         \
   template void launch_fine_up<T>(const Level<T> &, const Level<T> &, T *, double *,          \

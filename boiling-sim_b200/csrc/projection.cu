@@ -22,7 +22,7 @@ cudaError_t launch_stencil(float *out, const float *p, const float *div, const M
                            int ma, cudaStream_t s);
 int jacobi_solve_impl(float *p, float *p_tmp, const float *div_u, float *rhs_ws,
                       const uint8_t *mask, int nx, int ny, int nz, float dx, float dt, float rho,
-                      int n_iter, int tblock, cudaStream_t stream);
+                      int n_iter, int tblock, cudaStream_t stream, bool p_zero_nonfluid);
 
 // Block = (128 k, 2 j); grid = (k tiles, j tiles, i).  One cell per thread.
 __global__ void __launch_bounds__(256) divergence_kernel(
@@ -204,7 +204,7 @@ extern "C" int bsp_projection_jacobi(float *p, float *p_tmp, float *div_u, float
   // div_u belongs to the projection until the diagnostic divergence below
   // overwrites it, so it holds rho dx^2 div / dt (in place) during the sweeps.
   int st = jacobi_solve_impl(p, p_tmp, div_u, div_u, mask, nx, ny, nz, dx, dt, rho, n_iter,
-                             tblock, stream);
+                             tblock, stream, /*p zeroed above*/ true);
   if (st != BSP_OK) return st;
   e = gradient_impl(ux, uy, uz, p, mask, nx, ny, nz, dx, dt, rho, stream);
   if (e != cudaSuccess) return (int)e;

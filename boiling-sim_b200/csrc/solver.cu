@@ -897,6 +897,25 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+// FP64 residual pass (norm pass, or WRITE: rhat and e = 0): the column kernel
+// when level 0 runs on the column layout and div is 16-byte aligned, else the
+// per-row kernel.  Returns the number of partial blocks written.
+template <class T>
+int launch_resid(Ctx<T> &cx, const float *div, const double *x, double bscale, T *rhat, float *e,
+                 bool write, cudaStream_t s) {
+  if (cx.col && ((uintptr_t)div & 15u) == 0)
+    return launch_resid64_col<T>(cx.nx, cx.ny, cx.nz, cx.mask0, div, x, bscale, rhat, e,
+                                 cx.partials, cx.st, write, s);
+  const int nbr = row_blocks((int64_t)cx.nx * cx.ny);
+  if (write)
+    residual64_kernel<T, true><<<nbr, 256, 0, s>>>(cx.nx, cx.ny, cx.nz, cx.mask0, div, x, bscale,
+                                                  rhat, e, cx.partials, cx.st);
+  else
+    residual64_kernel<T, false><<<nbr, 256, 0, s>>>(cx.nx, cx.ny, cx.nz, cx.mask0, div, x,
+                                                   bscale, rhat, e, cx.partials, cx.st);
+  return nbr;
+}
+
 __global__ void f32_to_f64_kernel(int64_t n, const float *a, double *b, const uint8_t *mask) {
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += (int64_t)gridDim.x * blockDim.x)
@@ -971,14 +990,15 @@ int solve_impl(void *ws, const uint8_t *mask, const float *div, float *p_out, in
   // ||b||^2: a residual pass with x = 0
   e = cudaMemsetAsync(x, 0, sizeof(double) * cx.n, s);
   if (e != cudaSuccess) return (int)e;
+  (void)nbr;
+  int nres;
   {
     ProfScope ps(PROF_RESID64, s);
-    residual64_kernel<T, false><<<nbr, 256, 0, s>>>(nx, ny, nz, mask, div, x, bscale, nullptr,
-                                                   nullptr, cx.partials, cx.st);
+    nres = launch_resid<T>(cx, div, x, bscale, nullptr, nullptr, false, s);
   }
   {
     ProfScope ps(PROF_CONTROL, s);
-    bnorm_kernel<<<1, RED_THREADS, 0, s>>>(cx.st, cx.partials, nbr);
+    bnorm_kernel<<<1, RED_THREADS, 0, s>>>(cx.st, cx.partials, nres);
   }
   if (prm->warm_start && p_out) {
     ProfScope ps(PROF_CONTROL, s);
@@ -988,18 +1008,16 @@ int solve_impl(void *ws, const uint8_t *mask, const float *div, float *p_out, in
   for (int outer = 0; outer <= prm->max_outer; ++outer) {
     {
       ProfScope ps(PROF_RESID64, s);
-      residual64_kernel<T, false><<<nbr, 256, 0, s>>>(nx, ny, nz, mask, div, x, bscale,
-                                                     nullptr, nullptr, cx.partials, cx.st);
+      nres = launch_resid<T>(cx, div, x, bscale, nullptr, nullptr, false, s);
     }
     {
       ProfScope ps(PROF_CONTROL, s);
-      outer_check_kernel<<<1, RED_THREADS, 0, s>>>(cx.st, cx.partials, nbr,
+      outer_check_kernel<<<1, RED_THREADS, 0, s>>>(cx.st, cx.partials, nres,
                                                    prm->storage == BSP_STORE_FP32);
     }
     {
       ProfScope ps(PROF_RESID64, s);
-      residual64_kernel<T, true><<<nbr, 256, 0, s>>>(nx, ny, nz, mask, div, x, bscale,
-                                                    cx.lv[0].r, eb, cx.partials, cx.st);
+      launch_resid<T>(cx, div, x, bscale, cx.lv[0].r, eb, true, s);
     }
     // 4-byte flag read (pageable: the copy completes before the sync returns)
     e = cudaMemcpyAsync(&flag, &cx.st->done, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -1134,9 +1152,9 @@ cudaError_t append_solve(Ctx<T> &cx, const float *div, float *p_out, float dx, f
   init_state_kernel<<<1, 1, 0, cs>>>(st, prm->tol, prm->inner_tol, prm->max_outer,
                                      prm->max_inner);
   cudaMemsetAsync(x, 0, sizeof(double) * cx.n, cs);
-  residual64_kernel<T, false><<<nbr, 256, 0, cs>>>(nx, ny, nz, mask, div, x, bscale, nullptr,
-                                                  nullptr, cx.partials, st);
-  bnorm_kernel<<<1, RED_THREADS, 0, cs>>>(st, cx.partials, nbr);
+  (void)nbr;
+  const int nres = launch_resid<T>(cx, div, x, bscale, nullptr, nullptr, false, cs);
+  bnorm_kernel<<<1, RED_THREADS, 0, cs>>>(st, cx.partials, nres);
   if (prm->warm_start && p_out) f32_to_f64_kernel<<<nbf, 256, 0, cs>>>(cx.n, p_out, x, mask);
   if ((e = seg_end(cs, leaves)) != cudaSuccess) return e;
   cudaGraphConditionalHandle ho, hi;
@@ -1148,12 +1166,10 @@ cudaError_t append_solve(Ctx<T> &cx, const float *div, float *p_out, float dx, f
   if ((e = add_while(g, leaves, ho, &node_o, &body_o)) != cudaSuccess) return e;
   // outer body, part 1
   if ((e = seg_begin(cs, body_o, {})) != cudaSuccess) return e;
-  residual64_kernel<T, false><<<nbr, 256, 0, cs>>>(nx, ny, nz, mask, div, x, bscale, nullptr,
-                                                  nullptr, cx.partials, st);
-  outer_check_kernel<<<1, RED_THREADS, 0, cs>>>(st, cx.partials, nbr,
+  launch_resid<T>(cx, div, x, bscale, nullptr, nullptr, false, cs);
+  outer_check_kernel<<<1, RED_THREADS, 0, cs>>>(st, cx.partials, nres,
                                                 prm->storage == BSP_STORE_FP32);
-  residual64_kernel<T, true><<<nbr, 256, 0, cs>>>(nx, ny, nz, mask, div, x, bscale, cx.lv[0].r,
-                                                 eb, cx.partials, st);
+  launch_resid<T>(cx, div, x, bscale, cx.lv[0].r, eb, true, cs);
   arm_inner_kernel<<<1, 1, 0, cs>>>(hi, st);
   if ((e = seg_end(cs, leaves)) != cudaSuccess) return e;
   if ((e = add_while(body_o, leaves, hi, &node_i, &body_i)) != cudaSuccess) return e;

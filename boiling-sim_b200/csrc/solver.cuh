@@ -42,5 +42,10 @@ void launch_fine_up(const Level<T> &f, const Level<T> &c, T *z, double *partials
 template <class T>
 void launch_fine_down(const Level<T> &f, const Level<T> &c, const SolverState *st,
                       cudaStream_t s);
+// FP64 residual on the column layout; returns the number of partial blocks.
+template <class T>
+int launch_resid64_col(int nx, int ny, int nz, const uint8_t *mask, const float *div,
+                       const double *x, double bscale, T *rhat, float *e, double *partials,
+                       const SolverState *st, bool write, cudaStream_t s);
 
 }  // namespace bsp

@@ -65,7 +65,17 @@ __device__ __forceinline__ float4 ld4(const float *p) {
 // from L1 (neighbouring warps' rows); k +- 1 from warp shuffles.  Neighbour
 // values are chosen with sel_nbr (two prmt + one lop3, no branches); the sum
 // order is the reference's l, r, d, u, b, f.
-template <int OP, class MaskT, bool FULL>
+//
+// ZNF: the source field holds +0 on every non-fluid cell (true after one sweep,
+// and for a projection, which zeroes p first).  Then the neighbour rule
+// fluid -> p_n, air -> 0, solid -> p_self is exactly p_n | (p_self & solid) on
+// bit patterns (p_n is +0 on air and solid cells): one prmt + one lop3.
+__device__ __forceinline__ float znf_nbr(uint32_t sw, int q, float pn, float ps) {
+  const uint32_t sm = sign_bytes(sw, (uint32_t)(8 | q) * 0x1111u);
+  return __uint_as_float(__float_as_uint(pn) | (__float_as_uint(ps) & sm));
+}
+
+template <int OP, class MaskT, bool FULL, bool ZNF>
 __global__ void __launch_bounds__(256) stencil_col_kernel(
     float *__restrict__ out, const float *__restrict__ p, const float *__restrict__ src,
     const MaskT *__restrict__ mask, int nx, int ny, int nz, int bi, float rdd, float dt,
@@ -134,12 +144,22 @@ __global__ void __launch_bounds__(256) stencil_col_kernel(
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const float ps = f4(pc, q);
-        const float l = sel_nbr(mm, mm << 1, q, f4(pm, q), ps);
-        const float r = sel_nbr(mn, mn << 1, q, f4(pn, q), ps);
-        const float d = sel_nbr(mjm, mjm << 1, q, f4(pjm, q), ps);
-        const float u = sel_nbr(mjp, mjp << 1, q, f4(pjp, q), ps);
-        const float b = sel_nbr(mb, mb << 1, q, f4(pb, q), ps);
-        const float f = sel_nbr(mfw, mfw << 1, q, f4(pf, q), ps);
+        float l, r, d, u, b, f;
+        if (ZNF) {
+          l = znf_nbr(mm << 1, q, f4(pm, q), ps);
+          r = znf_nbr(mn << 1, q, f4(pn, q), ps);
+          d = znf_nbr(mjm << 1, q, f4(pjm, q), ps);
+          u = znf_nbr(mjp << 1, q, f4(pjp, q), ps);
+          b = znf_nbr(mb << 1, q, f4(pb, q), ps);
+          f = znf_nbr(mfw << 1, q, f4(pf, q), ps);
+        } else {
+          l = sel_nbr(mm, mm << 1, q, f4(pm, q), ps);
+          r = sel_nbr(mn, mn << 1, q, f4(pn, q), ps);
+          d = sel_nbr(mjm, mjm << 1, q, f4(pjm, q), ps);
+          u = sel_nbr(mjp, mjp << 1, q, f4(pjp, q), ps);
+          b = sel_nbr(mb, mb << 1, q, f4(pb, q), ps);
+          f = sel_nbr(mfw, mfw << 1, q, f4(pf, q), ps);
+        }
         float v;
         if (OP == OP_SPMV) {
           v = spmv_update(l, r, d, u, b, f, ps);
@@ -311,16 +331,37 @@ cudaError_t launch_stencil(float *out, const float *p, const float *div, const M
     const int bi = g_sweep_bi > 0 ? g_sweep_bi : pick_bi(nx, ny, nz);
     dim3 grid((nz / 4 + 31) / 32, (ny + 7) / 8, (nx + bi - 1) / bi);
     if (nz % 128 == 0)
-      stencil_col_kernel<OP, MaskT, true><<<grid, 256, 0, s>>>(out, p, div, mask, nx, ny, nz,
-                                                               bi, rdd, dt, mf, ma);
+      stencil_col_kernel<OP, MaskT, true, false><<<grid, 256, 0, s>>>(out, p, div, mask, nx, ny,
+                                                                      nz, bi, rdd, dt, mf, ma);
     else
-      stencil_col_kernel<OP, MaskT, false><<<grid, 256, 0, s>>>(out, p, div, mask, nx, ny, nz,
-                                                                bi, rdd, dt, mf, ma);
+      stencil_col_kernel<OP, MaskT, false, false><<<grid, 256, 0, s>>>(out, p, div, mask, nx, ny,
+                                                                       nz, bi, rdd, dt, mf, ma);
   } else {
     const int64_t n = (int64_t)nx * ny * nz;
     stencil_generic_kernel<OP, MaskT><<<generic_blocks(n), 256, 0, s>>>(out, p, div, mask, nx,
                                                                         ny, nz, rdd, dt, mf, ma);
   }
+  return cudaGetLastError();
+}
+
+// Jacobi sweep with precomputed rhs on a source whose non-fluid cells are +0
+// (the ZNF column kernel), or the general kernels when the layout does not
+// allow the column kernel.  Bit-identical to launch_stencil<OP_JACOBI_RHS>.
+cudaError_t launch_sweep_znf(float *out, const float *p, const float *rhs, const uint8_t *mask,
+                             int nx, int ny, int nz, cudaStream_t s) {
+  const bool col_ok = (nz % 4 == 0) && aligned16(out) && aligned16(p) && aligned16(rhs) &&
+                      (((uintptr_t)mask & 3u) == 0);
+  if (!col_ok)
+    return launch_stencil<OP_JACOBI_RHS, uint8_t>(out, p, rhs, mask, nx, ny, nz, 0.f, 1.f, 0.f,
+                                                  BSP_FLUID, BSP_AIR, s);
+  const int bi = g_sweep_bi > 0 ? g_sweep_bi : pick_bi(nx, ny, nz);
+  dim3 grid((nz / 4 + 31) / 32, (ny + 7) / 8, (nx + bi - 1) / bi);
+  if (nz % 128 == 0)
+    stencil_col_kernel<OP_JACOBI_RHS, uint8_t, true, true><<<grid, 256, 0, s>>>(
+        out, p, rhs, mask, nx, ny, nz, bi, 0.f, 1.f, BSP_FLUID, BSP_AIR);
+  else
+    stencil_col_kernel<OP_JACOBI_RHS, uint8_t, false, true><<<grid, 256, 0, s>>>(
+        out, p, rhs, mask, nx, ny, nz, bi, 0.f, 1.f, BSP_FLUID, BSP_AIR);
   return cudaGetLastError();
 }
 
