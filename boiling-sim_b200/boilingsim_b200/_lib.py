@@ -50,6 +50,9 @@ SIGNATURES = {
     "bsp_enforce_no_slip": (_I, [_P, _P, _P, _P, _I, _I, _I, _P]),
     "bsp_projection_jacobi": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I, _I,
                                    _P, _P]),
+    "bsp_step_projection_jacobi": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I,
+                                        _I, _P, _P]),
+    "bsp_noslip_divergence": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _P]),
     "bsp_spmv": (_I, [_P, _P, _P, _I, _I, _I, _P]),
     "bsp_selftest_div6": (_I, [_P, _P]),
     "bsp_solve_params_default": (None, [_P]),

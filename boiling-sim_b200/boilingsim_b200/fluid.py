@@ -35,6 +35,10 @@ class SolverConfig:
 
     pressure_tol: float = 1e-5
     pressure_max_iter: int = 200
+    # B200 extension, to-tolerance back-ends only: start each solve from the
+    # previous time step's pressure instead of zero (the reference always
+    # zeroes p, fluid.py:628-629).
+    pressure_warm_start: bool = False
 
 
 @dataclass
@@ -196,15 +200,8 @@ def pressure_projection(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, dt:
              ptr(grid.uy), ptr(grid.uz), ptr(mask), nx, ny, nz, dx, float(dt), float(rho),
              n_iter, 0, ptr(ws.max_div), s)
     elif solver.startswith("b200-"):
-        # to-tolerance back-ends: multigrid-preconditioned CG inside FP64
-        # refinement, stopping at ||b - A p|| <= pressure_tol ||b|| (FP64)
-        storage = {"b200-mg": "fp32", "b200-mixed": "fp16", "b200-bf16": "bf16"}[solver]
-        tol_solver = _tol_solver(grid, storage)
         compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, mask, dx)
-        tol_solver.solve(ws.div_u, dx, dt, rho, tol=float(cfg.solver.pressure_tol), p=grid.p,
-                         raise_on_fail=False)
-        subtract_pressure_gradient(grid.ux, grid.uy, grid.uz, grid.p, mask, dx, dt, rho)
-        compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, mask, dx, ws.max_div)
+        _tol_projection(grid, ws, cfg, solver, dt, rho)
     else:
         grid.p.zero_()
         ws.p_tmp.zero_()
@@ -227,3 +224,56 @@ def pressure_projection(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, dt:
         subtract_pressure_gradient(grid.ux, grid.uy, grid.uz, grid.p, mask, dx, dt, rho)
         compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, mask, dx, ws.max_div)
     return float(ws.max_div.item())
+
+
+def _tol_projection(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, solver: str,
+                    dt: float, rho: float) -> None:
+    """Solve, gradient and diagnostic divergence of the to-tolerance back-ends
+    (multigrid-preconditioned CG inside FP64 refinement, stopping at
+    ||b - A p|| <= pressure_tol ||b|| in FP64); ws.div_u holds the divergence."""
+    mask = grid_mask(grid)
+    dx = float(grid.dx)
+    storage = {"b200-mg": "fp32", "b200-mixed": "fp16", "b200-bf16": "bf16"}[solver]
+    tol_solver = _tol_solver(grid, storage)
+    tol_solver.solve(ws.div_u, dx, dt, rho, tol=float(cfg.solver.pressure_tol), p=grid.p,
+                     warm_start=bool(cfg.solver.pressure_warm_start), raise_on_fail=False)
+    subtract_pressure_gradient(grid.ux, grid.uy, grid.uz, grid.p, mask, dx, dt, rho)
+    compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, mask, dx, ws.max_div)
+
+
+def noslip_divergence(div_u, ux, uy, uz, mask, dx, stream=None):
+    """``enforce_no_slip`` then ``compute_divergence`` in one pass (bit-identical)."""
+    nx, ny, nz = div_u.shape
+    call("bsp_noslip_divergence", ptr(div_u), ptr(ux), ptr(uy), ptr(uz), ptr(mask), nx, ny, nz,
+         float(dx), stream_handle(stream))
+
+
+def projection_step(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, dt: float,
+                    rho: float, device: str = "cuda:0") -> float:
+    """Steps 5-7 of a time step (``pipeline.py:605-619``): no-slip, pressure
+    projection, no-slip; returns the projection's max |div u|.
+
+    On the B200 back-ends the first no-slip is fused into the divergence pass
+    and the second is skipped: the gradient subtract writes only faces between
+    two fluid cells, which no-slip leaves alone, so it would change nothing.
+    The reference launchers (``rust-jacobi``, ``cg-rust``) run the three calls
+    as written.  The result equals the reference sequence bit for bit on the
+    Jacobi back-ends.
+    """
+    nx, ny, nz = grid.shape
+    dx = float(grid.dx)
+    mask = grid_mask(grid)
+    solver = _select_pressure_solver()
+    if solver in ("jacobi", "b200-jacobi"):
+        call("bsp_step_projection_jacobi", ptr(grid.p), ptr(ws.p_tmp), ptr(ws.div_u),
+             ptr(grid.ux), ptr(grid.uy), ptr(grid.uz), ptr(mask), nx, ny, nz, dx, float(dt),
+             float(rho), int(cfg.solver.pressure_max_iter), 0, ptr(ws.max_div), stream_handle())
+        return float(ws.max_div.item())
+    if solver.startswith("b200-"):
+        noslip_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, mask, dx)
+        _tol_projection(grid, ws, cfg, solver, dt, rho)
+        return float(ws.max_div.item())
+    enforce_no_slip(grid, device)
+    out = pressure_projection(grid, ws, cfg, dt, rho, device)
+    enforce_no_slip(grid, device)
+    return out

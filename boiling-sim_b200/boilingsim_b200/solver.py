@@ -61,6 +61,7 @@ class TolSolver:
         # workspace at the same address), reuse them afterwards
         self.params.reuse_setup = 0
         self._setup_done = False
+        self.last: SolveResult | None = None  # result of the latest solve
 
     def solve(self, div: torch.Tensor, dx: float, dt: float, rho: float, tol: float = 1e-6,
               p: torch.Tensor | None = None, warm_start: bool = False, inner_tol: float | None = None,
@@ -94,8 +95,9 @@ class TolSolver:
         if code not in (0, 10005) or (raise_on_fail and code != 0):
             _lib.check("bsp_solve_tol", code)
         self._setup_done = True
-        return SolveResult(p, self.x64, code, info.outer_iterations, info.inner_iterations,
-                           info.levels, info.rel_residual)
+        self.last = SolveResult(p, self.x64, code, info.outer_iterations, info.inner_iterations,
+                                info.levels, info.rel_residual)
+        return self.last
 
 
 class BatchSolver:

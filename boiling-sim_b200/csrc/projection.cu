@@ -67,6 +67,49 @@ __global__ void __launch_bounds__(256) divergence_kernel(
   }
 }
 
+// enforce_no_slip (fluid.py:111-165) followed by compute_divergence
+// (fluid.py:201-218) in one pass.  One thread per lattice point (i, j, k) in
+// [0,nx] x [0,ny] x [0,nz]: it zeroes the x-, y- and z-face with its index
+// when that face touches a non-fluid cell or the domain boundary, and, on a
+// fluid cell, computes the divergence from its six faces with the same rule
+// applied to each face (a face is kept only between two fluid cells).  The
+// result equals no-slip then divergence bit for bit: kept faces are read
+// unchanged, zeroed faces contribute exactly 0.
+__global__ void __launch_bounds__(256) noslip_divergence_kernel(
+    float *__restrict__ div, float *__restrict__ ux, float *__restrict__ uy,
+    float *__restrict__ uz, const uint8_t *__restrict__ mask, int nx, int ny, int nz, float dx) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k > nz || j > ny) return;
+  auto fluid = [&](int a, int b, int c) {
+    return a >= 0 && a < nx && b >= 0 && b < ny && c >= 0 && c < nz &&
+           mcls(__ldg(mask + idx3(a, b, c, ny, nz))) == BSP_FLUID;
+  };
+  // faces owned by this lattice point
+  if (j < ny && k < nz && !(fluid(i - 1, j, k) && fluid(i, j, k)))
+    ux[((int64_t)i * ny + j) * nz + k] = 0.0f;
+  if (i < nx && k < nz && !(fluid(i, j - 1, k) && fluid(i, j, k)))
+    uy[((int64_t)i * (ny + 1) + j) * nz + k] = 0.0f;
+  if (i < nx && j < ny && !(fluid(i, j, k - 1) && fluid(i, j, k)))
+    uz[((int64_t)i * ny + j) * (nz + 1) + k] = 0.0f;
+  if (i >= nx || j >= ny || k >= nz) return;
+  const int64_t c = idx3(i, j, k, ny, nz);
+  float v = 0.0f;
+  if (fluid(i, j, k)) {
+    // a face of a fluid cell is kept iff the neighbour across it is fluid
+    const float u1 = fluid(i + 1, j, k) ? ux[((int64_t)(i + 1) * ny + j) * nz + k] : 0.0f;
+    const float u0 = fluid(i - 1, j, k) ? ux[((int64_t)i * ny + j) * nz + k] : 0.0f;
+    const float v1 = fluid(i, j + 1, k) ? uy[((int64_t)i * (ny + 1) + j + 1) * nz + k] : 0.0f;
+    const float v0 = fluid(i, j - 1, k) ? uy[((int64_t)i * (ny + 1) + j) * nz + k] : 0.0f;
+    const float w1 = fluid(i, j, k + 1) ? uz[((int64_t)i * ny + j) * (nz + 1) + k + 1] : 0.0f;
+    const float w0 = fluid(i, j, k - 1) ? uz[((int64_t)i * ny + j) * (nz + 1) + k] : 0.0f;
+    v = __fadd_rn(__fadd_rn(__fdiv_rn(__fsub_rn(u1, u0), dx), __fdiv_rn(__fsub_rn(v1, v0), dx)),
+                  __fdiv_rn(__fsub_rn(w1, w0), dx));
+  }
+  div[c] = v;
+}
+
 // One thread per cell c = (i, j, k): updates the x-face (i, j, k) if i >= 1,
 // the y-face if j >= 1 and the z-face if k >= 1, each only when both cells
 // adjacent to the face are fluid.  u -= ((dt/rho) * dp) / dx.
@@ -187,19 +230,37 @@ extern "C" int bsp_enforce_no_slip(float *ux, float *uy, float *uz, const uint8_
   return (int)cudaGetLastError();
 }
 
-extern "C" int bsp_projection_jacobi(float *p, float *p_tmp, float *div_u, float *ux, float *uy,
-                                     float *uz, const uint8_t *mask, int nx, int ny, int nz,
-                                     float dx, float dt, float rho, int n_iter, int tblock,
-                                     float *max_div_dev, cudaStream_t stream) {
+namespace bsp {
+
+cudaError_t noslip_divergence_impl(float *div, float *ux, float *uy, float *uz,
+                                   const uint8_t *mask, int nx, int ny, int nz, float dx,
+                                   cudaStream_t s) {
+  dim3 block(128, 2);
+  dim3 grid((nz + 1 + 127) / 128, (ny + 2) / 2, nx + 1);
+  ProfScope ps(PROF_PROJ, s);
+  noslip_divergence_kernel<<<grid, block, 0, s>>>(div, ux, uy, uz, mask, nx, ny, nz, dx);
+  return cudaGetLastError();
+}
+
+// The Jacobi projection of fluid.py:612-734; with no_slip it is the
+// no-slip / projection / no-slip sequence of pipeline.py:605-619, where the
+// first no-slip is fused into the divergence and the second is dropped: the
+// gradient subtract only writes faces between two fluid cells, and those are
+// exactly the faces no-slip keeps, so the second no-slip would change nothing.
+static int projection_jacobi(float *p, float *p_tmp, float *div_u, float *ux, float *uy,
+                             float *uz, const uint8_t *mask, int nx, int ny, int nz, float dx,
+                             float dt, float rho, int n_iter, int tblock, float *max_div_dev,
+                             cudaStream_t stream, bool no_slip) {
   if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_OK;
   if (!p || !p_tmp || !div_u || !ux || !uy || !uz || !mask) return BSP_ERR_NULL;
-  if (!dims_ok(nx, ny, nz)) return BSP_ERR_SHAPE;
+  if (!dims_ok(nx + 1, ny, nz)) return BSP_ERR_SHAPE;
   if (p == p_tmp) return BSP_ERR_ALIAS;
   const size_t bytes = sizeof(float) * (size_t)nx * ny * nz;
   cudaError_t e = cudaMemsetAsync(p, 0, bytes, stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(p_tmp, 0, bytes, stream);
   if (e != cudaSuccess) return (int)e;
-  e = divergence_impl(div_u, ux, uy, uz, mask, nx, ny, nz, dx, nullptr, stream);
+  e = no_slip ? noslip_divergence_impl(div_u, ux, uy, uz, mask, nx, ny, nz, dx, stream)
+              : divergence_impl(div_u, ux, uy, uz, mask, nx, ny, nz, dx, nullptr, stream);
   if (e != cudaSuccess) return (int)e;
   // div_u belongs to the projection until the diagnostic divergence below
   // overwrites it, so it holds rho dx^2 div / dt (in place) during the sweeps.
@@ -209,4 +270,32 @@ extern "C" int bsp_projection_jacobi(float *p, float *p_tmp, float *div_u, float
   e = gradient_impl(ux, uy, uz, p, mask, nx, ny, nz, dx, dt, rho, stream);
   if (e != cudaSuccess) return (int)e;
   return (int)divergence_impl(div_u, ux, uy, uz, mask, nx, ny, nz, dx, max_div_dev, stream);
+}
+
+}  // namespace bsp
+
+extern "C" int bsp_projection_jacobi(float *p, float *p_tmp, float *div_u, float *ux, float *uy,
+                                     float *uz, const uint8_t *mask, int nx, int ny, int nz,
+                                     float dx, float dt, float rho, int n_iter, int tblock,
+                                     float *max_div_dev, cudaStream_t stream) {
+  return projection_jacobi(p, p_tmp, div_u, ux, uy, uz, mask, nx, ny, nz, dx, dt, rho, n_iter,
+                           tblock, max_div_dev, stream, false);
+}
+
+extern "C" int bsp_step_projection_jacobi(float *p, float *p_tmp, float *div_u, float *ux,
+                                          float *uy, float *uz, const uint8_t *mask, int nx,
+                                          int ny, int nz, float dx, float dt, float rho,
+                                          int n_iter, int tblock, float *max_div_dev,
+                                          cudaStream_t stream) {
+  return projection_jacobi(p, p_tmp, div_u, ux, uy, uz, mask, nx, ny, nz, dx, dt, rho, n_iter,
+                           tblock, max_div_dev, stream, true);
+}
+
+extern "C" int bsp_noslip_divergence(float *div_u, float *ux, float *uy, float *uz,
+                                     const uint8_t *mask, int nx, int ny, int nz, float dx,
+                                     cudaStream_t stream) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_OK;
+  if (!div_u || !ux || !uy || !uz || !mask) return BSP_ERR_NULL;
+  if (!dims_ok(nx + 1, ny, nz)) return BSP_ERR_SHAPE;
+  return (int)noslip_divergence_impl(div_u, ux, uy, uz, mask, nx, ny, nz, dx, stream);
 }

@@ -202,6 +202,23 @@ int bsp_projection_jacobi(float *p, float *p_tmp, float *div_u, float *ux, float
                           float dt, float rho, int n_iter, int tblock, float *max_div_dev,
                           cudaStream_t stream);
 
+/* enforce_no_slip then compute_divergence (fluid.py:111-165, 201-218) in one
+ * pass: zeroes every face that touches a non-fluid cell or the domain
+ * boundary and writes the divergence of the result.  Bit-identical to the
+ * two calls in sequence. */
+int bsp_noslip_divergence(float *div_u, float *ux, float *uy, float *uz, const uint8_t *mask,
+                          int nx, int ny, int nz, float dx, cudaStream_t stream);
+
+/* The projection part of a time step, pipeline.py:605-619: no-slip,
+ * bsp_projection_jacobi, no-slip.  The first no-slip is fused into the
+ * divergence; the second is a no-op (the gradient subtract writes only faces
+ * between two fluid cells) and is not launched.  Same arguments and results
+ * as the three reference calls in sequence. */
+int bsp_step_projection_jacobi(float *p, float *p_tmp, float *div_u, float *ux, float *uy,
+                               float *uz, const uint8_t *mask, int nx, int ny, int nz,
+                               float dx, float dt, float rho, int n_iter, int tblock,
+                               float *max_div_dev, cudaStream_t stream);
+
 /* Ap = (6I - S) p on the uint8 mask (laplacian_spmv.cu:62-143). */
 int bsp_spmv(float *Ap, const float *p, const uint8_t *mask, int nx, int ny, int nz,
              cudaStream_t stream);
