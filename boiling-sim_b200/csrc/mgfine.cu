@@ -1,21 +1,27 @@
 // mgfine.cu -- fine-level (level 0) kernels of the to-tolerance solver on the
 // column layout of the sweep kernel.
 //
-// One generic driver, fine_col_kernel<Op>: a CTA is 8 warps; warp w owns fine
-// row j = 8*blockIdx.y + w and 128 consecutive k cells (4 per lane) and marches
-// i over an even-length chunk.  The Op supplies the stencil operand of a cell
-// (ps for A*ps; OMEGA r / D for the smoothers, plus the coarse correction for
-// the prolongation) and consumes, per cell, the centre operand and the
-// neighbour sum s = l + r + d + u + b + f under the boundary rule (fluid ->
-// operand, air -> 0, solid -> centre operand).  Operand planes i-1, i, i+1 and
-// their mask words stay in registers; rows j +- 1 are formed from L1-resident
-// loads; k +- 1 arrive by warp shuffles; neighbour selection is branch-free
-// (sel_nbr).
+// One generic driver, fine_tile_kernel<Op>: a CTA is 8 output warps plus two
+// halo warps; output warp w owns fine row j = 8*blockIdx.y + w and 128
+// consecutive k cells (4 per lane) and marches i over an even-length chunk.
+// The Op supplies the stencil operand of a cell (ps for A*ps; OMEGA r / D for
+// the smoothers, plus the coarse correction for the prolongation) and
+// consumes, per cell, the centre operand and the neighbour sum
+// s = l + r + d + u + b + f under the boundary rule (fluid -> operand, air ->
+// 0, solid -> centre operand).  Each operand is computed once per plane by the
+// warp owning its row (the halo warps own rows j0-1 and j0+8) and shared
+// through a double-buffered plane in shared memory for the j +- 1 neighbours;
+// planes i-1, i, i+1 stay in registers; k +- 1 arrive by warp shuffles.
 //
 // Requirements (checked by the caller; otherwise the row kernels of solver.cu
 // run): nz % 4 == 0 and 16-byte aligned level-0 fields.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+#include <type_traits>
 
 #include "bsp_common.cuh"
 #include "solver.cuh"
@@ -101,7 +107,7 @@ __device__ __forceinline__ float wcalc(uint32_t ns) {
   const float d = 6.0f - (float)ns;
   return d > 0.0f ? __fdividef(FOMEGA, d) : 0.0f;
 }
-// The 8 possible weights, filled once per CTA by fine_col_kernel: a lookup is
+// The 8 possible weights, filled once per CTA by fine_tile_kernel: a lookup is
 // one bit-field extract and one shared load.
 __shared__ float s_wtab[8];
 __device__ __forceinline__ float wdinv_ns(uint32_t ns) { return s_wtab[ns & 7u]; }
@@ -110,24 +116,31 @@ __device__ __forceinline__ uint32_t mload4(const uint8_t *m, int64_t o) {
   return __ldg(reinterpret_cast<const uint32_t *>(m + o));
 }
 
+__device__ __forceinline__ int block_linear() {
+  return blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+}
+
+template <int NW>
 __device__ __forceinline__ void block_partial(double v, double *partials, double *sh) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
   __syncthreads();
   if (threadIdx.x == 0) {
     double t = 0.0;
-    for (int w = 0; w < 8; ++w) t += sh[w];
-    partials[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = t;
+    for (int w = 0; w < NW; ++w) t += sh[w];
+    partials[block_linear()] = t;
   }
 }
 
 // ---- operations -------------------------------------------------------------------------
-// Interface: init(st), val4(i,j,k,o,mw), val1(i,j,k,o,mbyte), emit(...), finish(sh).
+// Interface: init(st); val4(i,j,k,o,mw) / val1(i,j,k,o,mbyte): the stencil
+// operand of 4 cells / 1 cell (exactly 0 on non-fluid cells); emit(...) per
+// output cell group; after_step(...) after the CTA barrier that ends plane i;
+// finish<NW>(sh) once at the end (all threads of the CTA).
 
 // ps = z + beta ps_prev (ps = z on the first iteration); Ap = 6 ps - s; partial ps.Ap
 template <class T>
 struct PsApOp {
-  static constexpr bool SYNC = false;
   const uint8_t *mask;
   const T *z, *prev;
   T *cur, *Ap;
@@ -152,9 +165,8 @@ struct PsApOp {
     const float zz = ld1s(z, o);
     return first ? zz : rt(fmaf(beta, ld1s(prev, o), zz), cur);
   }
-  __device__ void emit(int, int, int, int64_t o, bool act, uint32_t mc, const float4 &v,
+  __device__ void emit(int, int, int, int64_t o, uint32_t mc, const float4 &v,
                        const float (&s)[4], float2 *) {
-    if (!act) return;
     float ap[4], vv[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
@@ -166,25 +178,31 @@ struct PsApOp {
     st4s(cur, o, make_float4(vv[0], vv[1], vv[2], vv[3]));
     st4s(Ap, o, make_float4(ap[0], ap[1], ap[2], ap[3]));
   }
-  __device__ void finish(double *sh) { block_partial(acc, partials, sh); }
+  __device__ void after_step(int, int, int, bool, float2 *) {}
+  template <int NW>
+  __device__ void finish(double *sh) { block_partial<NW>(acc, partials, sh); }
+  __device__ void skip() const { partials[block_linear()] = 0.0; }
 };
 
-// e^ = OMEGA r / D + e1[parent];  z = e^ + OMEGA (r - (6 e^ - s)) / D;  partial r.z
+// e^ = OMEGA r / D + alpha e1[parent];  z = e^ + OMEGA (r - (6 e^ - s)) / D;
+// partial r.z
 template <class T>
 struct UpOp {
-  static constexpr bool SYNC = false;
   const uint8_t *mask;
   const T *r, *e1;
   T *z;
   double *partials;
   int ny1, nz1;
+  float alpha;
   double acc;
 
   __device__ void init(const SolverState *) { acc = 0.0; }
   __device__ float4 val4(int i, int j, int k, int64_t o, uint32_t mw) const {
     const float4 rr = ld4s(r, o);
     const int64_t P = ((int64_t)(i >> 1) * ny1 + (j >> 1)) * nz1 + (k >> 1);
-    const float2 ec = ld2s(e1, P);
+    float2 ec = ld2s(e1, P);
+    ec.x *= alpha;
+    ec.y *= alpha;
     // the coarse correction is not zero on non-fluid fine cells: mask it
     auto fl = [&](float v, int q) {
       return __uint_as_float(__float_as_uint(v) & fluid_word(mw, q));
@@ -194,11 +212,10 @@ struct UpOp {
   }
   __device__ float val1(int i, int j, int k, int64_t o, uint32_t mb) const {
     const int64_t P = ((int64_t)(i >> 1) * ny1 + (j >> 1)) * nz1 + (k >> 1);
-    return (mb & BSP_MFLUID) ? fmaf(ld1s(r, o), wdinv_ns(mb & 7u), ld1s(e1, P)) : 0.0f;
+    return (mb & BSP_MFLUID) ? fmaf(ld1s(r, o), wdinv_ns(mb & 7u), alpha * ld1s(e1, P)) : 0.0f;
   }
-  __device__ void emit(int, int, int, int64_t o, bool act, uint32_t mc, const float4 &v,
+  __device__ void emit(int, int, int, int64_t o, uint32_t mc, const float4 &v,
                        const float (&s)[4], float2 *) {
-    if (!act) return;
     const float4 rr = ld4s(r, o);
     float zz[4];
 #pragma unroll
@@ -210,15 +227,19 @@ struct UpOp {
     }
     st4s(z, o, make_float4(zz[0], zz[1], zz[2], zz[3]));
   }
-  __device__ void finish(double *sh) { block_partial(acc, partials, sh); }
+  __device__ void after_step(int, int, int, bool, float2 *) {}
+  template <int NW>
+  __device__ void finish(double *sh) { block_partial<NW>(acc, partials, sh); }
+  __device__ void skip() const { partials[block_linear()] = 0.0; }
 };
 
 // e = OMEGA r / D (pre-smoothing from zero); the residual r - (6 e - s) of the
 // 2x2x2 children of each coarse cell is summed, halved, into r1 (0 on coarse
-// cells that are not fluid).  Rows j (even) and j+1 meet in shared memory.
+// cells that are not fluid).  A pair of planes is summed in registers; rows j
+// (even warp) and j+1 (odd warp) meet in shared memory across the barrier that
+// ends the second plane of the pair.
 template <class T>
 struct DownOp {
-  static constexpr bool SYNC = true;
   const uint8_t *mask, *mask1;
   const T *r;
   T *r1;
@@ -234,28 +255,32 @@ struct DownOp {
   __device__ float val1(int, int, int, int64_t o, uint32_t mb) const {
     return ld1s(r, o) * wdinv_ns(mb & 7u);
   }
-  // Every warp of the CTA calls this for every plane (it may __syncthreads).
-  __device__ void emit(int i, int j, int k, int64_t o, bool act, uint32_t mc, const float4 &v,
+  __device__ bool pair_end(int i) const { return (i & 1) || i + 1 == nx; }
+  __device__ void emit(int i, int, int, int64_t o, uint32_t mc, const float4 &v,
                        const float (&s)[4], float2 *xch) {
-    if (act) {
-      const float4 rr = ld4s(r, o);
-      float res[4];
+    const float4 rr = ld4s(r, o);
+    float res[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const float rq = q4(rr, q) - (6.0f * q4(v, q) - s[q]);
-        res[q] = __uint_as_float(__float_as_uint(rq) & fluid_word(mc, q));
-      }
-      acc.x += res[0] + res[1];
-      acc.y += res[2] + res[3];
+    for (int q = 0; q < 4; ++q) {
+      const float rq = q4(rr, q) - (6.0f * q4(v, q) - s[q]);
+      res[q] = __uint_as_float(__float_as_uint(rq) & fluid_word(mc, q));
     }
-    if (!((i & 1) || i + 1 == nx)) return;  // uniform over the CTA
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp & 1) xch[(warp >> 1) * 32 + lane] = acc;
-    __syncthreads();
-    if (!(warp & 1) && act) {
+    acc.x += res[0] + res[1];
+    acc.y += res[2] + res[3];
+    const int warp = threadIdx.x >> 5;
+    if (pair_end(i) && (warp & 1)) {
+      xch[(warp >> 1) * 32 + (threadIdx.x & 31)] = acc;
+      acc = make_float2(0.f, 0.f);
+    }
+  }
+  // Called by the output warps (active or not) after the barrier ending plane i.
+  __device__ void after_step(int i, int j, int k, bool act, float2 *xch) {
+    const int warp = threadIdx.x >> 5;
+    if (!pair_end(i) || (warp & 1)) return;
+    if (act) {
       float2 t = acc;
       if (j + 1 < ny) {
-        const float2 o2 = xch[(warp >> 1) * 32 + lane];
+        const float2 o2 = xch[(warp >> 1) * 32 + (threadIdx.x & 31)];
         t.x += o2.x;
         t.y += o2.y;
       }
@@ -264,104 +289,553 @@ struct DownOp {
       st2s(r1, C, make_float2((m2 & BSP_MFLUID) ? 0.5f * t.x : 0.0f,
                               ((m2 >> 8) & BSP_MFLUID) ? 0.5f * t.y : 0.0f));
     }
-    __syncthreads();
     acc = make_float2(0.f, 0.f);
   }
+  template <int NW>
   __device__ void finish(double *) {}
+  __device__ void skip() const {}
 };
 
-// ---- generic driver -------------------------------------------------------------------
+// ---- tile driver ------------------------------------------------------------------------
+// A CTA owns ROWS consecutive j rows (output warps 0..ROWS-1, one row each, 128
+// k cells: float4 per lane) plus two halo warps for rows j0-1 and j0+ROWS, and
+// marches i over an even chunk [i0, i1).  Every operand value is computed once
+// per plane by the warp that owns its row and published in a double-buffered
+// shared-memory plane; rows j +- 1 are read back from there, planes i +- 1 stay
+// in registers, k +- 1 arrive by shuffles (lanes 0 and 31 fetch the row's k
+// halo together, in one branch).  One CTA barrier per plane.
+constexpr int TILE_ROWS = 8;
+constexpr int TILE_WARPS = TILE_ROWS + 2;
+constexpr int TILE_THREADS = TILE_WARPS * 32;
+
 template <class Op>
-__global__ void __launch_bounds__(256) fine_col_kernel(Op op, int nx, int ny, int nz, int bi,
-                                                       const SolverState *st) {
+__global__ void __launch_bounds__(TILE_THREADS, 4) fine_tile_kernel(Op op, int nx, int ny, int nz,
+                                                                 int bi, const uint8_t *tiles,
+                                                                 const SolverState *st) {
   if (st->inner_done) return;  // uniform: the whole grid returns
-  __shared__ double sh[8];
-  __shared__ float2 xch[4 * 32];
+  if (tiles && !tiles[block_linear()]) {
+    if (threadIdx.x == 0) op.skip();
+    return;
+  }
+  __shared__ double sh[TILE_WARPS];
+  __shared__ float2 xch[(TILE_ROWS / 2) * 32];
+  __shared__ float4 plane_buf[2][TILE_ROWS + 2][32];
   if (threadIdx.x < 8) s_wtab[threadIdx.x] = wcalc(threadIdx.x);
   __syncthreads();
   op.init(st);
   const int lane = threadIdx.x & 31;
-  const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
+  const int warp = threadIdx.x >> 5;
+  const int j0 = blockIdx.y * TILE_ROWS;
+  // row slot in plane_buf: 0 = j0-1, 1..ROWS = output rows, ROWS+1 = j0+ROWS
+  const int slot = warp < TILE_ROWS ? warp + 1 : (warp == TILE_ROWS ? 0 : TILE_ROWS + 1);
+  const int j = j0 + slot - 1;
   const int k = (blockIdx.x * 32 + lane) * 4;
-  const bool act = j < ny && k < nz;
+  const bool act = j >= 0 && j < ny && k < nz;
+  const bool out = warp < TILE_ROWS;
   const int i0 = blockIdx.z * bi;
   const int i1 = min(i0 + bi, nx);
   const int64_t plane = (int64_t)ny * nz;
-  const bool has_jm = j > 0, has_jp = j + 1 < ny;
   const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
   const uint8_t *mask = op.mask;
   int64_t o = act ? (int64_t)i0 * plane + (int64_t)j * nz + k : 0;
   float4 vm = z4, vc = z4;
-  uint32_t mm = 0u, mc = 0u;
-  if (act && i0 > 0) {
-    mm = mload4(mask, o - plane);
-    vm = op.val4(i0 - 1, j, k, o - plane, mm);
-  }
+  uint32_t mc = 0u;
   if (act) {
     mc = mload4(mask, o);
     vc = op.val4(i0, j, k, o, mc);
+    if (out && i0 > 0) vm = op.val4(i0 - 1, j, k, o - plane, mload4(mask, o - plane));
   }
+  plane_buf[i0 & 1][slot][lane] = vc;
+  __syncthreads();
   for (int i = i0; i < i1; ++i) {
-    float4 vn = z4, vjm = z4, vjp = z4;
-    uint32_t mn = 0u, mjm = 0u, mjp = 0u;
-    if (act) {
-      if (i + 1 < nx) {
-        mn = mload4(mask, o + plane);
-        vn = op.val4(i + 1, j, k, o + plane, mn);
-      }
-      if (has_jm) {
-        mjm = mload4(mask, o - nz);
-        vjm = op.val4(i, j - 1, k, o - nz, mjm);
-      }
-      if (has_jp) {
-        mjp = mload4(mask, o + nz);
-        vjp = op.val4(i, j + 1, k, o + nz, mjp);
-      }
+    float4 vn = z4;
+    uint32_t mn = 0u;
+    if (act && i + 1 < nx) {
+      mn = mload4(mask, o + plane);
+      vn = op.val4(i + 1, j, k, o + plane, mn);
     }
-    float vkm = __shfl_up_sync(0xffffffffu, vc.w, 1);
-    uint32_t mkm = __shfl_up_sync(0xffffffffu, mc, 1);
-    float vkp = __shfl_down_sync(0xffffffffu, vc.x, 1);
-    uint32_t mkp = __shfl_down_sync(0xffffffffu, mc, 1);
-    if (lane == 0) {
-      vkm = 0.0f;
-      mkm = 0u;
-      if (act && k > 0) {
-        const uint32_t mbyte = __ldg(mask + o - 1);
-        mkm = mbyte << 24;
-        vkm = op.val1(i, j, k - 1, o - 1, mbyte);
+    plane_buf[(i + 1) & 1][slot][lane] = vn;
+    if (out) {
+      const float4 vjm = plane_buf[i & 1][slot - 1][lane];
+      const float4 vjp = plane_buf[i & 1][slot + 1][lane];
+      float vkm = __shfl_up_sync(0xffffffffu, vc.w, 1);
+      float vkp = __shfl_down_sync(0xffffffffu, vc.x, 1);
+      // k halo of the row: k0 - 1 for lane 0, k0 + 128 for lane 31
+      const int kh = lane == 0 ? k - 1 : k + 4;
+      float vh = 0.0f;
+      if (act && (lane == 0 || lane == 31) && kh >= 0 && kh < nz) {
+        const int64_t oh = o + (kh - k);
+        vh = op.val1(i, j, kh, oh, __ldg(mask + oh));
       }
-    }
-    if (lane == 31) {
-      vkp = 0.0f;
-      mkp = 0u;
-      if (act && k + 4 < nz) {
-        const uint32_t mbyte = __ldg(mask + o + 4);
-        mkp = mbyte;
-        vkp = op.val1(i, j, k + 4, o + 4, mbyte);
-      }
-    }
-    // Every operand is exactly 0 on non-fluid cells and outside the grid, so the
-    // boundary rule (fluid -> operand, air -> 0, solid -> centre operand) is
-    // the plain sum of the six neighbours plus n_solid(centre) x centre.
-    (void)mkm;
-    (void)mkp;
-    const float4 vb = make_float4(vkm, vc.x, vc.y, vc.z);
-    const float4 vf = make_float4(vc.y, vc.z, vc.w, vkp);
-    float s[4];
+      if (lane == 0) vkm = vh;
+      if (lane == 31) vkp = vh;
+      // Every operand is exactly 0 on non-fluid cells and outside the grid, so
+      // the boundary rule (fluid -> operand, air -> 0, solid -> centre operand)
+      // is the plain sum of the six neighbours plus n_solid(centre) x centre.
+      const float4 vb = make_float4(vkm, vc.x, vc.y, vc.z);
+      const float4 vf = make_float4(vc.y, vc.z, vc.w, vkp);
+      float s[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const float ns = (float)((mc >> (8 * q)) & 7u);
-      s[q] = fmaf(ns, q4(vc, q),
-                  ((q4(vm, q) + q4(vn, q)) + (q4(vjm, q) + q4(vjp, q))) + (q4(vb, q) + q4(vf, q)));
+      for (int q = 0; q < 4; ++q) {
+        const float ns = (float)((mc >> (8 * q)) & 7u);
+        s[q] = fmaf(ns, q4(vc, q),
+                    ((q4(vm, q) + q4(vn, q)) + (q4(vjm, q) + q4(vjp, q))) +
+                        (q4(vb, q) + q4(vf, q)));
+      }
+      if (act) op.emit(i, j, k, o, mc, vc, s, xch);
     }
-    op.emit(i, j, k, o, act, mc, vc, s, xch);
+    __syncthreads();
+    if (out) op.after_step(i, j, k, act, xch);
     vm = vc;
-    mm = mc;
     vc = vn;
     mc = mn;
     if (act) o += plane;
   }
-  op.finish(sh);
+  op.template finish<TILE_WARPS>(sh);
+}
+
+// ---- TMA-fed tile driver ----------------------------------------------------------------
+// Same CTA shape and arithmetic as fine_tile_kernel, but the raw inputs of a
+// plane (fine operand sources, the mask, the coarse correction) arrive as TMA
+// tiles in a ring of STAGES shared-memory stages, issued STAGES-1 planes ahead
+// by one thread: the bytes in flight no longer depend on how many warps wait.
+// A tile covers rows j0-1 .. j0+8 and k0-PAD .. k0+127+PAD, so the j and k
+// halos (and every cell outside the grid, zero-filled by the TMA unit) come
+// with it; no global load is left on the plane loop but the stores.
+//
+// Stage layout (bytes): fine tensors A[, B] of T: 10 rows x (128 + 2 PAD)
+// elements, PAD = 16 / sizeof(T); mask: 10 rows x 160 bytes (PAD 16); coarse
+// tensor C of T: 6 rows x (64 + 2 PAD) elements.  All row strides are
+// multiples of 16 bytes.
+int fine_bi(int nx, int ny, int nz);
+dim3 fine_grid(int nx, int ny, int nz);
+
+constexpr int TMA_STAGES = 4;
+constexpr int TMA_ROWS = TILE_ROWS + 2;
+constexpr int MASK_W = 160;
+constexpr int MASK_PAD = 16;
+
+template <class T>
+struct TmaGeom {
+  static constexpr int PAD = 16 / (int)sizeof(T);
+  static constexpr int FW = 128 + 2 * PAD;        // fine row width (elements)
+  static constexpr int CW = 64 + 2 * PAD;         // coarse row width (elements)
+  static constexpr int CROWS = TILE_ROWS / 2 + 2;  // coarse rows j0/2-1 .. j0/2+4
+  static constexpr int FBYTES = TMA_ROWS * FW * (int)sizeof(T);
+  static constexpr int MBYTES = TMA_ROWS * MASK_W;
+  static constexpr int CBYTES = CROWS * CW * (int)sizeof(T);
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+// Bounded wait on phase `parity` of an mbarrier: false after ~2^20 polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  for (int it = 0; it < (1 << 20); ++it) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+// 3-D tiled TMA load (no multicast) completing on `bar`.
+__device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *map, int x, int y, int z,
+                                          uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Tensor maps of one launch.  a, b: fine tensors of T; m: mask; c: coarse T.
+struct TmaMaps {
+  CUtensorMap a, b, m, c;
+};
+
+// Operand sources read from a stage.  rr: tile row 0..9 (j = j0 - 1 + rr);
+// kl: k - k0 (-1 .. 128).
+template <class T>
+struct StageView {
+  const T *a, *b, *c;
+  const uint8_t *m;
+  __device__ uint32_t mask4(int rr, int lane) const {
+    return *reinterpret_cast<const uint32_t *>(m + rr * MASK_W + MASK_PAD + lane * 4);
+  }
+  __device__ uint32_t mask1(int rr, int kl) const { return m[rr * MASK_W + MASK_PAD + kl]; }
+  __device__ int fo(int rr, int kl) const { return rr * TmaGeom<T>::FW + TmaGeom<T>::PAD + kl; }
+  // coarse parent of fine (row rr, kl): coarse row (j >> 1) - (j0/2 - 1) = (rr + 1) >> 1
+  __device__ int co(int rr, int kl) const {
+    return ((rr + 1) >> 1) * TmaGeom<T>::CW + TmaGeom<T>::PAD + (kl >> 1);
+  }
+};
+
+template <class T>
+struct TPsAp {
+  static constexpr bool HAS_B = true, HAS_C = false;
+  T *cur, *Ap;
+  double *partials;
+  float beta;
+  bool first;
+  double acc;
+  __device__ void init(const SolverState *st) {
+    first = st->inner_it == 0;
+    beta = (float)st->beta;
+    acc = 0.0;
+  }
+  __device__ float4 val4(const StageView<T> &v, int rr, int lane, uint32_t) const {
+    const float4 zz = ld4s(v.a, v.fo(rr, lane * 4));
+    if (first) return zz;
+    const float4 pp = ld4s(v.b, v.fo(rr, lane * 4));
+    return make_float4(rt(fmaf(beta, pp.x, zz.x), cur), rt(fmaf(beta, pp.y, zz.y), cur),
+                       rt(fmaf(beta, pp.z, zz.z), cur), rt(fmaf(beta, pp.w, zz.w), cur));
+  }
+  __device__ float val1(const StageView<T> &v, int rr, int kl) const {
+    const float zz = ld1s(v.a, v.fo(rr, kl));
+    return first ? zz : rt(fmaf(beta, ld1s(v.b, v.fo(rr, kl)), zz), cur);
+  }
+  __device__ void emit(const StageView<T> &, int, int, int, int, int64_t o, uint32_t mc,
+                       const float4 &v, const float (&s)[4], float2 *) {
+    float ap[4], vv[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t fm = fluid_word(mc, q);
+      vv[q] = __uint_as_float(__float_as_uint(q4(v, q)) & fm);
+      ap[q] = rt(__uint_as_float(__float_as_uint(fmaf(6.0f, q4(v, q), -s[q])) & fm), cur);
+      acc += (double)vv[q] * (double)ap[q];
+    }
+    st4s(cur, o, make_float4(vv[0], vv[1], vv[2], vv[3]));
+    st4s(Ap, o, make_float4(ap[0], ap[1], ap[2], ap[3]));
+  }
+  __device__ void after_step(int, int, int, bool, float2 *) {}
+  template <int NW>
+  __device__ void finish(double *sh) { block_partial<NW>(acc, partials, sh); }
+  __device__ void skip() const { partials[block_linear()] = 0.0; }
+};
+
+template <class T>
+struct TUp {
+  static constexpr bool HAS_B = false, HAS_C = true;
+  T *z;
+  double *partials;
+  float alpha;
+  double acc;
+  __device__ void init(const SolverState *) { acc = 0.0; }
+  __device__ float4 val4(const StageView<T> &v, int rr, int lane, uint32_t mw) const {
+    const float4 r4 = ld4s(v.a, v.fo(rr, lane * 4));
+    float2 ec = ld2s(v.c, v.co(rr, lane * 4));
+    ec.x *= alpha;
+    ec.y *= alpha;
+    auto fl = [&](float x, int q) {
+      return __uint_as_float(__float_as_uint(x) & fluid_word(mw, q));
+    };
+    return make_float4(fl(fmaf(r4.x, wdq(mw, 0), ec.x), 0), fl(fmaf(r4.y, wdq(mw, 1), ec.x), 1),
+                       fl(fmaf(r4.z, wdq(mw, 2), ec.y), 2), fl(fmaf(r4.w, wdq(mw, 3), ec.y), 3));
+  }
+  __device__ float val1(const StageView<T> &v, int rr, int kl) const {
+    const uint32_t mb = v.mask1(rr, kl);
+    return (mb & BSP_MFLUID)
+               ? fmaf(ld1s(v.a, v.fo(rr, kl)), wdinv_ns(mb & 7u), alpha * ld1s(v.c, v.co(rr, kl)))
+               : 0.0f;
+  }
+  __device__ void emit(const StageView<T> &v, int rr, int lane, int, int, int64_t o,
+                       uint32_t mc, const float4 &e4, const float (&s)[4], float2 *) {
+    const float4 r4 = ld4s(v.a, v.fo(rr, lane * 4));
+    float zz[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float e = q4(e4, q);
+      const float zq = fmaf(q4(r4, q) - (6.0f * e - s[q]), wdq(mc, q), e);
+      zz[q] = rt(__uint_as_float(__float_as_uint(zq) & fluid_word(mc, q)), z);
+      acc += (double)q4(r4, q) * (double)zz[q];
+    }
+    st4s(z, o, make_float4(zz[0], zz[1], zz[2], zz[3]));
+  }
+  __device__ void after_step(int, int, int, bool, float2 *) {}
+  template <int NW>
+  __device__ void finish(double *sh) { block_partial<NW>(acc, partials, sh); }
+  __device__ void skip() const { partials[block_linear()] = 0.0; }
+};
+
+template <class T>
+struct TDown {
+  static constexpr bool HAS_B = false, HAS_C = false;
+  const uint8_t *mask1;
+  T *r1;
+  int nx, ny, ny1, nz1;
+  float2 acc;
+  __device__ void init(const SolverState *) { acc = make_float2(0.f, 0.f); }
+  __device__ float4 val4(const StageView<T> &v, int rr, int lane, uint32_t mw) const {
+    const float4 r4 = ld4s(v.a, v.fo(rr, lane * 4));
+    return make_float4(r4.x * wdq(mw, 0), r4.y * wdq(mw, 1), r4.z * wdq(mw, 2),
+                       r4.w * wdq(mw, 3));
+  }
+  __device__ float val1(const StageView<T> &v, int rr, int kl) const {
+    return ld1s(v.a, v.fo(rr, kl)) * wdinv_ns(v.mask1(rr, kl) & 7u);
+  }
+  __device__ bool pair_end(int i) const { return (i & 1) || i + 1 == nx; }
+  __device__ void emit(const StageView<T> &v, int rr, int lane, int i, int, int64_t,
+                       uint32_t mc, const float4 &e4, const float (&s)[4], float2 *xch) {
+    const float4 r4 = ld4s(v.a, v.fo(rr, lane * 4));
+    float res[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float rq = q4(r4, q) - (6.0f * q4(e4, q) - s[q]);
+      res[q] = __uint_as_float(__float_as_uint(rq) & fluid_word(mc, q));
+    }
+    acc.x += res[0] + res[1];
+    acc.y += res[2] + res[3];
+    const int warp = threadIdx.x >> 5;
+    if (pair_end(i) && (warp & 1)) {
+      xch[(warp >> 1) * 32 + lane] = acc;
+      acc = make_float2(0.f, 0.f);
+    }
+  }
+  __device__ void after_step(int i, int j, int k, bool act, float2 *xch) {
+    const int warp = threadIdx.x >> 5;
+    if (!pair_end(i) || (warp & 1)) return;
+    if (act) {
+      float2 t = acc;
+      if (j + 1 < ny) {
+        const float2 o2 = xch[(warp >> 1) * 32 + (threadIdx.x & 31)];
+        t.x += o2.x;
+        t.y += o2.y;
+      }
+      const int64_t C = ((int64_t)(i >> 1) * ny1 + (j >> 1)) * nz1 + (k >> 1);
+      const uint32_t m2 = __ldg(reinterpret_cast<const uint16_t *>(mask1 + C));
+      st2s(r1, C, make_float2((m2 & BSP_MFLUID) ? 0.5f * t.x : 0.0f,
+                              ((m2 >> 8) & BSP_MFLUID) ? 0.5f * t.y : 0.0f));
+    }
+    acc = make_float2(0.f, 0.f);
+  }
+  template <int NW>
+  __device__ void finish(double *) {}
+  __device__ void skip() const {}
+};
+
+constexpr int align128(int b) { return (b + 127) / 128 * 128; }
+
+// Every TMA destination starts on a 128-byte boundary.
+template <class T, class Op>
+struct TmaSmem {
+  static constexpr int FB = TmaGeom<T>::FBYTES, MB = TmaGeom<T>::MBYTES,
+                       CB = TmaGeom<T>::CBYTES;
+  static constexpr int OFF_B = align128(FB);
+  static constexpr int OFF_M = OFF_B + (Op::HAS_B ? align128(FB) : 0);
+  static constexpr int OFF_C = OFF_M + align128(MB);
+  static constexpr int STAGE = OFF_C + (Op::HAS_C ? align128(CB) : 0);
+  static constexpr uint32_t TX = (uint32_t)(FB + (Op::HAS_B ? FB : 0) + MB + (Op::HAS_C ? CB : 0));
+  static constexpr int RING = STAGE * TMA_STAGES;
+  // ring | plane_buf (2 x 10 x 32 float4) | mbarriers
+  static constexpr int OFF_PLANE = RING;
+  static constexpr int OFF_BAR = RING + 2 * TMA_ROWS * 32 * 16;
+  static constexpr int TOTAL = OFF_BAR + TMA_STAGES * 8;
+};
+
+template <class T, class Op>
+__global__ void __launch_bounds__(TILE_THREADS, 4) fine_tma_kernel(
+    Op op, const __grid_constant__ TmaMaps maps, int nx, int ny, int nz, int bi,
+    const uint8_t *tiles, const SolverState *st) {
+  if (st->inner_done) return;  // uniform: the whole grid returns
+  if (tiles && !tiles[block_linear()]) {
+    if (threadIdx.x == 0) op.skip();
+    return;
+  }
+  using L = TmaSmem<T, Op>;
+  extern __shared__ __align__(128) unsigned char dsm[];
+  __shared__ double sh[TILE_WARPS];
+  __shared__ float2 xch[(TILE_ROWS / 2) * 32];
+  float4(*plane_buf)[TMA_ROWS][32] = reinterpret_cast<float4(*)[TMA_ROWS][32]>(dsm + L::OFF_PLANE);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(dsm + L::OFF_BAR);
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const bool producer = threadIdx.x == TILE_ROWS * 32;  // lane 0 of the first halo warp
+  const int j0 = blockIdx.y * TILE_ROWS;
+  const int k0 = blockIdx.x * 128;
+  const int i0 = blockIdx.z * bi;
+  const int i1 = min(i0 + bi, nx);
+  const int pbase = i0 - 1;  // first plane of the ring
+  constexpr int PAD = TmaGeom<T>::PAD;
+  if (threadIdx.x < 8) s_wtab[threadIdx.x] = wcalc(threadIdx.x);
+  if (producer) {
+    for (int q = 0; q < TMA_STAGES; ++q) mbar_init(&bars[q], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  auto issue = [&](int p) {  // producer only: plane p into its stage
+    const int q = (p - pbase) % TMA_STAGES;
+    unsigned char *base = dsm + q * L::STAGE;
+    mbar_expect_tx(&bars[q], L::TX);
+    tma_load3(base, &maps.a, k0 - PAD, j0 - 1, p, &bars[q]);
+    if (Op::HAS_B) tma_load3(base + L::OFF_B, &maps.b, k0 - PAD, j0 - 1, p, &bars[q]);
+    tma_load3(base + L::OFF_M, &maps.m, k0 - MASK_PAD, j0 - 1, p, &bars[q]);
+    if (Op::HAS_C)
+      tma_load3(base + L::OFF_C, &maps.c, k0 / 2 - PAD, j0 / 2 - 1, p >> 1, &bars[q]);
+  };
+  auto view = [&](int p) {
+    const unsigned char *base = dsm + ((p - pbase) % TMA_STAGES) * L::STAGE;
+    StageView<T> v;
+    v.a = reinterpret_cast<const T *>(base);
+    v.b = reinterpret_cast<const T *>(base + L::OFF_B);
+    v.m = base + L::OFF_M;
+    v.c = reinterpret_cast<const T *>(base + L::OFF_C);
+    return v;
+  };
+  bool ok = true;
+  auto wait = [&](int p) {
+    const int n = p - pbase;
+    if (!mbar_wait(&bars[n % TMA_STAGES], (uint32_t)((n / TMA_STAGES) & 1))) ok = false;
+  };
+  if (producer)
+    for (int p = pbase; p <= min(pbase + TMA_STAGES - 1, i1); ++p) issue(p);
+  op.init(st);
+  // tile row of this warp: 0 = j0-1, 1..8 = output rows, 9 = j0+8
+  const int rr = warp < TILE_ROWS ? warp + 1 : (warp == TILE_ROWS ? 0 : TILE_ROWS + 1);
+  const int j = j0 + rr - 1;
+  const int k = k0 + lane * 4;
+  const bool act = j >= 0 && j < ny && k < nz;
+  const bool out = warp < TILE_ROWS;
+  const int64_t plane = (int64_t)ny * nz;
+  float4 vm = make_float4(0.f, 0.f, 0.f, 0.f), vc;
+  uint32_t mc;
+  wait(pbase);
+  if (out) {
+    const StageView<T> v = view(pbase);
+    vm = op.val4(v, rr, lane, v.mask4(rr, lane));
+  }
+  wait(i0);
+  {
+    const StageView<T> v = view(i0);
+    mc = v.mask4(rr, lane);
+    vc = op.val4(v, rr, lane, mc);
+  }
+  plane_buf[i0 & 1][rr][lane] = vc;
+  __syncthreads();
+  if (producer && pbase + TMA_STAGES <= i1) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    issue(pbase + TMA_STAGES);
+  }
+  int64_t o = (int64_t)i0 * plane + (int64_t)j * nz + k;
+  for (int i = i0; i < i1; ++i) {
+    wait(i + 1);
+    const StageView<T> vnx = view(i + 1);
+    const uint32_t mn = vnx.mask4(rr, lane);
+    const float4 vn = op.val4(vnx, rr, lane, mn);
+    plane_buf[(i + 1) & 1][rr][lane] = vn;
+    if (out) {
+      const StageView<T> v = view(i);
+      const float4 vjm = plane_buf[i & 1][rr - 1][lane];
+      const float4 vjp = plane_buf[i & 1][rr + 1][lane];
+      float vkm = __shfl_up_sync(0xffffffffu, vc.w, 1);
+      float vkp = __shfl_down_sync(0xffffffffu, vc.x, 1);
+      // k halo of the row from the tile's padding (zero outside the grid)
+      float vh = 0.0f;
+      if (lane == 0 || lane == 31) vh = op.val1(v, rr, lane == 0 ? -1 : 128);
+      if (lane == 0) vkm = vh;
+      if (lane == 31) vkp = vh;
+      const float4 vb = make_float4(vkm, vc.x, vc.y, vc.z);
+      const float4 vf = make_float4(vc.y, vc.z, vc.w, vkp);
+      float s[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const float ns = (float)((mc >> (8 * q)) & 7u);
+        s[q] = fmaf(ns, q4(vc, q),
+                    ((q4(vm, q) + q4(vn, q)) + (q4(vjm, q) + q4(vjp, q))) +
+                        (q4(vb, q) + q4(vf, q)));
+      }
+      if (act) op.emit(v, rr, lane, i, j, o, mc, vc, s, xch);
+    }
+    __syncthreads();
+    if (producer && i + TMA_STAGES <= i1) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(i + TMA_STAGES);
+    }
+    if (out) op.after_step(i, j, k, act, xch);
+    vm = vc;
+    vc = vn;
+    mc = mn;
+    o += plane;
+  }
+  if (producer) {
+    // every issued plane has been waited for above; confirm (bounded) that no
+    // copy is still in flight before the CTA's shared memory goes away
+    for (int p = max(pbase, i1 - TMA_STAGES + 1); p <= i1; ++p) wait(p);
+  }
+  if (!ok) atomicExch(const_cast<int *>(&st->dev_error), 1);
+  op.template finish<TILE_WARPS>(sh);
+}
+
+// ---- TMA launch helpers (host) ----------------------------------------------------------
+bool g_fine_tma_enabled = true;  // BSP_TUNE_FINE_TMA
+
+static PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault,
+                                         &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  });
+  return fn;
+}
+
+template <class T>
+constexpr CUtensorMapDataType tma_dtype() {
+  return sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
+                        : (std::is_same<T, __half>::value ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                          : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16);
+}
+
+// 3-D map of a C-contiguous (nx, ny, nz) array, box {bx, by, 1}; out-of-range
+// elements read as zero.
+static bool make_map(CUtensorMap *m, CUtensorMapDataType t, int esize, const void *base, int nx,
+                     int ny, int nz, int bx, int by) {
+  auto fn = encode_tiled();
+  if (!fn || ((uintptr_t)base & 15u) || ((int64_t)nz * esize) % 16) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)nz, (cuuint64_t)ny, (cuuint64_t)nx};
+  const cuuint64_t strides[2] = {(cuuint64_t)nz * esize, (cuuint64_t)ny * nz * esize};
+  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  return fn(m, t, 3, const_cast<void *>(base), dims, strides, box, es,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// The TMA path needs nz % 16 == 0 (16-byte mask rows) and 16-byte aligned bases.
+static bool tma_eligible(int nz) { return g_fine_tma_enabled && nz % 16 == 0 && encode_tiled(); }
+
+template <class T, class Op>
+static bool launch_tma(const Op &op, const TmaMaps &maps, int nx, int ny, int nz,
+                       const uint8_t *tiles, const SolverState *st, cudaStream_t s) {
+  using L = TmaSmem<T, Op>;
+  static std::once_flag once;
+  static cudaError_t attr = cudaSuccess;
+  std::call_once(once, [] {
+    attr = cudaFuncSetAttribute(fine_tma_kernel<T, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                L::TOTAL);
+  });
+  if (attr != cudaSuccess) return false;
+  fine_tma_kernel<T, Op><<<fine_grid(nx, ny, nz), TILE_THREADS, L::TOTAL, s>>>(
+      op, maps, nx, ny, nz, fine_bi(nx, ny, nz), tiles, st);
+  return true;
 }
 
 // ---- FP64 residual on the column layout --------------------------------------------------
@@ -383,11 +857,20 @@ __device__ __forceinline__ double dq(const D4 &v, int q) {
 
 template <class T, bool WRITE>
 __global__ void __launch_bounds__(256) resid64_col_kernel(int nx, int ny, int nz, int bi,
-                                                          const uint8_t *mask, const float *div,
+                                                          const uint8_t *mask,
+                                                          const uint8_t *tiles, const float *div,
                                                           const double *x, double bscale, T *rhat,
                                                           float *e, double *partials,
                                                           const SolverState *st) {
   if (st->done) return;
+  if (tiles && !tiles[block_linear()]) {
+    // no fluid: residual 0, and rhat and e are already 0 on these cells
+    if (threadIdx.x == 0) {
+      partials[block_linear()] = 0.0;
+      partials[PARTIAL_STRIDE + block_linear()] = 0.0;
+    }
+    return;
+  }
   const double scale = st->scale;
   __shared__ double shs[8], shm[8];
   const int lane = threadIdx.x & 31;
@@ -470,7 +953,7 @@ int num_sms();
 // CTAs per SM (coarse levels are short; long plane chunks there leave the
 // GPU idle).  Even, because the restriction pairs planes inside one CTA.
 int fine_bi(int nx, int ny, int nz) {
-  const int64_t cols = (int64_t)((nz / 4 + 31) / 32) * ((ny + 7) / 8);
+  const int64_t cols = (int64_t)((nz / 4 + 31) / 32) * ((ny + TILE_ROWS - 1) / TILE_ROWS);
   const int64_t target = 2LL * num_sms();
   int bi = 16;
   while (bi > 2 && cols * ((nx + bi - 1) / bi) < target) bi -= 2;
@@ -479,7 +962,7 @@ int fine_bi(int nx, int ny, int nz) {
 
 dim3 fine_grid(int nx, int ny, int nz) {
   const int bi = fine_bi(nx, ny, nz);
-  return dim3((nz / 4 + 31) / 32, (ny + 7) / 8, (nx + bi - 1) / bi);
+  return dim3((nz / 4 + 31) / 32, (ny + TILE_ROWS - 1) / TILE_ROWS, (nx + bi - 1) / bi);
 }
 int fine_grid_blocks(int nx, int ny, int nz) {
   const dim3 g = fine_grid(nx, ny, nz);
@@ -487,8 +970,22 @@ int fine_grid_blocks(int nx, int ny, int nz) {
 }
 
 template <class T>
-void launch_fine_psap(int nx, int ny, int nz, const uint8_t *mask, const T *z, const T *prev,
-                      T *cur, T *Ap, double *partials, const SolverState *st, cudaStream_t s) {
+void launch_fine_psap(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *tiles,
+                      const T *z, const T *prev, T *cur, T *Ap, double *partials,
+                      const SolverState *st, cudaStream_t s) {
+  if (tma_eligible(nz)) {
+    constexpr int FW = TmaGeom<T>::FW;
+    TmaMaps maps{};
+    if (make_map(&maps.a, tma_dtype<T>(), sizeof(T), z, nx, ny, nz, FW, TMA_ROWS) &&
+        make_map(&maps.b, tma_dtype<T>(), sizeof(T), prev, nx, ny, nz, FW, TMA_ROWS) &&
+        make_map(&maps.m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, mask, nx, ny, nz, MASK_W, TMA_ROWS)) {
+      TPsAp<T> op{};
+      op.cur = cur;
+      op.Ap = Ap;
+      op.partials = partials;
+      if (launch_tma<T>(op, maps, nx, ny, nz, tiles, st, s)) return;
+    }
+  }
   PsApOp<T> op{};
   op.mask = mask;
   op.z = z;
@@ -496,14 +993,30 @@ void launch_fine_psap(int nx, int ny, int nz, const uint8_t *mask, const T *z, c
   op.cur = cur;
   op.Ap = Ap;
   op.partials = partials;
-  fine_col_kernel<PsApOp<T>><<<fine_grid(nx, ny, nz), 256, 0, s>>>(op, nx, ny, nz,
-                                                                   fine_bi(nx, ny, nz), st);
+  fine_tile_kernel<PsApOp<T>><<<fine_grid(nx, ny, nz), TILE_THREADS, 0, s>>>(
+      op, nx, ny, nz, fine_bi(nx, ny, nz), tiles, st);
 }
 
 template <class T>
-void launch_fine_up(const Level<T> &f, const Level<T> &c, T *z, double *partials,
+void launch_fine_up(const Level<T> &f, const Level<T> &c, T *z, double *partials, float alpha,
                     const SolverState *st, cudaStream_t s) {
+  if (tma_eligible(f.nz) && c.nz * 2 == f.nz && c.ny * 2 >= f.ny && c.nx * 2 >= f.nx) {
+    TmaMaps maps{};
+    if (make_map(&maps.a, tma_dtype<T>(), sizeof(T), f.r, f.nx, f.ny, f.nz, TmaGeom<T>::FW,
+                 TMA_ROWS) &&
+        make_map(&maps.m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, f.mask, f.nx, f.ny, f.nz, MASK_W,
+                 TMA_ROWS) &&
+        make_map(&maps.c, tma_dtype<T>(), sizeof(T), c.e, c.nx, c.ny, c.nz, TmaGeom<T>::CW,
+                 TmaGeom<T>::CROWS)) {
+      TUp<T> op{};
+      op.z = z;
+      op.partials = partials;
+      op.alpha = alpha;
+      if (launch_tma<T>(op, maps, f.nx, f.ny, f.nz, f.tiles, st, s)) return;
+    }
+  }
   UpOp<T> op{};
+  op.alpha = alpha;
   op.mask = f.mask;
   op.r = f.r;
   op.e1 = c.e;
@@ -511,13 +1024,29 @@ void launch_fine_up(const Level<T> &f, const Level<T> &c, T *z, double *partials
   op.partials = partials;
   op.ny1 = c.ny;
   op.nz1 = c.nz;
-  fine_col_kernel<UpOp<T>><<<fine_grid(f.nx, f.ny, f.nz), 256, 0, s>>>(
-      op, f.nx, f.ny, f.nz, fine_bi(f.nx, f.ny, f.nz), st);
+  fine_tile_kernel<UpOp<T>><<<fine_grid(f.nx, f.ny, f.nz), TILE_THREADS, 0, s>>>(
+      op, f.nx, f.ny, f.nz, fine_bi(f.nx, f.ny, f.nz), f.tiles, st);
 }
 
 template <class T>
 void launch_fine_down(const Level<T> &f, const Level<T> &c, const SolverState *st,
                       cudaStream_t s) {
+  if (tma_eligible(f.nz)) {
+    TmaMaps maps{};
+    if (make_map(&maps.a, tma_dtype<T>(), sizeof(T), f.r, f.nx, f.ny, f.nz, TmaGeom<T>::FW,
+                 TMA_ROWS) &&
+        make_map(&maps.m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, f.mask, f.nx, f.ny, f.nz, MASK_W,
+                 TMA_ROWS)) {
+      TDown<T> op{};
+      op.mask1 = c.mask;
+      op.r1 = c.r;
+      op.nx = f.nx;
+      op.ny = f.ny;
+      op.ny1 = c.ny;
+      op.nz1 = c.nz;
+      if (launch_tma<T>(op, maps, f.nx, f.ny, f.nz, f.tiles, st, s)) return;
+    }
+  }
   DownOp<T> op{};
   op.mask = f.mask;
   op.mask1 = c.mask;
@@ -527,32 +1056,113 @@ void launch_fine_down(const Level<T> &f, const Level<T> &c, const SolverState *s
   op.ny = f.ny;
   op.ny1 = c.ny;
   op.nz1 = c.nz;
-  fine_col_kernel<DownOp<T>><<<fine_grid(f.nx, f.ny, f.nz), 256, 0, s>>>(
-      op, f.nx, f.ny, f.nz, fine_bi(f.nx, f.ny, f.nz), st);
+  fine_tile_kernel<DownOp<T>><<<fine_grid(f.nx, f.ny, f.nz), TILE_THREADS, 0, s>>>(
+      op, f.nx, f.ny, f.nz, fine_bi(f.nx, f.ny, f.nz), f.tiles, st);
 }
 
+// The FP64 residual keeps the 8-warp column layout (no operand to share: x
+// is read directly) on the same tiles as fine_grid (8 rows per CTA).
+static_assert(TILE_ROWS == 8, "the residual and update kernels share fine_grid's tiles");
 template <class T>
-int launch_resid64_col(int nx, int ny, int nz, const uint8_t *mask, const float *div,
-                       const double *x, double bscale, T *rhat, float *e, double *partials,
-                       const SolverState *st, bool write, cudaStream_t s) {
+int launch_resid64_col(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *tiles,
+                       const float *div, const double *x, double bscale, T *rhat, float *e,
+                       double *partials, const SolverState *st, bool write, cudaStream_t s) {
   const dim3 g = fine_grid(nx, ny, nz);
   const int bi = fine_bi(nx, ny, nz);
   if (write)
-    resid64_col_kernel<T, true><<<g, 256, 0, s>>>(nx, ny, nz, bi, mask, div, x, bscale, rhat, e,
-                                                  partials, st);
+    resid64_col_kernel<T, true><<<g, 256, 0, s>>>(nx, ny, nz, bi, mask, tiles, div, x, bscale,
+                                                  rhat, e, partials, st);
   else
-    resid64_col_kernel<T, false><<<g, 256, 0, s>>>(nx, ny, nz, bi, mask, div, x, bscale, rhat,
-                                                   e, partials, st);
+    resid64_col_kernel<T, false><<<g, 256, 0, s>>>(nx, ny, nz, bi, mask, tiles, div, x, bscale,
+                                                   rhat, e, partials, st);
   return (int)(g.x * g.y * g.z);
 }
 
+// e += alpha ps; r -= alpha Ap (r stored as T, read back rounded); partial
+// r.r.  One warp per row of a fine_grid tile, float4 per lane, marching i.
+// No mask: ps and Ap are zero on non-fluid cells, so e and r stay unchanged
+// there; tiles without fluid are skipped.
+template <class T>
+__global__ void __launch_bounds__(256) cg_update_col_kernel(int nx, int ny, int nz, int bi,
+                                                            const uint8_t *tiles, float *e, T *r,
+                                                            const T *ps, const T *Ap,
+                                                            double *partials,
+                                                            const SolverState *st) {
+  if (st->inner_done) return;
+  if (tiles && !tiles[block_linear()]) {
+    if (threadIdx.x == 0) partials[block_linear()] = 0.0;
+    return;
+  }
+  __shared__ double sh[8];
+  const float alpha = (float)st->alpha;
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
+  const int k = (blockIdx.x * 32 + lane) * 4;
+  double acc = 0.0;
+  if (j < ny && k < nz) {
+    const int i0 = blockIdx.z * bi, i1 = min(i0 + bi, nx);
+    const int64_t plane = (int64_t)ny * nz;
+    int64_t o = ((int64_t)i0 * ny + j) * nz + k;
+#pragma unroll 4
+    for (int i = i0; i < i1; ++i, o += plane) {
+      float4 ee = *reinterpret_cast<const float4 *>(e + o);
+      const float4 pp = ld4s(ps, o), aa = ld4s(Ap, o);
+      float4 rr = ld4s(r, o);
+      ee = make_float4(fmaf(alpha, pp.x, ee.x), fmaf(alpha, pp.y, ee.y), fmaf(alpha, pp.z, ee.z),
+                       fmaf(alpha, pp.w, ee.w));
+      rr = make_float4(rt(fmaf(-alpha, aa.x, rr.x), r), rt(fmaf(-alpha, aa.y, rr.y), r),
+                       rt(fmaf(-alpha, aa.z, rr.z), r), rt(fmaf(-alpha, aa.w, rr.w), r));
+      *reinterpret_cast<float4 *>(e + o) = ee;
+      st4s(r, o, rr);
+      acc += ((double)rr.x * rr.x + (double)rr.y * rr.y) +
+             ((double)rr.z * rr.z + (double)rr.w * rr.w);
+    }
+  }
+  block_partial<8>(acc, partials, sh);
+}
+
+template <class T>
+int launch_cg_update_col(int nx, int ny, int nz, const uint8_t *tiles, float *e, T *r,
+                         const T *ps, const T *Ap, double *partials, const SolverState *st,
+                         cudaStream_t s) {
+  const dim3 g = fine_grid(nx, ny, nz);
+  cg_update_col_kernel<T><<<g, 256, 0, s>>>(nx, ny, nz, fine_bi(nx, ny, nz), tiles, e, r, ps,
+                                            Ap, partials, st);
+  return (int)(g.x * g.y * g.z);
+}
+
+// flags[b] = 1 if tile b of fine_grid(nx, ny, nz) holds a fluid cell.
+__global__ void __launch_bounds__(256) tile_flags_kernel(int nx, int ny, int nz, int bi,
+                                                         const uint8_t *mask, uint8_t *flags) {
+  const int i0 = blockIdx.z * bi, i1 = min(i0 + bi, nx);
+  const int j0 = blockIdx.y * TILE_ROWS;
+  const int k0 = blockIdx.x * 128;
+  int any = 0;
+  for (int t = threadIdx.x; t < (i1 - i0) * TILE_ROWS * 128; t += blockDim.x) {
+    const int kk = k0 + t % 128, jj = j0 + (t / 128) % TILE_ROWS, ii = i0 + t / (128 * TILE_ROWS);
+    if (jj < ny && kk < nz && (mask[((int64_t)ii * ny + jj) * nz + kk] & BSP_MFLUID)) any = 1;
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) flags[block_linear()] = any ? 1 : 0;
+}
+
+void launch_tile_flags(int nx, int ny, int nz, const uint8_t *mask, uint8_t *flags,
+                       cudaStream_t s) {
+  tile_flags_kernel<<<fine_grid(nx, ny, nz), 256, 0, s>>>(nx, ny, nz, fine_bi(nx, ny, nz), mask,
+                                                          flags);
+}
+
 #define INST(T)                                                                              \
-  template int launch_resid64_col<T>(int, int, int, const uint8_t *, const float *,          \
-                                     const double *, double, T *, float *, double *,         \
-                                     const SolverState *, bool, cudaStream_t);               \
-  template void launch_fine_psap<T>(int, int, int, const uint8_t *, const T *, const T *, T *, \
-                                    T *, double *, const SolverState *, cudaStream_t);         \
-  template void launch_fine_up<T>(const Level<T> &, const Level<T> &, T *, double *,          \
+  template int launch_resid64_col<T>(int, int, int, const uint8_t *, const uint8_t *,        \
+                                     const float *, const double *, double, T *, float *,    \
+                                     double *, const SolverState *, bool, cudaStream_t);     \
+  template int launch_cg_update_col<T>(int, int, int, const uint8_t *, float *, T *,         \
+                                       const T *, const T *, double *, const SolverState *,  \
+                                       cudaStream_t);                                        \
+  template void launch_fine_psap<T>(int, int, int, const uint8_t *, const uint8_t *,         \
+                                    const T *, const T *, T *, T *, double *,                 \
+                                    const SolverState *, cudaStream_t);                       \
+  template void launch_fine_up<T>(const Level<T> &, const Level<T> &, T *, double *, float,   \
                                   const SolverState *, cudaStream_t);                         \
   template void launch_fine_down<T>(const Level<T> &, const Level<T> &, const SolverState *,  \
                                     cudaStream_t);

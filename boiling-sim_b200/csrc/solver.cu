@@ -42,6 +42,13 @@ int num_sms();
 constexpr float OMEGA = 6.0f / 7.0f;
 // BSP_TUNE_FINE_COLUMN: level-0 kernels on the column layout (1) or per row (0)
 bool g_fine_col_enabled = true;
+// BSP_TUNE_MG_ALPHA: scale of the coarse-grid correction added by every
+// prolongation (1 = plain correction; above 1 = over-correction).  Any value
+// > 0 keeps the V-cycle a symmetric positive definite preconditioner: the
+// coarse part alpha P A_c^-1 R is positive semi-definite and the damped
+// Jacobi smoother is convergent.
+float g_mg_alpha = 1.0f;
+extern bool g_fine_tma_enabled;  // BSP_TUNE_FINE_TMA (mgfine.cu)
 constexpr int COARSE_SWEEPS = 64;
 constexpr int RED_THREADS = 256;
 
@@ -394,7 +401,8 @@ __global__ void __launch_bounds__(512) mg_coarse_kernel(Level<T> L, const float 
 // partial r.z.
 template <class T, bool FINE>
 __global__ void __launch_bounds__(256) mg_up_kernel(Level<T> f, Level<T> co, T *out,
-                                                    double *partials, const SolverState *st) {
+                                                    double *partials, const SolverState *st,
+                                                    float alpha) {
   if (st->inner_done) return;
   RowIter it(f.nx, f.ny);
   const int lane = threadIdx.x & 31;
@@ -411,7 +419,7 @@ __global__ void __launch_bounds__(256) mg_up_kernel(Level<T> f, Level<T> co, T *
       }
       auto ehat = [&](int ii, int jj, int kk, int64_t cc, uint32_t mb) {
         const int64_t P = ((int64_t)(ii >> 1) * co.ny + (jj >> 1)) * co.nz + (kk >> 1);
-        return pre_e(f.r, cc, mb) + ld(co.e, P);
+        return fmaf(alpha, ld(co.e, P), pre_e(f.r, cc, mb));
       };
       const float ec = ehat(i, j, k, c, mc);
 #define NB(cond, di, dj, dk, off)                                                     \
@@ -579,6 +587,11 @@ __global__ void __launch_bounds__(RED_THREADS) outer_check_kernel(SolverState *s
   const double rr = reduce_slot(partials, 0, nblocks, false);
   const double rmax = reduce_slot(partials, 1, nblocks, true);
   if (threadIdx.x != 0) return;
+  if (st->dev_error) {
+    st->status = BSP_ERR_TIMEOUT;
+    st->done = 1;
+    return;
+  }
   st->r64_norm2 = rr;
   st->rel = st->b_norm2 > 0.0 ? sqrt(rr / st->b_norm2) : 0.0;
   if (!(rr == rr) || rr > 1e300) {
@@ -635,6 +648,12 @@ __global__ void __launch_bounds__(RED_THREADS) inner_check_kernel(SolverState *s
   st->inner_it += 1;
   st->total_inner += 1;
   st->rr_inner = rr;
+  if (st->dev_error) {
+    st->status = BSP_ERR_TIMEOUT;
+    st->inner_done = 1;
+    st->done = 1;
+    return;
+  }
   if (!(rr == rr) || rr <= st->eta_eff * st->eta_eff * st->rhat_norm2 ||
       st->inner_it >= st->max_inner || st->alpha == 0.0)
     st->inner_done = 1;
@@ -681,9 +700,10 @@ size_t storage_bytes(int storage) { return storage == BSP_STORE_FP32 ? 4 : 2; }
 //   | z, ps0, ps1, Ap, r (n T each) | per level l >= 1: mask, r, e (T)
 //   | per level l >= 1 ... ; level-0 effective-class scratch reuses the level-1 slot order.
 //   | coarsest-level dense inverse (float), its FP64 build scratch, direct flag
+//   | per-level column-tile fluid flags (PARTIAL_STRIDE bytes per level)
 struct Layout {
   size_t state, partials, x, e, z, ps0, ps1, Ap, r, lvl_mask[MAX_LEVELS], lvl_r[MAX_LEVELS],
-      lvl_e[MAX_LEVELS], eff0, cinv, cA, cflag, total;
+      lvl_e[MAX_LEVELS], eff0, cinv, cA, cflag, tflags, total;
   int L, dims[3 * MAX_LEVELS];
 };
 
@@ -721,6 +741,7 @@ Layout make_layout(int nx, int ny, int nz, int storage) {
     lo.cA = take(sizeof(double) * nc * nc + 8);
     lo.cflag = take(sizeof(int));
   }
+  lo.tflags = take((size_t)MAX_LEVELS * PARTIAL_STRIDE);  // column-tile fluid flags per level
   lo.total = off;
   return lo;
 }
@@ -766,6 +787,9 @@ Ctx<T> make_ctx(void *ws, const uint8_t *mask, int nx, int ny, int nz, int stora
       L.r = (T *)(cx.base + cx.lo.lvl_r[l]);
       L.e = (T *)(cx.base + cx.lo.lvl_e[l]);
     }
+    L.tiles = (L.nz % 4 == 0 && fine_grid_blocks(L.nx, L.ny, L.nz) <= PARTIAL_STRIDE)
+                  ? (const uint8_t *)(cx.base + cx.lo.tflags + (size_t)l * PARTIAL_STRIDE)
+                  : nullptr;
   }
   return cx;
 }
@@ -802,6 +826,26 @@ cudaError_t setup_levels(Ctx<T> &cx, cudaStream_t s) {
                                                                       c.ny, c.nz);
     }
     prev = c.mask;
+  }
+  // Every solver vector is zero on non-fluid cells and stays so (the kernels
+  // write masked values; column tiles without fluid are never written).
+  {
+    const size_t ts = sizeof(T);
+    cudaMemsetAsync(cx.base + cx.lo.z, 0, cx.lo.r + ts * cx.n - cx.lo.z, s);  // z ps0 ps1 Ap r
+    cudaMemsetAsync(cx.base + cx.lo.e, 0, sizeof(float) * cx.n, s);
+    for (int l = 1; l < cx.lo.L; ++l) {
+      const Level<T> &c = cx.lv[l];
+      const size_t nl = (size_t)c.nx * c.ny * c.nz;
+      cudaMemsetAsync(c.r, 0, ts * nl, s);
+      cudaMemsetAsync(c.e, 0, ts * nl, s);
+    }
+    for (int l = 0; l < cx.lo.L; ++l) {
+      const Level<T> &v = cx.lv[l];
+      if (v.tiles) {
+        ProfScope ps(PROF_CONTROL, s);
+        launch_tile_flags(v.nx, v.ny, v.nz, v.mask, const_cast<uint8_t *>(v.tiles), s);
+      }
+    }
   }
   {
     Level<T> &c = cx.lv[cx.lo.L - 1];
@@ -851,19 +895,20 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
     Level<T> &f = cx.lv[l], &c = cx.lv[l + 1];
     ProfScope ps(PROF_MG_COARSE, s);
     if (level_col(l))  // its r.e partial is written but unused
-      launch_fine_up<T>(f, c, f.e, cx.partials, st, s);
+      launch_fine_up<T>(f, c, f.e, cx.partials, g_mg_alpha, st, s);
     else
-      mg_up_kernel<T, false><<<row_blocks((int64_t)f.nx * f.ny), 256, 0, s>>>(f, c, f.e,
-                                                                              cx.partials, st);
+      mg_up_kernel<T, false><<<row_blocks((int64_t)f.nx * f.ny), 256, 0, s>>>(
+          f, c, f.e, cx.partials, st, g_mg_alpha);
   }
   T *z = (T *)(cx.base + cx.lo.z);
   const int nb0 = col ? fine_grid_blocks(cx.nx, cx.ny, cx.nz) : row_blocks((int64_t)cx.nx * cx.ny);
   {
     ProfScope ps(PROF_MG_UP0, s);
     if (col)
-      launch_fine_up<T>(cx.lv[0], cx.lv[1], z, cx.partials, st, s);
+      launch_fine_up<T>(cx.lv[0], cx.lv[1], z, cx.partials, g_mg_alpha, st, s);
     else
-      mg_up_kernel<T, true><<<nb0, 256, 0, s>>>(cx.lv[0], cx.lv[1], z, cx.partials, st);
+      mg_up_kernel<T, true><<<nb0, 256, 0, s>>>(cx.lv[0], cx.lv[1], z, cx.partials, st,
+                                                g_mg_alpha);
   }
   {
     ProfScope ps(PROF_CONTROL, s);
@@ -875,7 +920,8 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
   {
     ProfScope ps(PROF_CG_PSAP, s);
     if (col)
-      launch_fine_psap<T>(cx.nx, cx.ny, cx.nz, cx.mask0, z, prev, cur, Ap, cx.partials, st, s);
+      launch_fine_psap<T>(cx.nx, cx.ny, cx.nz, cx.mask0, cx.lv[0].tiles, z, prev, cur, Ap,
+                          cx.partials, st, s);
     else
       cg_ps_ap_kernel<T><<<nb0, 256, 0, s>>>(cx.nx, cx.ny, cx.nz, cx.mask0, z, prev, cur, Ap,
                                              cx.partials, st);
@@ -884,11 +930,16 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
     ProfScope ps(PROF_CONTROL, s);
     alpha_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials, nb0);
   }
-  const int nbf = flat_blocks(cx.n);
+  int nbf = flat_blocks(cx.n);
   {
     ProfScope ps(PROF_CG_UPDATE, s);
-    cg_update_kernel<T><<<nbf, 256, 0, s>>>(cx.n, cx.mask0, (float *)(cx.base + cx.lo.e),
-                                            cx.lv[0].r, cur, Ap, cx.partials, st);
+    if (col)
+      nbf = launch_cg_update_col<T>(cx.nx, cx.ny, cx.nz, cx.lv[0].tiles,
+                                    (float *)(cx.base + cx.lo.e), cx.lv[0].r, cur, Ap,
+                                    cx.partials, st, s);
+    else
+      cg_update_kernel<T><<<nbf, 256, 0, s>>>(cx.n, cx.mask0, (float *)(cx.base + cx.lo.e),
+                                              cx.lv[0].r, cur, Ap, cx.partials, st);
   }
   {
     ProfScope ps(PROF_CONTROL, s);
@@ -904,8 +955,8 @@ template <class T>
 int launch_resid(Ctx<T> &cx, const float *div, const double *x, double bscale, T *rhat, float *e,
                  bool write, cudaStream_t s) {
   if (cx.col && ((uintptr_t)div & 15u) == 0)
-    return launch_resid64_col<T>(cx.nx, cx.ny, cx.nz, cx.mask0, div, x, bscale, rhat, e,
-                                 cx.partials, cx.st, write, s);
+    return launch_resid64_col<T>(cx.nx, cx.ny, cx.nz, cx.mask0, cx.lv[0].tiles, div, x, bscale,
+                                 rhat, e, cx.partials, cx.st, write, s);
   const int nbr = row_blocks((int64_t)cx.nx * cx.ny);
   if (write)
     residual64_kernel<T, true><<<nbr, 256, 0, s>>>(cx.nx, cx.ny, cx.nz, cx.mask0, div, x, bscale,
@@ -1306,6 +1357,12 @@ static void key_params(GraphKey &k, const BspSolveParams *p) {
                       (uintptr_t)p->max_inner, (uintptr_t)p->storage,
                       (uintptr_t)p->warm_start})
     k.v.push_back(x);
+  // launch-time tuning captured into the graph
+  uint32_t a;
+  memcpy(&a, &g_mg_alpha, 4);
+  k.v.push_back((uintptr_t)a);
+  k.v.push_back((uintptr_t)g_fine_col_enabled);
+  k.v.push_back((uintptr_t)g_fine_tma_enabled);
 }
 
 }  // namespace bsp

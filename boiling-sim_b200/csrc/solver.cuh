@@ -15,6 +15,11 @@ struct Level {
   const uint8_t *mask;  // class | n_solid << 2 (effective classes for l >= 1)
   T *r;                 // right-hand side of this level
   T *e;                 // correction of this level (level 0: z)
+  // One byte per CTA tile of the column-layout grid (fine_grid): nonzero when
+  // the tile holds a fluid cell.  Tiles without fluid are skipped: every
+  // vector of the solver is zero on non-fluid cells and stays so.  Null: no
+  // skipping.
+  const uint8_t *tiles;
 };
 
 // Device-resident control block of one solve.  Written only by the one-block
@@ -25,7 +30,8 @@ struct SolverState {
   double rz, beta, alpha, rr_inner;
   int max_outer, max_inner;
   int outer_it, inner_it, total_inner;
-  int done, inner_done, status, finalize, pad;
+  int done, inner_done, status, finalize;
+  int dev_error;  // set by a kernel whose bounded wait gave up
   // loop guards of the graph-driven solve: counted by the condition kernels
   // themselves so every WHILE node ends even if other state went wrong
   int guard_inner, guard_outer;
@@ -34,18 +40,28 @@ struct SolverState {
 // Level-0 kernels on the column layout (mgfine.cu); nz % 4 == 0 required.
 int fine_grid_blocks(int nx, int ny, int nz);
 template <class T>
-void launch_fine_psap(int nx, int ny, int nz, const uint8_t *mask, const T *z, const T *prev,
-                      T *cur, T *Ap, double *partials, const SolverState *st, cudaStream_t s);
+void launch_fine_psap(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *tiles,
+                      const T *z, const T *prev, T *cur, T *Ap, double *partials,
+                      const SolverState *st, cudaStream_t s);
 template <class T>
-void launch_fine_up(const Level<T> &f, const Level<T> &c, T *z, double *partials,
+void launch_fine_up(const Level<T> &f, const Level<T> &c, T *z, double *partials, float alpha,
                     const SolverState *st, cudaStream_t s);
 template <class T>
 void launch_fine_down(const Level<T> &f, const Level<T> &c, const SolverState *st,
                       cudaStream_t s);
 // FP64 residual on the column layout; returns the number of partial blocks.
 template <class T>
-int launch_resid64_col(int nx, int ny, int nz, const uint8_t *mask, const float *div,
-                       const double *x, double bscale, T *rhat, float *e, double *partials,
-                       const SolverState *st, bool write, cudaStream_t s);
+int launch_resid64_col(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *tiles,
+                       const float *div, const double *x, double bscale, T *rhat, float *e,
+                       double *partials, const SolverState *st, bool write, cudaStream_t s);
+// e += alpha ps; r -= alpha Ap; partial r.r -- streaming over the column
+// tiles (no mask: ps and Ap are zero off fluid); returns the partial count.
+template <class T>
+int launch_cg_update_col(int nx, int ny, int nz, const uint8_t *tiles, float *e, T *r,
+                         const T *ps, const T *Ap, double *partials, const SolverState *st,
+                         cudaStream_t s);
+// One flag byte per column tile: any fluid cell in the tile.
+void launch_tile_flags(int nx, int ny, int nz, const uint8_t *mask, uint8_t *flags,
+                       cudaStream_t s);
 
 }  // namespace bsp

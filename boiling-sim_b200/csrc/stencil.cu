@@ -498,6 +498,8 @@ extern "C" int bsp_selftest_div6(unsigned long long *mismatches_dev, cudaStream_
 
 namespace bsp {
 extern bool g_fine_col_enabled;
+extern float g_mg_alpha;
+extern bool g_fine_tma_enabled;
 }
 
 extern "C" int bsp_set_tuning(int key, int value) {
@@ -509,6 +511,14 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_FINE_COLUMN:
       if (value < 0 || value > 1) return BSP_ERR_ARG;
       bsp::g_fine_col_enabled = value != 0;
+      return BSP_OK;
+    case BSP_TUNE_MG_ALPHA:
+      if (value < 100 || value > 3000) return BSP_ERR_ARG;
+      bsp::g_mg_alpha = (float)value / 1000.0f;
+      return BSP_OK;
+    case BSP_TUNE_FINE_TMA:
+      if (value < 0 || value > 1) return BSP_ERR_ARG;
+      bsp::g_fine_tma_enabled = value != 0;
       return BSP_OK;
     default:
       return BSP_ERR_ARG;

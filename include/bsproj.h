@@ -53,6 +53,8 @@ extern "C" {
 /* autotuner keys of bsp_set_tuning */
 #define BSP_TUNE_SWEEP_BI 1     /* i-planes per CTA of the sweep kernels (0 = heuristic) */
 #define BSP_TUNE_FINE_COLUMN 2  /* solver level-0 kernels: 1 column layout, 0 row layout */
+#define BSP_TUNE_MG_ALPHA 3     /* coarse-correction scale of the V-cycle, in 1/1000 (100..3000) */
+#define BSP_TUNE_FINE_TMA 4     /* column-layout solver kernels fed by TMA tiles: 1 on, 0 off */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */

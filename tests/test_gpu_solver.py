@@ -90,6 +90,30 @@ def test_column_and_row_level0_kernels_agree(cuda, pot64, storage):
     assert O.rel_error(out[1].p64, out[0].p64, mat) < 1e-5
 
 
+@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16"])
+@pytest.mark.parametrize("spec", [S.POT_64, S.PotSpec(66, 50, 80, 20, 3, 60, 5, 20)],
+                         ids=["pot64", "ny50_nz80"])
+def test_tma_and_shared_plane_kernels_bit_identical(cuda, storage, spec):
+    """The TMA-fed column kernels and the load-per-thread ones compute the same
+    operations in the same order: bit-identical iterates and counts."""
+    from boilingsim_b200 import _lib
+
+    mat = S.pot_mat(spec)
+    ux, uy, uz = S.velocity_field(mat, seed=5)
+    div = O.divergence(ux, uy, uz, mat, DX)
+    out = {}
+    try:
+        for tma in (1, 0):
+            _lib.call("bsp_set_tuning", 4, tma)
+            res = solve_tolerance(div, mat, DX, DT, RHO, tol=1e-7, storage=storage)
+            assert res.status == 0
+            out[tma] = (res.inner_iterations, res.outer_iterations, res.p64.copy())
+    finally:
+        _lib.call("bsp_set_tuning", 4, 1)
+    assert out[1][:2] == out[0][:2]
+    assert np.array_equal(out[1][2], out[0][2])
+
+
 @pytest.mark.parametrize("spec", [S.pot_192(2), S.PotSpec(70, 54, 37, 22, 3, 29, 5, 20),
                                   S.PotSpec(66, 50, 44, 20, 3, 33, 5, 20)],
                          ids=["pot192", "odd70x54x37", "odd_ny66x50x44"])
