@@ -49,6 +49,28 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+def active_tile_cells(mat, nsm: int) -> int:
+    """Cells in the level-0 column tiles that hold a fluid cell: tiles of 8 j
+    rows x 128 k x bi i planes, bi the largest even value <= 16 that still
+    gives two tiles per SM (the library's tiling rule)."""
+    nx, ny, nz = mat.shape
+    cols = ((nz // 4 + 31) // 32) * ((ny + 7) // 8)
+    bi = 16
+    while bi > 2 and cols * ((nx + bi - 1) // bi) < 2 * nsm:
+        bi -= 2
+    f = mat == 0
+    total = 0
+    for i0 in range(0, nx, bi):
+        fi = f[i0:i0 + bi]
+        for j0 in range(0, ny, 8):
+            fj = fi[:, j0:j0 + 8]
+            for k0 in range(0, nz, 128):
+                blk = fj[:, :, k0:k0 + 128]
+                if blk.any():
+                    total += blk.size
+    return int(total)
+
+
 def _workload():
     from boilingsim_b200 import scenes as S
 
@@ -329,8 +351,6 @@ def main():
     if dist:
         dist.barrier()
     clocks = Clocks(local)
-    _lib.call("bsp_profile_enable", 1)
-    _lib.lib().bsp_profile_read(None, None, 0)  # clear
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     ev0.record(stream)
@@ -339,9 +359,16 @@ def main():
     ev1.record(stream)
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1) / args.steps
+    clk = clocks.stop()
+    # Per-kernel-class breakdown: the same steps again with the library's event
+    # timing on (two events around every launch; not part of the timed value).
+    _lib.call("bsp_profile_enable", 1)
+    _lib.lib().bsp_profile_read(None, None, 0)  # clear
+    for _ in range(args.steps):
+        step()
+    torch.cuda.synchronize()
     _lib.call("bsp_profile_enable", 0)
     _lib.lib().bsp_profile_read(prof_ms, prof_n, ncls)
-    clk = clocks.stop()
     if dist:
         t = torch.tensor([ms], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -350,34 +377,37 @@ def main():
     res = last["res"]
 
     # ---- roofline of the dominant kernel class -------------------------------------
-    # Algorithmic bytes per grid cell per launch.  Stencil kernels touch every
-    # cell; the CG update and the FP64 residual read their vectors on fluid
-    # cells only (fraction ff of the grid).
-    ff = float((mat == 0).mean())
+    # Algorithmic bytes per launch = bytes per cell x the cells the kernel
+    # processes.  The level-0 column kernels (restriction, prolongation, A.ps,
+    # CG update, FP64 residual) skip CTA tiles holding no fluid cell, so they
+    # process n_act = the cells of the tiles with fluid; the x update is flat.
+    nsm = torch.cuda.get_device_properties(dev).multi_processor_count
+    n_act = active_tile_cells(mat, nsm)
     ts = 2 if args.storage != "fp32" else 4
-    per_cell = {0: 13.0,
-                1: ts + 1 + ts / 8,                      # r, mask -> r_coarse
-                2: ts + 1 + ts / 8 + ts,                 # r, mask, e_coarse -> z
-                3: 2 * ts + 1 + 2 * ts,                  # z, ps_prev, mask -> ps, Ap
-                4: 1 + ff * (4 + 3 * ts + 4 + ts),       # mask; e, ps, Ap, r -> e, r
-                5: 1 + ff * 12 + (ts + 4) / 2,           # mask, x, div; rhat, e (write pass)
-                6: 20.0}                                 # x, e -> x
+    per_launch = {0: 13.0 * n,
+                  1: (ts + 1 + ts / 8) * n_act,                # r, mask -> r_coarse
+                  2: (ts + 1 + ts / 8 + ts) * n_act,           # r, mask, e_coarse -> z
+                  3: (2 * ts + 1 + 2 * ts) * n_act,            # z, ps_prev, mask -> ps, Ap
+                  4: (4 + 3 * ts + 4 + ts) * n_act,            # e, ps, Ap, r -> e, r
+                  5: (13 + (ts + 4) / 2) * n_act,              # mask, x, div; rhat, e (write pass)
+                  6: 20.0 * n}                                 # x, e -> x
     names = {0: "jacobi_sweep", 1: "mg_restrict_fine", 2: "mg_prolong_smooth_fine",
              3: "cg_direction_Ap", 4: "cg_update", 5: "residual_fp64", 6: "x_update_fp64",
              7: "mg_coarse_levels", 8: "control_and_setup", 9: "divergence_gradient"}
-    dom = max((c for c in per_cell if prof_n[c] > 0), key=lambda c: prof_ms[c])
+    dom = max((c for c in per_launch if prof_n[c] > 0), key=lambda c: prof_ms[c])
     avg_ms = prof_ms[dom] / prof_n[dom]
-    bytes_launch = per_cell[dom] * n
+    bytes_launch = per_launch[dom]
     achieved = bytes_launch / (avg_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": names[dom], "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": None, "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": round(bytes_launch),
+                "cells_processed_per_launch": int(n if dom in (0, 6) else n_act),
                 "avg_launch_ms": round(avg_ms, 5),
-                "share_of_step": round(prof_ms[dom] / (ms * args.steps), 3)}
+                "share_of_step": round(prof_ms[dom] / sum(prof_ms[c] for c in range(ncls)), 3)}
     kernel_ms = {names[c]: round(prof_ms[c] / args.steps, 4) for c in range(ncls) if prof_n[c]}
-    kernel_gbs = {names[c]: round(per_cell[c] * n / (prof_ms[c] / prof_n[c] * 1e-3) / 1e9, 1)
-                  for c in per_cell if prof_n[c]}
+    kernel_gbs = {names[c]: round(per_launch[c] / (prof_ms[c] / prof_n[c] * 1e-3) / 1e9, 1)
+                  for c in per_launch if prof_n[c]}
     launches = int(sum(prof_n))  # every kernel launch of the timed steps is instrumented
 
     sweep = e2e = None
