@@ -1,0 +1,468 @@
+// mgcoarse.cu -- every coarse level of one V-cycle in one cooperative kernel.
+//
+// Below level 0 the grids are small (level 1 of the 384x384x256 pot is
+// 4.7 M cells and L2-resident; level 3 is 74 K cells) and one kernel launch
+// per level and direction costs more in launch and drain latency than the
+// work itself.  mg_cycle_kernel runs the whole coarse part of the V-cycle --
+// restriction from level 1 down to the coarsest level, the coarsest solve,
+// prolongation back up to level 1 -- in one launch with one CTA per SM:
+//
+//   down:  D1   t = OMEGA r / D on level 1                   (fluid; 0 elsewhere)
+//          per level l = 1 .. L-2:
+//          D2a  res = r - (6 t - s(t))                        (fluid)
+//          D2b  r[l+1] = 1/2 sum of the 2x2x2 children's res  (fluid coarse cells),
+//               and t[l+1] = OMEGA r[l+1] / D in the same pass
+//   coarsest level L-1:  e = M r, M the dense inverse (or 64 Jacobi sweeps)
+//   up, level l = L-2 .. 1:
+//          U1   t = OMEGA r / D + alpha e[l+1][parent]        (fluid)
+//          U2   e = t + OMEGA (r - (6 t - s(t))) / D          (fluid; 0 elsewhere)
+//
+// with s(t) = sum of the six neighbours' t + n_solid x centre t (t is 0 on
+// every non-fluid cell and outside the grid, which gives the reference's
+// boundary rule: fluid -> value, air -> 0, solid -> centre value).  These are
+// the operations of the level-0 kernels (mgfine.cu) and of the per-level row
+// kernels (solver.cu).  Phases on levels with more than TAIL_CELLS cells are
+// spread over the whole grid and separated by the bounded grid barrier; the
+// small levels below run in CTA 0 alone with __syncthreads between phases,
+// while the other CTAs wait at the next grid barrier.  Every phase works on
+// quads of 4 consecutive k cells (vector loads, nz % 4 == 0 on every level);
+// t and res live in an FP32 scratch vector.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "bsp_common.cuh"
+#include "grid_sync.cuh"
+#include "solver.cuh"
+
+namespace bsp {
+
+constexpr int CC_THREADS = 1024;
+constexpr int TAIL_CELLS = 16384;
+constexpr float CC_OMEGA = 6.0f / 7.0f;
+constexpr int CC_COARSE_SWEEPS = 64;
+
+__device__ __forceinline__ float cl(const float *p, int64_t c) { return p[c]; }
+__device__ __forceinline__ float cl(const __half *p, int64_t c) { return __half2float(p[c]); }
+__device__ __forceinline__ float cl(const __nv_bfloat16 *p, int64_t c) {
+  return __bfloat162float(p[c]);
+}
+__device__ __forceinline__ void cs(float *p, int64_t c, float v) { p[c] = v; }
+__device__ __forceinline__ void cs(__half *p, int64_t c, float v) { p[c] = __float2half_rn(v); }
+__device__ __forceinline__ void cs(__nv_bfloat16 *p, int64_t c, float v) {
+  p[c] = __float2bfloat16_rn(v);
+}
+// value as it reads back after a store through T
+__device__ __forceinline__ float cl_round(float v, const float *) { return v; }
+__device__ __forceinline__ float cl_round(float v, const __half *) {
+  return __half2float(__float2half_rn(v));
+}
+__device__ __forceinline__ float cl_round(float v, const __nv_bfloat16 *) {
+  return __bfloat162float(__float2bfloat16_rn(v));
+}
+
+template <class T>
+struct CoarseCycle {
+  Level<T> lv[MAX_LEVELS];
+  int L;
+  float *scratch;     // FP32 t, >= max(cells of level 1, 3 x cells of the coarsest level)
+  float *res;         // FP32 residuals of the restriction, >= cells of level 1
+  const float *cinv;  // coarsest dense inverse, symmetric, n x n
+  const int *cflag;   // 1: cinv valid
+  GridCtl *ctl;
+  float alpha;
+};
+
+struct Span {  // the warps that share a phase: warp w0 of nw
+  int w0, nw;
+};
+
+// OMEGA / (6 - n_solid) of a mask byte (0 when no neighbour is non-solid).
+__device__ __forceinline__ float cc_w(const float *wtab, uint32_t m) { return wtab[m & 7u]; }
+__device__ __forceinline__ float f4(const float4 &v, int q) {
+  return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ float4 ld4f(const float *p, int64_t c) {
+  return *reinterpret_cast<const float4 *>(p + c);
+}
+__device__ __forceinline__ void st4f(float *p, int64_t c, float4 v) {
+  *reinterpret_cast<float4 *>(p + c) = v;
+}
+__device__ __forceinline__ float4 ld4t(const float *p, int64_t c) { return ld4f(p, c); }
+__device__ __forceinline__ float4 ld4t(const __half *p, int64_t c) {
+  const uint2 u = *reinterpret_cast<const uint2 *>(p + c);
+  const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&u.x));
+  const float2 b = __half22float2(*reinterpret_cast<const __half2 *>(&u.y));
+  return make_float4(a.x, a.y, b.x, b.y);
+}
+__device__ __forceinline__ float4 ld4t(const __nv_bfloat16 *p, int64_t c) {
+  const uint2 u = *reinterpret_cast<const uint2 *>(p + c);
+  const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.x));
+  const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162 *>(&u.y));
+  return make_float4(a.x, a.y, b.x, b.y);
+}
+// Stores 4 values through T and returns them as they read back.
+template <class T>
+__device__ __forceinline__ float4 st4t(T *p, int64_t c, float4 v) {
+  cs(p, c, v.x);
+  cs(p, c + 1, v.y);
+  cs(p, c + 2, v.z);
+  cs(p, c + 3, v.w);
+  return make_float4(cl_round(v.x, p), cl_round(v.y, p), cl_round(v.z, p), cl_round(v.w, p));
+}
+__device__ __forceinline__ uint32_t ldm4(const uint8_t *m, int64_t c) {
+  return __ldg(reinterpret_cast<const uint32_t *>(m + c));
+}
+__device__ __forceinline__ float fl_mask(float v, uint32_t mw, int q) {
+  return ((mw >> (8 * q)) & BSP_MFLUID) ? v : 0.0f;
+}
+
+// Calls fn(i, j, k, c) for every quad (4 consecutive k cells, k % 4 == 0) of an
+// (nx, ny, nz) grid with nz % 4 == 0, spread over the span's warps: a warp
+// covers 32 / (nz/4) rows at a time when a row has fewer than 32 quads.
+template <class Fn>
+__device__ __forceinline__ void for_quads(int nx, int ny, int nz, Span sp, Fn fn) {
+  const int lane = threadIdx.x & 31;
+  const int nzq = nz >> 2;
+  const int rows = nx * ny;
+  if (nzq >= 32) {
+    for (int row = sp.w0; row < rows; row += sp.nw) {
+      const int i = row / ny, j = row - i * ny;
+      for (int kq = lane; kq < nzq; kq += 32) fn(i, j, 4 * kq, (int64_t)row * nz + 4 * kq);
+    }
+    return;
+  }
+  const int rpw = 32 / nzq, sub = lane / nzq, kq = lane - sub * nzq;
+  if (sub >= rpw) return;
+#pragma unroll 2
+  for (int row0 = sp.w0 * rpw; row0 < rows; row0 += sp.nw * rpw) {
+    const int row = row0 + sub;
+    if (row < rows) {
+      const int i = row / ny, j = row - i * ny;
+      fn(i, j, 4 * kq, (int64_t)row * nz + 4 * kq);
+    }
+  }
+}
+
+// Centre t and neighbour sum (without the n_solid term) of the 4 cells of a quad.
+template <class T>
+__device__ __forceinline__ void quad_nbr(const float *__restrict__ t, const Level<T> &f, int i,
+                                         int j, int k, int64_t c, float4 &tc, float (&s)[4]) {
+  const int64_t plane = (int64_t)f.ny * f.nz;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  tc = ld4f(t, c);
+  const float4 a = i > 0 ? ld4f(t, c - plane) : z4;
+  const float4 b = i + 1 < f.nx ? ld4f(t, c + plane) : z4;
+  const float4 d = j > 0 ? ld4f(t, c - f.nz) : z4;
+  const float4 u = j + 1 < f.ny ? ld4f(t, c + f.nz) : z4;
+  const float km = k > 0 ? t[c - 1] : 0.0f;
+  const float kp = k + 4 < f.nz ? t[c + 4] : 0.0f;
+  const float4 lo = make_float4(km, tc.x, tc.y, tc.z), hi = make_float4(tc.y, tc.z, tc.w, kp);
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    s[q] = ((f4(a, q) + f4(b, q)) + (f4(d, q) + f4(u, q))) + (f4(lo, q) + f4(hi, q));
+}
+
+// D1: t = OMEGA r / D on fluid cells.
+template <class T>
+__device__ void phase_d1(const Level<T> &f, float *__restrict__ t, const float *wtab, Span sp) {
+  for_quads(f.nx, f.ny, f.nz, sp, [&](int, int, int, int64_t c) {
+    const uint32_t m = ldm4(f.mask, c);
+    const float4 r = ld4t(f.r, c);
+    float v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = fl_mask(f4(r, q) * cc_w(wtab, m >> (8 * q)), m, q);
+    st4f(t, c, make_float4(v[0], v[1], v[2], v[3]));
+  });
+}
+
+// D2a: res = r - (6 t - s(t)) on fluid cells.
+template <class T>
+__device__ void phase_d2a(const Level<T> &f, const float *__restrict__ t, float *__restrict__ res,
+                          Span sp) {
+  for_quads(f.nx, f.ny, f.nz, sp, [&](int i, int j, int k, int64_t c) {
+    const uint32_t m = ldm4(f.mask, c);
+    const float4 r = ld4t(f.r, c);
+    float4 tc;
+    float s[4];
+    quad_nbr(t, f, i, j, k, c, tc, s);
+    float v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float sq = fmaf((float)((m >> (8 * q)) & 7u), f4(tc, q), s[q]);
+      v[q] = fl_mask(f4(r, q) - (6.0f * f4(tc, q) - sq), m, q);
+    }
+    st4f(res, c, make_float4(v[0], v[1], v[2], v[3]));
+  });
+}
+
+// D2b: r[l+1] = 1/2 sum of the 2x2x2 children's res (fluid coarse cells), and
+// the next level's D1, t[l+1] = OMEGA r[l+1] / D, in the same pass.
+template <class T>
+__device__ void phase_d2b(const Level<T> &f, const Level<T> &co, const float *__restrict__ res,
+                          float *__restrict__ t, const float *wtab, Span sp) {
+  for_quads(co.nx, co.ny, co.nz, sp, [&](int I, int J, int K, int64_t C) {
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const int i = 2 * I + a, j = 2 * J + b;
+        if (i < f.nx && j < f.ny) {
+          const int64_t c = ((int64_t)i * f.ny + j) * f.nz + 2 * K;
+          const float4 p = ld4f(res, c), q = ld4f(res, c + 4);
+          acc[0] += p.x + p.y;
+          acc[1] += p.z + p.w;
+          acc[2] += q.x + q.y;
+          acc[3] += q.z + q.w;
+        }
+      }
+    const uint32_t m = ldm4(co.mask, C);
+    float rv[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) rv[q] = fl_mask(0.5f * acc[q], m, q);
+    const float4 stored = st4t(co.r, C, make_float4(rv[0], rv[1], rv[2], rv[3]));
+    float v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) v[q] = f4(stored, q) * cc_w(wtab, m >> (8 * q));
+    st4f(t, C, make_float4(v[0], v[1], v[2], v[3]));
+  });
+}
+
+// U1: t = OMEGA r / D + alpha e[l+1][parent] on fluid cells.
+template <class T>
+__device__ void phase_u1(const Level<T> &f, const Level<T> &co, float *__restrict__ t,
+                         const float *wtab, float alpha, Span sp) {
+  for_quads(f.nx, f.ny, f.nz, sp, [&](int i, int j, int k, int64_t c) {
+    const uint32_t m = ldm4(f.mask, c);
+    const float4 r = ld4t(f.r, c);
+    const int64_t P = ((int64_t)(i >> 1) * co.ny + (j >> 1)) * co.nz + (k >> 1);
+    const float e0 = alpha * cl(co.e, P), e1 = alpha * cl(co.e, P + 1);
+    float v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      v[q] = fl_mask(fmaf(f4(r, q), cc_w(wtab, m >> (8 * q)), q < 2 ? e0 : e1), m, q);
+    st4f(t, c, make_float4(v[0], v[1], v[2], v[3]));
+  });
+}
+
+// U2: e = t + OMEGA (r - (6 t - s(t))) / D on fluid cells, 0 elsewhere.
+template <class T>
+__device__ void phase_u2(const Level<T> &f, const float *__restrict__ t, const float *wtab,
+                         Span sp) {
+  for_quads(f.nx, f.ny, f.nz, sp, [&](int i, int j, int k, int64_t c) {
+    const uint32_t m = ldm4(f.mask, c);
+    const float4 r = ld4t(f.r, c);
+    float4 tc;
+    float s[4];
+    quad_nbr(t, f, i, j, k, c, tc, s);
+    float v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float sq = fmaf((float)((m >> (8 * q)) & 7u), f4(tc, q), s[q]);
+      v[q] = fl_mask(fmaf(f4(r, q) - (6.0f * f4(tc, q) - sq), cc_w(wtab, m >> (8 * q)),
+                          f4(tc, q)),
+                     m, q);
+    }
+    st4t(f.e, c, make_float4(v[0], v[1], v[2], v[3]));
+  });
+}
+
+// Scalar neighbour sum for the coarsest-level sweeps.
+template <class T>
+__device__ __forceinline__ float nbr_sum1(const float *t, const Level<T> &f, int i, int j, int k,
+                                          int c) {
+  const int plane = f.ny * f.nz;
+  const float a = i > 0 ? t[c - plane] : 0.0f;
+  const float b = i + 1 < f.nx ? t[c + plane] : 0.0f;
+  const float d = j > 0 ? t[c - f.nz] : 0.0f;
+  const float u = j + 1 < f.ny ? t[c + f.nz] : 0.0f;
+  const float bk = k > 0 ? t[c - 1] : 0.0f;
+  const float fk = k + 1 < f.nz ? t[c + 1] : 0.0f;
+  return ((a + b) + (d + u)) + (bk + fk);
+}
+
+// Coarsest level, by CTA 0: e = M r with the symmetric dense inverse (warp per
+// output, lanes over the sum, fixed shuffle order), or, without one, damped
+// Jacobi sweeps from zero in the scratch vector.
+template <class T>
+__device__ void coarsest_solve(const CoarseCycle<T> &a, const float *wtab) {
+  const Level<T> &c = a.lv[a.L - 1];
+  const int n = c.nx * c.ny * c.nz;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (*a.cflag) {
+    for (int o = warp; o < n; o += nw) {
+      float acc = 0.0f;
+      for (int q = lane; q < n; q += 32) acc = fmaf(a.cinv[(int64_t)o * n + q], cl(c.r, q), acc);
+      for (int s = 16; s > 0; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s);
+      if (lane == 0) cs(c.e, o, (__ldg(c.mask + o) & BSP_MFLUID) ? acc : 0.0f);
+    }
+    return;
+  }
+  float *e0 = a.scratch, *e1 = a.scratch + n;
+  for (int q = threadIdx.x; q < n; q += blockDim.x) e0[q] = 0.0f;
+  __syncthreads();
+  for (int sw = 0; sw < CC_COARSE_SWEEPS; ++sw) {
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+      const uint32_t m = __ldg(c.mask + q);
+      float v = 0.0f;
+      if (m & BSP_MFLUID) {
+        const int k = q % c.nz, j = (q / c.nz) % c.ny, i = q / (c.nz * c.ny);
+        const float ec = e0[q];
+        const float s = fmaf((float)(m & 7u), ec, nbr_sum1(e0, c, i, j, k, q));
+        v = fmaf(cl(c.r, q) - (6.0f * ec - s), cc_w(wtab, m), ec);
+      }
+      e1[q] = v;
+    }
+    __syncthreads();
+    float *tmp = e0;
+    e0 = e1;
+    e1 = tmp;
+  }
+  for (int q = threadIdx.x; q < n; q += blockDim.x) cs(c.e, q, e0[q]);
+}
+
+template <class T>
+__global__ void __launch_bounds__(CC_THREADS, 1) mg_cycle_kernel(CoarseCycle<T> a,
+                                                                 SolverState *st) {
+  if (st->inner_done) return;  // uniform over the grid
+  __shared__ float wtab[8];
+  if (threadIdx.x < 8) {
+    const float d = 6.0f - (float)threadIdx.x;
+    wtab[threadIdx.x] = d > 0.0f ? __fdividef(CC_OMEGA, d) : 0.0f;
+  }
+  __syncthreads();
+  const int wpb = blockDim.x >> 5;
+  const Span all{(int)(blockIdx.x * wpb + (threadIdx.x >> 5)), (int)(gridDim.x * wpb)};
+  const Span one{(int)(threadIdx.x >> 5), wpb};
+  const int L = a.L;
+  auto cells = [&](int l) { return (int64_t)a.lv[l].nx * a.lv[l].ny * a.lv[l].nz; };
+  // levels >= tail run in CTA 0 alone
+  int tail = 1;
+  while (tail < L && cells(tail) > TAIL_CELLS) ++tail;
+  bool ok = true;
+  auto sync_all = [&]() {
+    if (ok && !grid_barrier(a.ctl)) ok = false;
+  };
+  // ---- down: t of level 1, then per level the residual pass and the
+  // restriction (which also forms t of the next level)
+  if (L > 2) {
+    if (1 < tail) {
+      phase_d1(a.lv[1], a.scratch, wtab, all);
+      sync_all();
+    } else if (blockIdx.x == 0) {
+      phase_d1(a.lv[1], a.scratch, wtab, one);
+      __syncthreads();
+    }
+  }
+  for (int l = 1; l + 1 < L && ok; ++l) {
+    if (l < tail) {
+      phase_d2a(a.lv[l], a.scratch, a.res, all);
+      sync_all();
+      phase_d2b(a.lv[l], a.lv[l + 1], a.res, a.scratch, wtab, all);
+      sync_all();
+    } else if (blockIdx.x == 0) {
+      phase_d2a(a.lv[l], a.scratch, a.res, one);
+      __syncthreads();
+      phase_d2b(a.lv[l], a.lv[l + 1], a.res, a.scratch, wtab, one);
+      __syncthreads();
+    }
+  }
+  if (blockIdx.x == 0 && ok) {
+    coarsest_solve(a, wtab);
+    __syncthreads();
+    for (int l = L - 2; l >= tail && l >= 1; --l) {
+      phase_u1(a.lv[l], a.lv[l + 1], a.scratch, wtab, a.alpha, one);
+      __syncthreads();
+      phase_u2(a.lv[l], a.scratch, wtab, one);
+      __syncthreads();
+    }
+  }
+  // ---- up through the big levels
+  const int top = min(tail, L - 1) - 1;  // highest-index big level still to prolongate
+  if (top >= 1) sync_all();
+  for (int l = top; l >= 1 && ok; --l) {
+    phase_u1(a.lv[l], a.lv[l + 1], a.scratch, wtab, a.alpha, all);
+    sync_all();
+    phase_u2(a.lv[l], a.scratch, wtab, all);
+    if (l > 1) sync_all();
+  }
+  if (!ok && threadIdx.x == 0) atomicExch(&st->dev_error, 1);
+}
+
+bool g_coarse_fused_enabled = true;  // BSP_TUNE_COARSE_FUSED
+
+// FP32 scratch of the coarse-cycle kernel: t (max(cells of level 1, 3 x cells
+// of the coarsest level), rounded up to 64 floats) followed by res (cells of
+// level 1).
+size_t coarse_cycle_scratch_floats(const int *dims, int L) {
+  if (L < 2) return 0;
+  const size_t n1 = (size_t)dims[3] * dims[4] * dims[5];
+  const size_t nc = (size_t)dims[3 * (L - 1)] * dims[3 * (L - 1) + 1] * dims[3 * (L - 1) + 2];
+  const size_t t = ((n1 > 3 * nc ? n1 : 3 * nc) + 63) / 64 * 64;
+  return t + n1;
+}
+
+// Launch the coarse part of a V-cycle (levels 1 .. L-1) as one cooperative
+// kernel.  Returns false (nothing launched) when the fused path is off, a
+// level below level 0 has nz % 4 != 0 (the phases work on 4-cell quads) or the
+// grid cannot be co-resident; the caller then runs the per-level kernels.
+template <class T>
+bool launch_coarse_cycle(const Level<T> *lv, int L, float *scratch, const float *cinv,
+                         const int *cflag, void *ctl, float alpha, SolverState *st,
+                         cudaStream_t s) {
+  if (!g_coarse_fused_enabled || L < 2) return false;
+  for (int l = 1; l < L; ++l) {
+    if ((int64_t)lv[l].nx * lv[l].ny * lv[l].nz >= ((int64_t)1 << 31)) return false;
+    if (lv[l].nz % 4) return false;
+  }
+  static int blocks = -1;
+  if (blocks < 0) {
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, mg_cycle_kernel<T>, CC_THREADS, 0) !=
+            cudaSuccess ||
+        per < 1)
+      blocks = 0;
+    else
+      blocks = sms;
+  }
+  if (blocks <= 0) return false;
+  CoarseCycle<T> a{};
+  int dims[3 * MAX_LEVELS];
+  for (int l = 0; l < L; ++l) {
+    a.lv[l] = lv[l];
+    dims[3 * l] = lv[l].nx;
+    dims[3 * l + 1] = lv[l].ny;
+    dims[3 * l + 2] = lv[l].nz;
+  }
+  a.L = L;
+  const size_t n1 = (size_t)lv[1].nx * lv[1].ny * lv[1].nz;
+  a.scratch = scratch;
+  a.res = scratch + (coarse_cycle_scratch_floats(dims, L) - n1);
+  a.cinv = cinv;
+  a.cflag = cflag;
+  a.ctl = reinterpret_cast<GridCtl *>(ctl);
+  a.alpha = alpha;
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(CC_THREADS);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, mg_cycle_kernel<T>, a, st) == cudaSuccess;
+}
+
+#define INST(T)                                                                             \
+  template bool launch_coarse_cycle<T>(const Level<T> *, int, float *, const float *,       \
+                                       const int *, void *, float, SolverState *, cudaStream_t);
+INST(float)
+INST(__half)
+INST(__nv_bfloat16)
+#undef INST
+
+}  // namespace bsp

@@ -48,7 +48,8 @@ bool g_fine_col_enabled = true;
 // coarse part alpha P A_c^-1 R is positive semi-definite and the damped
 // Jacobi smoother is convergent.
 float g_mg_alpha = 1.0f;
-extern bool g_fine_tma_enabled;  // BSP_TUNE_FINE_TMA (mgfine.cu)
+extern bool g_fine_tma_enabled;      // BSP_TUNE_FINE_TMA (mgfine.cu)
+extern bool g_coarse_fused_enabled;  // BSP_TUNE_COARSE_FUSED (mgcoarse.cu)
 constexpr int COARSE_SWEEPS = 64;
 constexpr int RED_THREADS = 256;
 
@@ -328,7 +329,12 @@ __global__ void __launch_bounds__(1024) coarse_invert_kernel(Level<T> L, double 
     }
     __syncthreads();
   }
-  for (int q = threadIdx.x; q < n * n; q += blockDim.x) minv[q] = (float)A[q];
+  // stored symmetric (A^-1 is; Gauss-Jordan rounding is not), so the coarsest
+  // solve keeps the V-cycle a symmetric preconditioner
+  for (int q = threadIdx.x; q < n * n; q += blockDim.x) {
+    const int r = q / n, c = q - r * n;
+    minv[q] = (float)(0.5 * (A[q] + A[(int64_t)c * n + r]));
+  }
   if (threadIdx.x == 0) *flag = 1;
 }
 
@@ -701,9 +707,10 @@ size_t storage_bytes(int storage) { return storage == BSP_STORE_FP32 ? 4 : 2; }
 //   | per level l >= 1 ... ; level-0 effective-class scratch reuses the level-1 slot order.
 //   | coarsest-level dense inverse (float), its FP64 build scratch, direct flag
 //   | per-level column-tile fluid flags (PARTIAL_STRIDE bytes per level)
+//   | FP32 scratch and grid-barrier word of the coarse-cycle kernel
 struct Layout {
   size_t state, partials, x, e, z, ps0, ps1, Ap, r, lvl_mask[MAX_LEVELS], lvl_r[MAX_LEVELS],
-      lvl_e[MAX_LEVELS], eff0, cinv, cA, cflag, tflags, total;
+      lvl_e[MAX_LEVELS], eff0, cinv, cA, cflag, tflags, cscratch, cctl, total;
   int L, dims[3 * MAX_LEVELS];
 };
 
@@ -742,6 +749,8 @@ Layout make_layout(int nx, int ny, int nz, int storage) {
     lo.cflag = take(sizeof(int));
   }
   lo.tflags = take((size_t)MAX_LEVELS * PARTIAL_STRIDE);  // column-tile fluid flags per level
+  lo.cscratch = take(sizeof(float) * coarse_cycle_scratch_floats(lo.dims, lo.L));
+  lo.cctl = take(64);  // grid barrier of the coarse-cycle kernel
   lo.total = off;
   return lo;
 }
@@ -833,6 +842,7 @@ cudaError_t setup_levels(Ctx<T> &cx, cudaStream_t s) {
     const size_t ts = sizeof(T);
     cudaMemsetAsync(cx.base + cx.lo.z, 0, cx.lo.r + ts * cx.n - cx.lo.z, s);  // z ps0 ps1 Ap r
     cudaMemsetAsync(cx.base + cx.lo.e, 0, sizeof(float) * cx.n, s);
+    cudaMemsetAsync(cx.base + cx.lo.cctl, 0, 64, s);
     for (int l = 1; l < cx.lo.L; ++l) {
       const Level<T> &c = cx.lv[l];
       const size_t nl = (size_t)c.nx * c.ny * c.nz;
@@ -875,30 +885,44 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
            (int64_t)v.nx * v.ny * v.nz >= 131072 &&
            fine_grid_blocks(v.nx, v.ny, v.nz) <= PARTIAL_STRIDE;
   };
-  // V-cycle on r -> z
-  for (int l = 0; l + 1 < L; ++l) {
+  // V-cycle on r -> z: level-0 restriction, the coarse levels (one
+  // cooperative kernel, or one kernel per level and direction), level-0
+  // prolongation
+  auto down = [&](int l) {
     Level<T> &f = cx.lv[l], &c = cx.lv[l + 1];
     ProfScope ps(l == 0 ? PROF_MG_DOWN0 : PROF_MG_COARSE, s);
     if (level_col(l))
       launch_fine_down<T>(f, c, st, s);
     else
       mg_down_kernel<T><<<row_blocks((int64_t)c.nx * c.ny), 256, 0, s>>>(f, c, st);
-  }
+  };
+  down(0);
+  bool fused;
   {
-    Level<T> &c = cx.lv[L - 1];
-    const int n = c.nx * c.ny * c.nz;
     ProfScope ps(PROF_MG_COARSE, s);
-    mg_coarse_kernel<T><<<1, 512, 3 * n * sizeof(float), s>>>(
-        c, (const float *)(cx.base + cx.lo.cinv), (const int *)(cx.base + cx.lo.cflag), st);
+    fused = launch_coarse_cycle<T>(cx.lv, L, (float *)(cx.base + cx.lo.cscratch),
+                                   (const float *)(cx.base + cx.lo.cinv),
+                                   (const int *)(cx.base + cx.lo.cflag), cx.base + cx.lo.cctl,
+                                   g_mg_alpha, st, s);
   }
-  for (int l = L - 2; l >= 1; --l) {
-    Level<T> &f = cx.lv[l], &c = cx.lv[l + 1];
-    ProfScope ps(PROF_MG_COARSE, s);
-    if (level_col(l))  // its r.e partial is written but unused
-      launch_fine_up<T>(f, c, f.e, cx.partials, g_mg_alpha, st, s);
-    else
-      mg_up_kernel<T, false><<<row_blocks((int64_t)f.nx * f.ny), 256, 0, s>>>(
-          f, c, f.e, cx.partials, st, g_mg_alpha);
+  if (!fused) {
+    for (int l = 1; l + 1 < L; ++l) down(l);
+    {
+      Level<T> &c = cx.lv[L - 1];
+      const int n = c.nx * c.ny * c.nz;
+      ProfScope ps(PROF_MG_COARSE, s);
+      mg_coarse_kernel<T><<<1, 512, 3 * n * sizeof(float), s>>>(
+          c, (const float *)(cx.base + cx.lo.cinv), (const int *)(cx.base + cx.lo.cflag), st);
+    }
+    for (int l = L - 2; l >= 1; --l) {
+      Level<T> &f = cx.lv[l], &c = cx.lv[l + 1];
+      ProfScope ps(PROF_MG_COARSE, s);
+      if (level_col(l))  // its r.e partial is written but unused
+        launch_fine_up<T>(f, c, f.e, cx.partials, g_mg_alpha, st, s);
+      else
+        mg_up_kernel<T, false><<<row_blocks((int64_t)f.nx * f.ny), 256, 0, s>>>(
+            f, c, f.e, cx.partials, st, g_mg_alpha);
+    }
   }
   T *z = (T *)(cx.base + cx.lo.z);
   const int nb0 = col ? fine_grid_blocks(cx.nx, cx.ny, cx.nz) : row_blocks((int64_t)cx.nx * cx.ny);
@@ -1363,6 +1387,7 @@ static void key_params(GraphKey &k, const BspSolveParams *p) {
   k.v.push_back((uintptr_t)a);
   k.v.push_back((uintptr_t)g_fine_col_enabled);
   k.v.push_back((uintptr_t)g_fine_tma_enabled);
+  k.v.push_back((uintptr_t)g_coarse_fused_enabled);
 }
 
 }  // namespace bsp

@@ -60,6 +60,13 @@ template <class T>
 int launch_cg_update_col(int nx, int ny, int nz, const uint8_t *tiles, float *e, T *r,
                          const T *ps, const T *Ap, double *partials, const SolverState *st,
                          cudaStream_t s);
+// The coarse part of a V-cycle (levels 1 .. L-1) as one cooperative kernel
+// (mgcoarse.cu); false when not launched (the per-level kernels then run).
+template <class T>
+bool launch_coarse_cycle(const Level<T> *lv, int L, float *scratch, const float *cinv,
+                         const int *cflag, void *ctl, float alpha, SolverState *st,
+                         cudaStream_t s);
+size_t coarse_cycle_scratch_floats(const int *dims, int L);
 // One flag byte per column tile: any fluid cell in the tile.
 void launch_tile_flags(int nx, int ny, int nz, const uint8_t *mask, uint8_t *flags,
                        cudaStream_t s);

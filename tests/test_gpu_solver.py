@@ -114,6 +114,32 @@ def test_tma_and_shared_plane_kernels_bit_identical(cuda, storage, spec):
     assert np.array_equal(out[1][2], out[0][2])
 
 
+@pytest.mark.parametrize("storage", ["fp32", "bf16"])
+@pytest.mark.parametrize("spec", [S.POT_64, S.pot_192(3)], ids=["pot64", "pot192"])
+def test_fused_coarse_cycle_matches_per_level_kernels(cuda, storage, spec):
+    """The one-launch coarse V-cycle (cooperative kernel) and the per-level
+    kernels apply the same operator (sums in another order): same convergence
+    and the same solution to the tolerance."""
+    from boilingsim_b200 import _lib
+
+    mat = S.pot_mat(spec)
+    ux, uy, uz = S.velocity_field(mat, seed=9)
+    div = O.divergence(ux, uy, uz, mat, DX)
+    out = {}
+    try:
+        for fused in (1, 0):
+            _lib.call("bsp_set_tuning", 5, fused)
+            res = solve_tolerance(div, mat, DX, DT, RHO, tol=1e-7, storage=storage)
+            assert res.status == 0
+            assert O.rel_residual64(res.p64, div, mat, DX, DT, RHO) <= 1e-7 * 1.0001
+            out[fused] = res
+    finally:
+        _lib.call("bsp_set_tuning", 5, 1)
+    slack = 2 if storage == "fp32" else max(3, out[0].inner_iterations // 8)
+    assert abs(out[1].inner_iterations - out[0].inner_iterations) <= slack
+    assert O.rel_error(out[1].p64, out[0].p64, mat) < 1e-5
+
+
 @pytest.mark.parametrize("spec", [S.pot_192(2), S.PotSpec(70, 54, 37, 22, 3, 29, 5, 20),
                                   S.PotSpec(66, 50, 44, 20, 3, 33, 5, 20)],
                          ids=["pot192", "odd70x54x37", "odd_ny66x50x44"])
