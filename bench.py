@@ -239,6 +239,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--storage", default="fp32", choices=["fp32", "fp16", "bf16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--graph", action="store_true",
+                    help="run each solve as one device-driven CUDA graph")
     ap.add_argument("--ref-iters", type=int, default=0,
                     help="reference PCG iteration count to use instead of measuring it")
     ap.add_argument("--skip-extras", action="store_true",
@@ -305,11 +307,11 @@ def main():
     stream = torch.cuda.current_stream()
     last = {}
 
-    def step():
+    def step(graph=args.graph):
         for a, b in zip(u, u0):
             a.copy_(b, non_blocking=True)
         F.compute_divergence(div, *u, mask, DX)
-        res = solver.solve(div, DX, DT, RHO, tol=TOL, p=p)
+        res = solver.solve(div, DX, DT, RHO, tol=TOL, p=p, graph=graph)
         F.subtract_pressure_gradient(*u, p, mask, DX, DT, RHO)
         F.compute_divergence(div, *u, mask, DX, max_div)
         last["res"] = res
@@ -362,10 +364,11 @@ def main():
     clk = clocks.stop()
     # Per-kernel-class breakdown: the same steps again with the library's event
     # timing on (two events around every launch; not part of the timed value).
+    # Host-driven: event timing is suspended inside graphs.
     _lib.call("bsp_profile_enable", 1)
     _lib.lib().bsp_profile_read(None, None, 0)  # clear
     for _ in range(args.steps):
-        step()
+        step(graph=False)
     torch.cuda.synchronize()
     _lib.call("bsp_profile_enable", 0)
     _lib.lib().bsp_profile_read(prof_ms, prof_n, ncls)

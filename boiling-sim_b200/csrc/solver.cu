@@ -766,6 +766,10 @@ struct Ctx {
   int64_t n;
   const uint8_t *mask0;
   bool col;  // level-0 kernels on the column layout (nz % 4 == 0, aligned mask)
+  // the coarse levels may run as one cooperative kernel, which needs the
+  // whole GPU: not while other instances' kernels run beside it (batched
+  // graphs with parallel branches)
+  bool coop = true;
 };
 
 template <class T>
@@ -900,7 +904,7 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
   bool fused;
   {
     ProfScope ps(PROF_MG_COARSE, s);
-    fused = launch_coarse_cycle<T>(cx.lv, L, (float *)(cx.base + cx.lo.cscratch),
+    fused = cx.coop && launch_coarse_cycle<T>(cx.lv, L, (float *)(cx.base + cx.lo.cscratch),
                                    (const float *)(cx.base + cx.lo.cinv),
                                    (const int *)(cx.base + cx.lo.cflag), cx.base + cx.lo.cctl,
                                    g_mg_alpha, st, s);
@@ -1329,6 +1333,7 @@ int solve_graph_batch(int count, const BspBatchItem *items, const BspSolveParams
   for (int q = 0; q < count; ++q) {
     const BspBatchItem &it = items[q];
     Ctx<T> cx = make_ctx<T>(it.workspace, it.mask, it.nx, it.ny, it.nz, prm->storage);
+    cx.coop = count == 1;
     const Level<T> &c = cx.lv[cx.lo.L - 1];
     if ((int64_t)c.nx * c.ny * c.nz > COARSEST_MAX) return BSP_ERR_SHAPE;
     if (!(prm->reuse_setup &&

@@ -22,11 +22,15 @@ def _scene(spec, seed):
     return mat, O.divergence(ux, uy, uz, mat, DX)
 
 
-@pytest.mark.parametrize("storage", ["fp32", "fp16"])
-def test_graph_solve_matches_host_driven_solve(cuda, storage):
+@pytest.mark.parametrize("storage,spec", [("fp32", S.POT_64), ("fp16", S.POT_64),
+                                          ("fp32", S.pot_192(3))],
+                         ids=["pot64-fp32", "pot64-fp16", "pot192-fp32"])
+def test_graph_solve_matches_host_driven_solve(cuda, storage, spec):
     """Same kernels in the same order: the graph-driven solve reproduces the
-    host-driven one bit for bit, and replaying the graph does too."""
-    mat, div = _scene(S.POT_64, 7)
+    host-driven one bit for bit, and replaying the graph does too.  The 192
+    pot (nz % 4 == 0 on every level) runs the coarse levels as one cooperative
+    kernel inside the graph's WHILE body."""
+    mat, div = _scene(spec, 7)
     solver = TolSolver(cell_mask(torch.as_tensor(mat).cuda()), storage)
     d = torch.as_tensor(div).cuda()
     r1 = solver.solve(d, DX, DT, RHO, tol=1e-6)
