@@ -394,7 +394,10 @@ def main():
                   4: (4 + 3 * ts + 4 + ts) * n_act,            # e, ps, Ap, r -> e, r
                   5: (13 + (ts + 4) / 2) * n_act,              # mask, x, div; rhat, e (write pass)
                   6: 20.0 * n}                                 # x, e -> x
-    names = {0: "jacobi_sweep", 1: "mg_restrict_fine", 2: "mg_prolong_smooth_fine",
+    if prof_n[4] == 0:
+        # CG update fused into the restriction: r_in, Ap, mask, e, ps -> r_out, e, r_coarse
+        per_launch[1] = (4 * ts + 9 + ts / 8) * n_act
+    names = {0: "jacobi_sweep", 1: "mg_restrict_fine" if prof_n[4] else "cg_update_restrict_fine", 2: "mg_prolong_smooth_fine",
              3: "cg_direction_Ap", 4: "cg_update", 5: "residual_fp64", 6: "x_update_fp64",
              7: "mg_coarse_levels", 8: "control_and_setup", 9: "divergence_gradient"}
     dom = max((c for c in per_launch if prof_n[c] > 0), key=lambda c: prof_ms[c])

@@ -410,7 +410,6 @@ __global__ void __launch_bounds__(TILE_THREADS, 4) fine_tile_kernel(Op op, int n
 int fine_bi(int nx, int ny, int nz);
 dim3 fine_grid(int nx, int ny, int nz);
 
-constexpr int TMA_STAGES = 4;
 constexpr int TMA_ROWS = TILE_ROWS + 2;
 constexpr int MASK_W = 160;
 constexpr int MASK_PAD = 16;
@@ -465,7 +464,7 @@ __device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *map, int
 
 // Tensor maps of one launch.  a, b: fine tensors of T; m: mask; c: coarse T.
 struct TmaMaps {
-  CUtensorMap a, b, m, c;
+  CUtensorMap a, b, m, c, e, p;
 };
 
 // Operand sources read from a stage.  rr: tile row 0..9 (j = j0 - 1 + rr);
@@ -474,6 +473,8 @@ template <class T>
 struct StageView {
   const T *a, *b, *c;
   const uint8_t *m;
+  const float *e;  // EP tiles: 8 output rows x 128 (no halo)
+  const T *ps;
   __device__ uint32_t mask4(int rr, int lane) const {
     return *reinterpret_cast<const uint32_t *>(m + rr * MASK_W + MASK_PAD + lane * 4);
   }
@@ -487,7 +488,8 @@ struct StageView {
 
 template <class T>
 struct TPsAp {
-  static constexpr bool HAS_B = true, HAS_C = false;
+  static constexpr bool HAS_B = true, HAS_C = false, HAS_EP = false;
+  static constexpr int STAGES = 4, MIN_BLOCKS = 3;
   T *cur, *Ap;
   double *partials;
   float beta;
@@ -530,7 +532,8 @@ struct TPsAp {
 
 template <class T>
 struct TUp {
-  static constexpr bool HAS_B = false, HAS_C = true;
+  static constexpr bool HAS_B = false, HAS_C = true, HAS_EP = false;
+  static constexpr int STAGES = 4, MIN_BLOCKS = 4;
   T *z;
   double *partials;
   float alpha;
@@ -574,7 +577,8 @@ struct TUp {
 
 template <class T>
 struct TDown {
-  static constexpr bool HAS_B = false, HAS_C = false;
+  static constexpr bool HAS_B = false, HAS_C = false, HAS_EP = false;
+  static constexpr int STAGES = 4, MIN_BLOCKS = 4;
   const uint8_t *mask1;
   T *r1;
   int nx, ny, ny1, nz1;
@@ -628,6 +632,102 @@ struct TDown {
   __device__ void skip() const {}
 };
 
+// The CG update of the previous iteration fused into the restriction:
+// r_out = r_in - alpha Ap (stored through T and read back, as the separate
+// update kernel), e += alpha ps on the CTA's output cells, partial ||r_out||^2,
+// and the restriction of r_out as TDown.  r_in and r_out are different
+// buffers: the tiles of neighbouring CTAs overlap, so an in-place update
+// could be applied twice.  Without a pending update (first inner iteration of
+// a refinement pass) r_out = r_in.
+template <class T>
+struct TDownU {
+  // e and ps of the 8 output rows come as TMA tiles too (EP); 3 stages keep
+  // three CTAs per SM
+  static constexpr bool HAS_B = true, HAS_C = false, HAS_EP = true;
+  static constexpr int STAGES = 3, MIN_BLOCKS = 3;
+  const uint8_t *mask1;
+  T *r1, *r_out;
+  float *e;
+  const T *ps;
+  double *partials;
+  int nx, ny, ny1, nz1;
+  float alpha;
+  bool upd;
+  float2 acc;
+  double rr;
+  __device__ void init(const SolverState *st) {
+    upd = st->pending != 0;
+    alpha = upd ? (float)st->alpha : 0.0f;
+    acc = make_float2(0.f, 0.f);
+    rr = 0.0;
+  }
+  __device__ float4 rnew4(const StageView<T> &v, int row, int lane) const {
+    const float4 r4 = ld4s(v.a, v.fo(row, lane * 4));
+    if (!upd) return r4;
+    const float4 a4 = ld4s(v.b, v.fo(row, lane * 4));
+    return make_float4(rt(fmaf(-alpha, a4.x, r4.x), r_out), rt(fmaf(-alpha, a4.y, r4.y), r_out),
+                       rt(fmaf(-alpha, a4.z, r4.z), r_out), rt(fmaf(-alpha, a4.w, r4.w), r_out));
+  }
+  __device__ float4 val4(const StageView<T> &v, int row, int lane, uint32_t mw) const {
+    const float4 r4 = rnew4(v, row, lane);
+    return make_float4(r4.x * wdq(mw, 0), r4.y * wdq(mw, 1), r4.z * wdq(mw, 2),
+                       r4.w * wdq(mw, 3));
+  }
+  __device__ float val1(const StageView<T> &v, int row, int kl) const {
+    float rv = ld1s(v.a, v.fo(row, kl));
+    if (upd) rv = rt(fmaf(-alpha, ld1s(v.b, v.fo(row, kl)), rv), r_out);
+    return rv * wdinv_ns(v.mask1(row, kl) & 7u);
+  }
+  __device__ bool pair_end(int i) const { return (i & 1) || i + 1 == nx; }
+  __device__ void emit(const StageView<T> &v, int row, int lane, int i, int, int64_t o,
+                       uint32_t mc, const float4 &e4, const float (&s)[4], float2 *xch) {
+    const float4 r4 = rnew4(v, row, lane);
+    st4s(r_out, o, r4);
+    if (upd) {
+      float4 ee = *reinterpret_cast<const float4 *>(v.e + (row - 1) * 128 + lane * 4);
+      const float4 pp = ld4s(v.ps, (row - 1) * 128 + lane * 4);
+      ee = make_float4(fmaf(alpha, pp.x, ee.x), fmaf(alpha, pp.y, ee.y), fmaf(alpha, pp.z, ee.z),
+                       fmaf(alpha, pp.w, ee.w));
+      *reinterpret_cast<float4 *>(e + o) = ee;
+    }
+    rr += ((double)r4.x * r4.x + (double)r4.y * r4.y) +
+          ((double)r4.z * r4.z + (double)r4.w * r4.w);
+    float res[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float rq = q4(r4, q) - (6.0f * q4(e4, q) - s[q]);
+      res[q] = __uint_as_float(__float_as_uint(rq) & fluid_word(mc, q));
+    }
+    acc.x += res[0] + res[1];
+    acc.y += res[2] + res[3];
+    const int warp = threadIdx.x >> 5;
+    if (pair_end(i) && (warp & 1)) {
+      xch[(warp >> 1) * 32 + lane] = acc;
+      acc = make_float2(0.f, 0.f);
+    }
+  }
+  __device__ void after_step(int i, int j, int k, bool act, float2 *xch) {
+    const int warp = threadIdx.x >> 5;
+    if (!pair_end(i) || (warp & 1)) return;
+    if (act) {
+      float2 t = acc;
+      if (j + 1 < ny) {
+        const float2 o2 = xch[(warp >> 1) * 32 + (threadIdx.x & 31)];
+        t.x += o2.x;
+        t.y += o2.y;
+      }
+      const int64_t C = ((int64_t)(i >> 1) * ny1 + (j >> 1)) * nz1 + (k >> 1);
+      const uint32_t m2 = __ldg(reinterpret_cast<const uint16_t *>(mask1 + C));
+      st2s(r1, C, make_float2((m2 & BSP_MFLUID) ? 0.5f * t.x : 0.0f,
+                              ((m2 >> 8) & BSP_MFLUID) ? 0.5f * t.y : 0.0f));
+    }
+    acc = make_float2(0.f, 0.f);
+  }
+  template <int NW>
+  __device__ void finish(double *sh) { block_partial<NW>(rr, partials, sh); }
+  __device__ void skip() const { partials[block_linear()] = 0.0; }
+};
+
 constexpr int align128(int b) { return (b + 127) / 128 * 128; }
 
 // Every TMA destination starts on a 128-byte boundary.
@@ -635,20 +735,25 @@ template <class T, class Op>
 struct TmaSmem {
   static constexpr int FB = TmaGeom<T>::FBYTES, MB = TmaGeom<T>::MBYTES,
                        CB = TmaGeom<T>::CBYTES;
+  static constexpr int EB = TILE_ROWS * 128 * 4, PB = TILE_ROWS * 128 * (int)sizeof(T);
+  static constexpr int NST = Op::STAGES;
   static constexpr int OFF_B = align128(FB);
   static constexpr int OFF_M = OFF_B + (Op::HAS_B ? align128(FB) : 0);
   static constexpr int OFF_C = OFF_M + align128(MB);
-  static constexpr int STAGE = OFF_C + (Op::HAS_C ? align128(CB) : 0);
-  static constexpr uint32_t TX = (uint32_t)(FB + (Op::HAS_B ? FB : 0) + MB + (Op::HAS_C ? CB : 0));
-  static constexpr int RING = STAGE * TMA_STAGES;
+  static constexpr int OFF_E = OFF_C + (Op::HAS_C ? align128(CB) : 0);
+  static constexpr int OFF_P = OFF_E + (Op::HAS_EP ? EB : 0);
+  static constexpr int STAGE = OFF_P + (Op::HAS_EP ? align128(PB) : 0);
+  static constexpr uint32_t TX = (uint32_t)(FB + (Op::HAS_B ? FB : 0) + MB + (Op::HAS_C ? CB : 0) +
+                                            (Op::HAS_EP ? EB + PB : 0));
+  static constexpr int RING = STAGE * NST;
   // ring | plane_buf (2 x 10 x 32 float4) | mbarriers
   static constexpr int OFF_PLANE = RING;
   static constexpr int OFF_BAR = RING + 2 * TMA_ROWS * 32 * 16;
-  static constexpr int TOTAL = OFF_BAR + TMA_STAGES * 8;
+  static constexpr int TOTAL = OFF_BAR + NST * 8;
 };
 
 template <class T, class Op>
-__global__ void __launch_bounds__(TILE_THREADS, 4) fine_tma_kernel(
+__global__ void __launch_bounds__(TILE_THREADS, Op::MIN_BLOCKS) fine_tma_kernel(
     Op op, const __grid_constant__ TmaMaps maps, int nx, int ny, int nz, int bi,
     const uint8_t *tiles, const SolverState *st) {
   if (st->inner_done) return;  // uniform: the whole grid returns
@@ -673,12 +778,12 @@ __global__ void __launch_bounds__(TILE_THREADS, 4) fine_tma_kernel(
   constexpr int PAD = TmaGeom<T>::PAD;
   if (threadIdx.x < 8) s_wtab[threadIdx.x] = wcalc(threadIdx.x);
   if (producer) {
-    for (int q = 0; q < TMA_STAGES; ++q) mbar_init(&bars[q], 1);
+    for (int q = 0; q < L::NST; ++q) mbar_init(&bars[q], 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
   auto issue = [&](int p) {  // producer only: plane p into its stage
-    const int q = (p - pbase) % TMA_STAGES;
+    const int q = (p - pbase) % L::NST;
     unsigned char *base = dsm + q * L::STAGE;
     mbar_expect_tx(&bars[q], L::TX);
     tma_load3(base, &maps.a, k0 - PAD, j0 - 1, p, &bars[q]);
@@ -686,23 +791,29 @@ __global__ void __launch_bounds__(TILE_THREADS, 4) fine_tma_kernel(
     tma_load3(base + L::OFF_M, &maps.m, k0 - MASK_PAD, j0 - 1, p, &bars[q]);
     if (Op::HAS_C)
       tma_load3(base + L::OFF_C, &maps.c, k0 / 2 - PAD, j0 / 2 - 1, p >> 1, &bars[q]);
+    if (Op::HAS_EP) {
+      tma_load3(base + L::OFF_E, &maps.e, k0, j0, p, &bars[q]);
+      tma_load3(base + L::OFF_P, &maps.p, k0, j0, p, &bars[q]);
+    }
   };
   auto view = [&](int p) {
-    const unsigned char *base = dsm + ((p - pbase) % TMA_STAGES) * L::STAGE;
+    const unsigned char *base = dsm + ((p - pbase) % L::NST) * L::STAGE;
     StageView<T> v;
     v.a = reinterpret_cast<const T *>(base);
     v.b = reinterpret_cast<const T *>(base + L::OFF_B);
     v.m = base + L::OFF_M;
     v.c = reinterpret_cast<const T *>(base + L::OFF_C);
+    v.e = reinterpret_cast<const float *>(base + L::OFF_E);
+    v.ps = reinterpret_cast<const T *>(base + L::OFF_P);
     return v;
   };
   bool ok = true;
   auto wait = [&](int p) {
     const int n = p - pbase;
-    if (!mbar_wait(&bars[n % TMA_STAGES], (uint32_t)((n / TMA_STAGES) & 1))) ok = false;
+    if (!mbar_wait(&bars[n % L::NST], (uint32_t)((n / L::NST) & 1))) ok = false;
   };
   if (producer)
-    for (int p = pbase; p <= min(pbase + TMA_STAGES - 1, i1); ++p) issue(p);
+    for (int p = pbase; p <= min(pbase + L::NST - 1, i1); ++p) issue(p);
   op.init(st);
   // tile row of this warp: 0 = j0-1, 1..8 = output rows, 9 = j0+8
   const int rr = warp < TILE_ROWS ? warp + 1 : (warp == TILE_ROWS ? 0 : TILE_ROWS + 1);
@@ -726,9 +837,9 @@ __global__ void __launch_bounds__(TILE_THREADS, 4) fine_tma_kernel(
   }
   plane_buf[i0 & 1][rr][lane] = vc;
   __syncthreads();
-  if (producer && pbase + TMA_STAGES <= i1) {
+  if (producer && pbase + L::NST <= i1) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    issue(pbase + TMA_STAGES);
+    issue(pbase + L::NST);
   }
   int64_t o = (int64_t)i0 * plane + (int64_t)j * nz + k;
   for (int i = i0; i < i1; ++i) {
@@ -761,9 +872,9 @@ __global__ void __launch_bounds__(TILE_THREADS, 4) fine_tma_kernel(
       if (act) op.emit(v, rr, lane, i, j, o, mc, vc, s, xch);
     }
     __syncthreads();
-    if (producer && i + TMA_STAGES <= i1) {
+    if (producer && i + L::NST <= i1) {
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue(i + TMA_STAGES);
+      issue(i + L::NST);
     }
     if (out) op.after_step(i, j, k, act, xch);
     vm = vc;
@@ -774,7 +885,7 @@ __global__ void __launch_bounds__(TILE_THREADS, 4) fine_tma_kernel(
   if (producer) {
     // every issued plane has been waited for above; confirm (bounded) that no
     // copy is still in flight before the CTA's shared memory goes away
-    for (int p = max(pbase, i1 - TMA_STAGES + 1); p <= i1; ++p) wait(p);
+    for (int p = max(pbase, i1 - L::NST + 1); p <= i1; ++p) wait(p);
   }
   if (!ok) atomicExch(const_cast<int *>(&st->dev_error), 1);
   op.template finish<TILE_WARPS>(sh);
@@ -821,6 +932,7 @@ static bool make_map(CUtensorMap *m, CUtensorMapDataType t, int esize, const voi
 
 // The TMA path needs nz % 16 == 0 (16-byte mask rows) and 16-byte aligned bases.
 static bool tma_eligible(int nz) { return g_fine_tma_enabled && nz % 16 == 0 && encode_tiled(); }
+bool fine_tma_available(int nz) { return tma_eligible(nz); }
 
 template <class T, class Op>
 static bool launch_tma(const Op &op, const TmaMaps &maps, int nx, int ny, int nz,
@@ -1060,6 +1172,38 @@ void launch_fine_down(const Level<T> &f, const Level<T> &c, const SolverState *s
       op, f.nx, f.ny, f.nz, fine_bi(f.nx, f.ny, f.nz), f.tiles, st);
 }
 
+// Level-0 restriction with the previous iteration's CG update fused in (TMA
+// path only; false when it cannot run).  f.r is r_in.
+template <class T>
+bool launch_fine_down_update(const Level<T> &f, const Level<T> &c, T *r_out, float *e,
+                             const T *ps, const T *Ap, double *partials, const SolverState *st,
+                             cudaStream_t s) {
+  if (!tma_eligible(f.nz)) return false;
+  TmaMaps maps{};
+  if (!(make_map(&maps.a, tma_dtype<T>(), sizeof(T), f.r, f.nx, f.ny, f.nz, TmaGeom<T>::FW,
+                 TMA_ROWS) &&
+        make_map(&maps.b, tma_dtype<T>(), sizeof(T), Ap, f.nx, f.ny, f.nz, TmaGeom<T>::FW,
+                 TMA_ROWS) &&
+        make_map(&maps.m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, f.mask, f.nx, f.ny, f.nz, MASK_W,
+                 TMA_ROWS) &&
+        make_map(&maps.e, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, e, f.nx, f.ny, f.nz, 128,
+                 TILE_ROWS) &&
+        make_map(&maps.p, tma_dtype<T>(), sizeof(T), ps, f.nx, f.ny, f.nz, 128, TILE_ROWS)))
+    return false;
+  TDownU<T> op{};
+  op.mask1 = c.mask;
+  op.r1 = c.r;
+  op.r_out = r_out;
+  op.e = e;
+  op.ps = ps;
+  op.partials = partials;
+  op.nx = f.nx;
+  op.ny = f.ny;
+  op.ny1 = c.ny;
+  op.nz1 = c.nz;
+  return launch_tma<T>(op, maps, f.nx, f.ny, f.nz, f.tiles, st, s);
+}
+
 // The FP64 residual keeps the 8-warp column layout (no operand to share: x
 // is read directly) on the same tiles as fine_grid (8 rows per CTA).
 static_assert(TILE_ROWS == 8, "the residual and update kernels share fine_grid's tiles");
@@ -1165,7 +1309,10 @@ void launch_tile_flags(int nx, int ny, int nz, const uint8_t *mask, uint8_t *fla
   template void launch_fine_up<T>(const Level<T> &, const Level<T> &, T *, double *, float,   \
                                   const SolverState *, cudaStream_t);                         \
   template void launch_fine_down<T>(const Level<T> &, const Level<T> &, const SolverState *,  \
-                                    cudaStream_t);
+                                    cudaStream_t);                                              \
+  template bool launch_fine_down_update<T>(const Level<T> &, const Level<T> &, T *, float *,   \
+                                           const T *, const T *, double *, const SolverState *, \
+                                           cudaStream_t);
 INST(float)
 INST(__half)
 INST(__nv_bfloat16)

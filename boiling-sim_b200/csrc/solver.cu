@@ -50,6 +50,8 @@ bool g_fine_col_enabled = true;
 float g_mg_alpha = 1.0f;
 extern bool g_fine_tma_enabled;      // BSP_TUNE_FINE_TMA (mgfine.cu)
 extern bool g_coarse_fused_enabled;  // BSP_TUNE_COARSE_FUSED (mgcoarse.cu)
+// BSP_TUNE_FUSE_UPDATE: CG update fused into the next level-0 restriction
+bool g_fuse_update_enabled = true;
 constexpr int COARSE_SWEEPS = 64;
 constexpr int RED_THREADS = 256;
 
@@ -621,6 +623,7 @@ __global__ void __launch_bounds__(RED_THREADS) outer_check_kernel(SolverState *s
   (void)fp32_store;
   st->inner_it = 0;
   st->inner_done = 0;
+  st->pending = 0;
   st->rhat_norm2 = rr * st->scale * st->scale;
   // Do not over-solve the last pass: an inner reduction by
   // 0.5 tol ||b|| / ||r|| already meets the outer target.
@@ -643,6 +646,32 @@ __global__ void __launch_bounds__(RED_THREADS) alpha_kernel(SolverState *st,
   const double pap = reduce_slot(partials, 0, nblocks, false);
   if (threadIdx.x != 0) return;
   st->alpha = pap > 0.0 ? st->rz / pap : 0.0;
+  st->pending = 1;  // applied by the next iteration's fused restriction, if any
+}
+
+// Inner check after the restriction that applied the pending CG update (the
+// update of iteration q is fused into the restriction of iteration q + 1):
+// the same test as inner_check_kernel on ||r||^2 of the updated residual.  No
+// pending update (first iteration of a refinement pass): nothing to test.
+__global__ void __launch_bounds__(RED_THREADS) inner_check_fused_kernel(SolverState *st,
+                                                                        const double *partials,
+                                                                        int nblocks) {
+  if (st->inner_done) return;
+  const double rr = reduce_slot(partials, 0, nblocks, false);
+  if (threadIdx.x != 0 || !st->pending) return;
+  st->pending = 0;
+  st->inner_it += 1;
+  st->total_inner += 1;
+  st->rr_inner = rr;
+  if (st->dev_error) {
+    st->status = BSP_ERR_TIMEOUT;
+    st->inner_done = 1;
+    st->done = 1;
+    return;
+  }
+  if (!(rr == rr) || rr <= st->eta_eff * st->eta_eff * st->rhat_norm2 ||
+      st->inner_it >= st->max_inner || st->alpha == 0.0)
+    st->inner_done = 1;
 }
 
 __global__ void __launch_bounds__(RED_THREADS) inner_check_kernel(SolverState *st,
@@ -703,13 +732,13 @@ size_t storage_bytes(int storage) { return storage == BSP_STORE_FP32 ? 4 : 2; }
 
 // Workspace layout (all 256-byte aligned):
 //   SolverState | partials (3 * PARTIAL_STRIDE doubles) | x (n doubles) | e (n floats)
-//   | z, ps0, ps1, Ap, r (n T each) | per level l >= 1: mask, r, e (T)
+//   | z, ps0, ps1, Ap, r, r2 (n T each) | per level l >= 1: mask, r, e (T)
 //   | per level l >= 1 ... ; level-0 effective-class scratch reuses the level-1 slot order.
 //   | coarsest-level dense inverse (float), its FP64 build scratch, direct flag
 //   | per-level column-tile fluid flags (PARTIAL_STRIDE bytes per level)
 //   | FP32 scratch and grid-barrier word of the coarse-cycle kernel
 struct Layout {
-  size_t state, partials, x, e, z, ps0, ps1, Ap, r, lvl_mask[MAX_LEVELS], lvl_r[MAX_LEVELS],
+  size_t state, partials, x, e, z, ps0, ps1, Ap, r, r2, lvl_mask[MAX_LEVELS], lvl_r[MAX_LEVELS],
       lvl_e[MAX_LEVELS], eff0, cinv, cA, cflag, tflags, cscratch, cctl, total;
   int L, dims[3 * MAX_LEVELS];
 };
@@ -732,6 +761,7 @@ Layout make_layout(int nx, int ny, int nz, int storage) {
   lo.ps1 = take(ts * n);
   lo.Ap = take(ts * n);
   lo.r = take(ts * n);
+  lo.r2 = take(ts * n);  // second level-0 residual buffer (fused CG update)
   lo.eff0 = take(n);
   lo.L = build_hierarchy(nx, ny, nz, lo.dims);
   for (int l = 1; l < lo.L; ++l) {
@@ -770,6 +800,10 @@ struct Ctx {
   // whole GPU: not while other instances' kernels run beside it (batched
   // graphs with parallel branches)
   bool coop = true;
+  // the CG update of iteration q runs inside the level-0 restriction of
+  // iteration q + 1 (TMA path); the residual then alternates between r and r2
+  bool fuse = false;
+  T *r_write() const { return fuse ? (T *)(base + lo.r2) : lv[0].r; }  // rhat target
 };
 
 template <class T>
@@ -786,6 +820,7 @@ Ctx<T> make_ctx(void *ws, const uint8_t *mask, int nx, int ny, int nz, int stora
   cx.mask0 = mask;
   cx.col = (nz % 4 == 0) && (((uintptr_t)mask & 15u) == 0) && g_fine_col_enabled &&
            fine_grid_blocks(nx, ny, nz) <= PARTIAL_STRIDE;
+  cx.fuse = cx.col && g_fuse_update_enabled && fine_tma_available(nz);
   for (int l = 0; l < cx.lo.L; ++l) {
     Level<T> &L = cx.lv[l];
     L.nx = cx.lo.dims[3 * l];
@@ -844,7 +879,7 @@ cudaError_t setup_levels(Ctx<T> &cx, cudaStream_t s) {
   // write masked values; column tiles without fluid are never written).
   {
     const size_t ts = sizeof(T);
-    cudaMemsetAsync(cx.base + cx.lo.z, 0, cx.lo.r + ts * cx.n - cx.lo.z, s);  // z ps0 ps1 Ap r
+    cudaMemsetAsync(cx.base + cx.lo.z, 0, cx.lo.r2 + ts * cx.n - cx.lo.z, s);  // z ps0 ps1 Ap r r2
     cudaMemsetAsync(cx.base + cx.lo.e, 0, sizeof(float) * cx.n, s);
     cudaMemsetAsync(cx.base + cx.lo.cctl, 0, 64, s);
     for (int l = 1; l < cx.lo.L; ++l) {
@@ -900,7 +935,29 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
     else
       mg_down_kernel<T><<<row_blocks((int64_t)c.nx * c.ny), 256, 0, s>>>(f, c, st);
   };
-  down(0);
+  T *cur = (T *)(cx.base + (it_parity ? cx.lo.ps1 : cx.lo.ps0));
+  T *prev = (T *)(cx.base + (it_parity ? cx.lo.ps0 : cx.lo.ps1));
+  T *Ap = (T *)(cx.base + cx.lo.Ap);
+  // level 0 of this iteration; with the fused update its residual is the
+  // buffer of this parity (written by the restriction from the other one)
+  Level<T> l0 = cx.lv[0];
+  if (cx.fuse) {
+    T *b0 = cx.lv[0].r, *b1 = (T *)(cx.base + cx.lo.r2);
+    Level<T> in = cx.lv[0];
+    in.r = it_parity ? b0 : b1;
+    l0.r = it_parity ? b1 : b0;
+    {
+      ProfScope ps(PROF_MG_DOWN0, s);
+      if (!launch_fine_down_update<T>(in, cx.lv[1], l0.r, (float *)(cx.base + cx.lo.e), prev,
+                                      Ap, cx.partials, st, s))
+        return cudaErrorNotSupported;
+    }
+    ProfScope ps(PROF_CONTROL, s);
+    inner_check_fused_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials,
+                                                       fine_grid_blocks(cx.nx, cx.ny, cx.nz));
+  } else {
+    down(0);
+  }
   bool fused;
   {
     ProfScope ps(PROF_MG_COARSE, s);
@@ -933,18 +990,14 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
   {
     ProfScope ps(PROF_MG_UP0, s);
     if (col)
-      launch_fine_up<T>(cx.lv[0], cx.lv[1], z, cx.partials, g_mg_alpha, st, s);
+      launch_fine_up<T>(l0, cx.lv[1], z, cx.partials, g_mg_alpha, st, s);
     else
-      mg_up_kernel<T, true><<<nb0, 256, 0, s>>>(cx.lv[0], cx.lv[1], z, cx.partials, st,
-                                                g_mg_alpha);
+      mg_up_kernel<T, true><<<nb0, 256, 0, s>>>(l0, cx.lv[1], z, cx.partials, st, g_mg_alpha);
   }
   {
     ProfScope ps(PROF_CONTROL, s);
     beta_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials, nb0);
   }
-  T *cur = (T *)(cx.base + (it_parity ? cx.lo.ps1 : cx.lo.ps0));
-  T *prev = (T *)(cx.base + (it_parity ? cx.lo.ps0 : cx.lo.ps1));
-  T *Ap = (T *)(cx.base + cx.lo.Ap);
   {
     ProfScope ps(PROF_CG_PSAP, s);
     if (col)
@@ -958,6 +1011,7 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
     ProfScope ps(PROF_CONTROL, s);
     alpha_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials, nb0);
   }
+  if (cx.fuse) return cudaGetLastError();  // the update runs in the next restriction
   int nbf = flat_blocks(cx.n);
   {
     ProfScope ps(PROF_CG_UPDATE, s);
@@ -1096,7 +1150,7 @@ int solve_impl(void *ws, const uint8_t *mask, const float *div, float *p_out, in
     }
     {
       ProfScope ps(PROF_RESID64, s);
-      launch_resid<T>(cx, div, x, bscale, cx.lv[0].r, eb, true, s);
+      launch_resid<T>(cx, div, x, bscale, cx.r_write(), eb, true, s);
     }
     // 4-byte flag read (pageable: the copy completes before the sync returns)
     e = cudaMemcpyAsync(&flag, &cx.st->done, sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -1248,7 +1302,7 @@ cudaError_t append_solve(Ctx<T> &cx, const float *div, float *p_out, float dx, f
   launch_resid<T>(cx, div, x, bscale, nullptr, nullptr, false, cs);
   outer_check_kernel<<<1, RED_THREADS, 0, cs>>>(st, cx.partials, nres,
                                                 prm->storage == BSP_STORE_FP32);
-  launch_resid<T>(cx, div, x, bscale, cx.lv[0].r, eb, true, cs);
+  launch_resid<T>(cx, div, x, bscale, cx.r_write(), eb, true, cs);
   arm_inner_kernel<<<1, 1, 0, cs>>>(hi, st);
   if ((e = seg_end(cs, leaves)) != cudaSuccess) return e;
   if ((e = add_while(body_o, leaves, hi, &node_i, &body_i)) != cudaSuccess) return e;
@@ -1393,6 +1447,7 @@ static void key_params(GraphKey &k, const BspSolveParams *p) {
   k.v.push_back((uintptr_t)g_fine_col_enabled);
   k.v.push_back((uintptr_t)g_fine_tma_enabled);
   k.v.push_back((uintptr_t)g_coarse_fused_enabled);
+  k.v.push_back((uintptr_t)g_fuse_update_enabled);
 }
 
 }  // namespace bsp

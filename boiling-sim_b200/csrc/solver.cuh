@@ -32,6 +32,7 @@ struct SolverState {
   int outer_it, inner_it, total_inner;
   int done, inner_done, status, finalize;
   int dev_error;  // set by a kernel whose bounded wait gave up
+  int pending;    // a CG update (alpha, ps, Ap) waits to be applied by the next restriction
   // loop guards of the graph-driven solve: counted by the condition kernels
   // themselves so every WHILE node ends even if other state went wrong
   int guard_inner, guard_outer;
@@ -60,6 +61,13 @@ template <class T>
 int launch_cg_update_col(int nx, int ny, int nz, const uint8_t *tiles, float *e, T *r,
                          const T *ps, const T *Ap, double *partials, const SolverState *st,
                          cudaStream_t s);
+// Level-0 restriction with the previous iteration's CG update fused in
+// (mgfine.cu, TMA path); false when it cannot run.  f.r is r_in.
+template <class T>
+bool launch_fine_down_update(const Level<T> &f, const Level<T> &c, T *r_out, float *e,
+                             const T *ps, const T *Ap, double *partials, const SolverState *st,
+                             cudaStream_t s);
+bool fine_tma_available(int nz);
 // The coarse part of a V-cycle (levels 1 .. L-1) as one cooperative kernel
 // (mgcoarse.cu); false when not launched (the per-level kernels then run).
 template <class T>

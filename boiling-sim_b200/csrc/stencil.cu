@@ -501,6 +501,7 @@ extern bool g_fine_col_enabled;
 extern float g_mg_alpha;
 extern bool g_fine_tma_enabled;
 extern bool g_coarse_fused_enabled;
+extern bool g_fuse_update_enabled;
 }
 
 extern "C" int bsp_set_tuning(int key, int value) {
@@ -524,6 +525,10 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_COARSE_FUSED:
       if (value < 0 || value > 1) return BSP_ERR_ARG;
       bsp::g_coarse_fused_enabled = value != 0;
+      return BSP_OK;
+    case BSP_TUNE_FUSE_UPDATE:
+      if (value < 0 || value > 1) return BSP_ERR_ARG;
+      bsp::g_fuse_update_enabled = value != 0;
       return BSP_OK;
     default:
       return BSP_ERR_ARG;

@@ -56,6 +56,7 @@ extern "C" {
 #define BSP_TUNE_MG_ALPHA 3     /* coarse-correction scale of the V-cycle, in 1/1000 (100..3000) */
 #define BSP_TUNE_FINE_TMA 4     /* column-layout solver kernels fed by TMA tiles: 1 on, 0 off */
 #define BSP_TUNE_COARSE_FUSED 5 /* coarse V-cycle levels in one cooperative kernel: 1 on, 0 off */
+#define BSP_TUNE_FUSE_UPDATE 6  /* CG update fused into the next restriction (TMA path): 1 on, 0 off */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */

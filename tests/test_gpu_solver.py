@@ -114,6 +114,32 @@ def test_tma_and_shared_plane_kernels_bit_identical(cuda, storage, spec):
     assert np.array_equal(out[1][2], out[0][2])
 
 
+@pytest.mark.parametrize("storage", ["fp32", "fp16", "bf16"])
+@pytest.mark.parametrize("spec", [S.POT_64, S.PotSpec(66, 50, 80, 20, 3, 60, 5, 20)],
+                         ids=["pot64", "ny50_nz80"])
+def test_update_fused_into_restriction_matches_separate_update(cuda, storage, spec):
+    """The CG update applied inside the next level-0 restriction computes the
+    same r and e values as the separate update kernel (only the FP64 sum of
+    ||r||^2 runs in another order): same iteration counts and iterate."""
+    from boilingsim_b200 import _lib
+
+    mat = S.pot_mat(spec)
+    ux, uy, uz = S.velocity_field(mat, seed=4)
+    div = O.divergence(ux, uy, uz, mat, DX)
+    out = {}
+    try:
+        for fuse in (1, 0):
+            _lib.call("bsp_set_tuning", 6, fuse)
+            res = solve_tolerance(div, mat, DX, DT, RHO, tol=1e-7, storage=storage)
+            assert res.status == 0
+            assert O.rel_residual64(res.p64, div, mat, DX, DT, RHO) <= 1e-7 * 1.0001
+            out[fuse] = (res.inner_iterations, res.outer_iterations, res.p64.copy())
+    finally:
+        _lib.call("bsp_set_tuning", 6, 1)
+    assert out[1][:2] == out[0][:2]
+    assert np.array_equal(out[1][2], out[0][2])
+
+
 @pytest.mark.parametrize("storage", ["fp32", "bf16"])
 @pytest.mark.parametrize("spec", [S.POT_64, S.pot_192(3)], ids=["pot64", "pot192"])
 def test_fused_coarse_cycle_matches_per_level_kernels(cuda, storage, spec):
