@@ -236,7 +236,8 @@ def _tol_projection(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, solver:
     storage = {"b200-mg": "fp32", "b200-mixed": "fp16", "b200-bf16": "bf16"}[solver]
     tol_solver = _tol_solver(grid, storage)
     tol_solver.solve(ws.div_u, dx, dt, rho, tol=float(cfg.solver.pressure_tol), p=grid.p,
-                     warm_start=bool(cfg.solver.pressure_warm_start), raise_on_fail=False)
+                     warm_start=bool(cfg.solver.pressure_warm_start), raise_on_fail=False,
+                     graph=True)
     subtract_pressure_gradient(grid.ux, grid.uy, grid.uz, grid.p, mask, dx, dt, rho)
     compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, mask, dx, ws.max_div)
 
