@@ -53,6 +53,20 @@ SIGNATURES = {
     "bsp_step_projection_jacobi": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I,
                                         _I, _P, _P]),
     "bsp_noslip_divergence": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _P]),
+    # learned warm start (unet.cu)
+    "bsp_unet_conv3_fwd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
+    "bsp_unet_wgrad_workspace_bytes": (ctypes.c_size_t, [_I, _I, _I, _I, _I]),
+    "bsp_unet_conv3_wgrad": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _P, ctypes.c_size_t, _P]),
+    "bsp_unet_flip_weights": (_I, [_P, _P, _I, _I, _P]),
+    "bsp_unet_relu_bwd": (_I, [_P, _P, _L, _P]),
+    "bsp_unet_pool": (_I, [_P, _P, _I, _I, _I, _I, _I, _I, _P]),
+    "bsp_unet_up": (_I, [_P, _P, _I, _I, _I, _I, _I, _P]),
+    "bsp_unet_add": (_I, [_P, _P, _L, _P]),
+    "bsp_unet_pack_input": (_I, [_P, _P, _P, _L, _F, _P]),
+    "bsp_unet_head_fwd": (_I, [_P, _P, _P, _P, _P, _L, _F, _P]),
+    "bsp_unet_head_loss": (_I, [_P, _P, _I, _P, _P, _P, _P, _P, _L, _F, _F, _P]),
+    "bsp_unet_sum_partials": (_I, [_P, _P, _I, _I, _P]),
+    "bsp_unet_adam": (_I, [_P, _P, _P, _P, _P, _L, _F, _F, _F, _F, _I, _P]),
     "bsp_spmv": (_I, [_P, _P, _P, _I, _I, _I, _P]),
     "bsp_selftest_div6": (_I, [_P, _P]),
     "bsp_solve_params_default": (None, [_P]),
