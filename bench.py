@@ -156,6 +156,49 @@ def cpu_reference(mat, ux, uy, uz, ref_iters):
             "s_per_projection": t_proj}
 
 
+def run_learned(args, dev, rank, world, dist):
+    """Learned warm start at 192x192x128 (walls 2/3/4 cells, plume 0.02 / 0.1 /
+    0.3 m/s): the trained U-Net's pressure starts the solve, which finishes to
+    FP64 rel-residual 1e-6.  Per scene: inner iterations cold and warm, the
+    network's relative error against the converged pressure, the prediction
+    and solve times (CUDA events).  value = projections/s of prediction +
+    warm solve; the plain line is the cold solve of the same storage."""
+    import torch
+
+    from boilingsim_b200 import learned as LR
+    from boilingsim_b200 import scenes as S
+
+    net = LR.UNet.load(device=dev)
+    rows = []
+    for tw in (2, 3, 4):
+        for plume in (0.02, 0.1, 0.3):
+            for r in LR.evaluate(net, S.pot_192(tw), seeds=(SEED,), plume=plume,
+                                 storage=args.storage):
+                r.update({"wall": tw, "plume": plume})
+                rows.append(r)
+    ms_learned = float(np.mean([r["predict_ms"] + r["warm_ms"] for r in rows]))
+    ms_plain = float(np.mean([r["cold_ms"] for r in rows]))
+    if rank == 0:
+        line = {
+            "metric": "projections/s (solve) to rel-residual 1e-6 at 192x192x128, learned warm "
+                      "start vs the same solve from zero",
+            "value": round(1e3 / ms_learned, 3), "unit": "projections/s", "n_gpus": world,
+            "higher_is_better": True, "dtype": "bf16 network / f32 solve",
+            "data": "synthetic", "config": {"workload": "pot_192 walls 2/3/4, plumes "
+                                                        "0.02/0.1/0.3 m/s, seed 7",
+                                            "storage": args.storage},
+            "plain_projections_per_s": round(1e3 / ms_plain, 3),
+            "inner_iterations_cold_mean": float(np.mean([r["cold_inner"] for r in rows])),
+            "inner_iterations_warm_mean": float(np.mean([r["warm_inner"] for r in rows])),
+            "net_rel_error_mean": float(np.mean([r["net_rel_error"] for r in rows])),
+            "predict_ms_mean": float(np.mean([r["predict_ms"] for r in rows])),
+            "rows": rows,
+        }
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
 def run_batched(args, dev, rank, world, dist):
     """64 pot instances of uneven sizes (seeded draw, 48^3 .. 128x128x96), each
     with its own seeded velocity field, solved FP32-stored to FP64 rel-residual
@@ -252,9 +295,11 @@ def main():
                          "baseline): the short form used under ncu")
     ap.add_argument("--only-sweep", action="store_true",
                     help="run only the plain FP32 Jacobi sweep measurement (for ncu)")
-    ap.add_argument("--config", default="projection", choices=["projection", "batched"],
+    ap.add_argument("--config", default="projection",
+                    choices=["projection", "batched", "learned"],
                     help="projection: the headline 384x384x256 projection; batched: 64 uneven "
-                         "pot scenes (48^3 .. 128x128x96) solved by one graph launch")
+                         "pot scenes (48^3 .. 128x128x96) solved by one graph launch; learned: "
+                         "the U-Net warm start on the 192x192x128 pots (walls 2/3/4)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -296,6 +341,9 @@ def main():
     dev = torch.device("cuda", local)
     if args.config == "batched":
         run_batched(args, dev, rank, world, dist)
+        return
+    if args.config == "learned":
+        run_learned(args, dev, rank, world, dist)
         return
     mat, ux, uy, uz = _workload()
     nx, ny, nz = mat.shape

@@ -14,7 +14,10 @@ Solver selection follows ``_select_pressure_solver`` (``fluid.py:585-609``):
 ``pressure_max_iter`` sweeps), ``cg-rust`` (Jacobi-preconditioned CG to
 ``pressure_tol``), ``b200-jacobi`` (the uint8-mask sweep path), and
 ``BOILINGSIM_USE_RUST_PRESSURE=1`` selects the fused fixed-count Jacobi
-launcher.  Every back-end runs on the GPU; there is no CPU path.
+launcher; ``b200-mg`` / ``b200-mixed`` / ``b200-bf16`` are the to-tolerance
+solver with FP32 / FP16 / BF16 iterate storage, and ``b200-learned`` starts
+the FP16 solve from the learned warm start (learned.py).  Every back-end runs
+on the GPU; there is no CPU path.
 """
 from __future__ import annotations
 
@@ -126,7 +129,8 @@ def _select_pressure_solver() -> str:
     """``fluid.py:585-609`` with the B200 back-ends added."""
     use_rust_jacobi = os.environ.get("BOILINGSIM_USE_RUST_PRESSURE") == "1"
     solver = os.environ.get("BOILINGSIM_PRESSURE_SOLVER", "jacobi").lower()
-    valid = ("jacobi", "cg-rust", "b200-jacobi", "b200-mg", "b200-mixed", "b200-bf16")
+    valid = ("jacobi", "cg-rust", "b200-jacobi", "b200-mg", "b200-mixed", "b200-bf16",
+             "b200-learned")
     if solver not in valid:
         raise ValueError(f"BOILINGSIM_PRESSURE_SOLVER={solver!r} is not recognised; "
                          f"valid values are {', '.join(repr(v) for v in valid)}.")
@@ -233,13 +237,32 @@ def _tol_projection(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, solver:
     ||b - A p|| <= pressure_tol ||b|| in FP64); ws.div_u holds the divergence."""
     mask = grid_mask(grid)
     dx = float(grid.dx)
-    storage = {"b200-mg": "fp32", "b200-mixed": "fp16", "b200-bf16": "bf16"}[solver]
+    storage = {"b200-mg": "fp32", "b200-mixed": "fp16", "b200-bf16": "bf16",
+               "b200-learned": "fp16"}[solver]
     tol_solver = _tol_solver(grid, storage)
+    warm = bool(cfg.solver.pressure_warm_start)
+    if solver == "b200-learned" and all(d % 8 == 0 for d in grid.shape):
+        # the network's pressure is the starting guess; the solve finishes it
+        # to the same tolerance (grids not divisible by 8 start from zero)
+        grid.p.copy_(_learned_net().predict(ws.div_u, mask, dx, dt, rho))
+        warm = True
     tol_solver.solve(ws.div_u, dx, dt, rho, tol=float(cfg.solver.pressure_tol), p=grid.p,
-                     warm_start=bool(cfg.solver.pressure_warm_start), raise_on_fail=False,
-                     graph=True)
+                     warm_start=warm, raise_on_fail=False, graph=True)
     subtract_pressure_gradient(grid.ux, grid.uy, grid.uz, grid.p, mask, dx, dt, rho)
     compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, mask, dx, ws.max_div)
+
+
+_NET = None
+
+
+def _learned_net():
+    """The trained warm-start network (boilingsim_b200/data/unet_warmstart.npz)."""
+    global _NET
+    if _NET is None:
+        from .learned import UNet
+
+        _NET = UNet.load()
+    return _NET
 
 
 def noslip_divergence(div_u, ux, uy, uz, mask, dx, stream=None):

@@ -17,9 +17,9 @@ gradient; pooling, upsampling, head, loss and Adam); torch tensors are only
 device buffers.  Grid dimensions must be multiples of 8 (three poolings).
 
 Scaling.  A p = b is linear, so the network sees div / s (s = RMS of the
-divergence over fluid cells) and predicts p / S with
-S = -(rho dx^2 / dt) s H^2, H the water depth in cells; the Dirichlet free
-surface makes p grow with H^2.
+divergence over fluid cells) and predicts p / S with S = -(rho dx^2 / dt) s,
+the solution of A (p / S) = div / s.  The loss is the relative squared error
+sum (y - t)^2 / sum t^2 over fluid cells, so every scene weighs the same.
 """
 from __future__ import annotations
 
@@ -65,13 +65,14 @@ class Layer:
 
 
 def scene_scales(div: torch.Tensor, mask: torch.Tensor, dx: float, dt: float, rho: float):
-    """(s, S): input scale (RMS divergence on fluid cells) and output scale."""
+    """(s, S, n_fluid): input scale s (RMS divergence on fluid cells) and
+    output scale S = -(rho dx^2 / dt) s, so that the target p / S solves
+    A (p / S) = div / s: dimensionless, O(1) per unit input."""
     fl = (mask & 0x80) != 0
     nfl = int(fl.sum().item())
     s = float(torch.sqrt((div[fl].double() ** 2).sum() / max(nfl, 1)).item()) if nfl else 1.0
     s = s if s > 0 else 1.0
-    depth = float(fl.sum(dim=2).max().item()) if nfl else 1.0
-    S = -(rho * dx * dx / dt) * s * depth * depth
+    S = -(rho * dx * dx / dt) * s
     return s, S, nfl
 
 
@@ -100,15 +101,28 @@ class UNet:
         return d
 
     def save(self, path: str = WEIGHTS_PATH):
+        """Convolution weights as BF16 bit patterns (the inference copy), biases
+        and head in FP32."""
         os.makedirs(os.path.dirname(path), exist_ok=True)
-        np.savez_compressed(path, **{k: v.astype(np.float32) for k, v in self.state().items()})
+        out = {}
+        for k, v in self.state().items():
+            if k.endswith(".w") and not k.startswith("head"):
+                b = torch.as_tensor(v).to(torch.bfloat16).view(torch.int16).numpy()
+                out[k + ".bf16"] = b
+            else:
+                out[k] = v.astype(np.float32)
+        np.savez_compressed(path, **out)
 
     @classmethod
     def load(cls, path: str = WEIGHTS_PATH, device="cuda") -> "UNet":
         net = cls(device=device)
         d = np.load(path)
         for L in net.layers:
-            L.w.copy_(torch.as_tensor(d[f"{L.name}.w"]))
+            if f"{L.name}.w.bf16" in d:
+                w = torch.as_tensor(d[f"{L.name}.w.bf16"]).view(torch.bfloat16).float()
+            else:
+                w = torch.as_tensor(d[f"{L.name}.w"])
+            L.w.copy_(w)
             L.wb.copy_(L.w.to(torch.bfloat16))
             L.b.copy_(torch.as_tensor(d[f"{L.name}.b"]))
         net.hw.copy_(torch.as_tensor(d["head.w"]))
@@ -221,7 +235,7 @@ class UNet:
         return self._conv(g, L, dims, relu=False, w=wt, cin=L.cout, cout=L.cin, bias=False)
 
     def backward(self, c, target):
-        """Loss (mean squared error of p / S on fluid cells) and gradients."""
+        """Loss (relative squared error of p / S on fluid cells) and gradients."""
         d1, d2, d3, d4 = c["dims"]
         s, S, nfl = c["scales"]
         n1 = d1[0] * d1[1] * d1[2]
@@ -230,8 +244,11 @@ class UNet:
         gx = _bf16((n1, 16), self.device)
         parts = torch.empty((18, HEAD_BLOCKS), dtype=torch.float32, device=self.device)
         pred = c["pred"]
+        fl = (c["mask"] & 0x80) != 0
+        norm = float(((target[fl].double() / S) ** 2).sum().item()) or 1.0
+        c["norm"] = norm
         call("bsp_unet_head_loss", ptr(gx), ptr(parts), HEAD_BLOCKS, ptr(pred), ptr(target),
-             ptr(c["u1"]), ptr(self.hw), ptr(c["mask"]), n1, 1.0 / S, 1.0 / max(nfl, 1), st)
+             ptr(c["u1"]), ptr(self.hw), ptr(c["mask"]), n1, 1.0 / S, 1.0 / norm, st)
         sums = torch.empty(18, dtype=torch.float32, device=self.device)
         call("bsp_unet_sum_partials", ptr(sums), ptr(parts), HEAD_BLOCKS, 18, st)
         self.g_hb = sums[1:2].clone()
@@ -296,3 +313,178 @@ class UNet:
         loss = self.backward(c, target)
         self.adam_step(lr)
         return loss
+
+
+# ---- training data: the plain solver on seeded pot variants ----------------------------------
+def training_specs(count: int, seed: int = 11):
+    """Pot variants of the batched configuration (48^3 .. 128x128x96 cells,
+    wall 2-4 cells, radius filling the box minus the wall and a 2-cell pad,
+    water level 0.6-0.85 of the height, carrot radius 4-10 cells) with every
+    dimension a multiple of 8 (the network pools three times)."""
+    from .scenes import PotSpec
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        nxy = int(rng.integers(6, 17)) * 8          # 48 .. 128
+        nz = int(rng.integers(6, 13)) * 8           # 48 .. 96
+        t_w = int(rng.integers(2, 5))
+        r_in = nxy / 2.0 - t_w - 2
+        level = float(rng.uniform(0.6, 0.85))
+        water = t_w + level * (nz - t_w)
+        cr = min(float(rng.integers(4, 11)), 0.45 * (water - t_w))
+        out.append(PotSpec(nxy, nxy, nz, r_in=r_in, t_w=t_w, water_line=water, carrot_r=cr,
+                           carrot_len=min(1.2 * r_in, 5.0 * cr)))
+    return out
+
+
+class SceneSource:
+    """Divergence fields of one pot geometry on the GPU: seeded N(0, 0.05)
+    face velocities, box-smoothed three times (edge-replicated 3x3x3 mean),
+    a Gaussian plume of amplitude A on fluid z-faces, no-slip; the divergence
+    of that field.  The same rules as scenes.velocity_field, drawn with torch's
+    generator so a new field costs no host work."""
+
+    def __init__(self, mat: np.ndarray, device="cuda", sigma: float = 3.0):
+        from .fluid import cell_mask
+
+        self.mat = mat
+        self.shape = mat.shape
+        self.device = torch.device(device)
+        self.mat_t = torch.as_tensor(np.ascontiguousarray(mat, np.int32)).to(self.device)
+        self.mask = cell_mask(self.mat_t)
+        nx, ny, nz = mat.shape
+        ci = torch.arange(nx, device=self.device, dtype=torch.float32)[:, None] + 0.5
+        cj = torch.arange(ny, device=self.device, dtype=torch.float32)[None, :] + 0.5
+        r2 = (ci - nx / 2.0) ** 2 + (cj - ny / 2.0) ** 2
+        self.gauss = torch.exp(-r2 / (2.0 * sigma * sigma))
+        f = torch.as_tensor(mat == 0, device=self.device)
+        ff = torch.zeros((nx, ny, nz + 1), dtype=torch.bool, device=self.device)
+        ff[:, :, 1:-1] = f[:, :, :-1] & f[:, :, 1:]
+        self.zface_fluid = ff
+
+    @staticmethod
+    def _box3(a):
+        import torch.nn.functional as Fn
+
+        x = a[None, None]
+        for _ in range(3):
+            x = Fn.avg_pool3d(Fn.pad(x, (1, 1, 1, 1, 1, 1), mode="replicate"), 3, stride=1)
+        return x[0, 0]
+
+    def draw(self, seed: int, plume: float, dx: float):
+        from .fluid import compute_divergence
+        from ._lib import call as _call
+
+        nx, ny, nz = self.shape
+        g = torch.Generator(device=self.device).manual_seed(int(seed))
+        U = []
+        for shp in ((nx + 1, ny, nz), (nx, ny + 1, nz), (nx, ny, nz + 1)):
+            U.append(self._box3(torch.randn(shp, generator=g, device=self.device) * 0.05)
+                     .contiguous())
+        U[2] += torch.where(self.zface_fluid, plume * self.gauss[:, :, None], 0.0)
+        _call("bsp_enforce_no_slip", ptr(U[0]), ptr(U[1]), ptr(U[2]), ptr(self.mask), nx, ny, nz,
+              stream_handle())
+        div = torch.empty(self.shape, dtype=torch.float32, device=self.device)
+        compute_divergence(div, *U, self.mask, dx)
+        return div
+
+
+def train(steps: int = 20000, n_geometries: int = 64, seed: int = 11, lr: float = 1e-3,
+          dx: float = 0.002, dt: float = 0.01, rho: float = 997.0, log_every: int = 500,
+          net: UNet | None = None, log=print) -> UNet:
+    """Train on ``steps`` fresh (divergence, mask, pressure) triples: geometry
+    ``step % n_geometries``, velocity seed ``step``, plume amplitude drawn in
+    [0.02, 0.3] m/s; the target is the plain solve to FP64 rel-residual 1e-6.
+    Adam with a cosine learning-rate decay to lr / 10."""
+    from .scenes import pot_mat
+    from .solver import TolSolver
+
+    net = net or UNet(seed=seed)
+    specs = training_specs(n_geometries, seed)
+    sources = [SceneSource(pot_mat(s)) for s in specs]
+    solvers = [TolSolver(src.mask, "fp32") for src in sources]
+    rng = np.random.default_rng(seed + 1)
+    running = None
+    for step in range(steps):
+        q = step % n_geometries
+        src = sources[q]
+        div = src.draw(seed * 1000003 + step, float(rng.uniform(0.02, 0.3)), dx)
+        p = torch.zeros_like(div)
+        solvers[q].solve(div, dx, dt, rho, tol=1e-6, p=p)
+        cur_lr = lr * (0.1 + 0.9 * 0.5 * (1.0 + math.cos(math.pi * step / max(steps, 1))))
+        loss = float(net.train_step(div, src.mask, p, dx, dt, rho, lr=cur_lr).item())
+        running = loss if running is None else 0.98 * running + 0.02 * loss
+        if log and (step % log_every == 0 or step == steps - 1):
+            log(f"step {step} loss {loss:.4g} running {running:.4g} lr {cur_lr:.2g}")
+    return net
+
+
+def evaluate(net: UNet, spec, seeds=(101, 102, 103), plume: float = 0.1, dx: float = 0.002,
+             dt: float = 0.01, rho: float = 997.0, storage: str = "fp32", tol: float = 1e-6):
+    """Cold and warm-started solves of held-out scenes: inner iterations of
+    each, the network's relative error against the converged pressure (on
+    fluid cells) before the finishing solve, and the times of the prediction
+    and of both solves (CUDA events)."""
+    from .scenes import pot_mat
+    from .solver import TolSolver
+
+    src = SceneSource(pot_mat(spec))
+    solver = TolSolver(src.mask, storage)
+    fl = (src.mask & 0x80) != 0
+    rows = []
+    for sd in seeds:
+        div = src.draw(sd, plume, dx)
+        p_cold = torch.zeros_like(div)
+        solver.solve(div, dx, dt, rho, tol=tol, p=p_cold)  # setup and warm-up
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+        p_cold.zero_()
+        ev[0].record()
+        rc = solver.solve(div, dx, dt, rho, tol=tol, p=p_cold)
+        ev[1].record()
+        ev[2].record()
+        p_net = net.predict(div, src.mask, dx, dt, rho)
+        ev[3].record()
+        p_warm = p_net.clone()
+        ev[4].record()
+        rw = solver.solve(div, dx, dt, rho, tol=tol, p=p_warm, warm_start=True)
+        ev[5].record()
+        torch.cuda.synchronize()
+        ref = p_cold[fl].double()
+        err = float(torch.linalg.norm(p_net[fl].double() - ref) / torch.linalg.norm(ref))
+        rows.append({"seed": sd, "cold_inner": rc.inner_iterations,
+                     "warm_inner": rw.inner_iterations, "net_rel_error": err,
+                     "cold_ms": ev[0].elapsed_time(ev[1]), "predict_ms": ev[2].elapsed_time(ev[3]),
+                     "warm_ms": ev[4].elapsed_time(ev[5]),
+                     "cold_rel_residual": rc.rel_residual, "warm_rel_residual": rw.rel_residual})
+    return rows
+
+
+def main(argv=None):
+    import argparse
+    import json
+    import time
+
+    ap = argparse.ArgumentParser(description="train / evaluate the learned warm start")
+    ap.add_argument("cmd", choices=["train", "eval"])
+    ap.add_argument("--steps", type=int, default=20000)
+    ap.add_argument("--out", default=WEIGHTS_PATH)
+    ap.add_argument("--weights", default=WEIGHTS_PATH)
+    args = ap.parse_args(argv)
+    if args.cmd == "train":
+        t0 = time.time()
+        net = train(args.steps)
+        torch.cuda.synchronize()
+        net.save(args.out)
+        print(json.dumps({"trained_steps": args.steps, "seconds": round(time.time() - t0, 1),
+                          "weights": args.out}))
+    else:
+        from .scenes import pot_192
+
+        net = UNet.load(args.weights)
+        for tw in (2, 3, 4):
+            print(json.dumps({"wall": tw, "rows": evaluate(net, pot_192(tw))}))
+
+
+if __name__ == "__main__":
+    main()

@@ -85,12 +85,13 @@ LAYERS = [("e1a", 16, 16), ("e1b", 16, 16), ("e2a", 16, 32), ("e2b", 32, 32),
           ("u1a", 32, 16), ("u1b", 16, 16)]
 
 
-def forward_backward(x0, P, fluid, target, scale, bf16=True):
+def forward_backward(x0, P, fluid, target, scale, bf16=True, norm=None):
     """The network's forward pass and the gradient of its loss.
 
     x0: packed input (nx, ny, nz, 16); P: dict of parameters (name.w [27, co, ci],
     name.b [co], head.w [16], head.b [1]); fluid: bool mask; target: pressure;
-    scale: S.  With ``bf16`` every activation and activation gradient is
+    scale: S; norm: the loss divides the squared error by it (default: the
+    number of fluid cells).  With ``bf16`` every activation and activation gradient is
     rounded to BF16 where the GPU stores one, and the convolution weights are
     the BF16 copies, so the comparison isolates summation order.  Returns
     (pred, loss, grads dict)."""
@@ -114,7 +115,7 @@ def forward_backward(x0, P, fluid, target, scale, bf16=True):
     u1 = cv("u1b", q(cv("u1a", up(u2)) + e1))
     y = u1 @ W["head.w"] + W["head.b"][0]
     pred = np.where(fluid, scale * y, 0.0)
-    nfl = max(int(fluid.sum()), 1)
+    nfl = norm if norm is not None else max(int(fluid.sum()), 1)
     d = np.where(fluid, (pred - target) / scale, 0.0)
     loss = float((d * d).sum() / nfl)
     gy = 2.0 * d / nfl

@@ -116,7 +116,7 @@ def test_network_forward_and_gradients_match_oracle(cuda):
     P["head.w"] = net.hw.cpu().numpy().astype(np.float64)
     P["head.b"] = net.hb.cpu().numpy().astype(np.float64)
     want_pred, want_loss, G = U.forward_backward(x0, P, fluid, host(target).astype(np.float64),
-                                                 Sc)
+                                                 Sc, norm=c["norm"])
     assert rel(host(pred), want_pred) < 2e-2
     assert abs(loss - want_loss) <= 2e-2 * abs(want_loss)
     for L in net.layers:
@@ -144,3 +144,43 @@ def test_training_lowers_the_loss(cuda):
     for _ in range(49):
         last = float(net.train_step(div, mask, p, dx, dt, rho, lr=2e-3).item())
     assert np.isfinite(last) and last < 0.3 * first
+
+
+def test_trained_network_saves_iterations(cuda):
+    """The committed weights (trained on 20k plain-solver triples of the
+    batched pot variants) on held-out scenes: the prediction is closer to the
+    converged pressure than the zero start, and the solve started from it
+    reaches the same FP64 tolerance in fewer inner iterations.  A network with
+    untrained weights does not come close."""
+    net = LR.UNet.load()
+    fresh = LR.UNet(seed=123)
+    for spec, sd in ((S.PotSpec(96, 96, 64, r_in=43.0, t_w=3, water_line=50.0, carrot_r=6.0,
+                                carrot_len=30.0), 7), (S.pot_192(4), 101)):
+        rows = LR.evaluate(net, spec, seeds=(sd,), plume=0.15)
+        cold = LR.evaluate(fresh, spec, seeds=(sd,), plume=0.15)
+        r = rows[0]
+        assert r["warm_rel_residual"] <= 1e-6 and r["cold_rel_residual"] <= 1e-6
+        assert r["net_rel_error"] < 0.7, r
+        assert r["warm_inner"] < r["cold_inner"], r
+        assert cold[0]["net_rel_error"] > 2 * r["net_rel_error"], (cold[0], r)
+
+
+def test_learned_projection_back_end(cuda, monkeypatch):
+    """BOILINGSIM_PRESSURE_SOLVER=b200-learned: the projection starts the FP16
+    solve from the network and still meets the tolerance."""
+    from boilingsim_b200 import fluid as F
+    import oracle as O
+
+    monkeypatch.setenv("BOILINGSIM_PRESSURE_SOLVER", "b200-learned")
+    monkeypatch.delenv("BOILINGSIM_USE_RUST_PRESSURE", raising=False)
+    mat = S.pot_mat(S.POT_64)
+    ux, uy, uz = S.velocity_field(mat, seed=13)
+    grid = F.Grid.from_numpy(mat, ux, uy, uz, 0.002)
+    ws = F.allocate_fluid_workspace(grid)
+    cfg = F.ScenarioConfig(F.SolverConfig(pressure_tol=1e-6))
+    div = O.divergence(ux, uy, uz, mat, 0.002)
+    F.pressure_projection(grid, ws, cfg, 0.01, 997.0)
+    res = F._TOL_SOLVERS[next(iter(F._TOL_SOLVERS))].last
+    assert res.status == 0
+    torch.cuda.synchronize()
+    assert O.rel_residual64(res.p64_dev.cpu().numpy(), div, mat, 0.002, 0.01, 997.0) <= 1e-6
