@@ -66,6 +66,7 @@ SIGNATURES = {
     "bsp_unet_head_fwd": (_I, [_P, _P, _P, _P, _P, _L, _F, _P]),
     "bsp_unet_head_loss": (_I, [_P, _P, _I, _P, _P, _P, _P, _P, _L, _F, _F, _P]),
     "bsp_unet_sum_partials": (_I, [_P, _P, _I, _I, _P]),
+    "bsp_unet_head_bwd": (_I, [_P, _P, _I, _P, _P, _P, _P, _L, _P]),
     "bsp_unet_adam": (_I, [_P, _P, _P, _P, _P, _L, _F, _F, _F, _F, _I, _P]),
     "bsp_spmv": (_I, [_P, _P, _P, _I, _I, _I, _P]),
     "bsp_selftest_div6": (_I, [_P, _P]),

@@ -487,6 +487,40 @@ __global__ void __launch_bounds__(256) head_loss_kernel(
   for (int c = 0; c < 16; ++c) reduce(dhw[c], 2 + c);
 }
 
+// Head gradient for a given output gradient gy (dL/dy per voxel, 0 off fluid):
+// gx[v][c] = gy[v] hw[c]; per-block partials of dhb (slot 0) and dhw (1..16).
+__global__ void __launch_bounds__(256) head_bwd_kernel(
+    __nv_bfloat16 *__restrict__ gx, float *__restrict__ partials, const float *__restrict__ gy,
+    const __nv_bfloat16 *__restrict__ x, const float *__restrict__ hw,
+    const uint8_t *__restrict__ mask, int64_t nvox) {
+  float dhw[16], dhb = 0.0f;
+#pragma unroll
+  for (int c = 0; c < 16; ++c) dhw[c] = 0.0f;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nvox;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const float g = (mask[v] & BSP_CLASS_FLUID) ? gy[v] : 0.0f;
+    dhb += g;
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+      dhw[c] = fmaf(g, __bfloat162float(x[v * 16 + c]), dhw[c]);
+      gx[v * 16 + c] = __float2bfloat16(g * hw[c]);
+    }
+  }
+  __shared__ float sh[256];
+  auto reduce = [&](float val, int slot) {
+    sh[threadIdx.x] = val;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+      if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) partials[(int64_t)slot * gridDim.x + blockIdx.x] = sh[0];
+    __syncthreads();
+  };
+  reduce(dhb, 0);
+  for (int c = 0; c < 16; ++c) reduce(dhw[c], 1 + c);
+}
+
 // Adam step on FP32 master weights, refreshing the BF16 copy.
 __global__ void adam_kernel(float *__restrict__ w, __nv_bfloat16 *__restrict__ wb,
                             float *__restrict__ m, float *__restrict__ vv,
@@ -623,6 +657,14 @@ extern "C" int bsp_unet_head_loss(__nv_bfloat16 *gx, float *partials, int nblock
   if (nblocks <= 0 || nblocks > 4096) return BSP_ERR_ARG;
   head_loss_kernel<<<nblocks, 256, 0, s>>>(gx, partials, pred, target, x, hw, mask, nvox,
                                            inv_scale, inv_nfl);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int bsp_unet_head_bwd(__nv_bfloat16 *gx, float *partials, int nblocks,
+                                 const float *gy, const __nv_bfloat16 *x, const float *hw,
+                                 const uint8_t *mask, int64_t nvox, cudaStream_t s) {
+  if (nblocks <= 0 || nblocks > 4096) return BSP_ERR_ARG;
+  head_bwd_kernel<<<nblocks, 256, 0, s>>>(gx, partials, gy, x, hw, mask, nvox);
   return (int)cudaGetLastError();
 }
 
