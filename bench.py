@@ -376,21 +376,36 @@ def main():
     peak, peak_kind = _peaks()
 
     def plain_sweep():
-        """200 sweeps of the reference-contract FP32 Jacobi kernel, event-timed."""
+        """200 sweeps of the reference-contract FP32 Jacobi kernel, event-timed:
+        one sweep per HBM pass (tblock 1; 13 B/cell, its roofline), and pairs of
+        sweeps per pass (temporal blocking, tblock 2; effective bandwidth =
+        13 B/cell per sweep / time per sweep, above the HBM peak when blocking
+        pays)."""
         rhs = torch.empty_like(p)
         q = torch.empty_like(p)
         F.compute_divergence(div, *u0, mask, DX)
-        _lib.call("bsp_profile_enable", 1)
-        _lib.lib().bsp_profile_read(None, None, 0)
-        _lib.call("bsp_jacobi_solve", _lib.ptr(p), _lib.ptr(q), _lib.ptr(div), _lib.ptr(rhs),
-                  _lib.ptr(mask), nx, ny, nz, DX, DT, RHO, 200, 0, _lib.stream_handle())
-        torch.cuda.synchronize()
-        _lib.call("bsp_profile_enable", 0)
-        _lib.lib().bsp_profile_read(prof_ms, prof_n, ncls)
-        sweep_ms = prof_ms[0] / max(1, prof_n[0])
-        gbs = 13.0 * n / (sweep_ms * 1e-3) / 1e9
-        return {"ms": round(sweep_ms, 5), "GB/s": round(gbs, 1), "frac": round(gbs / peak, 4),
-                "bytes_per_cell": 13}
+        out = {}
+        for tb in (1, 2):
+            p.zero_()
+            _lib.call("bsp_profile_enable", 1)
+            _lib.lib().bsp_profile_read(None, None, 0)
+            _lib.call("bsp_jacobi_solve", _lib.ptr(p), _lib.ptr(q), _lib.ptr(div),
+                      _lib.ptr(rhs), _lib.ptr(mask), nx, ny, nz, DX, DT, RHO, 200, tb,
+                      _lib.stream_handle())
+            torch.cuda.synchronize()
+            _lib.call("bsp_profile_enable", 0)
+            _lib.lib().bsp_profile_read(prof_ms, prof_n, ncls)
+            sweep_ms = prof_ms[0] / 200.0
+            gbs = 13.0 * n / (sweep_ms * 1e-3) / 1e9
+            out[tb] = {"ms_per_sweep": round(sweep_ms, 5), "GB/s": round(gbs, 1),
+                       "frac": round(gbs / peak, 4), "launches": int(prof_n[0])}
+        one = out[1]
+        return {"ms": one["ms_per_sweep"], "GB/s": one["GB/s"], "frac": one["frac"],
+                "bytes_per_cell": 13,
+                "temporal_blocking_2": {"ms_per_sweep": out[2]["ms_per_sweep"],
+                                        "effective_GB/s": out[2]["GB/s"],
+                                        "effective_frac": out[2]["frac"],
+                                        "passes": out[2]["launches"]}}
 
     if args.only_sweep:
         if rank == 0:

@@ -41,6 +41,7 @@ SIGNATURES = {
     "bsp_jacobi_sweep": (_I, [_P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _P]),
     "bsp_jacobi_solve": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I, _I, _P]),
     "bsp_set_tuning": (_I, [_I, _I]),
+    "bsp_sweep2_error": (_I, [_P]),
     "bsp_solve_batch": (_I, [_I, _P, _P, _P, _P]),
     "bsp_dot_noalloc": (_I, [_P, _P, _L, _P, _P]),
     "bsp_profile_enable": (_I, [_I]),

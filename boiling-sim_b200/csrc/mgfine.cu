@@ -25,6 +25,7 @@
 
 #include "bsp_common.cuh"
 #include "solver.cuh"
+#include "tma.cuh"
 
 namespace bsp {
 
@@ -424,43 +425,6 @@ struct TmaGeom {
   static constexpr int MBYTES = TMA_ROWS * MASK_W;
   static constexpr int CBYTES = CROWS * CW * (int)sizeof(T);
 };
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-               : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-// Bounded wait on phase `parity` of an mbarrier: false after ~2^20 polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-  const uint32_t a = smem_u32(bar);
-  for (int it = 0; it < (1 << 20); ++it) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (ok) return true;
-  }
-  return false;
-}
-// 3-D tiled TMA load (no multicast) completing on `bar`.
-__device__ __forceinline__ void tma_load3(void *dst, const CUtensorMap *map, int x, int y, int z,
-                                          uint64_t *bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
-      : "memory");
-}
 
 // Tensor maps of one launch.  a, b: fine tensors of T; m: mask; c: coarse T.
 struct TmaMaps {
@@ -893,42 +857,6 @@ __global__ void __launch_bounds__(TILE_THREADS, Op::MIN_BLOCKS) fine_tma_kernel(
 
 // ---- TMA launch helpers (host) ----------------------------------------------------------
 bool g_fine_tma_enabled = true;  // BSP_TUNE_FINE_TMA
-
-static PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
-  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-  static std::once_flag once;
-  std::call_once(once, [] {
-    void *f = nullptr;
-    cudaDriverEntryPointQueryResult q{};
-    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &f, 12000, cudaEnableDefault,
-                                         &q) == cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
-  });
-  return fn;
-}
-
-template <class T>
-constexpr CUtensorMapDataType tma_dtype() {
-  return sizeof(T) == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32
-                        : (std::is_same<T, __half>::value ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
-                                                          : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16);
-}
-
-// 3-D map of a C-contiguous (nx, ny, nz) array, box {bx, by, 1}; out-of-range
-// elements read as zero.
-static bool make_map(CUtensorMap *m, CUtensorMapDataType t, int esize, const void *base, int nx,
-                     int ny, int nz, int bx, int by) {
-  auto fn = encode_tiled();
-  if (!fn || ((uintptr_t)base & 15u) || ((int64_t)nz * esize) % 16) return false;
-  const cuuint64_t dims[3] = {(cuuint64_t)nz, (cuuint64_t)ny, (cuuint64_t)nx};
-  const cuuint64_t strides[2] = {(cuuint64_t)nz * esize, (cuuint64_t)ny * nz * esize};
-  const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
-  const cuuint32_t es[3] = {1, 1, 1};
-  return fn(m, t, 3, const_cast<void *>(base), dims, strides, box, es,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
-}
 
 // The TMA path needs nz % 16 == 0 (16-byte mask rows) and 16-byte aligned bases.
 static bool tma_eligible(int nz) { return g_fine_tma_enabled && nz % 16 == 0 && encode_tiled(); }

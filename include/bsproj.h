@@ -157,11 +157,19 @@ int bsp_jacobi_sweep(float *p_new, const float *p_old, const float *div_u,
  * on the uint8 mask).  If rhs_ws (n floats, 16-byte aligned) is given, the
  * per-cell constant rho dx^2 div / dt is evaluated into it once and the
  * sweeps read it (bit-identical results, no division per sweep); rhs_ws may
- * equal div_u, which then holds that constant afterwards.  tblock is
- * reserved (sweeps fused per HBM pass; 0 or 1 today). */
+ * equal div_u, which then holds that constant afterwards.  tblock: sweeps
+ * per HBM pass -- 0 or 1 (default) one, 2 fuses pairs of sweeps into one
+ * temporally blocked pass (needs rhs_ws, nz % 16 == 0 and the source zero
+ * off fluid, i.e. from the second sweep, or the first when p starts at
+ * zero); the result is bit-identical either way. */
 int bsp_jacobi_solve(float *p, float *p_tmp, const float *div_u, float *rhs_ws,
                      const uint8_t *mask, int nx, int ny, int nz, float dx, float dt, float rho,
                      int n_iter, int tblock, cudaStream_t stream);
+
+/* 1 in *flag_host if a temporally blocked sweep pass gave up a bounded
+ * device-side wait since the last call (its output is then invalid); clears
+ * the flag.  Synchronises the device.  No reference counterpart. */
+int bsp_sweep2_error(int *flag_host);
 
 /* Set an autotuner parameter (BSP_TUNE_*) for subsequent launches in this
  * process.  Not thread-safe against concurrent launches. */

@@ -109,6 +109,31 @@ def test_fixed_count_solve_single_carrot(cuda, n_iter):
         assert np.array_equal(bits(host(p2)), bits(want))
 
 
+@pytest.mark.parametrize("shape,n_iter", [((20, 18, 32), 2), ((24, 50, 48), 5),
+                                          ((9, 16, 144), 8), ((16, 16, 16), 3)])
+def test_temporally_blocked_sweeps_bit_exact(cuda, shape, n_iter):
+    """Pairs of sweeps fused into one pass (tblock 0 / 2) give the same bits as
+    one sweep per pass (tblock 1) and as the oracle, from a random start that
+    is not zero off fluid (the first sweep then runs alone)."""
+    rng = np.random.default_rng(n_iter + shape[2])
+    mat, p_old, div = S.parity_random_grid(rng, shape)
+    dx, dt, rho = 0.002, 0.01, 997.0
+    want = O.pressure_solve(p_old, div, mat, dx, dt, rho, n_iter)
+    nx, ny, nz = shape
+    m8 = mask_of(dev(mat, torch.int32))
+    d = dev(div)
+    for tblock in (0, 1, 2):
+        p = dev(p_old)
+        tmp = torch.zeros_like(p)
+        rhs = torch.zeros_like(p)
+        call("bsp_jacobi_solve", ptr(p), ptr(tmp), ptr(d), ptr(rhs), ptr(m8), nx, ny, nz, dx,
+             dt, rho, n_iter, tblock, 0)
+        assert np.array_equal(bits(host(p)), bits(want)), tblock
+    flag = ctypes.c_int(-1)
+    call("bsp_sweep2_error", ctypes.byref(flag))
+    assert flag.value == 0
+
+
 @pytest.mark.parametrize("spec", [S.POT_64, S.PotSpec(40, 36, 30, 14, 2, 24, 4, 12)],
                          ids=["pot64", "pot40x36x30"])
 def test_full_projection_bit_exact(cuda, spec):
