@@ -42,6 +42,9 @@ SIGNATURES = {
     "bsp_jacobi_solve": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I, _I, _P]),
     "bsp_set_tuning": (_I, [_I, _I]),
     "bsp_sweep2_error": (_I, [_P]),
+    "bsp_autotune_jacobi": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I, _P, _I, _P, _P]),
+    "bsp_autotune_solve": (_I, [_P, _P, _P, _I, _I, _I, _F, _F, _F, _P, _P, ctypes.c_size_t, _P,
+                                _I, _P, _P]),
     "bsp_solve_batch": (_I, [_I, _P, _P, _P, _P]),
     "bsp_dot_noalloc": (_I, [_P, _P, _L, _P, _P]),
     "bsp_profile_enable": (_I, [_I]),
@@ -95,6 +98,13 @@ class BspBatchItem(ctypes.Structure):
                 ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
                 ("dx", ctypes.c_float), ("dt", ctypes.c_float), ("rho", ctypes.c_float),
                 ("workspace", ctypes.c_void_p), ("workspace_bytes", ctypes.c_size_t)]
+
+
+class BspTuneChoice(ctypes.Structure):
+    """include/bsproj.h: BspTuneChoice."""
+
+    _fields_ = [("key", ctypes.c_int), ("value", ctypes.c_int), ("ms", ctypes.c_float),
+                ("status", ctypes.c_int)]
 
 
 class BspSolveInfo(ctypes.Structure):

@@ -265,6 +265,27 @@ def _learned_net():
     return _NET
 
 
+def autotune_jacobi(grid: Grid, ws: FluidWorkspace, dt: float, rho: float, sweeps: int = 20,
+                    stream=None) -> list[dict]:
+    """Time the sweep plane chunk x sweeps per HBM pass on this grid
+    (bsp_autotune_jacobi, on the workspace's buffers) and keep the fastest for
+    later Jacobi solves.  Returns one row per candidate (ms per sweep)."""
+    import ctypes
+
+    nx, ny, nz = grid.shape
+    mask = grid_mask(grid)
+    compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, mask, grid.dx)
+    rhs = torch.empty_like(ws.div_u)
+    p = torch.empty_like(ws.div_u)
+    rows = (_lib.BspTuneChoice * 32)()
+    n = ctypes.c_int(0)
+    call("bsp_autotune_jacobi", ptr(p), ptr(ws.p_tmp), ptr(ws.div_u), ptr(rhs), ptr(mask), nx, ny,
+         nz, float(grid.dx), float(dt), float(rho), int(sweeps),
+         ctypes.cast(rows, ctypes.c_void_p), 32, ctypes.byref(n), stream_handle(stream))
+    return [{"plane_chunk": r.value & 0xFFFF, "sweeps_per_pass": r.value >> 16,
+             "ms_per_sweep": r.ms, "status": r.status} for r in rows[:min(n.value, 32)]]
+
+
 def noslip_divergence(div_u, ux, uy, uz, mask, dx, stream=None):
     """``enforce_no_slip`` then ``compute_divergence`` in one pass (bit-identical)."""
     nx, ny, nz = div_u.shape

@@ -100,6 +100,26 @@ class TolSolver:
         return self.last
 
 
+    def autotune(self, div: torch.Tensor, dx: float, dt: float, rho: float, tol: float = 1e-6,
+                 graph: bool = True, stream=None) -> list[dict]:
+        """Time the level-0 tile plane chunk x the one-launch coarse cycle on
+        this problem (bsp_autotune_solve) and keep the fastest for later solves.
+        Returns one row per candidate."""
+        nx, ny, nz = self.shape
+        prm = BspSolveParams.from_buffer_copy(self.params)
+        prm.tol = float(tol)
+        prm.use_graph = 1 if graph else 0
+        p = torch.zeros(self.shape, dtype=torch.float32, device=self.mask.device)
+        rows = (_lib.BspTuneChoice * 32)()
+        n = ctypes.c_int(0)
+        _lib.call("bsp_autotune_solve", ptr(p), ptr(div), ptr(self.mask), nx, ny, nz, float(dx),
+                  float(dt), float(rho), ctypes.byref(prm), ptr(self.ws), self.ws.numel(),
+                  ctypes.cast(rows, ctypes.c_void_p), 32, ctypes.byref(n), stream_handle(stream))
+        self._setup_done = False  # the tile geometry may have changed
+        return [{"key": r.key, "plane_chunk": r.value & 0xFFFF, "coarse_fused": r.value >> 16,
+                 "ms": r.ms, "status": r.status} for r in rows[:min(n.value, 32)]]
+
+
 class BatchSolver:
     """Many independent pot scenes (uneven sizes) solved by one graph launch
     (``bsp_solve_batch``).  Each instance owns its workspace; the masks are

@@ -25,8 +25,10 @@ cudaError_t launch_sweep_znf(float *out, const float *p, const float *rhs, const
 // writes +0 there, so from the second sweep on the ZNF kernel applies.
 bool launch_sweep2(float *out, const float *p, const float *rhs, const uint8_t *mask, int nx,
                    int ny, int nz, cudaStream_t s);
+int g_sweep_tblock = 1;  // BSP_TUNE_SWEEP_TBLOCK: sweeps per pass when a call passes 0
 
-// n_iter sweeps p <-> p_tmp, result in p.  With tblock >= 2, the right-hand
+// n_iter sweeps p <-> p_tmp, result in p.  With tblock >= 2 (tblock 0: the
+// BSP_TUNE_SWEEP_TBLOCK setting, 1 unless the autotuner chose 2), the right-hand
 // side hoisted (rhs_ws) and the source zero off fluid, pairs of sweeps run as
 // one temporally blocked pass (sweep2.cu); every sweep is bit-identical to
 // the single-sweep kernel either way.  One sweep per pass is the default:
@@ -42,10 +44,11 @@ int jacobi_solve_impl(float *p, float *p_tmp, const float *div_u, float *rhs_ws,
     cudaError_t e = launch_rhs(rhs_ws, div_u, mask, n, dx, dt, rho, stream);
     if (e != cudaSuccess) return (int)e;
   }
+  const int depth = tblock > 0 ? tblock : g_sweep_tblock;
   float *cur = p, *oth = p_tmp;
   for (int it = 0; it < n_iter;) {
     const bool znf = it > 0 || p_zero_nonfluid;
-    if (rhs_ws && znf && tblock >= 2 && n_iter - it >= 2) {
+    if (rhs_ws && znf && depth >= 2 && n_iter - it >= 2) {
       bool done;
       {
         ProfScope ps(PROF_SWEEP, stream);

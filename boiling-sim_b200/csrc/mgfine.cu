@@ -992,7 +992,10 @@ int num_sms();
 // Planes per CTA: the largest even value <= 16 that still gives about two
 // CTAs per SM (coarse levels are short; long plane chunks there leave the
 // GPU idle).  Even, because the restriction pairs planes inside one CTA.
+int g_fine_bi = 0;  // BSP_TUNE_FINE_BI: plane chunk of the level-0 tiles (0 = rule)
+
 int fine_bi(int nx, int ny, int nz) {
+  if (g_fine_bi > 0) return g_fine_bi < 2 ? 2 : (g_fine_bi & ~1);
   const int64_t cols = (int64_t)((nz / 4 + 31) / 32) * ((ny + TILE_ROWS - 1) / TILE_ROWS);
   const int64_t target = 2LL * num_sms();
   int bi = 16;

@@ -1068,9 +1068,12 @@ __global__ void __launch_bounds__(RED_THREADS) bnorm_kernel(SolverState *st,
 // Host-side record of workspaces whose multigrid setup (coarse masks, coarsest
 // inverse) is current, for callers that pass reuse_setup = 1 (their mask does
 // not change between solves).
+// A setup depends on the tile geometry too (the per-tile fluid flags): the
+// level-0 plane chunk in force when it was built is part of its key.
+extern int g_fine_bi;
 struct SetupKey {
   const void *ws, *mask;
-  int nx, ny, nz, storage;
+  int nx, ny, nz, storage, fine_bi;
 };
 static std::mutex g_setup_mu;
 static SetupKey g_setups[16];
@@ -1080,7 +1083,7 @@ static bool setup_cached(const void *ws, const void *mask, int nx, int ny, int n
   std::lock_guard<std::mutex> lk(g_setup_mu);
   for (const SetupKey &k : g_setups)
     if (k.ws == ws && k.mask == mask && k.nx == nx && k.ny == ny && k.nz == nz &&
-        k.storage == storage)
+        k.storage == storage && k.fine_bi == g_fine_bi)
       return true;
   return false;
 }
@@ -1089,7 +1092,7 @@ static void remember_setup(const void *ws, const void *mask, int nx, int ny, int
   std::lock_guard<std::mutex> lk(g_setup_mu);
   for (SetupKey &k : g_setups)
     if (k.ws == ws) k.ws = nullptr;  // a workspace holds one setup
-  g_setups[g_setup_next] = SetupKey{ws, mask, nx, ny, nz, storage};
+  g_setups[g_setup_next] = SetupKey{ws, mask, nx, ny, nz, storage, g_fine_bi};
   g_setup_next = (g_setup_next + 1) % 16;
 }
 
@@ -1448,6 +1451,7 @@ static void key_params(GraphKey &k, const BspSolveParams *p) {
   k.v.push_back((uintptr_t)g_fine_tma_enabled);
   k.v.push_back((uintptr_t)g_coarse_fused_enabled);
   k.v.push_back((uintptr_t)g_fuse_update_enabled);
+  k.v.push_back((uintptr_t)g_fine_bi);
 }
 
 }  // namespace bsp

@@ -502,6 +502,8 @@ extern float g_mg_alpha;
 extern bool g_fine_tma_enabled;
 extern bool g_coarse_fused_enabled;
 extern bool g_fuse_update_enabled;
+extern int g_fine_bi;
+extern int g_sweep_tblock;
 }
 
 extern "C" int bsp_set_tuning(int key, int value) {
@@ -529,6 +531,14 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_FUSE_UPDATE:
       if (value < 0 || value > 1) return BSP_ERR_ARG;
       bsp::g_fuse_update_enabled = value != 0;
+      return BSP_OK;
+    case BSP_TUNE_FINE_BI:
+      if (value < 0 || value > 64) return BSP_ERR_ARG;
+      bsp::g_fine_bi = value;
+      return BSP_OK;
+    case BSP_TUNE_SWEEP_TBLOCK:
+      if (value < 1 || value > 2) return BSP_ERR_ARG;
+      bsp::g_sweep_tblock = value;
       return BSP_OK;
     default:
       return BSP_ERR_ARG;

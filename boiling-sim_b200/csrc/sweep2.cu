@@ -221,6 +221,7 @@ __global__ void __launch_bounds__(sw2::THREADS, 2) sweep2_kernel(
 // launch are then not valid); read back by bsp_sweep2_error.
 __device__ int g_sweep2_err;
 int num_sms();
+extern int g_sweep_bi;  // BSP_TUNE_SWEEP_BI (stencil.cu)
 
 // Two sweeps p0 -> out (rhs already hoisted, p0 zero off fluid).  False when
 // the TMA path cannot run (nz % 16 != 0, alignment, no driver entry point).
@@ -245,6 +246,7 @@ bool launch_sweep2(float *out, const float *p, const float *rhs, const uint8_t *
   const int64_t cols = (int64_t)((nz + 127) / 128) * ((ny + ROWS - 1) / ROWS);
   int bi = 16;
   while (bi > 2 && cols * ((nx + bi - 1) / bi) < 2LL * num_sms()) bi -= 2;
+  if (g_sweep_bi > 0) bi = g_sweep_bi;
   dim3 grid((nz + 127) / 128, (ny + ROWS - 1) / ROWS, (nx + bi - 1) / bi);
   sweep2_kernel<<<grid, THREADS, TOTAL, s>>>(out, maps, nx, ny, nz, bi, err);
   return cudaGetLastError() == cudaSuccess;

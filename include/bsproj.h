@@ -57,6 +57,8 @@ extern "C" {
 #define BSP_TUNE_FINE_TMA 4     /* column-layout solver kernels fed by TMA tiles: 1 on, 0 off */
 #define BSP_TUNE_COARSE_FUSED 5 /* coarse V-cycle levels in one cooperative kernel: 1 on, 0 off */
 #define BSP_TUNE_FUSE_UPDATE 6  /* CG update fused into the next restriction (TMA path): 1 on, 0 off */
+#define BSP_TUNE_FINE_BI 7      /* i-planes per CTA tile of the solver's level-0 kernels (0 = rule) */
+#define BSP_TUNE_SWEEP_TBLOCK 8 /* sweeps per HBM pass when a call passes tblock = 0 (1 or 2) */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */
@@ -321,6 +323,36 @@ int bsp_dot_noalloc(const float *x, const float *y, int64_t n, double *result_de
  * launch.  Batched pot scenes of the benchmark configuration (64 instances). */
 int bsp_solve_batch(int count, const BspBatchItem *items, const BspSolveParams *params,
                     BspSolveInfo *infos, cudaStream_t stream);
+
+/* ---- autotuner ------------------------------------------------------------
+ * Time the candidate decompositions of a kernel family on the caller's own
+ * problem (CUDA events on `stream`, one untimed run first) and keep the
+ * fastest through bsp_set_tuning.  out[0 .. min(*n_out, max_out)) receives
+ * one row per candidate: key, value (low 16 bits: the plane chunk, 0 = rule;
+ * bit 16: the second switch), milliseconds (per sweep / per solve) and the
+ * candidate's status.  The buffers are overwritten.  No reference
+ * counterpart (the reference has no tuning step). */
+typedef struct BspTuneChoice {
+  int key, value;
+  float ms;
+  int status;
+} BspTuneChoice;
+
+/* Sweep plane chunk x sweeps per HBM pass (one, or two temporally blocked);
+ * `sweeps` sweeps per candidate on p / p_tmp / rhs_ws (p is zeroed first). */
+int bsp_autotune_jacobi(float *p, float *p_tmp, const float *div_u, float *rhs_ws,
+                        const uint8_t *mask, int nx, int ny, int nz, float dx, float dt,
+                        float rho, int sweeps, BspTuneChoice *out, int max_out, int *n_out,
+                        cudaStream_t stream);
+
+/* Plane chunk of the to-tolerance solver's level-0 tiles x the one-launch
+ * coarse cycle, each candidate a full bsp_solve_tol with `params`. */
+int bsp_autotune_solve(float *p, const float *div_u, const uint8_t *mask, int nx, int ny,
+                       int nz, float dx, float dt, float rho, const struct BspSolveParams *params,
+                       void *workspace, size_t workspace_bytes, BspTuneChoice *out, int max_out,
+                       int *n_out, cudaStream_t stream);
+
+
 
 /* Exhaustive self-check of the device division-by-6 against IEEE division
  * over all 2^32 float bit patterns; the mismatch count is written to the

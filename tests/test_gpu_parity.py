@@ -345,3 +345,24 @@ def test_against_reference_cuda_kernel(cuda, seed, shape):
         assert L.jacobi_pressure_launch(ptr(ref), ptr(p), ptr(d), ptr(m), nx, ny, nz, dx, dt, rho,
                                         0, 2) == 0
         assert np.array_equal(bits(host(ref)), bits(host(ours)))
+
+
+def test_autotune_jacobi_choice_stays_bit_exact(cuda):
+    """After the sweep autotuner (plane chunk x sweeps per pass) the default
+    solve uses its choice and still matches the oracle bit for bit."""
+    from boilingsim_b200 import fluid as F
+
+    mat = S.pot_mat(S.POT_64)
+    ux, uy, uz = S.velocity_field(mat, seed=5)
+    grid = F.Grid.from_numpy(mat, ux, uy, uz, 0.002)
+    ws = F.allocate_fluid_workspace(grid)
+    try:
+        rows = F.autotune_jacobi(grid, ws, 0.01, 997.0, sweeps=10)
+        assert len(rows) == 12 and all(r["status"] == 0 for r in rows)
+        want = O.projection_jacobi(ux, uy, uz, mat, 0.002, 0.01, 997.0, 20)
+        cfg = F.ScenarioConfig(F.SolverConfig(pressure_max_iter=20))
+        F.pressure_projection(grid, ws, cfg, 0.01, 997.0)
+        assert np.array_equal(bits(host(grid.p)), bits(want["p"]))
+    finally:
+        call("bsp_set_tuning", 1, 0)
+        call("bsp_set_tuning", 8, 1)

@@ -176,3 +176,26 @@ def test_solve_other_shapes(cuda, spec):
     res = solve_tolerance(div, mat, DX, DT, RHO, tol=1e-6)
     assert res.status == 0
     assert O.rel_residual64(res.p64, div, mat, DX, DT, RHO) <= 1e-6
+
+
+def test_autotune_solve_keeps_a_working_choice(cuda):
+    """The autotuner times every plane chunk x coarse-cycle candidate on the
+    problem, keeps the fastest, and solves afterwards still meet the
+    tolerance (the setup is rebuilt for the new tile geometry)."""
+    from boilingsim_b200 import _lib
+
+    mat = S.pot_mat(S.pot_192(3))
+    ux, uy, uz = S.velocity_field(mat, seed=3)
+    div = O.divergence(ux, uy, uz, mat, DX)
+    solver = TolSolver(cell_mask(torch.as_tensor(mat).cuda()), "fp16")
+    d = torch.as_tensor(div).cuda()
+    try:
+        rows = solver.autotune(d, DX, DT, RHO, tol=1e-6)
+        assert len(rows) == 14 and all(r["status"] == 0 for r in rows)
+        assert all(r["ms"] > 0 for r in rows)
+        res = solver.solve(d, DX, DT, RHO, tol=1e-6)
+        assert res.status == 0
+        assert O.rel_residual64(res.p64, div, mat, DX, DT, RHO) <= 1e-6
+    finally:
+        _lib.call("bsp_set_tuning", 7, 0)
+        _lib.call("bsp_set_tuning", 5, 1)
