@@ -550,9 +550,12 @@ inline int grid_for(int64_t n, int threads = 256) {
 
 using namespace bsp::unet;
 
-extern "C" int bsp_unet_conv3_fwd(__nv_bfloat16 *out, const __nv_bfloat16 *in,
-                                  const __nv_bfloat16 *w, const float *bias, int nx, int ny,
+extern "C" int bsp_unet_conv3_fwd(bsp_bf16_t *out_, const bsp_bf16_t *in_,
+                                  const bsp_bf16_t *w_, const float *bias, int nx, int ny,
                                   int nz, int cin, int cout, int relu, cudaStream_t s) {
+  __nv_bfloat16 *out = reinterpret_cast<__nv_bfloat16 *>(out_);
+  const __nv_bfloat16 *in = reinterpret_cast<const __nv_bfloat16 *>(in_);
+  const __nv_bfloat16 *w = reinterpret_cast<const __nv_bfloat16 *>(w_);
   if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_OK;
   if (!out || !in || !w) return BSP_ERR_NULL;
   if (cin <= 0 || cin % 16 || cout <= 0 || cout % 16) return BSP_ERR_SHAPE;
@@ -575,10 +578,12 @@ extern "C" size_t bsp_unet_wgrad_workspace_bytes(int nx, int ny, int nz, int cin
   return (size_t)nchunk * 27 * cin * cout * sizeof(float);
 }
 
-extern "C" int bsp_unet_conv3_wgrad(float *dw, float *db, const __nv_bfloat16 *g,
-                                    const __nv_bfloat16 *in, int nx, int ny, int nz, int cin,
+extern "C" int bsp_unet_conv3_wgrad(float *dw, float *db, const bsp_bf16_t *g_,
+                                    const bsp_bf16_t *in_, int nx, int ny, int nz, int cin,
                                     int cout, float *workspace, size_t workspace_bytes,
                                     cudaStream_t s) {
+  const __nv_bfloat16 *g = reinterpret_cast<const __nv_bfloat16 *>(g_);
+  const __nv_bfloat16 *in = reinterpret_cast<const __nv_bfloat16 *>(in_);
   if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_OK;
   if (!dw || !g || !in || !workspace) return BSP_ERR_NULL;
   if (cin <= 0 || cin % 16 || cout <= 0 || cout % 16) return BSP_ERR_SHAPE;
@@ -595,22 +600,28 @@ extern "C" int bsp_unet_conv3_wgrad(float *dw, float *db, const __nv_bfloat16 *g
   return (int)cudaGetLastError();
 }
 
-extern "C" int bsp_unet_flip_weights(__nv_bfloat16 *wt, const __nv_bfloat16 *w, int cin,
+extern "C" int bsp_unet_flip_weights(bsp_bf16_t *wt_, const bsp_bf16_t *w_, int cin,
                                      int cout, cudaStream_t s) {
+  __nv_bfloat16 *wt = reinterpret_cast<__nv_bfloat16 *>(wt_);
+  const __nv_bfloat16 *w = reinterpret_cast<const __nv_bfloat16 *>(w_);
   if (!wt || !w) return BSP_ERR_NULL;
   flip_weights_kernel<<<grid_for(27LL * cin * cout), 256, 0, s>>>(wt, w, cin, cout);
   return (int)cudaGetLastError();
 }
 
-extern "C" int bsp_unet_relu_bwd(__nv_bfloat16 *g, const __nv_bfloat16 *act, int64_t n,
+extern "C" int bsp_unet_relu_bwd(bsp_bf16_t *g_, const bsp_bf16_t *act_, int64_t n,
                                  cudaStream_t s) {
+  __nv_bfloat16 *g = reinterpret_cast<__nv_bfloat16 *>(g_);
+  const __nv_bfloat16 *act = reinterpret_cast<const __nv_bfloat16 *>(act_);
   if (n <= 0) return BSP_OK;
   relu_bwd_kernel<<<grid_for(n), 256, 0, s>>>(g, act, n);
   return (int)cudaGetLastError();
 }
 
-extern "C" int bsp_unet_pool(__nv_bfloat16 *out, const __nv_bfloat16 *in, int nx, int ny,
+extern "C" int bsp_unet_pool(bsp_bf16_t *out_, const bsp_bf16_t *in_, int nx, int ny,
                              int nz, int c, int backward, int accumulate, cudaStream_t s) {
+  __nv_bfloat16 *out = reinterpret_cast<__nv_bfloat16 *>(out_);
+  const __nv_bfloat16 *in = reinterpret_cast<const __nv_bfloat16 *>(in_);
   if (nx % 2 || ny % 2 || nz % 2) return BSP_ERR_SHAPE;
   if (backward)
     pool_bwd_kernel<<<grid_for((int64_t)nx * ny * nz * c), 256, 0, s>>>(out, in, nx, ny, nz, c,
@@ -621,8 +632,10 @@ extern "C" int bsp_unet_pool(__nv_bfloat16 *out, const __nv_bfloat16 *in, int nx
   return (int)cudaGetLastError();
 }
 
-extern "C" int bsp_unet_up(__nv_bfloat16 *out, const __nv_bfloat16 *in, int nx, int ny, int nz,
+extern "C" int bsp_unet_up(bsp_bf16_t *out_, const bsp_bf16_t *in_, int nx, int ny, int nz,
                            int c, int backward, cudaStream_t s) {
+  __nv_bfloat16 *out = reinterpret_cast<__nv_bfloat16 *>(out_);
+  const __nv_bfloat16 *in = reinterpret_cast<const __nv_bfloat16 *>(in_);
   if (nx % 2 || ny % 2 || nz % 2) return BSP_ERR_SHAPE;
   if (backward)
     up_bwd_kernel<<<grid_for((int64_t)nx * ny * nz * c / 8), 256, 0, s>>>(out, in, nx, ny, nz, c);
@@ -631,38 +644,46 @@ extern "C" int bsp_unet_up(__nv_bfloat16 *out, const __nv_bfloat16 *in, int nx, 
   return (int)cudaGetLastError();
 }
 
-extern "C" int bsp_unet_add(__nv_bfloat16 *a, const __nv_bfloat16 *b, int64_t n, cudaStream_t s) {
+extern "C" int bsp_unet_add(bsp_bf16_t *a_, const bsp_bf16_t *b_, int64_t n, cudaStream_t s) {
+  __nv_bfloat16 *a = reinterpret_cast<__nv_bfloat16 *>(a_);
+  const __nv_bfloat16 *b = reinterpret_cast<const __nv_bfloat16 *>(b_);
   if (n <= 0) return BSP_OK;
   add_kernel<<<grid_for(n), 256, 0, s>>>(a, b, n);
   return (int)cudaGetLastError();
 }
 
-extern "C" int bsp_unet_pack_input(__nv_bfloat16 *x, const float *div, const uint8_t *mask,
+extern "C" int bsp_unet_pack_input(bsp_bf16_t *x_, const float *div, const uint8_t *mask,
                                    int64_t nvox, float inv_scale, cudaStream_t s) {
+  __nv_bfloat16 *x = reinterpret_cast<__nv_bfloat16 *>(x_);
   pack_input_kernel<<<grid_for(nvox), 256, 0, s>>>(x, div, mask, nvox, inv_scale);
   return (int)cudaGetLastError();
 }
 
-extern "C" int bsp_unet_head_fwd(float *p, const __nv_bfloat16 *x, const float *hw,
+extern "C" int bsp_unet_head_fwd(float *p, const bsp_bf16_t *x_, const float *hw,
                                  const float *hb, const uint8_t *mask, int64_t nvox, float scale,
                                  cudaStream_t s) {
+  const __nv_bfloat16 *x = reinterpret_cast<const __nv_bfloat16 *>(x_);
   head_fwd_kernel<<<grid_for(nvox), 256, 0, s>>>(p, x, hw, hb, mask, nvox, scale);
   return (int)cudaGetLastError();
 }
 
-extern "C" int bsp_unet_head_loss(__nv_bfloat16 *gx, float *partials, int nblocks,
-                                  const float *pred, const float *target, const __nv_bfloat16 *x,
+extern "C" int bsp_unet_head_loss(bsp_bf16_t *gx_, float *partials, int nblocks,
+                                  const float *pred, const float *target, const bsp_bf16_t *x_,
                                   const float *hw, const uint8_t *mask, int64_t nvox,
                                   float inv_scale, float inv_nfl, cudaStream_t s) {
+  __nv_bfloat16 *gx = reinterpret_cast<__nv_bfloat16 *>(gx_);
+  const __nv_bfloat16 *x = reinterpret_cast<const __nv_bfloat16 *>(x_);
   if (nblocks <= 0 || nblocks > 4096) return BSP_ERR_ARG;
   head_loss_kernel<<<nblocks, 256, 0, s>>>(gx, partials, pred, target, x, hw, mask, nvox,
                                            inv_scale, inv_nfl);
   return (int)cudaGetLastError();
 }
 
-extern "C" int bsp_unet_head_bwd(__nv_bfloat16 *gx, float *partials, int nblocks,
-                                 const float *gy, const __nv_bfloat16 *x, const float *hw,
+extern "C" int bsp_unet_head_bwd(bsp_bf16_t *gx_, float *partials, int nblocks,
+                                 const float *gy, const bsp_bf16_t *x_, const float *hw,
                                  const uint8_t *mask, int64_t nvox, cudaStream_t s) {
+  __nv_bfloat16 *gx = reinterpret_cast<__nv_bfloat16 *>(gx_);
+  const __nv_bfloat16 *x = reinterpret_cast<const __nv_bfloat16 *>(x_);
   if (nblocks <= 0 || nblocks > 4096) return BSP_ERR_ARG;
   head_bwd_kernel<<<nblocks, 256, 0, s>>>(gx, partials, gy, x, hw, mask, nvox);
   return (int)cudaGetLastError();
@@ -676,9 +697,10 @@ extern "C" int bsp_unet_sum_partials(float *out, const float *partials, int nblo
   return (int)cudaGetLastError();
 }
 
-extern "C" int bsp_unet_adam(float *w, __nv_bfloat16 *wb, float *m, float *v, const float *g,
+extern "C" int bsp_unet_adam(float *w, bsp_bf16_t *wb_, float *m, float *v, const float *g,
                              int64_t n, float lr, float b1, float b2, float eps, int step,
                              cudaStream_t s) {
+  __nv_bfloat16 *wb = reinterpret_cast<__nv_bfloat16 *>(wb_);
   if (n <= 0 || step <= 0) return BSP_ERR_ARG;
   const float c1 = 1.0f / (1.0f - powf(b1, (float)step));
   const float c2 = 1.0f / (1.0f - powf(b2, (float)step));

@@ -352,7 +352,62 @@ int bsp_autotune_solve(float *p, const float *div_u, const uint8_t *mask, int nx
                        void *workspace, size_t workspace_bytes, BspTuneChoice *out, int max_out,
                        int *n_out, cudaStream_t stream);
 
+/* ---- learned warm start: U-Net layers --------------------------------------
+ * Building blocks of the pressure warm-start network (a 3-level 3-D U-Net
+ * over channels-last BF16 activations [nx][ny][nz][c]).  bsp_bf16_t is the
+ * bfloat16 bit pattern.  No reference counterpart: the reference's warm
+ * start is the previous step's pressure (python/boilingsim/fluid.py). */
+typedef uint16_t bsp_bf16_t;
 
+/* 3x3x3 same-padded convolution, implicit GEMM on the BF16 tensor cores with
+ * FP32 accumulation: out[v][co] = relu?(bias[co] + sum w[tap][ci][co] *
+ * in[v+tap][ci]).  cin, cout multiples of 16; in, w 16-byte aligned. */
+int bsp_unet_conv3_fwd(bsp_bf16_t *out, const bsp_bf16_t *in, const bsp_bf16_t *w,
+                       const float *bias, int nx, int ny, int nz, int cin, int cout, int relu,
+                       cudaStream_t stream);
+/* Workspace for bsp_unet_conv3_wgrad (per-chunk partial weight gradients). */
+size_t bsp_unet_wgrad_workspace_bytes(int nx, int ny, int nz, int cin, int cout);
+/* Weight (FP32 [27][cin][cout]) and optional bias gradient of conv3 from the
+ * output gradient g and the layer input; deterministic chunk order. */
+int bsp_unet_conv3_wgrad(float *dw, float *db, const bsp_bf16_t *g, const bsp_bf16_t *in,
+                         int nx, int ny, int nz, int cin, int cout, float *workspace,
+                         size_t workspace_bytes, cudaStream_t stream);
+/* wt[26-tap][co][ci] = w[tap][ci][co]: the input-gradient convolution's weights. */
+int bsp_unet_flip_weights(bsp_bf16_t *wt, const bsp_bf16_t *w, int cin, int cout,
+                          cudaStream_t stream);
+/* g *= (act > 0) elementwise. */
+int bsp_unet_relu_bwd(bsp_bf16_t *g, const bsp_bf16_t *act, int64_t n, cudaStream_t stream);
+/* 2x2x2 average pool of the fine grid (nx, ny, nz even), or its adjoint
+ * (backward != 0; accumulate adds into out). */
+int bsp_unet_pool(bsp_bf16_t *out, const bsp_bf16_t *in, int nx, int ny, int nz, int c,
+                  int backward, int accumulate, cudaStream_t stream);
+/* Nearest 2x upsampling onto the fine grid (nx, ny, nz even), or its adjoint. */
+int bsp_unet_up(bsp_bf16_t *out, const bsp_bf16_t *in, int nx, int ny, int nz, int c,
+                int backward, cudaStream_t stream);
+/* a += b elementwise (skip connections). */
+int bsp_unet_add(bsp_bf16_t *a, const bsp_bf16_t *b, int64_t n, cudaStream_t stream);
+/* Network input channels from the scaled divergence and the cell mask. */
+int bsp_unet_pack_input(bsp_bf16_t *x, const float *div, const uint8_t *mask, int64_t nvox,
+                        float inv_scale, cudaStream_t stream);
+/* 1x1 output head: p = scale * (hb + hw . x) on fluid cells, 0 elsewhere. */
+int bsp_unet_head_fwd(float *p, const bsp_bf16_t *x, const float *hw, const float *hb,
+                      const uint8_t *mask, int64_t nvox, float scale, cudaStream_t stream);
+/* Scaled L2 loss of pred against target with its head-input gradient gx and
+ * per-block partial sums (loss, head weights, bias) in partials. */
+int bsp_unet_head_loss(bsp_bf16_t *gx, float *partials, int nblocks, const float *pred,
+                       const float *target, const bsp_bf16_t *x, const float *hw,
+                       const uint8_t *mask, int64_t nvox, float inv_scale, float inv_nfl,
+                       cudaStream_t stream);
+/* Head backward from a given output gradient gy (energy / residual losses). */
+int bsp_unet_head_bwd(bsp_bf16_t *gx, float *partials, int nblocks, const float *gy,
+                      const bsp_bf16_t *x, const float *hw, const uint8_t *mask, int64_t nvox,
+                      cudaStream_t stream);
+/* out[slot] = sum over blocks of partials[slot][block], in block order. */
+int bsp_unet_sum_partials(float *out, const float *partials, int nblocks, int nslots,
+                          cudaStream_t stream);
+/* One Adam step on FP32 master weights w with BF16 copy wb. */
+int bsp_unet_adam(float *w, bsp_bf16_t *wb, float *m, float *v, const float *g, int64_t n,
+                  float lr, float b1, float b2, float eps, int step, cudaStream_t stream);
 
 /* Exhaustive self-check of the device division-by-6 against IEEE division
  * over all 2^32 float bit patterns; the mismatch count is written to the
