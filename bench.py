@@ -156,6 +156,89 @@ def cpu_reference(mat, ux, uy, uz, ref_iters):
             "s_per_projection": t_proj}
 
 
+COND_SWEEPS = 50  # diffusion_max_iter of the reference's scenario files
+
+
+def conduction_bench(mat, dev, peak, peak_kind, cpu: bool):
+    """Backward-Euler conduction on the same 384x384x256 pot (steel pot, water,
+    carrot, air; thermal.py:259-388, 647-658): one conduction step = the
+    snapshot + COND_SWEEPS Jacobi sweeps, event-timed; the sweep kernel alone
+    (uint8 material ids) event-timed over 40 ping-pong launches.  Algorithmic
+    bytes per sweep = 1 B of material id per cell + 12 B (T_iter, T_old, store)
+    per non-air cell -- air cells are neither read nor written, as in the
+    reference kernel.  Fields total 490 MB (> 126 MB L2)."""
+    import torch
+
+    from boilingsim_b200 import _lib
+    from boilingsim_b200 import thermal as TH
+
+    nx, ny, nz = mat.shape
+    n = mat.size
+    n_solid = int((mat != TH.MAT_AIR).sum())
+    rng = np.random.default_rng(SEED)
+    base = np.array([330.0, 380.0, 295.15, 300.0], np.float32)[mat]
+    T0 = (base + rng.standard_normal(mat.shape).astype(np.float32)).astype(np.float32)
+    props = TH.MaterialProps.from_materials("steel_304", device=dev)
+    grid = TH.ThermalGrid(nx, ny, nz, DX, torch.as_tensor(T0).to(dev),
+                          torch.as_tensor(mat).to(dev))
+    grid.mat_id = TH.material_ids(grid.mat)
+    ws = TH.allocate_thermal_workspace(grid, device=dev)
+    cfg = TH.ThermalConfig()
+    cfg.solver.diffusion_max_iter = COND_SWEEPS
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(3):
+        TH.implicit_conduction_step(grid, props, ws, cfg, DT)
+    reps = 5
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        TH.implicit_conduction_step(grid, props, ws, cfg, DT)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    step_ms = e0.elapsed_time(e1) / reps
+    a, b = grid.T, ws.T_iter_alt
+    args = [_lib.ptr(grid.mat_id), nx, ny, nz, _lib.ptr(props.k_wp), _lib.ptr(props.rho_wp),
+            _lib.ptr(props.cp_wp), 4, DX, DT, 10.0, 295.15, TH.MAT_AIR, _lib.stream_handle()]
+    sweeps = 40
+    for it in range(4):
+        _lib.call("bsp_conduction_sweep_u8", _lib.ptr(b if it % 2 == 0 else a),
+                  _lib.ptr(a if it % 2 == 0 else b), _lib.ptr(ws.T_old_snapshot), *args)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for it in range(sweeps):
+        _lib.call("bsp_conduction_sweep_u8", _lib.ptr(b if it % 2 == 0 else a),
+                  _lib.ptr(a if it % 2 == 0 else b), _lib.ptr(ws.T_old_snapshot), *args)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    sweep_ms = e0.elapsed_time(e1) / sweeps
+    alg = n + 12.0 * n_solid
+    gbs = alg / (sweep_ms * 1e-3) / 1e9
+    out = {"workload": "pot 384x384x256 dx=0.5mm, steel pot / water / carrot / air, dt 0.01 s, "
+                       f"{COND_SWEEPS} backward-Euler Jacobi sweeps per step (uint8 material ids)",
+           "steps_per_s": round(1e3 / step_ms, 2), "ms_per_step": round(step_ms, 4),
+           "sweep": {"kernel": "be_col_kernel", "ms": round(sweep_ms, 5),
+                     "algorithmic_bytes": int(alg), "non_air_cells": n_solid,
+                     "GB/s": round(gbs, 1), "peak": peak, "peak_source": peak_kind,
+                     "frac": round(gbs / peak, 4)},
+           "gpu_launches_per_step": COND_SWEEPS + (COND_SWEEPS % 2)}
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        threads = os.cpu_count() or 1
+        O.set_threads(threads)
+        hp = (props.k, props.rho, props.c_p)
+        t0 = time.perf_counter()
+        O.conduction_sweep(T0, T0, T0, mat, hp, DX, DT, 10.0, 295.15)
+        t_sweep = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(1.0 / (COND_SWEEPS * t_sweep), 4),
+                               "unit": "conduction steps/s", "cores": threads, "kind": "port",
+                               "sample": f"one full-grid sweep of the C restatement "
+                                         f"({t_sweep*1e3:.0f} ms) x {COND_SWEEPS}"}
+    return out
+
+
 def run_learned(args, dev, rank, world, dist):
     """Learned warm start at 192x192x128 (walls 2/3/4 cells, plume 0.02 / 0.1 /
     0.3 m/s): the trained U-Net's pressure starts the solve, which finishes to
@@ -295,6 +378,8 @@ def main():
                          "baseline): the short form used under ncu")
     ap.add_argument("--only-sweep", action="store_true",
                     help="run only the plain FP32 Jacobi sweep measurement (for ncu)")
+    ap.add_argument("--only-conduction", action="store_true",
+                    help="run only the backward-Euler conduction measurement (for ncu)")
     ap.add_argument("--config", default="projection",
                     choices=["projection", "batched", "learned"],
                     help="projection: the headline 384x384x256 projection; batched: 64 uneven "
@@ -407,9 +492,12 @@ def main():
                                         "effective_frac": out[2]["frac"],
                                         "passes": out[2]["launches"]}}
 
-    if args.only_sweep:
-        if rank == 0:
+    if args.only_sweep or args.only_conduction:
+        if rank == 0 and args.only_sweep:
             print(json.dumps({"plain_fp32_jacobi_sweep": plain_sweep()}), flush=True)
+        if rank == 0 and args.only_conduction:
+            print(json.dumps({"conduction": conduction_bench(mat, dev, *_peaks(), cpu=False)}),
+                  flush=True)
         if dist:
             dist.destroy_process_group()
         return
@@ -483,11 +571,13 @@ def main():
                   for c in per_launch if prof_n[c]}
     launches = int(sum(prof_n))  # every kernel launch of the timed steps is instrumented
 
-    sweep = e2e = None
+    sweep = e2e = cond = None
     ref_iters = args.ref_iters or REF_PCG_ITERS_FALLBACK
     cpu = None
     if not args.skip_extras:
         sweep = plain_sweep()
+        cond = conduction_bench(mat, dev, peak, peak_kind,
+                                cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
 
         # ---- end to end through the public API with host buffers ----------------------
         host_u = [torch.as_tensor(a).pin_memory() for a in (ux, uy, uz)]
@@ -563,6 +653,7 @@ def main():
             "kernel_algorithmic_GBs": kernel_gbs,
             "roofline": roofline,
             "plain_fp32_jacobi_sweep": sweep,
+            "conduction": cond,
             "reference_pcg_iterations_to_tol": ref_iters,
             "cpu_baseline": cpu,
             "e2e": e2e,

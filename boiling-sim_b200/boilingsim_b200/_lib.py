@@ -57,6 +57,16 @@ SIGNATURES = {
     "bsp_step_projection_jacobi": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I,
                                         _I, _P, _P]),
     "bsp_noslip_divergence": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _P]),
+    # backward-Euler conduction (conduction.cu)
+    "bsp_conduction_sweep": (_I, [_P, _P, _P, _P, _I, _I, _I, _P, _P, _P, _I, _F, _F, _F, _F, _I,
+                                  _P]),
+    "bsp_conduction_sweep_u8": (_I, [_P, _P, _P, _P, _I, _I, _I, _P, _P, _P, _I, _F, _F, _F, _F,
+                                     _I, _P]),
+    "bsp_conduction_be": (_I, [_P, _P, _P, _P, _I, _I, _I, _P, _P, _P, _I, _F, _F, _F, _F, _I, _I,
+                               _P]),
+    "bsp_conduction_be_u8": (_I, [_P, _P, _P, _P, _I, _I, _I, _P, _P, _P, _I, _F, _F, _F, _F, _I,
+                                  _I, _P]),
+    "bsp_material_ids": (_I, [_P, _P, _L, _I, _P, _P]),
     # learned warm start (unet.cu)
     "bsp_unet_conv3_fwd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
     "bsp_unet_wgrad_workspace_bytes": (ctypes.c_size_t, [_I, _I, _I, _I, _I]),

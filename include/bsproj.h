@@ -352,6 +352,43 @@ int bsp_autotune_solve(float *p, const float *div_u, const uint8_t *mask, int nx
                        void *workspace, size_t workspace_bytes, BspTuneChoice *out, int max_out,
                        int *n_out, cudaStream_t stream);
 
+/* ---- backward-Euler conduction -------------------------------------------------
+ * The implicit conduction step of python/boilingsim/thermal.py.  mat holds
+ * material ids in [0, n_mat) (n_mat <= 8), indexing the device arrays k, rho,
+ * cp (W/(m K), kg/m^3, J/(kg K)); mat_air is the air id.  T in kelvin.
+ *
+ * One Jacobi sweep, apply_implicit_conduction_update (thermal.py:259-388):
+ *   T_dst = (T_old + sum gamma T_nbr) / (1 + sum gamma)
+ * on every non-air cell (faces -x, +x, -y, +y, -z, +z; domain-edge faces
+ * skipped; an air neighbour contributes gamma * T_amb with Newton cooling
+ * gamma = dt h_conv_air / (rho cp dx); otherwise the harmonic-mean face
+ * conductivity).  Air cells of T_dst are not written.  Bit-identical to the
+ * reference arithmetic.  T_dst must not alias T_iter. */
+int bsp_conduction_sweep(float *T_dst, const float *T_iter, const float *T_old,
+                         const int32_t *mat, int nx, int ny, int nz, const float *k,
+                         const float *rho, const float *cp, int n_mat, float dx, float dt,
+                         float h_conv_air, float T_amb, int mat_air, cudaStream_t stream);
+/* The same on uint8 material ids (bsp_material_ids): 13 B/cell per sweep. */
+int bsp_conduction_sweep_u8(float *T_dst, const float *T_iter, const float *T_old,
+                            const uint8_t *mat_id, int nx, int ny, int nz, const float *k,
+                            const float *rho, const float *cp, int n_mat, float dx, float dt,
+                            float h_conv_air, float T_amb, int mat_air, cudaStream_t stream);
+/* The backward-Euler branch of conduct_one_step (thermal.py:647-658):
+ * T_old <- T; n_iter sweeps ping-ponging T -> T_alt -> T ...; when n_iter is
+ * odd, T <- T_alt (every cell).  The snapshot is written by the first sweep. */
+int bsp_conduction_be(float *T, float *T_alt, float *T_old, const int32_t *mat, int nx, int ny,
+                      int nz, const float *k, const float *rho, const float *cp, int n_mat,
+                      float dx, float dt, float h_conv_air, float T_amb, int mat_air,
+                      int n_iter, cudaStream_t stream);
+int bsp_conduction_be_u8(float *T, float *T_alt, float *T_old, const uint8_t *mat_id, int nx,
+                         int ny, int nz, const float *k, const float *rho, const float *cp,
+                         int n_mat, float dx, float dt, float h_conv_air, float T_amb,
+                         int mat_air, int n_iter, cudaStream_t stream);
+/* uint8 material ids from the int32 material grid (geometry.py:359); ids
+ * outside [0, n_mat) are counted into *bad_count_dev (may be NULL). */
+int bsp_material_ids(uint8_t *mat_id, const int32_t *mat, int64_t n, int n_mat,
+                     int *bad_count_dev, cudaStream_t stream);
+
 /* ---- learned warm start: U-Net layers --------------------------------------
  * Building blocks of the pressure warm-start network (a 3-level 3-D U-Net
  * over channels-last BF16 activations [nx][ny][nz][c]).  bsp_bf16_t is the

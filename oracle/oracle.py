@@ -72,6 +72,10 @@ def lib() -> ctypes.CDLL:
             "or_cg_f64": (_I, [_f64p, _f64p, _i32p, _I, _I, _I, _I, _I, _D, _I,
                                ctypes.POINTER(ctypes.c_double)]),
             "or_rel_residual_f64": (_D, [_f32p, _f32p, _i32p, _I, _I, _I, _D, _D, _D, _I, _I]),
+            "or_conduction_sweep_f32": (None, [_f32p, _f32p, _f32p, _i32p, _I, _I, _I, _f32p,
+                                               _f32p, _f32p, _F, _F, _F, _F, _I]),
+            "or_conduction_be_f32": (None, [_f32p, _f32p, _f32p, _i32p, _I, _I, _I, _f32p,
+                                            _f32p, _f32p, _F, _F, _F, _F, _I, _I]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -286,6 +290,36 @@ def analytic_quadratic_field(shape):
 # ---------------------------------------------------------------------------
 # The reference's own CUDA, compiled from source (oracle/_ref)
 # ---------------------------------------------------------------------------
+
+# ---------------------------------------------------------------------------
+# Backward-Euler conduction (thermal.py:259-388, 647-658)
+# ---------------------------------------------------------------------------
+
+def conduction_sweep(T_dst, T_iter, T_old, mat, props, dx, dt, h_conv_air, T_amb,
+                     mat_air=MAT_AIR):
+    """One Jacobi sweep; returns a new array (T_dst's contents kept on air cells).
+    ``props`` = (k, rho, cp), float32 arrays indexed by material id."""
+    out = _c(T_dst, np.float32).copy()
+    k, rho, cp = (_c(a, np.float32) for a in props)
+    nx, ny, nz = out.shape
+    lib().or_conduction_sweep_f32(out, _c(T_iter, np.float32), _c(T_old, np.float32),
+                                  _c(mat, np.int32), nx, ny, nz, k, rho, cp, float(dx),
+                                  float(dt), float(h_conv_air), float(T_amb), int(mat_air))
+    return out
+
+
+def conduction_be(T, T_alt, mat, props, dx, dt, h_conv_air, T_amb, n_iter, mat_air=MAT_AIR):
+    """The backward-Euler conduction step: returns (T, T_alt, T_old) after it."""
+    T = _c(T, np.float32).copy()
+    T_alt = _c(T_alt, np.float32).copy()
+    T_old = np.empty_like(T)
+    k, rho, cp = (_c(a, np.float32) for a in props)
+    nx, ny, nz = T.shape
+    lib().or_conduction_be_f32(T, T_alt, T_old, _c(mat, np.int32), nx, ny, nz, k, rho, cp,
+                               float(dx), float(dt), float(h_conv_air), float(T_amb),
+                               int(mat_air), int(n_iter))
+    return T, T_alt, T_old
+
 
 def ref_library_path(fma: bool = True) -> str:
     return os.path.join(_HERE, "_ref", "libref_fma.so" if fma else "libref_nofma.so")

@@ -22,6 +22,8 @@
  *   diag_inverse_apply_kernel   crates/cuda-kernels/src/diag_inverse_apply.cu:44-89
  *   compute_b_kernel            crates/cuda-kernels/src/axpy_device.cu:105-123
  *   pressure_solve_pcg_launch   crates/cuda-kernels/src/pressure_solve_pcg.cu:89-243
+ *   apply_implicit_conduction_update  python/boilingsim/thermal.py:259-388
+ *   conduct_one_step (backward-Euler branch)  python/boilingsim/thermal.py:647-658
  *
  * Bit-faithfulness rules (FP32 part): every value is a C float, dx/dt/rho are
  * float before any arithmetic (Warp `float` is f32), operations are evaluated
@@ -563,4 +565,76 @@ double or_rel_residual_f64(const float *p, const float *div, const int32_t *mat,
     free(b);
     free(Ap);
     return bb > 0.0 ? sqrt(rr / bb) : 0.0;
+}
+
+/* ------------------------------------------------------------------ */
+/* Backward-Euler conduction (FP32 restatement)                        */
+/* ------------------------------------------------------------------ */
+
+/* Face coefficient gamma of thermal.py:300-388 for a non-air cell of
+ * material ms facing material mn: Newton cooling (h_conv, neighbour held at
+ * T_amb) when mn is air, else the harmonic-mean conductivity
+ *   k_face = ((2 ks) kn) / ((ks + kn) + 1e-12),  gamma = ((dt k_face) inv) / (dx dx)
+ * with inv = 1 / (rho cp) of the cell's own material (thermal.py:290-293). */
+static inline float be_gamma(int ms, int mn, const float *k, const float *rho,
+                             const float *cp, float dx, float dt, float h_conv_air,
+                             int mat_air) {
+    const float inv = 1.0f / (rho[ms] * cp[ms]);
+    if (mn == mat_air) return ((dt * h_conv_air) * inv) / dx;
+    const float ks = k[ms], kn = k[mn];
+    const float kf = ((2.0f * ks) * kn) / ((ks + kn) + 1.0e-12f);
+    return ((dt * kf) * inv) / (dx * dx);
+}
+
+/* One Jacobi sweep of the backward-Euler conduction system,
+ * apply_implicit_conduction_update (thermal.py:259-388):
+ *   T_dst = (T_old + sum gamma T_nbr) / (1 + sum gamma)
+ * faces visited -x, +x, -y, +y, -z, +z; a face on the domain edge is
+ * skipped; an air neighbour contributes gamma * T_amb.  Air cells are not
+ * written (T_dst keeps its previous contents there). */
+void or_conduction_sweep_f32(float *T_dst, const float *T_iter, const float *T_old,
+                             const int32_t *mat, int nx, int ny, int nz, const float *k,
+                             const float *rho, const float *cp, float dx, float dt,
+                             float h_conv_air, float T_amb, int mat_air) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int kk = 0; kk < nz; ++kk) {
+                const int64_t c = IDX(i, j, kk);
+                const int ms = mat[c];
+                if (ms == mat_air) continue;
+                float rhs_sum = 0.0f, diag_extra = 0.0f;
+                const int di[6] = {-1, 1, 0, 0, 0, 0};
+                const int dj[6] = {0, 0, -1, 1, 0, 0};
+                const int dk[6] = {0, 0, 0, 0, -1, 1};
+                for (int f = 0; f < 6; ++f) {
+                    const int a = i + di[f], b = j + dj[f], e = kk + dk[f];
+                    if (a < 0 || a >= nx || b < 0 || b >= ny || e < 0 || e >= nz) continue;
+                    const int64_t n = IDX(a, b, e);
+                    const int mn = mat[n];
+                    const float g = be_gamma(ms, mn, k, rho, cp, dx, dt, h_conv_air, mat_air);
+                    rhs_sum = rhs_sum + g * (mn == mat_air ? T_amb : T_iter[n]);
+                    diag_extra = diag_extra + g;
+                }
+                T_dst[c] = (T_old[c] + rhs_sum) / (1.0f + diag_extra);
+            }
+}
+
+/* The backward-Euler branch of conduct_one_step (thermal.py:647-658):
+ * T_old <- T; n_iter sweeps ping-ponging T -> T_alt -> T ...; an odd count
+ * ends with T <- T_alt (the whole array, air cells included). */
+void or_conduction_be_f32(float *T, float *T_alt, float *T_old, const int32_t *mat, int nx,
+                          int ny, int nz, const float *k, const float *rho, const float *cp,
+                          float dx, float dt, float h_conv_air, float T_amb, int mat_air,
+                          int n_iter) {
+    if (nx <= 0 || ny <= 0 || nz <= 0) return;
+    const size_t bytes = sizeof(float) * (size_t)nx * ny * nz;
+    memcpy(T_old, T, bytes);
+    for (int it = 0; it < n_iter; ++it) {
+        const float *src = (it % 2 == 0) ? T : T_alt;
+        float *dst = (it % 2 == 0) ? T_alt : T;
+        or_conduction_sweep_f32(dst, src, T_old, mat, nx, ny, nz, k, rho, cp, dx, dt,
+                                h_conv_air, T_amb, mat_air);
+    }
+    if (n_iter % 2 == 1) memcpy(T, T_alt, bytes);
 }
