@@ -162,8 +162,9 @@ COND_SWEEPS = 50  # diffusion_max_iter of the reference's scenario files
 def conduction_bench(mat, dev, peak, peak_kind, cpu: bool):
     """Backward-Euler conduction on the same 384x384x256 pot (steel pot, water,
     carrot, air; thermal.py:259-388, 647-658): one conduction step = the
-    snapshot + COND_SWEEPS Jacobi sweeps, event-timed; the sweep kernel alone
-    (uint8 material ids) event-timed over 40 ping-pong launches.  Algorithmic
+    snapshot + COND_SWEEPS Jacobi sweeps, event-timed; the sweep kernels alone
+    (on cell classes, and on uint8 material ids) event-timed over 40 ping-pong
+    launches each.  Algorithmic
     bytes per sweep = 1 B of material id per cell + 12 B (T_iter, T_old, store)
     per non-air cell -- air cells are neither read nor written, as in the
     reference kernel.  Fields total 490 MB (> 126 MB L2)."""
@@ -182,6 +183,7 @@ def conduction_bench(mat, dev, peak, peak_kind, cpu: bool):
     grid = TH.ThermalGrid(nx, ny, nz, DX, torch.as_tensor(T0).to(dev),
                           torch.as_tensor(mat).to(dev))
     grid.mat_id = TH.material_ids(grid.mat)
+    grid.classes = TH.cell_classes(grid.mat) or False
     ws = TH.allocate_thermal_workspace(grid, device=dev)
     cfg = TH.ThermalConfig()
     cfg.solver.diffusion_max_iter = COND_SWEEPS
@@ -198,30 +200,43 @@ def conduction_bench(mat, dev, peak, peak_kind, cpu: bool):
     torch.cuda.synchronize()
     step_ms = e0.elapsed_time(e1) / reps
     a, b = grid.T, ws.T_iter_alt
-    args = [_lib.ptr(grid.mat_id), nx, ny, nz, _lib.ptr(props.k_wp), _lib.ptr(props.rho_wp),
-            _lib.ptr(props.cp_wp), 4, DX, DT, 10.0, 295.15, TH.MAT_AIR, _lib.stream_handle()]
-    sweeps = 40
-    for it in range(4):
-        _lib.call("bsp_conduction_sweep_u8", _lib.ptr(b if it % 2 == 0 else a),
-                  _lib.ptr(a if it % 2 == 0 else b), _lib.ptr(ws.T_old_snapshot), *args)
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for it in range(sweeps):
-        _lib.call("bsp_conduction_sweep_u8", _lib.ptr(b if it % 2 == 0 else a),
-                  _lib.ptr(a if it % 2 == 0 else b), _lib.ptr(ws.T_old_snapshot), *args)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    sweep_ms = e0.elapsed_time(e1) / sweeps
+    common = [nx, ny, nz, _lib.ptr(props.k_wp), _lib.ptr(props.rho_wp), _lib.ptr(props.cp_wp), 4,
+              DX, DT, 10.0, 295.15]
+
+    def time_sweeps(fn, lead, tail, sweeps=40):
+        for it in range(4 + sweeps):
+            if it == 4:
+                torch.cuda.synchronize()
+                e0.record(stream)
+            _lib.call(fn, _lib.ptr(b if it % 2 == 0 else a), _lib.ptr(a if it % 2 == 0 else b),
+                      _lib.ptr(ws.T_old_snapshot), *lead, *common, *tail, _lib.stream_handle())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / sweeps
+
+    def sweep_entry(kernel, ms_):
+        g = alg / (ms_ * 1e-3) / 1e9
+        return {"kernel": kernel, "ms": round(ms_, 5), "algorithmic_bytes": int(alg),
+                "non_air_cells": n_solid, "GB/s": round(g, 1), "peak": peak,
+                "peak_source": peak_kind, "frac": round(g / peak, 4)}
+
     alg = n + 12.0 * n_solid
-    gbs = alg / (sweep_ms * 1e-3) / 1e9
+    ms_ids = time_sweeps("bsp_conduction_sweep_u8", [_lib.ptr(grid.mat_id)], [TH.MAT_AIR])
     out = {"workload": "pot 384x384x256 dx=0.5mm, steel pot / water / carrot / air, dt 0.01 s, "
-                       f"{COND_SWEEPS} backward-Euler Jacobi sweeps per step (uint8 material ids)",
+                       f"{COND_SWEEPS} backward-Euler Jacobi sweeps per step",
            "steps_per_s": round(1e3 / step_ms, 2), "ms_per_step": round(step_ms, 4),
-           "sweep": {"kernel": "be_col_kernel", "ms": round(sweep_ms, 5),
-                     "algorithmic_bytes": int(alg), "non_air_cells": n_solid,
-                     "GB/s": round(gbs, 1), "peak": peak, "peak_source": peak_kind,
-                     "frac": round(gbs / peak, 4)},
            "gpu_launches_per_step": COND_SWEEPS + (COND_SWEEPS % 2)}
+    c = grid.classes
+    if c:
+        ms_cls = time_sweeps("bsp_conduction_sweep_cls",
+                             [_lib.ptr(c.cls), _lib.ptr(c.patterns), c.n_classes],
+                             [TH.MAT_AIR])
+        out["sweep"] = sweep_entry("be_cls_tma_kernel" if nz % 16 == 0 else "be_cls_col_kernel",
+                                   ms_cls)
+        out["cell_classes"] = c.n_classes
+        out["sweep_material_ids"] = sweep_entry("be_col_kernel", ms_ids)
+    else:
+        out["sweep"] = sweep_entry("be_col_kernel", ms_ids)
     if cpu:
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle as O

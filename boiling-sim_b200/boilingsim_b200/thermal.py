@@ -14,7 +14,9 @@ Drop-in for the implicit-conduction part of ``python/boilingsim/thermal.py``:
   ``conduct_one_step`` (``thermal.py:647-658``): snapshot, ``diffusion_max_iter``
   sweeps ping-ponging ``grid.T`` and ``T_iter_alt``, odd-count copy back.  The
   source terms that ``conduct_one_step`` applies afterwards (stove base flux,
-  evaporative cooling) are the caller's.
+  evaporative cooling) are the caller's.  The first call on a grid numbers its
+  cell neighbourhoods (``cell_classes``) and later calls sweep on those class
+  bytes; a geometry with more than 255 neighbourhoods uses material ids.
 
 Every call runs the sm_100a kernels of libbsproj.so on the caller's stream;
 results are bit-identical to the reference arithmetic.  There is no CPU path.
@@ -97,6 +99,7 @@ class ThermalGrid:
     T: torch.Tensor    # (nx, ny, nz) f32, kelvin
     mat: torch.Tensor  # (nx, ny, nz) int32 material ids
     mat_id: torch.Tensor | None = None  # uint8 copy of mat, derived once
+    classes: "CellClasses | None" = None  # conduction cell classes, derived once
 
     @property
     def shape(self):
@@ -129,6 +132,41 @@ def material_ids(mat: torch.Tensor, n_mat: int = 4, stream=None) -> torch.Tensor
     return out
 
 
+@dataclass
+class CellClasses:
+    """Conduction cell classes of a geometry (bsp_conduction_prepare): one byte
+    per cell naming its neighbourhood, and each class's neighbourhood key."""
+
+    cls: torch.Tensor       # (nx, ny, nz) uint8, 0 = air
+    patterns: torch.Tensor  # (256,) int32 keys
+    n_classes: int
+
+
+def cell_classes(mat: torch.Tensor, n_mat: int = 4, mat_air: int = MAT_AIR,
+                 stream=None) -> CellClasses | None:
+    """Number the distinct cell neighbourhoods of ``mat``; None when there are
+    more than 255 (the material-id kernels then serve the geometry)."""
+    import ctypes
+
+    from . import _lib
+
+    if mat.dtype != torch.int32 or not mat.is_contiguous():
+        raise TypeError("mat must be a contiguous int32 CUDA tensor")
+    nx, ny, nz = mat.shape
+    cls = torch.empty(mat.shape, dtype=torch.uint8, device=mat.device)
+    patterns = torch.zeros(256, dtype=torch.int32, device=mat.device)
+    ws = torch.empty(int(_lib.lib().bsp_conduction_prepare_workspace_bytes()), dtype=torch.uint8,
+                     device=mat.device)
+    n = ctypes.c_int(0)
+    code = _lib.lib().bsp_conduction_prepare(ptr(cls), ptr(patterns), ctypes.byref(n), ptr(mat),
+                                              nx, ny, nz, int(n_mat), int(mat_air), ptr(ws),
+                                              ws.numel(), stream_handle(stream))
+    if code == 10010:  # BSP_ERR_CAPACITY
+        return None
+    _lib.check("bsp_conduction_prepare", code)
+    return CellClasses(cls, patterns, int(n.value))
+
+
 def _check_f32(*ts):
     for t in ts:
         if isinstance(t, torch.Tensor) and (t.dtype != torch.float32 or not t.is_contiguous()):
@@ -158,11 +196,21 @@ def implicit_conduction_step(grid, props: MaterialProps, ws: ThermalWorkspace, c
     """The backward-Euler branch of ``conduct_one_step`` (thermal.py:647-658)."""
     del device
     _check_f32(grid.T, ws.T_iter_alt, ws.T_old_snapshot)
+    nx, ny, nz = grid.shape
+    T_amb_k = float(cfg.heating.ambient_temp_c + 273.15)
+    h = float(cfg.solver.h_conv_outer_w_per_m2_k)
+    n_iter = int(cfg.solver.diffusion_max_iter)
+    props_args = (ptr(props.k_wp), ptr(props.rho_wp), ptr(props.cp_wp), props.n_mat)
+    if getattr(grid, "classes", None) is None and props.n_mat <= 7:
+        grid.classes = cell_classes(grid.mat, props.n_mat, MAT_AIR, stream) or False
+    if grid.classes:
+        c = grid.classes
+        call("bsp_conduction_be_cls", ptr(grid.T), ptr(ws.T_iter_alt), ptr(ws.T_old_snapshot),
+             ptr(c.cls), ptr(c.patterns), c.n_classes, nx, ny, nz, *props_args, float(grid.dx),
+             float(dt), h, T_amb_k, MAT_AIR, n_iter, stream_handle(stream))
+        return
     if getattr(grid, "mat_id", None) is None:
         grid.mat_id = material_ids(grid.mat, props.n_mat, stream)
-    nx, ny, nz = grid.shape
-    T_amb_k = cfg.heating.ambient_temp_c + 273.15
     call("bsp_conduction_be_u8", ptr(grid.T), ptr(ws.T_iter_alt), ptr(ws.T_old_snapshot),
-         ptr(grid.mat_id), nx, ny, nz, ptr(props.k_wp), ptr(props.rho_wp), ptr(props.cp_wp),
-         props.n_mat, float(grid.dx), float(dt), float(cfg.solver.h_conv_outer_w_per_m2_k),
-         float(T_amb_k), MAT_AIR, int(cfg.solver.diffusion_max_iter), stream_handle(stream))
+         ptr(grid.mat_id), nx, ny, nz, *props_args, float(grid.dx), float(dt), h, T_amb_k,
+         MAT_AIR, n_iter, stream_handle(stream))

@@ -37,6 +37,7 @@
 
 #include "../../include/bsproj.h"
 #include "bsp_common.cuh"
+#include "tma.cuh"
 
 namespace bsp {
 int num_sms();
@@ -265,6 +266,421 @@ __global__ void __launch_bounds__(256) be_col_kernel(float *__restrict__ dst,
   }
 }
 
+// ---- cell classes --------------------------------------------------------------------
+// A non-air cell's update is fixed by its own material and the codes of its
+// six neighbours (material id, or EDGE for a face on the domain edge): the
+// key own | code(-x) << 3 | code(+x) << 6 | ... | code(+z) << 18.  The
+// prepare pass numbers the distinct keys of a geometry 1..n (class 0 = air);
+// each CTA then turns the keys into a table of (1 + sum gamma, gamma_-x ..
+// gamma_+z) -- gamma 0 on EDGE faces, the denominator summed in face order as
+// the reference does -- so a cell costs one class byte and two shared loads
+// instead of six table lookups and the diagonal sum.
+constexpr int NCLS = 256;
+constexpr int KEYBITS = 21;
+constexpr uint32_t NKEYWORDS = 1u << (KEYBITS - 5);
+constexpr uint32_t EDGE = 7u;
+constexpr int SCAN_THREADS = 1024;
+
+template <class MatT>
+__device__ __forceinline__ uint32_t cell_key(const MatT *mat, int64_t c, int i, int j, int k,
+                                             int nx, int ny, int nz, int64_t plane) {
+  const uint32_t own = mbyte(mat, c) & 7u;
+  const uint32_t cxm = i > 0 ? mbyte(mat, c - plane) & 7u : EDGE;
+  const uint32_t cxp = i + 1 < nx ? mbyte(mat, c + plane) & 7u : EDGE;
+  const uint32_t cym = j > 0 ? mbyte(mat, c - nz) & 7u : EDGE;
+  const uint32_t cyp = j + 1 < ny ? mbyte(mat, c + nz) & 7u : EDGE;
+  const uint32_t czm = k > 0 ? mbyte(mat, c - 1) & 7u : EDGE;
+  const uint32_t czp = k + 1 < nz ? mbyte(mat, c + 1) & 7u : EDGE;
+  return own | cxm << 3 | cxp << 6 | cym << 9 | cyp << 12 | czm << 15 | czp << 18;
+}
+
+template <class MatT>
+__global__ void cls_mark_kernel(uint32_t *__restrict__ bitmap, const MatT *__restrict__ mat,
+                                int nx, int ny, int nz, uint32_t mair) {
+  const int64_t n = (int64_t)nx * ny * nz, plane = (int64_t)ny * nz;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    if (mbyte(mat, c) == mair) continue;
+    const int k = (int)(c % nz);
+    const int64_t t = c / nz;
+    const uint32_t key = cell_key(mat, c, (int)(t / ny), (int)(t % ny), k, nx, ny, nz, plane);
+    const uint32_t bit = 1u << (key & 31u);
+    if (!(__ldg(bitmap + (key >> 5)) & bit)) atomicOr(bitmap + (key >> 5), bit);
+  }
+}
+
+// Exclusive prefix of the bitmap words' population counts; *count = total.
+__global__ void __launch_bounds__(SCAN_THREADS) cls_scan_kernel(uint32_t *__restrict__ base,
+                                                                const uint32_t *__restrict__ bitmap,
+                                                                int *__restrict__ count) {
+  constexpr int PER = NKEYWORDS / SCAN_THREADS;
+  __shared__ uint32_t part[SCAN_THREADS];
+  const int t = threadIdx.x;
+  uint32_t sum = 0;
+  for (int w = 0; w < PER; ++w) sum += __popc(bitmap[t * PER + w]);
+  part[t] = sum;
+  __syncthreads();
+  for (int off = 1; off < SCAN_THREADS; off <<= 1) {  // Hillis-Steele inclusive scan
+    const uint32_t v = t >= off ? part[t - off] : 0u;
+    __syncthreads();
+    part[t] += v;
+    __syncthreads();
+  }
+  uint32_t run = part[t] - sum;
+  for (int w = 0; w < PER; ++w) {
+    base[t * PER + w] = run;
+    run += __popc(bitmap[t * PER + w]);
+  }
+  if (t == SCAN_THREADS - 1) *count = (int)part[t];
+}
+
+template <class MatT>
+__global__ void cls_assign_kernel(uint8_t *__restrict__ cls, uint32_t *__restrict__ patterns,
+                                  const uint32_t *__restrict__ bitmap,
+                                  const uint32_t *__restrict__ base, const MatT *__restrict__ mat,
+                                  int nx, int ny, int nz, uint32_t mair) {
+  const int64_t n = (int64_t)nx * ny * nz, plane = (int64_t)ny * nz;
+  if (blockIdx.x == 0 && threadIdx.x == 0) patterns[0] = 0xffffffffu;  // air
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    if (mbyte(mat, c) == mair) {
+      cls[c] = 0;
+      continue;
+    }
+    const int k = (int)(c % nz);
+    const int64_t t = c / nz;
+    const uint32_t key = cell_key(mat, c, (int)(t / ny), (int)(t % ny), k, nx, ny, nz, plane);
+    const uint32_t w = key >> 5, b = key & 31u;
+    const uint32_t id = 1u + __ldg(base + w) + __popc(__ldg(bitmap + w) & ((1u << b) - 1u));
+    cls[c] = (uint8_t)id;  // the host checked id < NCLS
+    patterns[id] = key;    // every cell of a class writes the same key
+  }
+}
+
+// Per-CTA class table: tab[2c] = (1 + sum gamma, g-x, g+x, g-y), tab[2c+1] =
+// (g+y, g-z, g+z, 0).  gamma of a material pair as in gamma_entry; EDGE and
+// ids >= n_mat give 0.  Class 0 (air) gets den 1 and zero gammas.
+__device__ __forceinline__ void build_class_table(float4 *tab, float *gt,
+                                                  const uint32_t *__restrict__ patterns, int ncls,
+                                                  const Params &P) {
+  if (threadIdx.x < MAXM * MAXM)
+    gt[threadIdx.x] = gamma_entry(threadIdx.x / MAXM, threadIdx.x % MAXM, P.k, P.rho, P.cp,
+                                  P.n_mat, P.dx, P.dt, P.h, P.mair);
+  __syncthreads();
+  for (int c = threadIdx.x; c < NCLS; c += blockDim.x) {
+    float g[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float diag = 0.0f;
+    if (c > 0 && c < ncls) {
+      const uint32_t key = __ldg(patterns + c);
+      const float *row = gt + (key & 7u) * MAXM;
+#pragma unroll
+      for (int f = 0; f < 6; ++f) {
+        g[f] = row[(key >> (3 + 3 * f)) & 7u];
+        diag = __fadd_rn(diag, g[f]);
+      }
+    }
+    tab[2 * c] = make_float4(__fadd_rn(1.0f, diag), g[0], g[1], g[2]);
+    tab[2 * c + 1] = make_float4(g[3], g[4], g[5], 0.0f);
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ float amb0(float v, uint32_t w, int q, float tamb) {
+  return byte_of(w, q) == 0u ? tamb : v;
+}
+__device__ __forceinline__ float4 amb04(float4 v, uint32_t w, float tamb) {
+  return make_float4(amb0(v.x, w, 0, tamb), amb0(v.y, w, 1, tamb), amb0(v.z, w, 2, tamb),
+                     amb0(v.w, w, 3, tamb));
+}
+__device__ __forceinline__ bool has_zero_byte(uint32_t x) {
+  return ((x - 0x01010101u) & ~x & 0x80808080u) != 0u;
+}
+
+// Column kernel on class bytes: the layout of be_col_kernel.  A zero class
+// byte is air (and cells outside the grid read as air: their faces have gamma
+// 0 in every class that touches them, so the value substituted, T_amb, adds 0).
+template <bool FULL, bool SNAP>
+__global__ void __launch_bounds__(256) be_cls_col_kernel(
+    float *__restrict__ dst, const float *__restrict__ src, const float *__restrict__ told,
+    float *__restrict__ snap, const uint8_t *__restrict__ cls,
+    const uint32_t *__restrict__ patterns, int ncls, int nx, int ny, int nz, int bi, Params P) {
+  __shared__ float4 tab[2 * NCLS];
+  __shared__ float gt[MAXM * MAXM];
+  build_class_table(tab, gt, patterns, ncls, P);
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
+  if (j >= ny) return;  // warp-uniform, after the last barrier
+  const int k = (blockIdx.x * 32 + lane) * 4;
+  const bool act = FULL || k < nz;
+  const int i0 = blockIdx.z * bi;
+  const int i1 = min(i0 + bi, nx);
+  const int64_t plane = (int64_t)ny * nz;
+  const bool has_jm = j > 0, has_jp = j + 1 < ny;
+  const float tamb = P.tamb;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  int64_t o = (int64_t)i0 * plane + (int64_t)j * nz + k;
+
+  uint32_t wm = 0u, wc = 0u, wjm = 0u, wjp = 0u, wn = 0u;
+  float4 pm = z4, pc = z4;
+  if (act) {
+    if (i0 > 0) {
+      wm = mword(cls, o - plane);
+      if (wm) pm = ld4(src + o - plane);
+    }
+    wc = mword(cls, o);
+    if (SNAP || wc) pc = ld4(src + o);
+    if (SNAP) st4(snap + o, pc);
+    if (has_jm) wjm = mword(cls, o - nz);
+    if (has_jp) wjp = mword(cls, o + nz);
+    if (i0 + 1 < nx) wn = mword(cls, o + plane);
+  }
+  pm = amb04(pm, wm, tamb);
+  pc = amb04(pc, wc, tamb);
+  for (int i = i0; i < i1; ++i, o += plane) {
+    const bool has_in = i + 1 < nx;
+    float4 pn = z4, pjm = z4, pjp = z4, tov = z4;
+    uint32_t wn2 = 0u, wjm2 = 0u, wjp2 = 0u;
+    if (act) {
+      if (has_in && (SNAP || wn)) pn = ld4(src + o + plane);
+      if (wjm) pjm = ld4(src + o - nz);
+      if (wjp) pjp = ld4(src + o + nz);
+      if (!SNAP && wc) tov = ld4(told + o);
+      if (has_in) {
+        if (has_jm) wjm2 = mword(cls, o + plane - nz);
+        if (has_jp) wjp2 = mword(cls, o + plane + nz);
+        if (i + 2 < nx) wn2 = mword(cls, o + 2 * plane);
+      }
+      if (SNAP && i + 1 < i1) st4(snap + o + plane, pn);  // this CTA's planes only
+    }
+    pn = amb04(pn, wn, tamb);
+    pjm = amb04(pjm, wjm, tamb);
+    pjp = amb04(pjp, wjp, tamb);
+    if (SNAP) tov = pc;
+    float pkm = __shfl_up_sync(0xffffffffu, pc.w, 1);
+    float pkp = __shfl_down_sync(0xffffffffu, pc.x, 1);
+    if (lane == 0) pkm = act && k > 0 && __ldg(cls + o - 1) ? __ldg(src + o - 1) : tamb;
+    if (lane == 31) pkp = act && k + 4 < nz && __ldg(cls + o + 4) ? __ldg(src + o + 4) : tamb;
+    if (__any_sync(0xffffffffu, act && wc != 0u)) {
+      const float4 pb = make_float4(pkm, pc.x, pc.y, pc.z);
+      const float4 pf = make_float4(pc.y, pc.z, pc.w, pkp);
+      float o4[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t c = byte_of(wc, q);
+        const float4 A = tab[2 * c], B = tab[2 * c + 1];
+        float rhs = __fadd_rn(0.0f, __fmul_rn(A.y, f4(pm, q)));
+        rhs = __fadd_rn(rhs, __fmul_rn(A.z, f4(pn, q)));
+        rhs = __fadd_rn(rhs, __fmul_rn(A.w, f4(pjm, q)));
+        rhs = __fadd_rn(rhs, __fmul_rn(B.x, f4(pjp, q)));
+        rhs = __fadd_rn(rhs, __fmul_rn(B.y, f4(pb, q)));
+        rhs = __fadd_rn(rhs, __fmul_rn(B.z, f4(pf, q)));
+        o4[q] = __fdiv_rn(__fadd_rn(f4(tov, q), rhs), A.x);
+      }
+      if (act && wc != 0u) {
+        if (!has_zero_byte(wc)) {
+          st4(dst + o, make_float4(o4[0], o4[1], o4[2], o4[3]));
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (byte_of(wc, q) != 0u) dst[o + q] = o4[q];
+        }
+      }
+    }
+    pm = pc;
+    pc = pn;
+    wc = wn;
+    wn = wn2;
+    wjm = wjm2;
+    wjp = wjp2;
+  }
+}
+
+// ---- TMA-fed class kernel ---------------------------------------------------------
+// The production sweep for nz % 16 == 0.  A CTA of 8 warps owns 8 rows x 128 k
+// of bi planes; one thread streams each plane's tiles -- T (rows j0-1 .. j0+8,
+// k0-4 .. k0+131), class bytes (same rows, k0-16 .. k0+143) and T_old (the 8
+// output rows) -- into a ring of NST shared-memory stages, NST-1 planes ahead
+// of the plane being computed, so the bytes in flight do not depend on how
+// many warps are waiting.  Everything outside the grid arrives as TMA zero
+// fill: class 0 (air), whose value T_amb meets a gamma of 0 in every class
+// that borders the domain edge.  No global load is left in the plane loop.
+// Waits are bounded: a wait that gives up sets *err and the results of the
+// launch are not valid.
+namespace tmac {
+constexpr int ROWS = 8, TR = ROWS + 2;
+constexpr int TP = 4, TW = 128 + 2 * TP;   // T tile row: 136 floats
+constexpr int CP = 16, CW = 128 + 2 * CP;  // class tile row: 160 bytes
+constexpr int NST = 4;
+constexpr int al128(int b) { return (b + 127) / 128 * 128; }
+constexpr int TB = TR * TW * 4, CB = TR * CW, OB = ROWS * 128 * 4;
+constexpr int OFF_C = al128(TB), OFF_O = OFF_C + al128(CB), STAGE = OFF_O + OB;
+constexpr int OFF_TAB = STAGE * NST, OFF_GT = OFF_TAB + 2 * NCLS * 16;
+constexpr int OFF_BAR = OFF_GT + MAXM * MAXM * 4, TOTAL = OFF_BAR + NST * 8;
+constexpr int THREADS = ROWS * 32;
+}  // namespace tmac
+
+struct CondMaps {
+  CUtensorMap t, c, o;
+};
+
+__device__ int g_cond_err;
+
+__device__ __forceinline__ float4 lds4(const float *p) {
+  return *reinterpret_cast<const float4 *>(p);
+}
+__device__ __forceinline__ uint32_t lds32(const uint8_t *p) {
+  return *reinterpret_cast<const uint32_t *>(p);
+}
+
+template <bool SNAP>
+__global__ void __launch_bounds__(tmac::THREADS, 4) be_cls_tma_kernel(
+    float *__restrict__ dst, float *__restrict__ snap, const __grid_constant__ CondMaps maps,
+    const uint32_t *__restrict__ patterns, int ncls, int nx, int ny, int nz, int bi, Params P) {
+  using namespace tmac;
+  extern __shared__ __align__(128) unsigned char dsm[];
+  float4 *tab = reinterpret_cast<float4 *>(dsm + OFF_TAB);
+  float *gt = reinterpret_cast<float *>(dsm + OFF_GT);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(dsm + OFF_BAR);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool producer = threadIdx.x == 0;
+  const int j0 = blockIdx.y * ROWS, k0 = blockIdx.x * 128;
+  const int i0 = blockIdx.z * bi, i1 = min(i0 + bi, nx);
+  const int pbase = i0 - 1;
+  if (producer) {
+    for (int q = 0; q < NST; ++q) mbar_init(&bars[q], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  build_class_table(tab, gt, patterns, ncls, P);  // ends with a barrier
+  auto issue = [&](int p) {
+    const int q = (p - pbase) % NST;
+    unsigned char *base = dsm + q * STAGE;
+    const bool own = !SNAP && p >= i0 && p < i1;  // T_old only for the computed planes
+    mbar_expect_tx(&bars[q], (uint32_t)(TB + CB + (own ? OB : 0)));
+    tma_load3(base, &maps.t, k0 - TP, j0 - 1, p, &bars[q]);
+    tma_load3(base + OFF_C, &maps.c, k0 - CP, j0 - 1, p, &bars[q]);
+    if (own) tma_load3(base + OFF_O, &maps.o, k0, j0, p, &bars[q]);
+  };
+  bool ok = true;
+  auto wait = [&](int p) {
+    const int n = p - pbase;
+    if (!mbar_wait(&bars[n % NST], (uint32_t)((n / NST) & 1))) ok = false;
+  };
+  auto tst = [&](int p) {
+    return reinterpret_cast<const float *>(dsm + ((p - pbase) % NST) * STAGE);
+  };
+  auto cst = [&](int p) { return dsm + ((p - pbase) % NST) * STAGE + OFF_C; };
+  auto ost = [&](int p) {
+    return reinterpret_cast<const float *>(dsm + ((p - pbase) % NST) * STAGE + OFF_O);
+  };
+  if (producer)
+    for (int p = pbase; p <= min(pbase + NST - 1, i1); ++p) issue(p);
+  const int rr = warp + 1;  // tile row of this warp's output row
+  const int j = j0 + warp;
+  const int k = k0 + lane * 4;
+  const bool act = j < ny && k < nz;
+  const float tamb = P.tamb;
+  const int64_t plane = (int64_t)ny * nz;
+  const int tro = rr * TW + TP + lane * 4, cro = rr * CW + CP + lane * 4;
+  wait(pbase);
+  float4 pm = amb04(lds4(tst(pbase) + tro), lds32(cst(pbase) + cro), tamb);
+  wait(i0);
+  uint32_t wc = lds32(cst(i0) + cro);
+  float4 pcr = lds4(tst(i0) + tro);
+  float4 pc = amb04(pcr, wc, tamb);
+  __syncthreads();  // stage pbase is free
+  if (producer && pbase + NST <= i1) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    issue(pbase + NST);
+  }
+  int64_t o = (int64_t)i0 * plane + (int64_t)j * nz + k;
+  for (int i = i0; i < i1; ++i, o += plane) {
+    wait(i + 1);
+    const uint32_t wn = lds32(cst(i + 1) + cro);
+    const float4 pnr = lds4(tst(i + 1) + tro);
+    const float4 pn = amb04(pnr, wn, tamb);
+    const float *tc = tst(i);
+    const uint8_t *cc = cst(i);
+    const float4 pjm = amb04(lds4(tc + tro - TW), lds32(cc + cro - CW), tamb);
+    const float4 pjp = amb04(lds4(tc + tro + TW), lds32(cc + cro + CW), tamb);
+    float pkm = __shfl_up_sync(0xffffffffu, pc.w, 1);
+    float pkp = __shfl_down_sync(0xffffffffu, pc.x, 1);
+    if (lane == 0) pkm = cc[cro - 1] ? tc[tro - 1] : tamb;
+    if (lane == 31) pkp = cc[cro + 4] ? tc[tro + 4] : tamb;
+    if (SNAP && act) st4(snap + o, pcr);
+    if (__any_sync(0xffffffffu, act && wc != 0u)) {
+      const float4 tov = SNAP ? pcr : lds4(ost(i) + warp * 128 + lane * 4);
+      const float4 pb = make_float4(pkm, pc.x, pc.y, pc.z);
+      const float4 pf = make_float4(pc.y, pc.z, pc.w, pkp);
+      float o4[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const uint32_t c = byte_of(wc, q);
+        const float4 A = tab[2 * c], B = tab[2 * c + 1];
+        float rhs = __fadd_rn(0.0f, __fmul_rn(A.y, f4(pm, q)));
+        rhs = __fadd_rn(rhs, __fmul_rn(A.z, f4(pn, q)));
+        rhs = __fadd_rn(rhs, __fmul_rn(A.w, f4(pjm, q)));
+        rhs = __fadd_rn(rhs, __fmul_rn(B.x, f4(pjp, q)));
+        rhs = __fadd_rn(rhs, __fmul_rn(B.y, f4(pb, q)));
+        rhs = __fadd_rn(rhs, __fmul_rn(B.z, f4(pf, q)));
+        o4[q] = __fdiv_rn(__fadd_rn(f4(tov, q), rhs), A.x);
+      }
+      if (act && wc != 0u) {
+        if (!has_zero_byte(wc)) {
+          st4(dst + o, make_float4(o4[0], o4[1], o4[2], o4[3]));
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (byte_of(wc, q) != 0u) dst[o + q] = o4[q];
+        }
+      }
+    }
+    __syncthreads();  // stage i is free
+    if (producer && i + NST <= i1) {
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      issue(i + NST);
+    }
+    pm = pc;
+    pc = pn;
+    pcr = pnr;
+    wc = wn;
+  }
+  if (producer)  // no copy may still be in flight when the CTA's shared memory goes away
+    for (int p = max(pbase, i1 - NST + 1); p <= i1; ++p) wait(p);
+  if (!ok) atomicExch(&g_cond_err, 1);
+}
+
+// Class kernel for any shape or alignment: one thread per cell.
+template <bool SNAP>
+__global__ void __launch_bounds__(256) be_cls_generic_kernel(
+    float *__restrict__ dst, const float *__restrict__ src, const float *__restrict__ told,
+    float *__restrict__ snap, const uint8_t *__restrict__ cls,
+    const uint32_t *__restrict__ patterns, int ncls, int nx, int ny, int nz, Params P) {
+  __shared__ float4 tab[2 * NCLS];
+  __shared__ float gt[MAXM * MAXM];
+  build_class_table(tab, gt, patterns, ncls, P);
+  const int64_t n = (int64_t)nx * ny * nz, plane = (int64_t)ny * nz;
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    if (SNAP) snap[c] = __ldg(src + c);
+    const uint32_t cl = __ldg(cls + c);
+    if (cl == 0u) continue;
+    const int k = (int)(c % nz);
+    const int64_t t = c / nz;
+    const int j = (int)(t % ny), i = (int)(t / ny);
+#define NB(cond, off) ((cond) && __ldg(cls + c + (off)) ? __ldg(src + c + (off)) : P.tamb)
+    const float tv[6] = {NB(i > 0, -plane), NB(i + 1 < nx, plane), NB(j > 0, -(int64_t)nz),
+                         NB(j + 1 < ny, (int64_t)nz), NB(k > 0, -1), NB(k + 1 < nz, 1)};
+#undef NB
+    const float4 A = tab[2 * cl], B = tab[2 * cl + 1];
+    const float g[6] = {A.y, A.z, A.w, B.x, B.y, B.z};
+    float rhs = 0.0f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) rhs = __fadd_rn(rhs, __fmul_rn(g[f], tv[f]));
+    const float to = SNAP ? __ldg(src + c) : __ldg(told + c);
+    dst[c] = __fdiv_rn(__fadd_rn(to, rhs), A.x);
+  }
+}
+
 // ---- generic kernel: one thread per cell, any shape or alignment ---------------------
 template <class MatT, bool SNAP>
 __global__ void __launch_bounds__(256) be_generic_kernel(float *__restrict__ dst,
@@ -401,6 +817,108 @@ int be_step(float *T, float *T_alt, float *T_old, const MatT *mat, int nx, int n
   return (int)e;
 }
 
+bool g_cond_tma = true;  // TMA-fed class kernel when the layout allows it
+
+int tma_bi(int nx, int ny, int nz) {
+  if (g_cond_bi > 0) return g_cond_bi;
+  const int64_t cols = (int64_t)((nz + 127) / 128) * ((ny + tmac::ROWS - 1) / tmac::ROWS);
+  int bi = 32;
+  while (bi > 8 && cols * ((nx + bi - 1) / bi) < 8LL * num_sms()) bi >>= 1;
+  return bi;
+}
+
+template <bool SNAP>
+bool launch_cls_tma(float *dst, const float *src, const float *told, float *snap,
+                    const uint8_t *cls, const uint32_t *patterns, int ncls, int nx, int ny, int nz,
+                    const Params &P, cudaStream_t s) {
+  using namespace tmac;
+  if (!g_cond_tma || nz % 16 || !al16(dst) || (SNAP && !al16(snap))) return false;
+  CondMaps maps;
+  if (!make_map(&maps.t, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, src, nx, ny, nz, TW, TR) ||
+      !make_map(&maps.c, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, cls, nx, ny, nz, CW, TR))
+    return false;
+  if (!SNAP && !make_map(&maps.o, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, told, nx, ny, nz, 128, ROWS))
+    return false;
+  if (SNAP) maps.o = maps.t;
+  static cudaError_t attr[2] = {cudaErrorNotReady, cudaErrorNotReady};
+  cudaError_t &a = attr[SNAP ? 1 : 0];
+  if (a == cudaErrorNotReady)
+    a = cudaFuncSetAttribute(be_cls_tma_kernel<SNAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             TOTAL);
+  if (a != cudaSuccess) return false;
+  const int bi = tma_bi(nx, ny, nz);
+  dim3 grid((nz + 127) / 128, (ny + ROWS - 1) / ROWS, (nx + bi - 1) / bi);
+  be_cls_tma_kernel<SNAP><<<grid, THREADS, TOTAL, s>>>(dst, snap, maps, patterns, ncls, nx, ny,
+                                                       nz, bi, P);
+  return true;
+}
+
+template <bool SNAP>
+cudaError_t launch_cls_sweep(float *dst, const float *src, const float *told, float *snap,
+                             const uint8_t *cls, const uint32_t *patterns, int ncls, int nx,
+                             int ny, int nz, const Params &P, cudaStream_t s) {
+  if (launch_cls_tma<SNAP>(dst, src, told, snap, cls, patterns, ncls, nx, ny, nz, P, s))
+    return cudaGetLastError();
+  const bool col_ok = nz % 4 == 0 && al16(dst) && al16(src) &&
+                      (SNAP ? al16(snap) : al16(told)) && (((uintptr_t)cls & 3u) == 0);
+  if (col_ok) {
+    const int bi = g_cond_bi > 0 ? g_cond_bi : pick_bi(nx, ny, nz);
+    dim3 grid((nz / 4 + 31) / 32, (ny + 7) / 8, (nx + bi - 1) / bi);
+    if (nz % 128 == 0)
+      be_cls_col_kernel<true, SNAP><<<grid, 256, 0, s>>>(dst, src, told, snap, cls, patterns,
+                                                         ncls, nx, ny, nz, bi, P);
+    else
+      be_cls_col_kernel<false, SNAP><<<grid, 256, 0, s>>>(dst, src, told, snap, cls, patterns,
+                                                          ncls, nx, ny, nz, bi, P);
+  } else {
+    const int64_t n = (int64_t)nx * ny * nz;
+    int64_t b = (n + 255) / 256, cap = (int64_t)num_sms() * 16;
+    be_cls_generic_kernel<SNAP><<<(int)(b < cap ? b : cap), 256, 0, s>>>(
+        dst, src, told, snap, cls, patterns, ncls, nx, ny, nz, P);
+  }
+  return cudaGetLastError();
+}
+
+size_t prepare_workspace_bytes() { return 2 * sizeof(uint32_t) * NKEYWORDS + 256; }
+
+template <class MatT>
+int prepare(uint8_t *cls, uint32_t *patterns, int *n_classes_host, const MatT *mat, int nx,
+            int ny, int nz, int n_mat, int mat_air, void *ws, size_t ws_bytes, cudaStream_t s) {
+  if (!cls || !patterns || !n_classes_host || !mat || !ws) return BSP_ERR_NULL;
+  if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_ERR_SHAPE;
+  if (n_mat < 1 || n_mat > MAXM - 1 || mat_air < 0 || mat_air >= n_mat) return BSP_ERR_ARG;
+  if (ws_bytes < prepare_workspace_bytes() || ((uintptr_t)ws & 15u)) return BSP_ERR_WORKSPACE;
+  uint32_t *bitmap = static_cast<uint32_t *>(ws);
+  uint32_t *base = bitmap + NKEYWORDS;
+  int *count = reinterpret_cast<int *>(base + NKEYWORDS);
+  const int64_t n = (int64_t)nx * ny * nz;
+  int64_t b = (n + 255) / 256, cap = (int64_t)num_sms() * 16;
+  const int blocks = (int)(b < cap ? b : cap);
+  cudaError_t e = cudaMemsetAsync(bitmap, 0, sizeof(uint32_t) * NKEYWORDS, s);
+  if (e != cudaSuccess) return (int)e;
+  cls_mark_kernel<MatT><<<blocks, 256, 0, s>>>(bitmap, mat, nx, ny, nz, (uint32_t)mat_air);
+  cls_scan_kernel<<<1, SCAN_THREADS, 0, s>>>(base, bitmap, count);
+  int host_count = 0;
+  e = cudaMemcpyAsync(&host_count, count, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return (int)e;
+  *n_classes_host = host_count + 1;
+  if (host_count + 1 > NCLS) return BSP_ERR_CAPACITY;
+  cls_assign_kernel<MatT><<<blocks, 256, 0, s>>>(cls, patterns, bitmap, base, mat, nx, ny, nz,
+                                                 (uint32_t)mat_air);
+  return (int)cudaGetLastError();
+}
+
+int cls_args(const void *a, const void *b, const uint8_t *cls, const uint32_t *patterns,
+             int ncls, const float *k, const float *rho, const float *cp, int n_mat, int mat_air,
+             float dx) {
+  if (!a || !b || !cls || !patterns || !k || !rho || !cp) return BSP_ERR_NULL;
+  if (ncls < 1 || ncls > NCLS || n_mat < 1 || n_mat > MAXM - 1 || mat_air < 0 ||
+      mat_air >= n_mat || !(dx > 0.0f))
+    return BSP_ERR_ARG;
+  return BSP_OK;
+}
+
 }  // namespace cond
 }  // namespace bsp
 
@@ -450,4 +968,70 @@ extern "C" int bsp_material_ids(uint8_t *mat_id, const int32_t *mat, int64_t n, 
   int64_t b = (n + 255) / 256, cap = (int64_t)bsp::num_sms() * 16;
   narrow_kernel<<<(int)(b < cap ? b : cap), 256, 0, s>>>(mat_id, mat, n, n_mat, bad_count_dev);
   return (int)cudaGetLastError();
+}
+
+extern "C" size_t bsp_conduction_prepare_workspace_bytes(void) {
+  return prepare_workspace_bytes();
+}
+
+extern "C" int bsp_conduction_prepare(uint8_t *cls, uint32_t *patterns, int *n_classes_host,
+                                      const int32_t *mat, int nx, int ny, int nz, int n_mat,
+                                      int mat_air, void *workspace, size_t workspace_bytes,
+                                      cudaStream_t s) {
+  return prepare<int32_t>(cls, patterns, n_classes_host, mat, nx, ny, nz, n_mat, mat_air,
+                          workspace, workspace_bytes, s);
+}
+
+extern "C" int bsp_conduction_sweep_cls(float *T_dst, const float *T_iter, const float *T_old,
+                                        const uint8_t *cls, const uint32_t *patterns,
+                                        int n_classes, int nx, int ny, int nz, const float *k,
+                                        const float *rho, const float *cp, int n_mat, float dx,
+                                        float dt, float h_conv_air, float T_amb, int mat_air,
+                                        cudaStream_t s) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_OK;
+  int st = cls_args(T_dst, T_iter, cls, patterns, n_classes, k, rho, cp, n_mat, mat_air, dx);
+  if (st != BSP_OK) return st;
+  if (!T_old) return BSP_ERR_NULL;
+  if (T_dst == T_iter) return BSP_ERR_ARG;
+  const Params P{k, rho, cp, n_mat, dx, dt, h_conv_air, T_amb, mat_air};
+  return (int)launch_cls_sweep<false>(T_dst, T_iter, T_old, nullptr, cls, patterns, n_classes,
+                                      nx, ny, nz, P, s);
+}
+
+extern "C" int bsp_conduction_be_cls(float *T, float *T_alt, float *T_old, const uint8_t *cls,
+                                     const uint32_t *patterns, int n_classes, int nx, int ny,
+                                     int nz, const float *k, const float *rho, const float *cp,
+                                     int n_mat, float dx, float dt, float h_conv_air,
+                                     float T_amb, int mat_air, int n_iter, cudaStream_t s) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_OK;
+  int st = cls_args(T, T_alt, cls, patterns, n_classes, k, rho, cp, n_mat, mat_air, dx);
+  if (st != BSP_OK) return st;
+  if (!T_old) return BSP_ERR_NULL;
+  if (n_iter < 0 || T == T_alt || T == T_old || T_alt == T_old) return BSP_ERR_ARG;
+  const size_t bytes = sizeof(float) * (size_t)nx * ny * nz;
+  const Params P{k, rho, cp, n_mat, dx, dt, h_conv_air, T_amb, mat_air};
+  if (n_iter == 0) return (int)cudaMemcpyAsync(T_old, T, bytes, cudaMemcpyDeviceToDevice, s);
+  cudaError_t e = launch_cls_sweep<true>(T_alt, T, nullptr, T_old, cls, patterns, n_classes, nx,
+                                         ny, nz, P, s);
+  for (int it = 1; it < n_iter && e == cudaSuccess; ++it) {
+    const float *src = (it % 2 == 0) ? T : T_alt;
+    float *dst = (it % 2 == 0) ? T_alt : T;
+    e = launch_cls_sweep<false>(dst, src, T_old, nullptr, cls, patterns, n_classes, nx, ny, nz,
+                                P, s);
+  }
+  if (e == cudaSuccess && n_iter % 2 == 1)
+    e = cudaMemcpyAsync(T, T_alt, bytes, cudaMemcpyDeviceToDevice, s);
+  return (int)e;
+}
+
+extern "C" int bsp_conduction_error(int *flag_host) {
+  if (!flag_host) return BSP_ERR_NULL;
+  int v = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&v, bsp::cond::g_cond_err, sizeof(int));
+  if (e == cudaSuccess) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbol(bsp::cond::g_cond_err, &zero, sizeof(int));
+  }
+  *flag_host = v;
+  return (int)e;
 }

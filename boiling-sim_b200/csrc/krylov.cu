@@ -178,6 +178,7 @@ extern "C" const char *bsp_error_string(int code) {
     case BSP_ERR_TIMEOUT: return "BSP_ERR_TIMEOUT: device-side wait gave up";
     case BSP_ERR_ALIGN: return "BSP_ERR_ALIGN: pointer alignment unusable";
     case BSP_ERR_ARG: return "BSP_ERR_ARG: invalid argument";
+    case BSP_ERR_CAPACITY: return "BSP_ERR_CAPACITY: more distinct cell classes than the table holds";
     default: return cudaGetErrorString((cudaError_t)code);
   }
 }

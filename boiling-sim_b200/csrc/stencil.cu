@@ -504,6 +504,10 @@ extern bool g_coarse_fused_enabled;
 extern bool g_fuse_update_enabled;
 extern int g_fine_bi;
 extern int g_sweep_tblock;
+namespace cond {
+extern int g_cond_bi;
+extern bool g_cond_tma;
+}  // namespace cond
 }
 
 extern "C" int bsp_set_tuning(int key, int value) {
@@ -539,6 +543,14 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_SWEEP_TBLOCK:
       if (value < 1 || value > 2) return BSP_ERR_ARG;
       bsp::g_sweep_tblock = value;
+      return BSP_OK;
+    case BSP_TUNE_COND_BI:
+      if (value < 0 || value > 4096) return BSP_ERR_ARG;
+      bsp::cond::g_cond_bi = value;
+      return BSP_OK;
+    case BSP_TUNE_COND_TMA:
+      if (value < 0 || value > 1) return BSP_ERR_ARG;
+      bsp::cond::g_cond_tma = value != 0;
       return BSP_OK;
     default:
       return BSP_ERR_ARG;

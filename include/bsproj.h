@@ -42,6 +42,7 @@ extern "C" {
 #define BSP_ERR_TIMEOUT 10007      /* device-side wait gave up */
 #define BSP_ERR_ALIGN 10008        /* pointer alignment unusable */
 #define BSP_ERR_ARG 10009          /* other invalid argument */
+#define BSP_ERR_CAPACITY 10010     /* more distinct cell classes than a table holds */
 
 /* uint8 cell mask: bit 7 fluid, bit 6 solid (air: neither -- a zero byte is
  * air, like a cell outside the grid), bits 0-2 number of solid face neighbours */
@@ -59,6 +60,8 @@ extern "C" {
 #define BSP_TUNE_FUSE_UPDATE 6  /* CG update fused into the next restriction (TMA path): 1 on, 0 off */
 #define BSP_TUNE_FINE_BI 7      /* i-planes per CTA tile of the solver's level-0 kernels (0 = rule) */
 #define BSP_TUNE_SWEEP_TBLOCK 8 /* sweeps per HBM pass when a call passes tblock = 0 (1 or 2) */
+#define BSP_TUNE_COND_BI 9      /* i-planes per CTA of the conduction sweeps (0 = rule) */
+#define BSP_TUNE_COND_TMA 10    /* conduction class sweep fed by TMA tiles: 1 on, 0 off */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */
@@ -388,6 +391,35 @@ int bsp_conduction_be_u8(float *T, float *T_alt, float *T_old, const uint8_t *ma
  * outside [0, n_mat) are counted into *bad_count_dev (may be NULL). */
 int bsp_material_ids(uint8_t *mat_id, const int32_t *mat, int64_t n, int n_mat,
                      int *bad_count_dev, cudaStream_t stream);
+
+/* Cell classes for the conduction sweep.  A non-air cell's update depends
+ * only on its material and its six neighbours' (domain edge included), so the
+ * distinct neighbourhoods of a geometry are numbered once: cls[c] = class of
+ * cell c (0 = air), patterns[0 .. n_classes) = each class's neighbourhood key
+ * (own id | code(-x) << 3 | code(+x) << 6 | ... | code(+z) << 18, code 7 = domain
+ * edge).  Requires n_mat <= 7.  Synchronises the stream once (reads the class
+ * count into *n_classes_host); returns BSP_ERR_CAPACITY when the geometry has
+ * more than 255 classes (use the material-id entry points then).  patterns
+ * holds 256 entries. */
+size_t bsp_conduction_prepare_workspace_bytes(void);
+int bsp_conduction_prepare(uint8_t *cls, uint32_t *patterns, int *n_classes_host,
+                           const int32_t *mat, int nx, int ny, int nz, int n_mat, int mat_air,
+                           void *workspace, size_t workspace_bytes, cudaStream_t stream);
+/* The sweep and the step of bsp_conduction_sweep / bsp_conduction_be on cell
+ * classes: the same results bit for bit, one class byte per cell. */
+int bsp_conduction_sweep_cls(float *T_dst, const float *T_iter, const float *T_old,
+                             const uint8_t *cls, const uint32_t *patterns, int n_classes, int nx,
+                             int ny, int nz, const float *k, const float *rho, const float *cp,
+                             int n_mat, float dx, float dt, float h_conv_air, float T_amb,
+                             int mat_air, cudaStream_t stream);
+/* Read and clear the device flag that a TMA-fed conduction sweep sets when a
+ * bounded wait gave up (its results are then not valid); synchronous. */
+int bsp_conduction_error(int *flag_host);
+int bsp_conduction_be_cls(float *T, float *T_alt, float *T_old, const uint8_t *cls,
+                          const uint32_t *patterns, int n_classes, int nx, int ny, int nz,
+                          const float *k, const float *rho, const float *cp, int n_mat, float dx,
+                          float dt, float h_conv_air, float T_amb, int mat_air, int n_iter,
+                          cudaStream_t stream);
 
 /* ---- learned warm start: U-Net layers --------------------------------------
  * Building blocks of the pressure warm-start network (a 3-level 3-D U-Net

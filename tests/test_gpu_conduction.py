@@ -6,6 +6,8 @@ fused snapshot, odd and even sweep counts, the pot scene at 192x192x128 and
 384x384x256, and the argument checks."""
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 import pytest
 import torch
@@ -122,6 +124,7 @@ def pot_temperature(mat, rng):
 
 @pytest.mark.parametrize("spec,n_iter", [(S.pot_192(), 50), (S.POT_384, 3)])
 def test_pot_scene_bit_exact(cuda, spec, n_iter):
+    """The production path: cell classes, TMA-fed sweeps."""
     rng = np.random.default_rng(7)
     mat = S.pot_mat(spec)
     T = pot_temperature(mat, rng)
@@ -135,9 +138,112 @@ def test_pot_scene_bit_exact(cuda, spec, n_iter):
     cfg.solver.diffusion_max_iter = n_iter
     cfg.heating.ambient_temp_c = TAMB - 273.15
     TH.implicit_conduction_step(grid, p, ws, cfg, 0.01)
+    assert grid.classes, "the pot scene should sweep on cell classes"
+    flag = ctypes.c_int(0)
+    call("bsp_conduction_error", ctypes.byref(flag))
+    assert flag.value == 0
     assert np.array_equal(bits(host(grid.T)), bits(wT))
     assert np.array_equal(bits(host(ws.T_iter_alt)), bits(wa))
     assert np.array_equal(bits(host(ws.T_old_snapshot)), bits(wo))
+
+
+def block_grid(shape):
+    """Nested boxes: an air border, a steel shell (open above mid height), water
+    with air above three quarters of the height, and a carrot block -- all
+    material pairs, the domain edge, and about a hundred distinct cell
+    neighbourhoods."""
+    nx, ny, nz = shape
+    i = np.arange(nx)[:, None, None]
+    j = np.arange(ny)[None, :, None]
+    k = np.arange(nz)[None, None, :]
+
+    def inside(m):
+        return (i >= m) & (i < nx - m) & (j >= m) & (j < ny - m) & (k >= m) & (k < nz - m)
+
+    mat = np.full(shape, TH.MAT_AIR, np.int32)
+    mat[inside(1) | ((k < nz // 2) & inside(0))] = TH.MAT_POT_WALL
+    mat[inside(2)] = TH.MAT_FLUID
+    mat[inside(2) & (k > (3 * nz) // 4)] = TH.MAT_AIR
+    mat[inside(3) & (np.abs(i - nx // 2) <= nx // 5) & (np.abs(j - ny // 2) <= ny // 5)
+        & (np.abs(k - nz // 3) <= nz // 6)] = TH.MAT_CARROT
+    return mat
+
+
+BSP_TUNE_COND_TMA = 10
+
+
+@pytest.fixture
+def tma_mode(request):
+    call("bsp_set_tuning", BSP_TUNE_COND_TMA, int(request.param))
+    yield request.param
+    call("bsp_set_tuning", BSP_TUNE_COND_TMA, 1)
+    flag = ctypes.c_int(0)
+    call("bsp_conduction_error", ctypes.byref(flag))
+    assert flag.value == 0, "a TMA-fed sweep gave up waiting"
+
+
+@pytest.mark.parametrize("tma_mode", [True, False], indirect=True)
+@pytest.mark.parametrize("shape", SHAPES + [(8, 12, 144), (5, 9, 16), (17, 3, 384)])
+def test_class_sweep_bit_exact(cuda, shape, tma_mode):
+    rng = np.random.default_rng(sum(shape) + 100)
+    mat = block_grid(shape)
+    T = (280 + 40 * rng.random(shape)).astype(np.float32)
+    Told = (280 + 40 * rng.random(shape)).astype(np.float32)
+    junk = (1000 * rng.random(shape)).astype(np.float32)
+    p, hp = props()
+    want = O.conduction_sweep(junk, T, Told, mat, hp, DX, DT, H, TAMB)
+    c = TH.cell_classes(dev(mat, torch.int32))
+    assert c is not None and 1 <= c.n_classes <= 256
+    # classes are dense 1..n on non-air cells, 0 on air
+    cl = host(c.cls)
+    assert np.array_equal(cl == 0, mat == TH.MAT_AIR)
+    if (mat != TH.MAT_AIR).any():
+        assert cl.max() == c.n_classes - 1
+    out, t_iter, t_old = dev(junk), dev(T), dev(Told)  # keep the inputs alive over the call
+    call("bsp_conduction_sweep_cls", ptr(out), ptr(t_iter), ptr(t_old), ptr(c.cls),
+         ptr(c.patterns), c.n_classes, *shape, ptr(p.k_wp), ptr(p.rho_wp), ptr(p.cp_wp), 4, DX,
+         DT, H, TAMB, TH.MAT_AIR, 0)
+    assert np.array_equal(bits(host(out)), bits(want))
+
+
+@pytest.mark.parametrize("tma_mode", [True, False], indirect=True)
+@pytest.mark.parametrize("n_iter", [0, 1, 2, 7])
+@pytest.mark.parametrize("shape", [(8, 12, 128), (6, 7, 9), (10, 9, 48)])
+def test_class_step_bit_exact(cuda, shape, n_iter, tma_mode):
+    rng = np.random.default_rng(n_iter + 31)
+    mat = block_grid(shape)
+    T = (280 + 40 * rng.random(shape)).astype(np.float32)
+    alt = (1000 * rng.random(shape)).astype(np.float32)
+    p, hp = props()
+    wT, wa, wo = O.conduction_be(T, alt, mat, hp, DX, DT, H, TAMB, n_iter)
+    grid = TH.ThermalGrid(*shape, DX, dev(T), dev(mat, torch.int32))
+    ws = TH.ThermalWorkspace(torch.full(shape, -3.0, device="cuda"), dev(alt))
+    cfg = TH.ThermalConfig()
+    cfg.solver.diffusion_max_iter = n_iter
+    cfg.heating.ambient_temp_c = TAMB - 273.15
+    TH.implicit_conduction_step(grid, p, ws, cfg, DT)
+    assert grid.classes
+    assert np.array_equal(bits(host(grid.T)), bits(wT))
+    assert np.array_equal(bits(host(ws.T_iter_alt)), bits(wa))
+    assert np.array_equal(bits(host(ws.T_old_snapshot)), bits(wo))
+
+
+def test_too_many_classes_falls_back_to_material_ids(cuda):
+    rng = np.random.default_rng(9)
+    shape = (24, 24, 32)
+    mat = rng.integers(0, 4, shape).astype(np.int32)
+    assert TH.cell_classes(dev(mat, torch.int32)) is None  # thousands of neighbourhoods
+    T = (280 + 40 * rng.random(shape)).astype(np.float32)
+    p, hp = props()
+    wT, wa, wo = O.conduction_be(T, np.zeros_like(T), mat, hp, DX, DT, H, TAMB, 4)
+    grid = TH.ThermalGrid(*shape, DX, dev(T), dev(mat, torch.int32))
+    ws = TH.allocate_thermal_workspace(grid)
+    cfg = TH.ThermalConfig()
+    cfg.solver.diffusion_max_iter = 4
+    cfg.heating.ambient_temp_c = TAMB - 273.15
+    TH.implicit_conduction_step(grid, p, ws, cfg, DT)
+    assert grid.classes is False and grid.mat_id is not None
+    assert np.array_equal(bits(host(grid.T)), bits(wT))
 
 
 def test_argument_checks(cuda):
