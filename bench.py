@@ -229,7 +229,8 @@ def conduction_bench(mat, dev, peak, peak_kind, cpu: bool):
     c = grid.classes
     if c:
         ms_cls = time_sweeps("bsp_conduction_sweep_cls",
-                             [_lib.ptr(c.cls), _lib.ptr(c.patterns), c.n_classes],
+                             [_lib.ptr(c.cls), _lib.ptr(c.patterns), c.n_classes,
+                              _lib.ptr(c.tiles)],
                              [TH.MAT_AIR])
         out["sweep"] = sweep_entry("be_cls_tma_kernel" if nz % 16 == 0 else "be_cls_col_kernel",
                                    ms_cls)

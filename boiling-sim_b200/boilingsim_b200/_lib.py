@@ -71,10 +71,12 @@ SIGNATURES = {
     "bsp_conduction_error": (_I, [_P]),
     "bsp_conduction_prepare": (_I, [_P, _P, ctypes.POINTER(ctypes.c_int), _P, _I, _I, _I, _I, _I,
                                     _P, ctypes.c_size_t, _P]),
-    "bsp_conduction_sweep_cls": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _I, _F, _F,
-                                      _F, _F, _I, _P]),
-    "bsp_conduction_be_cls": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _P, _P, _P, _I, _F, _F, _F,
-                                   _F, _I, _I, _P]),
+    "bsp_conduction_tile_flags_bytes": (ctypes.c_size_t, [_I, _I, _I]),
+    "bsp_conduction_tile_flags": (_I, [_P, _P, _I, _I, _I, _P]),
+    "bsp_conduction_sweep_cls": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _I, _I, _P, _P, _P, _I, _F,
+                                      _F, _F, _F, _I, _P]),
+    "bsp_conduction_be_cls": (_I, [_P, _P, _P, _P, _P, _I, _P, _I, _I, _I, _P, _P, _P, _I, _F, _F,
+                                   _F, _F, _I, _I, _P]),
     # learned warm start (unet.cu)
     "bsp_unet_conv3_fwd": (_I, [_P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
     "bsp_unet_wgrad_workspace_bytes": (ctypes.c_size_t, [_I, _I, _I, _I, _I]),

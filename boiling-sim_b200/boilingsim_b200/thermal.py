@@ -16,7 +16,7 @@ Drop-in for the implicit-conduction part of ``python/boilingsim/thermal.py``:
   source terms that ``conduct_one_step`` applies afterwards (stove base flux,
   evaporative cooling) are the caller's.  The first call on a grid numbers its
   cell neighbourhoods (``cell_classes``) and later calls sweep on those class
-  bytes; a geometry with more than 255 neighbourhoods uses material ids.
+  bytes; a geometry with more than 127 neighbourhoods uses material ids.
 
 Every call runs the sm_100a kernels of libbsproj.so on the caller's stream;
 results are bit-identical to the reference arithmetic.  There is no CPU path.
@@ -137,15 +137,16 @@ class CellClasses:
     """Conduction cell classes of a geometry (bsp_conduction_prepare): one byte
     per cell naming its neighbourhood, and each class's neighbourhood key."""
 
-    cls: torch.Tensor       # (nx, ny, nz) uint8, 0 = air
+    cls: torch.Tensor       # (nx, ny, nz) uint8, 0x80 = air
     patterns: torch.Tensor  # (256,) int32 keys
     n_classes: int
+    tiles: torch.Tensor | None = None  # tile occupancy for the TMA sweep (nz % 4 == 0)
 
 
 def cell_classes(mat: torch.Tensor, n_mat: int = 4, mat_air: int = MAT_AIR,
                  stream=None) -> CellClasses | None:
     """Number the distinct cell neighbourhoods of ``mat``; None when there are
-    more than 255 (the material-id kernels then serve the geometry)."""
+    more than 127 (the material-id kernels then serve the geometry)."""
     import ctypes
 
     from . import _lib
@@ -164,7 +165,13 @@ def cell_classes(mat: torch.Tensor, n_mat: int = 4, mat_air: int = MAT_AIR,
     if code == 10010:  # BSP_ERR_CAPACITY
         return None
     _lib.check("bsp_conduction_prepare", code)
-    return CellClasses(cls, patterns, int(n.value))
+    tiles = None
+    if nz % 4 == 0:
+        tiles = torch.empty(int(_lib.lib().bsp_conduction_tile_flags_bytes(nx, ny, nz)),
+                            dtype=torch.uint8, device=mat.device)
+        call("bsp_conduction_tile_flags", ptr(tiles), ptr(cls), nx, ny, nz,
+             stream_handle(stream))
+    return CellClasses(cls, patterns, int(n.value), tiles)
 
 
 def _check_f32(*ts):
@@ -206,8 +213,8 @@ def implicit_conduction_step(grid, props: MaterialProps, ws: ThermalWorkspace, c
     if grid.classes:
         c = grid.classes
         call("bsp_conduction_be_cls", ptr(grid.T), ptr(ws.T_iter_alt), ptr(ws.T_old_snapshot),
-             ptr(c.cls), ptr(c.patterns), c.n_classes, nx, ny, nz, *props_args, float(grid.dx),
-             float(dt), h, T_amb_k, MAT_AIR, n_iter, stream_handle(stream))
+             ptr(c.cls), ptr(c.patterns), c.n_classes, ptr(c.tiles), nx, ny, nz, *props_args,
+             float(grid.dx), float(dt), h, T_amb_k, MAT_AIR, n_iter, stream_handle(stream))
         return
     if getattr(grid, "mat_id", None) is None:
         grid.mat_id = material_ids(grid.mat, props.n_mat, stream)

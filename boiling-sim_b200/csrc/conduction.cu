@@ -270,12 +270,17 @@ __global__ void __launch_bounds__(256) be_col_kernel(float *__restrict__ dst,
 // A non-air cell's update is fixed by its own material and the codes of its
 // six neighbours (material id, or EDGE for a face on the domain edge): the
 // key own | code(-x) << 3 | code(+x) << 6 | ... | code(+z) << 18.  The
-// prepare pass numbers the distinct keys of a geometry 1..n (class 0 = air);
-// each CTA then turns the keys into a table of (1 + sum gamma, gamma_-x ..
-// gamma_+z) -- gamma 0 on EDGE faces, the denominator summed in face order as
-// the reference does -- so a cell costs one class byte and two shared loads
-// instead of six table lookups and the diagonal sum.
-constexpr int NCLS = 256;
+// prepare pass numbers the distinct keys of a geometry 1..n (n <= 127); an air
+// cell gets CLS_AIR (sign bit set), and 0 is what a TMA tile reads outside
+// the grid.  Each CTA turns the keys into a table of (1 + sum gamma,
+// gamma_-x .. gamma_+z) -- gamma 0 on EDGE faces, the denominator summed in
+// face order as the reference does -- so a cell costs one class byte and two
+// shared loads instead of six table lookups and the diagonal sum.  A value
+// outside the grid (0) always meets gamma 0; an air value is replaced by
+// T_amb, selected by the class byte's sign bit.
+constexpr int NCLS = 256;  // table entries (ids >= n_classes, air included, are zero)
+constexpr uint32_t CLS_AIR = 0x80u;
+constexpr int CLS_MAX = 127;
 constexpr int KEYBITS = 21;
 constexpr uint32_t NKEYWORDS = 1u << (KEYBITS - 5);
 constexpr uint32_t EDGE = 7u;
@@ -344,7 +349,7 @@ __global__ void cls_assign_kernel(uint8_t *__restrict__ cls, uint32_t *__restric
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += (int64_t)gridDim.x * blockDim.x) {
     if (mbyte(mat, c) == mair) {
-      cls[c] = 0;
+      cls[c] = (uint8_t)CLS_AIR;
       continue;
     }
     const int k = (int)(c % nz);
@@ -352,7 +357,7 @@ __global__ void cls_assign_kernel(uint8_t *__restrict__ cls, uint32_t *__restric
     const uint32_t key = cell_key(mat, c, (int)(t / ny), (int)(t % ny), k, nx, ny, nz, plane);
     const uint32_t w = key >> 5, b = key & 31u;
     const uint32_t id = 1u + __ldg(base + w) + __popc(__ldg(bitmap + w) & ((1u << b) - 1u));
-    cls[c] = (uint8_t)id;  // the host checked id < NCLS
+    cls[c] = (uint8_t)id;  // the host checked id <= CLS_MAX
     patterns[id] = key;    // every cell of a class writes the same key
   }
 }
@@ -385,20 +390,50 @@ __device__ __forceinline__ void build_class_table(float4 *tab, float *gt,
   __syncthreads();
 }
 
-__device__ __forceinline__ float amb0(float v, uint32_t w, int q, float tamb) {
-  return byte_of(w, q) == 0u ? tamb : v;
+// Air values -> T_amb by the sign bit of each class byte (one prmt + one lop3).
+__device__ __forceinline__ float ambq(float v, uint32_t w, int q, uint32_t tb) {
+  const uint32_t m = sign_bytes(w, (uint32_t)(8 | q) * 0x1111u);
+  return __uint_as_float((__float_as_uint(v) & ~m) | (tb & m));
 }
 __device__ __forceinline__ float4 amb04(float4 v, uint32_t w, float tamb) {
-  return make_float4(amb0(v.x, w, 0, tamb), amb0(v.y, w, 1, tamb), amb0(v.z, w, 2, tamb),
-                     amb0(v.w, w, 3, tamb));
+  const uint32_t tb = __float_as_uint(tamb);
+  return make_float4(ambq(v.x, w, 0, tb), ambq(v.y, w, 1, tb), ambq(v.z, w, 2, tb),
+                     ambq(v.w, w, 3, tb));
 }
-__device__ __forceinline__ bool has_zero_byte(uint32_t x) {
-  return ((x - 0x01010101u) & ~x & 0x80808080u) != 0u;
+__device__ __forceinline__ float amb1(float v, uint32_t b, float tamb) {
+  return (b & CLS_AIR) ? tamb : v;
+}
+// A word of four in-grid class bytes: some / every cell is not air.
+__device__ __forceinline__ bool cls_some(uint32_t w) {
+  return (w & 0x80808080u) != 0x80808080u;
+}
+__device__ __forceinline__ bool cls_every(uint32_t w) { return (w & 0x80808080u) == 0u; }
+
+// One cell of class c: rhs over the faces -x, +x, -y, +y, -z, +z in order.
+__device__ __forceinline__ float be_cell(const float4 *tab, uint32_t c, float tm, float tp,
+                                         float tjm, float tjp, float tkm, float tkp, float to) {
+  const float4 A = tab[2 * c], B = tab[2 * c + 1];
+  float rhs = __fadd_rn(0.0f, __fmul_rn(A.y, tm));
+  rhs = __fadd_rn(rhs, __fmul_rn(A.z, tp));
+  rhs = __fadd_rn(rhs, __fmul_rn(A.w, tjm));
+  rhs = __fadd_rn(rhs, __fmul_rn(B.x, tjp));
+  rhs = __fadd_rn(rhs, __fmul_rn(B.y, tkm));
+  rhs = __fadd_rn(rhs, __fmul_rn(B.z, tkp));
+  return __fdiv_rn(__fadd_rn(to, rhs), A.x);
+}
+// Store the non-air cells of a word.
+__device__ __forceinline__ void store_word(float *p, uint32_t w, const float (&v)[4]) {
+  if (cls_every(w)) {
+    *reinterpret_cast<float4 *>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if (!(byte_of(w, q) & CLS_AIR)) p[q] = v[q];
+  }
 }
 
-// Column kernel on class bytes: the layout of be_col_kernel.  A zero class
-// byte is air (and cells outside the grid read as air: their faces have gamma
-// 0 in every class that touches them, so the value substituted, T_amb, adds 0).
+// Column kernel on class bytes (nz % 4 == 0): the layout of be_col_kernel.
+// Words outside the grid are 0 (never loaded; their values are 0).
 template <bool FULL, bool SNAP>
 __global__ void __launch_bounds__(256) be_cls_col_kernel(
     float *__restrict__ dst, const float *__restrict__ src, const float *__restrict__ told,
@@ -419,16 +454,17 @@ __global__ void __launch_bounds__(256) be_cls_col_kernel(
   const float tamb = P.tamb;
   const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
   int64_t o = (int64_t)i0 * plane + (int64_t)j * nz + k;
+  auto live = [](uint32_t w) { return w != 0u && cls_some(w); };  // in grid, not all air
 
   uint32_t wm = 0u, wc = 0u, wjm = 0u, wjp = 0u, wn = 0u;
   float4 pm = z4, pc = z4;
   if (act) {
     if (i0 > 0) {
       wm = mword(cls, o - plane);
-      if (wm) pm = ld4(src + o - plane);
+      if (live(wm)) pm = ld4(src + o - plane);
     }
     wc = mword(cls, o);
-    if (SNAP || wc) pc = ld4(src + o);
+    if (SNAP || live(wc)) pc = ld4(src + o);
     if (SNAP) st4(snap + o, pc);
     if (has_jm) wjm = mword(cls, o - nz);
     if (has_jp) wjp = mword(cls, o + nz);
@@ -441,10 +477,10 @@ __global__ void __launch_bounds__(256) be_cls_col_kernel(
     float4 pn = z4, pjm = z4, pjp = z4, tov = z4;
     uint32_t wn2 = 0u, wjm2 = 0u, wjp2 = 0u;
     if (act) {
-      if (has_in && (SNAP || wn)) pn = ld4(src + o + plane);
-      if (wjm) pjm = ld4(src + o - nz);
-      if (wjp) pjp = ld4(src + o + nz);
-      if (!SNAP && wc) tov = ld4(told + o);
+      if (has_in && (SNAP || live(wn))) pn = ld4(src + o + plane);
+      if (live(wjm)) pjm = ld4(src + o - nz);
+      if (live(wjp)) pjp = ld4(src + o + nz);
+      if (!SNAP && live(wc)) tov = ld4(told + o);
       if (has_in) {
         if (has_jm) wjm2 = mword(cls, o + plane - nz);
         if (has_jp) wjp2 = mword(cls, o + plane + nz);
@@ -458,33 +494,16 @@ __global__ void __launch_bounds__(256) be_cls_col_kernel(
     if (SNAP) tov = pc;
     float pkm = __shfl_up_sync(0xffffffffu, pc.w, 1);
     float pkp = __shfl_down_sync(0xffffffffu, pc.x, 1);
-    if (lane == 0) pkm = act && k > 0 && __ldg(cls + o - 1) ? __ldg(src + o - 1) : tamb;
-    if (lane == 31) pkp = act && k + 4 < nz && __ldg(cls + o + 4) ? __ldg(src + o + 4) : tamb;
-    if (__any_sync(0xffffffffu, act && wc != 0u)) {
-      const float4 pb = make_float4(pkm, pc.x, pc.y, pc.z);
-      const float4 pf = make_float4(pc.y, pc.z, pc.w, pkp);
+    if (lane == 0) pkm = act && k > 0 ? amb1(__ldg(src + o - 1), __ldg(cls + o - 1), tamb) : 0.0f;
+    if (lane == 31)
+      pkp = act && k + 4 < nz ? amb1(__ldg(src + o + 4), __ldg(cls + o + 4), tamb) : 0.0f;
+    if (__any_sync(0xffffffffu, act && live(wc))) {
       float o4[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint32_t c = byte_of(wc, q);
-        const float4 A = tab[2 * c], B = tab[2 * c + 1];
-        float rhs = __fadd_rn(0.0f, __fmul_rn(A.y, f4(pm, q)));
-        rhs = __fadd_rn(rhs, __fmul_rn(A.z, f4(pn, q)));
-        rhs = __fadd_rn(rhs, __fmul_rn(A.w, f4(pjm, q)));
-        rhs = __fadd_rn(rhs, __fmul_rn(B.x, f4(pjp, q)));
-        rhs = __fadd_rn(rhs, __fmul_rn(B.y, f4(pb, q)));
-        rhs = __fadd_rn(rhs, __fmul_rn(B.z, f4(pf, q)));
-        o4[q] = __fdiv_rn(__fadd_rn(f4(tov, q), rhs), A.x);
-      }
-      if (act && wc != 0u) {
-        if (!has_zero_byte(wc)) {
-          st4(dst + o, make_float4(o4[0], o4[1], o4[2], o4[3]));
-        } else {
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            if (byte_of(wc, q) != 0u) dst[o + q] = o4[q];
-        }
-      }
+      for (int q = 0; q < 4; ++q)
+        o4[q] = be_cell(tab, byte_of(wc, q), f4(pm, q), f4(pn, q), f4(pjm, q), f4(pjp, q),
+                        q == 0 ? pkm : f4(pc, q - 1), q == 3 ? pkp : f4(pc, q + 1), f4(tov, q));
+      if (act && live(wc)) store_word(dst + o, wc, o4);
     }
     pm = pc;
     pc = pn;
@@ -496,16 +515,17 @@ __global__ void __launch_bounds__(256) be_cls_col_kernel(
 }
 
 // ---- TMA-fed class kernel ---------------------------------------------------------
-// The production sweep for nz % 16 == 0.  A CTA of 8 warps owns 8 rows x 128 k
-// of bi planes; one thread streams each plane's tiles -- T (rows j0-1 .. j0+8,
-// k0-4 .. k0+131), class bytes (same rows, k0-16 .. k0+143) and T_old (the 8
-// output rows) -- into a ring of NST shared-memory stages, NST-1 planes ahead
-// of the plane being computed, so the bytes in flight do not depend on how
-// many warps are waiting.  Everything outside the grid arrives as TMA zero
-// fill: class 0 (air), whose value T_amb meets a gamma of 0 in every class
-// that borders the domain edge.  No global load is left in the plane loop.
-// Waits are bounded: a wait that gives up sets *err and the results of the
-// launch are not valid.
+// The production sweep for nz % 16 == 0.  A CTA of 8 compute warps owns 8 rows
+// x 128 k of bi planes, one row per warp; a producer warp streams each plane's
+// tiles -- T
+// (rows j0-1 .. j0+8, k0-4 .. k0+131), class bytes (same rows, k0-16 ..
+// k0+143) and T_old (the 8 output rows) -- into a ring of NST shared-memory
+// stages, NST-1 planes ahead of the plane being computed, so the bytes in
+// flight do not depend on how many warps are waiting.  Everything outside the
+// grid arrives as TMA zero fill: class 0 and value 0, which meet gamma 0 in
+// every class bordering the domain edge.  No global load is left in the plane
+// loop.  Waits are bounded: a wait that gives up sets the error flag and the
+// launch's results are not valid.
 namespace tmac {
 constexpr int ROWS = 8, TR = ROWS + 2;
 constexpr int TP = 4, TW = 128 + 2 * TP;   // T tile row: 136 floats
@@ -517,6 +537,7 @@ constexpr int OFF_C = al128(TB), OFF_O = OFF_C + al128(CB), STAGE = OFF_O + OB;
 constexpr int OFF_TAB = STAGE * NST, OFF_GT = OFF_TAB + 2 * NCLS * 16;
 constexpr int OFF_BAR = OFF_GT + MAXM * MAXM * 4, TOTAL = OFF_BAR + NST * 8;
 constexpr int THREADS = ROWS * 32;
+constexpr int MAX_BI = 64;  // plane chunk cap of the TMA sweep
 }  // namespace tmac
 
 struct CondMaps {
@@ -532,121 +553,158 @@ __device__ __forceinline__ uint32_t lds32(const uint8_t *p) {
   return *reinterpret_cast<const uint32_t *>(p);
 }
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Warps 0..7 compute one row each; warp 8 is the producer.  Stage q has a
+// "full" barrier (the TMA bytes of its plane have landed) and an "empty"
+// barrier (all 8 compute warps are done with its plane); the producer refills
+// a stage once it is empty, so a compute warp runs up to NST-2 planes ahead of
+// the slowest one instead of meeting it at a CTA barrier every plane.
 template <bool SNAP>
-__global__ void __launch_bounds__(tmac::THREADS, 4) be_cls_tma_kernel(
+__global__ void __launch_bounds__(tmac::THREADS + 32, 4) be_cls_tma_kernel(
     float *__restrict__ dst, float *__restrict__ snap, const __grid_constant__ CondMaps maps,
-    const uint32_t *__restrict__ patterns, int ncls, int nx, int ny, int nz, int bi, Params P) {
+    const uint32_t *__restrict__ patterns, int ncls, const uint8_t *__restrict__ tiles, int nx,
+    int ny, int nz, int bi, Params P) {
   using namespace tmac;
   extern __shared__ __align__(128) unsigned char dsm[];
+  __shared__ uint8_t s_own[MAX_BI + 4];  // tile occupancy of planes pbase-1 .. i1+1
+  __shared__ uint64_t s_empty[NST];
   float4 *tab = reinterpret_cast<float4 *>(dsm + OFF_TAB);
   float *gt = reinterpret_cast<float *>(dsm + OFF_GT);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(dsm + OFF_BAR);
+  uint64_t *full = reinterpret_cast<uint64_t *>(dsm + OFF_BAR);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const bool producer = threadIdx.x == 0;
   const int j0 = blockIdx.y * ROWS, k0 = blockIdx.x * 128;
   const int i0 = blockIdx.z * bi, i1 = min(i0 + bi, nx);
   const int pbase = i0 - 1;
-  if (producer) {
-    for (int q = 0; q < NST; ++q) mbar_init(&bars[q], 1);
+  if (threadIdx.x == THREADS) {
+    for (int q = 0; q < NST; ++q) {
+      mbar_init(&full[q], 1);
+      mbar_init(&s_empty[q], ROWS);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  build_class_table(tab, gt, patterns, ncls, P);  // ends with a barrier
-  auto issue = [&](int p) {
-    const int q = (p - pbase) % NST;
-    unsigned char *base = dsm + q * STAGE;
-    const bool own = !SNAP && p >= i0 && p < i1;  // T_old only for the computed planes
-    mbar_expect_tx(&bars[q], (uint32_t)(TB + CB + (own ? OB : 0)));
-    tma_load3(base, &maps.t, k0 - TP, j0 - 1, p, &bars[q]);
-    tma_load3(base + OFF_C, &maps.c, k0 - CP, j0 - 1, p, &bars[q]);
-    if (own) tma_load3(base + OFF_O, &maps.o, k0, j0, p, &bars[q]);
-  };
+  for (int t = threadIdx.x; t < i1 - pbase + 3; t += blockDim.x) {
+    const int p = pbase - 1 + t;
+    s_own[t] = p < 0 || p >= nx
+                   ? 0
+                   : (tiles ? tiles[((int64_t)p * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x]
+                            : 1);
+  }
+  build_class_table(tab, gt, patterns, ncls, P);  // ends with a barrier (all 9 warps)
   bool ok = true;
+
+  if (warp == ROWS) {  // ---- producer warp ----
+    if (lane == 0) {
+      // Plane p's tiles into its stage.  Without a snapshot to take, T is
+      // loaded only when plane p-1, p or p+1 of the tile holds a non-air cell
+      // (nothing else reads it) and T_old only for computed planes that hold one.
+      for (int p = pbase; p <= i1; ++p) {
+        const uint32_t n = (uint32_t)(p - pbase), q = n & (NST - 1);
+        if (n >= NST && !mbar_wait(&s_empty[q], ((n - NST) / NST) & 1u)) {
+          ok = false;
+          break;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        unsigned char *base = dsm + q * STAGE;
+        const int f = p - pbase + 1;
+        const bool need_t = SNAP || s_own[f - 1] || s_own[f] || s_own[f + 1];
+        const bool need_o = !SNAP && p >= i0 && p < i1 && s_own[f];
+        mbar_expect_tx(&full[q], (uint32_t)(CB + (need_t ? TB : 0) + (need_o ? OB : 0)));
+        if (need_t) tma_load3(base, &maps.t, k0 - TP, j0 - 1, p, &full[q]);
+        tma_load3(base + OFF_C, &maps.c, k0 - CP, j0 - 1, p, &full[q]);
+        if (need_o) tma_load3(base + OFF_O, &maps.o, k0, j0, p, &full[q]);
+      }
+      // no copy may still be in flight when the CTA's shared memory goes away
+      for (int p = max(pbase, i1 - NST + 1); p <= i1; ++p) {
+        const uint32_t n = (uint32_t)(p - pbase);
+        if (!mbar_wait(&full[n & (NST - 1)], (n / NST) & 1u)) ok = false;
+      }
+      if (!ok) atomicExch(&g_cond_err, 1);
+    }
+    return;
+  }
+
+  // ---- compute warps ----
   auto wait = [&](int p) {
-    const int n = p - pbase;
-    if (!mbar_wait(&bars[n % NST], (uint32_t)((n / NST) & 1))) ok = false;
+    const uint32_t n = (uint32_t)(p - pbase);
+    if (!mbar_wait(&full[n & (NST - 1)], (n / NST) & 1u)) ok = false;
   };
-  auto tst = [&](int p) {
-    return reinterpret_cast<const float *>(dsm + ((p - pbase) % NST) * STAGE);
+  auto release = [&](uint32_t q) {  // this warp is done with stage q
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&s_empty[q]);
   };
-  auto cst = [&](int p) { return dsm + ((p - pbase) % NST) * STAGE + OFF_C; };
-  auto ost = [&](int p) {
-    return reinterpret_cast<const float *>(dsm + ((p - pbase) % NST) * STAGE + OFF_O);
-  };
-  if (producer)
-    for (int p = pbase; p <= min(pbase + NST - 1, i1); ++p) issue(p);
-  const int rr = warp + 1;  // tile row of this warp's output row
   const int j = j0 + warp;
   const int k = k0 + lane * 4;
   const bool act = j < ny && k < nz;
   const float tamb = P.tamb;
   const int64_t plane = (int64_t)ny * nz;
-  const int tro = rr * TW + TP + lane * 4, cro = rr * CW + CP + lane * 4;
+  // offsets of this lane's four cells in a stage (tile row warp + 1)
+  const int tro = (warp + 1) * TW + TP + lane * 4, cro = OFF_C + (warp + 1) * CW + CP + lane * 4;
+  const int oro = OFF_O + (warp * 128 + lane * 4) * 4;
   wait(pbase);
-  float4 pm = amb04(lds4(tst(pbase) + tro), lds32(cst(pbase) + cro), tamb);
+  float4 pm = amb04(lds4(reinterpret_cast<const float *>(dsm) + tro), lds32(dsm + cro), tamb);
+  release(0);
   wait(i0);
-  uint32_t wc = lds32(cst(i0) + cro);
-  float4 pcr = lds4(tst(i0) + tro);
+  const unsigned char *b1 = dsm + STAGE;  // plane i0 is in stage 1
+  uint32_t wc = lds32(b1 + cro);
+  float4 pcr = lds4(reinterpret_cast<const float *>(b1) + tro);
   float4 pc = amb04(pcr, wc, tamb);
-  __syncthreads();  // stage pbase is free
-  if (producer && pbase + NST <= i1) {
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    issue(pbase + NST);
-  }
+  uint32_t sc = 1;  // stage of plane i
   int64_t o = (int64_t)i0 * plane + (int64_t)j * nz + k;
   for (int i = i0; i < i1; ++i, o += plane) {
+    const uint32_t sn = (sc + 1) & (NST - 1);
     wait(i + 1);
-    const uint32_t wn = lds32(cst(i + 1) + cro);
-    const float4 pnr = lds4(tst(i + 1) + tro);
+    const unsigned char *bn = dsm + sn * STAGE;
+    const uint32_t wn = lds32(bn + cro);
+    const float4 pnr = lds4(reinterpret_cast<const float *>(bn) + tro);
     const float4 pn = amb04(pnr, wn, tamb);
-    const float *tc = tst(i);
-    const uint8_t *cc = cst(i);
-    const float4 pjm = amb04(lds4(tc + tro - TW), lds32(cc + cro - CW), tamb);
-    const float4 pjp = amb04(lds4(tc + tro + TW), lds32(cc + cro + CW), tamb);
-    float pkm = __shfl_up_sync(0xffffffffu, pc.w, 1);
-    float pkp = __shfl_down_sync(0xffffffffu, pc.x, 1);
-    if (lane == 0) pkm = cc[cro - 1] ? tc[tro - 1] : tamb;
-    if (lane == 31) pkp = cc[cro + 4] ? tc[tro + 4] : tamb;
     if (SNAP && act) st4(snap + o, pcr);
-    if (__any_sync(0xffffffffu, act && wc != 0u)) {
-      const float4 tov = SNAP ? pcr : lds4(ost(i) + warp * 128 + lane * 4);
-      const float4 pb = make_float4(pkm, pc.x, pc.y, pc.z);
-      const float4 pf = make_float4(pc.y, pc.z, pc.w, pkp);
+    const bool live = act && cls_some(wc);
+    if (__any_sync(0xffffffffu, live)) {
+      const unsigned char *bc = dsm + sc * STAGE;
+      const float *tc = reinterpret_cast<const float *>(bc);
+      const float4 pjm = amb04(lds4(tc + tro - TW), lds32(bc + cro - CW), tamb);
+      const float4 pjp = amb04(lds4(tc + tro + TW), lds32(bc + cro + CW), tamb);
+      float pkm = __shfl_up_sync(0xffffffffu, pc.w, 1);
+      float pkp = __shfl_down_sync(0xffffffffu, pc.x, 1);
+      if (lane == 0) pkm = amb1(tc[tro - 1], bc[cro - 1], tamb);
+      if (lane == 31) pkp = amb1(tc[tro + 4], bc[cro + 4], tamb);
+      const float4 tov = SNAP ? pcr : *reinterpret_cast<const float4 *>(bc + oro);
       float o4[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const uint32_t c = byte_of(wc, q);
-        const float4 A = tab[2 * c], B = tab[2 * c + 1];
-        float rhs = __fadd_rn(0.0f, __fmul_rn(A.y, f4(pm, q)));
-        rhs = __fadd_rn(rhs, __fmul_rn(A.z, f4(pn, q)));
-        rhs = __fadd_rn(rhs, __fmul_rn(A.w, f4(pjm, q)));
-        rhs = __fadd_rn(rhs, __fmul_rn(B.x, f4(pjp, q)));
-        rhs = __fadd_rn(rhs, __fmul_rn(B.y, f4(pb, q)));
-        rhs = __fadd_rn(rhs, __fmul_rn(B.z, f4(pf, q)));
-        o4[q] = __fdiv_rn(__fadd_rn(f4(tov, q), rhs), A.x);
-      }
-      if (act && wc != 0u) {
-        if (!has_zero_byte(wc)) {
-          st4(dst + o, make_float4(o4[0], o4[1], o4[2], o4[3]));
-        } else {
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            if (byte_of(wc, q) != 0u) dst[o + q] = o4[q];
-        }
-      }
+      for (int q = 0; q < 4; ++q)
+        o4[q] = be_cell(tab, byte_of(wc, q), f4(pm, q), f4(pn, q), f4(pjm, q), f4(pjp, q),
+                        q == 0 ? pkm : f4(pc, q - 1), q == 3 ? pkp : f4(pc, q + 1), f4(tov, q));
+      if (live) store_word(dst + o, wc, o4);
     }
-    __syncthreads();  // stage i is free
-    if (producer && i + NST <= i1) {
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      issue(i + NST);
-    }
+    release(sc);  // plane i's stage
     pm = pc;
     pc = pn;
     pcr = pnr;
     wc = wn;
+    sc = sn;
   }
-  if (producer)  // no copy may still be in flight when the CTA's shared memory goes away
-    for (int p = max(pbase, i1 - NST + 1); p <= i1; ++p) wait(p);
+  // plane i1 (the last one read) is in stage sc: nothing refills it, no release needed
   if (!ok) atomicExch(&g_cond_err, 1);
+}
+
+// Tile occupancy for the TMA sweep: tiles[(i * TY + j / ROWS) * TX + k / 128]
+// = 1 when that plane's ROWS x 128 tile holds a non-air cell (TY, TX: tiles
+// per plane along j and k).
+__global__ void tile_flags_kernel(uint8_t *__restrict__ tiles, const uint8_t *__restrict__ cls,
+                                  int nx, int ny, int nz) {
+  const int ty = (ny + tmac::ROWS - 1) / tmac::ROWS, tx = (nz + 127) / 128;
+  const int64_t nw = (int64_t)nx * ny * (nz / 4);
+  for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < nw;
+       w += (int64_t)gridDim.x * blockDim.x) {
+    if (!cls_some(__ldg(reinterpret_cast<const uint32_t *>(cls) + w))) continue;
+    const int k = (int)(w % (nz / 4)) * 4;
+    const int64_t t = w / (nz / 4);
+    const int j = (int)(t % ny), i = (int)(t / ny);
+    tiles[((int64_t)i * ty + j / tmac::ROWS) * tx + k / 128] = 1;
+  }
 }
 
 // Class kernel for any shape or alignment: one thread per cell.
@@ -663,11 +721,11 @@ __global__ void __launch_bounds__(256) be_cls_generic_kernel(
        c += (int64_t)gridDim.x * blockDim.x) {
     if (SNAP) snap[c] = __ldg(src + c);
     const uint32_t cl = __ldg(cls + c);
-    if (cl == 0u) continue;
+    if (cl & CLS_AIR) continue;
     const int k = (int)(c % nz);
     const int64_t t = c / nz;
     const int j = (int)(t % ny), i = (int)(t / ny);
-#define NB(cond, off) ((cond) && __ldg(cls + c + (off)) ? __ldg(src + c + (off)) : P.tamb)
+#define NB(cond, off) ((cond) ? amb1(__ldg(src + c + (off)), __ldg(cls + c + (off)), P.tamb) : 0.0f)
     const float tv[6] = {NB(i > 0, -plane), NB(i + 1 < nx, plane), NB(j > 0, -(int64_t)nz),
                          NB(j + 1 < ny, (int64_t)nz), NB(k > 0, -1), NB(k + 1 < nz, 1)};
 #undef NB
@@ -820,17 +878,17 @@ int be_step(float *T, float *T_alt, float *T_old, const MatT *mat, int nx, int n
 bool g_cond_tma = true;  // TMA-fed class kernel when the layout allows it
 
 int tma_bi(int nx, int ny, int nz) {
-  if (g_cond_bi > 0) return g_cond_bi;
+  if (g_cond_bi > 0) return min(g_cond_bi, tmac::MAX_BI);
   const int64_t cols = (int64_t)((nz + 127) / 128) * ((ny + tmac::ROWS - 1) / tmac::ROWS);
   int bi = 32;
-  while (bi > 8 && cols * ((nx + bi - 1) / bi) < 8LL * num_sms()) bi >>= 1;
+  while (bi > 8 && cols * ((nx + bi - 1) / bi) < 8LL * num_sms()) bi >>= 1;  // 4 CTAs / SM
   return bi;
 }
 
 template <bool SNAP>
 bool launch_cls_tma(float *dst, const float *src, const float *told, float *snap,
-                    const uint8_t *cls, const uint32_t *patterns, int ncls, int nx, int ny, int nz,
-                    const Params &P, cudaStream_t s) {
+                    const uint8_t *cls, const uint32_t *patterns, int ncls, const uint8_t *tiles,
+                    int nx, int ny, int nz, const Params &P, cudaStream_t s) {
   using namespace tmac;
   if (!g_cond_tma || nz % 16 || !al16(dst) || (SNAP && !al16(snap))) return false;
   CondMaps maps;
@@ -848,16 +906,17 @@ bool launch_cls_tma(float *dst, const float *src, const float *told, float *snap
   if (a != cudaSuccess) return false;
   const int bi = tma_bi(nx, ny, nz);
   dim3 grid((nz + 127) / 128, (ny + ROWS - 1) / ROWS, (nx + bi - 1) / bi);
-  be_cls_tma_kernel<SNAP><<<grid, THREADS, TOTAL, s>>>(dst, snap, maps, patterns, ncls, nx, ny,
-                                                       nz, bi, P);
+  be_cls_tma_kernel<SNAP><<<grid, THREADS + 32, TOTAL, s>>>(dst, snap, maps, patterns, ncls,
+                                                            tiles, nx, ny, nz, bi, P);
   return true;
 }
 
 template <bool SNAP>
 cudaError_t launch_cls_sweep(float *dst, const float *src, const float *told, float *snap,
-                             const uint8_t *cls, const uint32_t *patterns, int ncls, int nx,
-                             int ny, int nz, const Params &P, cudaStream_t s) {
-  if (launch_cls_tma<SNAP>(dst, src, told, snap, cls, patterns, ncls, nx, ny, nz, P, s))
+                             const uint8_t *cls, const uint32_t *patterns, int ncls,
+                             const uint8_t *tiles, int nx, int ny, int nz, const Params &P,
+                             cudaStream_t s) {
+  if (launch_cls_tma<SNAP>(dst, src, told, snap, cls, patterns, ncls, tiles, nx, ny, nz, P, s))
     return cudaGetLastError();
   const bool col_ok = nz % 4 == 0 && al16(dst) && al16(src) &&
                       (SNAP ? al16(snap) : al16(told)) && (((uintptr_t)cls & 3u) == 0);
@@ -903,7 +962,7 @@ int prepare(uint8_t *cls, uint32_t *patterns, int *n_classes_host, const MatT *m
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return (int)e;
   *n_classes_host = host_count + 1;
-  if (host_count + 1 > NCLS) return BSP_ERR_CAPACITY;
+  if (host_count > CLS_MAX) return BSP_ERR_CAPACITY;
   cls_assign_kernel<MatT><<<blocks, 256, 0, s>>>(cls, patterns, bitmap, base, mat, nx, ny, nz,
                                                  (uint32_t)mat_air);
   return (int)cudaGetLastError();
@@ -913,7 +972,7 @@ int cls_args(const void *a, const void *b, const uint8_t *cls, const uint32_t *p
              int ncls, const float *k, const float *rho, const float *cp, int n_mat, int mat_air,
              float dx) {
   if (!a || !b || !cls || !patterns || !k || !rho || !cp) return BSP_ERR_NULL;
-  if (ncls < 1 || ncls > NCLS || n_mat < 1 || n_mat > MAXM - 1 || mat_air < 0 ||
+  if (ncls < 1 || ncls > CLS_MAX + 1 || n_mat < 1 || n_mat > MAXM - 1 || mat_air < 0 ||
       mat_air >= n_mat || !(dx > 0.0f))
     return BSP_ERR_ARG;
   return BSP_OK;
@@ -984,7 +1043,8 @@ extern "C" int bsp_conduction_prepare(uint8_t *cls, uint32_t *patterns, int *n_c
 
 extern "C" int bsp_conduction_sweep_cls(float *T_dst, const float *T_iter, const float *T_old,
                                         const uint8_t *cls, const uint32_t *patterns,
-                                        int n_classes, int nx, int ny, int nz, const float *k,
+                                        int n_classes, const uint8_t *tiles, int nx, int ny,
+                                        int nz, const float *k,
                                         const float *rho, const float *cp, int n_mat, float dx,
                                         float dt, float h_conv_air, float T_amb, int mat_air,
                                         cudaStream_t s) {
@@ -995,12 +1055,13 @@ extern "C" int bsp_conduction_sweep_cls(float *T_dst, const float *T_iter, const
   if (T_dst == T_iter) return BSP_ERR_ARG;
   const Params P{k, rho, cp, n_mat, dx, dt, h_conv_air, T_amb, mat_air};
   return (int)launch_cls_sweep<false>(T_dst, T_iter, T_old, nullptr, cls, patterns, n_classes,
-                                      nx, ny, nz, P, s);
+                                      tiles, nx, ny, nz, P, s);
 }
 
 extern "C" int bsp_conduction_be_cls(float *T, float *T_alt, float *T_old, const uint8_t *cls,
-                                     const uint32_t *patterns, int n_classes, int nx, int ny,
-                                     int nz, const float *k, const float *rho, const float *cp,
+                                     const uint32_t *patterns, int n_classes,
+                                     const uint8_t *tiles, int nx, int ny, int nz,
+                                     const float *k, const float *rho, const float *cp,
                                      int n_mat, float dx, float dt, float h_conv_air,
                                      float T_amb, int mat_air, int n_iter, cudaStream_t s) {
   if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_OK;
@@ -1011,13 +1072,13 @@ extern "C" int bsp_conduction_be_cls(float *T, float *T_alt, float *T_old, const
   const size_t bytes = sizeof(float) * (size_t)nx * ny * nz;
   const Params P{k, rho, cp, n_mat, dx, dt, h_conv_air, T_amb, mat_air};
   if (n_iter == 0) return (int)cudaMemcpyAsync(T_old, T, bytes, cudaMemcpyDeviceToDevice, s);
-  cudaError_t e = launch_cls_sweep<true>(T_alt, T, nullptr, T_old, cls, patterns, n_classes, nx,
-                                         ny, nz, P, s);
+  cudaError_t e = launch_cls_sweep<true>(T_alt, T, nullptr, T_old, cls, patterns, n_classes,
+                                         tiles, nx, ny, nz, P, s);
   for (int it = 1; it < n_iter && e == cudaSuccess; ++it) {
     const float *src = (it % 2 == 0) ? T : T_alt;
     float *dst = (it % 2 == 0) ? T_alt : T;
-    e = launch_cls_sweep<false>(dst, src, T_old, nullptr, cls, patterns, n_classes, nx, ny, nz,
-                                P, s);
+    e = launch_cls_sweep<false>(dst, src, T_old, nullptr, cls, patterns, n_classes, tiles, nx,
+                                ny, nz, P, s);
   }
   if (e == cudaSuccess && n_iter % 2 == 1)
     e = cudaMemcpyAsync(T, T_alt, bytes, cudaMemcpyDeviceToDevice, s);
@@ -1034,4 +1095,22 @@ extern "C" int bsp_conduction_error(int *flag_host) {
   }
   *flag_host = v;
   return (int)e;
+}
+
+extern "C" size_t bsp_conduction_tile_flags_bytes(int nx, int ny, int nz) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return 0;
+  return (size_t)nx * ((ny + tmac::ROWS - 1) / tmac::ROWS) * ((nz + 127) / 128);
+}
+
+extern "C" int bsp_conduction_tile_flags(uint8_t *tiles, const uint8_t *cls, int nx, int ny,
+                                         int nz, cudaStream_t s) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_OK;
+  if (!tiles || !cls) return BSP_ERR_NULL;
+  if (nz % 4 || ((uintptr_t)cls & 3u)) return BSP_ERR_SHAPE;
+  cudaError_t e = cudaMemsetAsync(tiles, 0, bsp_conduction_tile_flags_bytes(nx, ny, nz), s);
+  if (e != cudaSuccess) return (int)e;
+  const int64_t nw = (int64_t)nx * ny * (nz / 4);
+  int64_t b = (nw + 255) / 256, cap = (int64_t)bsp::num_sms() * 16;
+  tile_flags_kernel<<<(int)(b < cap ? b : cap), 256, 0, s>>>(tiles, cls, nx, ny, nz);
+  return (int)cudaGetLastError();
 }

@@ -395,31 +395,40 @@ int bsp_material_ids(uint8_t *mat_id, const int32_t *mat, int64_t n, int n_mat,
 /* Cell classes for the conduction sweep.  A non-air cell's update depends
  * only on its material and its six neighbours' (domain edge included), so the
  * distinct neighbourhoods of a geometry are numbered once: cls[c] = class of
- * cell c (0 = air), patterns[0 .. n_classes) = each class's neighbourhood key
- * (own id | code(-x) << 3 | code(+x) << 6 | ... | code(+z) << 18, code 7 = domain
- * edge).  Requires n_mat <= 7.  Synchronises the stream once (reads the class
- * count into *n_classes_host); returns BSP_ERR_CAPACITY when the geometry has
- * more than 255 classes (use the material-id entry points then).  patterns
- * holds 256 entries. */
+ * cell c (1 .. n_classes-1; 0x80 = air), patterns[1 .. n_classes) = each
+ * class's neighbourhood key (own id | code(-x) << 3 | code(+x) << 6 | ... |
+ * code(+z) << 18, code 7 = domain edge).  Requires n_mat <= 7.  Synchronises
+ * the stream once (reads the class count into *n_classes_host); returns
+ * BSP_ERR_CAPACITY when the geometry has more than 127 classes (use the
+ * material-id entry points then).  patterns holds 256 entries. */
 size_t bsp_conduction_prepare_workspace_bytes(void);
 int bsp_conduction_prepare(uint8_t *cls, uint32_t *patterns, int *n_classes_host,
                            const int32_t *mat, int nx, int ny, int nz, int n_mat, int mat_air,
                            void *workspace, size_t workspace_bytes, cudaStream_t stream);
+/* Tile occupancy of a class grid for the TMA-fed sweep: one byte per plane
+ * and 8-row x 128-cell tile (nx x ceil(ny/8) x ceil(nz/128)), 1 when the
+ * tile holds a non-air cell; the sweep then skips loads no update reads.
+ * Needs nz % 4 == 0. */
+size_t bsp_conduction_tile_flags_bytes(int nx, int ny, int nz);
+int bsp_conduction_tile_flags(uint8_t *tiles, const uint8_t *cls, int nx, int ny, int nz,
+                              cudaStream_t stream);
 /* The sweep and the step of bsp_conduction_sweep / bsp_conduction_be on cell
- * classes: the same results bit for bit, one class byte per cell. */
+ * classes: the same results bit for bit, one class byte per cell.  tiles
+ * (from bsp_conduction_tile_flags, or NULL) lets the TMA-fed sweep skip the
+ * temperature tiles of all-air regions. */
 int bsp_conduction_sweep_cls(float *T_dst, const float *T_iter, const float *T_old,
-                             const uint8_t *cls, const uint32_t *patterns, int n_classes, int nx,
-                             int ny, int nz, const float *k, const float *rho, const float *cp,
-                             int n_mat, float dx, float dt, float h_conv_air, float T_amb,
-                             int mat_air, cudaStream_t stream);
+                             const uint8_t *cls, const uint32_t *patterns, int n_classes,
+                             const uint8_t *tiles, int nx, int ny, int nz, const float *k,
+                             const float *rho, const float *cp, int n_mat, float dx, float dt,
+                             float h_conv_air, float T_amb, int mat_air, cudaStream_t stream);
 /* Read and clear the device flag that a TMA-fed conduction sweep sets when a
  * bounded wait gave up (its results are then not valid); synchronous. */
 int bsp_conduction_error(int *flag_host);
 int bsp_conduction_be_cls(float *T, float *T_alt, float *T_old, const uint8_t *cls,
-                          const uint32_t *patterns, int n_classes, int nx, int ny, int nz,
-                          const float *k, const float *rho, const float *cp, int n_mat, float dx,
-                          float dt, float h_conv_air, float T_amb, int mat_air, int n_iter,
-                          cudaStream_t stream);
+                          const uint32_t *patterns, int n_classes, const uint8_t *tiles, int nx,
+                          int ny, int nz, const float *k, const float *rho, const float *cp,
+                          int n_mat, float dx, float dt, float h_conv_air, float T_amb,
+                          int mat_air, int n_iter, cudaStream_t stream);
 
 /* ---- learned warm start: U-Net layers --------------------------------------
  * Building blocks of the pressure warm-start network (a 3-level 3-D U-Net
