@@ -36,6 +36,12 @@
  *   b_c     = -rho dx^2 div_c / dt            (pressure_solve_pcg.cu:129-139)
  * and solves it with diagonal-preconditioned CG to give the "FP64 oracle" p*.
  *
+ * The backward-Euler conduction part (or_conduction_*) is parity unpinned
+ * against reference outputs: the reference kernel exists only as Warp code,
+ * which cannot run here, and its tests hold no vectors for it.  It restates
+ * the kernel operation by operation and is checked against closed-form
+ * answers of the discrete system (tests/test_conduction_oracle.py).
+ *
  * OpenMP parallelises the element-wise loops; reductions use a fixed
  * per-block partial-sum layout so results do not depend on the thread count.
  */
