@@ -255,6 +255,69 @@ def conduction_bench(mat, dev, peak, peak_kind, cpu: bool):
     return out
 
 
+def advection_bench(mat, ux, uy, uz, dev, peak, peak_kind, cpu: bool):
+    """Semi-Lagrangian advect_all (fluid.py:737-776) on the 384x384x256 pot with
+    the workload's velocities, dt 0.01 s, origin (-nx dx/2, -ny dx/2, -4 dx):
+    event-timed over 5 calls after 2 untimed, with the reference's copy back
+    into the grid and without it (results left in the workspace).
+    Algorithmic bytes per call without the copy: read ux, uy, uz, T, mask,
+    T_ext (4+4+4+4+1+4 per cell); write the three velocity buffers, T_ext and
+    T_tmp (12+4+4) = 41 B/cell; the copy back adds 32 B/cell."""
+    import torch
+
+    from boilingsim_b200 import _lib
+    from boilingsim_b200 import fluid as F
+
+    nx, ny, nz = mat.shape
+    n = mat.size
+    rng = np.random.default_rng(SEED)
+    T0 = (330.0 + rng.standard_normal(mat.shape)).astype(np.float32)
+    org = (-nx * DX / 2, -ny * DX / 2, -4 * DX)
+    mask = F.cell_mask(torch.as_tensor(mat).to(dev))
+    fields = [torch.as_tensor(a).to(dev) for a in (ux, uy, uz, T0)]
+    tmp = [torch.empty_like(a) for a in fields]
+    ext = torch.empty_like(fields[3])
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def run(copy_back):
+        _lib.call("bsp_advect_all", *(_lib.ptr(a) for a in (*fields, *tmp, ext, mask)), nx, ny,
+                  nz, *org, DX, DT, copy_back, _lib.stream_handle())
+
+    out = {"workload": "pot 384x384x256 dx=0.5mm, workload velocities (plume 0.1 m/s), "
+                       "T 330 K + N(0,1), dt 0.01 s, advect_all"}
+    for cb, key in ((0, "no_copy"), (1, "with_copy_back")):
+        for _ in range(2):
+            run(cb)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(5):
+            run(cb)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 5
+        alg = (41.0 + 32.0 * cb) * n
+        g = alg / (ms * 1e-3) / 1e9
+        out[key] = {"ms": round(ms, 4), "algorithmic_bytes": int(alg), "GB/s": round(g, 1),
+                    "peak": peak, "peak_source": peak_kind, "frac": round(g / peak, 4)}
+    out["calls_per_s"] = round(1e3 / out["with_copy_back"]["ms"], 2)
+    out["gpu_launches_per_call"] = 5
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        threads = os.cpu_count() or 1
+        O.set_threads(threads)
+        t0 = time.perf_counter()
+        O.advect_all(ux, uy, uz, T0, mat, org, DX, DT)
+        t = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(1.0 / t, 4), "unit": "advect_all calls/s",
+                               "cores": threads, "kind": "port",
+                               "sample": f"one full-grid advect_all of the C restatement "
+                                         f"({t*1e3:.0f} ms)"}
+    return out
+
+
 def run_learned(args, dev, rank, world, dist):
     """Learned warm start at 192x192x128 (walls 2/3/4 cells, plume 0.02 / 0.1 /
     0.3 m/s): the trained U-Net's pressure starts the solve, which finishes to
@@ -396,6 +459,8 @@ def main():
                     help="run only the plain FP32 Jacobi sweep measurement (for ncu)")
     ap.add_argument("--only-conduction", action="store_true",
                     help="run only the backward-Euler conduction measurement (for ncu)")
+    ap.add_argument("--only-advection", action="store_true",
+                    help="run only the semi-Lagrangian advection measurement (for ncu)")
     ap.add_argument("--config", default="projection",
                     choices=["projection", "batched", "learned"],
                     help="projection: the headline 384x384x256 projection; batched: 64 uneven "
@@ -508,12 +573,15 @@ def main():
                                         "effective_frac": out[2]["frac"],
                                         "passes": out[2]["launches"]}}
 
-    if args.only_sweep or args.only_conduction:
+    if args.only_sweep or args.only_conduction or args.only_advection:
         if rank == 0 and args.only_sweep:
             print(json.dumps({"plain_fp32_jacobi_sweep": plain_sweep()}), flush=True)
         if rank == 0 and args.only_conduction:
             print(json.dumps({"conduction": conduction_bench(mat, dev, *_peaks(), cpu=False)}),
                   flush=True)
+        if rank == 0 and args.only_advection:
+            print(json.dumps({"advection": advection_bench(mat, ux, uy, uz, dev, *_peaks(),
+                                                           cpu=False)}), flush=True)
         if dist:
             dist.destroy_process_group()
         return
@@ -587,13 +655,15 @@ def main():
                   for c in per_launch if prof_n[c]}
     launches = int(sum(prof_n))  # every kernel launch of the timed steps is instrumented
 
-    sweep = e2e = cond = None
+    sweep = e2e = cond = adv = None
     ref_iters = args.ref_iters or REF_PCG_ITERS_FALLBACK
     cpu = None
     if not args.skip_extras:
         sweep = plain_sweep()
         cond = conduction_bench(mat, dev, peak, peak_kind,
                                 cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
+        adv = advection_bench(mat, ux, uy, uz, dev, peak, peak_kind,
+                              cpu=rank == 0 and world == 1 and not args.no_cpu_baseline)
 
         # ---- end to end through the public API with host buffers ----------------------
         host_u = [torch.as_tensor(a).pin_memory() for a in (ux, uy, uz)]
@@ -670,6 +740,7 @@ def main():
             "roofline": roofline,
             "plain_fp32_jacobi_sweep": sweep,
             "conduction": cond,
+            "advection": adv,
             "reference_pcg_iterations_to_tol": ref_iters,
             "cpu_baseline": cpu,
             "e2e": e2e,

@@ -57,6 +57,12 @@ SIGNATURES = {
     "bsp_step_projection_jacobi": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _I,
                                         _I, _P, _P]),
     "bsp_noslip_divergence": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _P]),
+    # semi-Lagrangian advection (advect.cu)
+    "bsp_extend_temperature": (_I, [_P, _P, _P, _I, _I, _I, _P]),
+    "bsp_advect_temperature": (_I, [_P, _P, _P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _F, _F,
+                                    _P]),
+    "bsp_advect_velocity": (_I, [_I, _P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _F, _F, _P]),
+    "bsp_advect_all": (_I, [_P] * 10 + [_I, _I, _I, _F, _F, _F, _F, _F, _I, _P]),
     # backward-Euler conduction (conduction.cu)
     "bsp_conduction_sweep": (_I, [_P, _P, _P, _P, _I, _I, _I, _P, _P, _P, _I, _F, _F, _F, _F, _I,
                                   _P]),

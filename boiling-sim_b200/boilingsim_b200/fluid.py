@@ -63,6 +63,8 @@ class Grid:
     uy: torch.Tensor
     uz: torch.Tensor
     mask: torch.Tensor | None = None  # uint8 cell classes, derived once from mat
+    T: torch.Tensor | None = None      # (nx, ny, nz) f32 cell temperature (advection)
+    origin: tuple = (0.0, 0.0, 0.0)    # world position of the grid corner (advection)
 
     @property
     def shape(self):
@@ -83,6 +85,12 @@ class FluidWorkspace:
     div_u: torch.Tensor
     p_tmp: torch.Tensor
     max_div: torch.Tensor  # (1,) device float: max|div| of the last projection
+    # semi-Lagrangian advection buffers (fluid.py:500-528); allocated on first use
+    ux_tmp: torch.Tensor | None = None
+    uy_tmp: torch.Tensor | None = None
+    uz_tmp: torch.Tensor | None = None
+    T_tmp: torch.Tensor | None = None
+    T_ext: torch.Tensor | None = None
 
 
 def allocate_fluid_workspace(grid: Grid, device: str = "cuda:0") -> FluidWorkspace:
@@ -90,6 +98,16 @@ def allocate_fluid_workspace(grid: Grid, device: str = "cuda:0") -> FluidWorkspa
     return FluidWorkspace(torch.zeros(shp, dtype=torch.float32, device=device),
                           torch.zeros(shp, dtype=torch.float32, device=device),
                           torch.zeros(1, dtype=torch.float32, device=device))
+
+
+def _advection_buffers(grid: Grid, ws: FluidWorkspace) -> None:
+    nx, ny, nz = grid.shape
+    dev = grid.mat.device
+    z = lambda *shp: torch.zeros(shp, dtype=torch.float32, device=dev)  # noqa: E731
+    if ws.ux_tmp is None:
+        ws.ux_tmp, ws.uy_tmp, ws.uz_tmp = z(nx + 1, ny, nz), z(nx, ny + 1, nz), z(nx, ny, nz + 1)
+    if ws.T_tmp is None:
+        ws.T_tmp, ws.T_ext = z(nx, ny, nz), z(nx, ny, nz)
 
 
 def cell_mask(mat: torch.Tensor, mat_fluid: int = MAT_FLUID, mat_air: int = MAT_AIR,
@@ -322,3 +340,46 @@ def projection_step(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, dt: flo
     out = pressure_projection(grid, ws, cfg, dt, rho, device)
     enforce_no_slip(grid, device)
     return out
+
+
+# ---------------------------------------------------------------------------
+# Semi-Lagrangian advection (fluid.py:338-498, 737-776)
+# ---------------------------------------------------------------------------
+
+def extend_temperature_into_solids(T_ext, T, mask, stream=None) -> None:
+    """fluid.py:338-382 on the uint8 cell mask (``cell_mask``)."""
+    nx, ny, nz = T.shape
+    call("bsp_extend_temperature", ptr(T_ext), ptr(T), ptr(mask), nx, ny, nz,
+         stream_handle(stream))
+
+
+def advect_temperature(T_new, T_true, T_ext, ux, uy, uz, mask, origin, dx, dt,
+                       stream=None) -> None:
+    """fluid.py:385-411."""
+    nx, ny, nz = T_true.shape
+    call("bsp_advect_temperature", ptr(T_new), ptr(T_true), ptr(T_ext), ptr(ux), ptr(uy),
+         ptr(uz), ptr(mask), nx, ny, nz, *(float(o) for o in origin), float(dx), float(dt),
+         stream_handle(stream))
+
+
+def advect_velocity(axis: int, u_new, ux, uy, uz, mask, origin, dx, dt, stream=None) -> None:
+    """advect_ux / advect_uy / advect_uz (fluid.py:414-498) for axis 0 / 1 / 2."""
+    nx, ny, nz = mask.shape
+    call("bsp_advect_velocity", int(axis), ptr(u_new), ptr(ux), ptr(uy), ptr(uz), ptr(mask),
+         nx, ny, nz, *(float(o) for o in origin), float(dx), float(dt), stream_handle(stream))
+
+
+def advect_all(grid: Grid, ws: FluidWorkspace, dt: float, device: str = "cuda:0",
+               stream=None) -> None:
+    """``advect_all`` (fluid.py:737-776): semi-Lagrangian advection of ux, uy,
+    uz and T from the old fields into the workspace, then copied back into
+    the grid -- bit-identical to the reference arithmetic."""
+    del device
+    if grid.T is None:
+        raise ValueError("advect_all needs grid.T")
+    _advection_buffers(grid, ws)
+    nx, ny, nz = grid.shape
+    call("bsp_advect_all", ptr(grid.ux), ptr(grid.uy), ptr(grid.uz), ptr(grid.T),
+         ptr(ws.ux_tmp), ptr(ws.uy_tmp), ptr(ws.uz_tmp), ptr(ws.T_tmp), ptr(ws.T_ext),
+         ptr(grid_mask(grid)), nx, ny, nz, *(float(o) for o in grid.origin), float(grid.dx),
+         float(dt), 1, stream_handle(stream))

@@ -355,6 +355,37 @@ int bsp_autotune_solve(float *p, const float *div_u, const uint8_t *mask, int nx
                        void *workspace, size_t workspace_bytes, BspTuneChoice *out, int max_out,
                        int *n_out, cudaStream_t stream);
 
+/* ---- semi-Lagrangian advection --------------------------------------------------
+ * python/boilingsim/fluid.py:39-104, 338-498, 737-776 on the uint8 cell mask
+ * (bsp_mask_from_mat).  Bit-identical to the reference expressions evaluated
+ * one rounding per operation.  (ox, oy, oz) is the grid origin (world
+ * position of cell (0,0,0)'s corner), dx the cell size. */
+
+/* extend_temperature_into_solids: T_ext = T on fluid cells; elsewhere the T
+ * of the first fluid face neighbour in the order -x, +x, -y, +y, -z, +z, else
+ * the cell's own T. */
+int bsp_extend_temperature(float *T_ext, const float *T, const uint8_t *mask, int nx, int ny,
+                           int nz, cudaStream_t stream);
+/* advect_temperature: fluid cells sample T_ext (trilinear) at the point
+ * backtraced by the velocity at the cell centre; other cells copy T_true. */
+int bsp_advect_temperature(float *T_new, const float *T_true, const float *T_ext,
+                           const float *ux, const float *uy, const float *uz, const uint8_t *mask,
+                           int nx, int ny, int nz, float ox, float oy, float oz, float dx,
+                           float dt, cudaStream_t stream);
+/* advect_ux / advect_uy / advect_uz (axis 0 / 1 / 2) into u_new: boundary
+ * faces 0, faces between two non-fluid cells keep their value, others sample
+ * their component at the backtraced face centre. */
+int bsp_advect_velocity(int axis, float *u_new, const float *ux, const float *uy,
+                        const float *uz, const uint8_t *mask, int nx, int ny, int nz, float ox,
+                        float oy, float oz, float dx, float dt, cudaStream_t stream);
+/* advect_all: the three velocity components and T from the old fields into
+ * the tmp arrays (T via T_ext); copy_back != 0 then copies them into ux, uy,
+ * uz, T as the reference does (0 leaves the results in the tmp arrays). */
+int bsp_advect_all(float *ux, float *uy, float *uz, float *T, float *ux_tmp, float *uy_tmp,
+                   float *uz_tmp, float *T_tmp, float *T_ext, const uint8_t *mask, int nx,
+                   int ny, int nz, float ox, float oy, float oz, float dx, float dt,
+                   int copy_back, cudaStream_t stream);
+
 /* ---- backward-Euler conduction -------------------------------------------------
  * The implicit conduction step of python/boilingsim/thermal.py.  mat holds
  * material ids in [0, n_mat) (n_mat <= 8), indexing the device arrays k, rho,

@@ -76,6 +76,12 @@ def lib() -> ctypes.CDLL:
                                                _f32p, _f32p, _F, _F, _F, _F, _I]),
             "or_conduction_be_f32": (None, [_f32p, _f32p, _f32p, _i32p, _I, _I, _I, _f32p,
                                             _f32p, _f32p, _F, _F, _F, _F, _I, _I]),
+            "or_extend_temperature_f32": (None, [_f32p, _f32p, _i32p, _I, _I, _I, _I]),
+            "or_advect_temperature_f32": (None, [_f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
+                                                 _i32p, _I, _I, _I, _f32p, _F, _F, _I]),
+            "or_advect_velocity_f32": (None, [_I, _f32p, _f32p, _f32p, _f32p, _i32p, _I, _I, _I,
+                                              _f32p, _F, _F, _I]),
+            "or_advect_all_f32": (None, [_f32p] * 9 + [_i32p, _I, _I, _I, _f32p, _F, _F, _I]),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -319,6 +325,55 @@ def conduction_be(T, T_alt, mat, props, dx, dt, h_conv_air, T_amb, n_iter, mat_a
                                float(dx), float(dt), float(h_conv_air), float(T_amb),
                                int(mat_air), int(n_iter))
     return T, T_alt, T_old
+
+
+# ---------------------------------------------------------------------------
+# Semi-Lagrangian advection (fluid.py:39-104, 338-498, 737-776)
+# ---------------------------------------------------------------------------
+
+def _org(origin):
+    return np.ascontiguousarray(origin, dtype=np.float32).reshape(3)
+
+
+def extend_temperature(T, mat, mat_fluid=MAT_FLUID):
+    T = _c(T, np.float32)
+    out = np.empty_like(T)
+    nx, ny, nz = T.shape
+    lib().or_extend_temperature_f32(out, T, _c(mat, np.int32), nx, ny, nz, int(mat_fluid))
+    return out
+
+
+def advect_temperature(T_true, T_ext, ux, uy, uz, mat, origin, dx, dt, mat_fluid=MAT_FLUID):
+    T_true = _c(T_true, np.float32)
+    out = np.empty_like(T_true)
+    nx, ny, nz = T_true.shape
+    lib().or_advect_temperature_f32(out, T_true, _c(T_ext, np.float32), _c(ux, np.float32),
+                                    _c(uy, np.float32), _c(uz, np.float32), _c(mat, np.int32),
+                                    nx, ny, nz, _org(origin), float(dx), float(dt),
+                                    int(mat_fluid))
+    return out
+
+
+def advect_velocity(axis, ux, uy, uz, mat, origin, dx, dt, mat_fluid=MAT_FLUID):
+    """advect_ux / advect_uy / advect_uz: returns the new component ``axis``."""
+    nx, ny, nz = mat.shape
+    src = (ux, uy, uz)[axis]
+    out = np.empty(src.shape, np.float32)
+    lib().or_advect_velocity_f32(int(axis), out, _c(ux, np.float32), _c(uy, np.float32),
+                                 _c(uz, np.float32), _c(mat, np.int32), nx, ny, nz, _org(origin),
+                                 float(dx), float(dt), int(mat_fluid))
+    return out
+
+
+def advect_all(ux, uy, uz, T, mat, origin, dx, dt, mat_fluid=MAT_FLUID):
+    """advect_all: returns (ux, uy, uz, T, T_ext) after the step."""
+    ux, uy, uz, T = (_c(a, np.float32).copy() for a in (ux, uy, uz, T))
+    tmp = [np.empty_like(a) for a in (ux, uy, uz, T)]
+    T_ext = np.empty_like(T)
+    nx, ny, nz = T.shape
+    lib().or_advect_all_f32(ux, uy, uz, T, *tmp, T_ext, _c(mat, np.int32), nx, ny, nz,
+                            _org(origin), float(dx), float(dt), int(mat_fluid))
+    return ux, uy, uz, T, T_ext
 
 
 def ref_library_path(fma: bool = True) -> str:

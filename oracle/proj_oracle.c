@@ -24,6 +24,10 @@
  *   pressure_solve_pcg_launch   crates/cuda-kernels/src/pressure_solve_pcg.cu:89-243
  *   apply_implicit_conduction_update  python/boilingsim/thermal.py:259-388
  *   conduct_one_step (backward-Euler branch)  python/boilingsim/thermal.py:647-658
+ *   _tri_sample, _sample_velocity_at  python/boilingsim/fluid.py:39-104
+ *   extend_temperature_into_solids, advect_temperature, advect_u{x,y,z}
+ *                               python/boilingsim/fluid.py:338-498
+ *   advect_all                  python/boilingsim/fluid.py:737-776
  *
  * Bit-faithfulness rules (FP32 part): every value is a C float, dx/dt/rho are
  * float before any arithmetic (Warp `float` is f32), operations are evaluated
@@ -41,6 +45,12 @@
  * which cannot run here, and its tests hold no vectors for it.  It restates
  * the kernel operation by operation and is checked against closed-form
  * answers of the discrete system (tests/test_conduction_oracle.py).
+ * The advection part (or_*advect*, or_extend_temperature_f32) is likewise
+ * parity unpinned against reference outputs (Warp code; the reference's
+ * advection test checks a drift bound, restated in tests/test_advect_oracle.py).
+ * Both follow the expressions as written, one rounding per operation, as
+ * Warp's CPU build evaluates them; a GPU build that contracts multiply-adds
+ * (rhs + g*T, the trilinear blends) can differ in the last bit.
  *
  * OpenMP parallelises the element-wise loops; reductions use a fixed
  * per-block partial-sum layout so results do not depend on the thread count.
@@ -643,4 +653,152 @@ void or_conduction_be_f32(float *T, float *T_alt, float *T_old, const int32_t *m
                                 h_conv_air, T_amb, mat_air);
     }
     if (n_iter % 2 == 1) memcpy(T, T_alt, bytes);
+}
+
+/* ------------------------------------------------------------------ */
+/* Semi-Lagrangian advection (FP32 restatement)                        */
+/* ------------------------------------------------------------------ */
+
+/* _tri_sample (fluid.py:39-88): trilinear sample of a field of shape
+ * (fx_n, fy_n, fz_n) living on the lattice offset (ox, oy, oz) at world point
+ * (px, py, pz).  Coordinates clamp to [0, n - 1 - 1e-6] in float (for n above
+ * ~17 the upper bound rounds to n - 1 exactly; the +1 corner index is then
+ * clamped to n - 1 here, where the reference would read past the array). */
+static float tri_sample(const float *f, int fx_n, int fy_n, int fz_n, float px, float py,
+                        float pz, const float *org, float dx, float ox, float oy, float oz) {
+    float fx = (px - org[0]) / dx - ox;
+    float fy = (py - org[1]) / dx - oy;
+    float fz = (pz - org[2]) / dx - oz;
+    const float hx = (float)(fx_n - 1) - 1.0e-6f, hy = (float)(fy_n - 1) - 1.0e-6f,
+                hz = (float)(fz_n - 1) - 1.0e-6f;
+    fx = fminf(fmaxf(fx, 0.0f), hx);
+    fy = fminf(fmaxf(fy, 0.0f), hy);
+    fz = fminf(fmaxf(fz, 0.0f), hz);
+    const int i0 = (int)fx, j0 = (int)fy, k0 = (int)fz;
+    const float tx = fx - (float)i0, ty = fy - (float)j0, tz = fz - (float)k0;
+    const int i1 = i0 + 1 < fx_n ? i0 + 1 : fx_n - 1;
+    const int j1 = j0 + 1 < fy_n ? j0 + 1 : fy_n - 1;
+    const int k1 = k0 + 1 < fz_n ? k0 + 1 : fz_n - 1;
+#define F(a, b, c) f[((int64_t)(a) * fy_n + (b)) * fz_n + (c)]
+    const float c000 = F(i0, j0, k0), c100 = F(i1, j0, k0), c010 = F(i0, j1, k0),
+                c110 = F(i1, j1, k0), c001 = F(i0, j0, k1), c101 = F(i1, j0, k1),
+                c011 = F(i0, j1, k1), c111 = F(i1, j1, k1);
+#undef F
+    const float c00 = c000 * (1.0f - tx) + c100 * tx;
+    const float c10 = c010 * (1.0f - tx) + c110 * tx;
+    const float c01 = c001 * (1.0f - tx) + c101 * tx;
+    const float c11 = c011 * (1.0f - tx) + c111 * tx;
+    const float c0 = c00 * (1.0f - ty) + c10 * ty;
+    const float c1 = c01 * (1.0f - ty) + c11 * ty;
+    return c0 * (1.0f - tz) + c1 * tz;
+}
+
+/* _sample_velocity_at (fluid.py:91-104) then the backtrace p - u dt. */
+static void backtrace(float *bx, float *by, float *bz, float px, float py, float pz,
+                      const float *ux, const float *uy, const float *uz, int nx, int ny, int nz,
+                      const float *org, float dx, float dt) {
+    const float u = tri_sample(ux, nx + 1, ny, nz, px, py, pz, org, dx, 0.0f, 0.5f, 0.5f);
+    const float v = tri_sample(uy, nx, ny + 1, nz, px, py, pz, org, dx, 0.5f, 0.0f, 0.5f);
+    const float w = tri_sample(uz, nx, ny, nz + 1, px, py, pz, org, dx, 0.5f, 0.5f, 0.0f);
+    *bx = px - u * dt;
+    *by = py - v * dt;
+    *bz = pz - w * dt;
+}
+
+/* extend_temperature_into_solids (fluid.py:338-382). */
+void or_extend_temperature_f32(float *T_ext, const float *T, const int32_t *mat, int nx, int ny,
+                               int nz, int mat_fluid) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k) {
+                const int64_t c = IDX(i, j, k);
+                float v = T[c];
+                if (mat[c] != mat_fluid) {
+                    if (i > 0 && mat[IDX(i - 1, j, k)] == mat_fluid) v = T[IDX(i - 1, j, k)];
+                    else if (i < nx - 1 && mat[IDX(i + 1, j, k)] == mat_fluid) v = T[IDX(i + 1, j, k)];
+                    else if (j > 0 && mat[IDX(i, j - 1, k)] == mat_fluid) v = T[IDX(i, j - 1, k)];
+                    else if (j < ny - 1 && mat[IDX(i, j + 1, k)] == mat_fluid) v = T[IDX(i, j + 1, k)];
+                    else if (k > 0 && mat[IDX(i, j, k - 1)] == mat_fluid) v = T[IDX(i, j, k - 1)];
+                    else if (k < nz - 1 && mat[IDX(i, j, k + 1)] == mat_fluid) v = T[IDX(i, j, k + 1)];
+                }
+                T_ext[c] = v;
+            }
+}
+
+/* advect_temperature (fluid.py:385-411): p = origin + (idx + 0.5) dx per axis. */
+void or_advect_temperature_f32(float *T_new, const float *T_true, const float *T_ext,
+                               const float *ux, const float *uy, const float *uz,
+                               const int32_t *mat, int nx, int ny, int nz, const float *org,
+                               float dx, float dt, int mat_fluid) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < nx; ++i)
+        for (int j = 0; j < ny; ++j)
+            for (int k = 0; k < nz; ++k) {
+                const int64_t c = IDX(i, j, k);
+                if (mat[c] != mat_fluid) {
+                    T_new[c] = T_true[c];
+                    continue;
+                }
+                const float px = org[0] + ((float)i + 0.5f) * dx;
+                const float py = org[1] + ((float)j + 0.5f) * dx;
+                const float pz = org[2] + ((float)k + 0.5f) * dx;
+                float bx, by, bz;
+                backtrace(&bx, &by, &bz, px, py, pz, ux, uy, uz, nx, ny, nz, org, dx, dt);
+                T_new[c] = tri_sample(T_ext, nx, ny, nz, bx, by, bz, org, dx, 0.5f, 0.5f, 0.5f);
+            }
+}
+
+/* advect_ux / advect_uy / advect_uz (fluid.py:414-498), axis 0 / 1 / 2:
+ * boundary faces -> 0; faces whose two cells are both non-fluid keep their
+ * value; others sample their own component at the backtraced point. */
+void or_advect_velocity_f32(int axis, float *u_new, const float *ux, const float *uy,
+                            const float *uz, const int32_t *mat, int nx, int ny, int nz,
+                            const float *org, float dx, float dt, int mat_fluid) {
+    const int fx_n = nx + (axis == 0), fy_n = ny + (axis == 1), fz_n = nz + (axis == 2);
+    const float *u = axis == 0 ? ux : (axis == 1 ? uy : uz);
+    const float ox = axis == 0 ? 0.0f : 0.5f, oy = axis == 1 ? 0.0f : 0.5f,
+                oz = axis == 2 ? 0.0f : 0.5f;
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < fx_n; ++i)
+        for (int j = 0; j < fy_n; ++j)
+            for (int k = 0; k < fz_n; ++k) {
+                const int64_t f = ((int64_t)i * fy_n + j) * fz_n + k;
+                const int a = axis == 0 ? i : (axis == 1 ? j : k);
+                const int na = axis == 0 ? fx_n : (axis == 1 ? fy_n : fz_n);
+                if (a == 0 || a == na - 1) {
+                    u_new[f] = 0.0f;
+                    continue;
+                }
+                const int64_t c1 = IDX(i, j, k);
+                const int64_t c0 = axis == 0 ? IDX(i - 1, j, k)
+                                             : (axis == 1 ? IDX(i, j - 1, k) : IDX(i, j, k - 1));
+                if (mat[c0] != mat_fluid && mat[c1] != mat_fluid) {
+                    u_new[f] = u[f];
+                    continue;
+                }
+                const float px = org[0] + ((float)i + ox) * dx;
+                const float py = org[1] + ((float)j + oy) * dx;
+                const float pz = org[2] + ((float)k + oz) * dx;
+                float bx, by, bz;
+                backtrace(&bx, &by, &bz, px, py, pz, ux, uy, uz, nx, ny, nz, org, dx, dt);
+                u_new[f] = tri_sample(u, fx_n, fy_n, fz_n, bx, by, bz, org, dx, ox, oy, oz);
+            }
+}
+
+/* advect_all (fluid.py:737-776): velocities and T from the old fields into
+ * the tmp arrays, then copied back. */
+void or_advect_all_f32(float *ux, float *uy, float *uz, float *T, float *ux_tmp, float *uy_tmp,
+                       float *uz_tmp, float *T_tmp, float *T_ext, const int32_t *mat, int nx,
+                       int ny, int nz, const float *org, float dx, float dt, int mat_fluid) {
+    or_advect_velocity_f32(0, ux_tmp, ux, uy, uz, mat, nx, ny, nz, org, dx, dt, mat_fluid);
+    or_advect_velocity_f32(1, uy_tmp, ux, uy, uz, mat, nx, ny, nz, org, dx, dt, mat_fluid);
+    or_advect_velocity_f32(2, uz_tmp, ux, uy, uz, mat, nx, ny, nz, org, dx, dt, mat_fluid);
+    or_extend_temperature_f32(T_ext, T, mat, nx, ny, nz, mat_fluid);
+    or_advect_temperature_f32(T_tmp, T, T_ext, ux, uy, uz, mat, nx, ny, nz, org, dx, dt,
+                              mat_fluid);
+    memcpy(ux, ux_tmp, sizeof(float) * (size_t)(nx + 1) * ny * nz);
+    memcpy(uy, uy_tmp, sizeof(float) * (size_t)nx * (ny + 1) * nz);
+    memcpy(uz, uz_tmp, sizeof(float) * (size_t)nx * ny * (nz + 1));
+    memcpy(T, T_tmp, sizeof(float) * (size_t)nx * ny * nz);
 }
