@@ -14,10 +14,10 @@
 //   p_back = p - u * dt                             u from three trilinear samples at p
 //   f      = (p - origin) / dx - offset, clamped to [0, n - 1 - 1e-6] (float)
 //   value  = ((c000 (1-tx) + c100 tx) (1-ty) + (c010 (1-tx) + c110 tx) ty) (1-tz) + ...
-// (p - origin) / dx is the same for the three velocity samples at a point and
-// is computed once.  The clamp's upper bound rounds to n - 1 exactly for n
-// above ~17; the +1 corner is then clamped to n - 1 (the reference would read
-// one element past the array there).
+// (p - origin) / dx depends on the lattice index only and is computed once per
+// CTA for its plane, rows and columns.  The clamp's upper bound rounds to
+// n - 1 exactly for n above ~17; the +1 corner is then clamped to n - 1 (the
+// reference would read one element past the array there).
 //
 // One thread per output point, CTAs of 64 k x 4 j of one i plane: the eight
 // corners of each sample are read through the read-only cache, and a CTA's
@@ -39,6 +39,7 @@ constexpr int BK = 64, BJ = 4;
 
 // Trilinear sample of field f (shape fxn x fyn x fzn, lattice offset (sx, sy,
 // sz)) at the point whose scaled coordinates (p - origin) / dx are (gx, gy, gz).
+// Offsets are 32-bit (fields hold fewer than 2^31 elements).
 __device__ __forceinline__ float tri(const float *__restrict__ f, int fxn, int fyn, int fzn,
                                      float gx, float gy, float gz, float sx, float sy, float sz) {
   float fx = __fsub_rn(gx, sx), fy = __fsub_rn(gy, sy), fz = __fsub_rn(gz, sz);
@@ -48,14 +49,13 @@ __device__ __forceinline__ float tri(const float *__restrict__ f, int fxn, int f
   const int i0 = __float2int_rz(fx), j0 = __float2int_rz(fy), k0 = __float2int_rz(fz);
   const float tx = __fsub_rn(fx, (float)i0), ty = __fsub_rn(fy, (float)j0),
               tz = __fsub_rn(fz, (float)k0);
-  const int i1 = min(i0 + 1, fxn - 1), j1 = min(j0 + 1, fyn - 1), k1 = min(k0 + 1, fzn - 1);
-  const int64_t pl = (int64_t)fyn * fzn;
-  const int64_t a0 = i0 * pl, a1 = i1 * pl;
-  const int64_t b0 = (int64_t)j0 * fzn, b1 = (int64_t)j1 * fzn;
-  const float c000 = __ldg(f + a0 + b0 + k0), c100 = __ldg(f + a1 + b0 + k0);
-  const float c010 = __ldg(f + a0 + b1 + k0), c110 = __ldg(f + a1 + b1 + k0);
-  const float c001 = __ldg(f + a0 + b0 + k1), c101 = __ldg(f + a1 + b0 + k1);
-  const float c011 = __ldg(f + a0 + b1 + k1), c111 = __ldg(f + a1 + b1 + k1);
+  const int pl = fyn * fzn;
+  const int di = i0 + 1 < fxn ? pl : 0, dj = j0 + 1 < fyn ? fzn : 0, dk = k0 + 1 < fzn ? 1 : 0;
+  const float *q = f + (i0 * pl + j0 * fzn + k0);
+  const float c000 = __ldg(q), c001 = __ldg(q + dk);
+  const float c010 = __ldg(q + dj), c011 = __ldg(q + dj + dk);
+  const float c100 = __ldg(q + di), c101 = __ldg(q + di + dk);
+  const float c110 = __ldg(q + di + dj), c111 = __ldg(q + di + dj + dk);
   const float ux = __fsub_rn(1.0f, tx), uy = __fsub_rn(1.0f, ty), uz = __fsub_rn(1.0f, tz);
   const float c00 = __fadd_rn(__fmul_rn(c000, ux), __fmul_rn(c100, tx));
   const float c10 = __fadd_rn(__fmul_rn(c010, ux), __fmul_rn(c110, tx));
@@ -66,20 +66,43 @@ __device__ __forceinline__ float tri(const float *__restrict__ f, int fxn, int f
   return __fadd_rn(__fmul_rn(c0, uz), __fmul_rn(c1, tz));
 }
 
-// World point of lattice index (i, j, k) with offsets (sx, sy, sz); returns
-// its scaled coordinates and, through the velocity at it, the backtraced
-// point's scaled coordinates.
-__device__ __forceinline__ void backtrace(float &bx, float &by, float &bz, int i, int j, int k,
-                                          float sx, float sy, float sz,
+// World and scaled coordinates of a CTA's lattice points, computed once per
+// CTA: p = origin + (idx + s) dx and g = (p - origin) / dx per axis for its
+// plane i, its BJ rows and its BK columns (they depend on the index only).
+struct Coords {
+  float px, gx, py[BJ], gy[BJ], pz[BK], gz[BK];
+};
+
+__device__ __forceinline__ void coords(Coords &c, int i, float sx, float sy, float sz,
+                                       const Geo &g) {
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  if (ty == 0) {
+    const int k = blockIdx.x * BK + tx;
+    const float p = __fadd_rn(g.oz, __fmul_rn(__fadd_rn((float)k, sz), g.dx));
+    c.pz[tx] = p;
+    c.gz[tx] = __fdiv_rn(__fsub_rn(p, g.oz), g.dx);
+  } else if (ty == 1 && tx < BJ) {
+    const int j = blockIdx.y * BJ + tx;
+    const float p = __fadd_rn(g.oy, __fmul_rn(__fadd_rn((float)j, sy), g.dx));
+    c.py[tx] = p;
+    c.gy[tx] = __fdiv_rn(__fsub_rn(p, g.oy), g.dx);
+  } else if (ty == 2 && tx == 0) {
+    const float p = __fadd_rn(g.ox, __fmul_rn(__fadd_rn((float)i, sx), g.dx));
+    c.px = p;
+    c.gx = __fdiv_rn(__fsub_rn(p, g.ox), g.dx);
+  }
+  __syncthreads();
+}
+
+// The velocity at the point (three samples at its scaled coordinates) and the
+// backtraced point's scaled coordinates.
+__device__ __forceinline__ void backtrace(float &bx, float &by, float &bz, const Coords &c,
                                           const float *__restrict__ ux,
                                           const float *__restrict__ uy,
                                           const float *__restrict__ uz, const Geo &g) {
-  const float px = __fadd_rn(g.ox, __fmul_rn(__fadd_rn((float)i, sx), g.dx));
-  const float py = __fadd_rn(g.oy, __fmul_rn(__fadd_rn((float)j, sy), g.dx));
-  const float pz = __fadd_rn(g.oz, __fmul_rn(__fadd_rn((float)k, sz), g.dx));
-  const float gx = __fdiv_rn(__fsub_rn(px, g.ox), g.dx);
-  const float gy = __fdiv_rn(__fsub_rn(py, g.oy), g.dx);
-  const float gz = __fdiv_rn(__fsub_rn(pz, g.oz), g.dx);
+  const float px = c.px, gx = c.gx;
+  const float py = c.py[threadIdx.y], gy = c.gy[threadIdx.y];
+  const float pz = c.pz[threadIdx.x], gz = c.gz[threadIdx.x];
   const float u = tri(ux, g.nx + 1, g.ny, g.nz, gx, gy, gz, 0.0f, 0.5f, 0.5f);
   const float v = tri(uy, g.nx, g.ny + 1, g.nz, gx, gy, gz, 0.5f, 0.0f, 0.5f);
   const float w = tri(uz, g.nx, g.ny, g.nz + 1, gx, gy, gz, 0.5f, 0.5f, 0.0f);
@@ -119,8 +142,10 @@ __global__ void __launch_bounds__(BK *BJ) advect_T_kernel(
     float *__restrict__ T_new, const float *__restrict__ T_true, const float *__restrict__ T_ext,
     const float *__restrict__ ux, const float *__restrict__ uy, const float *__restrict__ uz,
     const uint8_t *__restrict__ m, Geo g) {
+  __shared__ Coords cs;
   const int k = blockIdx.x * BK + threadIdx.x, j = blockIdx.y * BJ + threadIdx.y,
             i = blockIdx.z;
+  coords(cs, i, 0.5f, 0.5f, 0.5f, g);
   if (k >= g.nz || j >= g.ny) return;
   const int64_t c = ((int64_t)i * g.ny + j) * g.nz + k;
   if (!fluid(m, c)) {
@@ -128,7 +153,7 @@ __global__ void __launch_bounds__(BK *BJ) advect_T_kernel(
     return;
   }
   float bx, by, bz;
-  backtrace(bx, by, bz, i, j, k, 0.5f, 0.5f, 0.5f, ux, uy, uz, g);
+  backtrace(bx, by, bz, cs, ux, uy, uz, g);
   T_new[c] = tri(T_ext, g.nx, g.ny, g.nz, bx, by, bz, 0.5f, 0.5f, 0.5f);
 }
 
@@ -138,9 +163,12 @@ __global__ void __launch_bounds__(BK *BJ) advect_u_kernel(float *__restrict__ u_
                                                           const float *__restrict__ uy,
                                                           const float *__restrict__ uz,
                                                           const uint8_t *__restrict__ m, Geo g) {
+  __shared__ Coords cs;
   const int fxn = g.nx + (AX == 0), fyn = g.ny + (AX == 1), fzn = g.nz + (AX == 2);
   const int k = blockIdx.x * BK + threadIdx.x, j = blockIdx.y * BJ + threadIdx.y,
             i = blockIdx.z;
+  const float sx = AX == 0 ? 0.0f : 0.5f, sy = AX == 1 ? 0.0f : 0.5f, sz = AX == 2 ? 0.0f : 0.5f;
+  coords(cs, i, sx, sy, sz, g);
   if (k >= fzn || j >= fyn) return;
   const int64_t f = ((int64_t)i * fyn + j) * fzn + k;
   const int a = AX == 0 ? i : (AX == 1 ? j : k);
@@ -157,9 +185,8 @@ __global__ void __launch_bounds__(BK *BJ) advect_u_kernel(float *__restrict__ u_
     u_new[f] = __ldg(u + f);
     return;
   }
-  const float sx = AX == 0 ? 0.0f : 0.5f, sy = AX == 1 ? 0.0f : 0.5f, sz = AX == 2 ? 0.0f : 0.5f;
   float bx, by, bz;
-  backtrace(bx, by, bz, i, j, k, sx, sy, sz, ux, uy, uz, g);
+  backtrace(bx, by, bz, cs, ux, uy, uz, g);
   u_new[f] = tri(u, fxn, fyn, fzn, bx, by, bz, sx, sy, sz);
 }
 
@@ -180,8 +207,10 @@ cudaError_t launch_velocity(int axis, float *u_new, const float *ux, const float
 }
 
 bool dims_ok(int nx, int ny, int nz) {
-  // grid.z = nx + 1 planes and grid.y = ceil((ny + 1) / BJ) rows must fit the launch limits
-  return nx + 1 <= 65535 && (ny + 1 + BJ - 1) / BJ <= 65535;
+  // grid.z = nx + 1 planes and grid.y = ceil((ny + 1) / BJ) rows must fit the launch limits;
+  // the samplers use 32-bit element offsets
+  return nx + 1 <= 65535 && (ny + 1 + BJ - 1) / BJ <= 65535 &&
+         (int64_t)(nx + 1) * (ny + 1) * (nz + 1) < (1LL << 31);
 }
 
 }  // namespace sl
