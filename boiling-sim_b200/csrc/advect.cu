@@ -128,12 +128,12 @@ __global__ void __launch_bounds__(BK *BJ) extend_kernel(float *__restrict__ T_ex
   const int64_t pl = (int64_t)ny * nz, c = i * pl + (int64_t)j * nz + k;
   int64_t s = c;
   if (!fluid(m, c)) {
-    if (i > 0 && fluid(m, c - pl)) s = c - pl;
-    else if (i < nx - 1 && fluid(m, c + pl)) s = c + pl;
-    else if (j > 0 && fluid(m, c - nz)) s = c - nz;
-    else if (j < ny - 1 && fluid(m, c + nz)) s = c + nz;
-    else if (k > 0 && fluid(m, c - 1)) s = c - 1;
-    else if (k < nz - 1 && fluid(m, c + 1)) s = c + 1;
+    // the six neighbour flags are loaded together, then the first fluid one
+    // in the order -x, +x, -y, +y, -z, +z is taken
+    const bool f0 = i > 0 && fluid(m, c - pl), f1 = i < nx - 1 && fluid(m, c + pl);
+    const bool f2 = j > 0 && fluid(m, c - nz), f3 = j < ny - 1 && fluid(m, c + nz);
+    const bool f4 = k > 0 && fluid(m, c - 1), f5 = k < nz - 1 && fluid(m, c + 1);
+    s = f0 ? c - pl : f1 ? c + pl : f2 ? c - nz : f3 ? c + nz : f4 ? c - 1 : f5 ? c + 1 : c;
   }
   T_ext[c] = __ldg(T + s);
 }
