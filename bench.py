@@ -38,6 +38,10 @@ WORKLOAD = ("pot 384x384x256 dx=0.5mm (R_in 168, wall 12, water line 213, carrot
 # iteration 8) on this workload; measured with this library's reference-
 # compatible pressure_solve_pcg_launch (same algorithm) when a GPU is present.
 REF_PCG_ITERS_FALLBACK = 1281
+# DRAM traffic per launch measured by ncu (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# dominant kernel class at 384x384x256: the fused CG update + restriction with FP16 storage
+# (286.2 + 119.6 MB; algorithmic 427.3 MB).
+CAPTURED_TRAFFIC = {("cg_update_restrict_fine", "fp16"): 405_800_000}
 
 
 def _peaks():
@@ -643,9 +647,14 @@ def main():
     avg_ms = prof_ms[dom] / prof_n[dom]
     bytes_launch = per_launch[dom]
     achieved = bytes_launch / (avg_ms * 1e-3) / 1e9
+    # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from one
+    # ncu capture of the kernel on this workload, for the configurations captured
+    traffic = CAPTURED_TRAFFIC.get((names[dom], args.storage)) if (nx, ny, nz) == (
+        384, 384, 256) else None
     roofline = {"bound": "hbm", "kernel": names[dom], "achieved": round(achieved, 1),
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                "traffic": None, "peak_source": peak_kind,
+                "traffic": traffic, "traffic_source": "ncu capture, one launch" if traffic
+                else None, "peak_source": peak_kind,
                 "algorithmic_bytes_per_launch": round(bytes_launch),
                 "cells_processed_per_launch": int(n if dom in (0, 6) else n_act),
                 "avg_launch_ms": round(avg_ms, 5),
