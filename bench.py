@@ -44,6 +44,24 @@ REF_PCG_ITERS_FALLBACK = 1281
 CAPTURED_TRAFFIC = {("cg_update_restrict_fine", "fp16"): 405_800_000}
 
 
+def max_over_ranks(ms: float, dist, device) -> float:
+    """The slowest replica's time; every rank takes part (the same collective
+    on every rank, in the same order).  Without a process group: ms itself."""
+    if dist is None:
+        return ms
+    import torch
+
+    t = torch.tensor([float(ms)], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(world: int, units_per_rank: float, ms: float) -> float:
+    """Whole-job units per second: `world` replicas each process
+    units_per_rank in ms (the max over ranks)."""
+    return world * units_per_rank * 1e3 / ms
+
+
 def _peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -415,14 +433,11 @@ def run_batched(args, dev, rank, world, dist):
     ev1.record()
     torch.cuda.synchronize()
     seq_ms = ev0.elapsed_time(ev1) / max(1, args.steps // 2)
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ms, dist, dev)
     if rank == 0:
         print(json.dumps({
             "metric": "instances/s, 64 uneven pot scenes to FP64 rel-residual 1e-6",
-            "value": round(world * 64e3 / ms, 2), "unit": "instances/s", "n_gpus": world,
+            "value": round(job_rate(world, 64, ms), 2), "unit": "instances/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
@@ -615,10 +630,8 @@ def main():
     torch.cuda.synchronize()
     _lib.call("bsp_profile_enable", 0)
     _lib.lib().bsp_profile_read(prof_ms, prof_n, ncls)
+    ms = max_over_ranks(ms, dist, dev)
     if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
         dist.barrier()
     res = last["res"]
 
@@ -728,7 +741,7 @@ def main():
             cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
     if rank == 0:
-        value = world * 1e3 / ms
+        value = job_rate(world, 1, ms)
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "projections/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
