@@ -1,4 +1,6 @@
-"""CPU oracle for the pressure-projection path (TEST INFRASTRUCTURE ONLY).
+"""CPU oracle for the pressure-projection path and the two steps widened
+around it, backward-Euler conduction and semi-Lagrangian advection (TEST
+INFRASTRUCTURE ONLY).
 
 Only tests/, ``__graft_entry__.smoke()`` and the cpu_baseline / reference arm
 of ``bench.py`` import this module.  It is the checker, never the product:
@@ -18,7 +20,12 @@ that takes and returns numpy arrays, plus:
 
 Parity pin: the FP32 restatement is checked bit-for-bit against outputs of
 the reference CUDA kernels (``tests/golden/*.npz``, generated on a B200 by
-``tests/golden/make_golden.py`` from ``oracle/_ref``).
+``tests/golden/make_golden.py`` from ``oracle/_ref``).  The conduction
+(``conduction_*``, ``thermal.py:259-388, 647-658``) and advection
+(``extend_temperature``, ``advect_*``, ``fluid.py:39-104, 338-498, 737-776``)
+restatements are parity unpinned against reference outputs (the reference
+runs them only as Warp code, which cannot run here); they are checked against
+closed-form answers and the reference's own drift test instead.
 """
 from __future__ import annotations
 
