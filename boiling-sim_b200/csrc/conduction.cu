@@ -299,19 +299,32 @@ __device__ __forceinline__ uint32_t cell_key(const MatT *mat, int64_t c, int i, 
   return own | cxm << 3 | cxp << 6 | cym << 9 | cyp << 12 | czm << 15 | czp << 18;
 }
 
+__device__ __forceinline__ int mraw(const uint8_t *m, int64_t c) { return __ldg(m + c); }
+__device__ __forceinline__ int mraw(const int32_t *m, int64_t c) { return __ldg(m + c); }
+
+// Marks the keys present; ids outside [0, n_mat) are counted into *bad and
+// marked nothing (the keys hold 3-bit codes).
 template <class MatT>
 __global__ void cls_mark_kernel(uint32_t *__restrict__ bitmap, const MatT *__restrict__ mat,
-                                int nx, int ny, int nz, uint32_t mair) {
+                                int nx, int ny, int nz, uint32_t mair, int n_mat,
+                                int *__restrict__ bad) {
   const int64_t n = (int64_t)nx * ny * nz, plane = (int64_t)ny * nz;
+  int local = 0;
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += (int64_t)gridDim.x * blockDim.x) {
-    if (mbyte(mat, c) == mair) continue;
+    const int raw = mraw(mat, c);
+    if (raw < 0 || raw >= n_mat) {
+      ++local;
+      continue;
+    }
+    if ((uint32_t)raw == mair) continue;
     const int k = (int)(c % nz);
     const int64_t t = c / nz;
     const uint32_t key = cell_key(mat, c, (int)(t / ny), (int)(t % ny), k, nx, ny, nz, plane);
     const uint32_t bit = 1u << (key & 31u);
     if (!(__ldg(bitmap + (key >> 5)) & bit)) atomicOr(bitmap + (key >> 5), bit);
   }
+  if (local) atomicAdd(bad, local);
 }
 
 // Exclusive prefix of the bitmap words' population counts; *count = total.
@@ -898,12 +911,18 @@ bool launch_cls_tma(float *dst, const float *src, const float *told, float *snap
   if (!SNAP && !make_map(&maps.o, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, told, nx, ny, nz, 128, ROWS))
     return false;
   if (SNAP) maps.o = maps.t;
-  static cudaError_t attr[2] = {cudaErrorNotReady, cudaErrorNotReady};
-  cudaError_t &a = attr[SNAP ? 1 : 0];
-  if (a == cudaErrorNotReady)
+  // the shared-memory opt-in is per device: 0 not yet set, 1 set, 2 refused
+  static int attr[2][64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  int dummy = 0;
+  int &a = dev < 64 ? attr[SNAP ? 1 : 0][dev] : dummy;
+  if (a == 0)
     a = cudaFuncSetAttribute(be_cls_tma_kernel<SNAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             TOTAL);
-  if (a != cudaSuccess) return false;
+                             TOTAL) == cudaSuccess
+            ? 1
+            : 2;
+  if (a != 1) return false;
   const int bi = tma_bi(nx, ny, nz);
   dim3 grid((nz + 127) / 128, (ny + ROWS - 1) / ROWS, (nx + bi - 1) / bi);
   be_cls_tma_kernel<SNAP><<<grid, THREADS + 32, TOTAL, s>>>(dst, snap, maps, patterns, ncls,
@@ -949,19 +968,26 @@ int prepare(uint8_t *cls, uint32_t *patterns, int *n_classes_host, const MatT *m
   if (ws_bytes < prepare_workspace_bytes() || ((uintptr_t)ws & 15u)) return BSP_ERR_WORKSPACE;
   uint32_t *bitmap = static_cast<uint32_t *>(ws);
   uint32_t *base = bitmap + NKEYWORDS;
-  int *count = reinterpret_cast<int *>(base + NKEYWORDS);
+  int *count = reinterpret_cast<int *>(base + NKEYWORDS);  // [0] classes, [1] bad ids
   const int64_t n = (int64_t)nx * ny * nz;
   int64_t b = (n + 255) / 256, cap = (int64_t)num_sms() * 16;
   const int blocks = (int)(b < cap ? b : cap);
   cudaError_t e = cudaMemsetAsync(bitmap, 0, sizeof(uint32_t) * NKEYWORDS, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(count, 0, 2 * sizeof(int), s);
   if (e != cudaSuccess) return (int)e;
-  cls_mark_kernel<MatT><<<blocks, 256, 0, s>>>(bitmap, mat, nx, ny, nz, (uint32_t)mat_air);
+  cls_mark_kernel<MatT><<<blocks, 256, 0, s>>>(bitmap, mat, nx, ny, nz, (uint32_t)mat_air,
+                                               n_mat, count + 1);
   cls_scan_kernel<<<1, SCAN_THREADS, 0, s>>>(base, bitmap, count);
-  int host_count = 0;
-  e = cudaMemcpyAsync(&host_count, count, sizeof(int), cudaMemcpyDeviceToHost, s);
+  int host[2] = {0, 0};
+  e = cudaMemcpyAsync(host, count, sizeof(host), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return (int)e;
+  const int host_count = host[0];
   *n_classes_host = host_count + 1;
+  if (host[1] > 0) {  // material ids outside [0, n_mat)
+    *n_classes_host = 0;
+    return BSP_ERR_ARG;
+  }
   if (host_count > CLS_MAX) return BSP_ERR_CAPACITY;
   cls_assign_kernel<MatT><<<blocks, 256, 0, s>>>(cls, patterns, bitmap, base, mat, nx, ny, nz,
                                                  (uint32_t)mat_air);

@@ -431,7 +431,8 @@ int bsp_material_ids(uint8_t *mat_id, const int32_t *mat, int64_t n, int n_mat,
  * code(+z) << 18, code 7 = domain edge).  Requires n_mat <= 7.  Synchronises
  * the stream once (reads the class count into *n_classes_host); returns
  * BSP_ERR_CAPACITY when the geometry has more than 127 classes (use the
- * material-id entry points then).  patterns holds 256 entries. */
+ * material-id entry points then) and BSP_ERR_ARG when mat holds an id
+ * outside [0, n_mat).  patterns holds 256 entries. */
 size_t bsp_conduction_prepare_workspace_bytes(void);
 int bsp_conduction_prepare(uint8_t *cls, uint32_t *patterns, int *n_classes_host,
                            const int32_t *mat, int nx, int ny, int nz, int n_mat, int mat_air,

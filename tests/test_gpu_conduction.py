@@ -266,3 +266,11 @@ def test_argument_checks(cuda):
     call("bsp_conduction_sweep", *base[:4], 0, 4, 4, *base[7:], 4, *tail)
     with pytest.raises(ValueError):
         TH.material_ids(torch.full((4, 4, 4), 5, dtype=torch.int32, device="cuda"))
+    # class preparation rejects ids outside [0, n_mat) instead of aliasing them
+    bad = torch.zeros((6, 5, 8), dtype=torch.int32, device="cuda")
+    bad[2, 2, 2] = 9
+    with pytest.raises(BspError):
+        TH.cell_classes(bad)
+    bad[2, 2, 2] = -1
+    with pytest.raises(BspError):
+        TH.cell_classes(bad)
