@@ -19,9 +19,10 @@
 // n - 1 exactly for n above ~17; the +1 corner is then clamped to n - 1 (the
 // reference would read one element past the array there).
 //
-// One thread per output point, CTAs of 64 k x 4 j of one i plane: the eight
-// corners of each sample are read through the read-only cache, and a CTA's
-// samples share most of their cache lines.
+// One thread per output point and plane, CTAs of 64 k x 4 j marching over 8
+// consecutive i planes: the eight corners of each sample are read through the
+// read-only cache, and a plane's samples reuse most of the lines fetched for
+// the plane before.
 #include <cuda_runtime.h>
 
 #include "../../include/bsproj.h"
@@ -35,7 +36,7 @@ struct Geo {
   float ox, oy, oz, dx, dt;
 };
 
-constexpr int BK = 64, BJ = 4;
+constexpr int BK = 64, BJ = 4, PL = 8;  // CTA: 64 k x 4 j, marching 8 planes
 
 // Trilinear sample of field f (shape fxn x fyn x fzn, lattice offset (sx, sy,
 // sz)) at the point whose scaled coordinates (p - origin) / dx are (gx, gy, gz).
@@ -70,11 +71,10 @@ __device__ __forceinline__ float tri(const float *__restrict__ f, int fxn, int f
 // CTA: p = origin + (idx + s) dx and g = (p - origin) / dx per axis for its
 // plane i, its BJ rows and its BK columns (they depend on the index only).
 struct Coords {
-  float px, gx, py[BJ], gy[BJ], pz[BK], gz[BK];
+  float px[PL], gx[PL], py[BJ], gy[BJ], pz[BK], gz[BK];
 };
 
-__device__ __forceinline__ void coords(Coords &c, int i, float sx, float sy, float sz,
-                                       const Geo &g) {
+__device__ __forceinline__ void coords(Coords &c, float sx, float sy, float sz, const Geo &g) {
   const int tx = threadIdx.x, ty = threadIdx.y;
   if (ty == 0) {
     const int k = blockIdx.x * BK + tx;
@@ -86,10 +86,11 @@ __device__ __forceinline__ void coords(Coords &c, int i, float sx, float sy, flo
     const float p = __fadd_rn(g.oy, __fmul_rn(__fadd_rn((float)j, sy), g.dx));
     c.py[tx] = p;
     c.gy[tx] = __fdiv_rn(__fsub_rn(p, g.oy), g.dx);
-  } else if (ty == 2 && tx == 0) {
+  } else if (ty == 2 && tx < PL) {
+    const int i = blockIdx.z * PL + tx;
     const float p = __fadd_rn(g.ox, __fmul_rn(__fadd_rn((float)i, sx), g.dx));
-    c.px = p;
-    c.gx = __fdiv_rn(__fsub_rn(p, g.ox), g.dx);
+    c.px[tx] = p;
+    c.gx[tx] = __fdiv_rn(__fsub_rn(p, g.ox), g.dx);
   }
   __syncthreads();
 }
@@ -97,10 +98,10 @@ __device__ __forceinline__ void coords(Coords &c, int i, float sx, float sy, flo
 // The velocity at the point (three samples at its scaled coordinates) and the
 // backtraced point's scaled coordinates.
 __device__ __forceinline__ void backtrace(float &bx, float &by, float &bz, const Coords &c,
-                                          const float *__restrict__ ux,
+                                          int ii, const float *__restrict__ ux,
                                           const float *__restrict__ uy,
                                           const float *__restrict__ uz, const Geo &g) {
-  const float px = c.px, gx = c.gx;
+  const float px = c.px[ii], gx = c.gx[ii];
   const float py = c.py[threadIdx.y], gy = c.gy[threadIdx.y];
   const float pz = c.pz[threadIdx.x], gz = c.gz[threadIdx.x];
   const float u = tri(ux, g.nx + 1, g.ny, g.nz, gx, gy, gz, 0.0f, 0.5f, 0.5f);
@@ -143,18 +144,21 @@ __global__ void __launch_bounds__(BK *BJ) advect_T_kernel(
     const float *__restrict__ ux, const float *__restrict__ uy, const float *__restrict__ uz,
     const uint8_t *__restrict__ m, Geo g) {
   __shared__ Coords cs;
-  const int k = blockIdx.x * BK + threadIdx.x, j = blockIdx.y * BJ + threadIdx.y,
-            i = blockIdx.z;
-  coords(cs, i, 0.5f, 0.5f, 0.5f, g);
+  const int k = blockIdx.x * BK + threadIdx.x, j = blockIdx.y * BJ + threadIdx.y;
+  coords(cs, 0.5f, 0.5f, 0.5f, g);
   if (k >= g.nz || j >= g.ny) return;
-  const int64_t c = ((int64_t)i * g.ny + j) * g.nz + k;
-  if (!fluid(m, c)) {
-    T_new[c] = __ldg(T_true + c);
-    return;
+  for (int ii = 0; ii < PL; ++ii) {
+    const int i = blockIdx.z * PL + ii;
+    if (i >= g.nx) break;
+    const int64_t c = ((int64_t)i * g.ny + j) * g.nz + k;
+    if (!fluid(m, c)) {
+      T_new[c] = __ldg(T_true + c);
+      continue;
+    }
+    float bx, by, bz;
+    backtrace(bx, by, bz, cs, ii, ux, uy, uz, g);
+    T_new[c] = tri(T_ext, g.nx, g.ny, g.nz, bx, by, bz, 0.5f, 0.5f, 0.5f);
   }
-  float bx, by, bz;
-  backtrace(bx, by, bz, cs, ux, uy, uz, g);
-  T_new[c] = tri(T_ext, g.nx, g.ny, g.nz, bx, by, bz, 0.5f, 0.5f, 0.5f);
 }
 
 template <int AX>
@@ -165,44 +169,52 @@ __global__ void __launch_bounds__(BK *BJ) advect_u_kernel(float *__restrict__ u_
                                                           const uint8_t *__restrict__ m, Geo g) {
   __shared__ Coords cs;
   const int fxn = g.nx + (AX == 0), fyn = g.ny + (AX == 1), fzn = g.nz + (AX == 2);
-  const int k = blockIdx.x * BK + threadIdx.x, j = blockIdx.y * BJ + threadIdx.y,
-            i = blockIdx.z;
+  const int k = blockIdx.x * BK + threadIdx.x, j = blockIdx.y * BJ + threadIdx.y;
   const float sx = AX == 0 ? 0.0f : 0.5f, sy = AX == 1 ? 0.0f : 0.5f, sz = AX == 2 ? 0.0f : 0.5f;
-  coords(cs, i, sx, sy, sz, g);
+  coords(cs, sx, sy, sz, g);
   if (k >= fzn || j >= fyn) return;
-  const int64_t f = ((int64_t)i * fyn + j) * fzn + k;
-  const int a = AX == 0 ? i : (AX == 1 ? j : k);
-  const int na = AX == 0 ? fxn : (AX == 1 ? fyn : fzn);
-  if (a == 0 || a == na - 1) {
-    u_new[f] = 0.0f;
-    return;
-  }
   const float *__restrict__ u = AX == 0 ? ux : (AX == 1 ? uy : uz);
   const int64_t pl = (int64_t)g.ny * g.nz;
-  const int64_t c1 = i * pl + (int64_t)j * g.nz + k;
-  const int64_t c0 = AX == 0 ? c1 - pl : (AX == 1 ? c1 - g.nz : c1 - 1);
-  if (!fluid(m, c0) && !fluid(m, c1)) {
-    u_new[f] = __ldg(u + f);
-    return;
+  for (int ii = 0; ii < PL; ++ii) {
+    const int i = blockIdx.z * PL + ii;
+    if (i >= fxn) break;
+    const int64_t f = ((int64_t)i * fyn + j) * fzn + k;
+    const int a = AX == 0 ? i : (AX == 1 ? j : k);
+    const int na = AX == 0 ? fxn : (AX == 1 ? fyn : fzn);
+    if (a == 0 || a == na - 1) {
+      u_new[f] = 0.0f;
+      continue;
+    }
+    const int64_t c1 = i * pl + (int64_t)j * g.nz + k;
+    const int64_t c0 = AX == 0 ? c1 - pl : (AX == 1 ? c1 - g.nz : c1 - 1);
+    if (!fluid(m, c0) && !fluid(m, c1)) {
+      u_new[f] = __ldg(u + f);
+      continue;
+    }
+    float bx, by, bz;
+    backtrace(bx, by, bz, cs, ii, ux, uy, uz, g);
+    u_new[f] = tri(u, fxn, fyn, fzn, bx, by, bz, sx, sy, sz);
   }
-  float bx, by, bz;
-  backtrace(bx, by, bz, cs, ux, uy, uz, g);
-  u_new[f] = tri(u, fxn, fyn, fzn, bx, by, bz, sx, sy, sz);
 }
 
 inline dim3 grid_for(int nx, int ny, int nz) {
   return dim3((unsigned)((nz + BK - 1) / BK), (unsigned)((ny + BJ - 1) / BJ), (unsigned)nx);
+}
+// CTAs of the marching kernels: PL planes each
+inline dim3 grid_pl(int nx, int ny, int nz) {
+  return dim3((unsigned)((nz + BK - 1) / BK), (unsigned)((ny + BJ - 1) / BJ),
+              (unsigned)((nx + PL - 1) / PL));
 }
 
 cudaError_t launch_velocity(int axis, float *u_new, const float *ux, const float *uy,
                             const float *uz, const uint8_t *m, const Geo &g, cudaStream_t s) {
   const dim3 blk(BK, BJ);
   if (axis == 0)
-    advect_u_kernel<0><<<grid_for(g.nx + 1, g.ny, g.nz), blk, 0, s>>>(u_new, ux, uy, uz, m, g);
+    advect_u_kernel<0><<<grid_pl(g.nx + 1, g.ny, g.nz), blk, 0, s>>>(u_new, ux, uy, uz, m, g);
   else if (axis == 1)
-    advect_u_kernel<1><<<grid_for(g.nx, g.ny + 1, g.nz), blk, 0, s>>>(u_new, ux, uy, uz, m, g);
+    advect_u_kernel<1><<<grid_pl(g.nx, g.ny + 1, g.nz), blk, 0, s>>>(u_new, ux, uy, uz, m, g);
   else
-    advect_u_kernel<2><<<grid_for(g.nx, g.ny, g.nz + 1), blk, 0, s>>>(u_new, ux, uy, uz, m, g);
+    advect_u_kernel<2><<<grid_pl(g.nx, g.ny, g.nz + 1), blk, 0, s>>>(u_new, ux, uy, uz, m, g);
   return cudaGetLastError();
 }
 
@@ -237,7 +249,7 @@ extern "C" int bsp_advect_temperature(float *T_new, const float *T_true, const f
   if (T_new == T_true || T_new == T_ext) return BSP_ERR_ALIAS;
   if (!dims_ok(nx, ny, nz) || !(dx > 0.0f)) return BSP_ERR_SHAPE;
   const Geo g{nx, ny, nz, ox, oy, oz, dx, dt};
-  advect_T_kernel<<<grid_for(nx, ny, nz), dim3(BK, BJ), 0, s>>>(T_new, T_true, T_ext, ux, uy,
+  advect_T_kernel<<<grid_pl(nx, ny, nz), dim3(BK, BJ), 0, s>>>(T_new, T_true, T_ext, ux, uy,
                                                                  uz, mask, g);
   return (int)cudaGetLastError();
 }
@@ -275,7 +287,7 @@ extern "C" int bsp_advect_all(float *ux, float *uy, float *uz, float *T, float *
                         s);
   if (e != cudaSuccess) return (int)e;
   extend_kernel<<<grid_for(nx, ny, nz), dim3(BK, BJ), 0, s>>>(T_ext, T, mask, nx, ny, nz);
-  advect_T_kernel<<<grid_for(nx, ny, nz), dim3(BK, BJ), 0, s>>>(T_tmp, T, T_ext, ux, uy, uz,
+  advect_T_kernel<<<grid_pl(nx, ny, nz), dim3(BK, BJ), 0, s>>>(T_tmp, T, T_ext, ux, uy, uz,
                                                                  mask, g);
   e = cudaGetLastError();
   if (e != cudaSuccess || !copy_back) return (int)e;
