@@ -123,20 +123,24 @@ __global__ void __launch_bounds__(BK *BJ) extend_kernel(float *__restrict__ T_ex
                                                         const float *__restrict__ T,
                                                         const uint8_t *__restrict__ m, int nx,
                                                         int ny, int nz) {
-  const int k = blockIdx.x * BK + threadIdx.x, j = blockIdx.y * BJ + threadIdx.y,
-            i = blockIdx.z;
+  const int k = blockIdx.x * BK + threadIdx.x, j = blockIdx.y * BJ + threadIdx.y;
   if (k >= nz || j >= ny) return;
-  const int64_t pl = (int64_t)ny * nz, c = i * pl + (int64_t)j * nz + k;
-  int64_t s = c;
-  if (!fluid(m, c)) {
-    // the six neighbour flags are loaded together, then the first fluid one
-    // in the order -x, +x, -y, +y, -z, +z is taken
-    const bool f0 = i > 0 && fluid(m, c - pl), f1 = i < nx - 1 && fluid(m, c + pl);
-    const bool f2 = j > 0 && fluid(m, c - nz), f3 = j < ny - 1 && fluid(m, c + nz);
-    const bool f4 = k > 0 && fluid(m, c - 1), f5 = k < nz - 1 && fluid(m, c + 1);
-    s = f0 ? c - pl : f1 ? c + pl : f2 ? c - nz : f3 ? c + nz : f4 ? c - 1 : f5 ? c + 1 : c;
+  const int64_t pl = (int64_t)ny * nz;
+  for (int ii = 0; ii < PL; ++ii) {
+    const int i = blockIdx.z * PL + ii;
+    if (i >= nx) break;
+    const int64_t c = i * pl + (int64_t)j * nz + k;
+    int64_t s = c;
+    if (!fluid(m, c)) {
+      // the six neighbour flags are loaded together, then the first fluid one
+      // in the order -x, +x, -y, +y, -z, +z is taken
+      const bool f0 = i > 0 && fluid(m, c - pl), f1 = i < nx - 1 && fluid(m, c + pl);
+      const bool f2 = j > 0 && fluid(m, c - nz), f3 = j < ny - 1 && fluid(m, c + nz);
+      const bool f4 = k > 0 && fluid(m, c - 1), f5 = k < nz - 1 && fluid(m, c + 1);
+      s = f0 ? c - pl : f1 ? c + pl : f2 ? c - nz : f3 ? c + nz : f4 ? c - 1 : f5 ? c + 1 : c;
+    }
+    T_ext[c] = __ldg(T + s);
   }
-  T_ext[c] = __ldg(T + s);
 }
 
 __global__ void __launch_bounds__(BK *BJ) advect_T_kernel(
@@ -197,10 +201,7 @@ __global__ void __launch_bounds__(BK *BJ) advect_u_kernel(float *__restrict__ u_
   }
 }
 
-inline dim3 grid_for(int nx, int ny, int nz) {
-  return dim3((unsigned)((nz + BK - 1) / BK), (unsigned)((ny + BJ - 1) / BJ), (unsigned)nx);
-}
-// CTAs of the marching kernels: PL planes each
+// CTAs of the kernels: 64 k x 4 j, PL planes each
 inline dim3 grid_pl(int nx, int ny, int nz) {
   return dim3((unsigned)((nz + BK - 1) / BK), (unsigned)((ny + BJ - 1) / BJ),
               (unsigned)((nx + PL - 1) / PL));
@@ -236,7 +237,7 @@ extern "C" int bsp_extend_temperature(float *T_ext, const float *T, const uint8_
   if (!T_ext || !T || !mask) return BSP_ERR_NULL;
   if (T_ext == T) return BSP_ERR_ALIAS;
   if (!dims_ok(nx, ny, nz)) return BSP_ERR_SHAPE;
-  extend_kernel<<<grid_for(nx, ny, nz), dim3(BK, BJ), 0, s>>>(T_ext, T, mask, nx, ny, nz);
+  extend_kernel<<<grid_pl(nx, ny, nz), dim3(BK, BJ), 0, s>>>(T_ext, T, mask, nx, ny, nz);
   return (int)cudaGetLastError();
 }
 
@@ -286,7 +287,7 @@ extern "C" int bsp_advect_all(float *ux, float *uy, float *uz, float *T, float *
     e = launch_velocity(ax, ax == 0 ? ux_tmp : (ax == 1 ? uy_tmp : uz_tmp), ux, uy, uz, mask, g,
                         s);
   if (e != cudaSuccess) return (int)e;
-  extend_kernel<<<grid_for(nx, ny, nz), dim3(BK, BJ), 0, s>>>(T_ext, T, mask, nx, ny, nz);
+  extend_kernel<<<grid_pl(nx, ny, nz), dim3(BK, BJ), 0, s>>>(T_ext, T, mask, nx, ny, nz);
   advect_T_kernel<<<grid_pl(nx, ny, nz), dim3(BK, BJ), 0, s>>>(T_tmp, T, T_ext, ux, uy, uz,
                                                                  mask, g);
   e = cudaGetLastError();
