@@ -99,7 +99,9 @@ class ThermalGrid:
     T: torch.Tensor    # (nx, ny, nz) f32, kelvin
     mat: torch.Tensor  # (nx, ny, nz) int32 material ids
     mat_id: torch.Tensor | None = None  # uint8 copy of mat, derived once
-    classes: "CellClasses | None" = None  # conduction cell classes, derived once
+    # conduction cell classes, derived on the first step; False when the geometry
+    # has more than 127 neighbourhoods (the material-id kernels serve it then)
+    classes: "CellClasses | bool | None" = None
 
     @property
     def shape(self):

@@ -128,3 +128,19 @@ def test_face_rules():
         inner = [slice(None)] * 3
         inner[ax] = slice(1, -1)
         assert np.array_equal(un[tuple(inner)][both], src[tuple(inner)][both])
+
+
+def test_uniform_flow_translates_a_linear_face_profile():
+    """advect_ux with ux = U + b y on all-fluid cells and uy = uz = 0: the
+    backtrace moves (U + b y) dt along x only, and ux is constant along x,
+    so interior faces keep their value (up to rounding)."""
+    n, dx, dt, U, b = 12, 0.002, 0.01, 0.05, 2.0
+    mat = np.full((n, n, n), F, np.int32)
+    y = (np.arange(n) + 0.5) * dx
+    ux = np.broadcast_to((U + b * y)[None, :, None], (n + 1, n, n)).astype(np.float32).copy()
+    uy = np.zeros((n, n + 1, n), np.float32)
+    uz = np.zeros((n, n, n + 1), np.float32)
+    un = O.advect_velocity(0, ux, uy, uz, mat, (0.0, 0.0, 0.0), dx, dt)
+    inner = (slice(2, n - 1), slice(1, n - 1), slice(1, n - 1))
+    np.testing.assert_allclose(un[inner], ux[inner], rtol=0, atol=1e-6)
+    assert np.all(un[0] == 0) and np.all(un[-1] == 0)

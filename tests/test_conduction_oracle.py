@@ -112,3 +112,21 @@ def test_odd_count_copies_the_ping_pong_buffer_back():
         else:
             cur = O.conduction_sweep(cur, a, T, mat, *args)
     assert np.array_equal(a, ao)
+
+
+def test_newton_cooling_pulls_a_uniform_block_toward_ambient():
+    """A steel block in air, uniform and above T_amb: every step lowers every
+    block cell and none falls below T_amb; the corners (three air faces) cool
+    fastest, the centre slowest."""
+    k, rho, cp = props()
+    mat = np.full((8, 8, 8), 2, np.int32)
+    mat[1:-1, 1:-1, 1:-1] = 1
+    T = np.full(mat.shape, 400.0, np.float32)
+    solid = mat == 1
+    prev = T
+    for _ in range(3):
+        Tn, _, _ = O.conduction_be(prev, np.zeros_like(prev), mat, (k, rho, cp), 0.002, 50.0,
+                                   10.0, 295.0, n_iter=30)
+        assert np.all(Tn[solid] < prev[solid]) and np.all(Tn[solid] > 295.0)
+        prev = Tn
+    assert prev[1, 1, 1] < prev[4, 4, 4]
