@@ -100,6 +100,7 @@ SIGNATURES = {
     "bsp_unet_adam": (_I, [_P, _P, _P, _P, _P, _L, _F, _F, _F, _F, _I, _P]),
     "bsp_spmv": (_I, [_P, _P, _P, _I, _I, _I, _P]),
     "bsp_selftest_div6": (_I, [_P, _P]),
+    "bsp_selftest_waits": (_I, [_P, _P, _P]),
     "bsp_solve_params_default": (None, [_P]),
     "bsp_solver_workspace_bytes": (ctypes.c_size_t, [_I, _I, _I, _I]),
     "bsp_solve_tol": (_I, [_P, _P, _P, _I, _I, _I, _F, _F, _F, _P, _P, ctypes.c_size_t, _P, _P,

@@ -280,6 +280,13 @@ extern "C" int bsp_advect_all(float *ux, float *uy, float *uz, float *T, float *
   for (const float *o : outs)
     for (const float *in : ins)
       if (o == in) return BSP_ERR_ALIAS;
+  // the five outputs are written by different kernels while T_ext is still
+  // being sampled: no two may share a base, and none may be the mask
+  for (int a = 0; a < 5; ++a) {
+    if ((const void *)outs[a] == (const void *)mask) return BSP_ERR_ALIAS;
+    for (int b = a + 1; b < 5; ++b)
+      if (outs[a] == outs[b]) return BSP_ERR_ALIAS;
+  }
   if (!dims_ok(nx, ny, nz) || !(dx > 0.0f)) return BSP_ERR_SHAPE;
   const Geo g{nx, ny, nz, ox, oy, oz, dx, dt};
   cudaError_t e = cudaSuccess;

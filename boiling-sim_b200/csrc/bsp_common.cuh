@@ -11,6 +11,8 @@
 // air (jacobi_pressure.cu:121-124).
 #pragma once
 #include <cstdint>
+#include <mutex>
+#include <vector>
 #include <cuda_runtime.h>
 #include "../../include/bsproj.h"
 
@@ -107,5 +109,28 @@ __device__ __forceinline__ float spmv_update(float l, float r, float d, float u,
 }
 
 __device__ __forceinline__ uint32_t byte_of(uint32_t w, int q) { return (w >> (8 * q)) & 0xffu; }
+
+// Opt kernel `fn` into `bytes` of dynamic shared memory on the current
+// device.  The attribute belongs to the device, so the answer is cached per
+// (kernel, device): a second GPU in the same process gets its own opt-in.
+// False when the device refuses (the caller then takes another path).
+inline bool smem_opt_in(const void *fn, int bytes) {
+  struct Entry {
+    const void *fn;
+    int dev;
+    bool ok;
+  };
+  static std::mutex mu;
+  static std::vector<Entry> done;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return false;
+  std::lock_guard<std::mutex> lk(mu);
+  for (const Entry &e : done)
+    if (e.fn == fn && e.dev == dev) return e.ok;
+  const bool ok = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) ==
+                  cudaSuccess;
+  done.push_back(Entry{fn, dev, ok});
+  return ok;
+}
 
 }  // namespace bsp

@@ -911,23 +911,13 @@ bool launch_cls_tma(float *dst, const float *src, const float *told, float *snap
   if (!SNAP && !make_map(&maps.o, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, told, nx, ny, nz, 128, ROWS))
     return false;
   if (SNAP) maps.o = maps.t;
-  // the shared-memory opt-in is per device: 0 not yet set, 1 set, 2 refused
-  static int attr[2][64];
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return false;
-  int dummy = 0;
-  int &a = dev < 64 ? attr[SNAP ? 1 : 0][dev] : dummy;
-  if (a == 0)
-    a = cudaFuncSetAttribute(be_cls_tma_kernel<SNAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             TOTAL) == cudaSuccess
-            ? 1
-            : 2;
-  if (a != 1) return false;
+  // the shared-memory opt-in is per device
+  if (!smem_opt_in((const void *)be_cls_tma_kernel<SNAP>, TOTAL)) return false;
   const int bi = tma_bi(nx, ny, nz);
   dim3 grid((nz + 127) / 128, (ny + ROWS - 1) / ROWS, (nx + bi - 1) / bi);
   be_cls_tma_kernel<SNAP><<<grid, THREADS + 32, TOTAL, s>>>(dst, snap, maps, patterns, ncls,
                                                             tiles, nx, ny, nz, bi, P);
-  return true;
+  return cudaGetLastError() == cudaSuccess;
 }
 
 template <bool SNAP>

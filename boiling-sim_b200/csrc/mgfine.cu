@@ -866,16 +866,10 @@ template <class T, class Op>
 static bool launch_tma(const Op &op, const TmaMaps &maps, int nx, int ny, int nz,
                        const uint8_t *tiles, const SolverState *st, cudaStream_t s) {
   using L = TmaSmem<T, Op>;
-  static std::once_flag once;
-  static cudaError_t attr = cudaSuccess;
-  std::call_once(once, [] {
-    attr = cudaFuncSetAttribute(fine_tma_kernel<T, Op>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                L::TOTAL);
-  });
-  if (attr != cudaSuccess) return false;
+  if (!smem_opt_in((const void *)fine_tma_kernel<T, Op>, L::TOTAL)) return false;
   fine_tma_kernel<T, Op><<<fine_grid(nx, ny, nz), TILE_THREADS, L::TOTAL, s>>>(
       op, maps, nx, ny, nz, fine_bi(nx, ny, nz), tiles, st);
-  return true;
+  return cudaGetLastError() == cudaSuccess;
 }
 
 // ---- FP64 residual on the column layout --------------------------------------------------

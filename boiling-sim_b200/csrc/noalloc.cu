@@ -18,9 +18,13 @@
 //     clearing, but calls that overlap on the GPU (different streams, or
 //     different host threads) race on the array and must be serialised;
 //   * host code cannot pass the array's name to a kernel (on the host it is only
-//     a stand-in symbol): the device address is looked up once per device with
-//     cudaGetSymbolAddress, with that device current, by the first call made on
-//     it.  That first call should therefore come before any stream capture.
+//     a stand-in symbol): the device address is looked up with
+//     cudaGetSymbolAddress, with the device current, by every call made
+//     outside a stream capture, and kept per device for calls made inside one.
+//     The first call on a device should therefore come before any stream
+//     capture; after a cudaDeviceReset, the first call should again come
+//     outside a capture (the module is loaded anew and the kept address is
+//     stale until a call outside a capture refreshes it).
 #include <mutex>
 
 #include "bsp_common.cuh"
@@ -32,7 +36,7 @@ constexpr int64_t NOALLOC_CHUNK = 65536;
 constexpr int NOALLOC_THREADS = 256;
 constexpr int MAX_DEVICES = 64;
 
-__device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_PARTIALS];
+static __device__ __align__(256) double g_noalloc_partials[NOALLOC_MAX_PARTIALS];
 
 namespace {
 std::mutex g_addr_mu;
@@ -75,18 +79,25 @@ __global__ void __launch_bounds__(NOALLOC_THREADS) noalloc_final_kernel(
   if (threadIdx.x == 0) *result = s;
 }
 
-// Device address of g_noalloc_partials on the current device (looked up once).
-static int noalloc_scratch(double **out) {
+// Device address of g_noalloc_partials on the current device: looked up on
+// every call outside a stream capture (so a module reloaded after
+// cudaDeviceReset is found again), taken from the per-device record inside one.
+static int noalloc_scratch(double **out, cudaStream_t stream) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return (int)e;
   if (dev < 0 || dev >= MAX_DEVICES) return BSP_ERR_ARG;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(stream, &cap);
+  if (e != cudaSuccess) return (int)e;
   std::lock_guard<std::mutex> lk(g_addr_mu);
-  if (!g_addr[dev]) {
+  if (cap == cudaStreamCaptureStatusNone) {
     double *ptr = nullptr;
     e = cudaGetSymbolAddress((void **)&ptr, g_noalloc_partials);
     if (e != cudaSuccess) return (int)e;
     g_addr[dev] = ptr;
+  } else if (!g_addr[dev]) {
+    return BSP_ERR_ARG;  // first call on this device made inside a capture
   }
   *out = g_addr[dev];
   return BSP_OK;
@@ -102,7 +113,7 @@ extern "C" int bsp_dot_noalloc(const float *x, const float *y, int64_t n, double
   if (n > (int64_t)NOALLOC_MAX_PARTIALS * NOALLOC_CHUNK) return BSP_ERR_SHAPE;
   if (n > 0 && (!x || !y)) return BSP_ERR_NULL;
   double *partials = nullptr;
-  int st = noalloc_scratch(&partials);
+  int st = noalloc_scratch(&partials, stream);
   if (st != BSP_OK) return st;
   if (n == 0) return (int)cudaMemsetAsync(result, 0, sizeof(double), stream);
   const int np = (int)((n + NOALLOC_CHUNK - 1) / NOALLOC_CHUNK);

@@ -31,7 +31,10 @@
 #include <mutex>
 #include <vector>
 
+#include <cstddef>
+
 #include "bsp_common.cuh"
+#include "grid_sync.cuh"
 #include "profile.cuh"
 #include "solver.cuh"
 
@@ -52,6 +55,9 @@ extern bool g_fine_tma_enabled;      // BSP_TUNE_FINE_TMA (mgfine.cu)
 extern bool g_coarse_fused_enabled;  // BSP_TUNE_COARSE_FUSED (mgcoarse.cu)
 // BSP_TUNE_FUSE_UPDATE: CG update fused into the next level-0 restriction
 bool g_fuse_update_enabled = true;
+// BSP_TUNE_TEST_BARRIER_ERROR (tests only): the next host-driven solve starts
+// with the coarse-cycle barrier's error word set
+bool g_test_barrier_error = false;
 constexpr int COARSE_SWEEPS = 64;
 constexpr int RED_THREADS = 256;
 
@@ -1113,6 +1119,22 @@ int solve_impl(void *ws, const uint8_t *mask, const float *div, float *p_out, in
   h.scale = 1.0;
   cudaError_t e = cudaMemcpyAsync(cx.st, &h, sizeof(h), cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return (int)e;
+  // the coarse-cycle grid barrier starts every solve clean: a barrier that
+  // gave up in an earlier solve leaves its error word and a partial count
+  e = cudaMemsetAsync(cx.base + cx.lo.cctl, 0, 64, s);
+  if (e != cudaSuccess) return (int)e;
+  if (g_test_barrier_error) {
+    // test hook (BSP_TUNE_TEST_BARRIER_ERROR): start this solve with the
+    // barrier's error word set, as a barrier that gave up leaves it; the
+    // coarse cycle then returns at its first barrier and the solve reports
+    // BSP_ERR_TIMEOUT.  One-shot.
+    g_test_barrier_error = false;
+    const int v = BSP_ERR_TIMEOUT;
+    e = cudaMemcpyAsync(cx.base + cx.lo.cctl + offsetof(GridCtl, err), &v, sizeof(int),
+                        cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // v lives on this stack frame
+    if (e != cudaSuccess) return (int)e;
+  }
   if (!(prm->reuse_setup && setup_cached(ws, mask, nx, ny, nz, prm->storage))) {
     e = setup_levels<T>(cx, s);
     if (e != cudaSuccess) return (int)e;
@@ -1287,6 +1309,9 @@ cudaError_t append_solve(Ctx<T> &cx, const float *div, float *p_out, float dx, f
   if ((e = seg_begin(cs, g, deps)) != cudaSuccess) return e;
   init_state_kernel<<<1, 1, 0, cs>>>(st, prm->tol, prm->inner_tol, prm->max_outer,
                                      prm->max_inner);
+  // every replay starts with a clean coarse-cycle grid barrier (error word,
+  // count and generation), whatever an earlier replay left there
+  cudaMemsetAsync(cx.base + cx.lo.cctl, 0, 64, cs);
   cudaMemsetAsync(x, 0, sizeof(double) * cx.n, cs);
   (void)nbr;
   const int nres = launch_resid<T>(cx, div, x, bscale, nullptr, nullptr, false, cs);

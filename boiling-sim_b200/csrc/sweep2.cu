@@ -234,13 +234,7 @@ bool launch_sweep2(float *out, const float *p, const float *rhs, const uint8_t *
         make_map(&maps.m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, mask, nx, ny, nz, MW, R0) &&
         make_map(&maps.r, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, rhs, nx, ny, nz, FW, R1)))
     return false;
-  static std::once_flag once;
-  static cudaError_t attr = cudaSuccess;
-  std::call_once(once, [] {
-    attr = cudaFuncSetAttribute(sweep2_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                TOTAL);
-  });
-  if (attr != cudaSuccess) return false;
+  if (!smem_opt_in((const void *)sweep2_kernel, TOTAL)) return false;
   int *err = nullptr;
   if (cudaGetSymbolAddress((void **)&err, g_sweep2_err) != cudaSuccess) return false;
   const int64_t cols = (int64_t)((nz + 127) / 128) * ((ny + ROWS - 1) / ROWS);

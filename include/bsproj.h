@@ -62,6 +62,10 @@ extern "C" {
 #define BSP_TUNE_SWEEP_TBLOCK 8 /* sweeps per HBM pass when a call passes tblock = 0 (1 or 2) */
 #define BSP_TUNE_COND_BI 9      /* i-planes per CTA of the conduction sweeps (0 = rule) */
 #define BSP_TUNE_COND_TMA 10    /* conduction class sweep fed by TMA tiles: 1 on, 0 off */
+/* Tests only: 1 makes the next host-driven bsp_solve_tol start with the
+ * coarse-cycle grid barrier's error word set, as a barrier that gave up
+ * leaves it (that solve returns BSP_ERR_TIMEOUT; the key clears itself). */
+#define BSP_TUNE_TEST_BARRIER_ERROR 11
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */
@@ -309,8 +313,11 @@ int bsp_solve_tol(float *p, const float *div_u, const uint8_t *mask, int nx, int
  * doubles (8 KiB per GPU, kept until exit); n may be at most 67,108,864
  * (1024 partials x 65,536 elements), larger n returns BSP_ERR_SHAPE.  All
  * calls share that array: calls that overlap on the GPU race and must be
- * serialised.  The first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) and should come before any stream capture.
+ * serialised.  Every call made outside a stream capture looks up the
+ * array's device address (cudaGetSymbolAddress) and keeps it per device for
+ * calls made inside one; the first call on a device, and the first after a
+ * cudaDeviceReset (which reloads the module), should therefore come outside
+ * any stream capture (a first call inside one returns BSP_ERR_ARG).
  * Allocates nothing; never calls cudaMalloc or cudaFree. */
 #define BSP_DOT_NOALLOC_MAX_N 67108864LL
 int bsp_dot_noalloc(const float *x, const float *y, int64_t n, double *result_dev,
@@ -518,6 +525,15 @@ int bsp_unet_sum_partials(float *out, const float *partials, int nblocks, int ns
 /* One Adam step on FP32 master weights w with BF16 copy wb. */
 int bsp_unet_adam(float *w, bsp_bf16_t *wb, float *m, float *v, const float *g, int64_t n,
                   float lr, float b1, float b2, float eps, int step, cudaStream_t stream);
+
+/* Self-check of the bounded device waits: one grid barrier that a block never
+ * reaches (grid_sync.cuh) and one mbarrier wait that nothing completes
+ * (tma.cuh), each given up after its poll bound (about a second).
+ * codes_dev[0] and codes_dev[1] (device ints) receive BSP_ERR_TIMEOUT when
+ * the wait gave up as designed; scratch_dev is >= 64 bytes of device memory
+ * for the barrier's control words (zeroed here).  The context stays usable.
+ * No reference counterpart (the reference has no bounded waits). */
+int bsp_selftest_waits(int *codes_dev, void *scratch_dev, cudaStream_t stream);
 
 /* Exhaustive self-check of the device division-by-6 against IEEE division
  * over all 2^32 float bit patterns; the mismatch count is written to the

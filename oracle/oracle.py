@@ -46,9 +46,20 @@ _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _I, _F, _D, _L = ctypes.c_int, ctypes.c_float, ctypes.c_double, ctypes.c_int64
 
 
+# Where the reference's hot-path CUDA sources lie when the reference tree is
+# mounted (the build recipe compiles them in place into oracle/_ref); override
+# with BOILINGSIM_REFERENCE_SRC.
+_REF_SRC_DEFAULT = "/root/reference/crates/cuda-kernels/src"
+
+
 def build() -> None:
-    """Compile liboracle.so (and oracle/_ref when the reference is present)."""
-    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    """Compile liboracle.so, and oracle/_ref when the reference sources are
+    present."""
+    src = os.environ.get("BOILINGSIM_REFERENCE_SRC", _REF_SRC_DEFAULT)
+    cmd = ["make", "-s", "-C", _HERE]
+    if os.path.isdir(src):
+        cmd.append(f"REF_SRC={src}")
+    subprocess.run(cmd, check=True)
 
 
 def lib() -> ctypes.CDLL:
@@ -73,6 +84,10 @@ def lib() -> ctypes.CDLL:
             "or_diag_inverse_f32": (None, [_f32p, _f32p, _i32p, _I, _I, _I, _I, _I]),
             "or_compute_b_f32": (None, [_f32p, _f32p, _i32p, _I, _I, _I, _F, _F, _F, _I]),
             "or_dot_f32_f64": (_D, [_f32p, _f32p, _L]),
+            "or_axpy_f32": (None, [_f32p, _f32p, _F, _L, _I]),
+            "or_scaled_axpy_f32": (None, [_f32p, _f32p, _f32p, _F, _L]),
+            "or_divide_f32": (_F, [_F, _F]),
+            "or_scale_f32": (None, [_f32p, _L, _F]),
             "or_pcg_f32": (_I, [_f32p, _f32p, _i32p, _I, _I, _I, _F, _F, _F, _I, _I, _F, _I]),
             "or_apply_A_f64": (None, [_f64p, _f64p, _i32p, _I, _I, _I, _I, _I]),
             "or_rhs_f64": (None, [_f64p, _f32p, _i32p, _L, _D, _D, _D, _I]),
@@ -209,6 +224,34 @@ def dot_f64(x, y):
     x = _c(x, np.float32).ravel()
     y = _c(y, np.float32).ravel()
     return float(lib().or_dot_f32_f64(x, y, x.size))
+
+
+def axpy(y, x, alpha, negate=False):
+    """axpy_device.cu:20-31 (FMA build): returns alpha x + y, alpha negated
+    first when ``negate``."""
+    out = _c(y, np.float32).copy()
+    lib().or_axpy_f32(out, _c(x, np.float32), np.float32(alpha), out.size, 1 if negate else 0)
+    return out
+
+
+def scaled_axpy(z, p_old, beta):
+    """axpy_device.cu:51-63 (FMA build): z + beta p_old."""
+    z = _c(z, np.float32)
+    out = np.empty_like(z)
+    lib().or_scaled_axpy_f32(out, z, _c(p_old, np.float32), np.float32(beta), z.size)
+    return out
+
+
+def divide_scalars(num, den):
+    """axpy_device.cu:84-91: num / den, 0 when den == 0."""
+    return np.float32(lib().or_divide_f32(np.float32(num), np.float32(den)))
+
+
+def scale(x, s):
+    """scale.cu:11-17: x * s."""
+    out = _c(x, np.float32).copy()
+    lib().or_scale_f32(out, out.size, np.float32(s))
+    return out
 
 
 def pcg(div, mat, dx, dt, rho, tol, max_iter, mat_fluid=MAT_FLUID, mat_air=MAT_AIR):

@@ -338,6 +338,24 @@ void or_compute_b_f32(float *b, const float *div, const int32_t *mat, int nx, in
     for (int64_t c = 0; c < n; ++c) b[c] = (mat[c] != mat_fluid) ? 0.0f : scale * div[c];
 }
 
+/* CG vector updates of axpy_device.cu, as the reference's default (FMA on)
+ * build evaluates them: y = alpha x + y contracted to fmaf (axpy_device.cu:
+ * 20-31; negate_alpha flips the sign of alpha first), p_out = z + beta p_old
+ * contracted to fmaf(beta, p_old, z) (:51-63), num / den with den == 0 -> 0
+ * (:84-91).  scale.cu:11-17 is a plain product. */
+void or_axpy_f32(float *y, const float *x, float alpha, int64_t n, int negate) {
+    const float a = negate ? -alpha : alpha;
+    for (int64_t c = 0; c < n; ++c) y[c] = fmaf(a, x[c], y[c]);
+}
+void or_scaled_axpy_f32(float *out, const float *z, const float *p_old, float beta,
+                        int64_t n) {
+    for (int64_t c = 0; c < n; ++c) out[c] = fmaf(beta, p_old[c], z[c]);
+}
+float or_divide_f32(float num, float den) { return den == 0.0f ? 0.0f : num / den; }
+void or_scale_f32(float *x, int64_t n, float s) {
+    for (int64_t c = 0; c < n; ++c) x[c] = x[c] * s;
+}
+
 /* Deterministic FP64 dot of two float vectors: fixed 4096-element blocks,
  * block partials summed in order. */
 double or_dot_f32_f64(const float *x, const float *y, int64_t n) {

@@ -151,3 +151,42 @@ def test_golden_fixed_count_solve(path):
 def test_golden_vectors_present():
     """The reference-generated fixtures are committed (parity is pinned)."""
     assert glob.glob(os.path.join(GOLDEN, "sweep_*.npz")), "no golden sweep fixtures"
+
+
+@pytest.mark.parametrize("name", ["pcg_box_0.01", "pcg_box_1e-06"])
+def test_oracle_pcg_matches_reference_pcg_goldens(name):
+    """The oracle's PCG against the reference's own pressure_solve_pcg_launch
+    (pressure_solve_pcg.cu:89-243, run on a B200 from oracle/_ref by
+    tests/golden/make_golden.py): the same iteration count (the check
+    cadence, every 5 iterations from iteration 8, makes a one-check difference
+    5 iterations) and the same pressure to within the FP32 PCG's own rounding
+    (the reference sums its dot products in FP32, the oracle in FP64)."""
+    d = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    dx, dt, rho, tol = (float(d[k]) for k in ("dx", "dt", "rho", "tol"))
+    p, it = O.pcg(d["div"], d["mat"], dx, dt, rho, tol, 200)
+    assert abs(it - int(d["iters"])) <= 5, (it, int(d["iters"]))
+    fl = d["mat"] == 0
+    ref = d["p"].astype(np.float64)
+    err = np.linalg.norm(p[fl] - ref[fl]) / np.linalg.norm(ref[fl])
+    assert err <= 1e-5, err
+    # both stop below the tolerance on the true residual within FP32 rounding
+    assert O.rel_residual(p, d["div"], d["mat"], dx, dt, rho) <= 1.5 * tol
+    b = O.compute_b(d["div"], d["mat"], dx, dt, rho)
+    assert O.dot_f64(b, b) == pytest.approx(float(d["bsq"]), rel=1e-6)
+
+
+def test_oracle_cg_vector_ops_known_answers():
+    """axpy_device.cu:20-99 and scale.cu:11-17 restated: fused multiply-add
+    rounding (one rounding, as the reference's FMA build), the negated alpha,
+    the den == 0 -> 0 rule of divide_scalars (axpy_device.cu:90)."""
+    x = np.array([1.0, 3.0, -2.0, 1e8], np.float32)
+    y = np.array([0.5, 1.0, 4.0, 1.0], np.float32)
+    a = np.float32(1.0 / 3.0)
+    got = O.axpy(y, x, a)
+    want = (a.astype(np.float64) * x.astype(np.float64) + y.astype(np.float64)).astype(np.float32)
+    assert np.array_equal(got, want)
+    assert np.array_equal(O.axpy(y, x, a, negate=True), O.axpy(y, x, -a))
+    assert np.array_equal(O.scaled_axpy(y, x, a), O.axpy(y, x, a))
+    assert O.divide_scalars(3.0, 0.0) == 0.0
+    assert O.divide_scalars(3.0, 2.0) == np.float32(1.5)
+    assert np.array_equal(O.scale(x, 2.0), x * np.float32(2.0))
