@@ -98,6 +98,19 @@ SIGNATURES = {
     "bsp_unet_sum_partials": (_I, [_P, _P, _I, _I, _P]),
     "bsp_unet_head_bwd": (_I, [_P, _P, _I, _P, _P, _P, _P, _L, _P]),
     "bsp_unet_adam": (_I, [_P, _P, _P, _P, _P, _L, _F, _F, _F, _F, _I, _P]),
+    # tensor-core (tcgen05) inference path on the padded layout (unet_tc.cu)
+    "bsp_unet_tc_rows": (_L, [_I, _I, _I]),
+    "bsp_unet_tc_weights": (_I, [_P, _P, _I, _I, _P]),
+    "bsp_unet_tc_conv3": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
+    "bsp_unet_tc_error": (_I, [_P]),
+    "bsp_unet_tc_pack": (_I, [_P, _P, _P, _I, _I, _I, _P, _P]),
+    "bsp_unet_scale_workspace_bytes": (ctypes.c_size_t, []),
+    "bsp_unet_input_scale": (_I, [_P, _P, _P, _I, _I, _I, _P, ctypes.c_size_t, _P]),
+    "bsp_unet_tc_pool": (_I, [_P, _P, _I, _I, _I, _I, _P]),
+    "bsp_unet_tc_up": (_I, [_P, _P, _I, _I, _I, _I, _P]),
+    "bsp_unet_tc_head": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _P, _F, _P]),
+    "bsp_unet_restrict_div": (_I, [_P, _P, _P, _P, _I, _I, _I, _P]),
+    "bsp_unet_prolong": (_I, [_P, _P, _P, _I, _I, _I, _P]),
     "bsp_spmv": (_I, [_P, _P, _P, _I, _I, _I, _P]),
     "bsp_selftest_div6": (_I, [_P, _P]),
     "bsp_selftest_waits": (_I, [_P, _P, _P]),

@@ -262,7 +262,7 @@ def _tol_projection(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, solver:
     if solver == "b200-learned" and all(d % 8 == 0 for d in grid.shape):
         # the network's pressure is the starting guess; the solve finishes it
         # to the same tolerance (grids not divisible by 8 start from zero)
-        grid.p.copy_(_learned_net().predict(ws.div_u, mask, dx, dt, rho))
+        _warm_start(grid, mask).guess(ws.div_u, dx, dt, rho, out=grid.p)
         warm = True
     tol_solver.solve(ws.div_u, dx, dt, rho, tol=float(cfg.solver.pressure_tol), p=grid.p,
                      warm_start=warm, raise_on_fail=False, graph=True)
@@ -271,6 +271,18 @@ def _tol_projection(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, solver:
 
 
 _NET = None
+_WARM_STARTS: dict = {}
+
+
+def _warm_start(grid: Grid, mask: torch.Tensor):
+    """The learned warm start of this grid (network resolution chosen by the
+    grid size, boilingsim_b200.learned.WarmStart), built once per grid."""
+    key = (id(grid), grid.shape)
+    if key not in _WARM_STARTS:
+        from .learned import WarmStart
+
+        _WARM_STARTS[key] = WarmStart(_learned_net(), grid.mat, mask)
+    return _WARM_STARTS[key]
 
 
 def _learned_net():

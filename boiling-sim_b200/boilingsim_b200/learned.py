@@ -200,10 +200,25 @@ class UNet:
         c["mask"] = mask
         return p, c
 
-    def predict(self, div, mask, dx, dt, rho) -> torch.Tensor:
+    def predict(self, div, mask, dx, dt, rho, backend: str = "tc") -> torch.Tensor:
+        """The network's pressure for ``div``.  ``backend="tc"``: inference on
+        the fifth-generation tensor cores (tcgen05 kernels, padded layout,
+        buffers kept per grid shape); ``"mma"``: the training forward pass
+        (mma.sync kernels), which also keeps the activations for backward."""
+        if backend == "tc":
+            return self.tc_plan(tuple(div.shape)).run(div, mask, dx, dt, rho)
         with torch.no_grad():
             p, _ = self.forward(div, mask, tuple(div.shape), dx, dt, rho)
         return p
+
+    def tc_plan(self, dims) -> "TcPlan":
+        plans = self.__dict__.setdefault("_tc_plans", {})
+        if dims not in plans:
+            plans[dims] = TcPlan(self, dims)
+        plan = plans[dims]
+        if plan.version != self.step:
+            plan.refresh_weights()
+        return plan
 
     # ---- backward -----------------------------------------------------------------------------
     def _wgrad_ws(self, dims, cin, cout):
@@ -351,6 +366,141 @@ class UNet:
         loss = self.backward(c, target, loss)
         self.adam_step(lr)
         return loss
+
+
+class TcPlan:
+    """Inference of the network on one grid shape with the tensor-core
+    kernels (``bsp_unet_tc_*``): activations on the padded layout (a one-cell
+    zero halo per level), every buffer allocated and zero-filled once, the
+    weight images rebuilt when the weights change.  The skip additions of the
+    decoder are fused into the epilogue of the convolution before them."""
+
+    def __init__(self, net: UNet, dims):
+        nx, ny, nz = dims
+        if nx % 8 or ny % 8 or nz % 8:
+            raise ValueError("U-Net grids need dimensions divisible by 8")
+        self.net = net
+        self.dims = (dims, (nx // 2, ny // 2, nz // 2), (nx // 4, ny // 4, nz // 4),
+                     (nx // 8, ny // 8, nz // 8))
+        lib = _lib.lib()
+        dev = net.device
+
+        def buf(level, c):
+            rows = int(lib.bsp_unet_tc_rows(*self.dims[level]))
+            return torch.zeros((rows, c), dtype=torch.bfloat16, device=dev)
+
+        # level-indexed activations (names as in UNet.forward)
+        spec = {"x0": (0, 16), "a1": (0, 16), "e1": (0, 16), "p1": (1, 16), "a2": (1, 32),
+                "e2": (1, 32), "p2": (2, 32), "a3": (2, 64), "e3": (2, 64), "p3": (3, 64),
+                "a4": (3, 128), "b4": (3, 128), "q3": (2, 128), "c3": (2, 64), "u3": (2, 64),
+                "q2": (1, 64), "c2": (1, 32), "u2": (1, 32), "q1": (0, 32), "c1": (0, 16),
+                "u1": (0, 16)}
+        self.a = {k: buf(lv, c) for k, (lv, c) in spec.items()}
+        self.wimg = {L.name: torch.empty(27 * L.cin * L.cout, dtype=torch.bfloat16, device=dev)
+                     for L in net.layers}
+        self.s_dev = torch.ones(1, dtype=torch.float32, device=dev)  # input scale s
+        nb = int(lib.bsp_unet_scale_workspace_bytes())
+        self.scale_ws = torch.empty((nb + 7) // 8, dtype=torch.float64, device=dev)
+        self.version = None
+        self.refresh_weights()
+
+    def refresh_weights(self):
+        st = stream_handle()
+        for L in self.net.layers:
+            call("bsp_unet_tc_weights", ptr(self.wimg[L.name]), ptr(L.wb), L.cin, L.cout, st)
+        self.version = self.net.step
+
+    def _conv(self, dst, src, name, level, skip=None):
+        L = self.net.by[name]
+        call("bsp_unet_tc_conv3", ptr(self.a[dst]), ptr(self.a[src]), ptr(self.wimg[name]),
+             ptr(L.b), ptr(self.a[skip]) if skip else None, *self.dims[level], L.cin, L.cout, 1,
+             stream_handle())
+
+    def run(self, div, mask, dx, dt, rho, out=None) -> torch.Tensor:
+        """Network pressure for ``div`` (no host synchronisation: the input
+        scale s is computed and applied on the device, S = -(rho dx^2/dt) s)."""
+        st = stream_handle()
+        d = self.dims
+        call("bsp_unet_input_scale", ptr(self.s_dev), ptr(div), ptr(mask), *d[0],
+             ptr(self.scale_ws), self.scale_ws.numel() * 8, st)
+        call("bsp_unet_tc_pack", ptr(self.a["x0"]), ptr(div), ptr(mask), *d[0], ptr(self.s_dev),
+             st)
+        self._conv("a1", "x0", "e1a", 0)
+        self._conv("e1", "a1", "e1b", 0)
+        call("bsp_unet_tc_pool", ptr(self.a["p1"]), ptr(self.a["e1"]), *d[0], 16, st)
+        self._conv("a2", "p1", "e2a", 1)
+        self._conv("e2", "a2", "e2b", 1)
+        call("bsp_unet_tc_pool", ptr(self.a["p2"]), ptr(self.a["e2"]), *d[1], 32, st)
+        self._conv("a3", "p2", "e3a", 2)
+        self._conv("e3", "a3", "e3b", 2)
+        call("bsp_unet_tc_pool", ptr(self.a["p3"]), ptr(self.a["e3"]), *d[2], 64, st)
+        self._conv("a4", "p3", "bta", 3)
+        self._conv("b4", "a4", "btb", 3)
+        call("bsp_unet_tc_up", ptr(self.a["q3"]), ptr(self.a["b4"]), *d[2], 128, st)
+        self._conv("c3", "q3", "u3a", 2, skip="e3")     # c3 = relu(conv) + e3
+        self._conv("u3", "c3", "u3b", 2)
+        call("bsp_unet_tc_up", ptr(self.a["q2"]), ptr(self.a["u3"]), *d[1], 64, st)
+        self._conv("c2", "q2", "u2a", 1, skip="e2")
+        self._conv("u2", "c2", "u2b", 1)
+        call("bsp_unet_tc_up", ptr(self.a["q1"]), ptr(self.a["u2"]), *d[0], 32, st)
+        self._conv("c1", "q1", "u1a", 0, skip="e1")
+        self._conv("u1", "c1", "u1b", 0)
+        p = out if out is not None else torch.empty(d[0], dtype=torch.float32,
+                                                    device=self.net.device)
+        call("bsp_unet_tc_head", ptr(p), ptr(self.a["u1"]), ptr(self.net.hw), ptr(self.net.hb),
+             ptr(mask), *d[0], ptr(self.s_dev), -(rho * dx * dx / dt), st)
+        return p
+
+
+def coarse_materials(mat_t: torch.Tensor) -> torch.Tensor:
+    """Material grid coarsened 2x (once per geometry): fluid where at least
+    half of the 8 children are fluid, else air where any child is air, else
+    solid -- the free surface stays a Dirichlet boundary on the coarse grid."""
+    nx, ny, nz = mat_t.shape
+    m = mat_t.view(nx // 2, 2, ny // 2, 2, nz // 2, 2)
+    nf = (m == 0).sum(dim=(1, 3, 5))
+    na = (m == 2).sum(dim=(1, 3, 5))
+    return torch.where(nf >= 4, 0, torch.where(na > 0, 2, 1)).to(torch.int32).contiguous()
+
+
+class WarmStart:
+    """The network's starting pressure for one grid.
+
+    ``mode="full"``: the network at the grid's own resolution.  ``"coarse"``:
+    the network on the grid coarsened 2x (divergence averaged over the fluid
+    children, classes by coarse_materials), its pressure interpolated back
+    onto the fine fluid cells (bsp_unet_restrict_div / bsp_unet_prolong) --
+    an eighth of the network's work, for grids large enough that a full-size
+    prediction would cost more than the iterations it saves."""
+
+    def __init__(self, net: UNet, mat_t: torch.Tensor, mask: torch.Tensor, mode: str = "auto"):
+        from .fluid import cell_mask
+
+        self.net = net
+        self.dims = tuple(mat_t.shape)
+        self.mask = mask
+        nx, ny, nz = self.dims
+        if mode == "auto":
+            mode = "coarse" if (nx % 16 == 0 and ny % 16 == 0 and nz % 16 == 0 and
+                                nx * ny * nz >= 16_000_000) else "full"
+        self.mode = mode
+        if mode == "coarse":
+            self.maskc = cell_mask(coarse_materials(mat_t))
+            self.divc = torch.zeros((nx // 2, ny // 2, nz // 2), dtype=torch.float32,
+                                    device=mat_t.device)
+            self.pc = torch.zeros_like(self.divc)
+
+    def guess(self, div, dx, dt, rho, out: torch.Tensor) -> torch.Tensor:
+        nx, ny, nz = self.dims
+        st = stream_handle()
+        if self.mode == "full":
+            return self.net.tc_plan(self.dims).run(div, self.mask, dx, dt, rho, out=out)
+        call("bsp_unet_restrict_div", ptr(self.divc), ptr(self.maskc), ptr(div), ptr(self.mask),
+             nx, ny, nz, st)
+        self.net.tc_plan(tuple(self.divc.shape)).run(self.divc, self.maskc, 2.0 * dx, dt, rho,
+                                                      out=self.pc)
+        call("bsp_unet_prolong", ptr(out), ptr(self.pc), ptr(self.mask), nx, ny, nz, st)
+        return out
 
 
 # ---- training data: the plain solver on seeded pot variants ----------------------------------

@@ -19,7 +19,8 @@ enum ProfClass {
   PROF_MG_COARSE = 7,  // all coarse-level multigrid kernels
   PROF_CONTROL = 8,    // one-block scalar kernels, level setup, conversions
   PROF_PROJ = 9,       // divergence, gradient subtract, no-slip, rhs
-  PROF_NCLASS = 10
+  PROF_UNET = 10,      // learned warm start: network layers, input packing, head
+  PROF_NCLASS = 11
 };
 
 bool prof_enabled();

@@ -1,0 +1,877 @@
+// unet_tc.cu -- inference path of the warm-start U-Net on the fifth-generation
+// tensor cores: tcgen05.mma with the accumulator in tensor memory (TMEM),
+// operand tiles staged in shared memory by TMA (cp.async.bulk.tensor, never
+// with cluster multicast), one elected thread issuing the MMAs, warp-
+// specialised producer / MMA / epilogue roles.
+//
+// Padded activation layout.  A level of interior size (nx, ny, nz) is stored
+// with a one-cell zero halo: row q = ((i+1)(ny+2) + (j+1))(nz+2) + (k+1) for
+// interior cell (i, j, k), act[q][c] BF16, channels innermost.  A 3x3x3 tap
+// (di, dj, dk) is then a constant shift of the row index, so every operand
+// tile of the implicit GEMM is a run of consecutive rows -- one TMA box, no
+// gather, and the zero halo supplies the convolution's zero padding.
+//
+// The GEMM.  A tile is a window of 128 consecutive rows w = 0..127 (rows
+// q0 - 1 + w); it produces outputs q0 + m, m = 0..125.  The three dk taps of
+// each (di, dj) pair are stacked along N: B = [W(dk=-1); W(dk=0); W(dk=+1)]
+// (N = 3 cout), so one MMA per (di, dj) and 16-channel chunk computes
+// D[w][dk block] = sum_ci in(q0 - 1 + w + di P + dj R)[ci] W[di,dj,dk][co][ci]
+// (P = (ny+2)(nz+2), R = nz+2), and the epilogue forms
+// out[m] = D[m][dk=-1] + D[m+1][dk=0] + D[m+2][dk=+1]
+// by exchanging neighbouring TMEM lanes through warp shuffles.  Stacking the
+// dk taps makes N three times larger than cout, so each byte of activation
+// read from shared memory by the tensor core feeds 3x the multiply-adds.
+//
+// Roles (one CTA per SM, persistent over work items = (row tile, cout tile)):
+//   warp 0   TMA producer: per 16-channel chunk, 9 (di, dj) slabs x 2 halves
+//            of 8 channels, each a {8 channels x 128 rows} box, into a ring of
+//            shared-memory stages (full / empty mbarriers); streams the chunk's
+//            weights too when they do not stay resident;
+//   warp 1   TMEM allocator and MMA issuer (one thread): 9 MMAs
+//            (M = 128, N = 3 cout_tile, K = 16) per chunk into one of two TMEM
+//            accumulators, tcgen05.commit to release stages and to hand the
+//            accumulator to the epilogue;
+//   warps 2-5 epilogue: tcgen05.ld of their 32 TMEM lanes, dk combination,
+//            bias, ReLU, optional skip add, BF16 store (halo rows get zeros).
+// Every mbarrier wait is bounded; on a timeout the kernel records
+// BSP_ERR_TIMEOUT in a device flag, drains its outstanding copies and MMAs
+// (bounded), frees its TMEM and returns.
+//
+// Shared-memory operand layout (K-major, no swizzle): a "core matrix" is 8
+// rows x 16 bytes (8 BF16 of K) stored as 128 contiguous bytes.  Each
+// 8-channel half of a slab is 128 rows x 16 B, rows contiguous, so the
+// descriptor uses stride-byte-offset 128 (next 8-row group) and
+// leading-byte-offset = distance between the two K halves.  The weights of a
+// (di, dj, chunk) are laid out the same way: N rows x 16 B per half.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+
+#include "bsp_common.cuh"
+#include "profile.cuh"
+#include "tma.cuh"
+
+namespace bsp {
+namespace utc {
+
+constexpr int M = 128;          // window rows per tile (TMEM lanes)
+constexpr int MOUT = 126;       // outputs per tile
+constexpr int THREADS = 192;    // 6 warps
+constexpr int SLAB_HALF = M * 16;          // bytes of one 8-channel half of a slab
+constexpr int A_STAGE = 9 * 2 * SLAB_HALF; // 36,864 bytes per 16-channel chunk
+constexpr int SMEM_MAX = 232448;           // dynamic shared memory per CTA (227 KB)
+constexpr int SMEM_MIN = 120 * 1024;       // keep one CTA per SM (TMEM is not shared)
+constexpr int WRES_MAX = 112 * 1024;       // weights stay resident up to this size
+
+__device__ int g_utc_err;  // BSP_ERR_TIMEOUT once any wait of this kernel gave up
+
+struct Params {
+  __nv_bfloat16 *out;          // padded output rows x cout
+  const __nv_bfloat16 *wimg;   // weight image (bsp_unet_tc_weights)
+  const float *bias;           // cout or NULL
+  const __nv_bfloat16 *skip;   // padded rows x cout, added after ReLU, or NULL
+  int nx, ny, nz, cin, cout;
+  int ct;        // cout per CTA tile (16, 32 or 64); N = 3 ct
+  int nct;       // cout tiles
+  int relu;
+  int64_t r0;    // first interior row
+  int64_t rows;  // total padded rows
+  int64_t ntiles;
+  int resident;  // weights resident in shared memory
+  int nst;       // A stages
+  int w_bytes_chunk;  // bytes of one chunk's weights (9 x 2 x N x 16)
+};
+
+// ---- PTX wrappers --------------------------------------------------------------------
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_shared() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void tma_load2(void *dst, const CUtensorMap *map, int x, int y,
+                                          uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+// 1-D bulk copy global -> shared (no multicast); size a multiple of 16
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes,
+                                          uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+          "r"(smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_mma(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                       uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+// 16 consecutive TMEM columns of this thread's lane from each of three column
+// offsets, then wait::ld -- in one asm statement, so no use of the registers
+// can be scheduled before the wait.
+__device__ __forceinline__ void tmem_ld3x16(uint32_t a0, uint32_t a1, uint32_t a2,
+                                           float (&x0)[16], float (&x1)[16], float (&x2)[16]) {
+  uint32_t r[48];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%48];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16, %17, %18, %19, %20, %21, %22, %23, %24, "
+      "%25, %26, %27, %28, %29, %30, %31}, [%49];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%32, %33, %34, %35, %36, %37, %38, %39, %40, "
+      "%41, %42, %43, %44, %45, %46, %47}, [%50];\n"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]),
+        "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]),
+        "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47])
+      : "r"(a0), "r"(a1), "r"(a2)
+      : "memory");
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    x0[q] = __uint_as_float(r[q]);
+    x1[q] = __uint_as_float(r[16 + q]);
+    x2[q] = __uint_as_float(r[32 + q]);
+  }
+}
+__device__ __forceinline__ void named_sync(int id, int n) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+// Shared-memory matrix descriptor, K-major, no swizzle (layout type 0),
+// descriptor version 1: start >> 4 in bits 0-13, leading-byte-offset >> 4 in
+// 16-29, stride-byte-offset >> 4 in 32-45, version in 46-47.
+__device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
+}
+// Instruction descriptor of kind::f16: FP32 accumulate (bits 4-5 = 1), BF16
+// A and B (bits 7-9, 10-12 = 1), both K-major, N >> 3 in bits 17-22,
+// M >> 4 in bits 24-28.
+__host__ __device__ constexpr uint32_t idesc_bf16(int n, int m) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) |
+         ((uint32_t)(m >> 4) << 24);
+}
+
+struct Ctl {
+  uint64_t full[8], empty[8], acc_full[2], acc_empty[2], wbar, drain;
+  uint32_t tmem_base;
+  int abort;
+  int ep_ok[2];       // accumulator-ready vote of the epilogue, per work-item parity
+  float xch0[4][16];  // lane-31 dk=-1 block of each epilogue quarter (one channel block)
+  float xch2[4][16];  // lane-0 dk=+1 block
+};
+
+__device__ __forceinline__ bool wait_or_abort(uint64_t *bar, uint32_t parity, Ctl *c) {
+  if (mbar_wait(bar, parity)) return true;
+  *(volatile int *)&c->abort = 1;
+  atomicExch(&g_utc_err, BSP_ERR_TIMEOUT);
+  return false;
+}
+
+__global__ void __launch_bounds__(THREADS, 1) conv_tc_kernel(
+    const __grid_constant__ CUtensorMap amap, const Params p) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int N = 3 * p.ct;
+  const int ncol = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
+  const int nchunk = p.cin >> 4;
+  const int wchunk = p.w_bytes_chunk;
+  // layout: [weights (resident: all chunks; else none)] [stages] [Ctl]
+  unsigned char *wres = smem;
+  const int wres_bytes = p.resident ? wchunk * nchunk : 0;
+  const int stage_bytes = A_STAGE + (p.resident ? 0 : wchunk);
+  unsigned char *stages = smem + wres_bytes;
+  Ctl *c = reinterpret_cast<Ctl *>(stages + (size_t)p.nst * stage_bytes);
+  const int64_t nwork = p.ntiles * p.nct;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < p.nst; ++s) {
+      mbar_init(&c->full[s], 1);
+      mbar_init(&c->empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&c->acc_full[b], 1);
+      mbar_init(&c->acc_empty[b], 4);
+    }
+    mbar_init(&c->wbar, 1);
+    mbar_init(&c->drain, 1);
+    c->abort = 0;
+    fence_barrier_init();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(&c->tmem_base)),
+                 "r"(2 * ncol)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_async_shared();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tbase = c->tmem_base;
+  const int64_t R = p.nz + 2, P = (int64_t)(p.ny + 2) * R;
+
+  if (warp == 0) {
+    // ---------------- producer ----------------
+    if (lane == 0) {
+      if (p.resident) {
+        const uint32_t total = (uint32_t)wres_bytes;
+        mbar_expect_tx(&c->wbar, total);
+        for (uint32_t off = 0; off < total; off += 16384) {
+          const uint32_t nb = total - off < 16384 ? total - off : 16384;
+          bulk_load(wres + off, reinterpret_cast<const unsigned char *>(p.wimg) + off, nb,
+                    &c->wbar);
+        }
+      }
+      int64_t it = 0;  // stage fills issued
+      for (int64_t wk = blockIdx.x; wk < nwork && !*(volatile int *)&c->abort;
+           wk += gridDim.x) {
+        const int64_t t = wk / p.nct;
+        const int ctile = (int)(wk - t * p.nct);
+        const int64_t base = p.r0 + t * MOUT - 1;
+        for (int kc = 0; kc < nchunk; ++kc, ++it) {
+          const int s = (int)(it % p.nst);
+          const uint32_t ph = (uint32_t)((it / p.nst) & 1);
+          if (!wait_or_abort(&c->empty[s], ph ^ 1u, c)) break;
+          unsigned char *st = stages + (size_t)s * stage_bytes;
+          mbar_expect_tx(&c->full[s], (uint32_t)stage_bytes);
+#pragma unroll 1
+          for (int sl = 0; sl < 9; ++sl) {
+            const int di = sl / 3 - 1, dj = sl % 3 - 1;
+            const int y = (int)(base + di * P + dj * R);
+            tma_load2(st + (sl * 2 + 0) * SLAB_HALF, &amap, kc * 16, y, &c->full[s]);
+            tma_load2(st + (sl * 2 + 1) * SLAB_HALF, &amap, kc * 16 + 8, y, &c->full[s]);
+          }
+          if (!p.resident)
+            bulk_load(st + A_STAGE,
+                      reinterpret_cast<const unsigned char *>(p.wimg) +
+                          ((size_t)ctile * nchunk + kc) * wchunk,
+                      (uint32_t)wchunk, &c->full[s]);
+        }
+        if (*(volatile int *)&c->abort) break;
+      }
+      // drain: every fill issued has landed (or the wait gives up)
+      if (*(volatile int *)&c->abort && it > 0) {
+        for (int64_t q = it > p.nst ? it - p.nst : 0; q < it; ++q)
+          mbar_wait(&c->full[q % p.nst], (uint32_t)((q / p.nst) & 1));
+      }
+    }
+  } else if (warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16(N, M);
+      bool ok = true;
+      if (p.resident) ok = wait_or_abort(&c->wbar, 0, c);
+      int64_t it = 0, li = 0;
+      for (int64_t wk = blockIdx.x; ok && wk < nwork; wk += gridDim.x, ++li) {
+        const int b = (int)(li & 1);
+        if (!wait_or_abort(&c->acc_empty[b], (uint32_t)(((li >> 1) & 1) ^ 1), c)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t dt = tbase + (uint32_t)(b * ncol);
+        for (int kc = 0; kc < nchunk; ++kc, ++it) {
+          const int s = (int)(it % p.nst);
+          if (!wait_or_abort(&c->full[s], (uint32_t)((it / p.nst) & 1), c)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          unsigned char *st = stages + (size_t)s * stage_bytes;
+          const unsigned char *wb = p.resident ? wres + (size_t)kc * wchunk : st + A_STAGE;
+          const uint32_t abase = smem_u32(st), bbase = smem_u32(wb);
+#pragma unroll 1
+          for (int sl = 0; sl < 9; ++sl) {
+            const uint64_t ad = sdesc(abase + sl * 2 * SLAB_HALF, SLAB_HALF, 128);
+            const uint64_t bd = sdesc(bbase + sl * 2 * N * 16, N * 16, 128);
+            tc_mma(dt, ad, bd, idesc, (kc > 0 || sl > 0) ? 1u : 0u);
+          }
+          tc_commit(&c->empty[s]);  // stage free once these MMAs have read it
+        }
+        if (!ok) break;
+        tc_commit(&c->acc_full[b]);  // accumulator complete
+      }
+      // drain: every MMA issued has completed before TMEM is freed
+      tc_commit(&c->drain);
+      mbar_wait(&c->drain, 0);
+    }
+  } else {
+    // ---------------- epilogue (warps 2..5) ----------------
+    const int qd = warp & 3;                 // TMEM lane quarter of this warp
+    const int w = qd * 32 + lane;            // window row
+    const int m = w - 1;                     // output of this thread
+    const int64_t rowsz = p.ny + 2;
+    int64_t li = 0;
+    for (int64_t wk = blockIdx.x; wk < nwork; wk += gridDim.x, ++li) {
+      const int b = (int)(li & 1);
+      // one thread waits (bounded) and the 128 epilogue threads take its
+      // answer through the named barrier, so they all leave together
+      if (threadIdx.x == 64)
+        c->ep_ok[b] = wait_or_abort(&c->acc_full[b], (uint32_t)((li >> 1) & 1), c) ? 1 : 0;
+      named_sync(1, 128);
+      if (!*(volatile int *)&c->ep_ok[b]) break;
+      tc_fence_after();
+      const int64_t t = wk / p.nct;
+      const int ctile = (int)(wk - t * p.nct);
+      const int64_t q = p.r0 + t * MOUT + m;
+      bool valid = m >= 0 && m < MOUT && q < p.rows;
+      bool interior = false;
+      if (valid) {
+        const int64_t k = q % R, r2 = q / R;
+        const int64_t j = r2 % rowsz, i = r2 / rowsz;
+        interior = k >= 1 && k <= p.nz && j >= 1 && j <= p.ny && i >= 1 && i <= p.nx;
+      }
+      const uint32_t trow = tbase + ((uint32_t)(qd * 32) << 16) + (uint32_t)(b * ncol);
+      for (int cb = 0; cb < p.ct; cb += 16) {
+        float x0[16], x1[16], x2[16];
+        tmem_ld3x16(trow + (uint32_t)(0 * p.ct + cb), trow + (uint32_t)(1 * p.ct + cb),
+                    trow + (uint32_t)(2 * p.ct + cb), x0, x1, x2);
+        if (lane == 31)
+          for (int e = 0; e < 16; ++e) c->xch0[qd][e] = x0[e];
+        if (lane == 0)
+          for (int e = 0; e < 16; ++e) c->xch2[qd][e] = x2[e];
+        named_sync(1, 128);
+        float v[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+          float up = __shfl_up_sync(0xffffffffu, x0[e], 1);     // D[w-1][dk=-1]
+          float dn = __shfl_down_sync(0xffffffffu, x2[e], 1);   // D[w+1][dk=+1]
+          if (lane == 0) up = qd > 0 ? c->xch0[qd - 1][e] : 0.0f;
+          if (lane == 31) dn = qd < 3 ? c->xch2[qd + 1][e] : 0.0f;
+          v[e] = (up + x1[e]) + dn;
+        }
+        named_sync(1, 128);  // the exchange slots are reused by the next block
+        if (valid) {
+          const int co0 = ctile * p.ct + cb;
+          __nv_bfloat16 *dst = p.out + q * p.cout + co0;
+          uint4 pk[2];
+          __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(pk);
+          if (interior) {
+            float y[16];
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+              float a = v[e] + (p.bias ? __ldg(p.bias + co0 + e) : 0.0f);
+              if (p.relu) a = fmaxf(a, 0.0f);
+              y[e] = a;
+            }
+            if (p.skip) {
+              const uint4 *sk = reinterpret_cast<const uint4 *>(p.skip + q * p.cout + co0);
+              uint4 s4[2] = {__ldg(sk), __ldg(sk + 1)};
+              const __nv_bfloat16 *sv = reinterpret_cast<const __nv_bfloat16 *>(s4);
+#pragma unroll
+              for (int e = 0; e < 16; ++e)
+                y[e] = __bfloat162float(__float2bfloat16(y[e])) + __bfloat162float(sv[e]);
+            }
+#pragma unroll
+            for (int e = 0; e < 8; ++e) h[e] = __floats2bfloat162_rn(y[2 * e], y[2 * e + 1]);
+          } else {
+            pk[0] = make_uint4(0, 0, 0, 0);
+            pk[1] = make_uint4(0, 0, 0, 0);
+          }
+          reinterpret_cast<uint4 *>(dst)[0] = pk[0];
+          reinterpret_cast<uint4 *>(dst)[1] = pk[1];
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&c->acc_empty[b]);
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 1)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase),
+                 "r"(2 * ncol)
+                 : "memory");
+}
+
+// ---- weight image ---------------------------------------------------------------------
+// wimg[ct][kc][s][h][n][8], n = dki * CT + col (dki 0..2 for dk = -1, 0, +1),
+// co = ct * CT + col, ci = 16 kc + 8 h + e; from w[tap][co][ci] with
+// tap = (di+1) 9 + (dj+1) 3 + (dk+1) and s = (di+1) 3 + (dj+1).
+__global__ void weight_image_kernel(__nv_bfloat16 *__restrict__ wimg,
+                                    const __nv_bfloat16 *__restrict__ w, int cin, int cout,
+                                    int CT) {
+  const int64_t total = 27LL * cin * cout;
+  const int N = 3 * CT;
+  const int nchunk = cin / 16;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    int64_t r = q;
+    const int e = (int)(r % 8);
+    r /= 8;
+    const int n = (int)(r % N);
+    r /= N;
+    const int h = (int)(r % 2);
+    r /= 2;
+    const int s = (int)(r % 9);
+    r /= 9;
+    const int kc = (int)(r % nchunk);
+    const int ct = (int)(r / nchunk);
+    const int dki = n / CT, col = n % CT;
+    const int co = ct * CT + col, ci = 16 * kc + 8 * h + e;
+    const int tap = (s / 3) * 9 + (s % 3) * 3 + dki;
+    wimg[q] = w[((int64_t)tap * cout + co) * cin + ci];
+  }
+}
+
+// ---- padded-layout helpers (pack, pool, upsample, head) --------------------------------------
+__device__ __forceinline__ bool unpad(int64_t q, int nx, int ny, int nz, int &i, int &j, int &k) {
+  const int64_t R = nz + 2;
+  const int64_t kk = q % R, r2 = q / R;
+  const int64_t jj = r2 % (ny + 2), ii = r2 / (ny + 2);
+  i = (int)ii - 1;
+  j = (int)jj - 1;
+  k = (int)kk - 1;
+  return i >= 0 && i < nx && j >= 0 && j < ny && k >= 0 && k < nz;
+}
+__device__ __forceinline__ int64_t padrow(int i, int j, int k, int ny, int nz) {
+  return ((int64_t)(i + 1) * (ny + 2) + (j + 1)) * (nz + 2) + (k + 1);
+}
+
+// x[q][0] = div / s on fluid, x[q][1] = fluid flag, x[q][2] = solid flag, other
+// channels and halo rows 0 (16 channels).
+__global__ void pack_pad_kernel(__nv_bfloat16 *__restrict__ x, const float *__restrict__ div,
+                                const uint8_t *__restrict__ mask, int nx, int ny, int nz,
+                                const float *__restrict__ s_dev, int64_t rows) {
+  const float inv_scale = 1.0f / s_dev[0];
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < rows;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    int i, j, k;
+    uint4 v[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+    if (unpad(q, nx, ny, nz, i, j, k)) {
+      const int64_t c = ((int64_t)i * ny + j) * nz + k;
+      const uint8_t m = mask[c];
+      const bool fl = (m & BSP_CLASS_FLUID) != 0;
+      __nv_bfloat16 *h = reinterpret_cast<__nv_bfloat16 *>(v);
+      h[0] = __float2bfloat16(fl ? div[c] * inv_scale : 0.0f);
+      h[1] = __float2bfloat16(fl ? 1.0f : 0.0f);
+      h[2] = __float2bfloat16((m & BSP_CLASS_SOLID) ? 1.0f : 0.0f);
+    }
+    uint4 *o = reinterpret_cast<uint4 *>(x + q * 16);
+    o[0] = v[0];
+    o[1] = v[1];
+  }
+}
+
+// 2x2x2 average of the fine level (nx, ny, nz) into the coarse padded level;
+// 8 channels per thread.  Halo rows of the output get zeros.
+__global__ void pool_pad_kernel(__nv_bfloat16 *__restrict__ out,
+                                const __nv_bfloat16 *__restrict__ in, int nx, int ny, int nz,
+                                int c) {
+  const int ox = nx / 2, oy = ny / 2, oz = nz / 2;
+  const int g = c / 8;
+  const int64_t rows = (int64_t)(ox + 2) * (oy + 2) * (oz + 2);
+  for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < rows * g;
+       u += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t q = u / g;
+    const int cg = (int)(u - q * g);
+    int i, j, k;
+    float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const bool in_ = unpad(q, ox, oy, oz, i, j, k);
+    if (in_) {
+      for (int a = 0; a < 8; ++a) {
+        const int64_t qf = padrow(2 * i + (a >> 2), 2 * j + ((a >> 1) & 1), 2 * k + (a & 1), ny, nz);
+        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(in + qf * c) + cg);
+        const __nv_bfloat16 *h = reinterpret_cast<const __nv_bfloat16 *>(&v);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) s[e] += __bfloat162float(h[e]);
+      }
+    }
+    uint4 o;
+    __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(&o);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) h[e] = __floats2bfloat162_rn(0.125f * s[2 * e], 0.125f * s[2 * e + 1]);
+    reinterpret_cast<uint4 *>(out + q * c)[cg] = o;
+  }
+}
+
+// nearest x2 upsampling of the coarse padded level onto the fine padded level
+// (nx, ny, nz); halo rows get zeros.
+__global__ void up_pad_kernel(__nv_bfloat16 *__restrict__ out, const __nv_bfloat16 *__restrict__ in,
+                              int nx, int ny, int nz, int c) {
+  const int g = c / 8;
+  const int64_t rows = (int64_t)(nx + 2) * (ny + 2) * (nz + 2);
+  for (int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; u < rows * g;
+       u += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t q = u / g;
+    const int cg = (int)(u - q * g);
+    int i, j, k;
+    uint4 v = make_uint4(0, 0, 0, 0);
+    if (unpad(q, nx, ny, nz, i, j, k))
+      v = __ldg(reinterpret_cast<const uint4 *>(in + padrow(i >> 1, j >> 1, k >> 1, ny / 2,
+                                                             nz / 2) * c) + cg);
+    reinterpret_cast<uint4 *>(out + q * c)[cg] = v;
+  }
+}
+
+// p[v] = scale (hb + hw . x[q]) on fluid cells, 0 elsewhere (unpadded FP32 out).
+__global__ void head_pad_kernel(float *__restrict__ p, const __nv_bfloat16 *__restrict__ x,
+                                const float *__restrict__ hw, const float *__restrict__ hb,
+                                const uint8_t *__restrict__ mask, int nx, int ny, int nz,
+                                const float *__restrict__ s_dev, float factor) {
+  const float scale = factor * s_dev[0];
+  const int64_t n = (int64_t)nx * ny * nz;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(v % nz);
+    const int64_t r = v / nz;
+    const int j = (int)(r % ny), i = (int)(r / ny);
+    const uint4 *xr = reinterpret_cast<const uint4 *>(x + padrow(i, j, k, ny, nz) * 16);
+    const uint4 a = __ldg(xr), b = __ldg(xr + 1);
+    const __nv_bfloat16 *h0 = reinterpret_cast<const __nv_bfloat16 *>(&a);
+    const __nv_bfloat16 *h1 = reinterpret_cast<const __nv_bfloat16 *>(&b);
+    float y = hb[0];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) y = fmaf(hw[e], __bfloat162float(h0[e]), y);
+#pragma unroll
+    for (int e = 0; e < 8; ++e) y = fmaf(hw[8 + e], __bfloat162float(h1[e]), y);
+    p[v] = (mask[v] & BSP_CLASS_FLUID) ? scale * y : 0.0f;
+  }
+}
+
+// Divergence of the grid coarsened 2x in each direction: the mean over the
+// fluid children of a coarse fluid cell (mask_c marks the coarse classes);
+// 0 elsewhere.  (nx, ny, nz) is the fine size (even).
+__global__ void restrict_div_kernel(float *__restrict__ divc, const uint8_t *__restrict__ maskc,
+                                    const float *__restrict__ div,
+                                    const uint8_t *__restrict__ mask, int nx, int ny, int nz) {
+  const int ox = nx / 2, oy = ny / 2, oz = nz / 2;
+  const int64_t n = (int64_t)ox * oy * oz;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const int k = (int)(v % oz);
+    const int64_t r = v / oz;
+    const int j = (int)(r % oy), i = (int)(r / oy);
+    float s = 0.0f;
+    int cnt = 0;
+    for (int a = 0; a < 8; ++a) {
+      const int64_t c = ((int64_t)(2 * i + (a >> 2)) * ny + 2 * j + ((a >> 1) & 1)) * nz + 2 * k +
+                        (a & 1);
+      if (mask[c] & BSP_CLASS_FLUID) {
+        s += div[c];
+        ++cnt;
+      }
+    }
+    divc[v] = ((maskc[v] & BSP_CLASS_FLUID) && cnt) ? s / (float)cnt : 0.0f;
+  }
+}
+
+// Trilinear interpolation of a cell-centred coarse field (nx/2, ny/2, nz/2)
+// onto the fine cells (half-cell offsets, edge values held), on fluid cells
+// only; 0 elsewhere.
+__device__ __forceinline__ void lin2(int d, int nc, int &a, int &b, float &wa) {
+  // fine index d -> coarse position d/2 - 1/4, clamped to [0, nc - 1]
+  if (d & 1) {
+    a = d >> 1;
+    b = min(a + 1, nc - 1);
+    wa = 0.75f;
+  } else {
+    b = d >> 1;
+    a = max(b - 1, 0);
+    wa = 0.25f;
+  }
+}
+__global__ void prolong_kernel(float *__restrict__ p, const float *__restrict__ pc,
+                               const uint8_t *__restrict__ mask, int nx, int ny, int nz) {
+  const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
+  const int64_t n = (int64_t)nx * ny * nz;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    if (!(mask[v] & BSP_CLASS_FLUID)) {
+      p[v] = 0.0f;
+      continue;
+    }
+    const int k = (int)(v % nz);
+    const int64_t r = v / nz;
+    const int j = (int)(r % ny), i = (int)(r / ny);
+    int i0, i1, j0, j1, k0, k1;
+    float wi, wj, wk;
+    lin2(i, cx, i0, i1, wi);
+    lin2(j, cy, j0, j1, wj);
+    lin2(k, cz, k0, k1, wk);
+    auto at = [&](int a, int b, int c) { return __ldg(pc + ((int64_t)a * cy + b) * cz + c); };
+    const float c00 = wk * at(i0, j0, k0) + (1.0f - wk) * at(i0, j0, k1);
+    const float c01 = wk * at(i0, j1, k0) + (1.0f - wk) * at(i0, j1, k1);
+    const float c10 = wk * at(i1, j0, k0) + (1.0f - wk) * at(i1, j0, k1);
+    const float c11 = wk * at(i1, j1, k0) + (1.0f - wk) * at(i1, j1, k1);
+    const float c0 = wj * c00 + (1.0f - wj) * c01, c1 = wj * c10 + (1.0f - wj) * c11;
+    p[v] = wi * c0 + (1.0f - wi) * c1;
+  }
+}
+
+// s = RMS of div over the fluid cells (1 when there is none or it is 0): the
+// network's input scale, on the device.  Per-block FP64 partials of
+// (sum div^2, count) in a fixed order, then one block sums them in order.
+constexpr int RMS_BLOCKS = 592;
+__global__ void __launch_bounds__(256) rms_partial_kernel(double *__restrict__ part,
+                                                          const float *__restrict__ div,
+                                                          const uint8_t *__restrict__ mask,
+                                                          int64_t n) {
+  __shared__ double sh[2][8];
+  double a = 0.0, c = 0.0;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (int64_t)gridDim.x * blockDim.x)
+    if (mask[v] & BSP_CLASS_FLUID) {
+      const double d = div[v];
+      a += d * d;
+      c += 1.0;
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = a;
+    sh[1][threadIdx.x >> 5] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sa = 0.0, sc = 0.0;
+    for (int w = 0; w < 8; ++w) {
+      sa += sh[0][w];
+      sc += sh[1][w];
+    }
+    part[2 * blockIdx.x] = sa;
+    part[2 * blockIdx.x + 1] = sc;
+  }
+}
+__global__ void rms_final_kernel(float *__restrict__ s_out, const double *__restrict__ part,
+                                 int nb) {
+  double a = 0.0, c = 0.0;
+  for (int b = 0; b < nb; ++b) {
+    a += part[2 * b];
+    c += part[2 * b + 1];
+  }
+  const double r = c > 0.0 ? sqrt(a / c) : 0.0;
+  s_out[0] = r > 0.0 ? (float)r : 1.0f;
+}
+
+inline int grid_for(int64_t n, int threads = 256) {
+  int64_t b = (n + threads - 1) / threads;
+  return (int)(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16);
+}
+
+static bool encode_rows(CUtensorMap *m, const void *base, int c, int64_t rows) {
+  auto fn = encode_tiled();
+  if (!fn || ((uintptr_t)base & 15u)) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)c, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {(cuuint64_t)c * 2};
+  const cuuint32_t box[2] = {8, (cuuint32_t)M};
+  const cuuint32_t es[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box,
+            es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int cout_tile(int cout) { return cout % 64 == 0 ? 64 : (cout % 32 == 0 ? 32 : 16); }
+
+int num_sms_dev() {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms > 0 ? sms : 148;
+}
+
+}  // namespace utc
+}  // namespace bsp
+
+using namespace bsp;
+using namespace bsp::utc;
+
+extern "C" int64_t bsp_unet_tc_rows(int nx, int ny, int nz) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return 0;
+  return (int64_t)(nx + 2) * (ny + 2) * (nz + 2);
+}
+
+extern "C" int bsp_unet_tc_weights(bsp_bf16_t *wimg, const bsp_bf16_t *w, int cin, int cout,
+                                   cudaStream_t s) {
+  if (!wimg || !w) return BSP_ERR_NULL;
+  if (cin <= 0 || cin % 16 || cout <= 0 || cout % 16) return BSP_ERR_SHAPE;
+  ProfScope ps(PROF_UNET, s);
+  weight_image_kernel<<<grid_for(27LL * cin * cout), 256, 0, s>>>(
+      reinterpret_cast<__nv_bfloat16 *>(wimg), reinterpret_cast<const __nv_bfloat16 *>(w), cin,
+      cout, cout_tile(cout));
+  return (int)cudaGetLastError();
+}
+
+extern "C" int bsp_unet_tc_conv3(bsp_bf16_t *out, const bsp_bf16_t *in, const bsp_bf16_t *wimg,
+                                 const float *bias, const bsp_bf16_t *skip, int nx, int ny, int nz,
+                                 int cin, int cout, int relu, cudaStream_t s) {
+  if (nx <= 0 || ny <= 0 || nz <= 0) return BSP_OK;
+  if (!out || !in || !wimg) return BSP_ERR_NULL;
+  if (cin <= 0 || cin % 16 || cout <= 0 || cout % 16 || cin > 1024) return BSP_ERR_SHAPE;
+  if (((uintptr_t)in & 15u) || ((uintptr_t)out & 15u) || ((uintptr_t)wimg & 15u) ||
+      ((uintptr_t)skip & 15u))
+    return BSP_ERR_ALIGN;
+  if ((const void *)out == (const void *)in || (skip && (const void *)skip == (const void *)out))
+    return BSP_ERR_ALIAS;
+  const int64_t rows = bsp_unet_tc_rows(nx, ny, nz);
+  if (rows >= ((int64_t)1 << 31)) return BSP_ERR_SHAPE;  // TMA row coordinates are 32-bit
+  Params p{};
+  p.out = reinterpret_cast<__nv_bfloat16 *>(out);
+  p.wimg = reinterpret_cast<const __nv_bfloat16 *>(wimg);
+  p.bias = bias;
+  p.skip = reinterpret_cast<const __nv_bfloat16 *>(skip);
+  p.nx = nx;
+  p.ny = ny;
+  p.nz = nz;
+  p.cin = cin;
+  p.cout = cout;
+  p.ct = cout_tile(cout);
+  p.nct = cout / p.ct;
+  p.relu = relu;
+  const int64_t R = nz + 2, P = (int64_t)(ny + 2) * R;
+  p.r0 = P + R + 1;
+  const int64_t rlast = (int64_t)nx * P + ny * R + nz;
+  p.rows = rows;
+  p.ntiles = (rlast - p.r0 + MOUT) / MOUT;
+  const int N = 3 * p.ct;
+  p.w_bytes_chunk = 9 * 2 * N * 16;
+  const int nchunk = cin / 16;
+  const int wtotal = p.w_bytes_chunk * nchunk;
+  const int ctl = (int)((sizeof(Ctl) + 127) / 128 * 128);
+  p.resident = (p.nct == 1 && wtotal <= WRES_MAX) ? 1 : 0;
+  const int stage = A_STAGE + (p.resident ? 0 : p.w_bytes_chunk);
+  const int avail = SMEM_MAX - ctl - (p.resident ? wtotal : 0);
+  p.nst = avail / stage;
+  if (p.nst > 8) p.nst = 8;
+  if (p.nst < 2) return BSP_ERR_SHAPE;
+  int bytes = (p.resident ? wtotal : 0) + p.nst * stage + ctl;
+  if (bytes < SMEM_MIN) bytes = SMEM_MIN;
+  CUtensorMap amap;
+  if (!encode_rows(&amap, in, cin, rows)) return BSP_ERR_ARG;
+  if (!smem_opt_in((const void *)conv_tc_kernel, SMEM_MAX)) return BSP_ERR_ARG;
+  const int64_t work = p.ntiles * p.nct;
+  const int grid = (int)(work < num_sms_dev() ? work : num_sms_dev());
+  ProfScope ps(PROF_UNET, s);
+  conv_tc_kernel<<<grid, THREADS, bytes, s>>>(amap, p);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int bsp_unet_tc_error(int *flag_host) {
+  if (!flag_host) return BSP_ERR_NULL;
+  int v = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&v, g_utc_err, sizeof(int));
+  if (e == cudaSuccess) {
+    const int zero = 0;
+    e = cudaMemcpyToSymbol(g_utc_err, &zero, sizeof(int));
+  }
+  *flag_host = v;
+  return (int)e;
+}
+
+extern "C" size_t bsp_unet_scale_workspace_bytes(void) {
+  return sizeof(double) * 2 * RMS_BLOCKS;
+}
+
+extern "C" int bsp_unet_input_scale(float *s_dev, const float *div, const uint8_t *mask, int nx,
+                                    int ny, int nz, void *workspace, size_t workspace_bytes,
+                                    cudaStream_t s) {
+  if (!s_dev || !div || !mask || !workspace) return BSP_ERR_NULL;
+  if (workspace_bytes < bsp_unet_scale_workspace_bytes() || ((uintptr_t)workspace & 7u))
+    return BSP_ERR_WORKSPACE;
+  ProfScope ps(PROF_UNET, s);
+  rms_partial_kernel<<<RMS_BLOCKS, 256, 0, s>>>(static_cast<double *>(workspace), div, mask,
+                                                (int64_t)nx * ny * nz);
+  rms_final_kernel<<<1, 1, 0, s>>>(s_dev, static_cast<const double *>(workspace), RMS_BLOCKS);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int bsp_unet_tc_pack(bsp_bf16_t *x, const float *div, const uint8_t *mask, int nx,
+                                int ny, int nz, const float *s_dev, cudaStream_t s) {
+  if (!x || !div || !mask || !s_dev) return BSP_ERR_NULL;
+  const int64_t rows = bsp_unet_tc_rows(nx, ny, nz);
+  ProfScope ps(PROF_UNET, s);
+  pack_pad_kernel<<<grid_for(rows), 256, 0, s>>>(reinterpret_cast<__nv_bfloat16 *>(x), div, mask,
+                                                 nx, ny, nz, s_dev, rows);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int bsp_unet_tc_pool(bsp_bf16_t *out, const bsp_bf16_t *in, int nx, int ny, int nz,
+                                int c, cudaStream_t s) {
+  if (!out || !in) return BSP_ERR_NULL;
+  if (nx % 2 || ny % 2 || nz % 2 || c % 8) return BSP_ERR_SHAPE;
+  const int64_t rows = bsp_unet_tc_rows(nx / 2, ny / 2, nz / 2);
+  ProfScope ps(PROF_UNET, s);
+  pool_pad_kernel<<<grid_for(rows * (c / 8)), 256, 0, s>>>(
+      reinterpret_cast<__nv_bfloat16 *>(out), reinterpret_cast<const __nv_bfloat16 *>(in), nx,
+      ny, nz, c);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int bsp_unet_tc_up(bsp_bf16_t *out, const bsp_bf16_t *in, int nx, int ny, int nz,
+                              int c, cudaStream_t s) {
+  if (!out || !in) return BSP_ERR_NULL;
+  if (nx % 2 || ny % 2 || nz % 2 || c % 8) return BSP_ERR_SHAPE;
+  const int64_t rows = bsp_unet_tc_rows(nx, ny, nz);
+  ProfScope ps(PROF_UNET, s);
+  up_pad_kernel<<<grid_for(rows * (c / 8)), 256, 0, s>>>(
+      reinterpret_cast<__nv_bfloat16 *>(out), reinterpret_cast<const __nv_bfloat16 *>(in), nx,
+      ny, nz, c);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int bsp_unet_tc_head(float *p, const bsp_bf16_t *x, const float *hw, const float *hb,
+                                const uint8_t *mask, int nx, int ny, int nz, const float *s_dev,
+                                float factor, cudaStream_t s) {
+  if (!p || !x || !hw || !hb || !mask || !s_dev) return BSP_ERR_NULL;
+  ProfScope ps(PROF_UNET, s);
+  head_pad_kernel<<<grid_for((int64_t)nx * ny * nz), 256, 0, s>>>(
+      p, reinterpret_cast<const __nv_bfloat16 *>(x), hw, hb, mask, nx, ny, nz, s_dev, factor);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int bsp_unet_restrict_div(float *divc, const uint8_t *maskc, const float *div,
+                                     const uint8_t *mask, int nx, int ny, int nz,
+                                     cudaStream_t s) {
+  if (!divc || !maskc || !div || !mask) return BSP_ERR_NULL;
+  if (nx % 2 || ny % 2 || nz % 2 || nx <= 0 || ny <= 0 || nz <= 0) return BSP_ERR_SHAPE;
+  ProfScope ps(PROF_UNET, s);
+  restrict_div_kernel<<<grid_for((int64_t)nx * ny * nz / 8), 256, 0, s>>>(divc, maskc, div, mask,
+                                                                            nx, ny, nz);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int bsp_unet_prolong(float *p, const float *pc, const uint8_t *mask, int nx, int ny,
+                                int nz, cudaStream_t s) {
+  if (!p || !pc || !mask) return BSP_ERR_NULL;
+  if (nx % 2 || ny % 2 || nz % 2 || nx <= 0 || ny <= 0 || nz <= 0) return BSP_ERR_SHAPE;
+  if ((const void *)p == (const void *)pc) return BSP_ERR_ALIAS;
+  ProfScope ps(PROF_UNET, s);
+  prolong_kernel<<<grid_for((int64_t)nx * ny * nz), 256, 0, s>>>(p, pc, mask, nx, ny, nz);
+  return (int)cudaGetLastError();
+}

@@ -189,11 +189,12 @@ int bsp_set_tuning(int key, int value);
  * 0 sweep, 1 restriction from the fine level, 2 prolongation onto the fine
  * level, 3 search direction + A ps, 4 CG vector update, 5 FP64 residual,
  * 6 FP64 iterate update, 7 coarse multigrid levels, 8 control / setup
- * kernels, 9 divergence / gradient / no-slip / rhs.
+ * kernels, 9 divergence / gradient / no-slip / rhs, 10 learned warm start
+ * (network layers on the tensor cores, input packing, head).
  * bsp_profile_read waits for the recorded launches, writes the summed
  * milliseconds and launch counts of classes 0..nclass-1 and clears the
  * record. */
-#define BSP_PROF_NCLASS 10
+#define BSP_PROF_NCLASS 11
 int bsp_profile_enable(int on);
 int bsp_profile_read(double *ms, long long *launches, int nclass);
 
@@ -534,6 +535,60 @@ int bsp_unet_adam(float *w, bsp_bf16_t *wb, float *m, float *v, const float *g, 
  * for the barrier's control words (zeroed here).  The context stays usable.
  * No reference counterpart (the reference has no bounded waits). */
 int bsp_selftest_waits(int *codes_dev, void *scratch_dev, cudaStream_t stream);
+
+/* ---- learned warm start: inference on the fifth-generation tensor cores -----
+ * The same network run by tcgen05.mma kernels (accumulators in tensor memory,
+ * operands staged by TMA) on a padded layout: a level of interior size
+ * (nx, ny, nz) is stored as bsp_unet_tc_rows(nx, ny, nz) rows x c channels
+ * (BF16), row ((i+1)(ny+2) + (j+1))(nz+2) + (k+1) for cell (i, j, k), with a
+ * one-cell halo of zeros that supplies the convolutions' zero padding.
+ * Buffers must start zero-filled (the first and last halo planes are never
+ * written) and 16-byte aligned.  No reference counterpart. */
+int64_t bsp_unet_tc_rows(int nx, int ny, int nz);
+/* Weight image of one layer for bsp_unet_tc_conv3 from w[27][cout][cin]
+ * (the layout of bsp_unet_conv3_fwd); 27 cin cout BF16, rebuilt whenever the
+ * weights change. */
+int bsp_unet_tc_weights(bsp_bf16_t *wimg, const bsp_bf16_t *w, int cin, int cout,
+                        cudaStream_t stream);
+/* 3x3x3 convolution on padded rows: out = relu?(conv(in) + bias), then + skip
+ * (rounded to BF16 before the add, as bsp_unet_add after the layer) when
+ * skip != NULL; halo rows of out get zeros.  cin, cout multiples of 16
+ * (cout > 64 in tiles of 64).  Persistent kernel, one CTA per SM. */
+int bsp_unet_tc_conv3(bsp_bf16_t *out, const bsp_bf16_t *in, const bsp_bf16_t *wimg,
+                      const float *bias, const bsp_bf16_t *skip, int nx, int ny, int nz,
+                      int cin, int cout, int relu, cudaStream_t stream);
+/* Reads and clears the flag a tensor-core convolution sets when a bounded
+ * wait gave up (its output is then not valid); synchronous. */
+int bsp_unet_tc_error(int *flag_host);
+/* The network's input scale on the device: *s_dev = RMS of div over the fluid
+ * cells (1 if there are none or it is 0), FP64 sums in a fixed order, in a
+ * caller workspace of bsp_unet_scale_workspace_bytes(). */
+size_t bsp_unet_scale_workspace_bytes(void);
+int bsp_unet_input_scale(float *s_dev, const float *div, const uint8_t *mask, int nx, int ny,
+                         int nz, void *workspace, size_t workspace_bytes, cudaStream_t stream);
+/* bsp_unet_pack_input, bsp_unet_pool (forward), bsp_unet_up (forward) and
+ * bsp_unet_head_fwd on the padded layout (every output row written, halo rows
+ * as zeros; the head writes the unpadded FP32 pressure).  The input is
+ * div / s_dev[0]; the head's output scale is factor * s_dev[0]. */
+int bsp_unet_tc_pack(bsp_bf16_t *x, const float *div, const uint8_t *mask, int nx, int ny,
+                     int nz, const float *s_dev, cudaStream_t stream);
+int bsp_unet_tc_pool(bsp_bf16_t *out, const bsp_bf16_t *in, int nx, int ny, int nz, int c,
+                     cudaStream_t stream);
+int bsp_unet_tc_up(bsp_bf16_t *out, const bsp_bf16_t *in, int nx, int ny, int nz, int c,
+                   cudaStream_t stream);
+int bsp_unet_tc_head(float *p, const bsp_bf16_t *x, const float *hw, const float *hb,
+                     const uint8_t *mask, int nx, int ny, int nz, const float *s_dev,
+                     float factor, cudaStream_t stream);
+
+/* The network run on the grid coarsened 2x: divc (nx/2, ny/2, nz/2) = mean
+ * divergence over the fluid children of each coarse fluid cell (maskc: the
+ * coarse cell classes), 0 elsewhere; and the coarse pressure pc brought back
+ * onto the fine fluid cells by trilinear interpolation (cell centres, edge
+ * values held), 0 elsewhere.  nx, ny, nz even. */
+int bsp_unet_restrict_div(float *divc, const uint8_t *maskc, const float *div,
+                          const uint8_t *mask, int nx, int ny, int nz, cudaStream_t stream);
+int bsp_unet_prolong(float *p, const float *pc, const uint8_t *mask, int nx, int ny, int nz,
+                     cudaStream_t stream);
 
 /* Exhaustive self-check of the device division-by-6 against IEEE division
  * over all 2^32 float bit patterns; the mismatch count is written to the
