@@ -70,6 +70,7 @@ struct CoarseCycle {
   const int *cflag;   // 1: cinv valid
   GridCtl *ctl;
   float alpha;
+  int fused_phases;   // 1: t formed where it is read (fewer phases and grid barriers)
 };
 
 struct Span {  // the warps that share a phase: warp w0 of nw
@@ -267,6 +268,137 @@ __device__ void phase_u2(const Level<T> &f, const float *__restrict__ t, const f
   });
 }
 
+// ---- fused phases: t is recomputed where it is read instead of stored --------------
+// D1 and U1 are pointwise, so the phase after each (D2a, U2) can form t at the
+// centre and at every neighbour itself; this removes a grid-wide phase, its
+// barrier and the t round trip through memory per level and direction, with
+// the same floating-point operations (bit-identical results).
+
+// t = OMEGA r / D (D1) of the 4 cells of quad c; 0 off fluid.
+template <class T>
+__device__ __forceinline__ float4 t_down4(const Level<T> &f, int64_t c, const float *wtab) {
+  const uint32_t m = ldm4(f.mask, c);
+  const float4 r = ld4t(f.r, c);
+  float v[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) v[q] = fl_mask(f4(r, q) * cc_w(wtab, m >> (8 * q)), m, q);
+  return make_float4(v[0], v[1], v[2], v[3]);
+}
+template <class T>
+__device__ __forceinline__ float t_down1(const Level<T> &f, int64_t c, const float *wtab) {
+  const uint32_t m = __ldg(f.mask + c);
+  return (m & BSP_MFLUID) ? cl(f.r, c) * cc_w(wtab, m) : 0.0f;
+}
+// t = OMEGA r / D + alpha e[l+1][parent] (U1) of the quad at (i, j, k); 0 off fluid.
+template <class T>
+__device__ __forceinline__ float4 t_up4(const Level<T> &f, const Level<T> &co, int i, int j,
+                                        int k, int64_t c, const float *wtab, float alpha) {
+  const uint32_t m = ldm4(f.mask, c);
+  const float4 r = ld4t(f.r, c);
+  const int64_t P = ((int64_t)(i >> 1) * co.ny + (j >> 1)) * co.nz + (k >> 1);
+  const float e0 = alpha * cl(co.e, P), e1 = alpha * cl(co.e, P + 1);
+  float v[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q)
+    v[q] = fl_mask(fmaf(f4(r, q), cc_w(wtab, m >> (8 * q)), q < 2 ? e0 : e1), m, q);
+  return make_float4(v[0], v[1], v[2], v[3]);
+}
+template <class T>
+__device__ __forceinline__ float t_up1(const Level<T> &f, const Level<T> &co, int i, int j, int k,
+                                       int64_t c, const float *wtab, float alpha) {
+  const uint32_t m = __ldg(f.mask + c);
+  if (!(m & BSP_MFLUID)) return 0.0f;
+  const int64_t P = ((int64_t)(i >> 1) * co.ny + (j >> 1)) * co.nz + (k >> 1);
+  return fmaf(cl(f.r, c), cc_w(wtab, m), alpha * cl(co.e, P));
+}
+
+// D1 + D2a: res = r - (6 t - s(t)) with t = OMEGA r / D formed on the fly.
+template <class T>
+__device__ void phase_down_fused(const Level<T> &f, float *__restrict__ res, const float *wtab,
+                                 Span sp) {
+  for_quads(f.nx, f.ny, f.nz, sp, [&](int i, int j, int k, int64_t c) {
+    const int64_t plane = (int64_t)f.ny * f.nz;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t m = ldm4(f.mask, c);
+    const float4 r = ld4t(f.r, c);
+    const float4 tc = t_down4(f, c, wtab);
+    const float4 a = i > 0 ? t_down4(f, c - plane, wtab) : z4;
+    const float4 b = i + 1 < f.nx ? t_down4(f, c + plane, wtab) : z4;
+    const float4 d = j > 0 ? t_down4(f, c - f.nz, wtab) : z4;
+    const float4 u = j + 1 < f.ny ? t_down4(f, c + f.nz, wtab) : z4;
+    const float km = k > 0 ? t_down1(f, c - 1, wtab) : 0.0f;
+    const float kp = k + 4 < f.nz ? t_down1(f, c + 4, wtab) : 0.0f;
+    const float4 lo = make_float4(km, tc.x, tc.y, tc.z), hi = make_float4(tc.y, tc.z, tc.w, kp);
+    float v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float s = ((f4(a, q) + f4(b, q)) + (f4(d, q) + f4(u, q))) + (f4(lo, q) + f4(hi, q));
+      const float sq = fmaf((float)((m >> (8 * q)) & 7u), f4(tc, q), s);
+      v[q] = fl_mask(f4(r, q) - (6.0f * f4(tc, q) - sq), m, q);
+    }
+    st4f(res, c, make_float4(v[0], v[1], v[2], v[3]));
+  });
+}
+
+// D2b without the next level's t (the next down phase forms it itself).
+template <class T>
+__device__ void phase_restrict(const Level<T> &f, const Level<T> &co, const float *__restrict__ res,
+                               Span sp) {
+  for_quads(co.nx, co.ny, co.nz, sp, [&](int I, int J, int K, int64_t C) {
+    float acc[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+      for (int b = 0; b < 2; ++b) {
+        const int i = 2 * I + a, j = 2 * J + b;
+        if (i < f.nx && j < f.ny) {
+          const int64_t c = ((int64_t)i * f.ny + j) * f.nz + 2 * K;
+          const float4 p = ld4f(res, c), q = ld4f(res, c + 4);
+          acc[0] += p.x + p.y;
+          acc[1] += p.z + p.w;
+          acc[2] += q.x + q.y;
+          acc[3] += q.z + q.w;
+        }
+      }
+    const uint32_t m = ldm4(co.mask, C);
+    float rv[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) rv[q] = fl_mask(0.5f * acc[q], m, q);
+    st4t(co.r, C, make_float4(rv[0], rv[1], rv[2], rv[3]));
+  });
+}
+
+// U1 + U2: e = t + OMEGA (r - (6 t - s(t))) / D with t = OMEGA r / D +
+// alpha e[l+1][parent] formed on the fly.
+template <class T>
+__device__ void phase_up_fused(const Level<T> &f, const Level<T> &co, const float *wtab,
+                               float alpha, Span sp) {
+  for_quads(f.nx, f.ny, f.nz, sp, [&](int i, int j, int k, int64_t c) {
+    const int64_t plane = (int64_t)f.ny * f.nz;
+    const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const uint32_t m = ldm4(f.mask, c);
+    const float4 r = ld4t(f.r, c);
+    const float4 tc = t_up4(f, co, i, j, k, c, wtab, alpha);
+    const float4 a = i > 0 ? t_up4(f, co, i - 1, j, k, c - plane, wtab, alpha) : z4;
+    const float4 b = i + 1 < f.nx ? t_up4(f, co, i + 1, j, k, c + plane, wtab, alpha) : z4;
+    const float4 d = j > 0 ? t_up4(f, co, i, j - 1, k, c - f.nz, wtab, alpha) : z4;
+    const float4 u = j + 1 < f.ny ? t_up4(f, co, i, j + 1, k, c + f.nz, wtab, alpha) : z4;
+    const float km = k > 0 ? t_up1(f, co, i, j, k - 1, c - 1, wtab, alpha) : 0.0f;
+    const float kp = k + 4 < f.nz ? t_up1(f, co, i, j, k + 4, c + 4, wtab, alpha) : 0.0f;
+    const float4 lo = make_float4(km, tc.x, tc.y, tc.z), hi = make_float4(tc.y, tc.z, tc.w, kp);
+    float v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float s = ((f4(a, q) + f4(b, q)) + (f4(d, q) + f4(u, q))) + (f4(lo, q) + f4(hi, q));
+      const float sq = fmaf((float)((m >> (8 * q)) & 7u), f4(tc, q), s);
+      v[q] = fl_mask(fmaf(f4(r, q) - (6.0f * f4(tc, q) - sq), cc_w(wtab, m >> (8 * q)),
+                          f4(tc, q)),
+                     m, q);
+    }
+    st4t(f.e, c, make_float4(v[0], v[1], v[2], v[3]));
+  });
+}
+
 // Scalar neighbour sum for the coarsest-level sweeps.
 template <class T>
 __device__ __forceinline__ float nbr_sum1(const float *t, const Level<T> &f, int i, int j, int k,
@@ -343,6 +475,36 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cycle_kernel(CoarseCycle<T> 
   auto sync_all = [&]() {
     if (ok && !grid_barrier(a.ctl)) ok = false;
   };
+  if (a.fused_phases) {
+    // ---- down: per level the residual (t formed on the fly) and the restriction
+    for (int l = 1; l + 1 < L && ok; ++l) {
+      if (l < tail) {
+        phase_down_fused(a.lv[l], a.res, wtab, all);
+        sync_all();
+        phase_restrict(a.lv[l], a.lv[l + 1], a.res, all);
+        sync_all();
+      } else if (blockIdx.x == 0) {
+        phase_down_fused(a.lv[l], a.res, wtab, one);
+        __syncthreads();
+        phase_restrict(a.lv[l], a.lv[l + 1], a.res, one);
+        __syncthreads();
+      }
+    }
+    if (blockIdx.x == 0 && ok) {
+      coarsest_solve(a, wtab);
+      __syncthreads();
+      for (int l = L - 2; l >= tail && l >= 1; --l) {
+        phase_up_fused(a.lv[l], a.lv[l + 1], wtab, a.alpha, one);
+        __syncthreads();
+      }
+    }
+    const int top = min(tail, L - 1) - 1;
+    if (top >= 1) sync_all();
+    for (int l = top; l >= 1 && ok; --l) {
+      phase_up_fused(a.lv[l], a.lv[l + 1], wtab, a.alpha, all);
+      if (l > 1) sync_all();
+    }
+  } else {
   // ---- down: t of level 1, then per level the residual pass and the
   // restriction (which also forms t of the next level)
   if (L > 2) {
@@ -386,10 +548,15 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cycle_kernel(CoarseCycle<T> 
     phase_u2(a.lv[l], a.scratch, wtab, all);
     if (l > 1) sync_all();
   }
+  }
   if (!ok && threadIdx.x == 0) atomicExch(&st->dev_error, 1);
 }
 
 bool g_coarse_fused_enabled = true;  // BSP_TUNE_COARSE_FUSED
+// BSP_TUNE_COARSE_PHASES: 1 (default) forms t where it is read -- D1 folded
+// into the residual pass, U1 into the post-smoothing pass; 0 runs them as
+// phases of their own with t stored.  The results are the same bits.
+bool g_coarse_phases_fused = true;
 
 // FP32 scratch of the coarse-cycle kernel: t (max(cells of level 1, 3 x cells
 // of the coarsest level), rounded up to 64 floats) followed by res (cells of
@@ -444,6 +611,7 @@ bool launch_coarse_cycle(const Level<T> *lv, int L, float *scratch, const float 
   a.cflag = cflag;
   a.ctl = reinterpret_cast<GridCtl *>(ctl);
   a.alpha = alpha;
+  a.fused_phases = g_coarse_phases_fused ? 1 : 0;
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(CC_THREADS);

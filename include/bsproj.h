@@ -66,6 +66,7 @@ extern "C" {
  * coarse-cycle grid barrier's error word set, as a barrier that gave up
  * leaves it (that solve returns BSP_ERR_TIMEOUT; the key clears itself). */
 #define BSP_TUNE_TEST_BARRIER_ERROR 11
+#define BSP_TUNE_COARSE_PHASES 12 /* coarse cycle forms t where it is read: 1 on (default), 0 off */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */
