@@ -741,7 +741,7 @@ def run_projection(args, dev, rank, world, local, dist):
             a.copy_(b, non_blocking=True)
         F.compute_divergence(div, *u, mask, DX)
         if kind == "learned":
-            warm.guess(div, DX, DT, RHO, out=p)
+            warm.guess(div, DX, DT, RHO, out=p, graph=graph)
             res = solvers["fp16"].solve(div, DX, DT, RHO, tol=TOL, p=p, warm_start=True,
                                         graph=graph)
         else:

@@ -49,6 +49,7 @@ SIGNATURES = {
     "bsp_dot_noalloc": (_I, [_P, _P, _L, _P, _P]),
     "bsp_profile_enable": (_I, [_I]),
     "bsp_profile_read": (_I, [_P, _P, _I]),
+    "bsp_coarse_trace_read": (_I, [_P, _I]),
     "bsp_divergence": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _P, _P]),
     "bsp_subtract_gradient": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _F, _F, _F, _P]),
     "bsp_enforce_no_slip": (_I, [_P, _P, _P, _P, _I, _I, _I, _P]),

@@ -490,7 +490,29 @@ class WarmStart:
                                     device=mat_t.device)
             self.pc = torch.zeros_like(self.divc)
 
-    def guess(self, div, dx, dt, rho, out: torch.Tensor) -> torch.Tensor:
+    def guess(self, div, dx, dt, rho, out: torch.Tensor, graph: bool = True) -> torch.Tensor:
+        """Writes the starting pressure into ``out``.  With ``graph`` the
+        launches of one guess (about 25 kernels) are captured once into a CUDA
+        graph per (div, out, dx, dt, rho) and replayed afterwards."""
+        if not graph:
+            return self._launch(div, dx, dt, rho, out)
+        key = (div.data_ptr(), out.data_ptr(), float(dx), float(dt), float(rho),
+               self.net.step)
+        g = self.__dict__.get("_graph")
+        if g is None or g[0] != key:
+            self._launch(div, dx, dt, rho, out)  # first run: plans, weights, opt-ins
+            cg = torch.cuda.CUDAGraph()
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s):
+                with torch.cuda.graph(cg, stream=s):
+                    self._launch(div, dx, dt, rho, out)
+            torch.cuda.current_stream().wait_stream(s)
+            self._graph = g = (key, cg)
+        g[1].replay()
+        return out
+
+    def _launch(self, div, dx, dt, rho, out: torch.Tensor) -> torch.Tensor:
         nx, ny, nz = self.dims
         st = stream_handle()
         if self.mode == "full":

@@ -113,6 +113,7 @@ __device__ __forceinline__ uint32_t byte_of(uint32_t w, int q) { return (w >> (8
 // Opt kernel `fn` into `bytes` of dynamic shared memory on the current
 // device.  The attribute belongs to the device, so the answer is cached per
 // (kernel, device): a second GPU in the same process gets its own opt-in.
+// Callers pass one fixed size per kernel (the largest they launch it with).
 // False when the device refuses (the caller then takes another path).
 inline bool smem_opt_in(const void *fn, int bytes) {
   struct Entry {

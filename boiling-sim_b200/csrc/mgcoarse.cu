@@ -33,6 +33,7 @@
 #include "bsp_common.cuh"
 #include "grid_sync.cuh"
 #include "solver.cuh"
+#include "tma.cuh"
 
 namespace bsp {
 
@@ -40,6 +41,9 @@ constexpr int CC_THREADS = 1024;
 constexpr int TAIL_CELLS = 16384;
 constexpr float CC_OMEGA = 6.0f / 7.0f;
 constexpr int CC_COARSE_SWEEPS = 64;
+constexpr int CC_TRACE_MAX = 48;
+// Phase-boundary stamps of the last traced coarse cycle (BSP_TUNE_COARSE_TRACE).
+__device__ unsigned long long g_cc_trace[CC_TRACE_MAX];
 
 __device__ __forceinline__ float cl(const float *p, int64_t c) { return p[c]; }
 __device__ __forceinline__ float cl(const __half *p, int64_t c) { return __half2float(p[c]); }
@@ -71,7 +75,22 @@ struct CoarseCycle {
   GridCtl *ctl;
   float alpha;
   int fused_phases;   // 1: t formed where it is read (fewer phases and grid barriers)
+  unsigned long long *trace;  // optional: CTA 0's %globaltimer at each phase boundary
+  int cinv_bytes;     // > 0: CTA 0 copies the dense inverse into shared memory at launch
 };
+
+// Dynamic shared memory of the coarse-cycle kernel: [dense inverse (CTA 0)]
+// [coarsest right-hand side, FP32] [mbarrier of the inverse's bulk copy].
+__device__ __forceinline__ float *cc_smem() {
+  extern __shared__ __align__(16) float cc_dyn[];
+  return cc_dyn;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
 
 struct Span {  // the warps that share a phase: warp w0 of nw
   int w0, nw;
@@ -314,25 +333,34 @@ __device__ __forceinline__ float t_up1(const Level<T> &f, const Level<T> &co, in
 
 // D1 + D2a: res = r - (6 t - s(t)) with t = OMEGA r / D formed on the fly.
 template <class T>
-__device__ void phase_down_fused(const Level<T> &f, float *__restrict__ res, const float *wtab,
+__device__ __forceinline__ void phase_down_fused(const Level<T> &f, float *__restrict__ res, const float *wtab,
                                  Span sp) {
   for_quads(f.nx, f.ny, f.nz, sp, [&](int i, int j, int k, int64_t c) {
     const int64_t plane = (int64_t)f.ny * f.nz;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    // neighbour pairs summed as soon as both are known (the same sums as
+    // ((a + b) + (d + u)) + (lo + hi), fewer live registers)
+    float4 ab, du;
+    {
+      const float4 a = i > 0 ? t_down4(f, c - plane, wtab) : z4;
+      const float4 b = i + 1 < f.nx ? t_down4(f, c + plane, wtab) : z4;
+      ab = make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+    }
+    {
+      const float4 d = j > 0 ? t_down4(f, c - f.nz, wtab) : z4;
+      const float4 u = j + 1 < f.ny ? t_down4(f, c + f.nz, wtab) : z4;
+      du = make_float4(d.x + u.x, d.y + u.y, d.z + u.z, d.w + u.w);
+    }
+    const float km = k > 0 ? t_down1(f, c - 1, wtab) : 0.0f;
+    const float kp = k + 4 < f.nz ? t_down1(f, c + 4, wtab) : 0.0f;
     const uint32_t m = ldm4(f.mask, c);
     const float4 r = ld4t(f.r, c);
     const float4 tc = t_down4(f, c, wtab);
-    const float4 a = i > 0 ? t_down4(f, c - plane, wtab) : z4;
-    const float4 b = i + 1 < f.nx ? t_down4(f, c + plane, wtab) : z4;
-    const float4 d = j > 0 ? t_down4(f, c - f.nz, wtab) : z4;
-    const float4 u = j + 1 < f.ny ? t_down4(f, c + f.nz, wtab) : z4;
-    const float km = k > 0 ? t_down1(f, c - 1, wtab) : 0.0f;
-    const float kp = k + 4 < f.nz ? t_down1(f, c + 4, wtab) : 0.0f;
     const float4 lo = make_float4(km, tc.x, tc.y, tc.z), hi = make_float4(tc.y, tc.z, tc.w, kp);
     float v[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const float s = ((f4(a, q) + f4(b, q)) + (f4(d, q) + f4(u, q))) + (f4(lo, q) + f4(hi, q));
+      const float s = (f4(ab, q) + f4(du, q)) + (f4(lo, q) + f4(hi, q));
       const float sq = fmaf((float)((m >> (8 * q)) & 7u), f4(tc, q), s);
       v[q] = fl_mask(f4(r, q) - (6.0f * f4(tc, q) - sq), m, q);
     }
@@ -342,7 +370,7 @@ __device__ void phase_down_fused(const Level<T> &f, float *__restrict__ res, con
 
 // D2b without the next level's t (the next down phase forms it itself).
 template <class T>
-__device__ void phase_restrict(const Level<T> &f, const Level<T> &co, const float *__restrict__ res,
+__device__ __forceinline__ void phase_restrict(const Level<T> &f, const Level<T> &co, const float *__restrict__ res,
                                Span sp) {
   for_quads(co.nx, co.ny, co.nz, sp, [&](int I, int J, int K, int64_t C) {
     float acc[4] = {0.f, 0.f, 0.f, 0.f};
@@ -371,25 +399,32 @@ __device__ void phase_restrict(const Level<T> &f, const Level<T> &co, const floa
 // U1 + U2: e = t + OMEGA (r - (6 t - s(t))) / D with t = OMEGA r / D +
 // alpha e[l+1][parent] formed on the fly.
 template <class T>
-__device__ void phase_up_fused(const Level<T> &f, const Level<T> &co, const float *wtab,
+__device__ __forceinline__ void phase_up_fused(const Level<T> &f, const Level<T> &co, const float *wtab,
                                float alpha, Span sp) {
   for_quads(f.nx, f.ny, f.nz, sp, [&](int i, int j, int k, int64_t c) {
     const int64_t plane = (int64_t)f.ny * f.nz;
     const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 ab, du;
+    {
+      const float4 a = i > 0 ? t_up4(f, co, i - 1, j, k, c - plane, wtab, alpha) : z4;
+      const float4 b = i + 1 < f.nx ? t_up4(f, co, i + 1, j, k, c + plane, wtab, alpha) : z4;
+      ab = make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+    }
+    {
+      const float4 d = j > 0 ? t_up4(f, co, i, j - 1, k, c - f.nz, wtab, alpha) : z4;
+      const float4 u = j + 1 < f.ny ? t_up4(f, co, i, j + 1, k, c + f.nz, wtab, alpha) : z4;
+      du = make_float4(d.x + u.x, d.y + u.y, d.z + u.z, d.w + u.w);
+    }
+    const float km = k > 0 ? t_up1(f, co, i, j, k - 1, c - 1, wtab, alpha) : 0.0f;
+    const float kp = k + 4 < f.nz ? t_up1(f, co, i, j, k + 4, c + 4, wtab, alpha) : 0.0f;
     const uint32_t m = ldm4(f.mask, c);
     const float4 r = ld4t(f.r, c);
     const float4 tc = t_up4(f, co, i, j, k, c, wtab, alpha);
-    const float4 a = i > 0 ? t_up4(f, co, i - 1, j, k, c - plane, wtab, alpha) : z4;
-    const float4 b = i + 1 < f.nx ? t_up4(f, co, i + 1, j, k, c + plane, wtab, alpha) : z4;
-    const float4 d = j > 0 ? t_up4(f, co, i, j - 1, k, c - f.nz, wtab, alpha) : z4;
-    const float4 u = j + 1 < f.ny ? t_up4(f, co, i, j + 1, k, c + f.nz, wtab, alpha) : z4;
-    const float km = k > 0 ? t_up1(f, co, i, j, k - 1, c - 1, wtab, alpha) : 0.0f;
-    const float kp = k + 4 < f.nz ? t_up1(f, co, i, j, k + 4, c + 4, wtab, alpha) : 0.0f;
     const float4 lo = make_float4(km, tc.x, tc.y, tc.z), hi = make_float4(tc.y, tc.z, tc.w, kp);
     float v[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const float s = ((f4(a, q) + f4(b, q)) + (f4(d, q) + f4(u, q))) + (f4(lo, q) + f4(hi, q));
+      const float s = (f4(ab, q) + f4(du, q)) + (f4(lo, q) + f4(hi, q));
       const float sq = fmaf((float)((m >> (8 * q)) & 7u), f4(tc, q), s);
       v[q] = fl_mask(fmaf(f4(r, q) - (6.0f * f4(tc, q) - sq), cc_w(wtab, m >> (8 * q)),
                           f4(tc, q)),
@@ -417,14 +452,21 @@ __device__ __forceinline__ float nbr_sum1(const float *t, const Level<T> &f, int
 // output, lanes over the sum, fixed shuffle order), or, without one, damped
 // Jacobi sweeps from zero in the scratch vector.
 template <class T>
-__device__ void coarsest_solve(const CoarseCycle<T> &a, const float *wtab) {
+__device__ void coarsest_solve(const CoarseCycle<T> &a, const float *wtab, const float *minv) {
   const Level<T> &c = a.lv[a.L - 1];
   const int n = c.nx * c.ny * c.nz;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (*a.cflag) {
+    // e = M r; r staged in shared memory, M read from shared memory when it
+    // was copied there at launch (minv), else from global memory
+    float *rs = cc_smem() + (a.cinv_bytes >> 2);
+    for (int q = threadIdx.x; q < n; q += blockDim.x) rs[q] = cl(c.r, q);
+    __syncthreads();
     for (int o = warp; o < n; o += nw) {
       float acc = 0.0f;
-      for (int q = lane; q < n; q += 32) acc = fmaf(a.cinv[(int64_t)o * n + q], cl(c.r, q), acc);
+      const float *row = minv + (int64_t)o * n;
+#pragma unroll 4
+      for (int q = lane; q < n; q += 32) acc = fmaf(row[q], rs[q], acc);
       for (int s = 16; s > 0; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s);
       if (lane == 0) cs(c.e, o, (__ldg(c.mask + o) & BSP_MFLUID) ? acc : 0.0f);
     }
@@ -471,10 +513,33 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cycle_kernel(CoarseCycle<T> 
   // levels >= tail run in CTA 0 alone
   int tail = 1;
   while (tail < L && cells(tail) > TAIL_CELLS) ++tail;
+  // CTA 0 fetches the coarsest level's dense inverse into shared memory while
+  // the grid works on the big levels (one bulk copy, bounded wait before use)
+  uint64_t *cbar = reinterpret_cast<uint64_t *>(cc_smem() + (a.cinv_bytes >> 2) +
+                                                ((a.cinv_bytes > 0) ? COARSEST_CELLS : 0));
+  const bool cinv_copy = a.cinv_bytes > 0 && blockIdx.x == 0;
+  bool cinv_waited = false;
+  if (cinv_copy && threadIdx.x == 0) {
+    mbar_init(cbar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_expect_tx(cbar, (uint32_t)a.cinv_bytes);
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+        "[%3];" ::"r"(smem_u32(cc_smem())),
+        "l"(a.cinv), "r"((uint32_t)a.cinv_bytes), "r"(smem_u32(cbar))
+        : "memory");
+  }
   bool ok = true;
+  int nmark = 0;
+  auto mark = [&]() {  // tracing: CTA 0 stamps each phase boundary
+    if (a.trace && blockIdx.x == 0 && threadIdx.x == 0 && nmark < CC_TRACE_MAX)
+      a.trace[nmark++] = global_ns();
+  };
   auto sync_all = [&]() {
     if (ok && !grid_barrier(a.ctl)) ok = false;
+    mark();
   };
+  mark();
   if (a.fused_phases) {
     // ---- down: per level the residual (t formed on the fly) and the restriction
     for (int l = 1; l + 1 < L && ok; ++l) {
@@ -488,14 +553,26 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cycle_kernel(CoarseCycle<T> 
         __syncthreads();
         phase_restrict(a.lv[l], a.lv[l + 1], a.res, one);
         __syncthreads();
+        mark();
       }
     }
     if (blockIdx.x == 0 && ok) {
-      coarsest_solve(a, wtab);
+      const float *minv = a.cinv;
+      if (cinv_copy) {
+        __shared__ int s_cok;
+        if (threadIdx.x == 0) s_cok = mbar_wait(cbar, 0) ? 1 : 0;
+        __syncthreads();
+        cinv_waited = true;
+        if (s_cok) minv = cc_smem();
+        else ok = false;
+      }
+      if (ok) coarsest_solve(a, wtab, minv);
       __syncthreads();
-      for (int l = L - 2; l >= tail && l >= 1; --l) {
+      mark();
+      for (int l = L - 2; l >= tail && l >= 1 && ok; --l) {
         phase_up_fused(a.lv[l], a.lv[l + 1], wtab, a.alpha, one);
         __syncthreads();
+        mark();
       }
     }
     const int top = min(tail, L - 1) - 1;
@@ -504,6 +581,7 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cycle_kernel(CoarseCycle<T> 
       phase_up_fused(a.lv[l], a.lv[l + 1], wtab, a.alpha, all);
       if (l > 1) sync_all();
     }
+    mark();
   } else {
   // ---- down: t of level 1, then per level the residual pass and the
   // restriction (which also forms t of the next level)
@@ -530,7 +608,16 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cycle_kernel(CoarseCycle<T> 
     }
   }
   if (blockIdx.x == 0 && ok) {
-    coarsest_solve(a, wtab);
+    const float *minv = a.cinv;
+    if (cinv_copy) {
+      __shared__ int s_cok2;
+      if (threadIdx.x == 0) s_cok2 = mbar_wait(cbar, 0) ? 1 : 0;
+      __syncthreads();
+      cinv_waited = true;
+      if (s_cok2) minv = cc_smem();
+      else ok = false;
+    }
+    if (ok) coarsest_solve(a, wtab, minv);
     __syncthreads();
     for (int l = L - 2; l >= tail && l >= 1; --l) {
       phase_u1(a.lv[l], a.lv[l + 1], a.scratch, wtab, a.alpha, one);
@@ -549,6 +636,8 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cycle_kernel(CoarseCycle<T> 
     if (l > 1) sync_all();
   }
   }
+  // the bulk copy must have landed before CTA 0's shared memory goes away
+  if (cinv_copy && !cinv_waited && threadIdx.x == 0) mbar_wait(cbar, 0);
   if (!ok && threadIdx.x == 0) atomicExch(&st->dev_error, 1);
 }
 
@@ -557,6 +646,9 @@ bool g_coarse_fused_enabled = true;  // BSP_TUNE_COARSE_FUSED
 // into the residual pass, U1 into the post-smoothing pass; 0 runs them as
 // phases of their own with t stored.  The results are the same bits.
 bool g_coarse_phases_fused = true;
+// BSP_TUNE_COARSE_TRACE: 1 makes every coarse-cycle launch record CTA 0's
+// %globaltimer at each phase boundary (bsp_coarse_trace_read); tracing only.
+bool g_coarse_trace = false;
 
 // FP32 scratch of the coarse-cycle kernel: t (max(cells of level 1, 3 x cells
 // of the coarsest level), rounded up to 64 floats) followed by res (cells of
@@ -612,10 +704,31 @@ bool launch_coarse_cycle(const Level<T> *lv, int L, float *scratch, const float 
   a.ctl = reinterpret_cast<GridCtl *>(ctl);
   a.alpha = alpha;
   a.fused_phases = g_coarse_phases_fused ? 1 : 0;
+  // the dense inverse of the coarsest level goes to CTA 0's shared memory when
+  // it is small (<= 96 KB); the copy size is rounded up to 16 bytes (the
+  // inverse's workspace slot is 256-byte aligned and at least that long)
+  const int64_t nc = (int64_t)lv[L - 1].nx * lv[L - 1].ny * lv[L - 1].nz;
+  a.cinv_bytes = 0;
+  size_t dyn = 0;
+  if (nc <= COARSEST_CELLS && nc * nc * 4 <= 96 * 1024 && ((uintptr_t)cinv & 15u) == 0) {
+    a.cinv_bytes = (int)((nc * nc * 4 + 15) / 16 * 16);
+    dyn = (size_t)a.cinv_bytes + COARSEST_CELLS * sizeof(float) + 16;
+  } else {
+    dyn = COARSEST_CELLS * sizeof(float) + 16;
+  }
+  // one opt-in per device at the largest size this launcher ever asks for
+  constexpr int DYN_MAX = 96 * 1024 + 16 + COARSEST_CELLS * (int)sizeof(float) + 16;
+  if (dyn > 48 * 1024 && !smem_opt_in((const void *)mg_cycle_kernel<T>, DYN_MAX)) {
+    a.cinv_bytes = 0;
+    dyn = COARSEST_CELLS * sizeof(float) + 16;
+  }
+  a.trace = nullptr;
+  if (g_coarse_trace && cudaGetSymbolAddress((void **)&a.trace, g_cc_trace) != cudaSuccess)
+    a.trace = nullptr;
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(CC_THREADS);
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = dyn;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeCooperative;
@@ -634,3 +747,14 @@ INST(__nv_bfloat16)
 #undef INST
 
 }  // namespace bsp
+
+// Copies the phase-boundary stamps of the last traced coarse cycle (ns,
+// %globaltimer of CTA 0; unused slots hold 0) and clears them; synchronous.
+extern "C" int bsp_coarse_trace_read(unsigned long long *host, int n) {
+  if (!host || n <= 0) return BSP_ERR_ARG;
+  if (n > bsp::CC_TRACE_MAX) n = bsp::CC_TRACE_MAX;
+  cudaError_t e = cudaMemcpyFromSymbol(host, bsp::g_cc_trace, sizeof(unsigned long long) * n);
+  if (e != cudaSuccess) return (int)e;
+  static const unsigned long long zero[bsp::CC_TRACE_MAX] = {0};
+  return (int)cudaMemcpyToSymbol(bsp::g_cc_trace, zero, sizeof(zero));
+}

@@ -506,6 +506,7 @@ extern int g_fine_bi;
 extern int g_sweep_tblock;
 extern bool g_test_barrier_error;
 extern bool g_coarse_phases_fused;
+extern bool g_coarse_trace;
 namespace cond {
 extern int g_cond_bi;
 extern bool g_cond_tma;
@@ -557,6 +558,10 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_COARSE_PHASES:
       if (value < 0 || value > 1) return BSP_ERR_ARG;
       bsp::g_coarse_phases_fused = value != 0;
+      return BSP_OK;
+    case BSP_TUNE_COARSE_TRACE:
+      if (value < 0 || value > 1) return BSP_ERR_ARG;
+      bsp::g_coarse_trace = value != 0;
       return BSP_OK;
     case BSP_TUNE_TEST_BARRIER_ERROR:
       if (value < 0 || value > 1) return BSP_ERR_ARG;

@@ -67,6 +67,7 @@ extern "C" {
  * leaves it (that solve returns BSP_ERR_TIMEOUT; the key clears itself). */
 #define BSP_TUNE_TEST_BARRIER_ERROR 11
 #define BSP_TUNE_COARSE_PHASES 12 /* coarse cycle forms t where it is read: 1 on (default), 0 off */
+#define BSP_TUNE_COARSE_TRACE 13  /* tracing: coarse-cycle launches stamp their phase boundaries */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */
@@ -196,6 +197,11 @@ int bsp_set_tuning(int key, int value);
  * milliseconds and launch counts of classes 0..nclass-1 and clears the
  * record. */
 #define BSP_PROF_NCLASS 11
+/* Tracing of the one-launch coarse V-cycle (with BSP_TUNE_COARSE_TRACE = 1):
+ * host[0 .. n) receives CTA 0's %globaltimer (ns) at each phase boundary of
+ * the last cycle launched (0 in unused slots, at most 48), and the record is
+ * cleared.  Synchronous. */
+int bsp_coarse_trace_read(unsigned long long *host, int n);
 int bsp_profile_enable(int on);
 int bsp_profile_read(double *ms, long long *launches, int nclass);
 
