@@ -47,8 +47,10 @@ def _pcg(mat, div, tol=1e-6, max_iter=200):
     z = lambda *s: torch.zeros(s, dtype=torch.float32, device="cuda")  # noqa: E731
     ws = [z(*shape) for _ in range(5)] + [z(1024)] + [z(1) for _ in range(7)]
     p = torch.zeros(shape, device="cuda")
-    it = SimCore(0).pressure_solve_pcg(ptr(p), ptr(torch.as_tensor(div).cuda()),
-                                       ptr(torch.as_tensor(mat).cuda()), *shape, DX, DT, RHO,
+    # named tensors: a temporary freed after ptr() could hand its memory to the
+    # next argument's allocation before the kernel reads it
+    div_d, mat_d = torch.as_tensor(div).cuda(), torch.as_tensor(mat).cuda()
+    it = SimCore(0).pressure_solve_pcg(ptr(p), ptr(div_d), ptr(mat_d), *shape, DX, DT, RHO,
                                        tol, max_iter, *[ptr(w) for w in ws])
     return it, p
 

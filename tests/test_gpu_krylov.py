@@ -108,8 +108,8 @@ def test_compute_b_launch_bit_exact(cuda, seed, shape):
     mat, _, div = S.parity_random_grid(rng, shape)
     scale = np.float32(-(997.0 * 0.002 * 0.002) / 0.01)
     b = torch.full(shape, 5.0, device="cuda")
-    assert call("compute_b_launch", ptr(b), ptr(dev(div)), ptr(dev(mat, torch.int32)), *shape,
-                float(scale), 0) == 0
+    div_d, mat_d = dev(div), dev(mat, torch.int32)
+    assert call("compute_b_launch", ptr(b), ptr(div_d), ptr(mat_d), *shape, float(scale), 0) == 0
     want = np.where(mat == 0, scale * div, np.float32(0.0)).astype(np.float32)
     assert np.array_equal(bits(host(b)), bits(want))
 
@@ -139,7 +139,8 @@ def test_dot_launch_fp64_accumulation(cuda, n):
     x, y = _vec(rng, n), _vec(rng, n)
     ws = torch.zeros(1024, device="cuda")
     res = torch.zeros(1, device="cuda")
-    assert call("dot_launch", ptr(dev(x)), ptr(dev(y)), n, ptr(ws), ptr(res)) == 0
+    xd, yd = dev(x), dev(y)
+    assert call("dot_launch", ptr(xd), ptr(yd), n, ptr(ws), ptr(res)) == 0
     exact = float(np.dot(x.astype(np.float64), y.astype(np.float64)))
     got = float(host(res)[0])
     assert abs(got - exact) <= 2 * abs(float(np.spacing(np.float32(exact)))) + 1e-12
@@ -163,8 +164,9 @@ def test_pcg_launch_matches_reference_pcg_goldens(cuda, name):
     shape = d["mat"].shape
     p = torch.full(shape, 3.0, device="cuda")
     ws = _pcg_ws(shape)
-    it = SimCore(0).pressure_solve_pcg(ptr(p), ptr(dev(d["div"])), ptr(dev(d["mat"], torch.int32)),
-                                       *shape, dx, dt, rho, tol, 200, *[ptr(w) for w in ws])
+    div_d, mat_d = dev(d["div"]), dev(d["mat"], torch.int32)
+    it = SimCore(0).pressure_solve_pcg(ptr(p), ptr(div_d), ptr(mat_d), *shape, dx, dt, rho, tol,
+                                       200, *[ptr(w) for w in ws])
     assert abs(it - int(d["iters"])) <= 5, (it, int(d["iters"]))
     fl = d["mat"] == 0
     got = host(p)
