@@ -471,14 +471,26 @@ class WarmStart:
     children, classes by coarse_materials), its pressure interpolated back
     onto the fine fluid cells (bsp_unet_restrict_div / bsp_unet_prolong) --
     an eighth of the network's work, for grids large enough that a full-size
-    prediction would cost more than the iterations it saves."""
+    prediction would cost more than the iterations it saves.
 
-    def __init__(self, net: UNet, mat_t: torch.Tensor, mask: torch.Tensor, mode: str = "auto"):
+    ``scale=True`` (default) multiplies the prediction by the energy-optimal
+    gamma = (b . p) / (p . A p) (bsp_unet_energy_scale), so the guess handed
+    to the solve is never farther from the solution than zero in the A-norm:
+    the plain solve stays the judge of the network's error."""
+
+    def __init__(self, net: UNet, mat_t: torch.Tensor, mask: torch.Tensor, mode: str = "auto",
+                 scale: bool = True):
         from .fluid import cell_mask
 
         self.net = net
         self.dims = tuple(mat_t.shape)
         self.mask = mask
+        self.scale = scale
+        if scale:
+            self.Ap = torch.empty(self.dims, dtype=torch.float32, device=mat_t.device)
+            nb = int(_lib.lib().bsp_unet_scale_workspace_bytes())
+            self.ws = torch.empty((nb + 7) // 8, dtype=torch.float64, device=mat_t.device)
+            self.gamma = torch.zeros(1, dtype=torch.float32, device=mat_t.device)
         nx, ny, nz = self.dims
         if mode == "auto":
             mode = "coarse" if (nx % 16 == 0 and ny % 16 == 0 and nz % 16 == 0 and
@@ -516,12 +528,18 @@ class WarmStart:
         nx, ny, nz = self.dims
         st = stream_handle()
         if self.mode == "full":
-            return self.net.tc_plan(self.dims).run(div, self.mask, dx, dt, rho, out=out)
-        call("bsp_unet_restrict_div", ptr(self.divc), ptr(self.maskc), ptr(div), ptr(self.mask),
-             nx, ny, nz, st)
-        self.net.tc_plan(tuple(self.divc.shape)).run(self.divc, self.maskc, 2.0 * dx, dt, rho,
-                                                      out=self.pc)
-        call("bsp_unet_prolong", ptr(out), ptr(self.pc), ptr(self.mask), nx, ny, nz, st)
+            self.net.tc_plan(self.dims).run(div, self.mask, dx, dt, rho, out=out)
+        else:
+            call("bsp_unet_restrict_div", ptr(self.divc), ptr(self.maskc), ptr(div),
+                 ptr(self.mask), nx, ny, nz, st)
+            self.net.tc_plan(tuple(self.divc.shape)).run(self.divc, self.maskc, 2.0 * dx, dt, rho,
+                                                          out=self.pc)
+            call("bsp_unet_prolong", ptr(out), ptr(self.pc), ptr(self.mask), nx, ny, nz, st)
+        if self.scale:
+            call("bsp_spmv", ptr(self.Ap), ptr(out), ptr(self.mask), nx, ny, nz, st)
+            call("bsp_unet_energy_scale", ptr(out), ptr(self.Ap), ptr(div), ptr(self.mask), nx, ny,
+                 nz, -(rho * dx * dx / dt), ptr(self.ws), self.ws.numel() * 8, ptr(self.gamma),
+                 st)
         return out
 
 

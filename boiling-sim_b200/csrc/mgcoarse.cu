@@ -642,10 +642,13 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cycle_kernel(CoarseCycle<T> 
 }
 
 bool g_coarse_fused_enabled = true;  // BSP_TUNE_COARSE_FUSED
-// BSP_TUNE_COARSE_PHASES: 1 (default) forms t where it is read -- D1 folded
-// into the residual pass, U1 into the post-smoothing pass; 0 runs them as
-// phases of their own with t stored.  The results are the same bits.
-bool g_coarse_phases_fused = true;
+// BSP_TUNE_COARSE_PHASES: 1 forms t where it is read -- D1 folded into the
+// residual pass, U1 into the post-smoothing pass (4 fewer grid barriers per
+// cycle, 7 recomputations of t per cell); 0 (default) runs them as phases of
+// their own with t stored.  The results are the same bits.  Measured at
+// 384x384x256: 14.44 ms per solve fused against 14.16 ms stored -- the level-1
+// phases are bound by their load latency, which recomputation lengthens.
+bool g_coarse_phases_fused = false;
 // BSP_TUNE_COARSE_TRACE: 1 makes every coarse-cycle launch record CTA 0's
 // %globaltimer at each phase boundary (bsp_coarse_trace_read); tracing only.
 bool g_coarse_trace = false;

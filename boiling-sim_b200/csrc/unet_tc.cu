@@ -23,10 +23,11 @@
 // read from shared memory by the tensor core feeds 3x the multiply-adds.
 //
 // Roles (one CTA per SM, persistent over work items = (row tile, cout tile)):
-//   warp 0   TMA producer: per 16-channel chunk, 9 (di, dj) slabs x 2 halves
-//            of 8 channels, each a {8 channels x 128 rows} box, into a ring of
-//            shared-memory stages (full / empty mbarriers); streams the chunk's
-//            weights too when they do not stay resident;
+//   warp 0   TMA producer: per 16-channel chunk, 9 (di, dj) slabs, each a
+//            {16 channels x 128 rows} box (32-byte rows, one sector each) with
+//            the 32-byte swizzle, into a ring of shared-memory stages (full /
+//            empty mbarriers); streams the chunk's weights too when they do
+//            not stay resident;
 //   warp 1   TMEM allocator and MMA issuer (one thread): 9 MMAs
 //            (M = 128, N = 3 cout_tile, K = 16) per chunk into one of two TMEM
 //            accumulators, tcgen05.commit to release stages and to hand the
@@ -37,12 +38,13 @@
 // BSP_ERR_TIMEOUT in a device flag, drains its outstanding copies and MMAs
 // (bounded), frees its TMEM and returns.
 //
-// Shared-memory operand layout (K-major, no swizzle): a "core matrix" is 8
-// rows x 16 bytes (8 BF16 of K) stored as 128 contiguous bytes.  Each
-// 8-channel half of a slab is 128 rows x 16 B, rows contiguous, so the
-// descriptor uses stride-byte-offset 128 (next 8-row group) and
-// leading-byte-offset = distance between the two K halves.  The weights of a
-// (di, dj, chunk) are laid out the same way: N rows x 16 B per half.
+// Shared-memory operand layouts (K-major).  Activations: a slab is 128 rows
+// x 32 bytes (16 channels), written by TMA with the 32-byte swizzle and read
+// by the MMA through a 32-byte-swizzle descriptor (8-row groups 256 bytes
+// apart).  Weights (no swizzle): a "core matrix" is 8 rows x 16 bytes (8 BF16
+// of K) stored as 128 contiguous bytes; each 8-channel half of a (di, dj,
+// chunk) block is N rows x 16 B, so its descriptor uses stride-byte-offset 128
+// and leading-byte-offset = the distance between the two K halves.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -61,11 +63,12 @@ namespace utc {
 constexpr int M = 128;          // window rows per tile (TMEM lanes)
 constexpr int MOUT = 126;       // outputs per tile
 constexpr int THREADS = 192;    // 6 warps
-constexpr int SLAB_HALF = M * 16;          // bytes of one 8-channel half of a slab
-constexpr int A_STAGE = 9 * 2 * SLAB_HALF; // 36,864 bytes per 16-channel chunk
+constexpr int SLAB = M * 32;               // one (di, dj) slab: 128 rows x 16 channels
+constexpr int A_STAGE = 9 * SLAB;          // 36,864 bytes per 16-channel chunk
 constexpr int SMEM_MAX = 232448;           // dynamic shared memory per CTA (227 KB)
 constexpr int SMEM_MIN = 120 * 1024;       // keep one CTA per SM (TMEM is not shared)
 constexpr int WRES_MAX = 112 * 1024;       // weights stay resident up to this size
+__host__ __device__ constexpr int round1k(int b) { return (b + 1023) / 1024 * 1024; }
 
 __device__ int g_utc_err;  // BSP_ERR_TIMEOUT once any wait of this kernel gave up
 
@@ -174,6 +177,15 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
   return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | ((uint64_t)1 << 46);
 }
+// The same for the activation slabs, written by TMA with the 32-byte swizzle:
+// rows of 32 bytes (the 16 channels of one K step), 8-row groups 256 bytes
+// apart, layout type 6 (32-byte swizzle) in bits 61-63; the leading byte
+// offset is not used by swizzled K-major layouts (encoded as 1).  The slab
+// base is 1024-byte aligned so the swizzle pattern starts with it.
+__device__ __forceinline__ uint64_t sdesc_sw32(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(256 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)6 << 61);
+}
 // Instruction descriptor of kind::f16: FP32 accumulate (bits 4-5 = 1), BF16
 // A and B (bits 7-9, 10-12 = 1), both K-major, N >> 3 in bits 17-22,
 // M >> 4 in bits 24-28.
@@ -206,11 +218,14 @@ __global__ void __launch_bounds__(THREADS, 1) conv_tc_kernel(
   const int ncol = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
   const int nchunk = p.cin >> 4;
   const int wchunk = p.w_bytes_chunk;
-  // layout: [weights (resident: all chunks; else none)] [stages] [Ctl]
-  unsigned char *wres = smem;
-  const int wres_bytes = p.resident ? wchunk * nchunk : 0;
-  const int stage_bytes = A_STAGE + (p.resident ? 0 : wchunk);
-  unsigned char *stages = smem + wres_bytes;
+  // layout (from a 1024-byte aligned base): [weights (resident: all chunks;
+  // else none)] [stages] [Ctl]; weights and stages padded to 1024 bytes
+  unsigned char *base0 = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(smem) + 1023) & ~(uintptr_t)1023);
+  unsigned char *wres = base0;
+  const int wres_bytes = p.resident ? round1k(wchunk * nchunk) : 0;
+  const int stage_bytes = round1k(A_STAGE + (p.resident ? 0 : wchunk));
+  unsigned char *stages = base0 + wres_bytes;
   Ctl *c = reinterpret_cast<Ctl *>(stages + (size_t)p.nst * stage_bytes);
   const int64_t nwork = p.ntiles * p.nct;
 
@@ -270,8 +285,7 @@ __global__ void __launch_bounds__(THREADS, 1) conv_tc_kernel(
           for (int sl = 0; sl < 9; ++sl) {
             const int di = sl / 3 - 1, dj = sl % 3 - 1;
             const int y = (int)(base + di * P + dj * R);
-            tma_load2(st + (sl * 2 + 0) * SLAB_HALF, &amap, kc * 16, y, &c->full[s]);
-            tma_load2(st + (sl * 2 + 1) * SLAB_HALF, &amap, kc * 16 + 8, y, &c->full[s]);
+            tma_load2(st + sl * SLAB, &amap, kc * 16, y, &c->full[s]);
           }
           if (!p.resident)
             bulk_load(st + A_STAGE,
@@ -314,7 +328,7 @@ __global__ void __launch_bounds__(THREADS, 1) conv_tc_kernel(
           const uint32_t abase = smem_u32(st), bbase = smem_u32(wb);
 #pragma unroll 1
           for (int sl = 0; sl < 9; ++sl) {
-            const uint64_t ad = sdesc(abase + sl * 2 * SLAB_HALF, SLAB_HALF, 128);
+            const uint64_t ad = sdesc_sw32(abase + sl * SLAB);
             const uint64_t bd = sdesc(bbase + sl * 2 * N * 16, N * 16, 128);
             tc_mma(dt, ad, bd, idesc, (kc > 0 || sl > 0) ? 1u : 0u);
           }
@@ -680,6 +694,63 @@ __global__ void rms_final_kernel(float *__restrict__ s_out, const double *__rest
   s_out[0] = r > 0.0 ? (float)r : 1.0f;
 }
 
+// Energy-optimal scale of a starting pressure: with b = factor div on fluid
+// cells, gamma = (b . p) / (p . A p) minimises ||p* - gamma p||_A, so the
+// scaled guess is never farther from the solution than zero in the A-norm.
+// Partials of (b . p, p . Ap) per block in FP64, fixed order.
+__global__ void __launch_bounds__(256) energy_partial_kernel(double *__restrict__ part,
+                                                             const float *__restrict__ p,
+                                                             const float *__restrict__ Ap,
+                                                             const float *__restrict__ div,
+                                                             const uint8_t *__restrict__ mask,
+                                                             int64_t n, float factor) {
+  __shared__ double sh[2][8];
+  double a = 0.0, c = 0.0;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (int64_t)gridDim.x * blockDim.x)
+    if (mask[v] & BSP_CLASS_FLUID) {
+      const double pv = p[v];
+      a += (double)(factor * div[v]) * pv;
+      c += pv * (double)Ap[v];
+    }
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    sh[0][threadIdx.x >> 5] = a;
+    sh[1][threadIdx.x >> 5] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sa = 0.0, sc = 0.0;
+    for (int w = 0; w < 8; ++w) {
+      sa += sh[0][w];
+      sc += sh[1][w];
+    }
+    part[2 * blockIdx.x] = sa;
+    part[2 * blockIdx.x + 1] = sc;
+  }
+}
+// gamma from the partials (0 when p . A p is not positive), then p *= gamma.
+__global__ void energy_scale_kernel(float *__restrict__ p, const double *__restrict__ part,
+                                    int nb, int64_t n, float *__restrict__ gamma_out) {
+  __shared__ float g;
+  if (threadIdx.x == 0) {
+    double a = 0.0, c = 0.0;
+    for (int b = 0; b < nb; ++b) {
+      a += part[2 * b];
+      c += part[2 * b + 1];
+    }
+    g = (c > 0.0 && a == a) ? (float)(a / c) : 0.0f;
+    if (blockIdx.x == 0 && gamma_out) *gamma_out = g;
+  }
+  __syncthreads();
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (int64_t)gridDim.x * blockDim.x)
+    p[v] *= g;
+}
+
 inline int grid_for(int64_t n, int threads = 256) {
   int64_t b = (n + threads - 1) / threads;
   return (int)(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16);
@@ -690,10 +761,10 @@ static bool encode_rows(CUtensorMap *m, const void *base, int c, int64_t rows) {
   if (!fn || ((uintptr_t)base & 15u)) return false;
   const cuuint64_t dims[2] = {(cuuint64_t)c, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)c * 2};
-  const cuuint32_t box[2] = {8, (cuuint32_t)M};
+  const cuuint32_t box[2] = {16, (cuuint32_t)M};  // 32-byte rows: one sector each
   const cuuint32_t es[2] = {1, 1};
   return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(base), dims, strides, box,
-            es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_32B,
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -765,12 +836,12 @@ extern "C" int bsp_unet_tc_conv3(bsp_bf16_t *out, const bsp_bf16_t *in, const bs
   const int wtotal = p.w_bytes_chunk * nchunk;
   const int ctl = (int)((sizeof(Ctl) + 127) / 128 * 128);
   p.resident = (p.nct == 1 && wtotal <= WRES_MAX) ? 1 : 0;
-  const int stage = A_STAGE + (p.resident ? 0 : p.w_bytes_chunk);
-  const int avail = SMEM_MAX - ctl - (p.resident ? wtotal : 0);
+  const int stage = round1k(A_STAGE + (p.resident ? 0 : p.w_bytes_chunk));
+  const int avail = SMEM_MAX - 1024 - ctl - (p.resident ? round1k(wtotal) : 0);
   p.nst = avail / stage;
   if (p.nst > 8) p.nst = 8;
   if (p.nst < 2) return BSP_ERR_SHAPE;
-  int bytes = (p.resident ? wtotal : 0) + p.nst * stage + ctl;
+  int bytes = 1024 + (p.resident ? round1k(wtotal) : 0) + p.nst * stage + ctl;
   if (bytes < SMEM_MIN) bytes = SMEM_MIN;
   CUtensorMap amap;
   if (!encode_rows(&amap, in, cin, rows)) return BSP_ERR_ARG;
@@ -873,5 +944,23 @@ extern "C" int bsp_unet_prolong(float *p, const float *pc, const uint8_t *mask, 
   if ((const void *)p == (const void *)pc) return BSP_ERR_ALIAS;
   ProfScope ps(PROF_UNET, s);
   prolong_kernel<<<grid_for((int64_t)nx * ny * nz), 256, 0, s>>>(p, pc, mask, nx, ny, nz);
+  return (int)cudaGetLastError();
+}
+
+extern "C" int bsp_unet_energy_scale(float *p, const float *Ap, const float *div,
+                                     const uint8_t *mask, int nx, int ny, int nz, float factor,
+                                     void *workspace, size_t workspace_bytes, float *gamma_dev,
+                                     cudaStream_t s) {
+  if (!p || !Ap || !div || !mask || !workspace) return BSP_ERR_NULL;
+  if (workspace_bytes < bsp_unet_scale_workspace_bytes() || ((uintptr_t)workspace & 7u))
+    return BSP_ERR_WORKSPACE;
+  if ((const void *)p == (const void *)Ap) return BSP_ERR_ALIAS;
+  const int64_t n = (int64_t)nx * ny * nz;
+  if (n <= 0) return BSP_OK;
+  ProfScope ps(PROF_UNET, s);
+  energy_partial_kernel<<<RMS_BLOCKS, 256, 0, s>>>(static_cast<double *>(workspace), p, Ap, div,
+                                                   mask, n, factor);
+  energy_scale_kernel<<<grid_for(n), 256, 0, s>>>(p, static_cast<const double *>(workspace),
+                                                  RMS_BLOCKS, n, gamma_dev);
   return (int)cudaGetLastError();
 }

@@ -66,7 +66,7 @@ extern "C" {
  * coarse-cycle grid barrier's error word set, as a barrier that gave up
  * leaves it (that solve returns BSP_ERR_TIMEOUT; the key clears itself). */
 #define BSP_TUNE_TEST_BARRIER_ERROR 11
-#define BSP_TUNE_COARSE_PHASES 12 /* coarse cycle forms t where it is read: 1 on (default), 0 off */
+#define BSP_TUNE_COARSE_PHASES 12 /* coarse cycle forms t where it is read: 1 on, 0 off (default) */
 #define BSP_TUNE_COARSE_TRACE 13  /* tracing: coarse-cycle launches stamp their phase boundaries */
 
 /* ------------------------------------------------------------------ */
@@ -596,6 +596,16 @@ int bsp_unet_restrict_div(float *divc, const uint8_t *maskc, const float *div,
                           const uint8_t *mask, int nx, int ny, int nz, cudaStream_t stream);
 int bsp_unet_prolong(float *p, const float *pc, const uint8_t *mask, int nx, int ny, int nz,
                      cudaStream_t stream);
+
+/* Energy-optimal scale of a starting pressure p (in place): with b = factor
+ * div on fluid cells (factor = -rho dx^2 / dt) and Ap = A p (bsp_spmv),
+ * p *= gamma = (b . p) / (p . A p), which minimises the A-norm error of
+ * gamma p, so the scaled guess is never worse than starting from zero (gamma
+ * = 0 when p . A p <= 0).  FP64 sums in a fixed order in a workspace of
+ * bsp_unet_scale_workspace_bytes(); gamma_dev (optional) receives gamma. */
+int bsp_unet_energy_scale(float *p, const float *Ap, const float *div, const uint8_t *mask,
+                          int nx, int ny, int nz, float factor, void *workspace,
+                          size_t workspace_bytes, float *gamma_dev, cudaStream_t stream);
 
 /* Exhaustive self-check of the device division-by-6 against IEEE division
  * over all 2^32 float bit patterns; the mismatch count is written to the

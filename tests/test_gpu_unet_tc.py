@@ -217,3 +217,41 @@ def test_tc_forward_matches_training_forward_and_oracle(cuda, dims):
     # repeated runs on the same plan give the same bits (buffers reused)
     p2 = net.predict(div, mask, 0.002, 0.01, 997.0, backend="tc")
     assert torch.equal(p2, p_tc)
+
+
+def test_energy_scale_of_a_guess(cuda):
+    """bsp_unet_energy_scale multiplies a starting pressure by
+    gamma = (b . p) / (p . A p), the scale that minimises the A-norm error; the
+    scaled guess is then no farther from the solution than zero."""
+    import oracle as O
+    from boilingsim_b200 import fluid as F
+
+    spec = S.PotSpec(32, 32, 24, r_in=13, t_w=2, water_line=19, carrot_r=3, carrot_len=12)
+    mat = S.pot_mat(spec)
+    ux, uy, uz = S.velocity_field(mat, seed=2)
+    dx, dt, rho = 0.002, 0.01, 997.0
+    div = O.divergence(ux, uy, uz, mat, dx)
+    rng = np.random.default_rng(3)
+    p = np.where(mat == 0, rng.standard_normal(mat.shape), 0.0).astype(np.float32)
+    mask = F.cell_mask(torch.as_tensor(mat).cuda())
+    pd, dd = torch.as_tensor(p).cuda(), torch.as_tensor(div).cuda()
+    Ap = torch.empty_like(pd)
+    call("bsp_spmv", ptr(Ap), ptr(pd), ptr(mask), *mat.shape, 0)
+    ws = torch.empty(int(_lib.lib().bsp_unet_scale_workspace_bytes()) // 8 + 1,
+                     dtype=torch.float64, device="cuda")
+    g = torch.zeros(1, device="cuda")
+    factor = -(rho * dx * dx / dt)
+    call("bsp_unet_energy_scale", ptr(pd), ptr(Ap), ptr(dd), ptr(mask), *mat.shape, factor,
+         ptr(ws), ws.numel() * 8, ptr(g), 0)
+    got = pd.cpu().numpy()
+    fl = mat == 0
+    b = np.where(fl, np.float32(factor) * div, 0.0).astype(np.float64)
+    Ap64 = Ap.cpu().numpy().astype(np.float64)
+    gamma = float((b * p).sum() / (p.astype(np.float64) * Ap64).sum())
+    assert abs(float(g.item()) - gamma) <= 1e-5 * abs(gamma)
+    assert np.allclose(got, p * np.float32(g.item()), rtol=0, atol=0)
+    # A-norm error of the scaled guess against the FP64 solution <= that of zero
+    pstar, _, _ = O.solve_f64(div, mat, dx, dt, rho, tol=1e-12)
+    e = got.astype(np.float64) - pstar
+    anorm = lambda v: float(v @ O.apply_A_f64(v.reshape(mat.shape), mat).ravel())  # noqa: E731
+    assert anorm(e.ravel()) <= anorm(pstar.ravel())
