@@ -77,6 +77,8 @@ struct CoarseCycle {
   int fused_phases;   // 1: t formed where it is read (fewer phases and grid barriers)
   unsigned long long *trace;  // optional: CTA 0's %globaltimer at each phase boundary
   int cinv_bytes;     // > 0: CTA 0 copies the dense inverse into shared memory at launch
+  int tail_smem;      // 1: the levels CTA 0 runs alone live in its shared memory
+  int tail_off;       // byte offset of that region in the dynamic shared memory
 };
 
 // Dynamic shared memory of the coarse-cycle kernel: [dense inverse (CTA 0)]
@@ -129,8 +131,10 @@ __device__ __forceinline__ float4 st4t(T *p, int64_t c, float4 v) {
   cs(p, c + 3, v.w);
   return make_float4(cl_round(v.x, p), cl_round(v.y, p), cl_round(v.z, p), cl_round(v.w, p));
 }
+// Mask loads are plain (generic) loads: the small levels may live in shared
+// memory (the tail staged by CTA 0), where the read-only global path cannot go.
 __device__ __forceinline__ uint32_t ldm4(const uint8_t *m, int64_t c) {
-  return __ldg(reinterpret_cast<const uint32_t *>(m + c));
+  return *reinterpret_cast<const uint32_t *>(m + c);
 }
 __device__ __forceinline__ float fl_mask(float v, uint32_t mw, int q) {
   return ((mw >> (8 * q)) & BSP_MFLUID) ? v : 0.0f;
@@ -305,7 +309,7 @@ __device__ __forceinline__ float4 t_down4(const Level<T> &f, int64_t c, const fl
 }
 template <class T>
 __device__ __forceinline__ float t_down1(const Level<T> &f, int64_t c, const float *wtab) {
-  const uint32_t m = __ldg(f.mask + c);
+  const uint32_t m = f.mask[c];
   return (m & BSP_MFLUID) ? cl(f.r, c) * cc_w(wtab, m) : 0.0f;
 }
 // t = OMEGA r / D + alpha e[l+1][parent] (U1) of the quad at (i, j, k); 0 off fluid.
@@ -325,7 +329,7 @@ __device__ __forceinline__ float4 t_up4(const Level<T> &f, const Level<T> &co, i
 template <class T>
 __device__ __forceinline__ float t_up1(const Level<T> &f, const Level<T> &co, int i, int j, int k,
                                        int64_t c, const float *wtab, float alpha) {
-  const uint32_t m = __ldg(f.mask + c);
+  const uint32_t m = f.mask[c];
   if (!(m & BSP_MFLUID)) return 0.0f;
   const int64_t P = ((int64_t)(i >> 1) * co.ny + (j >> 1)) * co.nz + (k >> 1);
   return fmaf(cl(f.r, c), cc_w(wtab, m), alpha * cl(co.e, P));
@@ -452,8 +456,8 @@ __device__ __forceinline__ float nbr_sum1(const float *t, const Level<T> &f, int
 // output, lanes over the sum, fixed shuffle order), or, without one, damped
 // Jacobi sweeps from zero in the scratch vector.
 template <class T>
-__device__ void coarsest_solve(const CoarseCycle<T> &a, const float *wtab, const float *minv) {
-  const Level<T> &c = a.lv[a.L - 1];
+__device__ void coarsest_solve(const CoarseCycle<T> &a, const Level<T> &c, const float *wtab,
+                               const float *minv) {
   const int n = c.nx * c.ny * c.nz;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   if (*a.cflag) {
@@ -468,7 +472,7 @@ __device__ void coarsest_solve(const CoarseCycle<T> &a, const float *wtab, const
 #pragma unroll 4
       for (int q = lane; q < n; q += 32) acc = fmaf(row[q], rs[q], acc);
       for (int s = 16; s > 0; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s);
-      if (lane == 0) cs(c.e, o, (__ldg(c.mask + o) & BSP_MFLUID) ? acc : 0.0f);
+      if (lane == 0) cs(c.e, o, (c.mask[o] & BSP_MFLUID) ? acc : 0.0f);
     }
     return;
   }
@@ -477,7 +481,7 @@ __device__ void coarsest_solve(const CoarseCycle<T> &a, const float *wtab, const
   __syncthreads();
   for (int sw = 0; sw < CC_COARSE_SWEEPS; ++sw) {
     for (int q = threadIdx.x; q < n; q += blockDim.x) {
-      const uint32_t m = __ldg(c.mask + q);
+      const uint32_t m = c.mask[q];
       float v = 0.0f;
       if (m & BSP_MFLUID) {
         const int k = q % c.nz, j = (q / c.nz) % c.ny, i = q / (c.nz * c.ny);
@@ -566,7 +570,7 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cycle_kernel(CoarseCycle<T> 
         if (s_cok) minv = cc_smem();
         else ok = false;
       }
-      if (ok) coarsest_solve(a, wtab, minv);
+      if (ok) coarsest_solve(a, a.lv[L - 1], wtab, minv);
       __syncthreads();
       mark();
       for (int l = L - 2; l >= tail && l >= 1 && ok; --l) {
@@ -600,7 +604,7 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cycle_kernel(CoarseCycle<T> 
       sync_all();
       phase_d2b(a.lv[l], a.lv[l + 1], a.res, a.scratch, wtab, all);
       sync_all();
-    } else if (blockIdx.x == 0) {
+    } else if (blockIdx.x == 0 && !a.tail_smem) {
       phase_d2a(a.lv[l], a.scratch, a.res, one);
       __syncthreads();
       phase_d2b(a.lv[l], a.lv[l + 1], a.res, a.scratch, wtab, one);
@@ -617,13 +621,75 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cycle_kernel(CoarseCycle<T> 
       if (s_cok2) minv = cc_smem();
       else ok = false;
     }
-    if (ok) coarsest_solve(a, wtab, minv);
-    __syncthreads();
-    for (int l = L - 2; l >= tail && l >= 1; --l) {
-      phase_u1(a.lv[l], a.lv[l + 1], a.scratch, wtab, a.alpha, one);
+    if (ok && a.tail_smem) {
+      // The small levels in shared memory: masks and the tail level's
+      // right-hand side copied in, every phase of the tail on-chip, the tail
+      // level's correction copied back out for the big levels' up phases.
+      Level<T> sv[MAX_LEVELS];
+      unsigned char *sp = reinterpret_cast<unsigned char *>(cc_smem()) + a.tail_off;
+      auto take = [&](int64_t b) {
+        unsigned char *q = sp;
+        sp += (b + 15) / 16 * 16;
+        return q;
+      };
+      for (int l = tail; l < L; ++l) {
+        const int64_t nl = cells(l);
+        sv[l] = a.lv[l];
+        sv[l].mask = take(nl);
+        sv[l].r = reinterpret_cast<T *>(take(nl * (int64_t)sizeof(T)));
+        sv[l].e = reinterpret_cast<T *>(take(nl * (int64_t)sizeof(T)));
+        const uint32_t *gm = reinterpret_cast<const uint32_t *>(a.lv[l].mask);
+        uint32_t *smk = reinterpret_cast<uint32_t *>(const_cast<uint8_t *>(sv[l].mask));
+        for (int64_t q = threadIdx.x; q < nl / 4; q += blockDim.x) smk[q] = gm[q];
+      }
+      float *ts = reinterpret_cast<float *>(take(cells(tail) * 4));
+      float *rs = reinterpret_cast<float *>(take(cells(tail) * 4));
+      {
+        const int64_t nb = cells(tail) * (int64_t)sizeof(T) / 8;  // 8-byte words
+        const uint2 *g = reinterpret_cast<const uint2 *>(a.lv[tail].r);
+        uint2 *d = reinterpret_cast<uint2 *>(sv[tail].r);
+        for (int64_t q = threadIdx.x; q < nb; q += blockDim.x) d[q] = g[q];
+      }
       __syncthreads();
-      phase_u2(a.lv[l], a.scratch, wtab, one);
+      mark();
+      if (tail + 1 < L) {
+        phase_d1(sv[tail], ts, wtab, one);
+        __syncthreads();
+      }
+      for (int l = tail; l + 1 < L; ++l) {
+        phase_d2a(sv[l], ts, rs, one);
+        __syncthreads();
+        phase_d2b(sv[l], sv[l + 1], rs, ts, wtab, one);
+        __syncthreads();
+      }
+      mark();
+      coarsest_solve(a, sv[L - 1], wtab, minv);
       __syncthreads();
+      mark();
+      for (int l = L - 2; l >= tail; --l) {
+        phase_u1(sv[l], sv[l + 1], ts, wtab, a.alpha, one);
+        __syncthreads();
+        phase_u2(sv[l], ts, wtab, one);
+        __syncthreads();
+      }
+      {
+        const int64_t nb = cells(tail) * (int64_t)sizeof(T) / 8;
+        const uint2 *g = reinterpret_cast<const uint2 *>(sv[tail].e);
+        uint2 *d = reinterpret_cast<uint2 *>(a.lv[tail].e);
+        for (int64_t q = threadIdx.x; q < nb; q += blockDim.x) d[q] = g[q];
+      }
+      __threadfence();
+      __syncthreads();
+      mark();
+    } else {
+      if (ok) coarsest_solve(a, a.lv[L - 1], wtab, minv);
+      __syncthreads();
+      for (int l = L - 2; l >= tail && l >= 1; --l) {
+        phase_u1(a.lv[l], a.lv[l + 1], a.scratch, wtab, a.alpha, one);
+        __syncthreads();
+        phase_u2(a.lv[l], a.scratch, wtab, one);
+        __syncthreads();
+      }
     }
   }
   // ---- up through the big levels
@@ -652,6 +718,11 @@ bool g_coarse_phases_fused = false;
 // BSP_TUNE_COARSE_TRACE: 1 makes every coarse-cycle launch record CTA 0's
 // %globaltimer at each phase boundary (bsp_coarse_trace_read); tracing only.
 bool g_coarse_trace = false;
+// BSP_TUNE_COARSE_TAIL: 1 (default) runs the levels CTA 0 handles alone out of
+// its shared memory (masks, right-hand sides, corrections and scratch copied
+// in, the top one's correction copied out); 0 keeps them in global memory.
+// The results are the same bits.
+bool g_coarse_tail_smem = true;
 
 // FP32 scratch of the coarse-cycle kernel: t (max(cells of level 1, 3 x cells
 // of the coarsest level), rounded up to 64 floats) followed by res (cells of
@@ -707,24 +778,43 @@ bool launch_coarse_cycle(const Level<T> *lv, int L, float *scratch, const float 
   a.ctl = reinterpret_cast<GridCtl *>(ctl);
   a.alpha = alpha;
   a.fused_phases = g_coarse_phases_fused ? 1 : 0;
-  // the dense inverse of the coarsest level goes to CTA 0's shared memory when
-  // it is small (<= 96 KB); the copy size is rounded up to 16 bytes (the
-  // inverse's workspace slot is 256-byte aligned and at least that long)
+  // CTA 0's dynamic shared memory: [dense inverse of the coarsest level, when
+  // small (<= 96 KB)] [coarsest right-hand side: COARSEST_CELLS floats]
+  // [mbarrier, 16 B] [the tail levels CTA 0 runs alone: masks, r, e of each,
+  // then two FP32 vectors of the first tail level].  The inverse's copy size
+  // is rounded up to 16 bytes (its workspace slot is 256-byte aligned and at
+  // least that long).  The tail goes on-chip when it fits; the inverse when
+  // what is left allows.
   const int64_t nc = (int64_t)lv[L - 1].nx * lv[L - 1].ny * lv[L - 1].nz;
-  a.cinv_bytes = 0;
-  size_t dyn = 0;
-  if (nc <= COARSEST_CELLS && nc * nc * 4 <= 96 * 1024 && ((uintptr_t)cinv & 15u) == 0) {
-    a.cinv_bytes = (int)((nc * nc * 4 + 15) / 16 * 16);
-    dyn = (size_t)a.cinv_bytes + COARSEST_CELLS * sizeof(float) + 16;
-  } else {
-    dyn = COARSEST_CELLS * sizeof(float) + 16;
+  auto r16 = [](int64_t b) { return (b + 15) / 16 * 16; };
+  int tail = 1;
+  while (tail < L && (int64_t)lv[tail].nx * lv[tail].ny * lv[tail].nz > TAIL_CELLS) ++tail;
+  int64_t tail_bytes = 0;
+  if (tail < L) {
+    for (int l = tail; l < L; ++l) {
+      const int64_t nl = (int64_t)lv[l].nx * lv[l].ny * lv[l].nz;
+      tail_bytes += r16(nl) + 2 * r16(nl * (int64_t)sizeof(T));
+    }
+    const int64_t nt = (int64_t)lv[tail].nx * lv[tail].ny * lv[tail].nz;
+    tail_bytes += 2 * r16(nt * 4);
   }
+  const int64_t base = COARSEST_CELLS * (int64_t)sizeof(float) + 16;
+  const int64_t cinv_b = (nc <= COARSEST_CELLS && nc * nc * 4 <= 96 * 1024 &&
+                          ((uintptr_t)cinv & 15u) == 0)
+                             ? r16(nc * nc * 4)
+                             : 0;
+  constexpr int64_t DYN_MAX = 200 * 1024;
+  bool use_tail = g_coarse_tail_smem && tail < L && tail_bytes + base <= DYN_MAX;
+  a.cinv_bytes = (int)((use_tail ? tail_bytes : 0) + base + cinv_b <= DYN_MAX ? cinv_b : 0);
+  size_t dyn = (size_t)(a.cinv_bytes + base + (use_tail ? tail_bytes : 0));
   // one opt-in per device at the largest size this launcher ever asks for
-  constexpr int DYN_MAX = 96 * 1024 + 16 + COARSEST_CELLS * (int)sizeof(float) + 16;
-  if (dyn > 48 * 1024 && !smem_opt_in((const void *)mg_cycle_kernel<T>, DYN_MAX)) {
+  if (dyn > 48 * 1024 && !smem_opt_in((const void *)mg_cycle_kernel<T>, (int)DYN_MAX)) {
     a.cinv_bytes = 0;
-    dyn = COARSEST_CELLS * sizeof(float) + 16;
+    use_tail = false;
+    dyn = (size_t)base;
   }
+  a.tail_smem = use_tail ? 1 : 0;
+  a.tail_off = (int)(a.cinv_bytes + base);
   a.trace = nullptr;
   if (g_coarse_trace && cudaGetSymbolAddress((void **)&a.trace, g_cc_trace) != cudaSuccess)
     a.trace = nullptr;

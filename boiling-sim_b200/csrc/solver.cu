@@ -54,6 +54,7 @@ float g_mg_alpha = 1.0f;
 extern bool g_fine_tma_enabled;      // BSP_TUNE_FINE_TMA (mgfine.cu)
 extern bool g_coarse_fused_enabled;  // BSP_TUNE_COARSE_FUSED (mgcoarse.cu)
 extern bool g_coarse_phases_fused;   // BSP_TUNE_COARSE_PHASES (mgcoarse.cu)
+extern bool g_coarse_tail_smem;      // BSP_TUNE_COARSE_TAIL (mgcoarse.cu)
 // BSP_TUNE_FUSE_UPDATE: CG update fused into the next level-0 restriction
 bool g_fuse_update_enabled = true;
 // BSP_TUNE_TEST_BARRIER_ERROR (tests only): the next host-driven solve starts
@@ -1477,6 +1478,7 @@ static void key_params(GraphKey &k, const BspSolveParams *p) {
   k.v.push_back((uintptr_t)g_fine_tma_enabled);
   k.v.push_back((uintptr_t)g_coarse_fused_enabled);
   k.v.push_back((uintptr_t)g_coarse_phases_fused);
+  k.v.push_back((uintptr_t)g_coarse_tail_smem);
   k.v.push_back((uintptr_t)g_fuse_update_enabled);
   k.v.push_back((uintptr_t)g_fine_bi);
 }

@@ -507,6 +507,7 @@ extern int g_sweep_tblock;
 extern bool g_test_barrier_error;
 extern bool g_coarse_phases_fused;
 extern bool g_coarse_trace;
+extern bool g_coarse_tail_smem;
 namespace cond {
 extern int g_cond_bi;
 extern bool g_cond_tma;
@@ -558,6 +559,10 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_COARSE_PHASES:
       if (value < 0 || value > 1) return BSP_ERR_ARG;
       bsp::g_coarse_phases_fused = value != 0;
+      return BSP_OK;
+    case BSP_TUNE_COARSE_TAIL:
+      if (value < 0 || value > 1) return BSP_ERR_ARG;
+      bsp::g_coarse_tail_smem = value != 0;
       return BSP_OK;
     case BSP_TUNE_COARSE_TRACE:
       if (value < 0 || value > 1) return BSP_ERR_ARG;

@@ -68,6 +68,7 @@ extern "C" {
 #define BSP_TUNE_TEST_BARRIER_ERROR 11
 #define BSP_TUNE_COARSE_PHASES 12 /* coarse cycle forms t where it is read: 1 on, 0 off (default) */
 #define BSP_TUNE_COARSE_TRACE 13  /* tracing: coarse-cycle launches stamp their phase boundaries */
+#define BSP_TUNE_COARSE_TAIL 14   /* coarse levels of CTA 0 in shared memory: 1 on (default), 0 off */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */

@@ -224,3 +224,28 @@ def test_coarse_cycle_fused_phases_bit_identical(cuda, size):
     assert out[0][1] == out[1][1]
     assert np.array_equal(out[0][0], out[1][0])
     assert O.rel_residual64(out[1][0], div, mat, DX, DT, RHO) <= 1.0001e-6
+
+
+@pytest.mark.parametrize("storage,size", [("fp16", 96), ("fp32", 192), ("bf16", 192)])
+def test_coarse_cycle_tail_in_shared_memory_bit_identical(cuda, storage, size):
+    """The levels CTA 0 runs alone, staged in its shared memory
+    (BSP_TUNE_COARSE_TAIL = 1, the default), give the same bits as the same
+    phases on global memory (= 0)."""
+    from boilingsim_b200 import _lib
+
+    spec = S.PotSpec(size, size, size * 2 // 3, r_in=size / 2 - 4, t_w=3,
+                     water_line=size * 0.45, carrot_r=5, carrot_len=size // 3)
+    mat = S.pot_mat(spec)
+    ux, uy, uz = S.velocity_field(mat, seed=9)
+    div = O.divergence(ux, uy, uz, mat, DX)
+    out = {}
+    try:
+        for tail in (0, 1):
+            _lib.call("bsp_set_tuning", 14, tail)
+            res = solve_tolerance(div, mat, DX, DT, RHO, tol=1e-6, storage=storage)
+            out[tail] = (res.p64.copy(), res.inner_iterations)
+    finally:
+        _lib.call("bsp_set_tuning", 14, 1)
+    assert out[0][1] == out[1][1]
+    assert np.array_equal(out[0][0], out[1][0])
+    assert O.rel_residual64(out[1][0], div, mat, DX, DT, RHO) <= 1.0001e-6
