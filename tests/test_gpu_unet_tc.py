@@ -255,3 +255,40 @@ def test_energy_scale_of_a_guess(cuda):
     e = got.astype(np.float64) - pstar
     anorm = lambda v: float(v @ O.apply_A_f64(v.reshape(mat.shape), mat).ravel())  # noqa: E731
     assert anorm(e.ravel()) <= anorm(pstar.ravel())
+
+
+@pytest.mark.parametrize("mode", ["full", "coarse"])
+def test_warm_start_guess_graph_and_solve(cuda, mode):
+    """WarmStart.guess: the CUDA-graph replay gives the same bits as the eager
+    launches; the guess is zero off fluid, scaled so that it is no farther
+    from the solution than zero in the A-norm, and the solve started from it
+    meets the FP64 tolerance."""
+    import oracle as O
+    from boilingsim_b200 import fluid as F
+    from boilingsim_b200.solver import TolSolver
+
+    mat = S.pot_mat(S.POT_64)
+    ux, uy, uz = S.velocity_field(mat, seed=5)
+    dx, dt, rho = 0.002, 0.01, 997.0
+    div = O.divergence(ux, uy, uz, mat, dx)
+    mat_t = torch.as_tensor(mat).cuda()
+    mask = F.cell_mask(mat_t)
+    dd = torch.as_tensor(div).cuda()
+    ws = LR.WarmStart(LR.UNet.load(), mat_t, mask, mode=mode)
+    a = torch.empty_like(dd)
+    b = torch.empty_like(dd)
+    ws.guess(dd, dx, dt, rho, out=a, graph=False)
+    ws.guess(dd, dx, dt, rho, out=b, graph=True)
+    ws.guess(dd, dx, dt, rho, out=b, graph=True)  # replay
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+    g = a.cpu().numpy()
+    assert np.isfinite(g).all() and np.all(g[mat != 0] == 0.0)
+    pstar, _, _ = O.solve_f64(div, mat, dx, dt, rho, tol=1e-12)
+    e = g.astype(np.float64) - pstar
+    anorm = lambda v: float((v * O.apply_A_f64(v, mat)).sum())  # noqa: E731
+    assert anorm(e) <= anorm(pstar) * (1 + 1e-6)
+    solver = TolSolver(mask, "fp16")
+    res = solver.solve(dd, dx, dt, rho, tol=1e-6, p=a.clone(), warm_start=True)
+    assert res.status == 0
+    assert O.rel_residual64(res.p64, div, mat, dx, dt, rho) <= 1.0001e-6
