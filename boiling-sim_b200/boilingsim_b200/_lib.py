@@ -104,6 +104,7 @@ SIGNATURES = {
     "bsp_unet_tc_weights": (_I, [_P, _P, _I, _I, _P]),
     "bsp_unet_tc_conv3": (_I, [_P, _P, _P, _P, _P, _I, _I, _I, _I, _I, _I, _P]),
     "bsp_unet_tc_error": (_I, [_P]),
+    "bsp_unet_tc_trace": (_I, [_P, _I]),
     "bsp_unet_tc_pack": (_I, [_P, _P, _P, _I, _I, _I, _P, _P]),
     "bsp_unet_scale_workspace_bytes": (ctypes.c_size_t, []),
     "bsp_unet_input_scale": (_I, [_P, _P, _P, _I, _I, _I, _P, ctypes.c_size_t, _P]),

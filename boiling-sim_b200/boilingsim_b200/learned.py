@@ -23,6 +23,7 @@ sum (y - t)^2 / sum t^2 over fluid cells, so every scene weighs the same.
 """
 from __future__ import annotations
 
+import ctypes
 import math
 import os
 from dataclasses import dataclass
@@ -410,6 +411,53 @@ class TcPlan:
             call("bsp_unet_tc_weights", ptr(self.wimg[L.name]), ptr(L.wb), L.cin, L.cout, st)
         self.version = self.net.step
 
+    # the convolutions of one forward pass: (output, input, layer, level, skip)
+    CONVS = (("a1", "x0", "e1a", 0, None), ("e1", "a1", "e1b", 0, None),
+             ("a2", "p1", "e2a", 1, None), ("e2", "a2", "e2b", 1, None),
+             ("a3", "p2", "e3a", 2, None), ("e3", "a3", "e3b", 2, None),
+             ("a4", "p3", "bta", 3, None), ("b4", "a4", "btb", 3, None),
+             ("c3", "q3", "u3a", 2, "e3"), ("u3", "c3", "u3b", 2, None),
+             ("c2", "q2", "u2a", 1, "e2"), ("u2", "c2", "u2b", 1, None),
+             ("c1", "q1", "u1a", 0, "e1"), ("u1", "c1", "u1b", 0, None))
+
+    def conv_timings(self, layers=None, reps: int = 10, warmup: int = 2, trace: bool = False):
+        """Per-layer device time of the tensor-core convolutions on this plan's
+        current activations (run() first): CUDA events around ``reps``
+        back-to-back launches after ``warmup`` untimed ones; with ``trace`` the
+        cycle accounting of one more launch (bsp_unet_tc_trace) as fractions
+        of the CTA lifetime."""
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        rows = []
+        for dst, src, name, level, skip in self.CONVS:
+            if layers and name not in layers:
+                continue
+            L = self.net.by[name]
+            for _ in range(warmup):
+                self._conv(dst, src, name, level, skip)
+            row = {"layer": name, "dims": list(self.dims[level]), "cin": L.cin, "cout": L.cout}
+            if reps > 0:
+                e0.record()
+                for _ in range(reps):
+                    self._conv(dst, src, name, level, skip)
+                e1.record()
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1) / reps
+                n = self.dims[level][0] * self.dims[level][1] * self.dims[level][2]
+                row.update(ms=round(ms, 4), TFLOPs=round(2.0 * 27 * L.cin * L.cout * n / ms / 1e9, 1))
+            if trace:
+                tr = np.zeros(8, np.uint64)
+                call("bsp_unet_tc_trace", None, 1)
+                self._conv(dst, src, name, level, skip)
+                torch.cuda.synchronize()
+                call("bsp_unet_tc_trace", tr.ctypes.data, 0)
+                life = max(float(tr[5]), 1.0)
+                keys = ("producer_wait", "mma_wait_stage", "mma_wait_accumulator",
+                        "epilogue_wait", "epilogue_busy", None, None, "mma_busy")
+                row["trace"] = {k: round(float(tr[i]) / life, 3) for i, k in enumerate(keys) if k}
+                row["trace"]["cycles_per_item"] = round(life / max(float(tr[6]), 1.0), 1)
+            rows.append(row)
+        return rows
+
     def _conv(self, dst, src, name, level, skip=None):
         L = self.net.by[name]
         call("bsp_unet_tc_conv3", ptr(self.a[dst]), ptr(self.a[src]), ptr(self.wimg[name]),
@@ -425,26 +473,27 @@ class TcPlan:
              ptr(self.scale_ws), self.scale_ws.numel() * 8, st)
         call("bsp_unet_tc_pack", ptr(self.a["x0"]), ptr(div), ptr(mask), *d[0], ptr(self.s_dev),
              st)
-        self._conv("a1", "x0", "e1a", 0)
-        self._conv("e1", "a1", "e1b", 0)
+        cv = self.CONVS
+        for c in cv[0:2]:
+            self._conv(*c)
         call("bsp_unet_tc_pool", ptr(self.a["p1"]), ptr(self.a["e1"]), *d[0], 16, st)
-        self._conv("a2", "p1", "e2a", 1)
-        self._conv("e2", "a2", "e2b", 1)
+        for c in cv[2:4]:
+            self._conv(*c)
         call("bsp_unet_tc_pool", ptr(self.a["p2"]), ptr(self.a["e2"]), *d[1], 32, st)
-        self._conv("a3", "p2", "e3a", 2)
-        self._conv("e3", "a3", "e3b", 2)
+        for c in cv[4:6]:
+            self._conv(*c)
         call("bsp_unet_tc_pool", ptr(self.a["p3"]), ptr(self.a["e3"]), *d[2], 64, st)
-        self._conv("a4", "p3", "bta", 3)
-        self._conv("b4", "a4", "btb", 3)
+        for c in cv[6:8]:
+            self._conv(*c)
         call("bsp_unet_tc_up", ptr(self.a["q3"]), ptr(self.a["b4"]), *d[2], 128, st)
-        self._conv("c3", "q3", "u3a", 2, skip="e3")     # c3 = relu(conv) + e3
-        self._conv("u3", "c3", "u3b", 2)
+        for c in cv[8:10]:   # c3 = relu(conv) + e3, then u3
+            self._conv(*c)
         call("bsp_unet_tc_up", ptr(self.a["q2"]), ptr(self.a["u3"]), *d[1], 64, st)
-        self._conv("c2", "q2", "u2a", 1, skip="e2")
-        self._conv("u2", "c2", "u2b", 1)
+        for c in cv[10:12]:
+            self._conv(*c)
         call("bsp_unet_tc_up", ptr(self.a["q1"]), ptr(self.a["u2"]), *d[0], 32, st)
-        self._conv("c1", "q1", "u1a", 0, skip="e1")
-        self._conv("u1", "c1", "u1b", 0)
+        for c in cv[12:14]:
+            self._conv(*c)
         p = out if out is not None else torch.empty(d[0], dtype=torch.float32,
                                                     device=self.net.device)
         call("bsp_unet_tc_head", ptr(p), ptr(self.a["u1"]), ptr(self.net.hw), ptr(self.net.hb),
@@ -703,12 +752,44 @@ def main(argv=None):
     import json
     import time
 
-    ap = argparse.ArgumentParser(description="train / evaluate the learned warm start")
-    ap.add_argument("cmd", choices=["train", "eval"])
+    ap = argparse.ArgumentParser(description="train / evaluate the learned warm start; time "
+                                 "its tensor-core convolutions")
+    ap.add_argument("cmd", choices=["train", "eval", "convs"])
     ap.add_argument("--steps", type=int, default=20000)
     ap.add_argument("--out", default=WEIGHTS_PATH)
     ap.add_argument("--weights", default=WEIGHTS_PATH)
+    ap.add_argument("--layers", default="", help="convs: comma-separated layer names (all)")
+    ap.add_argument("--reps", type=int, default=10, help="convs: timed launches per layer")
+    ap.add_argument("--warmup", type=int, default=2, help="convs: untimed launches per layer")
+    ap.add_argument("--trace", action="store_true", help="convs: cycle accounting per layer")
+    ap.add_argument("--epilogue", type=int, default=0,
+                    help="convs: epilogue warpgroups of the convolution kernel (2-4; 0 default)")
     args = ap.parse_args(argv)
+    if args.cmd == "convs":
+        if args.epilogue:
+            call("bsp_set_tuning", 16, args.epilogue)
+        # one forward pass on the 192x192x128 pot (synthetic divergence), then
+        # the convolutions one layer at a time on its activations
+        from .scenes import pot_192, pot_mat
+
+        net = UNet.load(args.weights)
+        src = SceneSource(pot_mat(pot_192(2)))
+        div = src.draw(5, 0.1, 0.002)
+        plan = net.tc_plan(tuple(div.shape))
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        plan.run(div, src.mask, 0.002, 0.01, 997.0)
+        e0.record()
+        plan.run(div, src.mask, 0.002, 0.01, 997.0)
+        e1.record()
+        torch.cuda.synchronize()
+        layers = [x for x in args.layers.split(",") if x]
+        rows = plan.conv_timings(layers, args.reps, args.warmup, args.trace)
+        flag = ctypes.c_int(0)
+        call("bsp_unet_tc_error", ctypes.addressof(flag))
+        print(json.dumps({"dims": list(plan.dims[0]), "forward_ms": round(e0.elapsed_time(e1), 4),
+                          "conv_total_ms": round(sum(r.get("ms", 0.0) for r in rows), 4),
+                          "convs": rows, "timeout_flag": flag.value}))
+        return
     if args.cmd == "train":
         t0 = time.time()
         net = train(args.steps)

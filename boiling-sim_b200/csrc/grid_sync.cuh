@@ -1,12 +1,17 @@
 // grid_sync.cuh -- bounded grid-wide barrier and deterministic FP64 reductions for
 // persistent (cooperatively launched) kernels.
 //
-// The barrier is a sense-free generation counter: each block's thread 0 arrives
-// with an acq_rel fetch_add; the last arrival resets the count and bumps the
-// generation; the others poll the generation.  Every poll loop is bounded: after
-// BAR_SPIN_LIMIT polls the block records BSP_ERR_TIMEOUT in ctl->err and returns
-// false, and every block leaves the kernel at its next barrier once err is set.
-// Cooperative launch guarantees co-residency, so the limit is only a guard.
+// The barrier is a sense-free generation counter: after a CTA barrier, each
+// block's thread 0 makes the block's writes visible (fence.acq_rel.gpu, which
+// is cumulative over what the CTA barrier ordered before it) and arrives with
+// a fetch_add; the last arrival resets the count and publishes the next
+// generation with a release store; the others poll the generation with
+// acquire loads, back to back (no sleep: a sleep's wake-up granularity is
+// longer than the barrier itself).  Every poll loop is bounded by wall time:
+// after BAR_TIMEOUT_NS on the global timer (or BAR_SPIN_LIMIT polls) the block
+// records BSP_ERR_TIMEOUT in ctl->err and returns false, and every block
+// leaves the kernel at its next barrier once err is set.  Cooperative launch
+// guarantees co-residency, so the limit is only a guard.
 #pragma once
 #include <cuda/atomic>
 #include "bsp_common.cuh"
@@ -22,7 +27,14 @@ struct GridCtl {
   int pad[3];
 };
 
-constexpr unsigned int BAR_SPIN_LIMIT = 1u << 24;  // ~2 s of 64 ns sleeps
+constexpr unsigned long long BAR_TIMEOUT_NS = 2000000000ull;  // 2 s
+constexpr unsigned int BAR_SPIN_LIMIT = 1u << 26;              // polls, a second guard
+
+__device__ __forceinline__ unsigned long long gs_global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
 
 __device__ __forceinline__ bool grid_barrier(GridCtl *ctl) {
   __shared__ int s_ok;
@@ -32,24 +44,34 @@ __device__ __forceinline__ bool grid_barrier(GridCtl *ctl) {
     cuda::atomic_ref<unsigned int, cuda::thread_scope_device> cnt(ctl->bar_count);
     cuda::atomic_ref<unsigned int, cuda::thread_scope_device> gen(ctl->bar_gen);
     cuda::atomic_ref<int, cuda::thread_scope_device> err(ctl->err);
-    const unsigned int g = gen.load(cuda::memory_order_acquire);
-    __threadfence();
+    // the generation cannot move before this block arrives, so this is the
+    // generation of the barrier being entered
+    const unsigned int g = gen.load(cuda::memory_order_relaxed);
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
     const unsigned int a = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
     if (a == gridDim.x - 1) {
       cnt.store(0u, cuda::memory_order_relaxed);
-      gen.fetch_add(1u, cuda::memory_order_release);
+      gen.store(g + 1u, cuda::memory_order_release);
     } else {
       unsigned int spins = 0;
+      unsigned long long t0 = 0;
       while (gen.load(cuda::memory_order_acquire) == g) {
-        if (++spins > BAR_SPIN_LIMIT) {
-          err.store(BSP_ERR_TIMEOUT, cuda::memory_order_relaxed);
-          ok = 0;
-          break;
+        if ((++spins & 255u) == 0) {
+          const unsigned long long now = gs_global_ns();
+          if (t0 == 0) t0 = now;
+          if (err.load(cuda::memory_order_relaxed) != 0) {  // another block gave up
+            ok = 0;
+            break;
+          }
+          if (now - t0 > BAR_TIMEOUT_NS || spins > BAR_SPIN_LIMIT) {
+            err.store(BSP_ERR_TIMEOUT, cuda::memory_order_relaxed);
+            ok = 0;
+            break;
+          }
         }
-        __nanosleep(64);
       }
     }
-    __threadfence();
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
     if (err.load(cuda::memory_order_relaxed) != 0) ok = 0;
     s_ok = ok;
   }

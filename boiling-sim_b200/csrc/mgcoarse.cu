@@ -718,11 +718,13 @@ bool g_coarse_phases_fused = false;
 // BSP_TUNE_COARSE_TRACE: 1 makes every coarse-cycle launch record CTA 0's
 // %globaltimer at each phase boundary (bsp_coarse_trace_read); tracing only.
 bool g_coarse_trace = false;
-// BSP_TUNE_COARSE_TAIL: 1 (default) runs the levels CTA 0 handles alone out of
-// its shared memory (masks, right-hand sides, corrections and scratch copied
-// in, the top one's correction copied out); 0 keeps them in global memory.
-// The results are the same bits.
-bool g_coarse_tail_smem = true;
+// BSP_TUNE_COARSE_TAIL: 1 runs the levels CTA 0 handles alone out of its
+// shared memory (masks, right-hand sides, corrections and scratch copied in,
+// the top one's correction copied out); 0 (default) keeps them in global
+// memory, where they stay in L2 between cycles: measured at 384x384x256 the
+// copies cost more than the on-chip phases save (4.76 against 4.38 ms of
+// coarse cycles per solve).  The results are the same bits.
+bool g_coarse_tail_smem = false;
 
 // FP32 scratch of the coarse-cycle kernel: t (max(cells of level 1, 3 x cells
 // of the coarsest level), rounded up to 64 floats) followed by res (cells of

@@ -1,8 +1,8 @@
 // selftest.cu -- self-checks of the bounded device waits.
 //
 // Every spin in this library is bounded: the grid barrier of the persistent
-// kernels (grid_sync.cuh) gives up after BAR_SPIN_LIMIT polls and records
-// BSP_ERR_TIMEOUT; the mbarrier wait of the TMA pipelines (tma.cuh) gives up
+// kernels (grid_sync.cuh) gives up after BAR_TIMEOUT_NS on the global timer
+// and records BSP_ERR_TIMEOUT; the mbarrier wait of the TMA pipelines (tma.cuh) gives up
 // after 2^20 polls.  These kernels make each wait run out on purpose -- a
 // barrier one block never reaches, an mbarrier nothing arrives at -- so a test
 // can check that the wait returns with the error status instead of hanging,

@@ -55,6 +55,11 @@ extern bool g_fine_tma_enabled;      // BSP_TUNE_FINE_TMA (mgfine.cu)
 extern bool g_coarse_fused_enabled;  // BSP_TUNE_COARSE_FUSED (mgcoarse.cu)
 extern bool g_coarse_phases_fused;   // BSP_TUNE_COARSE_PHASES (mgcoarse.cu)
 extern bool g_coarse_tail_smem;      // BSP_TUNE_COARSE_TAIL (mgcoarse.cu)
+// BSP_TUNE_COARSE_SPLIT: 1 runs level 1 of the V-cycle with the column tile
+// kernels of level 0 (restriction to level 2, prolongation and smoothing) and
+// the one-launch coarse cycle from level 2 down; 0 runs every coarse level in
+// the one launch.
+bool g_coarse_split = false;
 // BSP_TUNE_FUSE_UPDATE: CG update fused into the next level-0 restriction
 bool g_fuse_update_enabled = true;
 // BSP_TUNE_TEST_BARRIER_ERROR (tests only): the next host-driven solve starts
@@ -966,15 +971,52 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
   } else {
     down(0);
   }
-  bool fused;
-  {
+  bool fused = false;
+  // split: level 1 on the column tile kernels around a one-launch cycle of
+  // levels 2 .. L-1 (the cycle kernel takes the level above its first one as
+  // lv[0])
+  const bool split = g_coarse_split && cx.coop && L > 3 && level_col(1);
+  if (split) {
+    down(1);
+    {
+      ProfScope ps(PROF_MG_COARSE, s);
+      fused = launch_coarse_cycle<T>(cx.lv + 1, L - 1, (float *)(cx.base + cx.lo.cscratch),
+                                     (const float *)(cx.base + cx.lo.cinv),
+                                     (const int *)(cx.base + cx.lo.cflag), cx.base + cx.lo.cctl,
+                                     g_mg_alpha, st, s);
+    }
+    if (!fused) {
+      for (int l = 2; l + 1 < L; ++l) down(l);
+    }
+  } else {
     ProfScope ps(PROF_MG_COARSE, s);
     fused = cx.coop && launch_coarse_cycle<T>(cx.lv, L, (float *)(cx.base + cx.lo.cscratch),
                                    (const float *)(cx.base + cx.lo.cinv),
                                    (const int *)(cx.base + cx.lo.cflag), cx.base + cx.lo.cctl,
                                    g_mg_alpha, st, s);
   }
-  if (!fused) {
+  if (split) {
+    if (!fused) {
+      Level<T> &c = cx.lv[L - 1];
+      const int n = c.nx * c.ny * c.nz;
+      {
+        ProfScope ps(PROF_MG_COARSE, s);
+        mg_coarse_kernel<T><<<1, 512, 3 * n * sizeof(float), s>>>(
+            c, (const float *)(cx.base + cx.lo.cinv), (const int *)(cx.base + cx.lo.cflag), st);
+      }
+      for (int l = L - 2; l >= 2; --l) {
+        Level<T> &f = cx.lv[l], &c2 = cx.lv[l + 1];
+        ProfScope ps(PROF_MG_COARSE, s);
+        if (level_col(l))
+          launch_fine_up<T>(f, c2, f.e, cx.partials, g_mg_alpha, st, s);
+        else
+          mg_up_kernel<T, false><<<row_blocks((int64_t)f.nx * f.ny), 256, 0, s>>>(
+              f, c2, f.e, cx.partials, st, g_mg_alpha);
+      }
+    }
+    ProfScope ps(PROF_MG_COARSE, s);
+    launch_fine_up<T>(cx.lv[1], cx.lv[2], cx.lv[1].e, cx.partials, g_mg_alpha, st, s);
+  } else if (!fused) {
     for (int l = 1; l + 1 < L; ++l) down(l);
     {
       Level<T> &c = cx.lv[L - 1];
@@ -1479,6 +1521,7 @@ static void key_params(GraphKey &k, const BspSolveParams *p) {
   k.v.push_back((uintptr_t)g_coarse_fused_enabled);
   k.v.push_back((uintptr_t)g_coarse_phases_fused);
   k.v.push_back((uintptr_t)g_coarse_tail_smem);
+  k.v.push_back((uintptr_t)g_coarse_split);
   k.v.push_back((uintptr_t)g_fuse_update_enabled);
   k.v.push_back((uintptr_t)g_fine_bi);
 }

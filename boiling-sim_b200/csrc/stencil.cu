@@ -508,6 +508,10 @@ extern bool g_test_barrier_error;
 extern bool g_coarse_phases_fused;
 extern bool g_coarse_trace;
 extern bool g_coarse_tail_smem;
+extern bool g_coarse_split;
+namespace utc {
+extern int g_utc_nepi;
+}  // namespace utc
 namespace cond {
 extern int g_cond_bi;
 extern bool g_cond_tma;
@@ -555,6 +559,14 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_COND_TMA:
       if (value < 0 || value > 1) return BSP_ERR_ARG;
       bsp::cond::g_cond_tma = value != 0;
+      return BSP_OK;
+    case BSP_TUNE_CONV_EPILOGUE:
+      if (value < 2 || value > 4) return BSP_ERR_ARG;
+      bsp::utc::g_utc_nepi = value;
+      return BSP_OK;
+    case BSP_TUNE_COARSE_SPLIT:
+      if (value < 0 || value > 1) return BSP_ERR_ARG;
+      bsp::g_coarse_split = value != 0;
       return BSP_OK;
     case BSP_TUNE_COARSE_PHASES:
       if (value < 0 || value > 1) return BSP_ERR_ARG;

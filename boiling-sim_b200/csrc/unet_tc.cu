@@ -29,11 +29,16 @@
 //            empty mbarriers); streams the chunk's weights too when they do
 //            not stay resident;
 //   warp 1   TMEM allocator and MMA issuer (one thread): 9 MMAs
-//            (M = 128, N = 3 cout_tile, K = 16) per chunk into one of two TMEM
-//            accumulators, tcgen05.commit to release stages and to hand the
-//            accumulator to the epilogue;
-//   warps 2-5 epilogue: tcgen05.ld of their 32 TMEM lanes, dk combination,
-//            bias, ReLU, optional skip add, BF16 store (halo rows get zeros).
+//            (M = 128, N = 3 cout_tile, K = 16) per chunk into one of 8, 4 or 2
+//            TMEM accumulators (as many as 512 columns hold), tcgen05.commit to release
+//            stages and to hand the accumulator to the epilogue;
+//   warps 2-17 epilogue, four warpgroups taking work items in turn (as many
+//            as there are accumulators):
+//            tcgen05.ld of their 32 TMEM lanes, dk combination, bias, ReLU,
+//            optional skip add, BF16 store (halo rows get zeros).
+// Row indices stay in 32 bits (padded rows < 2^30) and the stage ring is
+// walked with running counters: no 64-bit division on the critical path of
+// the single-thread roles.
 // Every mbarrier wait is bounded; on a timeout the kernel records
 // BSP_ERR_TIMEOUT in a device flag, drains its outstanding copies and MMAs
 // (bounded), frees its TMEM and returns.
@@ -62,31 +67,41 @@ namespace utc {
 
 constexpr int M = 128;          // window rows per tile (TMEM lanes)
 constexpr int MOUT = 126;       // outputs per tile
-constexpr int THREADS = 192;    // 6 warps
+constexpr int NEPI_MAX = 4;     // epilogue warpgroups (take work items in turn), at most
+// producer warp, MMA warp, epilogue warpgroups
+__host__ __device__ constexpr int conv_threads(int nepi) { return 64 + nepi * 128; }
 constexpr int SLAB = M * 32;               // one (di, dj) slab: 128 rows x 16 channels
 constexpr int A_STAGE = 9 * SLAB;          // 36,864 bytes per 16-channel chunk
 constexpr int SMEM_MAX = 232448;           // dynamic shared memory per CTA (227 KB)
 constexpr int SMEM_MIN = 120 * 1024;       // keep one CTA per SM (TMEM is not shared)
 constexpr int WRES_MAX = 112 * 1024;       // weights stay resident up to this size
+constexpr int ROWS_MAX = 1 << 30;          // padded rows: row arithmetic stays in 32 bits
 __host__ __device__ constexpr int round1k(int b) { return (b + 1023) / 1024 * 1024; }
 
 __device__ int g_utc_err;  // BSP_ERR_TIMEOUT once any wait of this kernel gave up
+// Optional cycle accounting (bsp_unet_tc_trace), summed over CTAs:
+// 0 producer waiting for a free stage, 1 MMA issuer waiting for a full stage,
+// 2 MMA issuer waiting for a free accumulator, 3 epilogue waiting for a
+// complete accumulator, 4 epilogue busy (per warpgroup, from the accumulator
+// to its release), 5 CTA lifetime, 6 work items, 7 MMA issuer busy.
+__device__ unsigned long long g_utc_trace[8];
 
 struct Params {
   __nv_bfloat16 *out;          // padded output rows x cout
   const __nv_bfloat16 *wimg;   // weight image (bsp_unet_tc_weights)
-  const float *bias;           // cout or NULL
+  const float *bias;           // cout or NULL (16-byte aligned)
   const __nv_bfloat16 *skip;   // padded rows x cout, added after ReLU, or NULL
   int nx, ny, nz, cin, cout;
   int ct;        // cout per CTA tile (16, 32 or 64); N = 3 ct
   int nct;       // cout tiles
   int relu;
-  int64_t r0;    // first interior row
-  int64_t rows;  // total padded rows
-  int64_t ntiles;
+  int r0;        // first interior row
+  int rows;      // total padded rows (< ROWS_MAX)
+  int nwork;     // work items = row tiles x cout tiles
   int resident;  // weights resident in shared memory
   int nst;       // A stages
   int w_bytes_chunk;  // bytes of one chunk's weights (9 x 2 x N x 16)
+  int trace;     // accumulate g_utc_trace
 };
 
 // ---- PTX wrappers --------------------------------------------------------------------
@@ -166,6 +181,52 @@ __device__ __forceinline__ void tmem_ld3x16(uint32_t a0, uint32_t a1, uint32_t a
     x2[q] = __uint_as_float(r[32 + q]);
   }
 }
+// 16 columns of this thread's lane from each of two column offsets, then wait::ld.
+__device__ __forceinline__ void tmem_ld2x16(uint32_t a0, uint32_t a1, float (&x0)[16],
+                                           float (&x1)[16]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%32];\n"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16, %17, %18, %19, %20, %21, %22, %23, %24, "
+      "%25, %26, %27, %28, %29, %30, %31}, [%33];\n"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+        "=r"(r[31])
+      : "r"(a0), "r"(a1)
+      : "memory");
+#pragma unroll
+  for (int q = 0; q < 16; ++q) {
+    x0[q] = __uint_as_float(r[q]);
+    x1[q] = __uint_as_float(r[16 + q]);
+  }
+}
+// 16 columns of this thread's lane, then wait::ld.
+__device__ __forceinline__ void tmem_ld1x16(uint32_t a0, float (&x0)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15}, [%16];\n"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+        "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(a0)
+      : "memory");
+#pragma unroll
+  for (int q = 0; q < 16; ++q) x0[q] = __uint_as_float(r[q]);
+}
+// Two floats rounded to BF16 (round to nearest even) in one 32-bit word, lo
+// in the low half (the lower address).
+__device__ __forceinline__ uint32_t pack_bf16x2(float lo, float hi) {
+  uint32_t d;
+  asm("cvt.rn.bf16x2.f32 %0, %1, %2;" : "=r"(d) : "f"(hi), "f"(lo));
+  return d;
+}
 __device__ __forceinline__ void named_sync(int id, int n) {
   asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
 }
@@ -195,12 +256,14 @@ __host__ __device__ constexpr uint32_t idesc_bf16(int n, int m) {
 }
 
 struct Ctl {
-  uint64_t full[8], empty[8], acc_full[2], acc_empty[2], wbar, drain;
+  // lane-31 dk=-1 block and lane-0 dk=+1 block of each epilogue quarter, per
+  // warpgroup, double-buffered over the 16-channel blocks
+  __align__(16) float xch0[NEPI_MAX][2][4][16];
+  __align__(16) float xch2[NEPI_MAX][2][4][16];
+  uint64_t full[8], empty[8], acc_full[8], acc_empty[8], wbar, drain;
   uint32_t tmem_base;
   int abort;
-  int ep_ok[2];       // accumulator-ready vote of the epilogue, per work-item parity
-  float xch0[4][16];  // lane-31 dk=-1 block of each epilogue quarter (one channel block)
-  float xch2[4][16];  // lane-0 dk=+1 block
+  int ep_ok[NEPI_MAX][2];   // accumulator-ready vote of each epilogue warpgroup
 };
 
 __device__ __forceinline__ bool wait_or_abort(uint64_t *bar, uint32_t parity, Ctl *c) {
@@ -209,15 +272,35 @@ __device__ __forceinline__ bool wait_or_abort(uint64_t *bar, uint32_t parity, Ct
   atomicExch(&g_utc_err, BSP_ERR_TIMEOUT);
   return false;
 }
+// wait_or_abort that adds the cycles spent to `acc` when tracing
+__device__ __forceinline__ bool timed_wait(uint64_t *bar, uint32_t parity, Ctl *c, bool tr,
+                                           unsigned long long &acc) {
+  const long long t0 = tr ? clock64() : 0;
+  const bool ok = wait_or_abort(bar, parity, c);
+  if (tr) acc += (unsigned long long)(clock64() - t0);
+  return ok;
+}
 
-__global__ void __launch_bounds__(THREADS, 1) conv_tc_kernel(
+// NEPI epilogue warpgroups.  The register file is split over the four SM
+// sub-partitions (16 K registers each): 18 warps (NEPI = 4) put five warps on
+// two of them and allow 96 registers a thread, 14 warps (NEPI = 3) 128.
+template <int NEPI>
+__global__ void __launch_bounds__(conv_threads(NEPI), 1) conv_tc_kernel(
     const __grid_constant__ CUtensorMap amap, const Params p) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int N = 3 * p.ct;
   const int ncol = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
+  // accumulators in TMEM: as many as fit in the 512 columns (8, 4 or 2);
+  // epilogue warpgroups in use: at most one per accumulator
+  const int lgacc = ncol <= 64 ? 3 : (ncol <= 128 ? 2 : 1);
+  const int nacc = 1 << lgacc;
+  const int nwg = nacc < NEPI ? nacc : NEPI;
+  const uint32_t tcols = (uint32_t)(nacc * ncol);
   const int nchunk = p.cin >> 4;
   const int wchunk = p.w_bytes_chunk;
+  const bool tr = p.trace != 0;
+  const long long t_start = tr ? clock64() : 0;
   // layout (from a 1024-byte aligned base): [weights (resident: all chunks;
   // else none)] [stages] [Ctl]; weights and stages padded to 1024 bytes
   unsigned char *base0 = reinterpret_cast<unsigned char *>(
@@ -225,16 +308,17 @@ __global__ void __launch_bounds__(THREADS, 1) conv_tc_kernel(
   unsigned char *wres = base0;
   const int wres_bytes = p.resident ? round1k(wchunk * nchunk) : 0;
   const int stage_bytes = round1k(A_STAGE + (p.resident ? 0 : wchunk));
+  const uint32_t stage_tx = (uint32_t)(A_STAGE + (p.resident ? 0 : wchunk));  // bytes landing
   unsigned char *stages = base0 + wres_bytes;
   Ctl *c = reinterpret_cast<Ctl *>(stages + (size_t)p.nst * stage_bytes);
-  const int64_t nwork = p.ntiles * p.nct;
+  const int nwork = p.nwork;
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < p.nst; ++s) {
       mbar_init(&c->full[s], 1);
       mbar_init(&c->empty[s], 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < nacc; ++b) {
       mbar_init(&c->acc_full[b], 1);
       mbar_init(&c->acc_empty[b], 4);
     }
@@ -246,7 +330,7 @@ __global__ void __launch_bounds__(THREADS, 1) conv_tc_kernel(
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(&c->tmem_base)),
-                 "r"(2 * ncol)
+                 "r"(tcols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -255,13 +339,14 @@ __global__ void __launch_bounds__(THREADS, 1) conv_tc_kernel(
   __syncthreads();
   tc_fence_after();
   const uint32_t tbase = c->tmem_base;
-  const int64_t R = p.nz + 2, P = (int64_t)(p.ny + 2) * R;
+  const int R = p.nz + 2, P = (p.ny + 2) * R;
 
   if (warp == 0) {
     // ---------------- producer ----------------
     if (lane == 0) {
+      unsigned long long t_wait = 0;
       if (p.resident) {
-        const uint32_t total = (uint32_t)wres_bytes;
+        const uint32_t total = (uint32_t)(wchunk * nchunk);
         mbar_expect_tx(&c->wbar, total);
         for (uint32_t off = 0; off < total; off += 16384) {
           const uint32_t nb = total - off < 16384 ? total - off : 16384;
@@ -269,59 +354,63 @@ __global__ void __launch_bounds__(THREADS, 1) conv_tc_kernel(
                     &c->wbar);
         }
       }
-      int64_t it = 0;  // stage fills issued
-      for (int64_t wk = blockIdx.x; wk < nwork && !*(volatile int *)&c->abort;
-           wk += gridDim.x) {
-        const int64_t t = wk / p.nct;
-        const int ctile = (int)(wk - t * p.nct);
-        const int64_t base = p.r0 + t * MOUT - 1;
+      int it = 0, s = 0;  // stage fills issued; current stage
+      uint32_t ph = 0;    // its phase
+      for (int wk = blockIdx.x; wk < nwork && !*(volatile int *)&c->abort; wk += gridDim.x) {
+        const int t = wk / p.nct;
+        const int ctile = wk - t * p.nct;
+        const int base = p.r0 + t * MOUT - 1;
         for (int kc = 0; kc < nchunk; ++kc, ++it) {
-          const int s = (int)(it % p.nst);
-          const uint32_t ph = (uint32_t)((it / p.nst) & 1);
-          if (!wait_or_abort(&c->empty[s], ph ^ 1u, c)) break;
+          if (!timed_wait(&c->empty[s], ph ^ 1u, c, tr, t_wait)) break;
           unsigned char *st = stages + (size_t)s * stage_bytes;
-          mbar_expect_tx(&c->full[s], (uint32_t)stage_bytes);
+          mbar_expect_tx(&c->full[s], stage_tx);
 #pragma unroll 1
           for (int sl = 0; sl < 9; ++sl) {
             const int di = sl / 3 - 1, dj = sl % 3 - 1;
-            const int y = (int)(base + di * P + dj * R);
-            tma_load2(st + sl * SLAB, &amap, kc * 16, y, &c->full[s]);
+            tma_load2(st + sl * SLAB, &amap, kc * 16, base + di * P + dj * R, &c->full[s]);
           }
           if (!p.resident)
             bulk_load(st + A_STAGE,
                       reinterpret_cast<const unsigned char *>(p.wimg) +
                           ((size_t)ctile * nchunk + kc) * wchunk,
                       (uint32_t)wchunk, &c->full[s]);
+          if (++s == p.nst) {
+            s = 0;
+            ph ^= 1u;
+          }
         }
         if (*(volatile int *)&c->abort) break;
       }
       // drain: every fill issued has landed (or the wait gives up)
       if (*(volatile int *)&c->abort && it > 0) {
-        for (int64_t q = it > p.nst ? it - p.nst : 0; q < it; ++q)
+        for (int q = it > p.nst ? it - p.nst : 0; q < it; ++q)
           mbar_wait(&c->full[q % p.nst], (uint32_t)((q / p.nst) & 1));
       }
+      if (tr) atomicAdd(&g_utc_trace[0], t_wait);
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
     if (lane == 0) {
+      unsigned long long t_full = 0, t_acc = 0, t_busy = 0;
       const uint32_t idesc = idesc_bf16(N, M);
       bool ok = true;
       if (p.resident) ok = wait_or_abort(&c->wbar, 0, c);
-      int64_t it = 0, li = 0;
-      for (int64_t wk = blockIdx.x; ok && wk < nwork; wk += gridDim.x, ++li) {
-        const int b = (int)(li & 1);
-        if (!wait_or_abort(&c->acc_empty[b], (uint32_t)(((li >> 1) & 1) ^ 1), c)) {
+      int s = 0, li = 0;
+      uint32_t ph = 0;
+      for (int wk = blockIdx.x; ok && wk < nwork; wk += gridDim.x, ++li) {
+        const int b = li & (nacc - 1);
+        if (!timed_wait(&c->acc_empty[b], (uint32_t)(((li >> lgacc) & 1) ^ 1), c, tr, t_acc)) {
           ok = false;
           break;
         }
         tc_fence_after();
         const uint32_t dt = tbase + (uint32_t)(b * ncol);
-        for (int kc = 0; kc < nchunk; ++kc, ++it) {
-          const int s = (int)(it % p.nst);
-          if (!wait_or_abort(&c->full[s], (uint32_t)((it / p.nst) & 1), c)) {
+        for (int kc = 0; kc < nchunk; ++kc) {
+          if (!timed_wait(&c->full[s], ph, c, tr, t_full)) {
             ok = false;
             break;
           }
+          const long long t0 = tr ? clock64() : 0;
           tc_fence_after();
           unsigned char *st = stages + (size_t)s * stage_bytes;
           const unsigned char *wb = p.resident ? wres + (size_t)kc * wchunk : st + A_STAGE;
@@ -333,6 +422,11 @@ __global__ void __launch_bounds__(THREADS, 1) conv_tc_kernel(
             tc_mma(dt, ad, bd, idesc, (kc > 0 || sl > 0) ? 1u : 0u);
           }
           tc_commit(&c->empty[s]);  // stage free once these MMAs have read it
+          if (++s == p.nst) {
+            s = 0;
+            ph ^= 1u;
+          }
+          if (tr) t_busy += (unsigned long long)(clock64() - t0);
         }
         if (!ok) break;
         tc_commit(&c->acc_full[b]);  // accumulator complete
@@ -340,87 +434,161 @@ __global__ void __launch_bounds__(THREADS, 1) conv_tc_kernel(
       // drain: every MMA issued has completed before TMEM is freed
       tc_commit(&c->drain);
       mbar_wait(&c->drain, 0);
+      if (tr) {
+        atomicAdd(&g_utc_trace[1], t_full);
+        atomicAdd(&g_utc_trace[2], t_acc);
+        atomicAdd(&g_utc_trace[6], (unsigned long long)li);
+        atomicAdd(&g_utc_trace[7], t_busy);
+      }
     }
   } else {
-    // ---------------- epilogue (warps 2..5) ----------------
+    // ---------------- epilogue (warpgroups of warps 2-5, 6-9, ...) ----------------
+    // Warpgroup g < nwg takes the work items li = g, g + nwg, ...;
+    // accumulator li mod nacc.  Warp w reads TMEM lanes 32 (w mod 4) .. + 31.
+    const int g = (warp - 2) >> 2;
     const int qd = warp & 3;                 // TMEM lane quarter of this warp
     const int w = qd * 32 + lane;            // window row
     const int m = w - 1;                     // output of this thread
-    const int64_t rowsz = p.ny + 2;
-    int64_t li = 0;
-    for (int64_t wk = blockIdx.x; wk < nwork; wk += gridDim.x, ++li) {
-      const int b = (int)(li & 1);
-      // one thread waits (bounded) and the 128 epilogue threads take its
-      // answer through the named barrier, so they all leave together
-      if (threadIdx.x == 64)
-        c->ep_ok[b] = wait_or_abort(&c->acc_full[b], (uint32_t)((li >> 1) & 1), c) ? 1 : 0;
-      named_sync(1, 128);
-      if (!*(volatile int *)&c->ep_ok[b]) break;
+    const bool leader = threadIdx.x == 64 + 128 * g;
+    const int bar_id = 1 + g;
+    const int rowsz = p.ny + 2;
+    unsigned long long t_wait = 0, t_busy = 0;
+    int vote = 0;  // this warpgroup's vote slot, alternating
+    for (int li = g, wk = blockIdx.x + g * gridDim.x; g < nwg && wk < nwork;
+         li += nwg, wk += nwg * gridDim.x, vote ^= 1) {
+      const int b = li & (nacc - 1);
+      // one thread waits (bounded) and the 128 threads of the warpgroup take
+      // its answer through their named barrier, so they all leave together
+      if (leader)
+        c->ep_ok[g][vote] =
+            timed_wait(&c->acc_full[b], (uint32_t)((li >> lgacc) & 1), c, tr, t_wait) ? 1 : 0;
+      named_sync(bar_id, 128);
+      if (!*(volatile int *)&c->ep_ok[g][vote]) break;
+      const long long t0 = (tr && leader) ? clock64() : 0;
       tc_fence_after();
-      const int64_t t = wk / p.nct;
-      const int ctile = (int)(wk - t * p.nct);
-      const int64_t q = p.r0 + t * MOUT + m;
-      bool valid = m >= 0 && m < MOUT && q < p.rows;
+      const int t = wk / p.nct;
+      const int ctile = wk - t * p.nct;
+      const int q = p.r0 + t * MOUT + m;
+      const bool valid = m >= 0 && m < MOUT && q < p.rows;
       bool interior = false;
       if (valid) {
-        const int64_t k = q % R, r2 = q / R;
-        const int64_t j = r2 % rowsz, i = r2 / rowsz;
-        interior = k >= 1 && k <= p.nz && j >= 1 && j <= p.ny && i >= 1 && i <= p.nx;
+        const unsigned uq = (unsigned)q, r2 = uq / (unsigned)R;
+        const unsigned k = uq - r2 * (unsigned)R;
+        const unsigned i = r2 / (unsigned)rowsz, j = r2 - i * (unsigned)rowsz;
+        interior = k >= 1 && k <= (unsigned)p.nz && j >= 1 && j <= (unsigned)p.ny && i >= 1 &&
+                   i <= (unsigned)p.nx;
       }
       const uint32_t trow = tbase + ((uint32_t)(qd * 32) << 16) + (uint32_t)(b * ncol);
       for (int cb = 0; cb < p.ct; cb += 16) {
-        float x0[16], x1[16], x2[16];
-        tmem_ld3x16(trow + (uint32_t)(0 * p.ct + cb), trow + (uint32_t)(1 * p.ct + cb),
-                    trow + (uint32_t)(2 * p.ct + cb), x0, x1, x2);
-        if (lane == 31)
-          for (int e = 0; e < 16; ++e) c->xch0[qd][e] = x0[e];
-        if (lane == 0)
-          for (int e = 0; e < 16; ++e) c->xch2[qd][e] = x2[e];
-        named_sync(1, 128);
-        float v[16];
+        // the dk = -1 and +1 blocks first, the centre block (x1) after the
+        // shuffles have consumed them: at most 48 of these registers live
+        float x0[16], x2[16];
+        tmem_ld2x16(trow + (uint32_t)(0 * p.ct + cb), trow + (uint32_t)(2 * p.ct + cb), x0, x2);
+        // D[w-1][dk=-1] and D[w+1][dk=+1]: neighbouring lanes by shuffles, the
+        // rows across a lane-quarter boundary through shared memory (slot
+        // (cb / 16) mod 2: a slot is written again only after every reader
+        // of it has passed the barrier of the block in between)
+        const int xs = (cb >> 4) & 1;
+        // the boundary rows' blocks to shared memory first (x0, x2 then die
+        // as the shuffles consume them)
+        if (lane == 31) {
+          float4 *d4 = reinterpret_cast<float4 *>(c->xch0[g][xs][qd]);
+#pragma unroll
+          for (int e4 = 0; e4 < 4; ++e4)
+            d4[e4] = make_float4(x0[4 * e4], x0[4 * e4 + 1], x0[4 * e4 + 2], x0[4 * e4 + 3]);
+        }
+        if (lane == 0) {
+          float4 *d4 = reinterpret_cast<float4 *>(c->xch2[g][xs][qd]);
+#pragma unroll
+          for (int e4 = 0; e4 < 4; ++e4)
+            d4[e4] = make_float4(x2[4 * e4], x2[4 * e4 + 1], x2[4 * e4 + 2], x2[4 * e4 + 3]);
+        }
+        // v = (up + x1) + dn: a = up + x1 now (lane 0: x1, its up comes from
+        // the quarter above), dn now (lane 31: from the quarter below)
+        float a[16], dn[16];
 #pragma unroll
         for (int e = 0; e < 16; ++e) {
-          float up = __shfl_up_sync(0xffffffffu, x0[e], 1);     // D[w-1][dk=-1]
-          float dn = __shfl_down_sync(0xffffffffu, x2[e], 1);   // D[w+1][dk=+1]
-          if (lane == 0) up = qd > 0 ? c->xch0[qd - 1][e] : 0.0f;
-          if (lane == 31) dn = qd < 3 ? c->xch2[qd + 1][e] : 0.0f;
-          v[e] = (up + x1[e]) + dn;
+          a[e] = __shfl_up_sync(0xffffffffu, x0[e], 1);
+          dn[e] = __shfl_down_sync(0xffffffffu, x2[e], 1);
         }
-        named_sync(1, 128);  // the exchange slots are reused by the next block
+        {
+          float x1[16];
+          tmem_ld1x16(trow + (uint32_t)(1 * p.ct + cb), x1);
+#pragma unroll
+          for (int e = 0; e < 16; ++e) a[e] = lane == 0 ? x1[e] : a[e] + x1[e];
+        }
+        named_sync(bar_id, 128);
+        if (lane == 0) {
+          const float4 *s4 = reinterpret_cast<const float4 *>(c->xch0[g][xs][qd > 0 ? qd - 1 : 0]);
+#pragma unroll
+          for (int e4 = 0; e4 < 4; ++e4) {
+            const float4 t = qd > 0 ? s4[e4] : make_float4(0.f, 0.f, 0.f, 0.f);
+            a[4 * e4] = t.x + a[4 * e4];
+            a[4 * e4 + 1] = t.y + a[4 * e4 + 1];
+            a[4 * e4 + 2] = t.z + a[4 * e4 + 2];
+            a[4 * e4 + 3] = t.w + a[4 * e4 + 3];
+          }
+        }
+        if (lane == 31) {
+          const float4 *s4 = reinterpret_cast<const float4 *>(c->xch2[g][xs][qd < 3 ? qd + 1 : 3]);
+#pragma unroll
+          for (int e4 = 0; e4 < 4; ++e4) {
+            const float4 t = qd < 3 ? s4[e4] : make_float4(0.f, 0.f, 0.f, 0.f);
+            dn[4 * e4] = t.x;
+            dn[4 * e4 + 1] = t.y;
+            dn[4 * e4 + 2] = t.z;
+            dn[4 * e4 + 3] = t.w;
+          }
+        }
+        float v[16];
+#pragma unroll
+        for (int e = 0; e < 16; ++e) v[e] = a[e] + dn[e];
         if (valid) {
           const int co0 = ctile * p.ct + cb;
-          __nv_bfloat16 *dst = p.out + q * p.cout + co0;
-          uint4 pk[2];
-          __nv_bfloat162 *h = reinterpret_cast<__nv_bfloat162 *>(pk);
+          __nv_bfloat16 *dst = p.out + (size_t)q * p.cout + co0;
+          uint32_t w[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};  // halo rows: zeros
           if (interior) {
-            float y[16];
+            if (p.bias) {
+              const float4 *b4 = reinterpret_cast<const float4 *>(p.bias + co0);
 #pragma unroll
-            for (int e = 0; e < 16; ++e) {
-              float a = v[e] + (p.bias ? __ldg(p.bias + co0 + e) : 0.0f);
-              if (p.relu) a = fmaxf(a, 0.0f);
-              y[e] = a;
+              for (int e4 = 0; e4 < 4; ++e4) {
+                const float4 bb = __ldg(b4 + e4);
+                v[4 * e4 + 0] += bb.x;
+                v[4 * e4 + 1] += bb.y;
+                v[4 * e4 + 2] += bb.z;
+                v[4 * e4 + 3] += bb.w;
+              }
+            }
+            if (p.relu) {
+#pragma unroll
+              for (int e = 0; e < 16; ++e) v[e] = fmaxf(v[e], 0.0f);
             }
             if (p.skip) {
-              const uint4 *sk = reinterpret_cast<const uint4 *>(p.skip + q * p.cout + co0);
-              uint4 s4[2] = {__ldg(sk), __ldg(sk + 1)};
-              const __nv_bfloat16 *sv = reinterpret_cast<const __nv_bfloat16 *>(s4);
+              const uint4 *sk = reinterpret_cast<const uint4 *>(p.skip + (size_t)q * p.cout + co0);
+              const uint4 s0 = __ldg(sk), s1 = __ldg(sk + 1);
+              const uint32_t sw[8] = {s0.x, s0.y, s0.z, s0.w, s1.x, s1.y, s1.z, s1.w};
 #pragma unroll
-              for (int e = 0; e < 16; ++e)
-                y[e] = __bfloat162float(__float2bfloat16(y[e])) + __bfloat162float(sv[e]);
+              for (int e = 0; e < 16; ++e) {
+                const uint32_t u = sw[e >> 1];
+                const float sv = __uint_as_float((e & 1) ? (u & 0xffff0000u) : (u << 16));
+                v[e] = __bfloat162float(__float2bfloat16(v[e])) + sv;
+              }
             }
 #pragma unroll
-            for (int e = 0; e < 8; ++e) h[e] = __floats2bfloat162_rn(y[2 * e], y[2 * e + 1]);
-          } else {
-            pk[0] = make_uint4(0, 0, 0, 0);
-            pk[1] = make_uint4(0, 0, 0, 0);
+            for (int e = 0; e < 8; ++e) w[e] = pack_bf16x2(v[2 * e], v[2 * e + 1]);
           }
-          reinterpret_cast<uint4 *>(dst)[0] = pk[0];
-          reinterpret_cast<uint4 *>(dst)[1] = pk[1];
+          reinterpret_cast<uint4 *>(dst)[0] = make_uint4(w[0], w[1], w[2], w[3]);
+          reinterpret_cast<uint4 *>(dst)[1] = make_uint4(w[4], w[5], w[6], w[7]);
         }
       }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(&c->acc_empty[b]);
+      if (tr && leader) t_busy += (unsigned long long)(clock64() - t0);
+    }
+    if (tr && leader) {
+      atomicAdd(&g_utc_trace[3], t_wait);
+      atomicAdd(&g_utc_trace[4], t_busy);
     }
   }
   tc_fence_before();
@@ -428,8 +596,10 @@ __global__ void __launch_bounds__(THREADS, 1) conv_tc_kernel(
   tc_fence_after();
   if (warp == 1)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase),
-                 "r"(2 * ncol)
+                 "r"(tcols)
                  : "memory");
+  if (tr && threadIdx.x == 0)
+    atomicAdd(&g_utc_trace[5], (unsigned long long)(clock64() - t_start));
 }
 
 // ---- weight image ---------------------------------------------------------------------
@@ -768,6 +938,9 @@ static bool encode_rows(CUtensorMap *m, const void *base, int c, int64_t rows) {
             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
+static int g_utc_trace_on = 0;  // host switch of the cycle accounting
+int g_utc_nepi = 4;             // BSP_TUNE_CONV_EPILOGUE: epilogue warpgroups (2, 3 or 4)
+
 int cout_tile(int cout) { return cout % 64 == 0 ? 64 : (cout % 32 == 0 ? 32 : 16); }
 
 int num_sms_dev() {
@@ -810,8 +983,9 @@ extern "C" int bsp_unet_tc_conv3(bsp_bf16_t *out, const bsp_bf16_t *in, const bs
     return BSP_ERR_ALIGN;
   if ((const void *)out == (const void *)in || (skip && (const void *)skip == (const void *)out))
     return BSP_ERR_ALIAS;
+  if (((uintptr_t)bias & 15u)) return BSP_ERR_ALIGN;
   const int64_t rows = bsp_unet_tc_rows(nx, ny, nz);
-  if (rows >= ((int64_t)1 << 31)) return BSP_ERR_SHAPE;  // TMA row coordinates are 32-bit
+  if (rows >= ROWS_MAX) return BSP_ERR_SHAPE;  // 32-bit row arithmetic, TMA coordinates
   Params p{};
   p.out = reinterpret_cast<__nv_bfloat16 *>(out);
   p.wimg = reinterpret_cast<const __nv_bfloat16 *>(wimg);
@@ -826,10 +1000,12 @@ extern "C" int bsp_unet_tc_conv3(bsp_bf16_t *out, const bsp_bf16_t *in, const bs
   p.nct = cout / p.ct;
   p.relu = relu;
   const int64_t R = nz + 2, P = (int64_t)(ny + 2) * R;
-  p.r0 = P + R + 1;
+  p.r0 = (int)(P + R + 1);
   const int64_t rlast = (int64_t)nx * P + ny * R + nz;
-  p.rows = rows;
-  p.ntiles = (rlast - p.r0 + MOUT) / MOUT;
+  p.rows = (int)rows;
+  const int64_t ntiles = (rlast - p.r0 + MOUT) / MOUT;
+  p.nwork = (int)(ntiles * p.nct);
+  p.trace = g_utc_trace_on;
   const int N = 3 * p.ct;
   p.w_bytes_chunk = 9 * 2 * N * 16;
   const int nchunk = cin / 16;
@@ -845,12 +1021,30 @@ extern "C" int bsp_unet_tc_conv3(bsp_bf16_t *out, const bsp_bf16_t *in, const bs
   if (bytes < SMEM_MIN) bytes = SMEM_MIN;
   CUtensorMap amap;
   if (!encode_rows(&amap, in, cin, rows)) return BSP_ERR_ARG;
-  if (!smem_opt_in((const void *)conv_tc_kernel, SMEM_MAX)) return BSP_ERR_ARG;
-  const int64_t work = p.ntiles * p.nct;
-  const int grid = (int)(work < num_sms_dev() ? work : num_sms_dev());
+  const int grid = p.nwork < num_sms_dev() ? p.nwork : num_sms_dev();
   ProfScope ps(PROF_UNET, s);
-  conv_tc_kernel<<<grid, THREADS, bytes, s>>>(amap, p);
+  if (g_utc_nepi == 3) {
+    if (!smem_opt_in((const void *)conv_tc_kernel<3>, SMEM_MAX)) return BSP_ERR_ARG;
+    conv_tc_kernel<3><<<grid, conv_threads(3), bytes, s>>>(amap, p);
+  } else if (g_utc_nepi == 2) {
+    if (!smem_opt_in((const void *)conv_tc_kernel<2>, SMEM_MAX)) return BSP_ERR_ARG;
+    conv_tc_kernel<2><<<grid, conv_threads(2), bytes, s>>>(amap, p);
+  } else {
+    if (!smem_opt_in((const void *)conv_tc_kernel<4>, SMEM_MAX)) return BSP_ERR_ARG;
+    conv_tc_kernel<4><<<grid, conv_threads(4), bytes, s>>>(amap, p);
+  }
   return (int)cudaGetLastError();
+}
+
+extern "C" int bsp_unet_tc_trace(unsigned long long *counters_host, int enable) {
+  cudaError_t e = cudaSuccess;
+  if (counters_host) e = cudaMemcpyFromSymbol(counters_host, g_utc_trace, sizeof(g_utc_trace));
+  if (e == cudaSuccess) {
+    const unsigned long long zero[8] = {};
+    e = cudaMemcpyToSymbol(g_utc_trace, zero, sizeof(zero));
+  }
+  g_utc_trace_on = enable ? 1 : 0;
+  return (int)e;
 }
 
 extern "C" int bsp_unet_tc_error(int *flag_host) {

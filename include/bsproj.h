@@ -68,7 +68,9 @@ extern "C" {
 #define BSP_TUNE_TEST_BARRIER_ERROR 11
 #define BSP_TUNE_COARSE_PHASES 12 /* coarse cycle forms t where it is read: 1 on, 0 off (default) */
 #define BSP_TUNE_COARSE_TRACE 13  /* tracing: coarse-cycle launches stamp their phase boundaries */
-#define BSP_TUNE_COARSE_TAIL 14   /* coarse levels of CTA 0 in shared memory: 1 on (default), 0 off */
+#define BSP_TUNE_COARSE_TAIL 14   /* coarse levels of CTA 0 in shared memory: 1 on, 0 off (default) */
+#define BSP_TUNE_COARSE_SPLIT 15  /* level 1 on the column tile kernels, one-launch cycle from level 2 */
+#define BSP_TUNE_CONV_EPILOGUE 16 /* epilogue warpgroups of the tensor-core convolution (2..4) */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */
@@ -561,13 +563,22 @@ int bsp_unet_tc_weights(bsp_bf16_t *wimg, const bsp_bf16_t *w, int cin, int cout
 /* 3x3x3 convolution on padded rows: out = relu?(conv(in) + bias), then + skip
  * (rounded to BF16 before the add, as bsp_unet_add after the layer) when
  * skip != NULL; halo rows of out get zeros.  cin, cout multiples of 16
- * (cout > 64 in tiles of 64).  Persistent kernel, one CTA per SM. */
+ * (cout > 64 in tiles of 64); bias 16-byte aligned; at most 2^30 padded
+ * rows.  Persistent kernel, one CTA per SM. */
 int bsp_unet_tc_conv3(bsp_bf16_t *out, const bsp_bf16_t *in, const bsp_bf16_t *wimg,
                       const float *bias, const bsp_bf16_t *skip, int nx, int ny, int nz,
                       int cin, int cout, int relu, cudaStream_t stream);
 /* Reads and clears the flag a tensor-core convolution sets when a bounded
  * wait gave up (its output is then not valid); synchronous. */
 int bsp_unet_tc_error(int *flag_host);
+/* Cycle accounting of bsp_unet_tc_conv3, summed over CTAs since the last
+ * call: [0] producer waiting for a free stage, [1] MMA issuer waiting for a
+ * full stage, [2] MMA issuer waiting for a free accumulator, [3] epilogue
+ * waiting for a complete accumulator, [4] epilogue busy, [5] CTA lifetime,
+ * [6] work items, [7] MMA issuer busy.  Copies the counters into
+ * counters_host[8] (when not NULL), clears them and switches the accounting
+ * on (enable != 0) or off for later launches; synchronous. */
+int bsp_unet_tc_trace(unsigned long long *counters_host, int enable);
 /* The network's input scale on the device: *s_dev = RMS of div over the fluid
  * cells (1 if there are none or it is 0), FP64 sums in a fixed order, in a
  * caller workspace of bsp_unet_scale_workspace_bytes(). */

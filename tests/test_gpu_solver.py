@@ -229,8 +229,8 @@ def test_coarse_cycle_fused_phases_bit_identical(cuda, size):
 @pytest.mark.parametrize("storage,size", [("fp16", 96), ("fp32", 192), ("bf16", 192)])
 def test_coarse_cycle_tail_in_shared_memory_bit_identical(cuda, storage, size):
     """The levels CTA 0 runs alone, staged in its shared memory
-    (BSP_TUNE_COARSE_TAIL = 1, the default), give the same bits as the same
-    phases on global memory (= 0)."""
+    (BSP_TUNE_COARSE_TAIL = 1), give the same bits as the same phases on
+    global memory (= 0, the default)."""
     from boilingsim_b200 import _lib
 
     spec = S.PotSpec(size, size, size * 2 // 3, r_in=size / 2 - 4, t_w=3,
@@ -245,7 +245,33 @@ def test_coarse_cycle_tail_in_shared_memory_bit_identical(cuda, storage, size):
             res = solve_tolerance(div, mat, DX, DT, RHO, tol=1e-6, storage=storage)
             out[tail] = (res.p64.copy(), res.inner_iterations)
     finally:
-        _lib.call("bsp_set_tuning", 14, 1)
+        _lib.call("bsp_set_tuning", 14, 0)
     assert out[0][1] == out[1][1]
     assert np.array_equal(out[0][0], out[1][0])
     assert O.rel_residual64(out[1][0], div, mat, DX, DT, RHO) <= 1.0001e-6
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp16"])
+def test_coarse_split_level1_on_tile_kernels(cuda, storage):
+    """Level 1 on the column tile kernels with the one-launch cycle from level 2
+    (BSP_TUNE_COARSE_SPLIT = 1) applies the same V-cycle as the one launch over
+    every coarse level (sums in another order): same convergence, the same
+    solution to the tolerance, on a pot whose level 1 takes the column layout."""
+    from boilingsim_b200 import _lib
+
+    mat = S.pot_mat(S.pot_192(3))
+    ux, uy, uz = S.velocity_field(mat, seed=9)
+    div = O.divergence(ux, uy, uz, mat, DX)
+    out = {}
+    try:
+        for split in (1, 0):
+            _lib.call("bsp_set_tuning", 15, split)
+            res = solve_tolerance(div, mat, DX, DT, RHO, tol=1e-7, storage=storage)
+            assert res.status == 0
+            assert O.rel_residual64(res.p64, div, mat, DX, DT, RHO) <= 1e-7 * 1.0001
+            out[split] = res
+    finally:
+        _lib.call("bsp_set_tuning", 15, 0)
+    slack = 2 if storage == "fp32" else max(3, out[0].inner_iterations // 8)
+    assert abs(out[1].inner_iterations - out[0].inner_iterations) <= slack
+    assert O.rel_error(out[1].p64, out[0].p64, mat) < 1e-5

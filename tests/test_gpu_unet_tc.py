@@ -123,6 +123,46 @@ def test_tc_conv_matches_oracle_and_torch(cuda, cin, cout, dims, relu, bias, ski
     assert bool((full.reshape(-1, cout)[halo & span] == 0).all())
 
 
+@pytest.mark.parametrize("cin,cout,dims", [(16, 16, (40, 36, 64)), (32, 32, (20, 18, 32)),
+                                           (64, 128, (8, 6, 16))])
+def test_tc_conv_epilogue_warpgroups_bit_identical(cuda, cin, cout, dims):
+    """Two, three or four epilogue warpgroups (BSP_TUNE_CONV_EPILOGUE; the
+    work items rotate over 8, 4 or 2 TMEM accumulators) give the same bits,
+    and the cycle accounting counts every work item once."""
+    rng = np.random.default_rng(cin + cout)
+    x = bf64(rng.standard_normal(dims + (cin,)))
+    w = bf64(rng.standard_normal((27, cout, cin)) * (1.0 / np.sqrt(27 * cin)))
+    b = torch.as_tensor(rng.standard_normal(cout).astype(np.float32) * 0.1).cuda()
+    sk = pad(bf64(rng.standard_normal(dims + (cout,))))
+    xin = pad(x)
+    wd = torch.as_tensor(w, dtype=torch.float32).to(torch.bfloat16).cuda()
+    wimg = torch.empty(27 * cin * cout, dtype=torch.bfloat16, device="cuda")
+    call("bsp_unet_tc_weights", ptr(wimg), ptr(wd), cin, cout, 0)
+    nx, ny, nz = dims
+    R, P = nz + 2, (ny + 2) * (nz + 2)
+    tiles = (nx * P + ny * R + nz - (P + R + 1) + 126) // 126
+    ct = 64 if cout % 64 == 0 else (32 if cout % 32 == 0 else 16)
+    outs = {}
+    try:
+        for nepi in (4, 3, 2):
+            call("bsp_set_tuning", 16, nepi)
+            out = torch.zeros((rows_of(dims), cout), dtype=torch.bfloat16, device="cuda")
+            tr = np.zeros(8, np.uint64)
+            call("bsp_unet_tc_trace", None, 1)
+            call("bsp_unet_tc_conv3", ptr(out), ptr(xin), ptr(wimg), ptr(b), ptr(sk), *dims, cin,
+                 cout, 1, 0)
+            torch.cuda.synchronize()
+            call("bsp_unet_tc_trace", tr.ctypes.data, 0)
+            assert int(tr[6]) == tiles * (cout // ct)
+            outs[nepi] = out.view(torch.int16).cpu().numpy()
+    finally:
+        call("bsp_set_tuning", 16, 4)
+    flag = np.zeros(1, np.int32)
+    call("bsp_unet_tc_error", flag.ctypes.data)
+    assert flag[0] == 0
+    assert np.array_equal(outs[4], outs[3]) and np.array_equal(outs[4], outs[2])
+
+
 def test_tc_padded_layout_kernels_bit_exact(cuda):
     """pack / pool / upsample / head on the padded layout give the same bits as
     the unpadded kernels of the training path."""
