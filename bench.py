@@ -890,9 +890,13 @@ def run_projection(args, dev, rank, world, local, dist):
                "ms_per_step": round(prof_ms[top] / args.steps, 4),
                "launches_per_step": prof_n[top] / args.steps}
     if top == 7:
-        cycles = prof_n[7] / args.steps
-        largest.update({"bound": "latency (grid barriers of one cooperative launch per V-cycle)",
-                        "us_per_cycle": round(1e3 * prof_ms[7] / prof_n[7], 2),
+        # one level-0 prolongation per V-cycle; the coarse class holds, per
+        # cycle, level 1's tile kernels and one cooperative launch for the
+        # levels below
+        cycles = prof_n[2] / args.steps
+        largest.update({"bound": "latency (grid barriers of the cooperative launch for levels "
+                                 ">= 2; level 1 on four tile-kernel launches)",
+                        "us_per_cycle": round(1e3 * prof_ms[7] / max(prof_n[2], 1), 2),
                         "cycles_per_step": cycles})
     kernel_ms = {names[c]: round(prof_ms[c] / args.steps, 4) for c in range(ncls) if prof_n[c]}
     kernel_gbs = {names[c]: round(per_launch[c] / (prof_ms[c] / prof_n[c] * 1e-3) / 1e9, 1)

@@ -520,7 +520,10 @@ class WarmStart:
     children, classes by coarse_materials), its pressure interpolated back
     onto the fine fluid cells (bsp_unet_restrict_div / bsp_unet_prolong) --
     an eighth of the network's work, for grids large enough that a full-size
-    prediction would cost more than the iterations it saves.
+    prediction would cost more than the iterations it saves.  ``"coarse4"``:
+    the same through two coarsenings (a 64th of the work; the network then
+    sees the pot at 4x the cell size, where its receptive field spans more of
+    the domain).
 
     ``scale=True`` (default) multiplies the prediction by the energy-optimal
     gamma = (b . p) / (p . A p) (bsp_unet_energy_scale), so the guess handed
@@ -545,11 +548,17 @@ class WarmStart:
             mode = "coarse" if (nx % 16 == 0 and ny % 16 == 0 and nz % 16 == 0 and
                                 nx * ny * nz >= 16_000_000) else "full"
         self.mode = mode
-        if mode == "coarse":
-            self.maskc = cell_mask(coarse_materials(mat_t))
-            self.divc = torch.zeros((nx // 2, ny // 2, nz // 2), dtype=torch.float32,
-                                    device=mat_t.device)
-            self.pc = torch.zeros_like(self.divc)
+        # coarse levels 1 .. nlev: masks, divergence and pressure buffers
+        self.nlev = {"full": 0, "coarse": 1, "coarse4": 2}[mode]
+        self.maskc, self.divc, self.pc = [], [], []
+        m = mat_t
+        for lv in range(1, self.nlev + 1):
+            m = coarse_materials(m)
+            self.maskc.append(cell_mask(m))
+            f = 1 << lv
+            self.divc.append(torch.zeros((nx // f, ny // f, nz // f), dtype=torch.float32,
+                                         device=mat_t.device))
+            self.pc.append(torch.zeros_like(self.divc[-1]))
 
     def guess(self, div, dx, dt, rho, out: torch.Tensor, graph: bool = True) -> torch.Tensor:
         """Writes the starting pressure into ``out``.  With ``graph`` the
@@ -576,14 +585,24 @@ class WarmStart:
     def _launch(self, div, dx, dt, rho, out: torch.Tensor) -> torch.Tensor:
         nx, ny, nz = self.dims
         st = stream_handle()
-        if self.mode == "full":
+        if self.nlev == 0:
             self.net.tc_plan(self.dims).run(div, self.mask, dx, dt, rho, out=out)
         else:
-            call("bsp_unet_restrict_div", ptr(self.divc), ptr(self.maskc), ptr(div),
-                 ptr(self.mask), nx, ny, nz, st)
-            self.net.tc_plan(tuple(self.divc.shape)).run(self.divc, self.maskc, 2.0 * dx, dt, rho,
-                                                          out=self.pc)
-            call("bsp_unet_prolong", ptr(out), ptr(self.pc), ptr(self.mask), nx, ny, nz, st)
+            # restrict level by level, the network on the coarsest, prolong back
+            fine_d, fine_m, dims = div, self.mask, self.dims
+            for lv in range(self.nlev):
+                call("bsp_unet_restrict_div", ptr(self.divc[lv]), ptr(self.maskc[lv]), ptr(fine_d),
+                     ptr(fine_m), *dims, st)
+                fine_d, fine_m = self.divc[lv], self.maskc[lv]
+                dims = tuple(self.divc[lv].shape)
+            k = self.nlev - 1
+            self.net.tc_plan(dims).run(self.divc[k], self.maskc[k], float(1 << self.nlev) * dx,
+                                       dt, rho, out=self.pc[k])
+            for lv in range(k, -1, -1):
+                dst = out if lv == 0 else self.pc[lv - 1]
+                dmask = self.mask if lv == 0 else self.maskc[lv - 1]
+                ddims = self.dims if lv == 0 else tuple(self.pc[lv - 1].shape)
+                call("bsp_unet_prolong", ptr(dst), ptr(self.pc[lv]), ptr(dmask), *ddims, st)
         if self.scale:
             call("bsp_spmv", ptr(self.Ap), ptr(out), ptr(self.mask), nx, ny, nz, st)
             call("bsp_unet_energy_scale", ptr(out), ptr(self.Ap), ptr(div), ptr(self.mask), nx, ny,

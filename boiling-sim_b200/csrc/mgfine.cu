@@ -613,6 +613,100 @@ struct TDown {
   __device__ void skip() const {}
 };
 
+// The four values of a quad with the non-fluid ones set to 0.
+__device__ __forceinline__ float4 fluid4(const float4 &v, uint32_t mw) {
+  return make_float4(__uint_as_float(__float_as_uint(v.x) & fluid_word(mw, 0)),
+                     __uint_as_float(__float_as_uint(v.y) & fluid_word(mw, 1)),
+                     __uint_as_float(__float_as_uint(v.z) & fluid_word(mw, 2)),
+                     __uint_as_float(__float_as_uint(v.w) & fluid_word(mw, 3)));
+}
+
+// ---- two smoothing sweeps per side on a coarse level (TMA path) ----------------------
+// On a level l >= 1 the V-cycle can smooth twice before the restriction and
+// twice after the prolongation (symmetric, so the preconditioner stays SPD):
+//   TSmooth<T, false>  e_b = e_a + w (r - A e_a),  e_a = w r  formed on the fly
+//   TDownE             res = r - A e_b  (e_b stored), restricted as TDown
+//   TUpE               e_c = e_b + alpha P e_coarse (on the fly);
+//                      e_d = e_c + w (r - A e_c)
+//   TSmooth<T, true>   e = e_d + w (r - A e_d)  (e_d stored)
+// with w = OMEGA / D; every value masked to fluid cells.  These are the
+// operations of TDown / TUp with the stored correction as the smoothed
+// quantity.
+
+// One damped-Jacobi sweep: out = v + w (r - (6 v - s(v))); v = w r (FROM_B
+// false) or the stored correction in b (true).
+template <class T, bool FROM_B>
+struct TSmooth {
+  static constexpr bool HAS_B = FROM_B, HAS_C = false, HAS_EP = false;
+  static constexpr int STAGES = 4, MIN_BLOCKS = 4;
+  T *out;
+  __device__ void init(const SolverState *) {}
+  // the stored correction is read through the fluid mask: tiles without
+  // fluid are skipped and never written, so a scratch buffer may hold stale
+  // values there
+  __device__ float4 val4(const StageView<T> &v, int rr, int lane, uint32_t mw) const {
+    if (FROM_B) return fluid4(ld4s(v.b, v.fo(rr, lane * 4)), mw);
+    const float4 r4 = ld4s(v.a, v.fo(rr, lane * 4));
+    return make_float4(r4.x * wdq(mw, 0), r4.y * wdq(mw, 1), r4.z * wdq(mw, 2),
+                       r4.w * wdq(mw, 3));
+  }
+  __device__ float val1(const StageView<T> &v, int rr, int kl) const {
+    if (FROM_B) return (v.mask1(rr, kl) & BSP_MFLUID) ? ld1s(v.b, v.fo(rr, kl)) : 0.0f;
+    return ld1s(v.a, v.fo(rr, kl)) * wdinv_ns(v.mask1(rr, kl) & 7u);
+  }
+  __device__ void emit(const StageView<T> &v, int rr, int lane, int, int, int64_t o,
+                       uint32_t mc, const float4 &e4, const float (&s)[4], float2 *) {
+    const float4 r4 = ld4s(v.a, v.fo(rr, lane * 4));
+    float zz[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const float e = q4(e4, q);
+      const float zq = fmaf(q4(r4, q) - (6.0f * e - s[q]), wdq(mc, q), e);
+      zz[q] = __uint_as_float(__float_as_uint(zq) & fluid_word(mc, q));
+    }
+    st4s(out, o, make_float4(zz[0], zz[1], zz[2], zz[3]));
+  }
+  __device__ void after_step(int, int, int, bool, float2 *) {}
+  template <int NW>
+  __device__ void finish(double *) {}
+  __device__ void skip() const {}
+};
+
+// TDown with the pre-smoothed correction read from b (stored by TSmooth),
+// through the fluid mask.
+template <class T>
+struct TDownE : TDown<T> {
+  static constexpr bool HAS_B = true, HAS_C = false, HAS_EP = false;
+  __device__ float4 val4(const StageView<T> &v, int rr, int lane, uint32_t mw) const {
+    return fluid4(ld4s(v.b, v.fo(rr, lane * 4)), mw);
+  }
+  __device__ float val1(const StageView<T> &v, int rr, int kl) const {
+    return (v.mask1(rr, kl) & BSP_MFLUID) ? ld1s(v.b, v.fo(rr, kl)) : 0.0f;
+  }
+};
+
+// TUp with the pre-smoothed correction read from b instead of w r.
+template <class T>
+struct TUpE : TUp<T> {
+  static constexpr bool HAS_B = true, HAS_C = true, HAS_EP = false;
+  __device__ float4 val4(const StageView<T> &v, int rr, int lane, uint32_t mw) const {
+    const float4 b4 = ld4s(v.b, v.fo(rr, lane * 4));
+    float2 ec = ld2s(v.c, v.co(rr, lane * 4));
+    ec.x *= this->alpha;
+    ec.y *= this->alpha;
+    auto fl = [&](float x, int q) {
+      return __uint_as_float(__float_as_uint(x) & fluid_word(mw, q));
+    };
+    return make_float4(fl(b4.x + ec.x, 0), fl(b4.y + ec.x, 1), fl(b4.z + ec.y, 2),
+                       fl(b4.w + ec.y, 3));
+  }
+  __device__ float val1(const StageView<T> &v, int rr, int kl) const {
+    const uint32_t mb = v.mask1(rr, kl);
+    return (mb & BSP_MFLUID) ? ld1s(v.b, v.fo(rr, kl)) + this->alpha * ld1s(v.c, v.co(rr, kl))
+                             : 0.0f;
+  }
+};
+
 // The CG update of the previous iteration fused into the restriction:
 // r_out = r_in - alpha Ap (stored through T and read back, as the separate
 // update kernel), e += alpha ps on the CTA's output cells, partial ||r_out||^2,
@@ -1113,6 +1207,77 @@ void launch_fine_down(const Level<T> &f, const Level<T> &c, const SolverState *s
       op, f.nx, f.ny, f.nz, fine_bi(f.nx, f.ny, f.nz), f.tiles, st);
 }
 
+// Two-sweep smoothing launchers (TMA path only; false when it cannot run).
+// launch_fine_smooth: out = one sweep from e_in (or from w r when e_in is
+// NULL); launch_fine_down_e: residual of the stored e and its restriction to
+// c.r; launch_fine_up_e: out = e_in + alpha P c.e, then one sweep.
+template <class T>
+bool launch_fine_smooth(const Level<T> &f, const T *e_in, T *out, const SolverState *st,
+                        cudaStream_t s) {
+  if (!tma_eligible(f.nz)) return false;
+  TmaMaps maps{};
+  if (!(make_map(&maps.a, tma_dtype<T>(), sizeof(T), f.r, f.nx, f.ny, f.nz, TmaGeom<T>::FW,
+                 TMA_ROWS) &&
+        make_map(&maps.m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, f.mask, f.nx, f.ny, f.nz, MASK_W,
+                 TMA_ROWS)))
+    return false;
+  if (e_in) {
+    if (!make_map(&maps.b, tma_dtype<T>(), sizeof(T), e_in, f.nx, f.ny, f.nz, TmaGeom<T>::FW,
+                  TMA_ROWS))
+      return false;
+    TSmooth<T, true> op{};
+    op.out = out;
+    return launch_tma<T>(op, maps, f.nx, f.ny, f.nz, f.tiles, st, s);
+  }
+  TSmooth<T, false> op{};
+  op.out = out;
+  return launch_tma<T>(op, maps, f.nx, f.ny, f.nz, f.tiles, st, s);
+}
+
+template <class T>
+bool launch_fine_down_e(const Level<T> &f, const Level<T> &c, const T *e_in,
+                        const SolverState *st, cudaStream_t s) {
+  if (!tma_eligible(f.nz)) return false;
+  TmaMaps maps{};
+  if (!(make_map(&maps.a, tma_dtype<T>(), sizeof(T), f.r, f.nx, f.ny, f.nz, TmaGeom<T>::FW,
+                 TMA_ROWS) &&
+        make_map(&maps.b, tma_dtype<T>(), sizeof(T), e_in, f.nx, f.ny, f.nz, TmaGeom<T>::FW,
+                 TMA_ROWS) &&
+        make_map(&maps.m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, f.mask, f.nx, f.ny, f.nz, MASK_W,
+                 TMA_ROWS)))
+    return false;
+  TDownE<T> op{};
+  op.mask1 = c.mask;
+  op.r1 = c.r;
+  op.nx = f.nx;
+  op.ny = f.ny;
+  op.ny1 = c.ny;
+  op.nz1 = c.nz;
+  return launch_tma<T>(op, maps, f.nx, f.ny, f.nz, f.tiles, st, s);
+}
+
+template <class T>
+bool launch_fine_up_e(const Level<T> &f, const Level<T> &c, const T *e_in, T *out,
+                      double *partials, float alpha, const SolverState *st, cudaStream_t s) {
+  if (!(tma_eligible(f.nz) && c.nz * 2 == f.nz && c.ny * 2 >= f.ny && c.nx * 2 >= f.nx))
+    return false;
+  TmaMaps maps{};
+  if (!(make_map(&maps.a, tma_dtype<T>(), sizeof(T), f.r, f.nx, f.ny, f.nz, TmaGeom<T>::FW,
+                 TMA_ROWS) &&
+        make_map(&maps.b, tma_dtype<T>(), sizeof(T), e_in, f.nx, f.ny, f.nz, TmaGeom<T>::FW,
+                 TMA_ROWS) &&
+        make_map(&maps.m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, f.mask, f.nx, f.ny, f.nz, MASK_W,
+                 TMA_ROWS) &&
+        make_map(&maps.c, tma_dtype<T>(), sizeof(T), c.e, c.nx, c.ny, c.nz, TmaGeom<T>::CW,
+                 TmaGeom<T>::CROWS)))
+    return false;
+  TUpE<T> op{};
+  op.z = out;
+  op.partials = partials;
+  op.alpha = alpha;
+  return launch_tma<T>(op, maps, f.nx, f.ny, f.nz, f.tiles, st, s);
+}
+
 // Level-0 restriction with the previous iteration's CG update fused in (TMA
 // path only; false when it cannot run).  f.r is r_in.
 template <class T>
@@ -1252,7 +1417,13 @@ void launch_tile_flags(int nx, int ny, int nz, const uint8_t *mask, uint8_t *fla
                                     cudaStream_t);                                              \
   template bool launch_fine_down_update<T>(const Level<T> &, const Level<T> &, T *, float *,   \
                                            const T *, const T *, double *, const SolverState *, \
-                                           cudaStream_t);
+                                           cudaStream_t);                                       \
+  template bool launch_fine_smooth<T>(const Level<T> &, const T *, T *, const SolverState *,    \
+                                      cudaStream_t);                                            \
+  template bool launch_fine_down_e<T>(const Level<T> &, const Level<T> &, const T *,            \
+                                      const SolverState *, cudaStream_t);                       \
+  template bool launch_fine_up_e<T>(const Level<T> &, const Level<T> &, const T *, T *,         \
+                                    double *, float, const SolverState *, cudaStream_t);
 INST(float)
 INST(__half)
 INST(__nv_bfloat16)

@@ -50,6 +50,19 @@ void launch_fine_up(const Level<T> &f, const Level<T> &c, T *z, double *partials
 template <class T>
 void launch_fine_down(const Level<T> &f, const Level<T> &c, const SolverState *st,
                       cudaStream_t s);
+// Two smoothing sweeps per side on a coarse level (TMA tile kernels; false
+// when they cannot run): one sweep from e_in (w r when NULL) into out; the
+// residual of the stored e restricted to c.r; out = e_in + alpha P c.e and
+// one sweep.
+template <class T>
+bool launch_fine_smooth(const Level<T> &f, const T *e_in, T *out, const SolverState *st,
+                        cudaStream_t s);
+template <class T>
+bool launch_fine_down_e(const Level<T> &f, const Level<T> &c, const T *e_in,
+                        const SolverState *st, cudaStream_t s);
+template <class T>
+bool launch_fine_up_e(const Level<T> &f, const Level<T> &c, const T *e_in, T *out,
+                      double *partials, float alpha, const SolverState *st, cudaStream_t s);
 // FP64 residual on the column layout; returns the number of partial blocks.
 template <class T>
 int launch_resid64_col(int nx, int ny, int nz, const uint8_t *mask, const uint8_t *tiles,

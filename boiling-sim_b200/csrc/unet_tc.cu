@@ -75,6 +75,7 @@ constexpr int A_STAGE = 9 * SLAB;          // 36,864 bytes per 16-channel chunk
 constexpr int SMEM_MAX = 232448;           // dynamic shared memory per CTA (227 KB)
 constexpr int SMEM_MIN = 120 * 1024;       // keep one CTA per SM (TMEM is not shared)
 constexpr int WRES_MAX = 112 * 1024;       // weights stay resident up to this size
+constexpr int SMEM_PAIR = 112 * 1024;      // per CTA with two CTAs per SM
 constexpr int ROWS_MAX = 1 << 30;          // padded rows: row arithmetic stays in 32 bits
 __host__ __device__ constexpr int round1k(int b) { return (b + 1023) / 1024 * 1024; }
 
@@ -120,6 +121,15 @@ __device__ __forceinline__ void tma_load2(void *dst, const CUtensorMap *map, int
       "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
       " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+// The same with the shared-memory addresses already in the shared window.
+__device__ __forceinline__ void tma_load2u(uint32_t dst, const CUtensorMap *map, int x, int y,
+                                           uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
       : "memory");
 }
 // 1-D bulk copy global -> shared (no multicast); size a multiple of 16
@@ -284,16 +294,22 @@ __device__ __forceinline__ bool timed_wait(uint64_t *bar, uint32_t parity, Ctl *
 // NEPI epilogue warpgroups.  The register file is split over the four SM
 // sub-partitions (16 K registers each): 18 warps (NEPI = 4) put five warps on
 // two of them and allow 96 registers a thread, 14 warps (NEPI = 3) 128.
+// NEPI = 1 runs two CTAs per SM (each its own producer, MMA issuer and
+// epilogue warpgroup, half the shared memory and 256 TMEM columns): two
+// independent single-thread issue streams per SM.
 template <int NEPI>
-__global__ void __launch_bounds__(conv_threads(NEPI), 1) conv_tc_kernel(
+__global__ void __launch_bounds__(conv_threads(NEPI), NEPI == 1 ? 2 : 1) conv_tc_kernel(
     const __grid_constant__ CUtensorMap amap, const Params p) {
   extern __shared__ __align__(1024) unsigned char smem[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int N = 3 * p.ct;
   const int ncol = N <= 32 ? 32 : (N <= 64 ? 64 : (N <= 128 ? 128 : 256));
-  // accumulators in TMEM: as many as fit in the 512 columns (8, 4 or 2);
-  // epilogue warpgroups in use: at most one per accumulator
-  const int lgacc = ncol <= 64 ? 3 : (ncol <= 128 ? 2 : 1);
+  // accumulators in TMEM: as many as fit in this CTA's columns (512, or 256
+  // with two CTAs per SM), at most 8; epilogue warpgroups in use: at most one
+  // per accumulator
+  const int tmem_max = NEPI == 1 ? 256 : 512;
+  int lgacc = 0;
+  while (lgacc < 3 && (ncol << (lgacc + 1)) <= tmem_max) ++lgacc;
   const int nacc = 1 << lgacc;
   const int nwg = nacc < NEPI ? nacc : NEPI;
   const uint32_t tcols = (uint32_t)(nacc * ncol);
@@ -354,6 +370,13 @@ __global__ void __launch_bounds__(conv_threads(NEPI), 1) conv_tc_kernel(
                     &c->wbar);
         }
       }
+      // The issue loop is one thread's dependent instruction stream: the
+      // slabs' row offsets and the shared-memory addresses are formed once,
+      // the nine loads unrolled.
+      int yoff[9];
+#pragma unroll
+      for (int sl = 0; sl < 9; ++sl) yoff[sl] = (sl / 3 - 1) * P + (sl % 3 - 1) * R;
+      const uint32_t stages_u = smem_u32(stages), full_u = smem_u32(&c->full[0]);
       int it = 0, s = 0;  // stage fills issued; current stage
       uint32_t ph = 0;    // its phase
       for (int wk = blockIdx.x; wk < nwork && !*(volatile int *)&c->abort; wk += gridDim.x) {
@@ -363,12 +386,12 @@ __global__ void __launch_bounds__(conv_threads(NEPI), 1) conv_tc_kernel(
         for (int kc = 0; kc < nchunk; ++kc, ++it) {
           if (!timed_wait(&c->empty[s], ph ^ 1u, c, tr, t_wait)) break;
           unsigned char *st = stages + (size_t)s * stage_bytes;
+          const uint32_t st_u = stages_u + (uint32_t)(s * stage_bytes);
+          const uint32_t bar_u = full_u + 8u * (uint32_t)s;
           mbar_expect_tx(&c->full[s], stage_tx);
-#pragma unroll 1
-          for (int sl = 0; sl < 9; ++sl) {
-            const int di = sl / 3 - 1, dj = sl % 3 - 1;
-            tma_load2(st + sl * SLAB, &amap, kc * 16, base + di * P + dj * R, &c->full[s]);
-          }
+#pragma unroll
+          for (int sl = 0; sl < 9; ++sl)
+            tma_load2u(st_u + (uint32_t)(sl * SLAB), &amap, kc * 16, base + yoff[sl], bar_u);
           if (!p.resident)
             bulk_load(st + A_STAGE,
                       reinterpret_cast<const unsigned char *>(p.wimg) +
@@ -393,6 +416,7 @@ __global__ void __launch_bounds__(conv_threads(NEPI), 1) conv_tc_kernel(
     if (lane == 0) {
       unsigned long long t_full = 0, t_acc = 0, t_busy = 0;
       const uint32_t idesc = idesc_bf16(N, M);
+      const uint32_t stages_u = smem_u32(stages), wres_u = smem_u32(wres);
       bool ok = true;
       if (p.resident) ok = wait_or_abort(&c->wbar, 0, c);
       int s = 0, li = 0;
@@ -412,15 +436,17 @@ __global__ void __launch_bounds__(conv_threads(NEPI), 1) conv_tc_kernel(
           }
           const long long t0 = tr ? clock64() : 0;
           tc_fence_after();
-          unsigned char *st = stages + (size_t)s * stage_bytes;
-          const unsigned char *wb = p.resident ? wres + (size_t)kc * wchunk : st + A_STAGE;
-          const uint32_t abase = smem_u32(st), bbase = smem_u32(wb);
-#pragma unroll 1
-          for (int sl = 0; sl < 9; ++sl) {
-            const uint64_t ad = sdesc_sw32(abase + sl * SLAB);
-            const uint64_t bd = sdesc(bbase + sl * 2 * N * 16, N * 16, 128);
-            tc_mma(dt, ad, bd, idesc, (kc > 0 || sl > 0) ? 1u : 0u);
-          }
+          // descriptors of slab 0; slab sl starts sl SLAB bytes (A) and
+          // sl 2 N 16 bytes (B) further, i.e. + (offset >> 4) in the start
+          // field (shared addresses stay below 2^18, so no carry leaves it)
+          const uint32_t abase = stages_u + (uint32_t)(s * stage_bytes);
+          const uint32_t bbase = p.resident ? wres_u + (uint32_t)(kc * wchunk) : abase + A_STAGE;
+          const uint64_t ad0 = sdesc_sw32(abase), bd0 = sdesc(bbase, N * 16, 128);
+          const uint64_t bstep = (uint64_t)(2 * N);
+          tc_mma(dt, ad0, bd0, idesc, kc > 0 ? 1u : 0u);
+#pragma unroll
+          for (int sl = 1; sl < 9; ++sl)
+            tc_mma(dt, ad0 + (uint64_t)(sl * (SLAB >> 4)), bd0 + (uint64_t)sl * bstep, idesc, 1u);
           tc_commit(&c->empty[s]);  // stage free once these MMAs have read it
           if (++s == p.nst) {
             s = 0;
@@ -939,7 +965,8 @@ static bool encode_rows(CUtensorMap *m, const void *base, int c, int64_t rows) {
 }
 
 static int g_utc_trace_on = 0;  // host switch of the cycle accounting
-int g_utc_nepi = 4;             // BSP_TUNE_CONV_EPILOGUE: epilogue warpgroups (2, 3 or 4)
+// BSP_TUNE_CONV_EPILOGUE: epilogue warpgroups (1 = two CTAs per SM, 2, 3 or 4)
+int g_utc_nepi = 2;
 
 int cout_tile(int cout) { return cout % 64 == 0 ? 64 : (cout % 32 == 0 ? 32 : 16); }
 
@@ -1011,19 +1038,29 @@ extern "C" int bsp_unet_tc_conv3(bsp_bf16_t *out, const bsp_bf16_t *in, const bs
   const int nchunk = cin / 16;
   const int wtotal = p.w_bytes_chunk * nchunk;
   const int ctl = (int)((sizeof(Ctl) + 127) / 128 * 128);
-  p.resident = (p.nct == 1 && wtotal <= WRES_MAX) ? 1 : 0;
+  // one CTA per SM with up to 227 KB, or (one epilogue warpgroup) two CTAs per
+  // SM with 112 KB each; weights stay resident when they leave room for two
+  // stages
+  const int per_sm = g_utc_nepi == 1 ? 2 : 1;
+  const int budget = per_sm == 2 ? SMEM_PAIR : SMEM_MAX;
+  const int wres_max = per_sm == 2 ? budget - 1024 - ctl - 2 * A_STAGE : WRES_MAX;
+  p.resident = (p.nct == 1 && round1k(wtotal) <= wres_max) ? 1 : 0;
   const int stage = round1k(A_STAGE + (p.resident ? 0 : p.w_bytes_chunk));
-  const int avail = SMEM_MAX - 1024 - ctl - (p.resident ? round1k(wtotal) : 0);
+  const int avail = budget - 1024 - ctl - (p.resident ? round1k(wtotal) : 0);
   p.nst = avail / stage;
   if (p.nst > 8) p.nst = 8;
   if (p.nst < 2) return BSP_ERR_SHAPE;
   int bytes = 1024 + (p.resident ? round1k(wtotal) : 0) + p.nst * stage + ctl;
-  if (bytes < SMEM_MIN) bytes = SMEM_MIN;
+  if (per_sm == 1 && bytes < SMEM_MIN) bytes = SMEM_MIN;
   CUtensorMap amap;
   if (!encode_rows(&amap, in, cin, rows)) return BSP_ERR_ARG;
-  const int grid = p.nwork < num_sms_dev() ? p.nwork : num_sms_dev();
+  const int slots = per_sm * num_sms_dev();
+  const int grid = p.nwork < slots ? p.nwork : slots;
   ProfScope ps(PROF_UNET, s);
-  if (g_utc_nepi == 3) {
+  if (g_utc_nepi == 1) {
+    if (!smem_opt_in((const void *)conv_tc_kernel<1>, SMEM_MAX)) return BSP_ERR_ARG;
+    conv_tc_kernel<1><<<grid, conv_threads(1), bytes, s>>>(amap, p);
+  } else if (g_utc_nepi == 3) {
     if (!smem_opt_in((const void *)conv_tc_kernel<3>, SMEM_MAX)) return BSP_ERR_ARG;
     conv_tc_kernel<3><<<grid, conv_threads(3), bytes, s>>>(amap, p);
   } else if (g_utc_nepi == 2) {

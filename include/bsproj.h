@@ -69,8 +69,12 @@ extern "C" {
 #define BSP_TUNE_COARSE_PHASES 12 /* coarse cycle forms t where it is read: 1 on, 0 off (default) */
 #define BSP_TUNE_COARSE_TRACE 13  /* tracing: coarse-cycle launches stamp their phase boundaries */
 #define BSP_TUNE_COARSE_TAIL 14   /* coarse levels of CTA 0 in shared memory: 1 on, 0 off (default) */
-#define BSP_TUNE_COARSE_SPLIT 15  /* level 1 on the column tile kernels, one-launch cycle from level 2 */
-#define BSP_TUNE_CONV_EPILOGUE 16 /* epilogue warpgroups of the tensor-core convolution (2..4) */
+#define BSP_TUNE_COARSE_SPLIT 15  /* level 1 on the column tile kernels, one-launch cycle from level 2:
+                                     1 on (default), 0 off */
+#define BSP_TUNE_CONV_EPILOGUE 16 /* tensor-core convolution: epilogue warpgroups 2..4 (default 2),
+                                     1 = two CTAs per SM with one each */
+#define BSP_TUNE_L1_SWEEPS 17     /* with COARSE_SPLIT: smoothing sweeps a side on level 1, 1 or 2
+                                     (default) */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */
