@@ -1072,7 +1072,7 @@ def main():
     ap.add_argument("--method", default="learned", choices=["learned", "mixed", "fp32"],
                     help="the timed step: learned warm start + FP16-stored solve (the metric's "
                          "learned+mixed), the FP16-stored solve alone, or FP32 storage")
-    ap.add_argument("--warm-mode", default="auto", choices=["auto", "full", "coarse"],
+    ap.add_argument("--warm-mode", default="auto", choices=["auto", "full", "coarse", "coarse4"],
                     help="resolution of the network in the learned step")
     ap.add_argument("--plain-sweeps", type=int, default=8000,
                     help="plain FP32 Jacobi sweeps measured before extrapolating to tolerance")

@@ -55,12 +55,13 @@ extern bool g_fine_tma_enabled;      // BSP_TUNE_FINE_TMA (mgfine.cu)
 extern bool g_coarse_fused_enabled;  // BSP_TUNE_COARSE_FUSED (mgcoarse.cu)
 extern bool g_coarse_phases_fused;   // BSP_TUNE_COARSE_PHASES (mgcoarse.cu)
 extern bool g_coarse_tail_smem;      // BSP_TUNE_COARSE_TAIL (mgcoarse.cu)
-// BSP_TUNE_COARSE_SPLIT: 1 (default) runs level 1 of the V-cycle with the
-// column tile kernels of level 0 (restriction to level 2, prolongation and
-// smoothing) and the one-launch coarse cycle from level 2 down, when level 1
-// takes the column layout and the cooperative launch is available; 0 runs
-// every coarse level in the one launch.
-bool g_coarse_split = true;
+// BSP_TUNE_COARSE_SPLIT: S = 1 or 2 (default) runs levels 1 .. S of the
+// V-cycle with the column tile kernels of level 0 (restriction, prolongation
+// and smoothing) and the one-launch coarse cycle below them, as far as those
+// levels take the column layout and the cooperative launch is available; 0
+// runs every coarse level in the one launch.  Measured at 384x384x256 with two
+// sweeps on level 1: 12.79 ms (S = 1), 12.60 ms (S = 2) per solve.
+int g_coarse_split = 2;
 // BSP_TUNE_L1_SWEEPS (split mode): smoothing sweeps on level 1 before the
 // restriction and after the prolongation, 1 or 2 (default; symmetric, so the
 // V-cycle stays an SPD preconditioner).  Measured at 384x384x256 (FP16
@@ -978,44 +979,38 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
     down(0);
   }
   bool fused = false;
-  // split: level 1 on the column tile kernels around a one-launch cycle of
-  // levels 2 .. L-1 (the cycle kernel takes the level above its first one as
-  // lv[0])
-  const bool split = g_coarse_split && cx.coop && L > 3 && level_col(1);
+  // split: levels 1 .. S on the column tile kernels around a one-launch cycle
+  // of levels S+1 .. L-1 (the cycle kernel takes the level above its first
+  // one as lv[0])
+  int S = 0;
+  if (cx.coop)
+    while (S < g_coarse_split && L - (S + 1) > 2 && level_col(S + 1)) ++S;
   // two sweeps a side on level 1: the pre-smoothed correction in lv[1].e, the
   // post-smoothing's intermediate in the coarse cycle's scratch (free once
   // that kernel has run; >= level-1 cells x 4 bytes; read through the mask)
-  const bool two = split && g_l1_sweeps == 2 && fine_tma_available(cx.lv[1].nz) &&
+  const bool two = S >= 1 && g_l1_sweeps == 2 && fine_tma_available(cx.lv[1].nz) &&
                    cx.lv[2].nz * 2 == cx.lv[1].nz && cx.lv[2].ny * 2 >= cx.lv[1].ny &&
                    cx.lv[2].nx * 2 >= cx.lv[1].nx;
-  if (split) {
-    if (two) {
-      ProfScope ps(PROF_MG_COARSE, s);
-      if (!launch_fine_smooth<T>(cx.lv[1], nullptr, cx.lv[1].e, st, s) ||
-          !launch_fine_down_e<T>(cx.lv[1], cx.lv[2], cx.lv[1].e, st, s))
-        return cudaErrorNotSupported;
-    } else {
-      down(1);
+  if (S > 0) {
+    for (int l = 1; l <= S; ++l) {
+      if (l == 1 && two) {
+        ProfScope ps(PROF_MG_COARSE, s);
+        if (!launch_fine_smooth<T>(cx.lv[1], nullptr, cx.lv[1].e, st, s) ||
+            !launch_fine_down_e<T>(cx.lv[1], cx.lv[2], cx.lv[1].e, st, s))
+          return cudaErrorNotSupported;
+      } else {
+        down(l);
+      }
     }
     {
       ProfScope ps(PROF_MG_COARSE, s);
-      fused = launch_coarse_cycle<T>(cx.lv + 1, L - 1, (float *)(cx.base + cx.lo.cscratch),
+      fused = launch_coarse_cycle<T>(cx.lv + S, L - S, (float *)(cx.base + cx.lo.cscratch),
                                      (const float *)(cx.base + cx.lo.cinv),
                                      (const int *)(cx.base + cx.lo.cflag), cx.base + cx.lo.cctl,
                                      g_mg_alpha, st, s);
     }
     if (!fused) {
-      for (int l = 2; l + 1 < L; ++l) down(l);
-    }
-  } else {
-    ProfScope ps(PROF_MG_COARSE, s);
-    fused = cx.coop && launch_coarse_cycle<T>(cx.lv, L, (float *)(cx.base + cx.lo.cscratch),
-                                   (const float *)(cx.base + cx.lo.cinv),
-                                   (const int *)(cx.base + cx.lo.cflag), cx.base + cx.lo.cctl,
-                                   g_mg_alpha, st, s);
-  }
-  if (split) {
-    if (!fused) {
+      for (int l = S + 1; l + 1 < L; ++l) down(l);
       Level<T> &c = cx.lv[L - 1];
       const int n = c.nx * c.ny * c.nz;
       {
@@ -1023,7 +1018,7 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
         mg_coarse_kernel<T><<<1, 512, 3 * n * sizeof(float), s>>>(
             c, (const float *)(cx.base + cx.lo.cinv), (const int *)(cx.base + cx.lo.cflag), st);
       }
-      for (int l = L - 2; l >= 2; --l) {
+      for (int l = L - 2; l > S; --l) {
         Level<T> &f = cx.lv[l], &c2 = cx.lv[l + 1];
         ProfScope ps(PROF_MG_COARSE, s);
         if (level_col(l))
@@ -1033,17 +1028,26 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
               f, c2, f.e, cx.partials, st, g_mg_alpha);
       }
     }
-    ProfScope ps(PROF_MG_COARSE, s);
-    if (two) {
-      T *mid = (T *)(cx.base + cx.lo.cscratch);
-      if (!launch_fine_up_e<T>(cx.lv[1], cx.lv[2], cx.lv[1].e, mid, cx.partials, g_mg_alpha, st,
-                               s) ||
-          !launch_fine_smooth<T>(cx.lv[1], mid, cx.lv[1].e, st, s))
-        return cudaErrorNotSupported;
-    } else {
-      launch_fine_up<T>(cx.lv[1], cx.lv[2], cx.lv[1].e, cx.partials, g_mg_alpha, st, s);
+    for (int l = S; l >= 1; --l) {
+      ProfScope ps(PROF_MG_COARSE, s);
+      if (l == 1 && two) {
+        T *mid = (T *)(cx.base + cx.lo.cscratch);
+        if (!launch_fine_up_e<T>(cx.lv[1], cx.lv[2], cx.lv[1].e, mid, cx.partials, g_mg_alpha,
+                                 st, s) ||
+            !launch_fine_smooth<T>(cx.lv[1], mid, cx.lv[1].e, st, s))
+          return cudaErrorNotSupported;
+      } else {
+        launch_fine_up<T>(cx.lv[l], cx.lv[l + 1], cx.lv[l].e, cx.partials, g_mg_alpha, st, s);
+      }
     }
-  } else if (!fused) {
+  } else {
+    ProfScope ps(PROF_MG_COARSE, s);
+    fused = cx.coop && launch_coarse_cycle<T>(cx.lv, L, (float *)(cx.base + cx.lo.cscratch),
+                                   (const float *)(cx.base + cx.lo.cinv),
+                                   (const int *)(cx.base + cx.lo.cflag), cx.base + cx.lo.cctl,
+                                   g_mg_alpha, st, s);
+  }
+  if (S == 0 && !fused) {
     for (int l = 1; l + 1 < L; ++l) down(l);
     {
       Level<T> &c = cx.lv[L - 1];

@@ -508,7 +508,7 @@ extern bool g_test_barrier_error;
 extern bool g_coarse_phases_fused;
 extern bool g_coarse_trace;
 extern bool g_coarse_tail_smem;
-extern bool g_coarse_split;
+extern int g_coarse_split;
 extern int g_l1_sweeps;
 namespace utc {
 extern int g_utc_nepi;
@@ -562,7 +562,7 @@ extern "C" int bsp_set_tuning(int key, int value) {
       bsp::cond::g_cond_tma = value != 0;
       return BSP_OK;
     case BSP_TUNE_CONV_EPILOGUE:
-      if (value < 1 || value > 4) return BSP_ERR_ARG;
+      if (value < 0 || value > 4) return BSP_ERR_ARG;
       bsp::utc::g_utc_nepi = value;
       return BSP_OK;
     case BSP_TUNE_L1_SWEEPS:
@@ -570,8 +570,8 @@ extern "C" int bsp_set_tuning(int key, int value) {
       bsp::g_l1_sweeps = value;
       return BSP_OK;
     case BSP_TUNE_COARSE_SPLIT:
-      if (value < 0 || value > 1) return BSP_ERR_ARG;
-      bsp::g_coarse_split = value != 0;
+      if (value < 0 || value > 2) return BSP_ERR_ARG;
+      bsp::g_coarse_split = value;
       return BSP_OK;
     case BSP_TUNE_COARSE_PHASES:
       if (value < 0 || value > 1) return BSP_ERR_ARG;

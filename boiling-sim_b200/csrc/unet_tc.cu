@@ -965,8 +965,11 @@ static bool encode_rows(CUtensorMap *m, const void *base, int c, int64_t rows) {
 }
 
 static int g_utc_trace_on = 0;  // host switch of the cycle accounting
-// BSP_TUNE_CONV_EPILOGUE: epilogue warpgroups (1 = two CTAs per SM, 2, 3 or 4)
-int g_utc_nepi = 2;
+// BSP_TUNE_CONV_EPILOGUE: epilogue warpgroups (1 = two CTAs per SM, 2, 3 or
+// 4); 0 (default) chooses per layer: two CTAs per SM for 16 output channels
+// (N = 48: the issue streams, not the epilogue, limit those layers; measured
+// 0.252 -> 0.195 ms for 16 -> 16 at 192x192x128), else two warpgroups
+int g_utc_nepi = 0;
 
 int cout_tile(int cout) { return cout % 64 == 0 ? 64 : (cout % 32 == 0 ? 32 : 16); }
 
@@ -1041,15 +1044,23 @@ extern "C" int bsp_unet_tc_conv3(bsp_bf16_t *out, const bsp_bf16_t *in, const bs
   // one CTA per SM with up to 227 KB, or (one epilogue warpgroup) two CTAs per
   // SM with 112 KB each; weights stay resident when they leave room for two
   // stages
-  const int per_sm = g_utc_nepi == 1 ? 2 : 1;
-  const int budget = per_sm == 2 ? SMEM_PAIR : SMEM_MAX;
-  const int wres_max = per_sm == 2 ? budget - 1024 - ctl - 2 * A_STAGE : WRES_MAX;
-  p.resident = (p.nct == 1 && round1k(wtotal) <= wres_max) ? 1 : 0;
-  const int stage = round1k(A_STAGE + (p.resident ? 0 : p.w_bytes_chunk));
-  const int avail = budget - 1024 - ctl - (p.resident ? round1k(wtotal) : 0);
-  p.nst = avail / stage;
+  // (a layer whose streamed weights leave no room for two stages in half the
+  // shared memory runs one CTA per SM with two epilogue warpgroups)
+  int nepi = g_utc_nepi > 0 ? g_utc_nepi : (cout == 16 ? 1 : 2);
+  int per_sm = 1, budget = SMEM_MAX, wres_max = WRES_MAX;
+  for (int pass = 0; pass < 2; ++pass) {
+    per_sm = nepi == 1 ? 2 : 1;
+    budget = per_sm == 2 ? SMEM_PAIR : SMEM_MAX;
+    wres_max = per_sm == 2 ? budget - 1024 - ctl - 2 * A_STAGE : WRES_MAX;
+    p.resident = (p.nct == 1 && round1k(wtotal) <= wres_max) ? 1 : 0;
+    const int stage = round1k(A_STAGE + (p.resident ? 0 : p.w_bytes_chunk));
+    p.nst = (budget - 1024 - ctl - (p.resident ? round1k(wtotal) : 0)) / stage;
+    if (p.nst >= 2 || nepi != 1) break;
+    nepi = 2;
+  }
   if (p.nst > 8) p.nst = 8;
   if (p.nst < 2) return BSP_ERR_SHAPE;
+  const int stage = round1k(A_STAGE + (p.resident ? 0 : p.w_bytes_chunk));
   int bytes = 1024 + (p.resident ? round1k(wtotal) : 0) + p.nst * stage + ctl;
   if (per_sm == 1 && bytes < SMEM_MIN) bytes = SMEM_MIN;
   CUtensorMap amap;
@@ -1057,13 +1068,13 @@ extern "C" int bsp_unet_tc_conv3(bsp_bf16_t *out, const bsp_bf16_t *in, const bs
   const int slots = per_sm * num_sms_dev();
   const int grid = p.nwork < slots ? p.nwork : slots;
   ProfScope ps(PROF_UNET, s);
-  if (g_utc_nepi == 1) {
+  if (nepi == 1) {
     if (!smem_opt_in((const void *)conv_tc_kernel<1>, SMEM_MAX)) return BSP_ERR_ARG;
     conv_tc_kernel<1><<<grid, conv_threads(1), bytes, s>>>(amap, p);
-  } else if (g_utc_nepi == 3) {
+  } else if (nepi == 3) {
     if (!smem_opt_in((const void *)conv_tc_kernel<3>, SMEM_MAX)) return BSP_ERR_ARG;
     conv_tc_kernel<3><<<grid, conv_threads(3), bytes, s>>>(amap, p);
-  } else if (g_utc_nepi == 2) {
+  } else if (nepi == 2) {
     if (!smem_opt_in((const void *)conv_tc_kernel<2>, SMEM_MAX)) return BSP_ERR_ARG;
     conv_tc_kernel<2><<<grid, conv_threads(2), bytes, s>>>(amap, p);
   } else {

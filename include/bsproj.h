@@ -69,10 +69,10 @@ extern "C" {
 #define BSP_TUNE_COARSE_PHASES 12 /* coarse cycle forms t where it is read: 1 on, 0 off (default) */
 #define BSP_TUNE_COARSE_TRACE 13  /* tracing: coarse-cycle launches stamp their phase boundaries */
 #define BSP_TUNE_COARSE_TAIL 14   /* coarse levels of CTA 0 in shared memory: 1 on, 0 off (default) */
-#define BSP_TUNE_COARSE_SPLIT 15  /* level 1 on the column tile kernels, one-launch cycle from level 2:
-                                     1 on (default), 0 off */
-#define BSP_TUNE_CONV_EPILOGUE 16 /* tensor-core convolution: epilogue warpgroups 2..4 (default 2),
-                                     1 = two CTAs per SM with one each */
+#define BSP_TUNE_COARSE_SPLIT 15  /* levels 1..S (S = 0, 1, 2 default) on the column tile kernels,
+                                     the one-launch cycle below them */
+#define BSP_TUNE_CONV_EPILOGUE 16 /* tensor-core convolution: epilogue warpgroups 2..4, 1 = two CTAs
+                                     per SM with one each, 0 = per layer (default) */
 #define BSP_TUNE_L1_SWEEPS 17     /* with COARSE_SPLIT: smoothing sweeps a side on level 1, 1 or 2
                                      (default) */
 

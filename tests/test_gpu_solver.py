@@ -162,7 +162,7 @@ def test_fused_coarse_cycle_matches_per_level_kernels(cuda, storage, spec):
             out[fused] = res
     finally:
         _lib.call("bsp_set_tuning", 5, 1)
-        _lib.call("bsp_set_tuning", 15, 1)
+        _lib.call("bsp_set_tuning", 15, 2)
     slack = 2 if storage == "fp32" else max(3, out[0].inner_iterations // 8)
     assert abs(out[1].inner_iterations - out[0].inner_iterations) <= slack
     assert O.rel_error(out[1].p64, out[0].p64, mat) < 1e-5
@@ -256,7 +256,7 @@ def test_coarse_cycle_tail_in_shared_memory_bit_identical(cuda, storage, size):
 @pytest.mark.parametrize("storage", ["fp32", "fp16"])
 def test_coarse_split_level1_on_tile_kernels(cuda, storage):
     """Level 1 on the column tile kernels with the one-launch cycle from level 2
-    (BSP_TUNE_COARSE_SPLIT = 1, the default) applies the same V-cycle as the
+    (BSP_TUNE_COARSE_SPLIT = 1; the default 2 also takes level 2) applies the same V-cycle as the
     one launch over every coarse level (one sweep a side on level 1 in both;
     sums in another order): same convergence, the same solution to the
     tolerance, on a pot whose level 1 takes the column layout."""
@@ -275,7 +275,7 @@ def test_coarse_split_level1_on_tile_kernels(cuda, storage):
             assert O.rel_residual64(res.p64, div, mat, DX, DT, RHO) <= 1e-7 * 1.0001
             out[split] = res
     finally:
-        _lib.call("bsp_set_tuning", 15, 1)
+        _lib.call("bsp_set_tuning", 15, 2)
         _lib.call("bsp_set_tuning", 17, 2)
     slack = 2 if storage == "fp32" else max(3, out[0].inner_iterations // 8)
     assert abs(out[1].inner_iterations - out[0].inner_iterations) <= slack
@@ -304,5 +304,6 @@ def test_level1_two_sweeps_converge_faster(cuda, storage):
             out[sweeps] = res
     finally:
         _lib.call("bsp_set_tuning", 17, 2)
+        _lib.call("bsp_set_tuning", 15, 2)
     assert out[2].inner_iterations <= out[1].inner_iterations
     assert O.rel_error(out[2].p64, out[1].p64, mat) < 1e-5
