@@ -751,7 +751,7 @@ def run_projection(args, dev, rank, world, local, dist):
         F.compute_divergence(div, *u, mask, DX, max_div)
         last[kind] = res
 
-    ncls = 11
+    ncls = 12
     prof_ms = (ctypes.c_double * ncls)()
     prof_n = (ctypes.c_longlong * ncls)()
     peak, peak_kind = _peaks()
@@ -867,7 +867,8 @@ def run_projection(args, dev, rank, world, local, dist):
              1: "mg_restrict_fine" if prof_n[4] else "cg_update_restrict_fine",
              2: "mg_prolong_smooth_fine", 3: "cg_direction_Ap", 4: "cg_update",
              5: "residual_fp64", 6: "x_update_fp64", 7: "mg_coarse_levels",
-             8: "control_and_setup", 9: "divergence_gradient", 10: "learned_warm_start"}
+             8: "control_and_setup", 9: "divergence_gradient", 10: "learned_warm_start",
+             11: "mg_levels_1_2_tiles"}
     total_ms = sum(prof_ms[c] for c in range(ncls)) or 1.0
     top = max((c for c in range(ncls) if prof_n[c] > 0), key=lambda c: prof_ms[c])
     dom = max((c for c in per_launch if prof_n[c] > 0), key=lambda c: prof_ms[c])
@@ -890,12 +891,10 @@ def run_projection(args, dev, rank, world, local, dist):
                "ms_per_step": round(prof_ms[top] / args.steps, 4),
                "launches_per_step": prof_n[top] / args.steps}
     if top == 7:
-        # one level-0 prolongation per V-cycle; the coarse class holds, per
-        # cycle, level 1's tile kernels and one cooperative launch for the
-        # levels below
+        # one level-0 prolongation per V-cycle and one cooperative launch for
+        # the levels below the tile-kernel ones
         cycles = prof_n[2] / args.steps
-        largest.update({"bound": "latency (grid barriers of the cooperative launch for levels "
-                                 ">= 2; level 1 on four tile-kernel launches)",
+        largest.update({"bound": "latency (grid barriers of one cooperative launch per V-cycle)",
                         "us_per_cycle": round(1e3 * prof_ms[7] / max(prof_n[2], 1), 2),
                         "cycles_per_step": cycles})
     kernel_ms = {names[c]: round(prof_ms[c] / args.steps, 4) for c in range(ncls) if prof_n[c]}

@@ -24,7 +24,10 @@ namespace bsp {
 
 int num_sms();
 
-constexpr int PCG_THREADS = 512;
+// One 1024-thread CTA per SM (the grid a whole number of CTAs per SM: a grid of
+// 168 = 148 + 20 CTAs, the most the reference's 4 KB dot workspace has room
+// for, left 20 SMs with twice the work, and each barrier waits for them).
+constexpr int PCG_THREADS = 1024;
 
 template <class MaskT>
 struct PcgArgs {
@@ -222,8 +225,10 @@ static cudaError_t launch_pcg(PcgArgs<MaskT> &a, int max_blocks, cudaStream_t s)
       &occ, pcg_persistent_kernel<MaskT>, PCG_THREADS, 0);
   if (e != cudaSuccess) return e;
   if (occ <= 0) return cudaErrorCooperativeLaunchTooLarge;
-  int nb = occ * num_sms();
-  if (nb > max_blocks) nb = max_blocks;
+  const int sms = num_sms();
+  int per = max_blocks / sms;
+  if (per > occ) per = occ;
+  int nb = per >= 1 ? per * sms : max_blocks;
   const int64_t rows = (int64_t)a.nx * a.ny;
   const int64_t need = (rows + (PCG_THREADS / 32) - 1) / (PCG_THREADS / 32);
   if (need < nb) nb = (int)(need > 0 ? need : 1);

@@ -16,11 +16,12 @@ enum ProfClass {
   PROF_CG_UPDATE = 4,  // e += alpha ps, r -= alpha Ap
   PROF_RESID64 = 5,    // FP64 residual passes
   PROF_XUPDATE = 6,    // FP64 iterate update
-  PROF_MG_COARSE = 7,  // all coarse-level multigrid kernels
+  PROF_MG_COARSE = 7,  // coarse-level multigrid: the one-launch cycle (or per-level kernels)
   PROF_CONTROL = 8,    // one-block scalar kernels, level setup, conversions
   PROF_PROJ = 9,       // divergence, gradient subtract, no-slip, rhs
   PROF_UNET = 10,      // learned warm start: network layers, input packing, head
-  PROF_NCLASS = 11
+  PROF_MG_MID = 11,    // levels 1-2 of the V-cycle on the column tile kernels (split mode)
+  PROF_NCLASS = 12
 };
 
 bool prof_enabled();

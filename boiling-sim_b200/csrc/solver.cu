@@ -947,9 +947,9 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
   // V-cycle on r -> z: level-0 restriction, the coarse levels (one
   // cooperative kernel, or one kernel per level and direction), level-0
   // prolongation
-  auto down = [&](int l) {
+  auto down = [&](int l, int cls) {
     Level<T> &f = cx.lv[l], &c = cx.lv[l + 1];
-    ProfScope ps(l == 0 ? PROF_MG_DOWN0 : PROF_MG_COARSE, s);
+    ProfScope ps(cls, s);
     if (level_col(l))
       launch_fine_down<T>(f, c, st, s);
     else
@@ -976,7 +976,7 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
     inner_check_fused_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials,
                                                        fine_grid_blocks(cx.nx, cx.ny, cx.nz));
   } else {
-    down(0);
+    down(0, PROF_MG_DOWN0);
   }
   bool fused = false;
   // split: levels 1 .. S on the column tile kernels around a one-launch cycle
@@ -994,12 +994,12 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
   if (S > 0) {
     for (int l = 1; l <= S; ++l) {
       if (l == 1 && two) {
-        ProfScope ps(PROF_MG_COARSE, s);
+        ProfScope ps(PROF_MG_MID, s);
         if (!launch_fine_smooth<T>(cx.lv[1], nullptr, cx.lv[1].e, st, s) ||
             !launch_fine_down_e<T>(cx.lv[1], cx.lv[2], cx.lv[1].e, st, s))
           return cudaErrorNotSupported;
       } else {
-        down(l);
+        down(l, PROF_MG_MID);
       }
     }
     {
@@ -1010,7 +1010,7 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
                                      g_mg_alpha, st, s);
     }
     if (!fused) {
-      for (int l = S + 1; l + 1 < L; ++l) down(l);
+      for (int l = S + 1; l + 1 < L; ++l) down(l, PROF_MG_COARSE);
       Level<T> &c = cx.lv[L - 1];
       const int n = c.nx * c.ny * c.nz;
       {
@@ -1029,7 +1029,7 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
       }
     }
     for (int l = S; l >= 1; --l) {
-      ProfScope ps(PROF_MG_COARSE, s);
+      ProfScope ps(PROF_MG_MID, s);
       if (l == 1 && two) {
         T *mid = (T *)(cx.base + cx.lo.cscratch);
         if (!launch_fine_up_e<T>(cx.lv[1], cx.lv[2], cx.lv[1].e, mid, cx.partials, g_mg_alpha,
@@ -1048,7 +1048,7 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
                                    g_mg_alpha, st, s);
   }
   if (S == 0 && !fused) {
-    for (int l = 1; l + 1 < L; ++l) down(l);
+    for (int l = 1; l + 1 < L; ++l) down(l, PROF_MG_COARSE);
     {
       Level<T> &c = cx.lv[L - 1];
       const int n = c.nx * c.ny * c.nz;

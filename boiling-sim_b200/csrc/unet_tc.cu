@@ -779,18 +779,20 @@ __global__ void head_pad_kernel(float *__restrict__ p, const __nv_bfloat16 *__re
 __global__ void restrict_div_kernel(float *__restrict__ divc, const uint8_t *__restrict__ maskc,
                                     const float *__restrict__ div,
                                     const uint8_t *__restrict__ mask, int nx, int ny, int nz) {
+  // 32-bit index arithmetic (the host checks nx ny nz < 2^31)
   const int ox = nx / 2, oy = ny / 2, oz = nz / 2;
-  const int64_t n = (int64_t)ox * oy * oz;
-  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
-       v += (int64_t)gridDim.x * blockDim.x) {
-    const int k = (int)(v % oz);
-    const int64_t r = v / oz;
-    const int j = (int)(r % oy), i = (int)(r / oy);
+  const unsigned n = (unsigned)ox * (unsigned)oy * (unsigned)oz;
+  for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
+    const unsigned r = v / (unsigned)oz;
+    const int k = (int)(v - r * (unsigned)oz);
+    const unsigned ii = r / (unsigned)oy;
+    const int j = (int)(r - ii * (unsigned)oy), i = (int)ii;
     float s = 0.0f;
     int cnt = 0;
     for (int a = 0; a < 8; ++a) {
-      const int64_t c = ((int64_t)(2 * i + (a >> 2)) * ny + 2 * j + ((a >> 1) & 1)) * nz + 2 * k +
-                        (a & 1);
+      const unsigned c = ((unsigned)(2 * i + (a >> 2)) * (unsigned)ny + 2 * j + ((a >> 1) & 1)) *
+                             (unsigned)nz +
+                         2 * k + (a & 1);
       if (mask[c] & BSP_CLASS_FLUID) {
         s += div[c];
         ++cnt;
@@ -817,23 +819,26 @@ __device__ __forceinline__ void lin2(int d, int nc, int &a, int &b, float &wa) {
 }
 __global__ void prolong_kernel(float *__restrict__ p, const float *__restrict__ pc,
                                const uint8_t *__restrict__ mask, int nx, int ny, int nz) {
+  // 32-bit index arithmetic (the host checks nx ny nz < 2^31)
   const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
-  const int64_t n = (int64_t)nx * ny * nz;
-  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
-       v += (int64_t)gridDim.x * blockDim.x) {
+  const unsigned n = (unsigned)nx * (unsigned)ny * (unsigned)nz;
+  for (unsigned v = blockIdx.x * blockDim.x + threadIdx.x; v < n; v += gridDim.x * blockDim.x) {
     if (!(mask[v] & BSP_CLASS_FLUID)) {
       p[v] = 0.0f;
       continue;
     }
-    const int k = (int)(v % nz);
-    const int64_t r = v / nz;
-    const int j = (int)(r % ny), i = (int)(r / ny);
+    const unsigned r = v / (unsigned)nz;
+    const int k = (int)(v - r * (unsigned)nz);
+    const unsigned ii = r / (unsigned)ny;
+    const int j = (int)(r - ii * (unsigned)ny), i = (int)ii;
     int i0, i1, j0, j1, k0, k1;
     float wi, wj, wk;
     lin2(i, cx, i0, i1, wi);
     lin2(j, cy, j0, j1, wj);
     lin2(k, cz, k0, k1, wk);
-    auto at = [&](int a, int b, int c) { return __ldg(pc + ((int64_t)a * cy + b) * cz + c); };
+    auto at = [&](int a, int b, int c) {
+      return __ldg(pc + ((unsigned)a * (unsigned)cy + (unsigned)b) * (unsigned)cz + (unsigned)c);
+    };
     const float c00 = wk * at(i0, j0, k0) + (1.0f - wk) * at(i0, j0, k1);
     const float c01 = wk * at(i0, j1, k0) + (1.0f - wk) * at(i0, j1, k1);
     const float c10 = wk * at(i1, j0, k0) + (1.0f - wk) * at(i1, j0, k1);
@@ -900,15 +905,39 @@ __global__ void __launch_bounds__(256) energy_partial_kernel(double *__restrict_
                                                              const float *__restrict__ div,
                                                              const uint8_t *__restrict__ mask,
                                                              int64_t n, float factor) {
+  // four cells per step (float4 loads, one mask word): the four products
+  // summed in FP32, widened once, the sums over steps, threads and blocks in
+  // FP64 and a fixed order
   __shared__ double sh[2][8];
   double a = 0.0, c = 0.0;
-  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
-       v += (int64_t)gridDim.x * blockDim.x)
+  const int64_t n4 = n >> 2;
+  const float4 *p4 = reinterpret_cast<const float4 *>(p);
+  const float4 *a4 = reinterpret_cast<const float4 *>(Ap);
+  const float4 *d4 = reinterpret_cast<const float4 *>(div);
+  const uint32_t *m4 = reinterpret_cast<const uint32_t *>(mask);
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n4;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t mw = __ldg(m4 + v);
+    if (!(mw & 0x80808080u)) continue;  // no fluid cell among the four
+    const float4 pv = __ldg(p4 + v), av = __ldg(a4 + v), dv = __ldg(d4 + v);
+    // products of non-fluid cells selected away (never multiplied by 0, so a
+    // non-finite value there cannot leak in)
+    const bool q0 = mw & 0x80u, q1 = mw & 0x8000u, q2 = mw & 0x800000u, q3 = mw & 0x80000000u;
+    const float bp = ((q0 ? factor * dv.x * pv.x : 0.0f) + (q1 ? factor * dv.y * pv.y : 0.0f)) +
+                     ((q2 ? factor * dv.z * pv.z : 0.0f) + (q3 ? factor * dv.w * pv.w : 0.0f));
+    const float pa = ((q0 ? pv.x * av.x : 0.0f) + (q1 ? pv.y * av.y : 0.0f)) +
+                     ((q2 ? pv.z * av.z : 0.0f) + (q3 ? pv.w * av.w : 0.0f));
+    a += (double)bp;
+    c += (double)pa;
+  }
+  // the n mod 4 tail cells, by block 0
+  if (blockIdx.x == 0 && threadIdx.x < (int)(n & 3)) {
+    const int64_t v = (n4 << 2) + threadIdx.x;
     if (mask[v] & BSP_CLASS_FLUID) {
-      const double pv = p[v];
-      a += (double)(factor * div[v]) * pv;
-      c += pv * (double)Ap[v];
+      a += (double)(factor * div[v] * p[v]);
+      c += (double)(p[v] * Ap[v]);
     }
+  }
   for (int o = 16; o > 0; o >>= 1) {
     a += __shfl_xor_sync(0xffffffffu, a, o);
     c += __shfl_xor_sync(0xffffffffu, c, o);
@@ -929,22 +958,40 @@ __global__ void __launch_bounds__(256) energy_partial_kernel(double *__restrict_
   }
 }
 // gamma from the partials (0 when p . A p is not positive), then p *= gamma.
+// The first warp of each block sums the partials: lane l takes blocks
+// l, l + 32, ..., then a fixed shuffle tree (the same order in every block).
 __global__ void energy_scale_kernel(float *__restrict__ p, const double *__restrict__ part,
                                     int nb, int64_t n, float *__restrict__ gamma_out) {
   __shared__ float g;
-  if (threadIdx.x == 0) {
+  if (threadIdx.x < 32) {
     double a = 0.0, c = 0.0;
-    for (int b = 0; b < nb; ++b) {
+    for (int b = threadIdx.x; b < nb; b += 32) {
       a += part[2 * b];
       c += part[2 * b + 1];
     }
-    g = (c > 0.0 && a == a) ? (float)(a / c) : 0.0f;
-    if (blockIdx.x == 0 && gamma_out) *gamma_out = g;
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_xor_sync(0xffffffffu, a, o);
+      c += __shfl_xor_sync(0xffffffffu, c, o);
+    }
+    if (threadIdx.x == 0) {
+      g = (c > 0.0 && a == a) ? (float)(a / c) : 0.0f;
+      if (blockIdx.x == 0 && gamma_out) *gamma_out = g;
+    }
   }
   __syncthreads();
-  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
-       v += (int64_t)gridDim.x * blockDim.x)
-    p[v] *= g;
+  const float gg = g;
+  const int64_t n4 = n >> 2;
+  float4 *p4 = reinterpret_cast<float4 *>(p);
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n4;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    float4 x = p4[v];
+    x.x *= gg;
+    x.y *= gg;
+    x.z *= gg;
+    x.w *= gg;
+    p4[v] = x;
+  }
+  if (blockIdx.x == 0 && threadIdx.x < (int)(n & 3)) p[(n4 << 2) + threadIdx.x] *= gg;
 }
 
 inline int grid_for(int64_t n, int threads = 256) {
@@ -1173,6 +1220,7 @@ extern "C" int bsp_unet_restrict_div(float *divc, const uint8_t *maskc, const fl
                                      cudaStream_t s) {
   if (!divc || !maskc || !div || !mask) return BSP_ERR_NULL;
   if (nx % 2 || ny % 2 || nz % 2 || nx <= 0 || ny <= 0 || nz <= 0) return BSP_ERR_SHAPE;
+  if ((int64_t)nx * ny * nz >= ((int64_t)1 << 31)) return BSP_ERR_SHAPE;
   ProfScope ps(PROF_UNET, s);
   restrict_div_kernel<<<grid_for((int64_t)nx * ny * nz / 8), 256, 0, s>>>(divc, maskc, div, mask,
                                                                             nx, ny, nz);
@@ -1183,6 +1231,7 @@ extern "C" int bsp_unet_prolong(float *p, const float *pc, const uint8_t *mask, 
                                 int nz, cudaStream_t s) {
   if (!p || !pc || !mask) return BSP_ERR_NULL;
   if (nx % 2 || ny % 2 || nz % 2 || nx <= 0 || ny <= 0 || nz <= 0) return BSP_ERR_SHAPE;
+  if ((int64_t)nx * ny * nz >= ((int64_t)1 << 31)) return BSP_ERR_SHAPE;
   if ((const void *)p == (const void *)pc) return BSP_ERR_ALIAS;
   ProfScope ps(PROF_UNET, s);
   prolong_kernel<<<grid_for((int64_t)nx * ny * nz), 256, 0, s>>>(p, pc, mask, nx, ny, nz);
@@ -1197,12 +1246,15 @@ extern "C" int bsp_unet_energy_scale(float *p, const float *Ap, const float *div
   if (workspace_bytes < bsp_unet_scale_workspace_bytes() || ((uintptr_t)workspace & 7u))
     return BSP_ERR_WORKSPACE;
   if ((const void *)p == (const void *)Ap) return BSP_ERR_ALIAS;
+  // float4 / 4-byte mask-word access
+  if (((uintptr_t)p | (uintptr_t)Ap | (uintptr_t)div) & 15u || ((uintptr_t)mask & 3u))
+    return BSP_ERR_ALIGN;
   const int64_t n = (int64_t)nx * ny * nz;
   if (n <= 0) return BSP_OK;
   ProfScope ps(PROF_UNET, s);
   energy_partial_kernel<<<RMS_BLOCKS, 256, 0, s>>>(static_cast<double *>(workspace), p, Ap, div,
                                                    mask, n, factor);
-  energy_scale_kernel<<<grid_for(n), 256, 0, s>>>(p, static_cast<const double *>(workspace),
-                                                  RMS_BLOCKS, n, gamma_dev);
+  energy_scale_kernel<<<grid_for((n + 3) / 4), 256, 0, s>>>(
+      p, static_cast<const double *>(workspace), RMS_BLOCKS, n, gamma_dev);
   return (int)cudaGetLastError();
 }

@@ -203,7 +203,7 @@ int bsp_set_tuning(int key, int value);
  * bsp_profile_read waits for the recorded launches, writes the summed
  * milliseconds and launch counts of classes 0..nclass-1 and clears the
  * record. */
-#define BSP_PROF_NCLASS 11
+#define BSP_PROF_NCLASS 12
 /* Tracing of the one-launch coarse V-cycle (with BSP_TUNE_COARSE_TRACE = 1):
  * host[0 .. n) receives CTA 0's %globaltimer (ns) at each phase boundary of
  * the last cycle launched (0 in unused slots, at most 48), and the record is
