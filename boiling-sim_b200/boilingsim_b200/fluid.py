@@ -395,3 +395,62 @@ def advect_all(grid: Grid, ws: FluidWorkspace, dt: float, device: str = "cuda:0"
          ptr(ws.ux_tmp), ptr(ws.uy_tmp), ptr(ws.uz_tmp), ptr(ws.T_tmp), ptr(ws.T_ext),
          ptr(grid_mask(grid)), nx, ny, nz, *(float(o) for o in grid.origin), float(grid.dx),
          float(dt), 1, stream_handle(stream))
+
+
+def main(argv=None):
+    """``python -m boilingsim_b200.fluid sweeps --dims NX NY NZ --tblock T --sweeps N``:
+    N Jacobi sweeps of the reference contract (bsp_jacobi_solve, T sweeps per
+    HBM pass) on a synthetic pot of the given size, timed with CUDA events
+    after one untimed solve; prints ms per sweep and the effective bandwidth
+    at 13 bytes per cell per sweep."""
+    import argparse
+    import json
+
+    import numpy as np
+
+    from . import scenes
+
+    ap = argparse.ArgumentParser(description="time the Jacobi sweep kernels")
+    ap.add_argument("cmd", choices=["sweeps"])
+    ap.add_argument("--dims", type=int, nargs=3, default=[256, 256, 192])
+    ap.add_argument("--tblock", type=int, default=1, choices=[1, 2])
+    ap.add_argument("--sweeps", type=int, default=40)
+    ap.add_argument("--reps", type=int, default=3)
+    args = ap.parse_args(argv)
+    nx, ny, nz = args.dims
+    spec = scenes.PotSpec(nx, ny, nz, r_in=nx / 2 - 6, t_w=3, water_line=int(0.55 * nz),
+                          carrot_r=max(3, nx // 12), carrot_len=nx // 2)
+    mat = scenes.pot_mat(spec)
+    ux, uy, uz = scenes.velocity_field(mat, seed=7)
+    dev = torch.device("cuda", 0)
+    mask = cell_mask(torch.as_tensor(mat).to(dev))
+    u = [torch.as_tensor(a).to(dev) for a in (ux, uy, uz)]
+    dx, dt, rho = 0.002, 0.01, 997.0
+    div = torch.zeros(mat.shape, device=dev)
+    compute_divergence(div, *u, mask, dx)
+    p, q, rhs = (torch.zeros_like(div) for _ in range(3))
+    st = stream_handle()
+
+    def solve():
+        p.zero_()
+        call("bsp_jacobi_solve", ptr(p), ptr(q), ptr(div), ptr(rhs), ptr(mask), nx, ny, nz,
+             dx, dt, rho, args.sweeps, args.tblock, st)
+
+    solve()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    for _ in range(args.reps):
+        e0.record()
+        solve()
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1) / args.sweeps)
+    best = float(np.min(ms))
+    n = nx * ny * nz
+    print(json.dumps({"dims": [nx, ny, nz], "tblock": args.tblock, "sweeps": args.sweeps,
+                      "ms_per_sweep": round(best, 5),
+                      "effective_GBs": round(13.0 * n / (best * 1e-3) / 1e9, 1)}))
+
+
+if __name__ == "__main__":
+    main()

@@ -510,6 +510,7 @@ extern bool g_coarse_trace;
 extern bool g_coarse_tail_smem;
 extern int g_coarse_split;
 extern int g_l1_sweeps;
+extern bool g_pcg_quad;
 namespace utc {
 extern int g_utc_nepi;
 }  // namespace utc
@@ -564,6 +565,10 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_CONV_EPILOGUE:
       if (value < 0 || value > 4) return BSP_ERR_ARG;
       bsp::utc::g_utc_nepi = value;
+      return BSP_OK;
+    case BSP_TUNE_PCG_QUAD:
+      if (value < 0 || value > 1) return BSP_ERR_ARG;
+      bsp::g_pcg_quad = value != 0;
       return BSP_OK;
     case BSP_TUNE_L1_SWEEPS:
       if (value < 1 || value > 2) return BSP_ERR_ARG;

@@ -75,6 +75,7 @@ extern "C" {
                                      per SM with one each, 0 = per layer (default) */
 #define BSP_TUNE_L1_SWEEPS 17     /* with COARSE_SPLIT: smoothing sweeps a side on level 1, 1 or 2
                                      (default) */
+#define BSP_TUNE_PCG_QUAD 18      /* reference-compatible PCG: four-cell form 1 (default), one-cell 0 */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */

@@ -178,3 +178,32 @@ def test_pcg_launch_matches_reference_pcg_goldens(cuda, name):
     assert abs(it - ito) <= 5
     assert np.linalg.norm(got[fl] - po[fl]) / np.linalg.norm(po[fl]) <= 1e-5
     assert float(host(ws[10])[0]) == pytest.approx(float(d["bsq"]), rel=1e-6)  # dev_bsq
+
+
+@pytest.mark.parametrize("shape", [(40, 36, 64), (33, 20, 200), (24, 24, 12)])
+def test_pcg_quad_form_matches_one_cell_form(cuda, shape):
+    """The four-cell form of the PCG phases (BSP_TUNE_PCG_QUAD = 1, nz % 4 ==
+    0: vector loads, k neighbours by shuffles, units of 128 cells including a
+    partial one when nz % 128 != 0) performs the one-cell form's per-cell
+    operations; only the FP64 partial sums run in another order, so the
+    iteration counts agree within one check and the pressures to FP32
+    rounding of the recurrences."""
+    rng = np.random.default_rng(sum(shape))
+    mat, _, div = S.parity_random_grid(rng, shape)
+    out = {}
+    try:
+        for quad in (1, 0):
+            call("bsp_set_tuning", 18, quad)
+            p = torch.full(shape, 3.0, device="cuda")
+            ws = _pcg_ws(shape)
+            div_d, mat_d = dev(div), dev(mat, torch.int32)
+            it = SimCore(0).pressure_solve_pcg(ptr(p), ptr(div_d), ptr(mat_d), *shape, 0.002, 0.01,
+                                               997.0, 1e-6, 400, *[ptr(w) for w in ws])
+            out[quad] = (it, host(p).astype(np.float64))
+    finally:
+        call("bsp_set_tuning", 18, 1)
+    assert abs(out[1][0] - out[0][0]) <= 5
+    fl = mat == 0
+    a, b = out[1][1], out[0][1]
+    assert np.all(a[~fl] == 0.0)
+    assert np.linalg.norm(a[fl] - b[fl]) <= 1e-4 * np.linalg.norm(b[fl])
