@@ -87,6 +87,11 @@ __device__ __forceinline__ float ld1s(const __half *p, int64_t o) { return __hal
 __device__ __forceinline__ float ld1s(const __nv_bfloat16 *p, int64_t o) {
   return __bfloat162float(p[o]);
 }
+__device__ __forceinline__ void st1s(float *p, int64_t o, float v) { p[o] = v; }
+__device__ __forceinline__ void st1s(__half *p, int64_t o, float v) { p[o] = __float2half_rn(v); }
+__device__ __forceinline__ void st1s(__nv_bfloat16 *p, int64_t o, float v) {
+  p[o] = __float2bfloat16_rn(v);
+}
 // value as it reads back after a store through T
 __device__ __forceinline__ float rt(float v, const float *) { return v; }
 __device__ __forceinline__ float rt(float v, const __half *) {
@@ -445,7 +450,7 @@ struct TmaGeom {
 
 // Tensor maps of one launch.  a, b: fine tensors of T; m: mask; c: coarse T.
 struct TmaMaps {
-  CUtensorMap a, b, m, c, e, p;
+  CUtensorMap a, b, m, c, e, p, q;  // q: fine uint8 parent-pattern tiles (trilinear transfers)
 };
 
 // Operand sources read from a stage.  rr: tile row 0..9 (j = j0 - 1 + rr);
@@ -453,6 +458,9 @@ struct TmaMaps {
 template <class T>
 struct StageView {
   const T *a, *b, *c;
+  const T *c2;        // the second coarse plane (trilinear prolongation)
+  const uint8_t *q;   // fine parent-pattern tile (trilinear transfers)
+  int plane;          // fine plane of this stage
   const uint8_t *m;
   const float *e;  // EP tiles: 8 output rows x 128 (no halo)
   const T *ps;
@@ -707,6 +715,96 @@ struct TUpE : TUp<T> {
   }
 };
 
+// ---- trilinear transfers between levels 0 and 1 --------------------------------------
+// Cell-centred trilinear interpolation with the weights renormalised over the
+// fluid coarse parents: fine cell f takes
+//   P e_c (f) = sum_parents w(f, c) e_c / tot(f),  tot(f) = sum over fluid parents of w(f, c),
+// w the product of the 1-D weights 3/4 (nearer parent) and 1/4, the parents of
+// fine index x being (x - 1) >> 1 and the one after it (outside the grid: no
+// parent).  tot(f) depends on the parities of (i, j, k) and on which of the
+// eight parents are fluid: the fine "parent pattern" byte (bit 4a + 2b + c for
+// parent offsets a, b, c) and a 2048-entry table of 1 / tot indexed by
+// parity bits and pattern.  The restriction is R = 1/2 P^T: the residual
+// times 1 / tot(f), gathered by tri_restrict with the same weights.  (A CPU
+// model of the preconditioned CG: 22 -> 16 inner iterations on the 64x64x48
+// pot, 25 -> 19 at 96x96x64, both with two sweeps a side on level 1.)
+__device__ float g_tri_invtot[2048];
+
+// Prolongation of the coarse correction onto the 4 fine cells of (row rr,
+// lane) of a stage, times 1 / tot; the coarse tiles c (parent plane
+// (plane - 1) >> 1) and c2 (the next), rows rr >> 1 and + 1.
+template <class T>
+__device__ __forceinline__ float4 tri_prolong4(const StageView<T> &v, const float *tab, int rr,
+                                               int lane) {
+  constexpr int CW = TmaGeom<T>::CW, PAD = TmaGeom<T>::PAD;
+  const int pi = v.plane & 1, pj = (rr + 1) & 1;
+  const float wi0 = pi ? 0.75f : 0.25f, wi1 = pi ? 0.25f : 0.75f;
+  const float wj0 = pj ? 0.75f : 0.25f, wj1 = pj ? 0.25f : 0.75f;
+  const int r0 = (rr >> 1) * CW, r1 = r0 + CW;
+  const int col = PAD + 2 * lane - 1;
+  float X[4];
+#pragma unroll
+  for (int kk = 0; kk < 4; ++kk) {
+    const float a = fmaf(wj0, ld1s(v.c, r0 + col + kk), wj1 * ld1s(v.c, r1 + col + kk));
+    const float b = fmaf(wj0, ld1s(v.c2, r0 + col + kk), wj1 * ld1s(v.c2, r1 + col + kk));
+    X[kk] = fmaf(wi0, a, wi1 * b);
+  }
+  const uint32_t pat = *reinterpret_cast<const uint32_t *>(v.q + rr * MASK_W + MASK_PAD + lane * 4);
+  const int par = (pi << 10) | (pj << 9);
+  const float e0 = fmaf(0.25f, X[0], 0.75f * X[1]), e1 = fmaf(0.75f, X[1], 0.25f * X[2]);
+  const float e2 = fmaf(0.25f, X[1], 0.75f * X[2]), e3 = fmaf(0.75f, X[2], 0.25f * X[3]);
+  return make_float4(e0 * __ldg(tab + (par | (pat & 0xffu))),
+                     e1 * __ldg(tab + (par | 256 | ((pat >> 8) & 0xffu))),
+                     e2 * __ldg(tab + (par | ((pat >> 16) & 0xffu))),
+                     e3 * __ldg(tab + (par | 256 | (pat >> 24))));
+}
+// The same for one fine cell at kl (-1 or 128: the tile's k halo).
+template <class T>
+__device__ __forceinline__ float tri_prolong1(const StageView<T> &v, const float *tab, int rr,
+                                              int kl) {
+  constexpr int CW = TmaGeom<T>::CW, PAD = TmaGeom<T>::PAD;
+  const int pi = v.plane & 1, pj = (rr + 1) & 1, pk = kl & 1;
+  const float wi0 = pi ? 0.75f : 0.25f, wi1 = pi ? 0.25f : 0.75f;
+  const float wj0 = pj ? 0.75f : 0.25f, wj1 = pj ? 0.25f : 0.75f;
+  const float wk0 = pk ? 0.75f : 0.25f, wk1 = pk ? 0.25f : 0.75f;
+  const int r0 = (rr >> 1) * CW, r1 = r0 + CW;
+  const int col = PAD + ((kl - 1) >> 1);
+  float X[2];
+#pragma unroll
+  for (int kk = 0; kk < 2; ++kk) {
+    const float a = fmaf(wj0, ld1s(v.c, r0 + col + kk), wj1 * ld1s(v.c, r1 + col + kk));
+    const float b = fmaf(wj0, ld1s(v.c2, r0 + col + kk), wj1 * ld1s(v.c2, r1 + col + kk));
+    X[kk] = fmaf(wi0, a, wi1 * b);
+  }
+  const uint32_t pat = v.q[rr * MASK_W + MASK_PAD + kl];
+  return fmaf(wk0, X[0], wk1 * X[1]) * __ldg(tab + ((pi << 10) | (pj << 9) | (pk << 8) | pat));
+}
+
+// TUp with the trilinear prolongation from level 1.
+template <class T>
+struct TUp3 : TUp<T> {
+  static constexpr bool HAS_B = false, HAS_C = true, HAS_EP = false, HAS_C2 = true, HAS_Q = true;
+  const float *tab;
+  __device__ float4 val4(const StageView<T> &v, int rr, int lane, uint32_t mw) const {
+    const float4 r4 = ld4s(v.a, v.fo(rr, lane * 4));
+    const float4 ef = tri_prolong4(v, tab, rr, lane);
+    const float al = this->alpha;
+    auto fl = [&](float x, int q) {
+      return __uint_as_float(__float_as_uint(x) & fluid_word(mw, q));
+    };
+    return make_float4(fl(fmaf(r4.x, wdq(mw, 0), al * ef.x), 0),
+                       fl(fmaf(r4.y, wdq(mw, 1), al * ef.y), 1),
+                       fl(fmaf(r4.z, wdq(mw, 2), al * ef.z), 2),
+                       fl(fmaf(r4.w, wdq(mw, 3), al * ef.w), 3));
+  }
+  __device__ float val1(const StageView<T> &v, int rr, int kl) const {
+    const uint32_t mb = v.mask1(rr, kl);
+    return (mb & BSP_MFLUID) ? fmaf(ld1s(v.a, v.fo(rr, kl)), wdinv_ns(mb & 7u),
+                                    this->alpha * tri_prolong1(v, tab, rr, kl))
+                             : 0.0f;
+  }
+};
+
 // The CG update of the previous iteration fused into the restriction:
 // r_out = r_in - alpha Ap (stored through T and read back, as the separate
 // update kernel), e += alpha ps on the CTA's output cells, partial ||r_out||^2,
@@ -714,17 +812,21 @@ struct TUpE : TUp<T> {
 // buffers: the tiles of neighbouring CTAs overlap, so an in-place update
 // could be applied twice.  Without a pending update (first inner iteration of
 // a refinement pass) r_out = r_in.
-template <class T>
+template <class T, bool TRI = false>
 struct TDownU {
   // e and ps of the 8 output rows come as TMA tiles too (EP); 3 stages keep
-  // three CTAs per SM
-  static constexpr bool HAS_B = true, HAS_C = false, HAS_EP = true;
+  // three CTAs per SM.  TRI: the trilinear restriction instead of the 2x2x2
+  // sums -- the residual divided by its parents' weight sum (the parent-pattern
+  // tile q and the table tab) goes to rs, and tri_restrict gathers it.
+  static constexpr bool HAS_B = true, HAS_C = false, HAS_EP = true, HAS_Q = TRI;
   static constexpr int STAGES = 3, MIN_BLOCKS = 3;
   const uint8_t *mask1;
   T *r1, *r_out;
   float *e;
   const T *ps;
   double *partials;
+  T *rs;             // TRI: scaled residual (level-0 sized)
+  const float *tab;  // TRI: 1 / parents' weight sum by parity and pattern
   int nx, ny, ny1, nz1;
   float alpha;
   bool upd;
@@ -754,8 +856,9 @@ struct TDownU {
     return rv * wdinv_ns(v.mask1(row, kl) & 7u);
   }
   __device__ bool pair_end(int i) const { return (i & 1) || i + 1 == nx; }
-  __device__ void emit(const StageView<T> &v, int row, int lane, int i, int, int64_t o,
+  __device__ void emit(const StageView<T> &v, int row, int lane, int i, int, int64_t o_,
                        uint32_t mc, const float4 &e4, const float (&s)[4], float2 *xch) {
+    const int64_t o = o_;
     const float4 r4 = rnew4(v, row, lane);
     st4s(r_out, o, r4);
     if (upd) {
@@ -772,6 +875,17 @@ struct TDownU {
       const float rq = q4(r4, q) - (6.0f * q4(e4, q) - s[q]);
       res[q] = __uint_as_float(__float_as_uint(rq) & fluid_word(mc, q));
     }
+    if (TRI) {
+      const uint32_t pat = *reinterpret_cast<const uint32_t *>(v.q + row * MASK_W + MASK_PAD +
+                                                               lane * 4);
+      const int par = ((i & 1) << 10) | (((row + 1) & 1) << 9);
+      float o[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        o[q] = res[q] * __ldg(tab + (par | ((q & 1) << 8) | ((pat >> (8 * q)) & 0xffu)));
+      st4s(rs, o_, make_float4(o[0], o[1], o[2], o[3]));
+      return;
+    }
     acc.x += res[0] + res[1];
     acc.y += res[2] + res[3];
     const int warp = threadIdx.x >> 5;
@@ -781,6 +895,7 @@ struct TDownU {
     }
   }
   __device__ void after_step(int i, int j, int k, bool act, float2 *xch) {
+    if (TRI) return;
     const int warp = threadIdx.x >> 5;
     if (!pair_end(i) || (warp & 1)) return;
     if (act) {
@@ -805,19 +920,33 @@ struct TDownU {
 constexpr int align128(int b) { return (b + 127) / 128 * 128; }
 
 // Every TMA destination starts on a 128-byte boundary.
+// Optional operand flags of an op (false when the op does not declare them).
+template <class Op, class = void>
+struct op_c2 : std::false_type {};
+template <class Op>
+struct op_c2<Op, std::void_t<decltype(Op::HAS_C2)>> : std::integral_constant<bool, Op::HAS_C2> {};
+template <class Op, class = void>
+struct op_q : std::false_type {};
+template <class Op>
+struct op_q<Op, std::void_t<decltype(Op::HAS_Q)>> : std::integral_constant<bool, Op::HAS_Q> {};
+
 template <class T, class Op>
 struct TmaSmem {
   static constexpr int FB = TmaGeom<T>::FBYTES, MB = TmaGeom<T>::MBYTES,
                        CB = TmaGeom<T>::CBYTES;
   static constexpr int EB = TILE_ROWS * 128 * 4, PB = TILE_ROWS * 128 * (int)sizeof(T);
+  static constexpr bool C2 = op_c2<Op>::value, Q = op_q<Op>::value;
   static constexpr int NST = Op::STAGES;
   static constexpr int OFF_B = align128(FB);
   static constexpr int OFF_M = OFF_B + (Op::HAS_B ? align128(FB) : 0);
   static constexpr int OFF_C = OFF_M + align128(MB);
-  static constexpr int OFF_E = OFF_C + (Op::HAS_C ? align128(CB) : 0);
+  static constexpr int OFF_C2 = OFF_C + (Op::HAS_C ? align128(CB) : 0);
+  static constexpr int OFF_Q = OFF_C2 + (C2 ? align128(CB) : 0);
+  static constexpr int OFF_E = OFF_Q + (Q ? align128(MB) : 0);
   static constexpr int OFF_P = OFF_E + (Op::HAS_EP ? EB : 0);
   static constexpr int STAGE = OFF_P + (Op::HAS_EP ? align128(PB) : 0);
   static constexpr uint32_t TX = (uint32_t)(FB + (Op::HAS_B ? FB : 0) + MB + (Op::HAS_C ? CB : 0) +
+                                            (C2 ? CB : 0) + (Q ? MB : 0) +
                                             (Op::HAS_EP ? EB + PB : 0));
   static constexpr int RING = STAGE * NST;
   // ring | plane_buf (2 x 10 x 32 float4) | mbarriers
@@ -863,8 +992,14 @@ __global__ void __launch_bounds__(TILE_THREADS, Op::MIN_BLOCKS) fine_tma_kernel(
     tma_load3(base, &maps.a, k0 - PAD, j0 - 1, p, &bars[q]);
     if (Op::HAS_B) tma_load3(base + L::OFF_B, &maps.b, k0 - PAD, j0 - 1, p, &bars[q]);
     tma_load3(base + L::OFF_M, &maps.m, k0 - MASK_PAD, j0 - 1, p, &bars[q]);
-    if (Op::HAS_C)
-      tma_load3(base + L::OFF_C, &maps.c, k0 / 2 - PAD, j0 / 2 - 1, p >> 1, &bars[q]);
+    if (Op::HAS_C) {
+      // trilinear: the two parent planes (p - 1) >> 1 and the one after it
+      // (plane -1 arrives as zeros); else the parent plane p >> 1
+      const int pc = L::C2 ? ((p - 1) >> 1) : (p >> 1);
+      tma_load3(base + L::OFF_C, &maps.c, k0 / 2 - PAD, j0 / 2 - 1, pc, &bars[q]);
+      if (L::C2) tma_load3(base + L::OFF_C2, &maps.c, k0 / 2 - PAD, j0 / 2 - 1, pc + 1, &bars[q]);
+    }
+    if (L::Q) tma_load3(base + L::OFF_Q, &maps.q, k0 - MASK_PAD, j0 - 1, p, &bars[q]);
     if (Op::HAS_EP) {
       tma_load3(base + L::OFF_E, &maps.e, k0, j0, p, &bars[q]);
       tma_load3(base + L::OFF_P, &maps.p, k0, j0, p, &bars[q]);
@@ -877,6 +1012,9 @@ __global__ void __launch_bounds__(TILE_THREADS, Op::MIN_BLOCKS) fine_tma_kernel(
     v.b = reinterpret_cast<const T *>(base + L::OFF_B);
     v.m = base + L::OFF_M;
     v.c = reinterpret_cast<const T *>(base + L::OFF_C);
+    v.c2 = reinterpret_cast<const T *>(base + L::OFF_C2);
+    v.q = base + L::OFF_Q;
+    v.plane = p;
     v.e = reinterpret_cast<const float *>(base + L::OFF_E);
     v.ps = reinterpret_cast<const T *>(base + L::OFF_P);
     return v;
@@ -1278,12 +1416,153 @@ bool launch_fine_up_e(const Level<T> &f, const Level<T> &c, const T *e_in, T *ou
   return launch_tma<T>(op, maps, f.nx, f.ny, f.nz, f.tiles, st, s);
 }
 
+// ---- trilinear transfers: setup, restriction, launchers ----------------------------
+// Parent pattern of every fine fluid cell (0 elsewhere) from the coarse classes.
+__global__ void tri_pattern_kernel(uint8_t *__restrict__ pat, const uint8_t *__restrict__ mask,
+                                   const uint8_t *__restrict__ mask1, int nx, int ny, int nz,
+                                   int cx, int cy, int cz) {
+  const int64_t n = (int64_t)nx * ny * nz;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < n;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    uint32_t bits = 0;
+    if (mask[v] & BSP_MFLUID) {
+      const int k = (int)(v % nz);
+      const int64_t r = v / nz;
+      const int j = (int)(r % ny), i = (int)(r / ny);
+      const int i0 = (i - 1) >> 1, j0 = (j - 1) >> 1, k0 = (k - 1) >> 1;
+      for (int b = 0; b < 8; ++b) {
+        const int ci = i0 + (b >> 2), cj = j0 + ((b >> 1) & 1), ck = k0 + (b & 1);
+        if (ci < 0 || cj < 0 || ck < 0 || ci >= cx || cj >= cy || ck >= cz) continue;
+        if (mask1[((int64_t)ci * cy + cj) * cz + ck] & BSP_MFLUID) bits |= 1u << b;
+      }
+    }
+    pat[v] = (uint8_t)bits;
+  }
+}
+
+// r1 = 1/2 P^T applied to the scaled residual rs (already divided by tot):
+// coarse cell c takes the fine cells 2c-1 .. 2c+2 of each axis with weights
+// 1/4, 3/4, 3/4, 1/4; fluid coarse cells only.  A thread owns one coarse
+// (j, k) column and marches a chunk of coarse planes, each fine plane's
+// 4 x 4 sum computed once and shared by the two coarse planes it feeds.
+template <class T>
+__global__ void __launch_bounds__(128) tri_restrict_kernel(T *__restrict__ r1,
+                                                           const T *__restrict__ rs,
+                                                           const uint8_t *__restrict__ mask1,
+                                                           int nx, int ny, int nz, int cx, int cy,
+                                                           int cz, int cpc,
+                                                           const SolverState *st) {
+  if (st->inner_done) return;
+  const int kc = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jc = blockIdx.y;
+  const int c0 = blockIdx.z * cpc, c1 = min(c0 + cpc, cx);
+  if (kc >= cz || jc >= cy) return;
+  const float w[4] = {0.25f, 0.75f, 0.75f, 0.25f};
+  auto plane_sum = [&](int f) {
+    float sum = 0.0f;
+    if (f < 0 || f >= nx) return sum;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+      const int fj = 2 * jc - 1 + b;
+      if (fj < 0 || fj >= ny) continue;
+      const T *row = rs + ((int64_t)f * ny + fj) * nz;
+      float t = 0.0f;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        const int fk = 2 * kc - 1 + a;
+        if (fk >= 0 && fk < nz) t = fmaf(w[a], ld1s(row, fk), t);
+      }
+      sum = fmaf(w[b], t, sum);
+    }
+    return sum;
+  };
+  float pm = plane_sum(2 * c0 - 1), p0 = plane_sum(2 * c0);
+  for (int c = c0; c < c1; ++c) {
+    const float p1 = plane_sum(2 * c + 1), p2 = plane_sum(2 * c + 2);
+    const float acc = fmaf(0.25f, p2, fmaf(0.75f, p1, fmaf(0.75f, p0, 0.25f * pm)));
+    const int64_t C = ((int64_t)c * cy + jc) * cz + kc;
+    st1s(r1, C, (mask1[C] & BSP_MFLUID) ? 0.5f * acc : 0.0f);
+    pm = p1;
+    p0 = p2;
+  }
+}
+
+// 1 / tot for parity bits (pi << 10 | pj << 9 | pk << 8) and parent pattern,
+// copied to the device once per device (a synchronous copy: call it outside
+// any stream capture, as the solve entry points do); NULL if that failed.
+const float *tri_table() {
+  static std::once_flag once[64];
+  static bool ok[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+  std::call_once(once[dev & 63], [dev] {
+    float h[2048];
+    auto w = [](int par, int a) { return par ? (a ? 0.25f : 0.75f) : (a ? 0.75f : 0.25f); };
+    for (int idx = 0; idx < 2048; ++idx) {
+      const int pi = (idx >> 10) & 1, pj = (idx >> 9) & 1, pk = (idx >> 8) & 1, pat = idx & 255;
+      float tot = 0.0f;
+      for (int n = 0; n < 8; ++n)
+        if (pat & (1 << n)) tot += w(pi, n >> 2) * w(pj, (n >> 1) & 1) * w(pk, n & 1);
+      h[idx] = tot > 0.0f ? 1.0f / tot : 0.0f;
+    }
+    ok[dev & 63] = cudaMemcpyToSymbol(g_tri_invtot, h, sizeof(h)) == cudaSuccess;
+  });
+  if (!ok[dev & 63]) return nullptr;
+  void *p = nullptr;
+  if (cudaGetSymbolAddress(&p, g_tri_invtot) != cudaSuccess) return nullptr;
+  return static_cast<const float *>(p);
+}
+
+template <class T>
+void launch_tri_setup(uint8_t *pat, const Level<T> &f, const Level<T> &c, cudaStream_t s) {
+  const int64_t n = (int64_t)f.nx * f.ny * f.nz;
+  int64_t b = (n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  tri_pattern_kernel<<<(int)(b > 0 ? b : 1), 256, 0, s>>>(pat, f.mask, c.mask, f.nx, f.ny, f.nz,
+                                                          c.nx, c.ny, c.nz);
+}
+
+template <class T>
+void launch_tri_restrict(const Level<T> &f, const Level<T> &c, const T *rs, const SolverState *st,
+                         cudaStream_t s) {
+  const int cpc = 8;
+  dim3 grid((c.nz + 127) / 128, c.ny, (c.nx + cpc - 1) / cpc);
+  tri_restrict_kernel<T><<<grid, 128, 0, s>>>(c.r, rs, c.mask, f.nx, f.ny, f.nz, c.nx, c.ny,
+                                               c.nz, cpc, st);
+}
+
+// The trilinear prolongation + post-smoothing onto level 0 (TMA path only;
+// false when it cannot run).
+template <class T>
+bool launch_fine_up_tri(const Level<T> &f, const Level<T> &c, T *z, double *partials,
+                        float alpha, const uint8_t *pat, const float *tab, const SolverState *st,
+                        cudaStream_t s) {
+  if (!(tma_eligible(f.nz) && c.nz * 2 == f.nz && c.ny * 2 >= f.ny && c.nx * 2 >= f.nx && tab))
+    return false;
+  TmaMaps maps{};
+  if (!(make_map(&maps.a, tma_dtype<T>(), sizeof(T), f.r, f.nx, f.ny, f.nz, TmaGeom<T>::FW,
+                 TMA_ROWS) &&
+        make_map(&maps.m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, f.mask, f.nx, f.ny, f.nz, MASK_W,
+                 TMA_ROWS) &&
+        make_map(&maps.q, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, pat, f.nx, f.ny, f.nz, MASK_W,
+                 TMA_ROWS) &&
+        make_map(&maps.c, tma_dtype<T>(), sizeof(T), c.e, c.nx, c.ny, c.nz, TmaGeom<T>::CW,
+                 TmaGeom<T>::CROWS)))
+    return false;
+  TUp3<T> op{};
+  op.z = z;
+  op.partials = partials;
+  op.alpha = alpha;
+  op.tab = tab;
+  return launch_tma<T>(op, maps, f.nx, f.ny, f.nz, f.tiles, st, s);
+}
+
 // Level-0 restriction with the previous iteration's CG update fused in (TMA
 // path only; false when it cannot run).  f.r is r_in.
 template <class T>
 bool launch_fine_down_update(const Level<T> &f, const Level<T> &c, T *r_out, float *e,
                              const T *ps, const T *Ap, double *partials, const SolverState *st,
-                             cudaStream_t s) {
+                             cudaStream_t s, T *rs, const uint8_t *pat, const float *tab) {
   if (!tma_eligible(f.nz)) return false;
   TmaMaps maps{};
   if (!(make_map(&maps.a, tma_dtype<T>(), sizeof(T), f.r, f.nx, f.ny, f.nz, TmaGeom<T>::FW,
@@ -1296,6 +1575,27 @@ bool launch_fine_down_update(const Level<T> &f, const Level<T> &c, T *r_out, flo
                  TILE_ROWS) &&
         make_map(&maps.p, tma_dtype<T>(), sizeof(T), ps, f.nx, f.ny, f.nz, 128, TILE_ROWS)))
     return false;
+  if (rs) {
+    // trilinear: the scaled residual to rs (tri_restrict gathers it)
+    if (!pat || !tab ||
+        !make_map(&maps.q, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, pat, f.nx, f.ny, f.nz, MASK_W,
+                  TMA_ROWS))
+      return false;
+    TDownU<T, true> op{};
+    op.mask1 = c.mask;
+    op.r1 = c.r;
+    op.r_out = r_out;
+    op.e = e;
+    op.ps = ps;
+    op.partials = partials;
+    op.rs = rs;
+    op.tab = tab;
+    op.nx = f.nx;
+    op.ny = f.ny;
+    op.ny1 = c.ny;
+    op.nz1 = c.nz;
+    return launch_tma<T>(op, maps, f.nx, f.ny, f.nz, f.tiles, st, s);
+  }
   TDownU<T> op{};
   op.mask1 = c.mask;
   op.r1 = c.r;
@@ -1417,7 +1717,14 @@ void launch_tile_flags(int nx, int ny, int nz, const uint8_t *mask, uint8_t *fla
                                     cudaStream_t);                                              \
   template bool launch_fine_down_update<T>(const Level<T> &, const Level<T> &, T *, float *,   \
                                            const T *, const T *, double *, const SolverState *, \
-                                           cudaStream_t);                                       \
+                                           cudaStream_t, T *, const uint8_t *, const float *);  \
+  template void launch_tri_setup<T>(uint8_t *, const Level<T> &, const Level<T> &,              \
+                                    cudaStream_t);                                              \
+  template void launch_tri_restrict<T>(const Level<T> &, const Level<T> &, const T *,           \
+                                       const SolverState *, cudaStream_t);                      \
+  template bool launch_fine_up_tri<T>(const Level<T> &, const Level<T> &, T *, double *, float, \
+                                      const uint8_t *, const float *, const SolverState *,      \
+                                      cudaStream_t);                                            \
   template bool launch_fine_smooth<T>(const Level<T> &, const T *, T *, const SolverState *,    \
                                       cudaStream_t);                                            \
   template bool launch_fine_down_e<T>(const Level<T> &, const Level<T> &, const T *,            \

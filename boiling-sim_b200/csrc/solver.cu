@@ -67,6 +67,9 @@ int g_coarse_split = 2;
 // V-cycle stays an SPD preconditioner).  Measured at 384x384x256 (FP16
 // storage): 36 -> 31 inner iterations, 13.8 -> 12.8 ms per solve.
 int g_l1_sweeps = 2;
+// BSP_TUNE_L0_TRILINEAR: 1 uses trilinear transfers between levels 0 and 1
+// (fused TMA path, level 1 exactly half of level 0 in k), 0 piecewise-constant
+bool g_l0_trilinear = false;
 // BSP_TUNE_FUSE_UPDATE: CG update fused into the next level-0 restriction
 bool g_fuse_update_enabled = true;
 // BSP_TUNE_TEST_BARRIER_ERROR (tests only): the next host-driven solve starts
@@ -754,12 +757,13 @@ size_t storage_bytes(int storage) { return storage == BSP_STORE_FP32 ? 4 : 2; }
 //   SolverState | partials (3 * PARTIAL_STRIDE doubles) | x (n doubles) | e (n floats)
 //   | z, ps0, ps1, Ap, r, r2 (n T each) | per level l >= 1: mask, r, e (T)
 //   | per level l >= 1 ... ; level-0 effective-class scratch reuses the level-1 slot order.
+//   | level-0 parent patterns of the trilinear transfers (n bytes)
 //   | coarsest-level dense inverse (float), its FP64 build scratch, direct flag
 //   | per-level column-tile fluid flags (PARTIAL_STRIDE bytes per level)
 //   | FP32 scratch and grid-barrier word of the coarse-cycle kernel
 struct Layout {
   size_t state, partials, x, e, z, ps0, ps1, Ap, r, r2, lvl_mask[MAX_LEVELS], lvl_r[MAX_LEVELS],
-      lvl_e[MAX_LEVELS], eff0, cinv, cA, cflag, tflags, cscratch, cctl, total;
+      lvl_e[MAX_LEVELS], eff0, ppat, cinv, cA, cflag, tflags, cscratch, cctl, total;
   int L, dims[3 * MAX_LEVELS];
 };
 
@@ -783,6 +787,7 @@ Layout make_layout(int nx, int ny, int nz, int storage) {
   lo.r = take(ts * n);
   lo.r2 = take(ts * n);  // second level-0 residual buffer (fused CG update)
   lo.eff0 = take(n);
+  lo.ppat = take(n);  // level-0 parent patterns of the trilinear transfers
   lo.L = build_hierarchy(nx, ny, nz, lo.dims);
   for (int l = 1; l < lo.L; ++l) {
     const size_t nl = (size_t)lo.dims[3 * l] * lo.dims[3 * l + 1] * lo.dims[3 * l + 2];
@@ -823,6 +828,11 @@ struct Ctx {
   // the CG update of iteration q runs inside the level-0 restriction of
   // iteration q + 1 (TMA path); the residual then alternates between r and r2
   bool fuse = false;
+  // trilinear transfers between levels 0 and 1 (BSP_TUNE_L0_TRILINEAR, on the
+  // fused TMA path): the scaled residual goes through z (free between the
+  // restriction and the prolongation), patterns in lo.ppat
+  bool tri = false;
+  const float *tab = nullptr;
   T *r_write() const { return fuse ? (T *)(base + lo.r2) : lv[0].r; }  // rhat target
 };
 
@@ -859,6 +869,13 @@ Ctx<T> make_ctx(void *ws, const uint8_t *mask, int nx, int ny, int nz, int stora
                   ? (const uint8_t *)(cx.base + cx.lo.tflags + (size_t)l * PARTIAL_STRIDE)
                   : nullptr;
   }
+  if (g_l0_trilinear && cx.fuse && cx.lo.L >= 2) {
+    const Level<T> &c = cx.lv[1];
+    if (c.nz * 2 == nz && c.ny * 2 >= ny && c.nx * 2 >= nx) {
+      cx.tab = tri_table();  // built by the solve entry points, outside any capture
+      cx.tri = cx.tab != nullptr;
+    }
+  }
   return cx;
 }
 
@@ -894,6 +911,10 @@ cudaError_t setup_levels(Ctx<T> &cx, cudaStream_t s) {
                                                                       c.ny, c.nz);
     }
     prev = c.mask;
+  }
+  if (cx.tri) {
+    ProfScope ps(PROF_CONTROL, s);
+    launch_tri_setup<T>((uint8_t *)(cx.base + cx.lo.ppat), cx.lv[0], cx.lv[1], s);
   }
   // Every solver vector is zero on non-fluid cells and stays so (the kernels
   // write masked values; column tiles without fluid are never written).
@@ -969,12 +990,21 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
     {
       ProfScope ps(PROF_MG_DOWN0, s);
       if (!launch_fine_down_update<T>(in, cx.lv[1], l0.r, (float *)(cx.base + cx.lo.e), prev,
-                                      Ap, cx.partials, st, s))
+                                      Ap, cx.partials, st, s,
+                                      cx.tri ? (T *)(cx.base + cx.lo.z) : nullptr,
+                                      (const uint8_t *)(cx.base + cx.lo.ppat), cx.tab))
         return cudaErrorNotSupported;
     }
-    ProfScope ps(PROF_CONTROL, s);
-    inner_check_fused_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials,
-                                                       fine_grid_blocks(cx.nx, cx.ny, cx.nz));
+    {
+      ProfScope ps(PROF_CONTROL, s);
+      inner_check_fused_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials,
+                                                         fine_grid_blocks(cx.nx, cx.ny, cx.nz));
+    }
+    if (cx.tri) {
+      // the trilinear restriction of the scaled residual (in z) to level 1
+      ProfScope ps(PROF_MG_DOWN0, s);
+      launch_tri_restrict<T>(cx.lv[0], cx.lv[1], (const T *)(cx.base + cx.lo.z), st, s);
+    }
   } else {
     down(0, PROF_MG_DOWN0);
   }
@@ -1070,7 +1100,11 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
   const int nb0 = col ? fine_grid_blocks(cx.nx, cx.ny, cx.nz) : row_blocks((int64_t)cx.nx * cx.ny);
   {
     ProfScope ps(PROF_MG_UP0, s);
-    if (col)
+    if (cx.tri) {
+      if (!launch_fine_up_tri<T>(l0, cx.lv[1], z, cx.partials, g_mg_alpha,
+                                 (const uint8_t *)(cx.base + cx.lo.ppat), cx.tab, st, s))
+        return cudaErrorNotSupported;
+    } else if (col)
       launch_fine_up<T>(l0, cx.lv[1], z, cx.partials, g_mg_alpha, st, s);
     else
       mg_up_kernel<T, true><<<nb0, 256, 0, s>>>(l0, cx.lv[1], z, cx.partials, st, g_mg_alpha);
@@ -1154,7 +1188,7 @@ __global__ void __launch_bounds__(RED_THREADS) bnorm_kernel(SolverState *st,
 extern int g_fine_bi;
 struct SetupKey {
   const void *ws, *mask;
-  int nx, ny, nz, storage, fine_bi;
+  int nx, ny, nz, storage, fine_bi, tri;  // tri: the parent patterns were built too
 };
 static std::mutex g_setup_mu;
 static SetupKey g_setups[16];
@@ -1164,7 +1198,7 @@ static bool setup_cached(const void *ws, const void *mask, int nx, int ny, int n
   std::lock_guard<std::mutex> lk(g_setup_mu);
   for (const SetupKey &k : g_setups)
     if (k.ws == ws && k.mask == mask && k.nx == nx && k.ny == ny && k.nz == nz &&
-        k.storage == storage && k.fine_bi == g_fine_bi)
+        k.storage == storage && k.fine_bi == g_fine_bi && k.tri == (int)g_l0_trilinear)
       return true;
   return false;
 }
@@ -1173,7 +1207,8 @@ static void remember_setup(const void *ws, const void *mask, int nx, int ny, int
   std::lock_guard<std::mutex> lk(g_setup_mu);
   for (SetupKey &k : g_setups)
     if (k.ws == ws) k.ws = nullptr;  // a workspace holds one setup
-  g_setups[g_setup_next] = SetupKey{ws, mask, nx, ny, nz, storage, g_fine_bi};
+  g_setups[g_setup_next] = SetupKey{ws, mask, nx, ny, nz, storage, g_fine_bi,
+                                     (int)g_l0_trilinear};
   g_setup_next = (g_setup_next + 1) % 16;
 }
 
@@ -1554,6 +1589,7 @@ static void key_params(GraphKey &k, const BspSolveParams *p) {
   k.v.push_back((uintptr_t)g_coarse_tail_smem);
   k.v.push_back((uintptr_t)g_coarse_split);
   k.v.push_back((uintptr_t)g_l1_sweeps);
+  k.v.push_back((uintptr_t)g_l0_trilinear);
   k.v.push_back((uintptr_t)g_fuse_update_enabled);
   k.v.push_back((uintptr_t)g_fine_bi);
 }
@@ -1592,6 +1628,7 @@ extern "C" int bsp_solve_tol(float *p, const float *div_u, const uint8_t *mask, 
   if (params->storage < 0 || params->storage > 2 || params->check_every <= 0 ||
       params->max_inner <= 0 || params->max_outer < 0 || !(params->tol >= 0.0))
     return BSP_ERR_ARG;
+  if (g_l0_trilinear) tri_table();  // one synchronous copy per device, before any capture
   int st;
   if (params->use_graph) {
     const BspBatchItem item{p, div_u, mask, nx, ny, nz, dx, dt, rho, workspace, workspace_bytes};
@@ -1644,6 +1681,7 @@ extern "C" int bsp_solve_batch(int count, const BspBatchItem *items,
     if (it.workspace_bytes < bsp_solver_workspace_bytes(it.nx, it.ny, it.nz, params->storage))
       return BSP_ERR_WORKSPACE;
   }
+  if (g_l0_trilinear) tri_table();  // one synchronous copy per device, before any capture
   switch (params->storage) {
     case BSP_STORE_FP16:
       return solve_graph_batch<__half>(count, items, params, infos, stream);

@@ -79,7 +79,22 @@ int launch_cg_update_col(int nx, int ny, int nz, const uint8_t *tiles, float *e,
 template <class T>
 bool launch_fine_down_update(const Level<T> &f, const Level<T> &c, T *r_out, float *e,
                              const T *ps, const T *Ap, double *partials, const SolverState *st,
-                             cudaStream_t s);
+                             cudaStream_t s, T *rs = nullptr, const uint8_t *pat = nullptr,
+                             const float *tab = nullptr);
+// Trilinear transfers between levels 0 and 1 (mgfine.cu): the 1 / tot table
+// (device address, built once per device), the fine parent patterns (once per
+// geometry), the gather of the scaled residual into c.r, and the prolongation
+// + post-smoothing onto level 0 (TMA path; false when it cannot run).
+const float *tri_table();
+template <class T>
+void launch_tri_setup(uint8_t *pat, const Level<T> &f, const Level<T> &c, cudaStream_t s);
+template <class T>
+void launch_tri_restrict(const Level<T> &f, const Level<T> &c, const T *rs, const SolverState *st,
+                         cudaStream_t s);
+template <class T>
+bool launch_fine_up_tri(const Level<T> &f, const Level<T> &c, T *z, double *partials,
+                        float alpha, const uint8_t *pat, const float *tab, const SolverState *st,
+                        cudaStream_t s);
 bool fine_tma_available(int nz);
 // The coarse part of a V-cycle (levels 1 .. L-1) as one cooperative kernel
 // (mgcoarse.cu); false when not launched (the per-level kernels then run).

@@ -511,6 +511,7 @@ extern bool g_coarse_tail_smem;
 extern int g_coarse_split;
 extern int g_l1_sweeps;
 extern bool g_pcg_quad;
+extern bool g_l0_trilinear;
 namespace utc {
 extern int g_utc_nepi;
 }  // namespace utc
@@ -565,6 +566,10 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_CONV_EPILOGUE:
       if (value < 0 || value > 4) return BSP_ERR_ARG;
       bsp::utc::g_utc_nepi = value;
+      return BSP_OK;
+    case BSP_TUNE_L0_TRILINEAR:
+      if (value < 0 || value > 1) return BSP_ERR_ARG;
+      bsp::g_l0_trilinear = value != 0;
       return BSP_OK;
     case BSP_TUNE_PCG_QUAD:
       if (value < 0 || value > 1) return BSP_ERR_ARG;

@@ -76,6 +76,7 @@ extern "C" {
 #define BSP_TUNE_L1_SWEEPS 17     /* with COARSE_SPLIT: smoothing sweeps a side on level 1, 1 or 2
                                      (default) */
 #define BSP_TUNE_PCG_QUAD 18      /* reference-compatible PCG: four-cell form 1 (default), one-cell 0 */
+#define BSP_TUNE_L0_TRILINEAR 19  /* trilinear transfers between levels 0 and 1: 1 on, 0 off */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */
