@@ -1522,10 +1522,14 @@ void launch_tri_setup(uint8_t *pat, const Level<T> &f, const Level<T> &c, cudaSt
                                                           c.nx, c.ny, c.nz);
 }
 
+// Coarse planes per thread of tri_restrict (BSP_TUNE_TRI_CPC, default 8: a fine
+// plane's 4 x 4 sum serves two coarse planes; 1 and 2 measured slower).
+int g_tri_cpc = 8;
+
 template <class T>
 void launch_tri_restrict(const Level<T> &f, const Level<T> &c, const T *rs, const SolverState *st,
                          cudaStream_t s) {
-  const int cpc = 8;
+  const int cpc = g_tri_cpc;
   dim3 grid((c.nz + 127) / 128, c.ny, (c.nx + cpc - 1) / cpc);
   tri_restrict_kernel<T><<<grid, 128, 0, s>>>(c.r, rs, c.mask, f.nx, f.ny, f.nz, c.nx, c.ny,
                                                c.nz, cpc, st);

@@ -70,6 +70,7 @@ int g_l1_sweeps = 2;
 // BSP_TUNE_L0_TRILINEAR: 1 uses trilinear transfers between levels 0 and 1
 // (fused TMA path, level 1 exactly half of level 0 in k), 0 piecewise-constant
 bool g_l0_trilinear = false;
+extern int g_tri_cpc;  // BSP_TUNE_TRI_CPC (mgfine.cu)
 // BSP_TUNE_FUSE_UPDATE: CG update fused into the next level-0 restriction
 bool g_fuse_update_enabled = true;
 // BSP_TUNE_TEST_BARRIER_ERROR (tests only): the next host-driven solve starts
@@ -1590,6 +1591,7 @@ static void key_params(GraphKey &k, const BspSolveParams *p) {
   k.v.push_back((uintptr_t)g_coarse_split);
   k.v.push_back((uintptr_t)g_l1_sweeps);
   k.v.push_back((uintptr_t)g_l0_trilinear);
+  k.v.push_back((uintptr_t)g_tri_cpc);
   k.v.push_back((uintptr_t)g_fuse_update_enabled);
   k.v.push_back((uintptr_t)g_fine_bi);
 }

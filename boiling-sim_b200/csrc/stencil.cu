@@ -512,6 +512,7 @@ extern int g_coarse_split;
 extern int g_l1_sweeps;
 extern bool g_pcg_quad;
 extern bool g_l0_trilinear;
+extern int g_tri_cpc;
 namespace utc {
 extern int g_utc_nepi;
 }  // namespace utc
@@ -566,6 +567,10 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_CONV_EPILOGUE:
       if (value < 0 || value > 4) return BSP_ERR_ARG;
       bsp::utc::g_utc_nepi = value;
+      return BSP_OK;
+    case BSP_TUNE_TRI_CPC:
+      if (value < 1 || value > 64) return BSP_ERR_ARG;
+      bsp::g_tri_cpc = value;
       return BSP_OK;
     case BSP_TUNE_L0_TRILINEAR:
       if (value < 0 || value > 1) return BSP_ERR_ARG;
