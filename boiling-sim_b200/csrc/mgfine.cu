@@ -22,6 +22,7 @@
 
 #include <mutex>
 #include <type_traits>
+#include <utility>
 
 #include "bsp_common.cuh"
 #include "solver.cuh"
@@ -955,13 +956,73 @@ struct TmaSmem {
   static constexpr int TOTAL = OFF_BAR + NST * 8;
 };
 
+// The scalar update after a reducing level-0 kernel, run by its last CTA
+// (kind != TAIL_NONE): every CTA, once its partial is written, takes a ticket;
+// the CTA with the last one sums the partials in a fixed order (thread t the
+// blocks t, t + TILE_THREADS, ..., then a fixed shuffle tree and the warps in
+// order) and applies the update, then resets the ticket counter.
+__device__ __forceinline__ void fine_tail(SolverState *st, int kind, const double *partials) {
+  if (kind == TAIL_NONE || !partials) return;
+  __shared__ int s_last;
+  __shared__ double s_w[TILE_WARPS];
+  const int nb = (int)(gridDim.x * gridDim.y * gridDim.z);
+  __syncthreads();  // this CTA's partial is written
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&st->tail_count, 1) == nb - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double v = 0.0;
+  for (int b = threadIdx.x; b < nb; b += TILE_THREADS)
+    v += *reinterpret_cast<const volatile double *>(partials + b);
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) s_w[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < TILE_WARPS; ++w) t += s_w[w];
+    apply_tail(st, kind, t);
+    st->tail_count = 0;
+  }
+}
+
+// An op's FP64 partials (slot 0, one per CTA), or NULL for ops that reduce nothing.
+template <class Op, class = void>
+struct has_partials : std::false_type {};
+template <class Op>
+struct has_partials<Op, std::void_t<decltype(std::declval<Op>().partials)>> : std::true_type {};
+template <class Op>
+__device__ __forceinline__ const double *op_partials(const Op &op) {
+  if constexpr (has_partials<Op>::value)
+    return op.partials;
+  else
+    return nullptr;
+}
+
+// The host side: one pending request, consumed by the next TMA launch.
+struct TailReq {
+  SolverState *st = nullptr;
+  int kind = TAIL_NONE;
+  bool taken = false;
+};
+static thread_local TailReq t_tail;
+void fine_tail_request(SolverState *st, int kind) { t_tail = TailReq{st, kind, false}; }
+bool fine_tail_taken() {
+  const bool t = t_tail.taken;
+  t_tail = TailReq{};
+  return t;
+}
+
 template <class T, class Op>
 __global__ void __launch_bounds__(TILE_THREADS, Op::MIN_BLOCKS) fine_tma_kernel(
     Op op, const __grid_constant__ TmaMaps maps, int nx, int ny, int nz, int bi,
-    const uint8_t *tiles, const SolverState *st) {
+    const uint8_t *tiles, const SolverState *st, SolverState *tail_st, int tail_kind) {
   if (st->inner_done) return;  // uniform: the whole grid returns
   if (tiles && !tiles[block_linear()]) {
     if (threadIdx.x == 0) op.skip();
+    fine_tail(tail_st, tail_kind, op_partials(op));
     return;
   }
   using L = TmaSmem<T, Op>;
@@ -1101,6 +1162,7 @@ __global__ void __launch_bounds__(TILE_THREADS, Op::MIN_BLOCKS) fine_tma_kernel(
   }
   if (!ok) atomicExch(const_cast<int *>(&st->dev_error), 1);
   op.template finish<TILE_WARPS>(sh);
+  fine_tail(tail_st, tail_kind, op_partials(op));
 }
 
 // ---- TMA launch helpers (host) ----------------------------------------------------------
@@ -1115,9 +1177,17 @@ static bool launch_tma(const Op &op, const TmaMaps &maps, int nx, int ny, int nz
                        const uint8_t *tiles, const SolverState *st, cudaStream_t s) {
   using L = TmaSmem<T, Op>;
   if (!smem_opt_in((const void *)fine_tma_kernel<T, Op>, L::TOTAL)) return false;
+  // a pending scalar-update request goes with this launch (ops that write a
+  // partial per CTA to slot 0 of their partials)
+  SolverState *tst = t_tail.st;
+  int tkind = tst ? t_tail.kind : TAIL_NONE;
+  t_tail.st = nullptr;
+  t_tail.kind = TAIL_NONE;
   fine_tma_kernel<T, Op><<<fine_grid(nx, ny, nz), TILE_THREADS, L::TOTAL, s>>>(
-      op, maps, nx, ny, nz, fine_bi(nx, ny, nz), tiles, st);
-  return cudaGetLastError() == cudaSuccess;
+      op, maps, nx, ny, nz, fine_bi(nx, ny, nz), tiles, st, tst, tkind);
+  const bool ok = cudaGetLastError() == cudaSuccess;
+  if (ok && tkind != TAIL_NONE) t_tail.taken = true;
+  return ok;
 }
 
 // ---- FP64 residual on the column layout --------------------------------------------------

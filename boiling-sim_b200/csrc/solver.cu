@@ -70,6 +70,9 @@ int g_l1_sweeps = 2;
 // BSP_TUNE_L0_TRILINEAR: 1 uses trilinear transfers between levels 0 and 1
 // (fused TMA path, level 1 exactly half of level 0 in k), 0 piecewise-constant
 bool g_l0_trilinear = false;
+// BSP_TUNE_FUSE_SCALARS: 1 runs the inner check, beta and alpha in the last CTA
+// of the level-0 TMA kernel before each (no one-block launches); 0 launches them
+bool g_fuse_scalars = true;
 extern int g_tri_cpc;  // BSP_TUNE_TRI_CPC (mgfine.cu)
 // BSP_TUNE_FUSE_UPDATE: CG update fused into the next level-0 restriction
 bool g_fuse_update_enabled = true;
@@ -660,8 +663,7 @@ __global__ void __launch_bounds__(RED_THREADS) beta_kernel(SolverState *st,
   if (st->inner_done) return;
   const double rz = reduce_slot(partials, 0, nblocks, false);
   if (threadIdx.x != 0) return;
-  st->beta = (st->inner_it == 0 || st->rz == 0.0) ? 0.0 : rz / st->rz;
-  st->rz = rz;
+  apply_beta(st, rz);
 }
 
 __global__ void __launch_bounds__(RED_THREADS) alpha_kernel(SolverState *st,
@@ -669,8 +671,7 @@ __global__ void __launch_bounds__(RED_THREADS) alpha_kernel(SolverState *st,
   if (st->inner_done) return;
   const double pap = reduce_slot(partials, 0, nblocks, false);
   if (threadIdx.x != 0) return;
-  st->alpha = pap > 0.0 ? st->rz / pap : 0.0;
-  st->pending = 1;  // applied by the next iteration's fused restriction, if any
+  apply_alpha(st, pap);  // applied by the next iteration's fused restriction, if any
 }
 
 // Inner check after the restriction that applied the pending CG update (the
@@ -682,20 +683,8 @@ __global__ void __launch_bounds__(RED_THREADS) inner_check_fused_kernel(SolverSt
                                                                         int nblocks) {
   if (st->inner_done) return;
   const double rr = reduce_slot(partials, 0, nblocks, false);
-  if (threadIdx.x != 0 || !st->pending) return;
-  st->pending = 0;
-  st->inner_it += 1;
-  st->total_inner += 1;
-  st->rr_inner = rr;
-  if (st->dev_error) {
-    st->status = BSP_ERR_TIMEOUT;
-    st->inner_done = 1;
-    st->done = 1;
-    return;
-  }
-  if (!(rr == rr) || rr <= st->eta_eff * st->eta_eff * st->rhat_norm2 ||
-      st->inner_it >= st->max_inner || st->alpha == 0.0)
-    st->inner_done = 1;
+  if (threadIdx.x != 0) return;
+  apply_inner_check(st, rr);
 }
 
 __global__ void __launch_bounds__(RED_THREADS) inner_check_kernel(SolverState *st,
@@ -988,15 +977,19 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
     Level<T> in = cx.lv[0];
     in.r = it_parity ? b0 : b1;
     l0.r = it_parity ? b1 : b0;
+    bool tail = false;
     {
       ProfScope ps(PROF_MG_DOWN0, s);
-      if (!launch_fine_down_update<T>(in, cx.lv[1], l0.r, (float *)(cx.base + cx.lo.e), prev,
-                                      Ap, cx.partials, st, s,
-                                      cx.tri ? (T *)(cx.base + cx.lo.z) : nullptr,
-                                      (const uint8_t *)(cx.base + cx.lo.ppat), cx.tab))
-        return cudaErrorNotSupported;
+      // the inner check runs in the restriction's last CTA (BSP_TUNE_FUSE_SCALARS)
+      if (g_fuse_scalars) fine_tail_request(st, TAIL_INNER_CHECK);
+      const bool ok = launch_fine_down_update<T>(
+          in, cx.lv[1], l0.r, (float *)(cx.base + cx.lo.e), prev, Ap, cx.partials, st, s,
+          cx.tri ? (T *)(cx.base + cx.lo.z) : nullptr, (const uint8_t *)(cx.base + cx.lo.ppat),
+          cx.tab);
+      tail = fine_tail_taken();
+      if (!ok) return cudaErrorNotSupported;
     }
-    {
+    if (!tail) {
       ProfScope ps(PROF_CONTROL, s);
       inner_check_fused_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials,
                                                          fine_grid_blocks(cx.nx, cx.ny, cx.nz));
@@ -1099,31 +1092,41 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
   }
   T *z = (T *)(cx.base + cx.lo.z);
   const int nb0 = col ? fine_grid_blocks(cx.nx, cx.ny, cx.nz) : row_blocks((int64_t)cx.nx * cx.ny);
+  bool tail = false;
   {
     ProfScope ps(PROF_MG_UP0, s);
+    if (g_fuse_scalars && col) fine_tail_request(st, TAIL_BETA);
     if (cx.tri) {
-      if (!launch_fine_up_tri<T>(l0, cx.lv[1], z, cx.partials, g_mg_alpha,
-                                 (const uint8_t *)(cx.base + cx.lo.ppat), cx.tab, st, s))
-        return cudaErrorNotSupported;
-    } else if (col)
+      const bool ok = launch_fine_up_tri<T>(l0, cx.lv[1], z, cx.partials, g_mg_alpha,
+                                            (const uint8_t *)(cx.base + cx.lo.ppat), cx.tab, st,
+                                            s);
+      tail = fine_tail_taken();
+      if (!ok) return cudaErrorNotSupported;
+    } else if (col) {
       launch_fine_up<T>(l0, cx.lv[1], z, cx.partials, g_mg_alpha, st, s);
-    else
+      tail = fine_tail_taken();
+    } else {
       mg_up_kernel<T, true><<<nb0, 256, 0, s>>>(l0, cx.lv[1], z, cx.partials, st, g_mg_alpha);
+    }
   }
-  {
+  if (!tail) {
     ProfScope ps(PROF_CONTROL, s);
     beta_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials, nb0);
   }
+  tail = false;
   {
     ProfScope ps(PROF_CG_PSAP, s);
-    if (col)
+    if (col) {
+      if (g_fuse_scalars) fine_tail_request(st, TAIL_ALPHA);
       launch_fine_psap<T>(cx.nx, cx.ny, cx.nz, cx.mask0, cx.lv[0].tiles, z, prev, cur, Ap,
                           cx.partials, st, s);
-    else
+      tail = fine_tail_taken();
+    } else {
       cg_ps_ap_kernel<T><<<nb0, 256, 0, s>>>(cx.nx, cx.ny, cx.nz, cx.mask0, z, prev, cur, Ap,
                                              cx.partials, st);
+    }
   }
-  {
+  if (!tail) {
     ProfScope ps(PROF_CONTROL, s);
     alpha_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials, nb0);
   }
@@ -1592,6 +1595,7 @@ static void key_params(GraphKey &k, const BspSolveParams *p) {
   k.v.push_back((uintptr_t)g_l1_sweeps);
   k.v.push_back((uintptr_t)g_l0_trilinear);
   k.v.push_back((uintptr_t)g_tri_cpc);
+  k.v.push_back((uintptr_t)g_fuse_scalars);
   k.v.push_back((uintptr_t)g_fuse_update_enabled);
   k.v.push_back((uintptr_t)g_fine_bi);
 }

@@ -2,6 +2,8 @@
 #pragma once
 #include <cstdint>
 
+#include "bsp_common.cuh"
+
 namespace bsp {
 
 constexpr int MAX_LEVELS = 12;
@@ -36,7 +38,49 @@ struct SolverState {
   // loop guards of the graph-driven solve: counted by the condition kernels
   // themselves so every WHILE node ends even if other state went wrong
   int guard_inner, guard_outer;
+  int tail_count;  // CTAs of the current level-0 kernel done (its last CTA runs the scalar update)
 };
+
+// The scalar updates that follow a level-0 kernel's FP64 partial sums: by a
+// one-block kernel (solver.cu) or by the last CTA of the producing kernel
+// (fine_tma_kernel), the same code either way.
+enum TailKind { TAIL_NONE = 0, TAIL_INNER_CHECK = 1, TAIL_BETA = 2, TAIL_ALPHA = 3 };
+// after the fused update + restriction: count the iteration, test ||r||
+__device__ __forceinline__ void apply_inner_check(SolverState *st, double rr) {
+  if (!st->pending) return;
+  st->pending = 0;
+  st->inner_it += 1;
+  st->total_inner += 1;
+  st->rr_inner = rr;
+  if (st->dev_error) {
+    st->status = BSP_ERR_TIMEOUT;
+    st->inner_done = 1;
+    st->done = 1;
+    return;
+  }
+  if (!(rr == rr) || rr <= st->eta_eff * st->eta_eff * st->rhat_norm2 ||
+      st->inner_it >= st->max_inner || st->alpha == 0.0)
+    st->inner_done = 1;
+}
+// after the prolongation (z and r.z): beta = rz_new / rz
+__device__ __forceinline__ void apply_beta(SolverState *st, double rz) {
+  st->beta = (st->inner_it == 0 || st->rz == 0.0) ? 0.0 : rz / st->rz;
+  st->rz = rz;
+}
+// after A ps (ps.Ap): alpha = rz / ps.Ap; the update is applied by the next restriction
+__device__ __forceinline__ void apply_alpha(SolverState *st, double pap) {
+  st->alpha = pap > 0.0 ? st->rz / pap : 0.0;
+  st->pending = 1;
+}
+__device__ __forceinline__ void apply_tail(SolverState *st, int kind, double v) {
+  if (kind == TAIL_INNER_CHECK) apply_inner_check(st, v);
+  else if (kind == TAIL_BETA) apply_beta(st, v);
+  else if (kind == TAIL_ALPHA) apply_alpha(st, v);
+}
+// Host: the next level-0 TMA launch runs `kind` in its last CTA;
+// fine_tail_taken() says whether it did (clearing the request either way).
+void fine_tail_request(SolverState *st, int kind);
+bool fine_tail_taken();
 
 // Level-0 kernels on the column layout (mgfine.cu); nz % 4 == 0 required.
 int fine_grid_blocks(int nx, int ny, int nz);

@@ -513,6 +513,7 @@ extern int g_l1_sweeps;
 extern bool g_pcg_quad;
 extern bool g_l0_trilinear;
 extern int g_tri_cpc;
+extern bool g_fuse_scalars;
 namespace utc {
 extern int g_utc_nepi;
 }  // namespace utc
@@ -567,6 +568,10 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_CONV_EPILOGUE:
       if (value < 0 || value > 4) return BSP_ERR_ARG;
       bsp::utc::g_utc_nepi = value;
+      return BSP_OK;
+    case BSP_TUNE_FUSE_SCALARS:
+      if (value < 0 || value > 1) return BSP_ERR_ARG;
+      bsp::g_fuse_scalars = value != 0;
       return BSP_OK;
     case BSP_TUNE_TRI_CPC:
       if (value < 1 || value > 64) return BSP_ERR_ARG;
