@@ -71,8 +71,11 @@ int g_l1_sweeps = 2;
 // (fused TMA path, level 1 exactly half of level 0 in k), 0 piecewise-constant
 bool g_l0_trilinear = false;
 // BSP_TUNE_FUSE_SCALARS: 1 runs the inner check, beta and alpha in the last CTA
-// of the level-0 TMA kernel before each (no one-block launches); 0 launches them
-bool g_fuse_scalars = true;
+// of the level-0 TMA kernel before each (no one-block launches); 0 (default)
+// launches them.  Measured at 384x384x256: 13.53 ms per solve fused against
+// 13.21 ms with the launches -- every CTA's fence and ticket before it exits
+// costs each level-0 kernel about 7 us, more than the launches it saves.
+bool g_fuse_scalars = false;
 extern int g_tri_cpc;  // BSP_TUNE_TRI_CPC (mgfine.cu)
 // BSP_TUNE_FUSE_UPDATE: CG update fused into the next level-0 restriction
 bool g_fuse_update_enabled = true;

@@ -339,8 +339,8 @@ def test_l0_trilinear_transfers_converge_faster(cuda, storage, spec):
 @pytest.mark.parametrize("storage", ["fp32", "fp16"])
 def test_scalars_in_last_cta_match_one_block_kernels(cuda, pot64, storage):
     """The inner check, beta and alpha computed by the last CTA of the level-0
-    kernel before each (BSP_TUNE_FUSE_SCALARS = 1, the default) and by the
-    one-block kernels (= 0) apply the same updates to FP64 sums taken in
+    kernel before each (BSP_TUNE_FUSE_SCALARS = 1) and by the one-block
+    kernels (= 0, the default) apply the same updates to FP64 sums taken in
     another fixed order: the same iteration counts and the same pressure to
     FP64 rounding of the recurrences."""
     from boilingsim_b200 import _lib
@@ -356,7 +356,7 @@ def test_scalars_in_last_cta_match_one_block_kernels(cuda, pot64, storage):
                 assert res.status == 0
                 out[fuse, graph] = res
     finally:
-        _lib.call("bsp_set_tuning", 21, 1)
+        _lib.call("bsp_set_tuning", 21, 0)
     for graph in (False, True):
         a, b = out[1, graph], out[0, graph]
         assert (a.inner_iterations, a.outer_iterations) == (b.inner_iterations, b.outer_iterations)
