@@ -102,9 +102,32 @@ def _workload():
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """SM clock and clock-event reasons sampled every 10 ms during the timed
+    region (NVML reads from a background thread; nvidia-smi at 100 ms when
+    NVML is not importable).  Reads only: no clock or power setting changes."""
+
+    # NVML clock-event reason bits
+    REASONS = {0x8: "hw_slowdown", 0x40: "hw_thermal_slowdown", 0x20: "sw_thermal_slowdown",
+               0x4: "sw_power_cap"}
 
     def __init__(self, index: int):
+        import threading
+
+        self.samples, self.max_mhz, self.reasons = [], 0.0, set()
+        self.proc = None
+        self.stop_ev = threading.Event()
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._run, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         self.path = f"/tmp/bsp_clocks_{os.getpid()}.csv"
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -116,7 +139,29 @@ class Clocks:
         except Exception:
             self.proc = None
 
+    def _run(self):
+        nv = self.nvml
+        while not self.stop_ev.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for b, nm in self.REASONS.items():
+                    if bits & b:
+                        self.reasons.add(nm)
+            except Exception:
+                pass
+            self.stop_ev.wait(0.01)
+
     def stop(self):
+        if self.nvml is not None:
+            self.stop_ev.set()
+            self.thread.join(timeout=2)
+            sm = self.samples
+            if not sm:
+                return None
+            load = [x for x in sm if x > 0.5 * max(sm)] or sm
+            return {"sm_mhz": float(np.median(load)), "sm_max_mhz": self.max_mhz,
+                    "reasons": sorted(self.reasons), "samples": len(sm), "source": "nvml, 10 ms"}
         if self.proc is None:
             return None
         self.proc.terminate()
@@ -142,7 +187,7 @@ class Clocks:
             return None
         load = [s for s in sm if s > 0.5 * max(sm)] or sm
         return {"sm_mhz": float(np.median(load)), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi, 100 ms"}
 
 
 def cpu_reference(mat, ux, uy, uz, ref_iters):
