@@ -119,6 +119,14 @@ __device__ __forceinline__ float wcalc(uint32_t ns) {
 __shared__ float s_wtab[8];
 __device__ __forceinline__ float wdinv_ns(uint32_t ns) { return s_wtab[ns & 7u]; }
 __device__ __forceinline__ float wdq(uint32_t mw, int q) { return s_wtab[(mw >> (8 * q)) & 7u]; }
+// Ops with SUM6 = true take s as the plain sum of the six neighbour values
+// (their smoothing step is written without the n_solid x centre term);
+// the others s = that sum + n_solid x centre.
+template <class Op, class = void>
+struct op_sum6 : std::false_type {};
+template <class Op>
+struct op_sum6<Op, std::void_t<decltype(Op::SUM6)>> : std::integral_constant<bool, Op::SUM6> {};
+constexpr float FOMEGA_C = 1.0f - 6.0f / 7.0f;  // 1 - OMEGA
 __device__ __forceinline__ uint32_t mload4(const uint8_t *m, int64_t o) {
   return __ldg(reinterpret_cast<const uint32_t *>(m + o));
 }
@@ -212,6 +220,7 @@ struct PsApOp {
 // partial r.z
 template <class T>
 struct UpOp {
+  static constexpr bool SUM6 = true;
   const uint8_t *mask;
   const T *r, *e1;
   T *z;
@@ -244,8 +253,10 @@ struct UpOp {
     float zz[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
+      // z = e + w (r - A e) = (1 - OMEGA) e + w (r + sum6), w = OMEGA / D
       const float e = q4(v, q);
-      const float zq = fmaf(q4(rr, q) - (6.0f * e - s[q]), wdq(mc, q), e);
+      const float w = wdq(mc, q);
+      const float zq = w > 0.0f ? fmaf(w, q4(rr, q) + s[q], FOMEGA_C * e) : e;
       zz[q] = rt(__uint_as_float(__float_as_uint(zq) & fluid_word(mc, q)), z);
     }
     acc += dot4w(rr, zz);
@@ -401,10 +412,14 @@ __global__ void __launch_bounds__(TILE_THREADS, 4) fine_tile_kernel(Op op, int n
       float s[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const float ns = (float)((mc >> (8 * q)) & 7u);
-        s[q] = fmaf(ns, q4(vc, q),
-                    ((q4(vm, q) + q4(vn, q)) + (q4(vjm, q) + q4(vjp, q))) +
-                        (q4(vb, q) + q4(vf, q)));
+        const float sum6 = ((q4(vm, q) + q4(vn, q)) + (q4(vjm, q) + q4(vjp, q))) +
+                           (q4(vb, q) + q4(vf, q));
+        if constexpr (op_sum6<Op>::value) {
+          s[q] = sum6;
+        } else {
+          const float ns = (float)((mc >> (8 * q)) & 7u);
+          s[q] = fmaf(ns, q4(vc, q), sum6);
+        }
       }
       if (act) op.emit(i, j, k, o, mc, vc, s, xch);
     }
@@ -522,7 +537,7 @@ struct TPsAp {
 
 template <class T>
 struct TUp {
-  static constexpr bool HAS_B = false, HAS_C = true, HAS_EP = false;
+  static constexpr bool HAS_B = false, HAS_C = true, HAS_EP = false, SUM6 = true;
   static constexpr int STAGES = 4, MIN_BLOCKS = 4;
   T *z;
   double *partials;
@@ -552,8 +567,10 @@ struct TUp {
     float zz[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
+      // z = e + w (r - A e) = (1 - OMEGA) e + w (r + sum6), w = OMEGA / D
       const float e = q4(e4, q);
-      const float zq = fmaf(q4(r4, q) - (6.0f * e - s[q]), wdq(mc, q), e);
+      const float w = wdq(mc, q);
+      const float zq = w > 0.0f ? fmaf(w, q4(r4, q) + s[q], FOMEGA_C * e) : e;
       zz[q] = rt(__uint_as_float(__float_as_uint(zq) & fluid_word(mc, q)), z);
     }
     acc += dot4w(r4, zz);
@@ -1029,6 +1046,9 @@ __global__ void __launch_bounds__(TILE_THREADS, Op::MIN_BLOCKS) fine_tma_kernel(
   extern __shared__ __align__(128) unsigned char dsm[];
   __shared__ double sh[TILE_WARPS];
   __shared__ float2 xch[(TILE_ROWS / 2) * 32];
+  // k-halo operands (k0 - 1, k0 + 128) of the output rows, per plane parity,
+  // computed by the second halo warp one plane ahead
+  __shared__ float hbuf[2][TILE_ROWS + 2][2];
   float4(*plane_buf)[TMA_ROWS][32] = reinterpret_cast<float4(*)[TMA_ROWS][32]>(dsm + L::OFF_PLANE);
   uint64_t *bars = reinterpret_cast<uint64_t *>(dsm + L::OFF_BAR);
   const int lane = threadIdx.x & 31;
@@ -1102,11 +1122,18 @@ __global__ void __launch_bounds__(TILE_THREADS, Op::MIN_BLOCKS) fine_tma_kernel(
     const StageView<T> v = view(pbase);
     vm = op.val4(v, rr, lane, v.mask4(rr, lane));
   }
+  // the second halo warp's lanes 0..15: the k-halo operand of output row
+  // 1 + lane / 2, side lane % 2 (k0 - 1, k0 + 128), of plane p
+  const bool hw = warp == TILE_ROWS + 1 && lane < 2 * TILE_ROWS;
+  auto halo = [&](const StageView<T> &v, int p) {
+    if (hw) hbuf[p & 1][1 + (lane >> 1)][lane & 1] = op.val1(v, 1 + (lane >> 1), (lane & 1) ? 128 : -1);
+  };
   wait(i0);
   {
     const StageView<T> v = view(i0);
     mc = v.mask4(rr, lane);
     vc = op.val4(v, rr, lane, mc);
+    halo(v, i0);
   }
   plane_buf[i0 & 1][rr][lane] = vc;
   __syncthreads();
@@ -1121,26 +1148,30 @@ __global__ void __launch_bounds__(TILE_THREADS, Op::MIN_BLOCKS) fine_tma_kernel(
     const uint32_t mn = vnx.mask4(rr, lane);
     const float4 vn = op.val4(vnx, rr, lane, mn);
     plane_buf[(i + 1) & 1][rr][lane] = vn;
+    if (i + 1 < i1) halo(vnx, i + 1);
     if (out) {
       const StageView<T> v = view(i);
       const float4 vjm = plane_buf[i & 1][rr - 1][lane];
       const float4 vjp = plane_buf[i & 1][rr + 1][lane];
       float vkm = __shfl_up_sync(0xffffffffu, vc.w, 1);
       float vkp = __shfl_down_sync(0xffffffffu, vc.x, 1);
-      // k halo of the row from the tile's padding (zero outside the grid)
-      float vh = 0.0f;
-      if (lane == 0 || lane == 31) vh = op.val1(v, rr, lane == 0 ? -1 : 128);
-      if (lane == 0) vkm = vh;
-      if (lane == 31) vkp = vh;
+      // k halo of the row from the tile's padding (zero outside the grid),
+      // computed one plane ahead by the halo warp
+      if (lane == 0) vkm = hbuf[i & 1][rr][0];
+      if (lane == 31) vkp = hbuf[i & 1][rr][1];
       const float4 vb = make_float4(vkm, vc.x, vc.y, vc.z);
       const float4 vf = make_float4(vc.y, vc.z, vc.w, vkp);
       float s[4];
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
-        const float ns = (float)((mc >> (8 * q)) & 7u);
-        s[q] = fmaf(ns, q4(vc, q),
-                    ((q4(vm, q) + q4(vn, q)) + (q4(vjm, q) + q4(vjp, q))) +
-                        (q4(vb, q) + q4(vf, q)));
+        const float sum6 = ((q4(vm, q) + q4(vn, q)) + (q4(vjm, q) + q4(vjp, q))) +
+                           (q4(vb, q) + q4(vf, q));
+        if constexpr (op_sum6<Op>::value) {
+          s[q] = sum6;
+        } else {
+          const float ns = (float)((mc >> (8 * q)) & 7u);
+          s[q] = fmaf(ns, q4(vc, q), sum6);
+        }
       }
       if (act) op.emit(v, rr, lane, i, j, o, mc, vc, s, xch);
     }
@@ -1306,10 +1337,14 @@ int num_sms();
 // GPU idle).  Even, because the restriction pairs planes inside one CTA.
 int g_fine_bi = 0;  // BSP_TUNE_FINE_BI: plane chunk of the level-0 tiles (0 = rule)
 
+// BSP_TUNE_FINE_CTAS: CTAs per SM the plane chunking aims for (the chunk is
+// the largest even plane count that still gives that many CTAs)
+int g_fine_ctas = 2;
+
 int fine_bi(int nx, int ny, int nz) {
   if (g_fine_bi > 0) return g_fine_bi < 2 ? 2 : (g_fine_bi & ~1);
   const int64_t cols = (int64_t)((nz / 4 + 31) / 32) * ((ny + TILE_ROWS - 1) / TILE_ROWS);
-  const int64_t target = 2LL * num_sms();
+  const int64_t target = (int64_t)g_fine_ctas * num_sms();
   int bi = 16;
   while (bi > 2 && cols * ((nx + bi - 1) / bi) < target) bi -= 2;
   return bi;

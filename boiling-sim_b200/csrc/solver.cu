@@ -76,6 +76,7 @@ bool g_l0_trilinear = false;
 // 13.21 ms with the launches -- every CTA's fence and ticket before it exits
 // costs each level-0 kernel about 7 us, more than the launches it saves.
 bool g_fuse_scalars = false;
+extern int g_fine_ctas;  // BSP_TUNE_FINE_CTAS (mgfine.cu)
 extern int g_tri_cpc;  // BSP_TUNE_TRI_CPC (mgfine.cu)
 // BSP_TUNE_FUSE_UPDATE: CG update fused into the next level-0 restriction
 bool g_fuse_update_enabled = true;
@@ -1196,6 +1197,7 @@ extern int g_fine_bi;
 struct SetupKey {
   const void *ws, *mask;
   int nx, ny, nz, storage, fine_bi, tri;  // tri: the parent patterns were built too
+  int fine_ctas;                           // tile flags follow the plane chunking
 };
 static std::mutex g_setup_mu;
 static SetupKey g_setups[16];
@@ -1205,7 +1207,8 @@ static bool setup_cached(const void *ws, const void *mask, int nx, int ny, int n
   std::lock_guard<std::mutex> lk(g_setup_mu);
   for (const SetupKey &k : g_setups)
     if (k.ws == ws && k.mask == mask && k.nx == nx && k.ny == ny && k.nz == nz &&
-        k.storage == storage && k.fine_bi == g_fine_bi && k.tri == (int)g_l0_trilinear)
+        k.storage == storage && k.fine_bi == g_fine_bi && k.tri == (int)g_l0_trilinear &&
+        k.fine_ctas == g_fine_ctas)
       return true;
   return false;
 }
@@ -1215,7 +1218,7 @@ static void remember_setup(const void *ws, const void *mask, int nx, int ny, int
   for (SetupKey &k : g_setups)
     if (k.ws == ws) k.ws = nullptr;  // a workspace holds one setup
   g_setups[g_setup_next] = SetupKey{ws, mask, nx, ny, nz, storage, g_fine_bi,
-                                     (int)g_l0_trilinear};
+                                     (int)g_l0_trilinear, g_fine_ctas};
   g_setup_next = (g_setup_next + 1) % 16;
 }
 
@@ -1599,6 +1602,7 @@ static void key_params(GraphKey &k, const BspSolveParams *p) {
   k.v.push_back((uintptr_t)g_l0_trilinear);
   k.v.push_back((uintptr_t)g_tri_cpc);
   k.v.push_back((uintptr_t)g_fuse_scalars);
+  k.v.push_back((uintptr_t)g_fine_ctas);
   k.v.push_back((uintptr_t)g_fuse_update_enabled);
   k.v.push_back((uintptr_t)g_fine_bi);
 }
