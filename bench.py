@@ -935,6 +935,12 @@ def run_projection(args, dev, rank, world, local, dist):
     largest = {"kernel": names[top], "share_of_step": round(prof_ms[top] / total_ms, 3),
                "ms_per_step": round(prof_ms[top] / args.steps, 4),
                "launches_per_step": prof_n[top] / args.steps}
+    if top == 11:
+        cycles = prof_n[2] / args.steps
+        largest.update({"bound": "latency (six tile-kernel launches per V-cycle on levels 1-2, "
+                                 "L2-resident: two smoothing sweeps a side on level 1)",
+                        "us_per_cycle": round(1e3 * prof_ms[11] / max(prof_n[2], 1), 2),
+                        "cycles_per_step": cycles})
     if top == 7:
         # one level-0 prolongation per V-cycle and one cooperative launch for
         # the levels below the tile-kernel ones
