@@ -170,3 +170,46 @@ def solve_tolerance(div, mat, dx, dt, rho, tol=1e-6, storage="fp32", **kw) -> So
     div_t = torch.as_tensor(np.ascontiguousarray(div, np.float32)).cuda()
     solver = TolSolver(cell_mask(mat_t), storage)
     return solver.solve(div_t, dx, dt, rho, tol=tol, **kw)
+
+
+def main(argv=None):
+    """``python -m boilingsim_b200.solver solve [--storage fp16] [--max-inner N]
+    [--graph]``: one tolerance solve on the 384x384x256 benchmark pot
+    (synthetic velocities, seed 7); prints iterations, residual and time.
+    With a small ``--max-inner`` and host-driven launches it is the small,
+    repeatable run the level-0 kernels are profiled on."""
+    import argparse
+    import json
+    import time
+
+    from . import scenes
+    from .fluid import cell_mask, compute_divergence
+
+    ap = argparse.ArgumentParser(description="one tolerance solve on the benchmark pot")
+    ap.add_argument("cmd", choices=["solve"])
+    ap.add_argument("--storage", default="fp16", choices=["fp32", "fp16", "bf16"])
+    ap.add_argument("--max-inner", type=int, default=200)
+    ap.add_argument("--max-outer", type=int, default=10)
+    ap.add_argument("--graph", action="store_true")
+    args = ap.parse_args(argv)
+    dx = 0.0005
+    mat = scenes.pot_mat(scenes.POT_384)
+    ux, uy, uz = scenes.velocity_field(mat, seed=7)
+    mask = cell_mask(torch.as_tensor(mat).cuda())
+    u = [torch.as_tensor(a).cuda() for a in (ux, uy, uz)]
+    div = torch.zeros(mat.shape, device="cuda")
+    compute_divergence(div, *u, mask, dx)
+    s = TolSolver(mask, args.storage)
+    p = torch.zeros_like(div)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = s.solve(div, dx, 0.01, 997.0, tol=1e-6, p=p, max_outer=args.max_outer,
+                max_inner=args.max_inner, graph=args.graph, raise_on_fail=False)
+    torch.cuda.synchronize()
+    print(json.dumps({"status": r.status, "inner": r.inner_iterations, "outer": r.outer_iterations,
+                      "rel_residual": r.rel_residual,
+                      "ms_host_clock": round((time.perf_counter() - t0) * 1e3, 3)}))
+
+
+if __name__ == "__main__":
+    main()
