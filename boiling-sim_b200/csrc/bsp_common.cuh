@@ -22,6 +22,35 @@
 
 namespace bsp {
 
+// Programmatic dependent launch: a kernel launched with the programmatic-
+// stream-serialization attribute may start while the kernel before it
+// drains; it waits here, before touching anything that kernel wrote, until
+// that kernel has completed and its writes are visible.  A no-op for kernels
+// launched without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// Lets the dependent kernel launch once every CTA of this one has called it
+// (or exited).
+__device__ __forceinline__ void pdl_trigger() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+// Host: launch `kernel` with the programmatic-stream-serialization attribute
+// when `pdl` is set (BSP_TUNE_PDL), plainly otherwise.
+template <class... Exp, class... Act>
+inline cudaError_t launch_maybe_pdl(bool pdl, dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                    void (*kernel)(Exp...), Act &&...args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<Act &&>(args)...);
+}
+
 __device__ __forceinline__ int64_t idx3(int i, int j, int k, int ny, int nz) {
   return ((int64_t)i * ny + j) * nz + k;
 }

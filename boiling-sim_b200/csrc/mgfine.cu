@@ -1036,8 +1036,11 @@ template <class T, class Op>
 __global__ void __launch_bounds__(TILE_THREADS, Op::MIN_BLOCKS) fine_tma_kernel(
     Op op, const __grid_constant__ TmaMaps maps, int nx, int ny, int nz, int bi,
     const uint8_t *tiles, const SolverState *st, SolverState *tail_st, int tail_kind) {
-  if (st->inner_done) return;  // uniform: the whole grid returns
+  // the tile flags are written at setup only; everything the previous kernel
+  // of the stream writes is read (and the partials written) after pdl_wait
   if (tiles && !tiles[block_linear()]) {
+    pdl_wait();
+    if (st->inner_done) return;
     if (threadIdx.x == 0) op.skip();
     fine_tail(tail_st, tail_kind, op_partials(op));
     return;
@@ -1066,6 +1069,8 @@ __global__ void __launch_bounds__(TILE_THREADS, Op::MIN_BLOCKS) fine_tma_kernel(
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  pdl_wait();
+  if (st->inner_done) return;  // uniform: the whole grid returns
   auto issue = [&](int p) {  // producer only: plane p into its stage
     const int q = (p - pbase) % L::NST;
     unsigned char *base = dsm + q * L::STAGE;
@@ -1192,12 +1197,16 @@ __global__ void __launch_bounds__(TILE_THREADS, Op::MIN_BLOCKS) fine_tma_kernel(
     for (int p = max(pbase, i1 - L::NST + 1); p <= i1; ++p) wait(p);
   }
   if (!ok) atomicExch(const_cast<int *>(&st->dev_error), 1);
+  pdl_trigger();
   op.template finish<TILE_WARPS>(sh);
   fine_tail(tail_st, tail_kind, op_partials(op));
 }
 
 // ---- TMA launch helpers (host) ----------------------------------------------------------
 bool g_fine_tma_enabled = true;  // BSP_TUNE_FINE_TMA
+// BSP_TUNE_PDL: the tile kernels and the scalar kernels of an inner iteration
+// launched with programmatic dependent launch
+bool g_pdl = false;
 
 // The TMA path needs nz % 16 == 0 (16-byte mask rows) and 16-byte aligned bases.
 static bool tma_eligible(int nz) { return g_fine_tma_enabled && nz % 16 == 0 && encode_tiled(); }
@@ -1214,9 +1223,11 @@ static bool launch_tma(const Op &op, const TmaMaps &maps, int nx, int ny, int nz
   int tkind = tst ? t_tail.kind : TAIL_NONE;
   t_tail.st = nullptr;
   t_tail.kind = TAIL_NONE;
-  fine_tma_kernel<T, Op><<<fine_grid(nx, ny, nz), TILE_THREADS, L::TOTAL, s>>>(
-      op, maps, nx, ny, nz, fine_bi(nx, ny, nz), tiles, st, tst, tkind);
-  const bool ok = cudaGetLastError() == cudaSuccess;
+  const bool ok =
+      launch_maybe_pdl(g_pdl, fine_grid(nx, ny, nz), dim3(TILE_THREADS), L::TOTAL, s,
+                       fine_tma_kernel<T, Op>, op, maps, nx, ny, nz, fine_bi(nx, ny, nz), tiles,
+                       st, tst, tkind) == cudaSuccess &&
+      cudaGetLastError() == cudaSuccess;
   if (ok && tkind != TAIL_NONE) t_tail.taken = true;
   return ok;
 }

@@ -77,6 +77,7 @@ bool g_l0_trilinear = false;
 // costs each level-0 kernel about 7 us, more than the launches it saves.
 bool g_fuse_scalars = false;
 extern int g_fine_ctas;  // BSP_TUNE_FINE_CTAS (mgfine.cu)
+extern bool g_pdl;       // BSP_TUNE_PDL (mgfine.cu)
 extern int g_tri_cpc;  // BSP_TUNE_TRI_CPC (mgfine.cu)
 // BSP_TUNE_FUSE_UPDATE: CG update fused into the next level-0 restriction
 bool g_fuse_update_enabled = true;
@@ -664,6 +665,8 @@ __global__ void __launch_bounds__(RED_THREADS) outer_check_kernel(SolverState *s
 
 __global__ void __launch_bounds__(RED_THREADS) beta_kernel(SolverState *st,
                                                            const double *partials, int nblocks) {
+  pdl_wait();
+  pdl_trigger();
   if (st->inner_done) return;
   const double rz = reduce_slot(partials, 0, nblocks, false);
   if (threadIdx.x != 0) return;
@@ -672,6 +675,8 @@ __global__ void __launch_bounds__(RED_THREADS) beta_kernel(SolverState *st,
 
 __global__ void __launch_bounds__(RED_THREADS) alpha_kernel(SolverState *st,
                                                             const double *partials, int nblocks) {
+  pdl_wait();
+  pdl_trigger();
   if (st->inner_done) return;
   const double pap = reduce_slot(partials, 0, nblocks, false);
   if (threadIdx.x != 0) return;
@@ -685,6 +690,8 @@ __global__ void __launch_bounds__(RED_THREADS) alpha_kernel(SolverState *st,
 __global__ void __launch_bounds__(RED_THREADS) inner_check_fused_kernel(SolverState *st,
                                                                         const double *partials,
                                                                         int nblocks) {
+  pdl_wait();
+  pdl_trigger();
   if (st->inner_done) return;
   const double rr = reduce_slot(partials, 0, nblocks, false);
   if (threadIdx.x != 0) return;
@@ -995,8 +1002,8 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
     }
     if (!tail) {
       ProfScope ps(PROF_CONTROL, s);
-      inner_check_fused_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials,
-                                                         fine_grid_blocks(cx.nx, cx.ny, cx.nz));
+      launch_maybe_pdl(g_pdl, dim3(1), dim3(RED_THREADS), 0, s, inner_check_fused_kernel, st,
+                       (const double *)cx.partials, fine_grid_blocks(cx.nx, cx.ny, cx.nz));
     }
     if (cx.tri) {
       // the trilinear restriction of the scaled residual (in z) to level 1
@@ -1115,7 +1122,8 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
   }
   if (!tail) {
     ProfScope ps(PROF_CONTROL, s);
-    beta_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials, nb0);
+    launch_maybe_pdl(g_pdl, dim3(1), dim3(RED_THREADS), 0, s, beta_kernel, st,
+                     (const double *)cx.partials, nb0);
   }
   tail = false;
   {
@@ -1132,7 +1140,8 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
   }
   if (!tail) {
     ProfScope ps(PROF_CONTROL, s);
-    alpha_kernel<<<1, RED_THREADS, 0, s>>>(st, cx.partials, nb0);
+    launch_maybe_pdl(g_pdl, dim3(1), dim3(RED_THREADS), 0, s, alpha_kernel, st,
+                     (const double *)cx.partials, nb0);
   }
   if (cx.fuse) return cudaGetLastError();  // the update runs in the next restriction
   int nbf = flat_blocks(cx.n);
@@ -1603,6 +1612,7 @@ static void key_params(GraphKey &k, const BspSolveParams *p) {
   k.v.push_back((uintptr_t)g_tri_cpc);
   k.v.push_back((uintptr_t)g_fuse_scalars);
   k.v.push_back((uintptr_t)g_fine_ctas);
+  k.v.push_back((uintptr_t)g_pdl);
   k.v.push_back((uintptr_t)g_fuse_update_enabled);
   k.v.push_back((uintptr_t)g_fine_bi);
 }

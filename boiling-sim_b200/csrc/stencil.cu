@@ -515,6 +515,7 @@ extern bool g_l0_trilinear;
 extern int g_tri_cpc;
 extern bool g_fuse_scalars;
 extern int g_fine_ctas;
+extern bool g_pdl;
 namespace utc {
 extern int g_utc_nepi;
 }  // namespace utc
@@ -569,6 +570,10 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_CONV_EPILOGUE:
       if (value < 0 || value > 4) return BSP_ERR_ARG;
       bsp::utc::g_utc_nepi = value;
+      return BSP_OK;
+    case BSP_TUNE_PDL:
+      if (value < 0 || value > 1) return BSP_ERR_ARG;
+      bsp::g_pdl = value != 0;
       return BSP_OK;
     case BSP_TUNE_FINE_CTAS:
       if (value < 1 || value > 16) return BSP_ERR_ARG;

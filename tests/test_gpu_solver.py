@@ -361,3 +361,29 @@ def test_scalars_in_last_cta_match_one_block_kernels(cuda, pot64, storage):
         a, b = out[1, graph], out[0, graph]
         assert (a.inner_iterations, a.outer_iterations) == (b.inner_iterations, b.outer_iterations)
         assert O.rel_error(a.p64, b.p64, mat) < 1e-9
+
+
+@pytest.mark.parametrize("storage", ["fp32", "fp16"])
+def test_programmatic_dependent_launch_bit_identical(cuda, pot64, storage):
+    """The tile and scalar kernels launched with programmatic dependent launch
+    (BSP_TUNE_PDL = 1: each waits in griddepcontrol.wait for the kernel before
+    it) compute exactly what the plainly serialised launches compute, host-
+    driven and through the device-driven graph."""
+    from boilingsim_b200 import _lib
+
+    mat, div, _ = pot64
+    out = {}
+    try:
+        for pdl in (1, 0):
+            _lib.call("bsp_set_tuning", 23, pdl)
+            for graph in (False, True):
+                res = solve_tolerance(div, mat, DX, DT, RHO, tol=1e-7, storage=storage,
+                                      graph=graph)
+                assert res.status == 0
+                out[pdl, graph] = res
+    finally:
+        _lib.call("bsp_set_tuning", 23, 0)
+    for graph in (False, True):
+        a, b = out[1, graph], out[0, graph]
+        assert (a.inner_iterations, a.outer_iterations) == (b.inner_iterations, b.outer_iterations)
+        assert np.array_equal(a.p64, b.p64)
