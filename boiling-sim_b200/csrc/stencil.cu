@@ -66,16 +66,17 @@ __device__ __forceinline__ float4 ld4(const float *p) {
 // values are chosen with sel_nbr (two prmt + one lop3, no branches); the sum
 // order is the reference's l, r, d, u, b, f.
 //
-// ZNF: the source field holds +0 on every non-fluid cell (true after one sweep,
-// and for a projection, which zeroes p first).  Then the neighbour rule
-// fluid -> p_n, air -> 0, solid -> p_self is exactly p_n | (p_self & solid) on
-// bit patterns (p_n is +0 on air and solid cells): one prmt + one lop3.
+// ZNF (sweep_znf_kernel below): the source field holds +0 on every non-fluid
+// cell (true after one sweep, and for a projection, which zeroes p first).
+// Then the neighbour rule fluid -> p_n, air -> 0, solid -> p_self is exactly
+// p_n | (p_self & solid) on bit patterns (p_n is +0 on air and solid cells):
+// one prmt + one lop3.
 __device__ __forceinline__ float znf_nbr(uint32_t sw, int q, float pn, float ps) {
   const uint32_t sm = sign_bytes(sw, (uint32_t)(8 | q) * 0x1111u);
   return __uint_as_float(__float_as_uint(pn) | (__float_as_uint(ps) & sm));
 }
 
-template <int OP, class MaskT, bool FULL, bool ZNF>
+template <int OP, class MaskT, bool FULL>
 __global__ void __launch_bounds__(256) stencil_col_kernel(
     float *__restrict__ out, const float *__restrict__ p, const float *__restrict__ src,
     const MaskT *__restrict__ mask, int nx, int ny, int nz, int bi, float rdd, float dt,
@@ -144,22 +145,12 @@ __global__ void __launch_bounds__(256) stencil_col_kernel(
 #pragma unroll
       for (int q = 0; q < 4; ++q) {
         const float ps = f4(pc, q);
-        float l, r, d, u, b, f;
-        if (ZNF) {
-          l = znf_nbr(mm << 1, q, f4(pm, q), ps);
-          r = znf_nbr(mn << 1, q, f4(pn, q), ps);
-          d = znf_nbr(mjm << 1, q, f4(pjm, q), ps);
-          u = znf_nbr(mjp << 1, q, f4(pjp, q), ps);
-          b = znf_nbr(mb << 1, q, f4(pb, q), ps);
-          f = znf_nbr(mfw << 1, q, f4(pf, q), ps);
-        } else {
-          l = sel_nbr(mm, mm << 1, q, f4(pm, q), ps);
-          r = sel_nbr(mn, mn << 1, q, f4(pn, q), ps);
-          d = sel_nbr(mjm, mjm << 1, q, f4(pjm, q), ps);
-          u = sel_nbr(mjp, mjp << 1, q, f4(pjp, q), ps);
-          b = sel_nbr(mb, mb << 1, q, f4(pb, q), ps);
-          f = sel_nbr(mfw, mfw << 1, q, f4(pf, q), ps);
-        }
+        const float l = sel_nbr(mm, mm << 1, q, f4(pm, q), ps);
+        const float r = sel_nbr(mn, mn << 1, q, f4(pn, q), ps);
+        const float d = sel_nbr(mjm, mjm << 1, q, f4(pjm, q), ps);
+        const float u = sel_nbr(mjp, mjp << 1, q, f4(pjp, q), ps);
+        const float b = sel_nbr(mb, mb << 1, q, f4(pb, q), ps);
+        const float f = sel_nbr(mfw, mfw << 1, q, f4(pf, q), ps);
         float v;
         if (OP == OP_SPMV) {
           v = spmv_update(l, r, d, u, b, f, ps);
@@ -172,6 +163,140 @@ __global__ void __launch_bounds__(256) stencil_col_kernel(
       }
       *reinterpret_cast<float4 *>(out + o) = make_float4(o4[0], o4[1], o4[2], o4[3]);
     }
+    pm = pc;
+    mm = mc;
+    pc = pn;
+    mc = mn;
+  }
+}
+
+// ---- ZNF sweep kernel -----------------------------------------------------------
+// The column kernel's layout and arithmetic for p_new = (s - rhs) / 6 on a
+// source that is +0 off fluid, with two warp-uniform shortcuts, both exact:
+//  * a 128-cell row segment without a fluid cell stores +0 (a non-fluid
+//    cell's result is +0 whatever its operands) and reads neither its j
+//    neighbours nor rhs: 9 instead of 13 B/cell;
+//  * a segment whose fluid cells have no solid face neighbour (mask bits 0-2,
+//    the solid-neighbour count, zero on every fluid byte) sums the raw
+//    neighbour values: fluid neighbours give p_n, air ones p_n = +0, which is
+//    what the boundary rule selects, in the same order l, r, d, u, b, f.
+// Other segments take the per-neighbour select of stencil_col_kernel.
+template <bool RAW>
+__device__ __forceinline__ float4 znf_segment(const float *__restrict__ p,
+                                              const float *__restrict__ rhs,
+                                              const uint8_t *__restrict__ mask, int64_t o,
+                                              int lane, int k, int nz, bool act, bool has_jm,
+                                              bool has_jp, const float4 &pm, const float4 &pc,
+                                              const float4 &pn, uint32_t mm, uint32_t mc,
+                                              uint32_t mn) {
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  float4 pjm = z4, pjp = z4, sv = z4;
+  uint32_t mjm = 0u, mjp = 0u;
+  if (act) {
+    if (has_jm) {
+      pjm = ld4(p + o - nz);
+      if (!RAW) mjm = mw4(mask, o - nz, 0, 0);
+    }
+    if (has_jp) {
+      pjp = ld4(p + o + nz);
+      if (!RAW) mjp = mw4(mask, o + nz, 0, 0);
+    }
+    sv = ld4(rhs + o);
+  }
+  float pkm = __shfl_up_sync(0xffffffffu, pc.w, 1);
+  float pkp = __shfl_down_sync(0xffffffffu, pc.x, 1);
+  uint32_t mkm = 0u, mkp = 0u;
+  if (!RAW) {
+    mkm = __shfl_up_sync(0xffffffffu, mc, 1);
+    mkp = __shfl_down_sync(0xffffffffu, mc, 1);
+  }
+  if (lane == 0) {
+    const bool in = act && k > 0;
+    pkm = in ? __ldg(p + o - 1) : 0.0f;
+    if (!RAW) mkm = in ? (uint32_t)__ldg(mask + o - 1) << 24 : 0u;
+  }
+  if (lane == 31) {
+    const bool in = act && k + 4 < nz;
+    pkp = in ? __ldg(p + o + 4) : 0.0f;
+    if (!RAW) mkp = in ? (uint32_t)__ldg(mask + o + 4) : 0u;
+  }
+  const uint32_t mb = (mc << 8) | (mkm >> 24);
+  const uint32_t mfw = (mc >> 8) | (mkp << 24);
+  const float4 pb = make_float4(pkm, pc.x, pc.y, pc.z);
+  const float4 pf = make_float4(pc.y, pc.z, pc.w, pkp);
+  float o4[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float ps = f4(pc, q);
+    float l, r, d, u, b, f;
+    if (RAW) {
+      l = f4(pm, q);
+      r = f4(pn, q);
+      d = f4(pjm, q);
+      u = f4(pjp, q);
+      b = f4(pb, q);
+      f = f4(pf, q);
+    } else {
+      l = znf_nbr(mm << 1, q, f4(pm, q), ps);
+      r = znf_nbr(mn << 1, q, f4(pn, q), ps);
+      d = znf_nbr(mjm << 1, q, f4(pjm, q), ps);
+      u = znf_nbr(mjp << 1, q, f4(pjp, q), ps);
+      b = znf_nbr(mb << 1, q, f4(pb, q), ps);
+      f = znf_nbr(mfw << 1, q, f4(pf, q), ps);
+    }
+    const float sum = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(l, r), d), u), b), f);
+    const float v = div6(__fsub_rn(sum, f4(sv, q)));
+    o4[q] = __uint_as_float(__float_as_uint(v) & fluid_word(mc, q));
+  }
+  return make_float4(o4[0], o4[1], o4[2], o4[3]);
+}
+
+template <bool FULL>
+__global__ void __launch_bounds__(256) sweep_znf_kernel(float *__restrict__ out,
+                                                        const float *__restrict__ p,
+                                                        const float *__restrict__ rhs,
+                                                        const uint8_t *__restrict__ mask, int nx,
+                                                        int ny, int nz, int bi) {
+  const int lane = threadIdx.x & 31;
+  const int j = blockIdx.y * 8 + (threadIdx.x >> 5);
+  if (j >= ny) return;  // warp-uniform
+  const int k = (blockIdx.x * 32 + lane) * 4;
+  const bool act = FULL || k < nz;
+  const int i0 = blockIdx.z * bi;
+  const int i1 = min(i0 + bi, nx);
+  const int64_t plane = (int64_t)ny * nz;
+  const bool has_jm = j > 0, has_jp = j + 1 < ny;
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  int64_t o = (int64_t)i0 * plane + (int64_t)j * nz + k;
+  float4 pm = z4, pc = z4;
+  uint32_t mm = 0u, mc = 0u;  // 0 = air
+  if (act && i0 > 0) {
+    pm = ld4(p + o - plane);
+    mm = mw4(mask, o - plane, 0, 0);
+  }
+  if (act) {
+    pc = ld4(p + o);
+    mc = mw4(mask, o, 0, 0);
+  }
+  for (int i = i0; i < i1; ++i, o += plane) {
+    float4 pn = z4;
+    uint32_t mn = 0u;
+    if (act && i + 1 < nx) {
+      pn = ld4(p + o + plane);
+      mn = mw4(mask, o + plane, 0, 0);
+    }
+    float4 v = z4;
+    if (__any_sync(0xffffffffu, (mc & 0x80808080u) != 0u)) {
+      // fluid bytes' solid-neighbour counts: bit 0 of each fluid byte times 7
+      const uint32_t fl7 = ((mc >> 7) & 0x01010101u) * 7u;
+      if (__all_sync(0xffffffffu, (mc & fl7) == 0u))
+        v = znf_segment<true>(p, rhs, mask, o, lane, k, nz, act, has_jm, has_jp, pm, pc, pn, mm,
+                              mc, mn);
+      else
+        v = znf_segment<false>(p, rhs, mask, o, lane, k, nz, act, has_jm, has_jp, pm, pc, pn, mm,
+                               mc, mn);
+    }
+    if (act) *reinterpret_cast<float4 *>(out + o) = v;
     pm = pc;
     mm = mc;
     pc = pn;
@@ -331,11 +456,11 @@ cudaError_t launch_stencil(float *out, const float *p, const float *div, const M
     const int bi = g_sweep_bi > 0 ? g_sweep_bi : pick_bi(nx, ny, nz);
     dim3 grid((nz / 4 + 31) / 32, (ny + 7) / 8, (nx + bi - 1) / bi);
     if (nz % 128 == 0)
-      stencil_col_kernel<OP, MaskT, true, false><<<grid, 256, 0, s>>>(out, p, div, mask, nx, ny,
-                                                                      nz, bi, rdd, dt, mf, ma);
+      stencil_col_kernel<OP, MaskT, true><<<grid, 256, 0, s>>>(out, p, div, mask, nx, ny, nz, bi,
+                                                               rdd, dt, mf, ma);
     else
-      stencil_col_kernel<OP, MaskT, false, false><<<grid, 256, 0, s>>>(out, p, div, mask, nx, ny,
-                                                                       nz, bi, rdd, dt, mf, ma);
+      stencil_col_kernel<OP, MaskT, false><<<grid, 256, 0, s>>>(out, p, div, mask, nx, ny, nz, bi,
+                                                                rdd, dt, mf, ma);
   } else {
     const int64_t n = (int64_t)nx * ny * nz;
     stencil_generic_kernel<OP, MaskT><<<generic_blocks(n), 256, 0, s>>>(out, p, div, mask, nx,
@@ -357,11 +482,9 @@ cudaError_t launch_sweep_znf(float *out, const float *p, const float *rhs, const
   const int bi = g_sweep_bi > 0 ? g_sweep_bi : pick_bi(nx, ny, nz);
   dim3 grid((nz / 4 + 31) / 32, (ny + 7) / 8, (nx + bi - 1) / bi);
   if (nz % 128 == 0)
-    stencil_col_kernel<OP_JACOBI_RHS, uint8_t, true, true><<<grid, 256, 0, s>>>(
-        out, p, rhs, mask, nx, ny, nz, bi, 0.f, 1.f, BSP_FLUID, BSP_AIR);
+    sweep_znf_kernel<true><<<grid, 256, 0, s>>>(out, p, rhs, mask, nx, ny, nz, bi);
   else
-    stencil_col_kernel<OP_JACOBI_RHS, uint8_t, false, true><<<grid, 256, 0, s>>>(
-        out, p, rhs, mask, nx, ny, nz, bi, 0.f, 1.f, BSP_FLUID, BSP_AIR);
+    sweep_znf_kernel<false><<<grid, 256, 0, s>>>(out, p, rhs, mask, nx, ny, nz, bi);
   return cudaGetLastError();
 }
 

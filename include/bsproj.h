@@ -81,7 +81,7 @@ extern "C" {
 #define BSP_TUNE_FUSE_SCALARS 21  /* CG scalars in the last CTA of the level-0 kernels: 1, 0 (default) */
 #define BSP_TUNE_FINE_CTAS 22     /* CTAs per SM the tile kernels' plane chunking aims for (default 4) */
 #define BSP_TUNE_PDL 23           /* tile and scalar kernels of an inner iteration by programmatic
-                                     dependent launch: 1 on, 0 off (default) */
+                                     dependent launch: 1 on (default), 0 off */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */

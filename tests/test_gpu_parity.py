@@ -134,6 +134,41 @@ def test_temporally_blocked_sweeps_bit_exact(cuda, shape, n_iter):
     assert flag.value == 0
 
 
+def _segment_mat(nz):
+    """Rows of 128-cell k segments of the three kinds the ZNF sweep tells
+    apart: no fluid cell (air, or air and solid), fluid without a solid face
+    neighbour, and fluid beside solid."""
+    mat = np.full((6, 10, nz), 2, np.int32)   # air
+    mat[1:5, 2:5, 130:nz - 6] = 0                # fluid next to air only
+    mat[1:5, 6, 3:100] = 0                       # fluid ...
+    mat[1:5, 6, 100] = 1                         # ... beside a wall cell
+    mat[2, 8, 10:40] = 3                         # solid among air: no fluid
+    mat[3, 3, 60:70] = 0                         # a fluid pocket in segment 0
+    mat[3, 3, 70] = 3
+    return mat
+
+
+@pytest.mark.parametrize("nz", [256, 200])
+def test_znf_sweep_segment_shortcuts_bit_exact(cuda, nz):
+    """The ZNF sweep's warp-uniform shortcuts (+0 for segments without fluid,
+    raw neighbour sums where no fluid cell touches a solid one) give the bits
+    of the oracle's sweeps, full and partial k segments (nz 256 and 200)."""
+    mat = _segment_mat(nz)
+    rng = np.random.default_rng(nz)
+    div = rng.standard_normal(mat.shape).astype(np.float32) * 0.3
+    p_old = rng.standard_normal(mat.shape).astype(np.float32)
+    dx, dt, rho = 0.002, 0.01, 997.0
+    nx, ny, _ = mat.shape
+    want = O.pressure_solve(p_old, div, mat, dx, dt, rho, 6)
+    m8 = mask_of(dev(mat, torch.int32))
+    p = dev(p_old)
+    tmp = torch.zeros_like(p)
+    rhs = torch.zeros_like(p)
+    call("bsp_jacobi_solve", ptr(p), ptr(tmp), ptr(dev(div)), ptr(rhs), ptr(m8), nx, ny, nz,
+         dx, dt, rho, 6, 1, 0)
+    assert np.array_equal(bits(host(p)), bits(want))
+
+
 @pytest.mark.parametrize("spec", [S.POT_64, S.PotSpec(40, 36, 30, 14, 2, 24, 4, 12)],
                          ids=["pot64", "pot40x36x30"])
 def test_full_projection_bit_exact(cuda, spec):

@@ -382,7 +382,7 @@ def test_programmatic_dependent_launch_bit_identical(cuda, pot64, storage):
                 assert res.status == 0
                 out[pdl, graph] = res
     finally:
-        _lib.call("bsp_set_tuning", 23, 0)
+        _lib.call("bsp_set_tuning", 23, 1)
     for graph in (False, True):
         a, b = out[1, graph], out[0, graph]
         assert (a.inner_iterations, a.outer_iterations) == (b.inner_iterations, b.outer_iterations)
