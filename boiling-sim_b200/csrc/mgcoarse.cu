@@ -707,6 +707,204 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cycle_kernel(CoarseCycle<T> 
   if (!ok && threadIdx.x == 0) atomicExch(&st->dev_error, 1);
 }
 
+// ---- the coarse cycle in one thread-block cluster ----------------------------------
+// The stored-t phases of mg_cycle_kernel spread over the CTAs of ONE cluster
+// (BSP_TUNE_COARSE_CLUSTER CTAs, one per SM) and separated by the hardware
+// cluster barrier -- arrive with release, wait with acquire semantics at
+// cluster scope, so one phase's global stores are visible to every CTA of the
+// cluster in the next -- instead of the software barrier over all SMs.  The
+// levels below the cycle's top level are L2-resident and their phases bound
+// by load latency, not by the number of SMs; a cluster barrier costs a
+// fraction of a grid-wide one.  Levels of at most CL_TAIL_CELLS cells run in
+// the cluster's CTA 0 alone with __syncthreads; the coarsest solve uses the
+// dense inverse copied into CTA 0's shared memory at launch.  A cluster's CTAs
+// are co-scheduled by the hardware: no spin wait.
+constexpr int CL_TAIL_CELLS = 2048;
+__device__ __forceinline__ void cluster_sync_all() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
+                   : "memory");
+}
+__device__ __forceinline__ uint32_t cluster_rank() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ uint32_t cluster_ctas() {
+  uint32_t r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+
+template <class T>
+__global__ void __launch_bounds__(CC_THREADS, 1) mg_cluster_cycle_kernel(CoarseCycle<T> a,
+                                                                         SolverState *st) {
+  if (st->inner_done) return;  // uniform over the cluster
+  __shared__ float wtab[8];
+  if (threadIdx.x < 8) {
+    const float d = 6.0f - (float)threadIdx.x;
+    wtab[threadIdx.x] = d > 0.0f ? __fdividef(CC_OMEGA, d) : 0.0f;
+  }
+  __syncthreads();
+  const int rank = (int)cluster_rank(), nct = (int)cluster_ctas();
+  const int wpb = blockDim.x >> 5;
+  const Span all{rank * wpb + (int)(threadIdx.x >> 5), nct * wpb};
+  const Span one{(int)(threadIdx.x >> 5), wpb};
+  const bool lead = rank == 0;
+  const int L = a.L;
+  auto cells = [&](int l) { return (int64_t)a.lv[l].nx * a.lv[l].ny * a.lv[l].nz; };
+  int tail = 1;  // levels >= tail run in CTA 0 of the cluster alone
+  while (tail < L && cells(tail) > CL_TAIL_CELLS) ++tail;
+  uint64_t *cbar = reinterpret_cast<uint64_t *>(cc_smem() + (a.cinv_bytes >> 2) +
+                                                ((a.cinv_bytes > 0) ? COARSEST_CELLS : 0));
+  const bool cinv_copy = a.cinv_bytes > 0 && lead;
+  bool cinv_waited = false;
+  if (cinv_copy && threadIdx.x == 0) {
+    mbar_init(cbar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    mbar_expect_tx(cbar, (uint32_t)a.cinv_bytes);
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, "
+        "[%3];" ::"r"(smem_u32(cc_smem())),
+        "l"(a.cinv), "r"((uint32_t)a.cinv_bytes), "r"(smem_u32(cbar))
+        : "memory");
+  }
+  bool ok = true;
+  int nmark = 0;
+  auto mark = [&]() {
+    if (a.trace && lead && threadIdx.x == 0 && nmark < CC_TRACE_MAX)
+      a.trace[nmark++] = global_ns();
+  };
+  auto csync = [&]() {
+    cluster_sync_all();
+    mark();
+  };
+  mark();
+  // ---- down: t of the cycle's first level, then per level the residual pass
+  // and the restriction (which also forms t of the next level)
+  if (L > 2) {
+    if (1 < tail) {
+      phase_d1(a.lv[1], a.scratch, wtab, all);
+      csync();
+    } else if (lead) {
+      phase_d1(a.lv[1], a.scratch, wtab, one);
+      __syncthreads();
+    }
+  }
+  for (int l = 1; l + 1 < L && l < tail; ++l) {
+    phase_d2a(a.lv[l], a.scratch, a.res, all);
+    csync();
+    phase_d2b(a.lv[l], a.lv[l + 1], a.res, a.scratch, wtab, all);
+    csync();
+  }
+  if (lead) {
+    const float *minv = a.cinv;
+    if (cinv_copy) {
+      __shared__ int s_cok;
+      if (threadIdx.x == 0) s_cok = mbar_wait(cbar, 0) ? 1 : 0;
+      __syncthreads();
+      cinv_waited = true;
+      if (s_cok) minv = cc_smem();
+      else ok = false;
+    }
+    if (a.tail_smem && tail < L) {
+      // The tail levels in shared memory: masks and the first tail level's
+      // right-hand side and t copied in (its down phases ran above: the
+      // restriction into it left r and t in global memory), the rest of the
+      // tail on-chip, the first tail level's correction copied back out.
+      Level<T> sv[MAX_LEVELS];
+      unsigned char *sp = reinterpret_cast<unsigned char *>(cc_smem()) + a.tail_off;
+      auto take = [&](int64_t b) {
+        unsigned char *q = sp;
+        sp += (b + 15) / 16 * 16;
+        return q;
+      };
+      for (int l = tail; l < L; ++l) {
+        const int64_t nl = cells(l);
+        sv[l] = a.lv[l];
+        sv[l].mask = take(nl);
+        sv[l].r = reinterpret_cast<T *>(take(nl * (int64_t)sizeof(T)));
+        sv[l].e = reinterpret_cast<T *>(take(nl * (int64_t)sizeof(T)));
+        const uint32_t *gm = reinterpret_cast<const uint32_t *>(a.lv[l].mask);
+        uint32_t *smk = reinterpret_cast<uint32_t *>(const_cast<uint8_t *>(sv[l].mask));
+        for (int64_t q = threadIdx.x; q < nl / 4; q += blockDim.x) smk[q] = gm[q];
+      }
+      const int64_t nt = cells(tail);
+      float *ts = reinterpret_cast<float *>(take(nt * 4));
+      float *rs = reinterpret_cast<float *>(take(nt * 4));
+      {
+        const int64_t nb = nt * (int64_t)sizeof(T) / 8;  // 8-byte words
+        const uint2 *g = reinterpret_cast<const uint2 *>(a.lv[tail].r);
+        uint2 *d = reinterpret_cast<uint2 *>(sv[tail].r);
+        for (int64_t q = threadIdx.x; q < nb; q += blockDim.x) d[q] = g[q];
+        const float4 *gt = reinterpret_cast<const float4 *>(a.scratch);
+        float4 *dt = reinterpret_cast<float4 *>(ts);
+        for (int64_t q = threadIdx.x; q < nt / 4; q += blockDim.x) dt[q] = gt[q];
+      }
+      __syncthreads();
+      for (int l = tail; l + 1 < L; ++l) {
+        phase_d2a(sv[l], ts, rs, one);
+        __syncthreads();
+        phase_d2b(sv[l], sv[l + 1], rs, ts, wtab, one);
+        __syncthreads();
+      }
+      if (ok) coarsest_solve(a, sv[L - 1], wtab, minv);
+      __syncthreads();
+      for (int l = L - 2; l >= tail; --l) {
+        phase_u1(sv[l], sv[l + 1], ts, wtab, a.alpha, one);
+        __syncthreads();
+        phase_u2(sv[l], ts, wtab, one);
+        __syncthreads();
+      }
+      {
+        const int64_t nb = nt * (int64_t)sizeof(T) / 8;
+        const uint2 *g = reinterpret_cast<const uint2 *>(sv[tail].e);
+        uint2 *d = reinterpret_cast<uint2 *>(a.lv[tail].e);
+        for (int64_t q = threadIdx.x; q < nb; q += blockDim.x) d[q] = g[q];
+      }
+      __syncthreads();
+    } else {
+      for (int l = tail; l + 1 < L; ++l) {
+        phase_d2a(a.lv[l], a.scratch, a.res, one);
+        __syncthreads();
+        phase_d2b(a.lv[l], a.lv[l + 1], a.res, a.scratch, wtab, one);
+        __syncthreads();
+      }
+      if (ok) coarsest_solve(a, a.lv[L - 1], wtab, minv);
+      __syncthreads();
+      for (int l = L - 2; l >= tail && l >= 1; --l) {
+        phase_u1(a.lv[l], a.lv[l + 1], a.scratch, wtab, a.alpha, one);
+        __syncthreads();
+        phase_u2(a.lv[l], a.scratch, wtab, one);
+        __syncthreads();
+      }
+    }
+    mark();
+  }
+  // ---- up through the levels the whole cluster runs
+  const int top = min(tail, L - 1) - 1;
+  if (top >= 1) csync();
+  for (int l = top; l >= 1; --l) {
+    phase_u1(a.lv[l], a.lv[l + 1], a.scratch, wtab, a.alpha, all);
+    csync();
+    phase_u2(a.lv[l], a.scratch, wtab, all);
+    if (l > 1) csync();
+  }
+  mark();
+  if (cinv_copy && !cinv_waited && threadIdx.x == 0) mbar_wait(cbar, 0);
+  if (!ok && threadIdx.x == 0) atomicExch(&st->dev_error, 1);
+}
+
+// BSP_TUNE_CLUSTER_TAIL: the cluster kernel's tail levels staged in CTA 0's
+// shared memory.  Measured slower at 384x384x256 (the tail 10.5 -> 17.4 us:
+// staging in and out costs more than the on-chip phases save), so off.
+bool g_coarse_cluster_tail_smem = false;
+
+// BSP_TUNE_COARSE_CLUSTER: CTAs of the one cluster that runs the coarse cycle
+// (2..16), or 0 for the cooperative kernel over every SM.  Measured at
+// 384x384x256 (levels 3-6 of the cycle): 12.18 ms per solve cooperative,
+// 11.86 with 8 CTAs, 11.80 with 16 (coarse cycle 46 -> 38 us).
+int g_coarse_cluster = 16;
+
 bool g_coarse_fused_enabled = true;  // BSP_TUNE_COARSE_FUSED
 // BSP_TUNE_COARSE_PHASES: 1 forms t where it is read -- D1 folded into the
 // residual pass, U1 into the post-smoothing pass (4 fewer grid barriers per
@@ -820,6 +1018,60 @@ bool launch_coarse_cycle(const Level<T> *lv, int L, float *scratch, const float 
   a.trace = nullptr;
   if (g_coarse_trace && cudaGetSymbolAddress((void **)&a.trace, g_cc_trace) != cudaSuccess)
     a.trace = nullptr;
+  if (g_coarse_cluster >= 2 && g_coarse_cluster <= 16 && !a.fused_phases) {
+    // one cluster: the inverse (and the coarsest right-hand side) and the
+    // levels of at most CL_TAIL_CELLS cells in CTA 0's shared memory
+    CoarseCycle<T> c = a;
+    int ctail = 1;
+    while (ctail < L && (int64_t)lv[ctail].nx * lv[ctail].ny * lv[ctail].nz > CL_TAIL_CELLS)
+      ++ctail;
+    int64_t ctail_bytes = 0;
+    if (ctail < L) {
+      for (int l = ctail; l < L; ++l) {
+        const int64_t nl = (int64_t)lv[l].nx * lv[l].ny * lv[l].nz;
+        ctail_bytes += r16(nl) + 2 * r16(nl * (int64_t)sizeof(T));
+      }
+      ctail_bytes += 2 * r16((int64_t)lv[ctail].nx * lv[ctail].ny * lv[ctail].nz * 4);
+    }
+    c.cinv_bytes = cinv_b;  // the cooperative kernel's budget does not apply here
+    c.tail_smem = (g_coarse_cluster_tail_smem && ctail < L &&
+                   c.cinv_bytes + base + ctail_bytes <= DYN_MAX) ? 1 : 0;
+    if (c.cinv_bytes + base > DYN_MAX) c.cinv_bytes = 0;
+    c.tail_off = (int)(c.cinv_bytes + base);
+    const int64_t cdyn = c.cinv_bytes + base + (c.tail_smem ? ctail_bytes : 0);
+    static bool attr_ok[16] = {false};
+    static bool attr_done[16] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const int di = dev & 15;
+    if (!attr_done[di]) {
+      attr_done[di] = true;
+      attr_ok[di] =
+          cudaFuncSetAttribute(mg_cluster_cycle_kernel<T>,
+                               cudaFuncAttributeNonPortableClusterSizeAllowed, 1) == cudaSuccess &&
+          smem_opt_in((const void *)mg_cluster_cycle_kernel<T>, (int)DYN_MAX);
+    }
+    if (attr_ok[di]) {
+      cudaLaunchConfig_t cc{};
+      cc.gridDim = dim3(g_coarse_cluster);
+      cc.blockDim = dim3(CC_THREADS);
+      cc.dynamicSmemBytes = (size_t)cdyn;
+      cc.stream = s;
+      cudaLaunchAttribute ca[1];
+      ca[0].id = cudaLaunchAttributeClusterDimension;
+      ca[0].val.clusterDim.x = g_coarse_cluster;
+      ca[0].val.clusterDim.y = 1;
+      ca[0].val.clusterDim.z = 1;
+      cc.attrs = ca;
+      cc.numAttrs = 1;
+      int nclusters = 0;
+      if (cudaOccupancyMaxActiveClusters(&nclusters, mg_cluster_cycle_kernel<T>, &cc) ==
+              cudaSuccess &&
+          nclusters >= 1)
+        return cudaLaunchKernelEx(&cc, mg_cluster_cycle_kernel<T>, c, st) == cudaSuccess;
+      cudaGetLastError();  // clear a refused query; the cooperative kernel follows
+    }
+  }
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3(blocks);
   cfg.blockDim = dim3(CC_THREADS);

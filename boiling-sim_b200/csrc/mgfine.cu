@@ -559,11 +559,8 @@ struct TPsAp {
     const float4 zz = ld4s(v.a, v.fo(rr, lane * 4));
     if (first) return zz;
     const float4 pp = ld4s(v.b, v.fo(rr, lane * 4));
-    float4 back;
-    pk4(make_float4(fmaf(beta, pp.x, zz.x), fmaf(beta, pp.y, zz.y), fmaf(beta, pp.z, zz.z),
-                    fmaf(beta, pp.w, zz.w)),
-        back, cur);
-    return back;
+    return make_float4(rt(fmaf(beta, pp.x, zz.x), cur), rt(fmaf(beta, pp.y, zz.y), cur),
+                       rt(fmaf(beta, pp.z, zz.z), cur), rt(fmaf(beta, pp.w, zz.w), cur));
   }
   __device__ float val1(const StageView<T> &v, int rr, int kl) const {
     const float zz = ld1s(v.a, v.fo(rr, kl));
@@ -576,16 +573,11 @@ struct TPsAp {
     for (int q = 0; q < 4; ++q) {
       const uint32_t fm = fluid_word(mc, q);
       vv[q] = __uint_as_float(__float_as_uint(q4(v, q)) & fm);
-      ap[q] = __uint_as_float(__float_as_uint(fmaf(6.0f, q4(v, q), -s[q])) & fm);
+      ap[q] = rt(__uint_as_float(__float_as_uint(fmaf(6.0f, q4(v, q), -s[q])) & fm), cur);
     }
-    float4 apb;
-    const Pk4<T> apk = pk4(make_float4(ap[0], ap[1], ap[2], ap[3]), apb, Ap);
-    float4 vvb;  // vv is already a stored value (or 0): the pack is exact
-    const Pk4<T> vpk = pk4(make_float4(vv[0], vv[1], vv[2], vv[3]), vvb, cur);
-    const float apr[4] = {apb.x, apb.y, apb.z, apb.w};
-    acc += dot4w(vv, apr);
-    s4p(cur, o, vpk);
-    s4p(Ap, o, apk);
+    acc += dot4w(vv, ap);
+    st4s(cur, o, make_float4(vv[0], vv[1], vv[2], vv[3]));
+    st4s(Ap, o, make_float4(ap[0], ap[1], ap[2], ap[3]));
   }
   __device__ void after_step(int, int, int, bool, float2 *) {}
   template <int NW>

@@ -639,6 +639,8 @@ extern int g_tri_cpc;
 extern bool g_fuse_scalars;
 extern int g_fine_ctas;
 extern bool g_pdl;
+extern int g_coarse_cluster;
+extern bool g_coarse_cluster_tail_smem;
 namespace utc {
 extern int g_utc_nepi;
 }  // namespace utc
@@ -693,6 +695,14 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_CONV_EPILOGUE:
       if (value < 0 || value > 4) return BSP_ERR_ARG;
       bsp::utc::g_utc_nepi = value;
+      return BSP_OK;
+    case BSP_TUNE_CLUSTER_TAIL:
+      if (value < 0 || value > 1) return BSP_ERR_ARG;
+      bsp::g_coarse_cluster_tail_smem = value != 0;
+      return BSP_OK;
+    case BSP_TUNE_COARSE_CLUSTER:
+      if (value != 0 && (value < 2 || value > 16)) return BSP_ERR_ARG;
+      bsp::g_coarse_cluster = value;
       return BSP_OK;
     case BSP_TUNE_PDL:
       if (value < 0 || value > 1) return BSP_ERR_ARG;

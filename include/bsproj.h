@@ -82,6 +82,11 @@ extern "C" {
 #define BSP_TUNE_FINE_CTAS 22     /* CTAs per SM the tile kernels' plane chunking aims for (default 4) */
 #define BSP_TUNE_PDL 23           /* tile and scalar kernels of an inner iteration by programmatic
                                      dependent launch: 1 on (default), 0 off */
+#define BSP_TUNE_COARSE_CLUSTER 24 /* coarse cycle in one thread-block cluster of 2..16 CTAs with
+                                      hardware cluster barriers (default 16); 0: cooperative
+                                      kernel over all SMs */
+#define BSP_TUNE_CLUSTER_TAIL 25  /* with COARSE_CLUSTER: levels of <= 2048 cells in CTA 0's shared
+                                     memory, 1 on, 0 off (default) */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */
@@ -629,6 +634,15 @@ int bsp_unet_prolong(float *p, const float *pc, const uint8_t *mask, int nx, int
 int bsp_unet_energy_scale(float *p, const float *Ap, const float *div, const uint8_t *mask,
                           int nx, int ny, int nz, float factor, void *workspace,
                           size_t workspace_bytes, float *gamma_dev, cudaStream_t stream);
+/* bsp_unet_energy_scale with a keep rule: the scaled guess is kept only when
+ * its relative residual ||b - gamma A p|| / ||b|| (from the same FP64 sums)
+ * is below keep_below, else p is zeroed (gamma = 0) and the solve starts from
+ * zero; keep_below <= 0 always keeps it.  relres_dev (optional) receives that
+ * residual.  Device-side, no host synchronisation. */
+int bsp_unet_energy_scale_keep(float *p, const float *Ap, const float *div, const uint8_t *mask,
+                               int nx, int ny, int nz, float factor, float keep_below,
+                               void *workspace, size_t workspace_bytes, float *gamma_dev,
+                               float *relres_dev, cudaStream_t stream);
 
 /* Exhaustive self-check of the device division-by-6 against IEEE division
  * over all 2^32 float bit patterns; the mismatch count is written to the

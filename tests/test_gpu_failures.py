@@ -34,6 +34,7 @@ pytestmark = pytest.mark.gpu
 DX, DT, RHO = 0.002, 0.01, 997.0
 NONFINITE, NOT_CONVERGED, TIMEOUT = 10006, 10005, 10007
 BSP_TUNE_TEST_BARRIER_ERROR = 11
+BSP_TUNE_COARSE_CLUSTER = 24
 
 
 def _pot(spec=S.POT_64, seed=7):
@@ -152,16 +153,23 @@ def test_bounded_waits_give_up_and_context_survives(cuda):
 def test_coarse_barrier_timeout_then_next_solve_succeeds(cuda):
     """A coarse-cycle barrier that gave up leaves its error word set; that
     solve returns BSP_ERR_TIMEOUT, and the next solve on the same workspace
-    (setup reused) starts from clean barrier words and succeeds."""
+    (setup reused) starts from clean barrier words and succeeds.  The
+    software grid barrier belongs to the cooperative form of the coarse
+    cycle (BSP_TUNE_COARSE_CLUSTER = 0); the cluster form waits in the
+    hardware cluster barrier."""
     spec = S.PotSpec(96, 96, 64, r_in=42, t_w=2, water_line=50, carrot_r=6, carrot_len=30)
     mat, div = _pot(spec)
-    solver = TolSolver(cell_mask(torch.as_tensor(mat).cuda()), "fp16")
-    div_t = torch.as_tensor(div).cuda()
-    assert solver.solve(div_t, DX, DT, RHO, tol=1e-6).status == 0  # builds the setup
-    call("bsp_set_tuning", BSP_TUNE_TEST_BARRIER_ERROR, 1)
-    with pytest.raises(BspError) as e:
-        solver.solve(div_t, DX, DT, RHO, tol=1e-6)
-    assert e.value.code == TIMEOUT
-    res = solver.solve(div_t, DX, DT, RHO, tol=1e-6)
-    assert res.status == 0
-    assert O.rel_residual64(res.p64, div, mat, DX, DT, RHO) <= 1.0001e-6
+    call("bsp_set_tuning", BSP_TUNE_COARSE_CLUSTER, 0)
+    try:
+        solver = TolSolver(cell_mask(torch.as_tensor(mat).cuda()), "fp16")
+        div_t = torch.as_tensor(div).cuda()
+        assert solver.solve(div_t, DX, DT, RHO, tol=1e-6).status == 0  # builds the setup
+        call("bsp_set_tuning", BSP_TUNE_TEST_BARRIER_ERROR, 1)
+        with pytest.raises(BspError) as e:
+            solver.solve(div_t, DX, DT, RHO, tol=1e-6)
+        assert e.value.code == TIMEOUT
+        res = solver.solve(div_t, DX, DT, RHO, tol=1e-6)
+        assert res.status == 0
+        assert O.rel_residual64(res.p64, div, mat, DX, DT, RHO) <= 1.0001e-6
+    finally:
+        call("bsp_set_tuning", BSP_TUNE_COARSE_CLUSTER, 16)

@@ -16,6 +16,8 @@ pytestmark = pytest.mark.gpu
 
 DX, DT, RHO = 0.002, 0.01, 997.0
 
+COARSE_CLUSTER_DEFAULT = 16  # BSP_TUNE_COARSE_CLUSTER as the library starts
+
 
 @pytest.fixture(scope="module")
 def pot64():
@@ -242,15 +244,51 @@ def test_coarse_cycle_tail_in_shared_memory_bit_identical(cuda, storage, size):
     div = O.divergence(ux, uy, uz, mat, DX)
     out = {}
     try:
+        _lib.call("bsp_set_tuning", 24, 0)  # the cooperative kernel, where the option lives
         for tail in (0, 1):
             _lib.call("bsp_set_tuning", 14, tail)
             res = solve_tolerance(div, mat, DX, DT, RHO, tol=1e-6, storage=storage)
             out[tail] = (res.p64.copy(), res.inner_iterations)
     finally:
         _lib.call("bsp_set_tuning", 14, 0)
+        _lib.call("bsp_set_tuning", 24, COARSE_CLUSTER_DEFAULT)
     assert out[0][1] == out[1][1]
     assert np.array_equal(out[0][0], out[1][0])
     assert O.rel_residual64(out[1][0], div, mat, DX, DT, RHO) <= 1.0001e-6
+
+
+@pytest.mark.parametrize("storage,size", [("fp16", 96), ("fp32", 192), ("fp16", 192)])
+def test_coarse_cycle_in_one_cluster_bit_identical(cuda, storage, size):
+    """The coarse cycle run by one thread-block cluster with hardware cluster
+    barriers (BSP_TUNE_COARSE_CLUSTER = 8 or 16 CTAs), its smallest levels in
+    CTA 0's shared memory or not (BSP_TUNE_CLUSTER_TAIL), gives the bits of
+    the cooperative kernel over every SM (= 0), host-driven and in the
+    device-driven graph: the same phases on the same quads, only spread over
+    other CTAs."""
+    from boilingsim_b200 import _lib
+
+    spec = S.PotSpec(size, size, size * 2 // 3, r_in=size / 2 - 4, t_w=3,
+                     water_line=size * 0.45, carrot_r=5, carrot_len=size // 3)
+    mat = S.pot_mat(spec)
+    ux, uy, uz = S.velocity_field(mat, seed=11)
+    div = O.divergence(ux, uy, uz, mat, DX)
+    out = {}
+    try:
+        for cl, tail in ((0, 1), (8, 1), (16, 1), (16, 0)):
+            _lib.call("bsp_set_tuning", 24, cl)
+            _lib.call("bsp_set_tuning", 25, tail)
+            for graph in (False, True):
+                res = solve_tolerance(div, mat, DX, DT, RHO, tol=1e-6, storage=storage,
+                                      graph=graph)
+                assert res.status == 0
+                out[cl, tail, graph] = (res.p64.copy(), res.inner_iterations)
+    finally:
+        _lib.call("bsp_set_tuning", 24, COARSE_CLUSTER_DEFAULT)
+        _lib.call("bsp_set_tuning", 25, 0)
+    for key, (p64, its) in out.items():
+        assert its == out[0, 1, key[2]][1], key
+        assert np.array_equal(p64, out[0, 1, key[2]][0]), key
+    assert O.rel_residual64(out[16, 1, True][0], div, mat, DX, DT, RHO) <= 1.0001e-6
 
 
 @pytest.mark.parametrize("storage", ["fp32", "fp16"])
