@@ -1088,6 +1088,14 @@ def run_projection(args, dev, rank, world, local, dist):
             "method": {"name": kind, "description": method[kind],
                        "launch": ("host-driven refinement loop" if args.host_driven else
                                   "one device-driven CUDA graph per solve")},
+            "guess": ({"mode": warm.mode, "keep_below": warm.keep_below,
+                       "rel_residual_of_scaled_guess": round(float(warm.relres.item()), 4),
+                       "gamma": float(warm.gamma.item()),
+                       "kept": float(warm.gamma.item()) != 0.0,
+                       "rule": "the energy-scaled guess starts the solve only when its "
+                               "relative residual is below keep_below, else the solve "
+                               "starts from zero (decided on the device; the network's time "
+                               "stays in the step)"} if kind == "learned" else None),
             "solve": {"inner_iterations": res.inner_iterations,
                       "outer_iterations": res.outer_iterations, "levels": res.levels,
                       "rel_residual_fp64": res.rel_residual, "status": res.status},

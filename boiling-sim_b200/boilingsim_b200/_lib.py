@@ -114,6 +114,8 @@ SIGNATURES = {
     "bsp_unet_restrict_div": (_I, [_P, _P, _P, _P, _I, _I, _I, _P]),
     "bsp_unet_prolong": (_I, [_P, _P, _P, _I, _I, _I, _P]),
     "bsp_unet_energy_scale": (_I, [_P, _P, _P, _P, _I, _I, _I, _F, _P, ctypes.c_size_t, _P, _P]),
+    "bsp_unet_energy_scale_keep": (_I, [_P, _P, _P, _P, _I, _I, _I, _F, _F, _P, ctypes.c_size_t,
+                                        _P, _P, _P]),
     "bsp_spmv": (_I, [_P, _P, _P, _I, _I, _I, _P]),
     "bsp_selftest_div6": (_I, [_P, _P]),
     "bsp_selftest_waits": (_I, [_P, _P, _P]),

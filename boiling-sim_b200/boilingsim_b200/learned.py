@@ -526,23 +526,31 @@ class WarmStart:
     the domain).
 
     ``scale=True`` (default) multiplies the prediction by the energy-optimal
-    gamma = (b . p) / (p . A p) (bsp_unet_energy_scale), so the guess handed
-    to the solve is never farther from the solution than zero in the A-norm:
-    the plain solve stays the judge of the network's error."""
+    gamma = (b . p) / (p . A p) (bsp_unet_energy_scale_keep), so the guess
+    handed to the solve is never farther from the solution than zero in the
+    A-norm: the plain solve stays the judge of the network's error.  With
+    ``keep_below`` > 0 the scaled guess is kept only when its relative
+    residual ||b - A p|| / ||b|| is below that value, else the solve starts
+    from zero (decided on the device, no host synchronisation; the residual
+    of the last guess is in ``relres``).  The default 0.1: measured on the
+    384x384x256 pot, guesses with relative residuals 1.01 and 0.60 took 34
+    and 35 inner iterations and one at 0.10 took 31, against 31 from zero."""
 
     def __init__(self, net: UNet, mat_t: torch.Tensor, mask: torch.Tensor, mode: str = "auto",
-                 scale: bool = True):
+                 scale: bool = True, keep_below: float = 0.1):
         from .fluid import cell_mask
 
         self.net = net
         self.dims = tuple(mat_t.shape)
         self.mask = mask
         self.scale = scale
+        self.keep_below = float(keep_below)
         if scale:
             self.Ap = torch.empty(self.dims, dtype=torch.float32, device=mat_t.device)
             nb = int(_lib.lib().bsp_unet_scale_workspace_bytes())
             self.ws = torch.empty((nb + 7) // 8, dtype=torch.float64, device=mat_t.device)
             self.gamma = torch.zeros(1, dtype=torch.float32, device=mat_t.device)
+            self.relres = torch.zeros(1, dtype=torch.float32, device=mat_t.device)
         nx, ny, nz = self.dims
         if mode == "auto":
             # large grids: the network two coarsenings down when the
@@ -614,9 +622,9 @@ class WarmStart:
                 call("bsp_unet_prolong", ptr(dst), ptr(self.pc[lv]), ptr(dmask), *ddims, st)
         if self.scale:
             call("bsp_spmv", ptr(self.Ap), ptr(out), ptr(self.mask), nx, ny, nz, st)
-            call("bsp_unet_energy_scale", ptr(out), ptr(self.Ap), ptr(div), ptr(self.mask), nx, ny,
-                 nz, -(rho * dx * dx / dt), ptr(self.ws), self.ws.numel() * 8, ptr(self.gamma),
-                 st)
+            call("bsp_unet_energy_scale_keep", ptr(out), ptr(self.Ap), ptr(div), ptr(self.mask),
+                 nx, ny, nz, -(rho * dx * dx / dt), self.keep_below, ptr(self.ws),
+                 self.ws.numel() * 8, ptr(self.gamma), ptr(self.relres), st)
         return out
 
 

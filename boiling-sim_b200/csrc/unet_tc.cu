@@ -898,7 +898,10 @@ __global__ void rms_final_kernel(float *__restrict__ s_out, const double *__rest
 // Energy-optimal scale of a starting pressure: with b = factor div on fluid
 // cells, gamma = (b . p) / (p . A p) minimises ||p* - gamma p||_A, so the
 // scaled guess is never farther from the solution than zero in the A-norm.
-// Partials of (b . p, p . Ap) per block in FP64, fixed order.
+// Partials of (b . p, p . Ap, b . b, b . Ap, Ap . Ap) per block in FP64,
+// fixed order; the last three give the residual of the scaled guess,
+// ||b - gamma A p||^2 = b.b - 2 gamma b.Ap + gamma^2 Ap.Ap.
+constexpr int EN_SUMS = 5;
 __global__ void __launch_bounds__(256) energy_partial_kernel(double *__restrict__ part,
                                                              const float *__restrict__ p,
                                                              const float *__restrict__ Ap,
@@ -908,8 +911,8 @@ __global__ void __launch_bounds__(256) energy_partial_kernel(double *__restrict_
   // four cells per step (float4 loads, one mask word): the four products
   // summed in FP32, widened once, the sums over steps, threads and blocks in
   // FP64 and a fixed order
-  __shared__ double sh[2][8];
-  double a = 0.0, c = 0.0;
+  __shared__ double sh[EN_SUMS][8];
+  double acc[EN_SUMS] = {0.0, 0.0, 0.0, 0.0, 0.0};
   const int64_t n4 = n >> 2;
   const float4 *p4 = reinterpret_cast<const float4 *>(p);
   const float4 *a4 = reinterpret_cast<const float4 *>(Ap);
@@ -920,62 +923,74 @@ __global__ void __launch_bounds__(256) energy_partial_kernel(double *__restrict_
     const uint32_t mw = __ldg(m4 + v);
     if (!(mw & 0x80808080u)) continue;  // no fluid cell among the four
     const float4 pv = __ldg(p4 + v), av = __ldg(a4 + v), dv = __ldg(d4 + v);
-    // products of non-fluid cells selected away (never multiplied by 0, so a
+    // values of non-fluid cells selected away (never multiplied by 0, so a
     // non-finite value there cannot leak in)
     const bool q0 = mw & 0x80u, q1 = mw & 0x8000u, q2 = mw & 0x800000u, q3 = mw & 0x80000000u;
-    const float bp = ((q0 ? factor * dv.x * pv.x : 0.0f) + (q1 ? factor * dv.y * pv.y : 0.0f)) +
-                     ((q2 ? factor * dv.z * pv.z : 0.0f) + (q3 ? factor * dv.w * pv.w : 0.0f));
-    const float pa = ((q0 ? pv.x * av.x : 0.0f) + (q1 ? pv.y * av.y : 0.0f)) +
-                     ((q2 ? pv.z * av.z : 0.0f) + (q3 ? pv.w * av.w : 0.0f));
-    a += (double)bp;
-    c += (double)pa;
+    const float b0 = q0 ? factor * dv.x : 0.0f, b1 = q1 ? factor * dv.y : 0.0f;
+    const float b2 = q2 ? factor * dv.z : 0.0f, b3 = q3 ? factor * dv.w : 0.0f;
+    const float p0 = q0 ? pv.x : 0.0f, p1 = q1 ? pv.y : 0.0f, p2 = q2 ? pv.z : 0.0f,
+                p3 = q3 ? pv.w : 0.0f;
+    const float A0 = q0 ? av.x : 0.0f, A1 = q1 ? av.y : 0.0f, A2 = q2 ? av.z : 0.0f,
+                A3 = q3 ? av.w : 0.0f;
+    acc[0] += (double)((b0 * p0 + b1 * p1) + (b2 * p2 + b3 * p3));
+    acc[1] += (double)((p0 * A0 + p1 * A1) + (p2 * A2 + p3 * A3));
+    acc[2] += (double)((b0 * b0 + b1 * b1) + (b2 * b2 + b3 * b3));
+    acc[3] += (double)((b0 * A0 + b1 * A1) + (b2 * A2 + b3 * A3));
+    acc[4] += (double)((A0 * A0 + A1 * A1) + (A2 * A2 + A3 * A3));
   }
   // the n mod 4 tail cells, by block 0
   if (blockIdx.x == 0 && threadIdx.x < (int)(n & 3)) {
     const int64_t v = (n4 << 2) + threadIdx.x;
     if (mask[v] & BSP_CLASS_FLUID) {
-      a += (double)(factor * div[v] * p[v]);
-      c += (double)(p[v] * Ap[v]);
+      const float b = factor * div[v];
+      acc[0] += (double)(b * p[v]);
+      acc[1] += (double)(p[v] * Ap[v]);
+      acc[2] += (double)(b * b);
+      acc[3] += (double)(b * Ap[v]);
+      acc[4] += (double)(Ap[v] * Ap[v]);
     }
   }
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_xor_sync(0xffffffffu, a, o);
-    c += __shfl_xor_sync(0xffffffffu, c, o);
-  }
-  if ((threadIdx.x & 31) == 0) {
-    sh[0][threadIdx.x >> 5] = a;
-    sh[1][threadIdx.x >> 5] = c;
-  }
+#pragma unroll
+  for (int k = 0; k < EN_SUMS; ++k)
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+  if ((threadIdx.x & 31) == 0)
+#pragma unroll
+    for (int k = 0; k < EN_SUMS; ++k) sh[k][threadIdx.x >> 5] = acc[k];
   __syncthreads();
-  if (threadIdx.x == 0) {
-    double sa = 0.0, sc = 0.0;
-    for (int w = 0; w < 8; ++w) {
-      sa += sh[0][w];
-      sc += sh[1][w];
-    }
-    part[2 * blockIdx.x] = sa;
-    part[2 * blockIdx.x + 1] = sc;
+  if (threadIdx.x < EN_SUMS) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += sh[threadIdx.x][w];
+    part[EN_SUMS * blockIdx.x + threadIdx.x] = t;
   }
 }
 // gamma from the partials (0 when p . A p is not positive), then p *= gamma.
-// The first warp of each block sums the partials: lane l takes blocks
-// l, l + 32, ..., then a fixed shuffle tree (the same order in every block).
+// With keep_below > 0 the guess is dropped (gamma = 0: the solve starts from
+// zero) unless the relative residual of the scaled guess,
+// ||b - gamma A p|| / ||b||, is below keep_below.  The first warp of each
+// block sums the partials: lane l takes blocks l, l + 32, ..., then a fixed
+// shuffle tree (the same order in every block).
 __global__ void energy_scale_kernel(float *__restrict__ p, const double *__restrict__ part,
-                                    int nb, int64_t n, float *__restrict__ gamma_out) {
+                                    int nb, int64_t n, float keep_below,
+                                    float *__restrict__ gamma_out,
+                                    float *__restrict__ relres_out) {
   __shared__ float g;
   if (threadIdx.x < 32) {
-    double a = 0.0, c = 0.0;
-    for (int b = threadIdx.x; b < nb; b += 32) {
-      a += part[2 * b];
-      c += part[2 * b + 1];
-    }
-    for (int o = 16; o > 0; o >>= 1) {
-      a += __shfl_xor_sync(0xffffffffu, a, o);
-      c += __shfl_xor_sync(0xffffffffu, c, o);
-    }
+    double t[EN_SUMS] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int b = threadIdx.x; b < nb; b += 32)
+#pragma unroll
+      for (int k = 0; k < EN_SUMS; ++k) t[k] += part[EN_SUMS * b + k];
+#pragma unroll
+    for (int k = 0; k < EN_SUMS; ++k)
+      for (int o = 16; o > 0; o >>= 1) t[k] += __shfl_xor_sync(0xffffffffu, t[k], o);
     if (threadIdx.x == 0) {
-      g = (c > 0.0 && a == a) ? (float)(a / c) : 0.0f;
+      const double a = t[0], c = t[1], bb = t[2], bA = t[3], AA = t[4];
+      const double gd = (c > 0.0 && a == a) ? a / c : 0.0;
+      const double rr = fmax(bb - 2.0 * gd * bA + gd * gd * AA, 0.0);
+      const double rel = bb > 0.0 ? sqrt(rr / bb) : 0.0;
+      const bool keep = keep_below <= 0.0f || rel < (double)keep_below;
+      g = keep ? (float)gd : 0.0f;
       if (blockIdx.x == 0 && gamma_out) *gamma_out = g;
+      if (blockIdx.x == 0 && relres_out) *relres_out = (float)rel;
     }
   }
   __syncthreads();
@@ -1155,7 +1170,7 @@ extern "C" int bsp_unet_tc_error(int *flag_host) {
 }
 
 extern "C" size_t bsp_unet_scale_workspace_bytes(void) {
-  return sizeof(double) * 2 * RMS_BLOCKS;
+  return sizeof(double) * EN_SUMS * RMS_BLOCKS;
 }
 
 extern "C" int bsp_unet_input_scale(float *s_dev, const float *div, const uint8_t *mask, int nx,
@@ -1238,10 +1253,25 @@ extern "C" int bsp_unet_prolong(float *p, const float *pc, const uint8_t *mask, 
   return (int)cudaGetLastError();
 }
 
+extern "C" int bsp_unet_energy_scale_keep(float *p, const float *Ap, const float *div,
+                                          const uint8_t *mask, int nx, int ny, int nz,
+                                          float factor, float keep_below, void *workspace,
+                                          size_t workspace_bytes, float *gamma_dev,
+                                          float *relres_dev, cudaStream_t s);
+
 extern "C" int bsp_unet_energy_scale(float *p, const float *Ap, const float *div,
                                      const uint8_t *mask, int nx, int ny, int nz, float factor,
                                      void *workspace, size_t workspace_bytes, float *gamma_dev,
                                      cudaStream_t s) {
+  return bsp_unet_energy_scale_keep(p, Ap, div, mask, nx, ny, nz, factor, 0.0f, workspace,
+                                    workspace_bytes, gamma_dev, nullptr, s);
+}
+
+extern "C" int bsp_unet_energy_scale_keep(float *p, const float *Ap, const float *div,
+                                          const uint8_t *mask, int nx, int ny, int nz,
+                                          float factor, float keep_below, void *workspace,
+                                          size_t workspace_bytes, float *gamma_dev,
+                                          float *relres_dev, cudaStream_t s) {
   if (!p || !Ap || !div || !mask || !workspace) return BSP_ERR_NULL;
   if (workspace_bytes < bsp_unet_scale_workspace_bytes() || ((uintptr_t)workspace & 7u))
     return BSP_ERR_WORKSPACE;
@@ -1255,6 +1285,7 @@ extern "C" int bsp_unet_energy_scale(float *p, const float *Ap, const float *div
   energy_partial_kernel<<<RMS_BLOCKS, 256, 0, s>>>(static_cast<double *>(workspace), p, Ap, div,
                                                    mask, n, factor);
   energy_scale_kernel<<<grid_for((n + 3) / 4), 256, 0, s>>>(
-      p, static_cast<const double *>(workspace), RMS_BLOCKS, n, gamma_dev);
+      p, static_cast<const double *>(workspace), RMS_BLOCKS, n, keep_below, gamma_dev,
+      relres_dev);
   return (int)cudaGetLastError();
 }

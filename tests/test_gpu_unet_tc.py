@@ -297,6 +297,20 @@ def test_energy_scale_of_a_guess(cuda):
     e = got.astype(np.float64) - pstar
     anorm = lambda v: float(v @ O.apply_A_f64(v.reshape(mat.shape), mat).ravel())  # noqa: E731
     assert anorm(e.ravel()) <= anorm(pstar.ravel())
+    # the keep rule: the relative residual ||b - gamma A p|| / ||b|| of the
+    # scaled guess from the same sums; kept below keep_below, else zeroed
+    rel = float(np.linalg.norm(b - gamma * Ap64) / np.linalg.norm(b))
+    for keep_below, kept in ((rel * 1.5, True), (rel * 0.5, False), (0.0, True)):
+        pk = torch.as_tensor(p).cuda()
+        gk = torch.zeros(1, device="cuda")
+        rk = torch.zeros(1, device="cuda")
+        call("bsp_unet_energy_scale_keep", ptr(pk), ptr(Ap), ptr(dd), ptr(mask), *mat.shape,
+             factor, keep_below, ptr(ws), ws.numel() * 8, ptr(gk), ptr(rk), 0)
+        assert abs(float(rk.item()) - rel) <= 1e-4 * rel
+        if kept:
+            assert torch.equal(pk, pd) and float(gk.item()) == float(g.item())
+        else:
+            assert float(gk.item()) == 0.0 and not torch.any(pk != 0)
 
 
 @pytest.mark.parametrize("mode", ["full", "coarse", "coarse4"])
