@@ -248,26 +248,126 @@ def pressure_projection(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, dt:
     return float(ws.max_div.item())
 
 
+_STORAGE = {"b200-mg": "fp32", "b200-mixed": "fp16", "b200-bf16": "bf16",
+            "b200-learned": "fp16"}
+
+
 def _tol_projection(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, solver: str,
-                    dt: float, rho: float) -> None:
+                    dt: float, rho: float, tol_solver=None, warm_start=None,
+                    wait: bool = True) -> None:
     """Solve, gradient and diagnostic divergence of the to-tolerance back-ends
     (multigrid-preconditioned CG inside FP64 refinement, stopping at
-    ||b - A p|| <= pressure_tol ||b|| in FP64); ws.div_u holds the divergence."""
+    ||b - A p|| <= pressure_tol ||b|| in FP64); ws.div_u holds the divergence.
+    tol_solver / warm_start: the caller's own objects (else the per-grid
+    caches).  wait=False: the solve is only enqueued (no host synchronisation
+    once its graph exists)."""
     mask = grid_mask(grid)
     dx = float(grid.dx)
-    storage = {"b200-mg": "fp32", "b200-mixed": "fp16", "b200-bf16": "bf16",
-               "b200-learned": "fp16"}[solver]
-    tol_solver = _tol_solver(grid, storage)
+    if tol_solver is None:
+        tol_solver = _tol_solver(grid, _STORAGE[solver])
     warm = bool(cfg.solver.pressure_warm_start)
     if solver == "b200-learned" and all(d % 8 == 0 for d in grid.shape):
         # the network's pressure is the starting guess; the solve finishes it
         # to the same tolerance (grids not divisible by 8 start from zero)
-        _warm_start(grid, mask).guess(ws.div_u, dx, dt, rho, out=grid.p)
+        (warm_start or _warm_start(grid, mask)).guess(ws.div_u, dx, dt, rho, out=grid.p)
         warm = True
     tol_solver.solve(ws.div_u, dx, dt, rho, tol=float(cfg.solver.pressure_tol), p=grid.p,
-                     warm_start=warm, raise_on_fail=False, graph=True)
+                     warm_start=warm, raise_on_fail=False, graph=True, wait=wait)
     subtract_pressure_gradient(grid.ux, grid.uy, grid.uz, grid.p, mask, dx, dt, rho)
     compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, mask, dx, ws.max_div)
+
+
+class ProjectionPipeline:
+    """Independent pressure projections of one geometry with host velocity
+    buffers, ``depth`` of them in flight.
+
+    Each slot owns its device fields, workspace, solver, learned warm start
+    (with its own network buffers) and CUDA stream.  ``submit`` enqueues on
+    the slot's stream the host->device copy of the velocities (pinned host
+    tensors), the projection (``pressure_projection``'s operations: the
+    divergence, the solve to ``pressure_tol``, the gradient subtraction and
+    the diagnostic divergence) and the device->host copies of the corrected
+    velocities, the pressure and max |div u|, and returns a ticket at once;
+    ``result`` waits for that projection and returns its max |div u|.  The
+    copy engines then move one projection's fields while another computes.
+    The host buffers given to ``submit`` must stay untouched until its
+    ``result`` is taken.  Back-ends: the to-tolerance ones (``b200-mg``,
+    ``b200-mixed``, ``b200-bf16``, ``b200-learned``) and ``b200-jacobi``,
+    chosen as ``pressure_projection`` chooses (BOILINGSIM_PRESSURE_SOLVER)."""
+
+    def __init__(self, mat: torch.Tensor, dx: float, cfg: ScenarioConfig, depth: int = 2):
+        from .solver import TolSolver
+
+        if mat.dtype != torch.int32 or not mat.is_cuda:
+            raise TypeError("mat must be an int32 CUDA tensor")
+        if depth < 1:
+            raise ValueError("depth must be >= 1")
+        self.solver = _select_pressure_solver()
+        if self.solver not in ("b200-jacobi", "jacobi") and self.solver not in _STORAGE:
+            raise ValueError(f"{self.solver!r} launches on the legacy default stream; "
+                             "ProjectionPipeline needs a stream-ordered back-end")
+        self.cfg = cfg
+        self.dx = float(dx)
+        nx, ny, nz = mat.shape
+        dev = mat.device
+        mask = cell_mask(mat)
+        z = lambda *shp: torch.zeros(shp, dtype=torch.float32, device=dev)  # noqa: E731
+        self.slots = []
+        for _ in range(depth):
+            grid = Grid(nx, ny, nz, self.dx, z(nx, ny, nz), mat, z(nx + 1, ny, nz),
+                        z(nx, ny + 1, nz), z(nx, ny, nz + 1), mask=mask)
+            ws = FluidWorkspace(z(nx, ny, nz), z(nx, ny, nz), z(1))
+            slot = {"grid": grid, "ws": ws, "stream": torch.cuda.Stream(device=dev),
+                    "done": None, "max_div": torch.zeros(1, dtype=torch.float32).pin_memory(),
+                    "tol": None, "warm": None}
+            if self.solver in _STORAGE:
+                slot["tol"] = TolSolver(mask, _STORAGE[self.solver], device=dev)
+                if self.solver == "b200-learned" and all(d % 8 == 0 for d in grid.shape):
+                    from .learned import UNet, WarmStart
+
+                    slot["warm"] = WarmStart(UNet.load(device=dev), mat, mask)
+            self.slots.append(slot)
+        # the mask, weights and buffers above were made on the current stream;
+        # the slots' streams start after them
+        torch.cuda.synchronize(dev)
+        self.issued = 0
+
+    def submit(self, ux_h, uy_h, uz_h, ux_out, uy_out, uz_out, p_out, dt: float,
+               rho: float) -> int:
+        slot = self.slots[self.issued % len(self.slots)]
+        if slot["done"] is not None:
+            slot["done"].synchronize()  # the slot's previous projection has left the device
+        grid, ws = slot["grid"], slot["ws"]
+        with torch.cuda.stream(slot["stream"]):
+            for d, h in zip((grid.ux, grid.uy, grid.uz), (ux_h, uy_h, uz_h)):
+                d.copy_(h, non_blocking=True)
+            if self.solver in ("b200-jacobi", "jacobi"):
+                nx, ny, nz = grid.shape
+                call("bsp_projection_jacobi", ptr(grid.p), ptr(ws.p_tmp), ptr(ws.div_u),
+                     ptr(grid.ux), ptr(grid.uy), ptr(grid.uz), ptr(grid.mask), nx, ny, nz,
+                     self.dx, float(dt), float(rho), int(self.cfg.solver.pressure_max_iter), 0,
+                     ptr(ws.max_div), stream_handle())
+            else:
+                compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, grid.mask, self.dx)
+                _tol_projection(grid, ws, self.cfg, self.solver, dt, rho,
+                                tol_solver=slot["tol"], warm_start=slot["warm"], wait=False)
+            p_out.copy_(grid.p, non_blocking=True)
+            for h, d in zip((ux_out, uy_out, uz_out), (grid.ux, grid.uy, grid.uz)):
+                h.copy_(d, non_blocking=True)
+            slot["max_div"].copy_(ws.max_div, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record()
+        slot["done"] = ev
+        slot["ticket"] = self.issued
+        self.issued += 1
+        return self.issued - 1
+
+    def result(self, ticket: int) -> float:
+        slot = self.slots[ticket % len(self.slots)]
+        if slot.get("ticket") != ticket:
+            raise ValueError("that projection's slot has been reused; take results in order")
+        slot["done"].synchronize()
+        return float(slot["max_div"].item())
 
 
 _NET = None

@@ -67,10 +67,13 @@ class TolSolver:
               p: torch.Tensor | None = None, warm_start: bool = False, inner_tol: float | None = None,
               max_outer: int | None = None, max_inner: int | None = None,
               check_every: int | None = None, stream=None, raise_on_fail: bool = True,
-              graph: bool = False) -> SolveResult:
+              graph: bool = False, wait: bool = True) -> SolveResult:
         """Solve A p = b for the divergence ``div``.  ``graph=True`` runs the
         whole solve as one device-driven CUDA graph (built on the first call
-        with this set of buffers, replayed afterwards)."""
+        with this set of buffers, replayed afterwards).  ``wait=False`` (with
+        ``graph``, after the first solve on these buffers) only enqueues the
+        graph: p is written when the stream reaches it and the returned
+        result carries no iteration counts (status 0, counts -1)."""
         nx, ny, nz = self.shape
         if p is None:
             p = torch.zeros(self.shape, dtype=torch.float32, device=self.mask.device)
@@ -88,15 +91,20 @@ class TolSolver:
         if check_every is not None:
             prm.check_every = int(check_every)
         info = BspSolveInfo()
+        enqueue_only = graph and not wait and self._setup_done
         code = _lib.lib().bsp_solve_tol(ptr(p), ptr(div), ptr(self.mask), nx, ny, nz, float(dx),
                                          float(dt), float(rho), ctypes.byref(prm), ptr(self.ws),
-                                         self.ws.numel(), ptr(self.x64), ctypes.byref(info),
+                                         self.ws.numel(), ptr(self.x64),
+                                         None if enqueue_only else ctypes.byref(info),
                                          stream_handle(stream))
         if code not in (0, 10005) or (raise_on_fail and code != 0):
             _lib.check("bsp_solve_tol", code)
         self._setup_done = True
-        self.last = SolveResult(p, self.x64, code, info.outer_iterations, info.inner_iterations,
-                                info.levels, info.rel_residual)
+        if enqueue_only:
+            self.last = SolveResult(p, self.x64, code, -1, -1, -1, float("nan"))
+        else:
+            self.last = SolveResult(p, self.x64, code, info.outer_iterations,
+                                    info.inner_iterations, info.levels, info.rel_residual)
         return self.last
 
 

@@ -251,7 +251,17 @@ __device__ __forceinline__ float4 znf_segment(const float *__restrict__ p,
   return make_float4(o4[0], o4[1], o4[2], o4[3]);
 }
 
-template <bool FULL>
+// L2 prefetch of one 128-byte line (no register result, does not block).
+__device__ __forceinline__ void prefetch_l2(const void *ptr) {
+  asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+}
+
+// PF > 0: each plane step also prefetches into L2 the p and mask rows of
+// plane i + PF and, when plane i + 1 holds fluid in this segment, its rhs
+// row, so that the next steps' loads wait on L2 instead of DRAM (one lane per
+// 128-byte line).  Measured at 384x384x256: 93.5 us per sweep without, 81.4
+// with PF = 2.
+template <bool FULL, int PF>
 __global__ void __launch_bounds__(256) sweep_znf_kernel(float *__restrict__ out,
                                                         const float *__restrict__ p,
                                                         const float *__restrict__ rhs,
@@ -285,6 +295,10 @@ __global__ void __launch_bounds__(256) sweep_znf_kernel(float *__restrict__ out,
       pn = ld4(p + o + plane);
       mn = mw4(mask, o + plane, 0, 0);
     }
+    if (PF > 0 && act && i + PF < nx && (lane & 7) == 0) {
+      prefetch_l2(p + o + PF * plane);
+      if (lane == 0) prefetch_l2(mask + o + PF * plane);
+    }
     float4 v = z4;
     if (__any_sync(0xffffffffu, (mc & 0x80808080u) != 0u)) {
       // fluid bytes' solid-neighbour counts: bit 0 of each fluid byte times 7
@@ -297,12 +311,18 @@ __global__ void __launch_bounds__(256) sweep_znf_kernel(float *__restrict__ out,
                                mc, mn);
     }
     if (act) *reinterpret_cast<float4 *>(out + o) = v;
+    if (PF > 0 && __any_sync(0xffffffffu, (mn & 0x80808080u) != 0u) && act && (lane & 7) == 0)
+      prefetch_l2(rhs + o + plane);
     pm = pc;
     mm = mc;
     pc = pn;
     mc = mn;
   }
 }
+
+// BSP_TUNE_SWEEP_PREFETCH: the ZNF sweep's L2 prefetch distance in planes
+// (0 off, 2 default, 3).
+int g_sweep_prefetch = 2;
 
 // ---- generic kernel -----------------------------------------------------------
 template <int OP, class MaskT>
@@ -482,9 +502,15 @@ cudaError_t launch_sweep_znf(float *out, const float *p, const float *rhs, const
   const int bi = g_sweep_bi > 0 ? g_sweep_bi : pick_bi(nx, ny, nz);
   dim3 grid((nz / 4 + 31) / 32, (ny + 7) / 8, (nx + bi - 1) / bi);
   if (nz % 128 == 0)
-    sweep_znf_kernel<true><<<grid, 256, 0, s>>>(out, p, rhs, mask, nx, ny, nz, bi);
+    (g_sweep_prefetch == 3   ? sweep_znf_kernel<true, 3>
+     : g_sweep_prefetch == 2 ? sweep_znf_kernel<true, 2>
+                             : sweep_znf_kernel<true, 0>)<<<grid, 256, 0, s>>>(
+        out, p, rhs, mask, nx, ny, nz, bi);
   else
-    sweep_znf_kernel<false><<<grid, 256, 0, s>>>(out, p, rhs, mask, nx, ny, nz, bi);
+    (g_sweep_prefetch == 3   ? sweep_znf_kernel<false, 3>
+     : g_sweep_prefetch == 2 ? sweep_znf_kernel<false, 2>
+                             : sweep_znf_kernel<false, 0>)<<<grid, 256, 0, s>>>(
+        out, p, rhs, mask, nx, ny, nz, bi);
   return cudaGetLastError();
 }
 
@@ -695,6 +721,10 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_CONV_EPILOGUE:
       if (value < 0 || value > 4) return BSP_ERR_ARG;
       bsp::utc::g_utc_nepi = value;
+      return BSP_OK;
+    case BSP_TUNE_SWEEP_PREFETCH:
+      if (value != 0 && value != 2 && value != 3) return BSP_ERR_ARG;
+      bsp::g_sweep_prefetch = value;
       return BSP_OK;
     case BSP_TUNE_CLUSTER_TAIL:
       if (value < 0 || value > 1) return BSP_ERR_ARG;

@@ -87,6 +87,8 @@ extern "C" {
                                       kernel over all SMs */
 #define BSP_TUNE_CLUSTER_TAIL 25  /* with COARSE_CLUSTER: levels of <= 2048 cells in CTA 0's shared
                                      memory, 1 on, 0 off (default) */
+#define BSP_TUNE_SWEEP_PREFETCH 26 /* plain Jacobi sweep's L2 prefetch distance in planes:
+                                      0 off, 2 (default) or 3 */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */

@@ -161,12 +161,17 @@ def test_znf_sweep_segment_shortcuts_bit_exact(cuda, nz):
     nx, ny, _ = mat.shape
     want = O.pressure_solve(p_old, div, mat, dx, dt, rho, 6)
     m8 = mask_of(dev(mat, torch.int32))
-    p = dev(p_old)
-    tmp = torch.zeros_like(p)
-    rhs = torch.zeros_like(p)
-    call("bsp_jacobi_solve", ptr(p), ptr(tmp), ptr(dev(div)), ptr(rhs), ptr(m8), nx, ny, nz,
-         dx, dt, rho, 6, 1, 0)
-    assert np.array_equal(bits(host(p)), bits(want))
+    try:
+        for prefetch in (0, 2, 3):  # BSP_TUNE_SWEEP_PREFETCH
+            call("bsp_set_tuning", 26, prefetch)
+            p = dev(p_old)
+            tmp = torch.zeros_like(p)
+            rhs = torch.zeros_like(p)
+            call("bsp_jacobi_solve", ptr(p), ptr(tmp), ptr(dev(div)), ptr(rhs), ptr(m8), nx, ny,
+                 nz, dx, dt, rho, 6, 1, 0)
+            assert np.array_equal(bits(host(p)), bits(want)), prefetch
+    finally:
+        call("bsp_set_tuning", 26, 2)
 
 
 @pytest.mark.parametrize("spec", [S.POT_64, S.PotSpec(40, 36, 30, 14, 2, 24, 4, 12)],
