@@ -788,10 +788,11 @@ def run_projection(args, dev, rank, world, local, dist):
         if kind == "learned":
             warm.guess(div, DX, DT, RHO, out=p, graph=graph)
             res = solvers["fp16"].solve(div, DX, DT, RHO, tol=TOL, p=p, warm_start=True,
-                                        graph=graph)
+                                        graph=graph, want_x64=False)
         else:
             res = solvers["fp32" if kind == "fp32" else "fp16"].solve(div, DX, DT, RHO, tol=TOL,
-                                                                      p=p, graph=graph)
+                                                                      p=p, graph=graph,
+                                                                      want_x64=False)
         F.subtract_pressure_gradient(*u, p, mask, DX, DT, RHO)
         F.compute_divergence(div, *u, mask, DX, max_div)
         last[kind] = res

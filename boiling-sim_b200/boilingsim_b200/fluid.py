@@ -254,13 +254,14 @@ _STORAGE = {"b200-mg": "fp32", "b200-mixed": "fp16", "b200-bf16": "bf16",
 
 def _tol_projection(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, solver: str,
                     dt: float, rho: float, tol_solver=None, warm_start=None,
-                    wait: bool = True) -> None:
+                    wait: bool = True, want_x64: bool = True) -> None:
     """Solve, gradient and diagnostic divergence of the to-tolerance back-ends
     (multigrid-preconditioned CG inside FP64 refinement, stopping at
     ||b - A p|| <= pressure_tol ||b|| in FP64); ws.div_u holds the divergence.
     tol_solver / warm_start: the caller's own objects (else the per-grid
     caches).  wait=False: the solve is only enqueued (no host synchronisation
-    once its graph exists)."""
+    once its graph exists); want_x64=False: the solver's FP64 iterate is not
+    copied out (its ``last.p64`` is then stale)."""
     mask = grid_mask(grid)
     dx = float(grid.dx)
     if tol_solver is None:
@@ -272,7 +273,8 @@ def _tol_projection(grid: Grid, ws: FluidWorkspace, cfg: ScenarioConfig, solver:
         (warm_start or _warm_start(grid, mask)).guess(ws.div_u, dx, dt, rho, out=grid.p)
         warm = True
     tol_solver.solve(ws.div_u, dx, dt, rho, tol=float(cfg.solver.pressure_tol), p=grid.p,
-                     warm_start=warm, raise_on_fail=False, graph=True, wait=wait)
+                     warm_start=warm, raise_on_fail=False, graph=True, wait=wait,
+                     want_x64=want_x64)
     subtract_pressure_gradient(grid.ux, grid.uy, grid.uz, grid.p, mask, dx, dt, rho)
     compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, mask, dx, ws.max_div)
 
@@ -350,7 +352,8 @@ class ProjectionPipeline:
             else:
                 compute_divergence(ws.div_u, grid.ux, grid.uy, grid.uz, grid.mask, self.dx)
                 _tol_projection(grid, ws, self.cfg, self.solver, dt, rho,
-                                tol_solver=slot["tol"], warm_start=slot["warm"], wait=False)
+                                tol_solver=slot["tol"], warm_start=slot["warm"], wait=False,
+                                want_x64=False)
             p_out.copy_(grid.p, non_blocking=True)
             for h, d in zip((ux_out, uy_out, uz_out), (grid.ux, grid.uy, grid.uz)):
                 h.copy_(d, non_blocking=True)

@@ -67,13 +67,16 @@ class TolSolver:
               p: torch.Tensor | None = None, warm_start: bool = False, inner_tol: float | None = None,
               max_outer: int | None = None, max_inner: int | None = None,
               check_every: int | None = None, stream=None, raise_on_fail: bool = True,
-              graph: bool = False, wait: bool = True) -> SolveResult:
+              graph: bool = False, wait: bool = True, want_x64: bool = True) -> SolveResult:
         """Solve A p = b for the divergence ``div``.  ``graph=True`` runs the
         whole solve as one device-driven CUDA graph (built on the first call
         with this set of buffers, replayed afterwards).  ``wait=False`` (with
         ``graph``, after the first solve on these buffers) only enqueues the
         graph: p is written when the stream reaches it and the returned
-        result carries no iteration counts (status 0, counts -1)."""
+        result carries no iteration counts (status 0, counts -1).
+        ``want_x64=False`` skips the copy of the FP64 iterate out of the
+        workspace (a device-to-device pass over n doubles); the result's
+        ``p64`` is then not this solve's."""
         nx, ny, nz = self.shape
         if p is None:
             p = torch.zeros(self.shape, dtype=torch.float32, device=self.mask.device)
@@ -94,7 +97,7 @@ class TolSolver:
         enqueue_only = graph and not wait and self._setup_done
         code = _lib.lib().bsp_solve_tol(ptr(p), ptr(div), ptr(self.mask), nx, ny, nz, float(dx),
                                          float(dt), float(rho), ctypes.byref(prm), ptr(self.ws),
-                                         self.ws.numel(), ptr(self.x64),
+                                         self.ws.numel(), ptr(self.x64) if want_x64 else None,
                                          None if enqueue_only else ctypes.byref(info),
                                          stream_handle(stream))
         if code not in (0, 10005) or (raise_on_fail and code != 0):

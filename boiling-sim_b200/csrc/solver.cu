@@ -55,13 +55,14 @@ extern bool g_fine_tma_enabled;      // BSP_TUNE_FINE_TMA (mgfine.cu)
 extern bool g_coarse_fused_enabled;  // BSP_TUNE_COARSE_FUSED (mgcoarse.cu)
 extern bool g_coarse_phases_fused;   // BSP_TUNE_COARSE_PHASES (mgcoarse.cu)
 extern bool g_coarse_tail_smem;      // BSP_TUNE_COARSE_TAIL (mgcoarse.cu)
-// BSP_TUNE_COARSE_SPLIT: S = 1 or 2 (default) runs levels 1 .. S of the
+// BSP_TUNE_COARSE_SPLIT: S = 1, 2 (default) or 3 runs levels 1 .. S of the
 // V-cycle with the column tile kernels of level 0 (restriction, prolongation
 // and smoothing) and the one-launch coarse cycle below them, as far as those
 // levels take the column layout and the cooperative launch is available; 0
 // runs every coarse level in the one launch.  Measured at 384x384x256 with two
-// sweeps on level 1: 12.79 ms (S = 1), 12.60 ms (S = 2) per solve.
-int g_coarse_split = 2;
+// sweeps on level 1: 12.79 ms (S = 1), 12.60 ms (S = 2) per solve; with the
+// one-cluster cycle below: 11.77 ms (S = 2), 11.56 ms (S = 3).
+int g_coarse_split = 3;
 // BSP_TUNE_L1_SWEEPS (split mode): smoothing sweeps on level 1 before the
 // restriction and after the prolongation, 1 or 2 (default; symmetric, so the
 // V-cycle stays an SPD preconditioner).  Measured at 384x384x256 (FP16
@@ -963,9 +964,12 @@ cudaError_t launch_inner_iteration(Ctx<T> &cx, int it_parity, cudaStream_t s) {
   auto level_col = [&](int l) {
     const Level<T> &v = cx.lv[l];
     if (l == 0) return col;
-    // coarse levels: only while a row keeps at least 16 lanes busy
-    return g_fine_col_enabled && v.nz % 4 == 0 && v.nz >= 64 &&
-           (int64_t)v.nx * v.ny * v.nz >= 131072 &&
+    // coarse levels: only while a row keeps at least 16 lanes busy (8 on
+    // level 3 with BSP_TUNE_COARSE_SPLIT = 3, which takes it onto the tile
+    // kernels)
+    const bool deep = g_coarse_split >= 3 && l >= 3;
+    return g_fine_col_enabled && v.nz % 4 == 0 && v.nz >= (deep ? 32 : 64) &&
+           (int64_t)v.nx * v.ny * v.nz >= (deep ? 32768 : 131072) &&
            fine_grid_blocks(v.nx, v.ny, v.nz) <= PARTIAL_STRIDE;
   };
   // V-cycle on r -> z: level-0 restriction, the coarse levels (one

@@ -763,7 +763,7 @@ extern "C" int bsp_set_tuning(int key, int value) {
       bsp::g_l1_sweeps = value;
       return BSP_OK;
     case BSP_TUNE_COARSE_SPLIT:
-      if (value < 0 || value > 2) return BSP_ERR_ARG;
+      if (value < 0 || value > 3) return BSP_ERR_ARG;
       bsp::g_coarse_split = value;
       return BSP_OK;
     case BSP_TUNE_COARSE_PHASES:

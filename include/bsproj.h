@@ -69,7 +69,7 @@ extern "C" {
 #define BSP_TUNE_COARSE_PHASES 12 /* coarse cycle forms t where it is read: 1 on, 0 off (default) */
 #define BSP_TUNE_COARSE_TRACE 13  /* tracing: coarse-cycle launches stamp their phase boundaries */
 #define BSP_TUNE_COARSE_TAIL 14   /* coarse levels of CTA 0 in shared memory: 1 on, 0 off (default) */
-#define BSP_TUNE_COARSE_SPLIT 15  /* levels 1..S (S = 0, 1, 2 default) on the column tile kernels,
+#define BSP_TUNE_COARSE_SPLIT 15  /* levels 1..S (S = 0..3, 3 default) on the column tile kernels,
                                      the one-launch cycle below them */
 #define BSP_TUNE_CONV_EPILOGUE 16 /* tensor-core convolution: epilogue warpgroups 2..4, 1 = two CTAs
                                      per SM with one each, 0 = per layer (default) */

@@ -164,7 +164,7 @@ def test_fused_coarse_cycle_matches_per_level_kernels(cuda, storage, spec):
             out[fused] = res
     finally:
         _lib.call("bsp_set_tuning", 5, 1)
-        _lib.call("bsp_set_tuning", 15, 2)
+        _lib.call("bsp_set_tuning", 15, 3)
     slack = 2 if storage == "fp32" else max(3, out[0].inner_iterations // 8)
     assert abs(out[1].inner_iterations - out[0].inner_iterations) <= slack
     assert O.rel_error(out[1].p64, out[0].p64, mat) < 1e-5
@@ -291,10 +291,37 @@ def test_coarse_cycle_in_one_cluster_bit_identical(cuda, storage, size):
     assert O.rel_residual64(out[16, 1, True][0], div, mat, DX, DT, RHO) <= 1.0001e-6
 
 
+def test_coarse_split_level3_on_tile_kernels(cuda):
+    """Level 3 on the tile kernels too (BSP_TUNE_COARSE_SPLIT = 3, the
+    default; it applies where level 3 keeps 32-cell rows and 32 K cells, here
+    a 256^3 pot) against the cluster cycle from level 3 (= 2): the same
+    V-cycle with sums in another order -- the same convergence, the same
+    solution to the tolerance."""
+    from boilingsim_b200 import _lib
+
+    spec = S.PotSpec(256, 256, 256, r_in=118, t_w=4, water_line=190, carrot_r=12,
+                     carrot_len=80)
+    mat = S.pot_mat(spec)
+    ux, uy, uz = S.velocity_field(mat, seed=13)
+    div = O.divergence(ux, uy, uz, mat, DX)
+    out = {}
+    try:
+        for split in (3, 2):
+            _lib.call("bsp_set_tuning", 15, split)
+            res = solve_tolerance(div, mat, DX, DT, RHO, tol=1e-6, storage="fp16", graph=True)
+            assert res.status == 0
+            assert O.rel_residual64(res.p64, div, mat, DX, DT, RHO) <= 1e-6 * 1.0001
+            out[split] = res
+    finally:
+        _lib.call("bsp_set_tuning", 15, 3)
+    assert abs(out[3].inner_iterations - out[2].inner_iterations) <= 2
+    assert O.rel_error(out[3].p64, out[2].p64, mat) < 1e-5
+
+
 @pytest.mark.parametrize("storage", ["fp32", "fp16"])
 def test_coarse_split_level1_on_tile_kernels(cuda, storage):
     """Level 1 on the column tile kernels with the one-launch cycle from level 2
-    (BSP_TUNE_COARSE_SPLIT = 1; the default 2 also takes level 2) applies the same V-cycle as the
+    (BSP_TUNE_COARSE_SPLIT = 1; the default 3 also takes levels 2-3) applies the same V-cycle as the
     one launch over every coarse level (one sweep a side on level 1 in both;
     sums in another order): same convergence, the same solution to the
     tolerance, on a pot whose level 1 takes the column layout."""
@@ -313,7 +340,7 @@ def test_coarse_split_level1_on_tile_kernels(cuda, storage):
             assert O.rel_residual64(res.p64, div, mat, DX, DT, RHO) <= 1e-7 * 1.0001
             out[split] = res
     finally:
-        _lib.call("bsp_set_tuning", 15, 2)
+        _lib.call("bsp_set_tuning", 15, 3)
         _lib.call("bsp_set_tuning", 17, 2)
     slack = 2 if storage == "fp32" else max(3, out[0].inner_iterations // 8)
     assert abs(out[1].inner_iterations - out[0].inner_iterations) <= slack
@@ -342,7 +369,7 @@ def test_level1_two_sweeps_converge_faster(cuda, storage):
             out[sweeps] = res
     finally:
         _lib.call("bsp_set_tuning", 17, 2)
-        _lib.call("bsp_set_tuning", 15, 2)
+        _lib.call("bsp_set_tuning", 15, 3)
     assert out[2].inner_iterations <= out[1].inner_iterations
     assert O.rel_error(out[2].p64, out[1].p64, mat) < 1e-5
 
