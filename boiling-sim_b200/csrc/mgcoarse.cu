@@ -79,6 +79,7 @@ struct CoarseCycle {
   int cinv_bytes;     // > 0: CTA 0 copies the dense inverse into shared memory at launch
   int tail_smem;      // 1: the levels CTA 0 runs alone live in its shared memory
   int tail_off;       // byte offset of that region in the dynamic shared memory
+  int tail_cells;     // cluster kernel: levels of at most this many cells run in CTA 0
 };
 
 // Dynamic shared memory of the coarse-cycle kernel: [dense inverse (CTA 0)]
@@ -719,7 +720,11 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cycle_kernel(CoarseCycle<T> 
 // the cluster's CTA 0 alone with __syncthreads; the coarsest solve uses the
 // dense inverse copied into CTA 0's shared memory at launch.  A cluster's CTAs
 // are co-scheduled by the hardware: no spin wait.
-constexpr int CL_TAIL_CELLS = 2048;
+// default of BSP_TUNE_CLUSTER_TAIL_CELLS.  With levels 1-3 on the tile kernels
+// the cycle's levels hold 9,216 cells and fewer at 384x384x256, and CTA 0 alone
+// runs them faster than the cluster with its barriers: 11.61 ms per solve at
+// 2048, 11.52 at 16384 (0, every level cluster-wide: 11.66).
+constexpr int CL_TAIL_CELLS = 16384;
 __device__ __forceinline__ void cluster_sync_all() {
   asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::
                    : "memory");
@@ -753,7 +758,7 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cluster_cycle_kernel(CoarseC
   const int L = a.L;
   auto cells = [&](int l) { return (int64_t)a.lv[l].nx * a.lv[l].ny * a.lv[l].nz; };
   int tail = 1;  // levels >= tail run in CTA 0 of the cluster alone
-  while (tail < L && cells(tail) > CL_TAIL_CELLS) ++tail;
+  while (tail < L && cells(tail) > a.tail_cells) ++tail;
   uint64_t *cbar = reinterpret_cast<uint64_t *>(cc_smem() + (a.cinv_bytes >> 2) +
                                                 ((a.cinv_bytes > 0) ? COARSEST_CELLS : 0));
   const bool cinv_copy = a.cinv_bytes > 0 && lead;
@@ -899,6 +904,10 @@ __global__ void __launch_bounds__(CC_THREADS, 1) mg_cluster_cycle_kernel(CoarseC
 // staging in and out costs more than the on-chip phases save), so off.
 bool g_coarse_cluster_tail_smem = false;
 
+// BSP_TUNE_CLUSTER_TAIL_CELLS: levels of at most this many cells run in the
+// cluster's CTA 0 alone (with __syncthreads instead of cluster barriers).
+int g_cluster_tail_cells = CL_TAIL_CELLS;
+
 // BSP_TUNE_COARSE_CLUSTER: CTAs of the one cluster that runs the coarse cycle
 // (2..16), or 0 for the cooperative kernel over every SM.  Measured at
 // 384x384x256 (levels 3-6 of the cycle): 12.18 ms per solve cooperative,
@@ -1023,7 +1032,8 @@ bool launch_coarse_cycle(const Level<T> *lv, int L, float *scratch, const float 
     // levels of at most CL_TAIL_CELLS cells in CTA 0's shared memory
     CoarseCycle<T> c = a;
     int ctail = 1;
-    while (ctail < L && (int64_t)lv[ctail].nx * lv[ctail].ny * lv[ctail].nz > CL_TAIL_CELLS)
+    c.tail_cells = g_cluster_tail_cells;
+    while (ctail < L && (int64_t)lv[ctail].nx * lv[ctail].ny * lv[ctail].nz > c.tail_cells)
       ++ctail;
     int64_t ctail_bytes = 0;
     if (ctail < L) {
@@ -1052,14 +1062,17 @@ bool launch_coarse_cycle(const Level<T> *lv, int L, float *scratch, const float 
           smem_opt_in((const void *)mg_cluster_cycle_kernel<T>, (int)DYN_MAX);
     }
     if (attr_ok[di]) {
+      // every level of the cycle in CTA 0: one CTA is the whole launch (its
+      // cluster barriers are then those of a one-CTA cluster)
+      const int nct = ctail <= 1 ? 1 : g_coarse_cluster;
       cudaLaunchConfig_t cc{};
-      cc.gridDim = dim3(g_coarse_cluster);
+      cc.gridDim = dim3(nct);
       cc.blockDim = dim3(CC_THREADS);
       cc.dynamicSmemBytes = (size_t)cdyn;
       cc.stream = s;
       cudaLaunchAttribute ca[1];
       ca[0].id = cudaLaunchAttributeClusterDimension;
-      ca[0].val.clusterDim.x = g_coarse_cluster;
+      ca[0].val.clusterDim.x = nct;
       ca[0].val.clusterDim.y = 1;
       ca[0].val.clusterDim.z = 1;
       cc.attrs = ca;

@@ -89,6 +89,8 @@ extern "C" {
                                      memory, 1 on, 0 off (default) */
 #define BSP_TUNE_SWEEP_PREFETCH 26 /* plain Jacobi sweep's L2 prefetch distance in planes:
                                       0 off, 2 (default) or 3 */
+#define BSP_TUNE_CLUSTER_TAIL_CELLS 27 /* cluster coarse cycle: levels of at most this many cells
+                                          run in its CTA 0 alone (default 16384) */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */

@@ -261,7 +261,8 @@ def test_coarse_cycle_tail_in_shared_memory_bit_identical(cuda, storage, size):
 def test_coarse_cycle_in_one_cluster_bit_identical(cuda, storage, size):
     """The coarse cycle run by one thread-block cluster with hardware cluster
     barriers (BSP_TUNE_COARSE_CLUSTER = 8 or 16 CTAs), its smallest levels in
-    CTA 0's shared memory or not (BSP_TUNE_CLUSTER_TAIL), gives the bits of
+    CTA 0's shared memory or not (BSP_TUNE_CLUSTER_TAIL), in CTA 0 alone below
+    0, 2048 or 16384 cells (BSP_TUNE_CLUSTER_TAIL_CELLS), gives the bits of
     the cooperative kernel over every SM (= 0), host-driven and in the
     device-driven graph: the same phases on the same quads, only spread over
     other CTAs."""
@@ -274,21 +275,24 @@ def test_coarse_cycle_in_one_cluster_bit_identical(cuda, storage, size):
     div = O.divergence(ux, uy, uz, mat, DX)
     out = {}
     try:
-        for cl, tail in ((0, 1), (8, 1), (16, 1), (16, 0)):
+        for cl, tail, cells in ((0, 0, 2048), (8, 0, 2048), (16, 1, 2048), (16, 0, 2048),
+                                (16, 0, 16384), (16, 0, 0)):
             _lib.call("bsp_set_tuning", 24, cl)
             _lib.call("bsp_set_tuning", 25, tail)
+            _lib.call("bsp_set_tuning", 27, cells)
             for graph in (False, True):
                 res = solve_tolerance(div, mat, DX, DT, RHO, tol=1e-6, storage=storage,
                                       graph=graph)
                 assert res.status == 0
-                out[cl, tail, graph] = (res.p64.copy(), res.inner_iterations)
+                out[cl, tail, cells, graph] = (res.p64.copy(), res.inner_iterations)
     finally:
         _lib.call("bsp_set_tuning", 24, COARSE_CLUSTER_DEFAULT)
         _lib.call("bsp_set_tuning", 25, 0)
+        _lib.call("bsp_set_tuning", 27, 16384)
     for key, (p64, its) in out.items():
-        assert its == out[0, 1, key[2]][1], key
-        assert np.array_equal(p64, out[0, 1, key[2]][0]), key
-    assert O.rel_residual64(out[16, 1, True][0], div, mat, DX, DT, RHO) <= 1.0001e-6
+        assert its == out[0, 0, 2048, key[3]][1], key
+        assert np.array_equal(p64, out[0, 0, 2048, key[3]][0]), key
+    assert O.rel_residual64(out[16, 0, 2048, True][0], div, mat, DX, DT, RHO) <= 1.0001e-6
 
 
 def test_coarse_split_level3_on_tile_kernels(cuda):
