@@ -167,6 +167,128 @@ __global__ void __launch_bounds__(256) no_slip_kernel(float *__restrict__ ux,
   }
 }
 
+// Four consecutive k cells per thread (nz % 4 == 0, 16-byte aligned fields):
+// the same per-cell operations as divergence_kernel / gradient_kernel, so the
+// same bits, with 16-byte loads of the mask word, ux, uy and div (the rows of
+// uz are nz + 1 long and are read as scalars).  Block = (32 k-quads, 8 j).
+__device__ __forceinline__ float q4v(const float4 &v, int q) {
+  return q == 0 ? v.x : (q == 1 ? v.y : (q == 2 ? v.z : v.w));
+}
+
+__global__ void __launch_bounds__(256) divergence4_kernel(
+    float *__restrict__ div, const float *__restrict__ ux, const float *__restrict__ uy,
+    const float *__restrict__ uz, const uint8_t *__restrict__ mask, int nx, int ny, int nz,
+    float dx, unsigned int *__restrict__ max_bits) {
+  const int k = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  unsigned int bits = 0u;  // max |div| of the thread's cells as a bit pattern
+  if (k < nz && j < ny) {
+    const int64_t c = idx3(i, j, k, ny, nz);
+    const uint32_t mw = __ldg(reinterpret_cast<const uint32_t *>(mask + c));
+    float v[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (mw & 0x80808080u) {
+      const int64_t plane = (int64_t)ny * nz;
+      const float4 u1 = __ldg(reinterpret_cast<const float4 *>(ux + c + plane));
+      const float4 u0 = __ldg(reinterpret_cast<const float4 *>(ux + c));
+      const int64_t cy = ((int64_t)i * (ny + 1) + j) * nz + k;
+      const float4 v1 = __ldg(reinterpret_cast<const float4 *>(uy + cy + nz));
+      const float4 v0 = __ldg(reinterpret_cast<const float4 *>(uy + cy));
+      const float *wz = uz + ((int64_t)i * ny + j) * (nz + 1) + k;
+      float w[5];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) w[q] = __ldg(wz + q);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if ((mw >> (8 * q)) & BSP_MFLUID) {
+          const float dudx = __fdiv_rn(__fsub_rn(q4v(u1, q), q4v(u0, q)), dx);
+          const float dvdy = __fdiv_rn(__fsub_rn(q4v(v1, q), q4v(v0, q)), dx);
+          const float dwdz = __fdiv_rn(__fsub_rn(w[q + 1], w[q]), dx);
+          v[q] = __fadd_rn(__fadd_rn(dudx, dvdy), dwdz);
+        }
+      }
+    }
+    *reinterpret_cast<float4 *>(div + c) = make_float4(v[0], v[1], v[2], v[3]);
+    // |div| >= 0, so its bit pattern orders like the value (a NaN orders
+    // above every number, as in the one-cell kernel)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) bits = max(bits, __float_as_uint(fabsf(v[q])));
+  }
+  if (max_bits) {
+    for (int o = 16; o > 0; o >>= 1) bits = max(bits, __shfl_xor_sync(0xffffffffu, bits, o));
+    __shared__ unsigned int wmax[8];
+    const int t = threadIdx.y * blockDim.x + threadIdx.x;
+    if ((t & 31) == 0) wmax[t >> 5] = bits;
+    __syncthreads();
+    if (t == 0) {
+      unsigned int m = 0;
+      for (int w = 0; w < (int)(blockDim.x * blockDim.y) / 32; ++w) m = max(m, wmax[w]);
+      atomicMax(max_bits, m);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) gradient4_kernel(
+    float *__restrict__ ux, float *__restrict__ uy, float *__restrict__ uz,
+    const float *__restrict__ p, const uint8_t *__restrict__ mask, int nx, int ny, int nz,
+    float dx, float dtr) {
+  const int k = (blockIdx.x * blockDim.x + threadIdx.x) * 4;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y;
+  const int i = blockIdx.z;
+  if (k >= nz || j >= ny) return;
+  const int64_t c = idx3(i, j, k, ny, nz);
+  const uint32_t mw = __ldg(reinterpret_cast<const uint32_t *>(mask + c));
+  if (!(mw & 0x80808080u)) return;
+  const int64_t plane = (int64_t)ny * nz;
+  const float4 pc = __ldg(reinterpret_cast<const float4 *>(p + c));
+  auto grad = [&](float f, float pa, float pb) {
+    return __fsub_rn(f, __fdiv_rn(__fmul_rn(dtr, __fsub_rn(pa, pb)), dx));
+  };
+  // a face is updated when both cells beside it are fluid (bit 7 of both bytes)
+  if (i >= 1) {
+    const uint32_t both = mw & __ldg(reinterpret_cast<const uint32_t *>(mask + c - plane));
+    if (both & 0x80808080u) {
+      const float4 pi = __ldg(reinterpret_cast<const float4 *>(p + c - plane));
+      float4 *fp = reinterpret_cast<float4 *>(ux + c);
+      const float4 f = *fp;
+      float r[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if ((both >> (8 * q)) & BSP_MFLUID) r[q] = grad(r[q], q4v(pc, q), q4v(pi, q));
+      *fp = make_float4(r[0], r[1], r[2], r[3]);
+    }
+  }
+  if (j >= 1) {
+    const uint32_t both = mw & __ldg(reinterpret_cast<const uint32_t *>(mask + c - nz));
+    if (both & 0x80808080u) {
+      const float4 pj = __ldg(reinterpret_cast<const float4 *>(p + c - nz));
+      float4 *fp = reinterpret_cast<float4 *>(uy + ((int64_t)i * (ny + 1) + j) * nz + k);
+      const float4 f = *fp;
+      float r[4] = {f.x, f.y, f.z, f.w};
+#pragma unroll
+      for (int q = 0; q < 4; ++q)
+        if ((both >> (8 * q)) & BSP_MFLUID) r[q] = grad(r[q], q4v(pc, q), q4v(pj, q));
+      *fp = make_float4(r[0], r[1], r[2], r[3]);
+    }
+  }
+  // k faces: byte q of mk is the cell below cell q (for q = 0 the byte before
+  // the word; no face below k = 0)
+  const uint32_t below0 = k >= 1 ? (uint32_t)__ldg(mask + c - 1) : 0u;
+  const uint32_t both = mw & ((mw << 8) | below0);
+  if (both & 0x80808080u) {
+    const float pkm = k >= 1 ? __ldg(p + c - 1) : 0.0f;
+    const float pb[4] = {pkm, pc.x, pc.y, pc.z};
+    float *fz = uz + ((int64_t)i * ny + j) * (nz + 1) + k;
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+      if ((both >> (8 * q)) & BSP_MFLUID) fz[q] = grad(fz[q], q4v(pc, q), pb[q]);
+  }
+}
+
+static inline bool aligned16_all(const void *a, const void *b, const void *c) {
+  return (((uintptr_t)a | (uintptr_t)b | (uintptr_t)c) & 15u) == 0;
+}
+
 cudaError_t divergence_impl(float *div, const float *ux, const float *uy, const float *uz,
                             const uint8_t *mask, int nx, int ny, int nz, float dx,
                             float *max_abs_div, cudaStream_t s) {
@@ -174,9 +296,16 @@ cudaError_t divergence_impl(float *div, const float *ux, const float *uy, const 
     cudaError_t e = cudaMemsetAsync(max_abs_div, 0, sizeof(float), s);
     if (e != cudaSuccess) return e;
   }
+  ProfScope ps(PROF_PROJ, s);
+  if (nz % 4 == 0 && aligned16_all(div, ux, uy) && ((uintptr_t)mask & 3u) == 0) {
+    dim3 block(32, 8);
+    dim3 grid((nz / 4 + 31) / 32, (ny + 7) / 8, nx);
+    divergence4_kernel<<<grid, block, 0, s>>>(div, ux, uy, uz, mask, nx, ny, nz, dx,
+                                              reinterpret_cast<unsigned int *>(max_abs_div));
+    return cudaGetLastError();
+  }
   dim3 block(128, 2);
   dim3 grid((nz + 127) / 128, (ny + 1) / 2, nx);
-  ProfScope ps(PROF_PROJ, s);
   divergence_kernel<<<grid, block, 0, s>>>(div, ux, uy, uz, mask, nx, ny, nz, dx,
                                            reinterpret_cast<unsigned int *>(max_abs_div));
   return cudaGetLastError();
@@ -185,9 +314,15 @@ cudaError_t divergence_impl(float *div, const float *ux, const float *uy, const 
 cudaError_t gradient_impl(float *ux, float *uy, float *uz, const float *p, const uint8_t *mask,
                           int nx, int ny, int nz, float dx, float dt, float rho, cudaStream_t s) {
   const float dtr = dt / rho;
+  ProfScope ps(PROF_PROJ, s);
+  if (nz % 4 == 0 && aligned16_all(p, ux, uy) && ((uintptr_t)mask & 3u) == 0) {
+    dim3 block(32, 8);
+    dim3 grid((nz / 4 + 31) / 32, (ny + 7) / 8, nx);
+    gradient4_kernel<<<grid, block, 0, s>>>(ux, uy, uz, p, mask, nx, ny, nz, dx, dtr);
+    return cudaGetLastError();
+  }
   dim3 block(128, 2);
   dim3 grid((nz + 127) / 128, (ny + 1) / 2, nx);
-  ProfScope ps(PROF_PROJ, s);
   gradient_kernel<<<grid, block, 0, s>>>(ux, uy, uz, p, mask, nx, ny, nz, dx, dtr);
   return cudaGetLastError();
 }

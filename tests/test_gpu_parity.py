@@ -238,8 +238,15 @@ def test_spmv_and_diag_bit_exact(cuda, seed, shape):
     assert np.array_equal(bits(host(z)), bits(O.diag_inverse(p, mat)))
 
 
-def test_divergence_gradient_no_slip_bit_exact(cuda):
-    mat = S.pot_mat(S.PotSpec(24, 20, 28, 8, 2, 20, 3, 8))
+@pytest.mark.parametrize("spec", [S.PotSpec(24, 20, 28, 8, 2, 20, 3, 8),
+                                  S.PotSpec(24, 20, 30, 8, 2, 20, 3, 8),
+                                  S.PotSpec(16, 40, 132, 6, 2, 100, 3, 6)],
+                         ids=["four-cell", "one-cell", "four-cell-partial"])
+def test_divergence_gradient_no_slip_bit_exact(cuda, spec):
+    """Divergence (with max|div|), gradient subtraction and no-slip against the
+    oracle, bit for bit: nz % 4 == 0 takes the four-cell kernels (a partial
+    last block of k quads at nz = 132), nz = 30 the one-cell ones."""
+    mat = S.pot_mat(spec)
     rng = np.random.default_rng(4)
     nx, ny, nz = mat.shape
     ux = rng.standard_normal((nx + 1, ny, nz)).astype(np.float32)
