@@ -56,6 +56,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "bsp_common.cuh"
@@ -848,6 +849,49 @@ __global__ void prolong_kernel(float *__restrict__ p, const float *__restrict__ 
   }
 }
 
+// The same interpolation for four consecutive k cells per thread (nz % 4 ==
+// 0, p 16-byte aligned): the row and column terms and the index divisions once
+// per four cells, the mask read as one word, p written as one float4.
+__global__ void prolong4_kernel(float *__restrict__ p, const float *__restrict__ pc,
+                                const uint8_t *__restrict__ mask, int nx, int ny, int nz) {
+  const int cx = nx / 2, cy = ny / 2, cz = nz / 2;
+  const unsigned nzq = (unsigned)nz / 4u;
+  const unsigned nq = (unsigned)nx * (unsigned)ny * nzq;
+  for (unsigned u = blockIdx.x * blockDim.x + threadIdx.x; u < nq; u += gridDim.x * blockDim.x) {
+    const unsigned v = 4u * u;
+    const uint32_t mw = *reinterpret_cast<const uint32_t *>(mask + v);
+    float o[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if (mw & 0x80808080u) {
+      const unsigned r = u / nzq;
+      const int k = 4 * (int)(u - r * nzq);
+      const unsigned ii = r / (unsigned)ny;
+      const int j = (int)(r - ii * (unsigned)ny), i = (int)ii;
+      int i0, i1, j0, j1;
+      float wi, wj;
+      lin2(i, cx, i0, i1, wi);
+      lin2(j, cy, j0, j1, wj);
+      const float *r00 = pc + ((unsigned)i0 * (unsigned)cy + (unsigned)j0) * (unsigned)cz;
+      const float *r01 = pc + ((unsigned)i0 * (unsigned)cy + (unsigned)j1) * (unsigned)cz;
+      const float *r10 = pc + ((unsigned)i1 * (unsigned)cy + (unsigned)j0) * (unsigned)cz;
+      const float *r11 = pc + ((unsigned)i1 * (unsigned)cy + (unsigned)j1) * (unsigned)cz;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (!((mw >> (8 * q)) & BSP_CLASS_FLUID)) continue;
+        int k0, k1;
+        float wk;
+        lin2(k + q, cz, k0, k1, wk);
+        const float c00 = wk * __ldg(r00 + k0) + (1.0f - wk) * __ldg(r00 + k1);
+        const float c01 = wk * __ldg(r01 + k0) + (1.0f - wk) * __ldg(r01 + k1);
+        const float c10 = wk * __ldg(r10 + k0) + (1.0f - wk) * __ldg(r10 + k1);
+        const float c11 = wk * __ldg(r11 + k0) + (1.0f - wk) * __ldg(r11 + k1);
+        const float c0 = wj * c00 + (1.0f - wj) * c01, c1 = wj * c10 + (1.0f - wj) * c11;
+        o[q] = wi * c0 + (1.0f - wi) * c1;
+      }
+    }
+    *reinterpret_cast<float4 *>(p + v) = make_float4(o[0], o[1], o[2], o[3]);
+  }
+}
+
 // s = RMS of div over the fluid cells (1 when there is none or it is 0): the
 // network's input scale, on the device.  Per-block FP64 partials of
 // (sum div^2, count) in a fixed order, then one block sums them in order.
@@ -886,13 +930,20 @@ __global__ void __launch_bounds__(256) rms_partial_kernel(double *__restrict__ p
 }
 __global__ void rms_final_kernel(float *__restrict__ s_out, const double *__restrict__ part,
                                  int nb) {
+  // one warp: lane l sums blocks l, l + 32, ..., then a fixed shuffle tree
   double a = 0.0, c = 0.0;
-  for (int b = 0; b < nb; ++b) {
+  for (int b = threadIdx.x; b < nb; b += 32) {
     a += part[2 * b];
     c += part[2 * b + 1];
   }
-  const double r = c > 0.0 ? sqrt(a / c) : 0.0;
-  s_out[0] = r > 0.0 ? (float)r : 1.0f;
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  if (threadIdx.x == 0) {
+    const double r = c > 0.0 ? sqrt(a / c) : 0.0;
+    s_out[0] = r > 0.0 ? (float)r : 1.0f;
+  }
 }
 
 // Energy-optimal scale of a starting pressure: with b = factor div on fluid
@@ -1182,7 +1233,7 @@ extern "C" int bsp_unet_input_scale(float *s_dev, const float *div, const uint8_
   ProfScope ps(PROF_UNET, s);
   rms_partial_kernel<<<RMS_BLOCKS, 256, 0, s>>>(static_cast<double *>(workspace), div, mask,
                                                 (int64_t)nx * ny * nz);
-  rms_final_kernel<<<1, 1, 0, s>>>(s_dev, static_cast<const double *>(workspace), RMS_BLOCKS);
+  rms_final_kernel<<<1, 32, 0, s>>>(s_dev, static_cast<const double *>(workspace), RMS_BLOCKS);
   return (int)cudaGetLastError();
 }
 
@@ -1249,7 +1300,10 @@ extern "C" int bsp_unet_prolong(float *p, const float *pc, const uint8_t *mask, 
   if ((int64_t)nx * ny * nz >= ((int64_t)1 << 31)) return BSP_ERR_SHAPE;
   if ((const void *)p == (const void *)pc) return BSP_ERR_ALIAS;
   ProfScope ps(PROF_UNET, s);
-  prolong_kernel<<<grid_for((int64_t)nx * ny * nz), 256, 0, s>>>(p, pc, mask, nx, ny, nz);
+  if (nz % 4 == 0 && ((uintptr_t)p & 15u) == 0 && ((uintptr_t)mask & 3u) == 0)
+    prolong4_kernel<<<grid_for((int64_t)nx * ny * nz / 4), 256, 0, s>>>(p, pc, mask, nx, ny, nz);
+  else
+    prolong_kernel<<<grid_for((int64_t)nx * ny * nz), 256, 0, s>>>(p, pc, mask, nx, ny, nz);
   return (int)cudaGetLastError();
 }
 
@@ -1284,7 +1338,9 @@ extern "C" int bsp_unet_energy_scale_keep(float *p, const float *Ap, const float
   ProfScope ps(PROF_UNET, s);
   energy_partial_kernel<<<RMS_BLOCKS, 256, 0, s>>>(static_cast<double *>(workspace), p, Ap, div,
                                                    mask, n, factor);
-  energy_scale_kernel<<<grid_for((n + 3) / 4), 256, 0, s>>>(
+  // every block first sums the partials: two blocks per SM, grid-stride
+  const int sblocks = std::min(grid_for((n + 3) / 4), 2 * num_sms_dev());
+  energy_scale_kernel<<<sblocks, 256, 0, s>>>(
       p, static_cast<const double *>(workspace), RMS_BLOCKS, n, keep_below, gamma_dev,
       relres_dev);
   return (int)cudaGetLastError();

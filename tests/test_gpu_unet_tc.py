@@ -352,3 +352,40 @@ def test_warm_start_guess_graph_and_solve(cuda, mode):
     res = solver.solve(dd, dx, dt, rho, tol=1e-6, p=a.clone(), warm_start=True)
     assert res.status == 0
     assert O.rel_residual64(res.p64, div, mat, dx, dt, rho) <= 1.0001e-6
+
+
+@pytest.mark.parametrize("dims", [(8, 12, 16), (6, 10, 14)], ids=["four-cell", "one-cell"])
+def test_prolong_matches_trilinear(cuda, dims):
+    """bsp_unet_prolong (the four-cell kernel when nz % 4 == 0, the one-cell one
+    otherwise): every fluid fine cell gets the trilinear interpolation of the
+    coarse field at fine position / 2 - 1/4 (clamped), non-fluid cells 0."""
+    from boilingsim_b200 import fluid as F
+
+    rng = np.random.default_rng(5)
+    nx, ny, nz = dims
+    mat = np.where(rng.random(dims) < 0.7, 0, 2).astype(np.int32)
+    mask = F.cell_mask(torch.as_tensor(mat).cuda())
+    pc = rng.standard_normal((nx // 2, ny // 2, nz // 2)).astype(np.float32)
+    out = torch.full(dims, 7.0, device="cuda")
+    call("bsp_unet_prolong", ptr(out), ptr(torch.as_tensor(pc).cuda()), ptr(mask), *dims, 0)
+
+    def lin(d, nc):
+        if d & 1:
+            return d >> 1, min((d >> 1) + 1, nc - 1), 0.75
+        return max((d >> 1) - 1, 0), d >> 1, 0.25
+
+    want = np.zeros(dims, np.float64)
+    for i in range(nx):
+        i0, i1, wi = lin(i, nx // 2)
+        for j in range(ny):
+            j0, j1, wj = lin(j, ny // 2)
+            for k in range(nz):
+                if mat[i, j, k] != 0:
+                    continue
+                k0, k1, wk = lin(k, nz // 2)
+                c = lambda a, b: wk * pc[a, b, k0] + (1 - wk) * pc[a, b, k1]  # noqa: E731
+                want[i, j, k] = wi * (wj * c(i0, j0) + (1 - wj) * c(i0, j1)) + \
+                    (1 - wi) * (wj * c(i1, j0) + (1 - wj) * c(i1, j1))
+    got = out.cpu().numpy()
+    assert np.all(got[mat != 0] == 0.0)
+    assert np.allclose(got, want, rtol=1e-5, atol=1e-6)
