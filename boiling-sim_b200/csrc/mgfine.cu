@@ -1007,6 +1007,17 @@ struct TDownU {
   __device__ void skip() const { partials[block_linear()] = 0.0; }
 };
 
+// TDownU compiled for four CTAs per SM (registers capped at 48 a thread).
+template <class T>
+struct TDownU4 : TDownU<T> {
+  static constexpr int MIN_BLOCKS = 4;
+};
+
+// BSP_TUNE_DOWNU_BLOCKS: CTAs per SM the fused update + restriction kernel is
+// compiled for, 3 (default) or 4.  Measured at 384x384x256: 11.53 ms per
+// solve with 3, 11.60 with 4 (48 registers and a small spill).
+int g_downu_blocks = 3;
+
 constexpr int align128(int b) { return (b + 127) / 128 * 128; }
 
 // Every TMA destination starts on a 128-byte boundary.
@@ -1807,18 +1818,21 @@ bool launch_fine_down_update(const Level<T> &f, const Level<T> &c, T *r_out, flo
     op.nz1 = c.nz;
     return launch_tma<T>(op, maps, f.nx, f.ny, f.nz, f.tiles, st, s);
   }
-  TDownU<T> op{};
-  op.mask1 = c.mask;
-  op.r1 = c.r;
-  op.r_out = r_out;
-  op.e = e;
-  op.ps = ps;
-  op.partials = partials;
-  op.nx = f.nx;
-  op.ny = f.ny;
-  op.ny1 = c.ny;
-  op.nz1 = c.nz;
-  return launch_tma<T>(op, maps, f.nx, f.ny, f.nz, f.tiles, st, s);
+  auto run = [&](auto op) {
+    op.mask1 = c.mask;
+    op.r1 = c.r;
+    op.r_out = r_out;
+    op.e = e;
+    op.ps = ps;
+    op.partials = partials;
+    op.nx = f.nx;
+    op.ny = f.ny;
+    op.ny1 = c.ny;
+    op.nz1 = c.nz;
+    return launch_tma<T>(op, maps, f.nx, f.ny, f.nz, f.tiles, st, s);
+  };
+  if (g_downu_blocks == 4) return run(TDownU4<T>{});
+  return run(TDownU<T>{});
 }
 
 // The FP64 residual keeps the 8-warp column layout (no operand to share: x

@@ -81,6 +81,7 @@ extern int g_fine_ctas;  // BSP_TUNE_FINE_CTAS (mgfine.cu)
 extern bool g_pdl;       // BSP_TUNE_PDL (mgfine.cu)
 extern int g_coarse_cluster;  // BSP_TUNE_COARSE_CLUSTER (mgcoarse.cu)
 extern int g_cluster_tail_cells;  // BSP_TUNE_CLUSTER_TAIL_CELLS (mgcoarse.cu)
+extern int g_downu_blocks;        // BSP_TUNE_DOWNU_BLOCKS (mgfine.cu)
 extern bool g_coarse_cluster_tail_smem;  // BSP_TUNE_CLUSTER_TAIL (mgcoarse.cu)
 extern int g_tri_cpc;  // BSP_TUNE_TRI_CPC (mgfine.cu)
 // BSP_TUNE_FUSE_UPDATE: CG update fused into the next level-0 restriction
@@ -1655,6 +1656,7 @@ static void key_params(GraphKey &k, const BspSolveParams *p) {
   k.v.push_back((uintptr_t)g_pdl);
   k.v.push_back((uintptr_t)g_coarse_cluster);
   k.v.push_back((uintptr_t)g_cluster_tail_cells);
+  k.v.push_back((uintptr_t)g_downu_blocks);
   k.v.push_back((uintptr_t)g_coarse_cluster_tail_smem);
   k.v.push_back((uintptr_t)g_fuse_update_enabled);
   k.v.push_back((uintptr_t)g_fine_bi);

@@ -667,6 +667,7 @@ extern int g_fine_ctas;
 extern bool g_pdl;
 extern int g_coarse_cluster;
 extern int g_cluster_tail_cells;
+extern int g_downu_blocks;
 extern bool g_coarse_cluster_tail_smem;
 namespace utc {
 extern int g_utc_nepi;
@@ -722,6 +723,10 @@ extern "C" int bsp_set_tuning(int key, int value) {
     case BSP_TUNE_CONV_EPILOGUE:
       if (value < 0 || value > 4) return BSP_ERR_ARG;
       bsp::utc::g_utc_nepi = value;
+      return BSP_OK;
+    case BSP_TUNE_DOWNU_BLOCKS:
+      if (value != 3 && value != 4) return BSP_ERR_ARG;
+      bsp::g_downu_blocks = value;
       return BSP_OK;
     case BSP_TUNE_CLUSTER_TAIL_CELLS:
       if (value < 0 || value > (1 << 20)) return BSP_ERR_ARG;

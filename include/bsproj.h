@@ -91,6 +91,8 @@ extern "C" {
                                       0 off, 2 (default) or 3 */
 #define BSP_TUNE_CLUSTER_TAIL_CELLS 27 /* cluster coarse cycle: levels of at most this many cells
                                           run in its CTA 0 alone (default 16384) */
+#define BSP_TUNE_DOWNU_BLOCKS 28  /* CTAs per SM of the fused CG update + restriction: 3 (default)
+                                     or 4 (48 registers a thread) */
 
 /* ------------------------------------------------------------------ */
 /* 1. reference-compatible launchers                                   */
