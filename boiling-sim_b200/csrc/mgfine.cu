@@ -1357,6 +1357,7 @@ __global__ void __launch_bounds__(256) resid64_col_kernel(int nx, int ny, int nz
                                                           float *e, double *partials,
                                                           const SolverState *st) {
   if (st->done) return;
+  if (!WRITE && st->norm_cached) return;  // x = 0: the ||b|| pass's partials stand
   if (tiles && !tiles[block_linear()]) {
     // no fluid: residual 0, and rhat and e are already 0 on these cells
     if (threadIdx.x == 0) {

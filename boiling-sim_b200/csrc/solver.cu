@@ -570,6 +570,7 @@ __global__ void __launch_bounds__(256) residual64_kernel(int nx, int ny, int nz,
                                                          T *rhat, float *e, double *partials,
                                                          const SolverState *st) {
   if (st->done) return;
+  if (!WRITE && st->norm_cached) return;  // x = 0: the ||b|| pass's partials stand
   const double scale = st->scale;
   RowIter it(nx, ny);
   const int lane = threadIdx.x & 31;
@@ -632,6 +633,7 @@ __global__ void __launch_bounds__(RED_THREADS) outer_check_kernel(SolverState *s
   const double rr = reduce_slot(partials, 0, nblocks, false);
   const double rmax = reduce_slot(partials, 1, nblocks, true);
   if (threadIdx.x != 0) return;
+  st->norm_cached = 0;  // later outer passes see a nonzero iterate
   if (st->dev_error) {
     st->status = BSP_ERR_TIMEOUT;
     st->done = 1;
@@ -1197,22 +1199,34 @@ __device__ __forceinline__ bool conv_vec(const void *f, const void *d, const uin
   return (n & 3) == 0 && ((((uintptr_t)f | (uintptr_t)d) & 15u) == 0) &&
          (((uintptr_t)m & 3u) == 0);
 }
-__global__ void f32_to_f64_kernel(int64_t n, const float *a, double *b, const uint8_t *mask) {
+// With st, a fluid value other than 0 clears st->norm_cached (the first outer
+// residual is then not the ||b|| pass's).
+__global__ void f32_to_f64_kernel(int64_t n, const float *a, double *b, const uint8_t *mask,
+                                  SolverState *st) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  int nonzero = 0;
   if (conv_vec(a, b, mask, n)) {
     for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < n / 4; q += stride) {
       const uint32_t mw = *reinterpret_cast<const uint32_t *>(mask + 4 * q);
       const float4 v = *reinterpret_cast<const float4 *>(a + 4 * q);
+      const double d0 = (mw & BSP_MFLUID) ? (double)v.x : 0.0;
+      const double d1 = ((mw >> 8) & BSP_MFLUID) ? (double)v.y : 0.0;
+      const double d2 = ((mw >> 16) & BSP_MFLUID) ? (double)v.z : 0.0;
+      const double d3 = ((mw >> 24) & BSP_MFLUID) ? (double)v.w : 0.0;
       double2 *o = reinterpret_cast<double2 *>(b + 4 * q);
-      o[0] = make_double2((mw & BSP_MFLUID) ? (double)v.x : 0.0,
-                          ((mw >> 8) & BSP_MFLUID) ? (double)v.y : 0.0);
-      o[1] = make_double2(((mw >> 16) & BSP_MFLUID) ? (double)v.z : 0.0,
-                          ((mw >> 24) & BSP_MFLUID) ? (double)v.w : 0.0);
+      o[0] = make_double2(d0, d1);
+      o[1] = make_double2(d2, d3);
+      nonzero |= (d0 != 0.0) | (d1 != 0.0) | (d2 != 0.0) | (d3 != 0.0);
     }
-    return;
+  } else {
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += stride) {
+      const double d = mcls(mask[c]) == BSP_FLUID ? (double)a[c] : 0.0;
+      b[c] = d;
+      nonzero |= d != 0.0;
+    }
   }
-  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += stride)
-    b[c] = mcls(mask[c]) == BSP_FLUID ? (double)a[c] : 0.0;
+  // a NaN compares unequal to 0, so it also clears the flag
+  if (__syncthreads_or(nonzero) && threadIdx.x == 0 && st) st->norm_cached = 0;
 }
 __global__ void f64_to_f32_kernel(int64_t n, const double *a, float *b, const uint8_t *mask) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -1235,7 +1249,10 @@ __global__ void f64_to_f32_kernel(int64_t n, const double *a, float *b, const ui
 __global__ void __launch_bounds__(RED_THREADS) bnorm_kernel(SolverState *st,
                                                             const double *partials, int nblocks) {
   const double bb = reduce_slot(partials, 0, nblocks, false);
-  if (threadIdx.x == 0) st->b_norm2 = bb;
+  if (threadIdx.x == 0) {
+    st->b_norm2 = bb;
+    st->norm_cached = 1;  // x is zero here; a nonzero warm start clears it
+  }
 }
 
 // Host-side record of workspaces whose multigrid setup (coarse masks, coarsest
@@ -1330,7 +1347,7 @@ int solve_impl(void *ws, const uint8_t *mask, const float *div, float *p_out, in
   }
   if (prm->warm_start && p_out) {
     ProfScope ps(PROF_CONTROL, s);
-    f32_to_f64_kernel<<<nbf, 256, 0, s>>>(cx.n, p_out, x, mask);
+    f32_to_f64_kernel<<<nbf, 256, 0, s>>>(cx.n, p_out, x, mask, cx.st);
   }
   int flag = 0;
   for (int outer = 0; outer <= prm->max_outer; ++outer) {
@@ -1486,7 +1503,7 @@ cudaError_t append_solve(Ctx<T> &cx, const float *div, float *p_out, float dx, f
   (void)nbr;
   const int nres = launch_resid<T>(cx, div, x, bscale, nullptr, nullptr, false, cs);
   bnorm_kernel<<<1, RED_THREADS, 0, cs>>>(st, cx.partials, nres);
-  if (prm->warm_start && p_out) f32_to_f64_kernel<<<nbf, 256, 0, cs>>>(cx.n, p_out, x, mask);
+  if (prm->warm_start && p_out) f32_to_f64_kernel<<<nbf, 256, 0, cs>>>(cx.n, p_out, x, mask, st);
   if ((e = seg_end(cs, leaves)) != cudaSuccess) return e;
   cudaGraphConditionalHandle ho, hi;
   if ((e = cudaGraphConditionalHandleCreate(&ho, g, 1, cudaGraphCondAssignDefault)) != cudaSuccess)

@@ -39,6 +39,10 @@ struct SolverState {
   // themselves so every WHILE node ends even if other state went wrong
   int guard_inner, guard_outer;
   int tail_count;  // CTAs of the current level-0 kernel done (its last CTA runs the scalar update)
+  // 1 from the ||b|| pass until the first outer check while the iterate is
+  // still zero: the partials of that pass are the first outer residual's, so
+  // the norm pass before the first outer check returns at entry
+  int norm_cached;
 };
 
 // The scalar updates that follow a level-0 kernel's FP64 partial sums: by a
