@@ -1378,20 +1378,23 @@ __global__ void __launch_bounds__(256) resid64_col_kernel(int nx, int ny, int nz
   const D4 z4{0, 0, 0, 0};
   int64_t o = act ? (int64_t)i0 * plane + (int64_t)j * nz + k : 0;
   D4 xm = z4, xc = z4;
-  if (act && i0 > 0) xm = ld4d(x, o - plane);
-  if (act) xc = ld4d(x, o);
+  // while the iterate is known to be zero its loads are skipped: the
+  // operands keep their +0.0 defaults, the values the zeroed x holds
+  const bool lx = act && !st->x_zero;
+  if (lx && i0 > 0) xm = ld4d(x, o - plane);
+  if (lx) xc = ld4d(x, o);
   double rr = 0.0, rmax = 0.0;
   for (int i = i0; i < i1; ++i) {
     D4 xn = z4, xjm = z4, xjp = z4;
-    if (act) {
+    if (lx) {
       if (i + 1 < nx) xn = ld4d(x, o + plane);
       if (j > 0) xjm = ld4d(x, o - nz);
       if (j + 1 < ny) xjp = ld4d(x, o + nz);
     }
     double xkm = __shfl_up_sync(0xffffffffu, xc.d, 1);
     double xkp = __shfl_down_sync(0xffffffffu, xc.a, 1);
-    if (lane == 0) xkm = (act && k > 0) ? x[o - 1] : 0.0;
-    if (lane == 31) xkp = (act && k + 4 < nz) ? x[o + 4] : 0.0;
+    if (lane == 0) xkm = (lx && k > 0) ? x[o - 1] : 0.0;
+    if (lane == 31) xkp = (lx && k + 4 < nz) ? x[o + 4] : 0.0;
     if (act) {
       const uint32_t mc = __ldg(reinterpret_cast<const uint32_t *>(mask + o));
       const float4 dv = *reinterpret_cast<const float4 *>(div + o);

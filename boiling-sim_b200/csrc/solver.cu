@@ -609,10 +609,11 @@ __global__ void __launch_bounds__(256) residual64_kernel(int nx, int ny, int nz,
 
 // x += e / scale (FP64); at the end the float output is refreshed too.
 __global__ void xupdate_kernel(int64_t n, double *x, const float *e, float *p_out,
-                               const SolverState *st) {
+                               SolverState *st) {
   if (st->done && !st->finalize) return;
   const double inv = 1.0 / st->scale;
   const bool add = !st->done;
+  if (add && blockIdx.x == 0 && threadIdx.x == 0) st->x_zero = 0;  // read by later passes only
   for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += (int64_t)gridDim.x * blockDim.x) {
     double v = x[c];
@@ -1200,7 +1201,7 @@ __device__ __forceinline__ bool conv_vec(const void *f, const void *d, const uin
          (((uintptr_t)m & 3u) == 0);
 }
 // With st, a fluid value other than 0 clears st->norm_cached (the first outer
-// residual is then not the ||b|| pass's).
+// residual is then not the ||b|| pass's) and st->x_zero.
 __global__ void f32_to_f64_kernel(int64_t n, const float *a, double *b, const uint8_t *mask,
                                   SolverState *st) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -1226,7 +1227,10 @@ __global__ void f32_to_f64_kernel(int64_t n, const float *a, double *b, const ui
     }
   }
   // a NaN compares unequal to 0, so it also clears the flag
-  if (__syncthreads_or(nonzero) && threadIdx.x == 0 && st) st->norm_cached = 0;
+  if (__syncthreads_or(nonzero) && threadIdx.x == 0 && st) {
+    st->norm_cached = 0;
+    st->x_zero = 0;
+  }
 }
 __global__ void f64_to_f32_kernel(int64_t n, const double *a, float *b, const uint8_t *mask) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
@@ -1304,6 +1308,7 @@ int solve_impl(void *ws, const uint8_t *mask, const float *div, float *p_out, in
   h.max_outer = prm->max_outer;
   h.max_inner = prm->max_inner;
   h.scale = 1.0;
+  h.x_zero = 1;  // x is zeroed before the first residual pass
   cudaError_t e = cudaMemcpyAsync(cx.st, &h, sizeof(h), cudaMemcpyHostToDevice, s);
   if (e != cudaSuccess) return (int)e;
   // the coarse-cycle grid barrier starts every solve clean: a barrier that
@@ -1421,6 +1426,7 @@ __global__ void init_state_kernel(SolverState *st, double tol, double eta, int m
   s.max_outer = max_outer;
   s.max_inner = max_inner;
   s.scale = 1.0;
+  s.x_zero = 1;  // x is zeroed before the first residual pass
   *st = s;
 }
 __global__ void arm_inner_kernel(cudaGraphConditionalHandle hi, SolverState *st) {

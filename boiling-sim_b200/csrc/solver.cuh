@@ -43,6 +43,10 @@ struct SolverState {
   // still zero: the partials of that pass are the first outer residual's, so
   // the norm pass before the first outer check returns at entry
   int norm_cached;
+  // 1 while the FP64 iterate x is known to be all zero (x is zeroed before
+  // the first residual pass; cleared by a nonzero warm start and by the
+  // first x update): the residual kernels then skip its loads
+  int x_zero;
 };
 
 // The scalar updates that follow a level-0 kernel's FP64 partial sums: by a
