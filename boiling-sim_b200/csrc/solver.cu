@@ -1192,6 +1192,14 @@ int launch_resid(Ctx<T> &cx, const float *div, const double *x, double bscale, T
   return nbr;
 }
 
+// x is zeroed before the ||b|| pass unless that pass runs on the column kernel
+// (which skips the loads of an iterate known to be zero) and a warm start then
+// writes every cell of x.
+template <class T>
+bool x_needs_zeroing(const Ctx<T> &cx, const float *div, bool warm) {
+  return !(warm && cx.col && ((uintptr_t)div & 15u) == 0);
+}
+
 // FP32 <-> FP64 copies of the iterate on fluid cells (0 elsewhere).  Four
 // cells per step (16-byte float, 2 x 16-byte double and one mask word) when
 // the pointers allow it, one otherwise; the same values either way.
@@ -1338,8 +1346,10 @@ int solve_impl(void *ws, const uint8_t *mask, const float *div, float *p_out, in
   const int nbf = flat_blocks(cx.n);
   const double bscale = -((double)rho * (double)dx * (double)dx) / (double)dt;
   // ||b||^2: a residual pass with x = 0
-  e = cudaMemsetAsync(x, 0, sizeof(double) * cx.n, s);
-  if (e != cudaSuccess) return (int)e;
+  if (x_needs_zeroing<T>(cx, div, prm->warm_start && p_out)) {
+    e = cudaMemsetAsync(x, 0, sizeof(double) * cx.n, s);
+    if (e != cudaSuccess) return (int)e;
+  }
   (void)nbr;
   int nres;
   {
@@ -1505,7 +1515,8 @@ cudaError_t append_solve(Ctx<T> &cx, const float *div, float *p_out, float dx, f
   // every replay starts with a clean coarse-cycle grid barrier (error word,
   // count and generation), whatever an earlier replay left there
   cudaMemsetAsync(cx.base + cx.lo.cctl, 0, 64, cs);
-  cudaMemsetAsync(x, 0, sizeof(double) * cx.n, cs);
+  if (x_needs_zeroing<T>(cx, div, prm->warm_start && p_out))
+    cudaMemsetAsync(x, 0, sizeof(double) * cx.n, cs);
   (void)nbr;
   const int nres = launch_resid<T>(cx, div, x, bscale, nullptr, nullptr, false, cs);
   bnorm_kernel<<<1, RED_THREADS, 0, cs>>>(st, cx.partials, nres);
